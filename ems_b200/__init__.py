@@ -1,0 +1,584 @@
+"""B200-native FDTD time stepping for ems, behind the reference engine's API.
+
+The package mirrors the reference's engine-level interface
+(src/engine/mod.rs ``EngineBuilder`` / ``Engine``, src/engine/boundary/cpml.rs
+``CpmlBoundary``, src/engine/dispersive.rs ``Dispersive``, src/engine/port.rs
+``LumpedPort``, src/engine/excite.rs ``EdgeSource``, src/engine/probe.rs
+``Probe``, src/engine/run.rs ``run_until``): a :class:`Model` restates the
+host-side set-up in C++ (``libems_host.so``) and hands the tables to the
+CUDA engine (``libems_gpu.so``, :class:`Engine`). There is no CPU path: an
+engine needs a CUDA device and raises if the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+# Face order x_min, x_max, y_min, y_max, z_min, z_max (src/fdtd.rs Face::ALL).
+FACES = ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max")
+X, Y, Z = 0, 1, 2
+SOFT_E, HARD_E, SOFT_H, HARD_H = 0, 1, 2, 3
+VOLTAGE, CURRENT = 0, 1
+PEC, PMC = 0, 1
+LORENTZ, DRUDE, DEBYE = 0, 1, 2
+TRAPEZOIDAL, LEAPFROG = 0, 1
+GAUSSIAN = 0
+
+OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE = 1, 2, 3, 4, 5
+
+
+class EngineError(RuntimeError):
+    """An engine call failed; ``status`` is the ems_status code."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"ems status {status}: {msg}")
+        self.status = status
+
+
+# ----------------------------------------------------------------------------
+# ctypes declarations of include/ems_gpu.h and include/ems_host.h
+
+
+class EngineDesc(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_uint64 * 3),
+        ("dt", C.c_double),
+        ("coeff", C.c_void_p * 12),
+        ("n_ops", C.c_size_t),
+        ("ops", C.c_void_p),
+    ]
+
+
+class Stepper(C.Structure):
+    _fields_ = [
+        ("ctx", C.c_void_p),
+        ("run", C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)),
+        ("step_with_energy", C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double))),
+    ]
+
+
+class RunLimits(C.Structure):
+    """``RunLimits`` (src/engine/run.rs:24-53) for :func:`run_until`."""
+
+    _fields_ = [
+        ("max_timesteps", C.c_uint64),
+        ("has_end_criteria", C.c_int),
+        ("energy_ratio", C.c_double),
+        ("check_interval", C.c_uint64),
+        ("has_excitation_end", C.c_int),
+        ("excitation_end", C.c_double),
+        ("dt", C.c_double),
+    ]
+
+
+class RunOutcome(C.Structure):
+    """``RunOutcome`` (src/engine/run.rs:195-214); reason 0 energy decay,
+    1 max timesteps, 2 diverged, 3 engine error."""
+
+    _fields_ = [
+        ("reason", C.c_int),
+        ("steps", C.c_uint64),
+        ("energy", C.c_double),
+        ("max_energy", C.c_double),
+        ("ratio_db", C.c_double),
+        ("checks", C.c_uint64),
+    ]
+
+
+_host = None
+_gpu = None
+
+
+def _u64(v: Sequence[int]):
+    return (C.c_uint64 * len(v))(*[int(x) for x in v])
+
+
+def _f64(v: Sequence[float]):
+    return (C.c_double * len(v))(*[float(x) for x in v])
+
+
+def host_lib() -> C.CDLL:
+    """The host set-up library (built in-tree by ``ems_b200.build``)."""
+    global _host
+    if _host is None:
+        path = os.path.join(HERE, "libems_host.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `python -m ems_b200.build`")
+        L = C.CDLL(path)
+        p, u, d, i, sz = C.c_void_p, C.c_uint64, C.c_double, C.c_int, C.c_size_t
+        sig = {
+            "ems_model_new": (p, [p, sz, p, sz, p, sz]),
+            "ems_model_free": (None, [p]),
+            "ems_model_error": (C.c_char_p, [p]),
+            "ems_model_nodes": (None, [p, p]),
+            "ems_model_material": (i, [p, p, p, p, p]),
+            "ems_cellset_new": (p, [p]),
+            "ems_cellset_free": (None, [p]),
+            "ems_cellset_box": (i, [p, p, p]),
+            "ems_cellset_sphere": (i, [p, p, d]),
+            "ems_cellset_count": (u, [p]),
+            "ems_model_fill": (i, [p, p, i]),
+            "ems_model_pec_edges": (i, [p, i, p, p]),
+            "ems_model_faces": (i, [p, p]),
+            "ems_model_build": (i, [p, d, d]),
+            "ems_model_dt": (d, [p]),
+            "ems_model_courant_limit": (d, [p]),
+            "ems_model_coeff": (p, [p, i]),
+            "ems_model_add_cpml": (i, [p, p, d, d, d, d, i]),
+            "ems_model_cpml_index": (d, [p, i]),
+            "ems_dispersive_new": (p, []),
+            "ems_dispersive_free": (None, [p]),
+            "ems_dispersive_fill": (i, [p, p, p, i, sz, p, p, p, p]),
+            "ems_model_add_dispersive": (i, [p, p, i]),
+            "ems_waveform_value": (d, [i, d, d, d, d]),
+            "ems_waveform_duration": (d, [i, d, d]),
+            "ems_model_add_lumped_port": (i, [p, i, p, p, d, i, d, d, d, u]),
+            "ems_model_add_source": (i, [p, i, sz, p, p, p, i, d, d, u]),
+            "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
+            "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
+            "ems_model_desc": (p, [p]),
+            "ems_dft": (None, [d, d, p, sz, p, sz, p, p]),
+            "ems_drive": (i, [p, p, p]),
+            "ems_const_eps0": (d, []),
+            "ems_const_mu0": (d, []),
+            "ems_const_c0": (d, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _host = L
+    return _host
+
+
+GPU_SYMBOLS = {
+    "ems_gpu_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "ems_gpu_destroy": (C.c_int, [C.c_void_p]),
+    "ems_gpu_run": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ems_gpu_step_with_energy": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_timestep": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_download_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "ems_gpu_upload_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "ems_gpu_samples": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "ems_gpu_last_error": (C.c_char_p, [C.c_void_p]),
+    "ems_gpu_launch_count": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+}
+
+
+def gpu_lib() -> C.CDLL:
+    """The CUDA engine library. Raises if it is missing: there is no CPU path."""
+    global _gpu
+    if _gpu is None:
+        path = os.path.join(HERE, "libems_gpu.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: the CUDA engine is not built (python -m ems_b200.build)")
+        L = C.CDLL(path)
+        for name, (res, args) in GPU_SYMBOLS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _gpu = L
+    return _gpu
+
+
+def eps0() -> float:
+    return host_lib().ems_const_eps0()
+
+
+def mu0() -> float:
+    return host_lib().ems_const_mu0()
+
+
+def c0() -> float:
+    return host_lib().ems_const_c0()
+
+
+def waveform_value(f0: float, fc: float, t: float, dt: float = 0.0) -> float:
+    """``Waveform::Gaussian{f0, fc}.value(t, dt)`` (src/waveform.rs:455-463)."""
+    return host_lib().ems_waveform_value(GAUSSIAN, f0, fc, t, dt)
+
+
+def waveform_duration(f0: float, fc: float) -> float:
+    """``Waveform::duration``: 2T of the Gaussian (src/waveform.rs:485-492)."""
+    return host_lib().ems_waveform_duration(GAUSSIAN, f0, fc)
+
+
+# ----------------------------------------------------------------------------
+# host-side model (the reference's EngineBuilder + operator set-up)
+
+
+class CellSet:
+    """A set of cells (boxes, spheres) for materials and dispersive media."""
+
+    def __init__(self, model: "Model"):
+        self._lib = host_lib()
+        self._p = self._lib.ems_cellset_new(model._p)
+
+    def box(self, lo: Sequence[int], hi: Sequence[int]) -> "CellSet":
+        if self._lib.ems_cellset_box(self._p, _u64(lo), _u64(hi)) != 0:
+            raise ValueError(f"cell box {lo}..{hi} outside the grid")
+        return self
+
+    def sphere(self, centre: Sequence[float], radius: float) -> "CellSet":
+        self._lib.ems_cellset_sphere(self._p, _f64(centre), float(radius))
+        return self
+
+    def count(self) -> int:
+        return int(self._lib.ems_cellset_count(self._p))
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            self._lib.ems_cellset_free(self._p)
+            self._p = None
+
+
+@dataclass
+class Pole:
+    """``Pole`` (src/engine/dispersive.rs:211-244), frequencies in rad/s."""
+
+    kind: int
+    p1: float
+    p2: float = 0.0
+    p3: float = 0.0
+
+    @staticmethod
+    def lorentz(omega_p: float, omega_0: float, gamma: float) -> "Pole":
+        return Pole(LORENTZ, omega_p, omega_0, gamma)
+
+    @staticmethod
+    def drude(omega_p: float, gamma: float) -> "Pole":
+        return Pole(DRUDE, omega_p, gamma)
+
+    @staticmethod
+    def debye(delta_eps: float, tau: float) -> "Pole":
+        return Pole(DEBYE, delta_eps, tau)
+
+
+class Dispersive:
+    """``Dispersive`` (src/engine/dispersive.rs:1800-1985): collect poles
+    with :meth:`fill_cells`, install with :meth:`Model.add_dispersive`."""
+
+    def __init__(self):
+        self._lib = host_lib()
+        self._p = self._lib.ems_dispersive_new()
+
+    def fill_cells(self, model: "Model", cells: CellSet, poles: Sequence[Pole], field: int = 0) -> "Dispersive":
+        n = len(poles)
+        kinds = (C.c_int * n)(*[p.kind for p in poles])
+        r = self._lib.ems_dispersive_fill(self._p, model._p, cells._p, field, n, kinds,
+                                          _f64([p.p1 for p in poles]), _f64([p.p2 for p in poles]),
+                                          _f64([p.p3 for p in poles]))
+        if r != 0:
+            raise ValueError("invalid dispersive pole")
+        return self
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            self._lib.ems_dispersive_free(self._p)
+            self._p = None
+
+
+class Model:
+    """A compiled model: grid, materials, coefficients and operator tables.
+
+    Restates ``Engine::builder(grid).materials(m).faces(f).timestep(t).build()``
+    and the operators' set-up (src/engine/mod.rs:325-381) on the host.
+    """
+
+    def __init__(self, x: Sequence[float], y: Sequence[float], z: Sequence[float]):
+        self._lib = host_lib()
+        self._keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z)]
+        a = self._keep
+        self._p = self._lib.ems_model_new(a[0].ctypes.data, len(a[0]), a[1].ctypes.data, len(a[1]),
+                                          a[2].ctypes.data, len(a[2]))
+        if not self._p:
+            raise ValueError("invalid grid lines (need >= 2 strictly increasing finite lines per axis)")
+        self.ops: list[tuple[int, str]] = []
+
+    @staticmethod
+    def uniform(cells: Sequence[int], size: Sequence[float]) -> "Model":
+        """``Grid::uniform`` (src/engine/grid.rs:514-519)."""
+        return Model(*[np.arange(cells[a] + 1, dtype=np.float64) * size[a] for a in range(3)])
+
+    def _check(self, r: int, what: str) -> int:
+        if r < 0 or (what.endswith("!") and r != 0):
+            raise ValueError(f"{what.rstrip('!')}: {self._lib.ems_model_error(self._p).decode()}")
+        return r
+
+    @property
+    def nodes(self) -> tuple[int, int, int]:
+        n = (C.c_uint64 * 3)()
+        self._lib.ems_model_nodes(self._p, n)
+        return (int(n[0]), int(n[1]), int(n[2]))
+
+    def material(self, eps_r=1.0, mu_r=1.0, kappa=0.0, sigma_m=0.0) -> int:
+        """``Material`` (src/engine/material.rs): scalars or per-axis triples."""
+        v = lambda x: _f64(list(x) if hasattr(x, "__len__") else [x] * 3)  # noqa: E731
+        return self._check(self._lib.ems_model_material(self._p, v(eps_r), v(mu_r), v(kappa), v(sigma_m)), "material")
+
+    def cells(self) -> CellSet:
+        return CellSet(self)
+
+    def fill(self, cells: CellSet, mat: int) -> "Model":
+        self._check(self._lib.ems_model_fill(self._p, cells._p, mat), "fill!")
+        return self
+
+    def pec_edges(self, axis: int, lo: Sequence[int], hi: Sequence[int]) -> "Model":
+        self._check(self._lib.ems_model_pec_edges(self._p, axis, _u64(lo), _u64(hi)), "pec_edges!")
+        return self
+
+    def fill_pec_box(self, lo: Sequence[int], hi: Sequence[int]) -> "Model":
+        """``CellMaterials::fill_pec_box`` over the node ranges lo..hi (half-open):
+        every edge of every axis with both ends in the box."""
+        for a in range(3):
+            top = [h - 1 for h in hi]
+            top[a] = hi[a] - 2
+            if top[a] >= lo[a] and all(top[t] >= lo[t] for t in range(3)):
+                self.pec_edges(a, lo, top)
+        return self
+
+    def faces(self, faces: Sequence[int]) -> "Model":
+        self._check(self._lib.ems_model_faces(self._p, (C.c_int * 6)(*faces)), "faces!")
+        return self
+
+    def build(self, courant: float = 0.99, dt: float | None = None) -> "Model":
+        self._check(self._lib.ems_model_build(self._p, courant, dt or 0.0), "build!")
+        return self
+
+    @property
+    def dt(self) -> float:
+        return self._lib.ems_model_dt(self._p)
+
+    @property
+    def courant_limit(self) -> float:
+        return self._lib.ems_model_courant_limit(self._p)
+
+    def coeff(self, lane: int) -> np.ndarray:
+        """Coefficient lane (ca 0-2, cb 3-5, da 6-8, db 9-11), reference layout (a copy)."""
+        n = int(np.prod(self.nodes))
+        p = self._lib.ems_model_coeff(self._p, lane)
+        return np.ctypeslib.as_array((C.c_float * n).from_address(p)).copy().reshape(self.nodes)
+
+    def add_cpml(self, cells: Sequence[int], grading: float = 3.0, sigma_factor: float = 1.0,
+                 kappa_max: float = 1.0, alpha_max: float = 0.0, linear: bool = True) -> int:
+        """``CpmlBoundary::new(engine, faces)`` (src/engine/boundary/cpml.rs:941-951)."""
+        r = self._check(self._lib.ems_model_add_cpml(self._p, _u64(cells), grading, sigma_factor, kappa_max,
+                                                     alpha_max, 1 if linear else 0), "add_cpml")
+        self.ops.append((OP_CPML, "cpml"))
+        return r
+
+    def cpml_index(self, face: int) -> float:
+        return self._lib.ems_model_cpml_index(self._p, face)
+
+    def add_dispersive(self, d: Dispersive, scheme: int = TRAPEZOIDAL) -> int:
+        r = self._check(self._lib.ems_model_add_dispersive(self._p, d._p, scheme), "add_dispersive")
+        self.ops.append((OP_POLES, "poles"))
+        return r
+
+    def add_lumped_port(self, axis: int, lo: Sequence[int], hi: Sequence[int], r: float, f0: float, fc: float,
+                        amplitude: float, n_steps: int) -> int:
+        """``LumpedPort::new(LumpedBox(axis, lo, hi), r).excite_waveform(Gaussian{f0, fc}, amplitude)``."""
+        k = self._check(self._lib.ems_model_add_lumped_port(self._p, axis, _u64(lo), _u64(hi), r, GAUSSIAN, f0, fc,
+                                                            amplitude, n_steps), "add_lumped_port")
+        self.ops.append((OP_LUMPED, "port"))
+        return k
+
+    def add_source(self, kind: int, edges: Sequence[tuple[int, Sequence[int], float]], f0: float, fc: float,
+                   n_steps: int) -> int:
+        """``EdgeSource::new(|t| Gaussian{f0, fc}.value(t)).kind(kind).edge(axis, node, w)...``"""
+        n = len(edges)
+        axis = (C.c_int * n)(*[e[0] for e in edges])
+        nodes = _u64([c for e in edges for c in e[1]])
+        w = _f64([e[2] for e in edges])
+        k = self._check(self._lib.ems_model_add_source(self._p, kind, n, axis, nodes, w, GAUSSIAN, f0, fc, n_steps),
+                        "add_source")
+        self.ops.append((OP_SOURCE, "source"))
+        return k
+
+    def add_source_table(self, kind: int, edges: Sequence[tuple[int, Sequence[int], float]],
+                         amplitude: np.ndarray) -> int:
+        """``EdgeSource::new(f)`` with f sampled by the caller: ``amplitude[n]``
+        is f at the kind's sample time of step n ((n+½)dt for soft E)."""
+        n = len(edges)
+        axis = (C.c_int * n)(*[e[0] for e in edges])
+        nodes = _u64([c for e in edges for c in e[1]])
+        w = _f64([e[2] for e in edges])
+        amp = np.ascontiguousarray(amplitude, dtype=np.float64)
+        k = self._check(self._lib.ems_model_add_source_table(self._p, kind, n, axis, nodes, w, amp.ctypes.data,
+                                                             len(amp)), "add_source_table")
+        self.ops.append((OP_SOURCE, "source"))
+        return k
+
+    def add_source_arrays(self, kind: int, axis: np.ndarray, nodes: np.ndarray, weight: np.ndarray, f0: float,
+                          fc: float, n_steps: int) -> int:
+        """:meth:`add_source` from arrays (n axes, n×3 nodes, n weights)."""
+        axis = np.ascontiguousarray(axis, dtype=np.int32)
+        nodes = np.ascontiguousarray(nodes, dtype=np.uint64)
+        weight = np.ascontiguousarray(weight, dtype=np.float64)
+        k = self._check(self._lib.ems_model_add_source(self._p, kind, len(axis), axis.ctypes.data, nodes.ctypes.data,
+                                                       weight.ctypes.data, GAUSSIAN, f0, fc, n_steps), "add_source")
+        self.ops.append((OP_SOURCE, "source"))
+        return k
+
+    def add_probe(self, quantity: int, entries: Sequence[tuple[int, Sequence[int], float]], interval: int = 1) -> int:
+        """``Probe::new(quantity).entry(axis, node, w)...interval(n)`` (src/engine/probe.rs)."""
+        n = len(entries)
+        axis = (C.c_int * n)(*[e[0] for e in entries])
+        nodes = _u64([c for e in entries for c in e[1]])
+        w = _f64([e[2] for e in entries])
+        k = self._check(self._lib.ems_model_add_probe(self._p, quantity, n, axis, nodes, w, interval), "add_probe")
+        self.ops.append((OP_PROBE, "probe"))
+        return k
+
+    @property
+    def desc(self) -> int:
+        """Address of the ems_engine_desc (valid while the model is alive and unchanged)."""
+        p = self._lib.ems_model_desc(self._p)
+        if not p:
+            raise ValueError("model not built")
+        return p
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            self._lib.ems_model_free(self._p)
+            self._p = None
+
+
+# ----------------------------------------------------------------------------
+# the CUDA engine
+
+
+class Engine:
+    """The CUDA engine for a built :class:`Model` (``Engine``, src/engine/mod.rs)."""
+
+    def __init__(self, model: Model, device: int = 0):
+        self._lib = gpu_lib()
+        self._model = model
+        h = C.c_void_p()
+        st = self._lib.ems_gpu_create(model.desc, device, C.byref(h))
+        if st != 0:
+            raise EngineError(st, "ems_gpu_create failed")
+        self._h = h
+        self.nodes = model.nodes
+        self.dt = model.dt
+
+    def _ck(self, st: int) -> None:
+        if st != 0:
+            raise EngineError(st, self._lib.ems_gpu_last_error(self._h).decode())
+
+    def run(self, n: int) -> None:
+        self._ck(self._lib.ems_gpu_run(self._h, n))
+
+    def step_with_energy(self) -> float:
+        w = C.c_double()
+        self._ck(self._lib.ems_gpu_step_with_energy(self._h, C.byref(w)))
+        return w.value
+
+    @property
+    def timestep(self) -> int:
+        n = C.c_uint64()
+        self._ck(self._lib.ems_gpu_timestep(self._h, C.byref(n)))
+        return n.value
+
+    @property
+    def launches(self) -> int:
+        n = C.c_uint64()
+        self._ck(self._lib.ems_gpu_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def set_schedule(self, s: int) -> None:
+        self._ck(self._lib.ems_gpu_set_schedule(self._h, s))
+
+    def field(self, field: int, axis: int) -> np.ndarray:
+        """``u_component`` (field 0) / ``i_component`` (field 1), shape nodes."""
+        out = np.empty(self.nodes, dtype=np.float32)
+        self._ck(self._lib.ems_gpu_download_field(self._h, field, axis, out.ctypes.data))
+        return out
+
+    def set_field(self, field: int, axis: int, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        self._ck(self._lib.ems_gpu_upload_field(self._h, field, axis, v.ctypes.data))
+
+    def samples(self, op: int, which: int = 0) -> np.ndarray:
+        n = C.c_size_t()
+        self._ck(self._lib.ems_gpu_samples(self._h, op, which, None, 0, C.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        if n.value:
+            self._ck(self._lib.ems_gpu_samples(self._h, op, which, out.ctypes.data, n.value, C.byref(n)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ems_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def run_until(stepper, limits: RunLimits) -> RunOutcome:
+    """``Engine::run_until`` (src/engine/run.rs:221-540) over any object with
+    ``run(n)`` and ``step_with_energy()``, driven by the host's run loop."""
+    lib = host_lib()
+    err: list[BaseException] = []
+
+    @C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
+    def _run(_ctx, n):
+        try:
+            stepper.run(n)
+            return 0
+        except BaseException as e:  # surfaced below
+            err.append(e)
+            return 1
+
+    @C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double))
+    def _swe(_ctx, w):
+        try:
+            w[0] = stepper.step_with_energy()
+            return 0
+        except BaseException as e:
+            err.append(e)
+            return 1
+
+    s = Stepper(None, _run, _swe)
+    out = RunOutcome()
+    lib.ems_drive(C.byref(s), C.byref(limits), C.byref(out))
+    if err:
+        raise err[0]
+    return out
+
+
+def energy_decay_limits(max_steps: int, db: float, dt: float, excitation_end: float | None = None,
+                        interval: int = 50) -> RunLimits:
+    """``RunLimits::new(max).end_criteria(EndCriteria::energy_decay_db(db)).excitation_end(end)``."""
+    return RunLimits(max_steps, 1, 10.0 ** (db / 10.0), interval, 1 if excitation_end is not None else 0,
+                     excitation_end or 0.0, dt)
+
+
+def dft(t0: float, dt: float, x: np.ndarray, freqs: Sequence[float]) -> np.ndarray:
+    """``post::dft`` (src/post/dft.rs:218): Σ x(t0+n·dt)·e^{-j2πf·t_n}·dt."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    f = np.ascontiguousarray(freqs, dtype=np.float64)
+    re = np.empty(len(f))
+    im = np.empty(len(f))
+    host_lib().ems_dft(t0, dt, x.ctypes.data, len(x), f.ctypes.data, len(f), re.ctypes.data, im.ctypes.data)
+    return re + 1j * im
+
+
+def port_result(v: np.ndarray, i: np.ndarray, dt: float, freqs: Sequence[float], z_ref: float = 50.0):
+    """``LumpedPort::analyze`` (src/engine/port.rs:191-205) → (Z_in, S11) per
+    frequency (src/post/port.rs:202-209): V at (n+1)dt, I at (n+½)dt."""
+    V = dft(dt, dt, v, freqs)
+    I = dft(0.5 * dt, dt, i, freqs)
+    z_in = V / I
+    a = (V + z_ref * I) / (2.0 * np.sqrt(z_ref))
+    b = (V - np.conj(z_ref) * I) / (2.0 * np.sqrt(z_ref))
+    return z_in, b / a

@@ -1,0 +1,639 @@
+// engine.cu — the B200 FDTD time-stepping engine behind include/ems_gpu.h.
+//
+// Replaces the reference engine's step (src/engine/pool.rs drive, kernel.rs
+// h_row/e_row, boundary/cpml.rs Slab::apply, dispersive.rs Side::correct,
+// lumped.rs post_e_impl, excite.rs, probe.rs) with CUDA kernels for sm_100a.
+//
+// Arithmetic: every field value is produced by the reference's expression in
+// the reference's order, in IEEE f32 without contraction (built with
+// --fmad=false, denormals kept, results flushed like kernel.rs flush), the
+// branch state in f64 with IEEE division. So fields, probes and port series
+// equal the reference's bit for bit; only the energy sums (a reduction)
+// differ in order.
+//
+// Layout in HBM: the reference's node layout (i*ny + j)*nz + k with the row
+// pitch padded to a multiple of 32 floats (128 B) so every z-row starts on a
+// sector boundary; one array per field component and per coefficient lane.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ems_gpu.h"
+#include "kernels.cuh"
+
+using namespace emsk;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+struct ems_gpu {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Grid g{};
+    double dt = 0.0;
+    uint64_t step = 0;
+    uint64_t launches = 0;
+    int schedule = 0;
+    std::string err;
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    float* u[3] = {nullptr, nullptr, nullptr};
+    float* i[3] = {nullptr, nullptr, nullptr};
+    float* co[12] = {};
+    double* partials = nullptr;   // energy partial sums per block
+    size_t n_partials = 0;
+    double* d_energy = nullptr;   // [0] field part, [1] operator part
+    struct CpmlDev {
+        SlabDev s;
+    };
+    struct PoleDev {
+        PoleSideDev e, h;
+    };
+    struct LumpedDev {
+        LumpedDevT d;
+        int axis = 0;
+        size_t n_edges = 0;
+        size_t n_amp = 0;
+        std::vector<double> amp;   // host copy of the source values (activity test)
+        bool has_src = false, record = false, has_branch = false;
+        uint64_t columns = 0;
+        size_t count = 0, cap = 0;
+        double* rec = nullptr;
+        double* pv = nullptr;
+        double* pi = nullptr;
+    };
+    struct SourceDev {
+        int kind = 0;
+        size_t n = 0;
+        uint32_t* node = nullptr;
+        uint8_t* axis = nullptr;
+        float* weight = nullptr;
+        std::vector<float> amp;
+    };
+    struct ProbeDev {
+        ProbeDevT d;
+        int quantity = 0;
+        uint64_t interval = 1;
+        size_t count = 0, cap = 0;
+        double* values = nullptr;
+    };
+    struct Op {
+        int kind = 0;
+        std::vector<SlabDev> cpml;
+        PoleDev poles;
+        LumpedDev lumped;
+        SourceDev source;
+        ProbeDev probe;
+    };
+    std::vector<Op> ops;
+
+    template <class T>
+    T* alloc(size_t n) {
+        auto b = std::make_unique<DevBuf>();
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        if (cudaMalloc(&b->p, bytes) != cudaSuccess) return nullptr;
+        cudaMemsetAsync(b->p, 0, bytes, stream);
+        b->bytes = bytes;
+        T* p = (T*)b->p;
+        bufs.push_back(std::move(b));
+        return p;
+    }
+    template <class T>
+    T* upload(const T* h, size_t n) {
+        T* d = alloc<T>(n);
+        if (d && n && h) cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, stream);
+        return d;
+    }
+    void release(void* p) {
+        for (size_t k = 0; k < bufs.size(); ++k)
+            if (bufs[k]->p == p) {
+                bufs.erase(bufs.begin() + k);
+                return;
+            }
+    }
+};
+
+namespace {
+
+ems_status fail(ems_gpu* h, ems_status s, const std::string& m) {
+    if (h) h->err = m;
+    return s;
+}
+
+ems_status check(ems_gpu* h, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return EMS_OK;
+    return fail(h, EMS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Remaps a reference node index (i*ny + j)*nz + k to the padded device index.
+inline uint32_t dev_index(const Grid& g, uint64_t idx) {
+    uint64_t k = idx % g.nz;
+    uint64_t r = idx / g.nz;
+    return (uint32_t)(r * g.pitch + k);
+}
+
+// Grows a sample buffer to hold `need` values (copying what it holds).
+ems_status grow(ems_gpu* h, double** buf, size_t count, size_t* cap, size_t need) {
+    if (need <= *cap) return EMS_OK;
+    size_t nc = std::max<size_t>(need, std::max<size_t>(1024, *cap * 2));
+    double* nb = h->alloc<double>(nc);
+    if (!nb) return fail(h, EMS_ERR_NOMEM, "sample buffer");
+    if (*buf && count) cudaMemcpyAsync(nb, *buf, count * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+    if (*buf) {
+        cudaStreamSynchronize(h->stream);
+        h->release(*buf);
+    }
+    *buf = nb;
+    *cap = nc;
+    return EMS_OK;
+}
+
+ems_status make_side(ems_gpu* h, const ems_pole_side& t, PoleSideDev& d) {
+    d.n_edges = t.n_edges;
+    d.n_poles = t.n_poles;
+    if (!t.n_edges) return EMS_OK;
+    if (!t.axis || !t.node || !t.sum_inv_z || !t.pole_end || (t.n_poles && (!t.kind || !t.a || !t.inv_c || !t.inv_z || !t.half_l)))
+        return fail(h, EMS_ERR_INVALID, "pole table: missing array");
+    std::vector<uint32_t> node(t.n_edges);
+    uint32_t prev = 0;
+    for (size_t e = 0; e < t.n_edges; ++e) {
+        if (t.node[e] >= h->g.n || t.axis[e] > 2) return fail(h, EMS_ERR_INVALID, "pole table: edge outside the grid");
+        if (t.pole_end[e] < prev || t.pole_end[e] - prev > kMaxPoles)
+            return fail(h, EMS_ERR_INVALID, "pole table: bad pole_end (at most 16 poles per edge)");
+        prev = t.pole_end[e];
+        node[e] = dev_index(h->g, t.node[e]);
+    }
+    if (prev != t.n_poles) return fail(h, EMS_ERR_INVALID, "pole table: pole_end does not end at n_poles");
+    d.axis = h->upload(t.axis, t.n_edges);
+    d.node = h->upload(node.data(), t.n_edges);
+    d.sum_inv_z = h->upload(t.sum_inv_z, t.n_edges);
+    d.pole_end = h->upload(t.pole_end, t.n_edges);
+    d.kind = h->upload(t.kind, t.n_poles);
+    d.a = h->upload(t.a, t.n_poles);
+    d.inv_c = h->upload(t.inv_c, t.n_poles);
+    d.inv_z = h->upload(t.inv_z, t.n_poles);
+    d.half_l = h->upload(t.half_l, t.n_poles);
+    d.prev = h->alloc<float>(t.n_edges);
+    d.j = h->alloc<double>(t.n_poles);
+    d.q = h->alloc<double>(t.n_poles);
+    if (!d.axis || !d.node || !d.sum_inv_z || !d.pole_end || !d.kind || !d.a || !d.inv_c || !d.inv_z || !d.half_l ||
+        !d.prev || !d.j || !d.q)
+        return fail(h, EMS_ERR_NOMEM, "pole table");
+    return EMS_OK;
+}
+
+unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// One step through the separate-kernel schedule; energy: record the
+// invariant's field part into d_energy[0].
+ems_status run_step(ems_gpu* h, bool energy) {
+    const Grid& g = h->g;
+    cudaStream_t s = h->stream;
+    Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    Coeffs c;
+    for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
+    dim3 blk(kRowThreads, 1, 1);
+    dim3 grd(blocks_for(g.nz, kRowThreads), (unsigned)g.ny, (unsigned)g.nx);
+    if (energy) {
+        k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
+    } else {
+        k_update_h<false><<<grd, blk, 0, s>>>(g, f, c, nullptr);
+    }
+    ++h->launches;
+    if (energy) {
+        k_reduce_partials<<<1, 1024, 0, s>>>(h->partials, h->n_partials, h->d_energy);
+        ++h->launches;
+    }
+    // Slab hooks after the H update, in registration order.
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_CPML) {
+            for (const SlabDev& sd : op.cpml) {
+                if (sd.e_side) continue;
+                dim3 sg(blocks_for(sd.hi[2] - sd.lo[2], 64), (unsigned)(sd.hi[1] - sd.lo[1]), (unsigned)(sd.hi[0] - sd.lo[0]));
+                k_cpml<false><<<sg, 64, 0, s>>>(g, f, c, sd);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_POLES) {
+            if (op.poles.h.n_edges) {
+                k_poles_correct<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.h, false, h->dt);
+                ++h->launches;
+            }
+            if (op.poles.e.n_edges) {
+                k_poles_capture<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, op.poles.e, true);
+                ++h->launches;
+            }
+        }
+    }
+    // Serial post_h hooks: magnetic sources, current probes.
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_SOURCE && (op.source.kind == EMS_SOFT_H || op.source.kind == EMS_HARD_H)) {
+            const ems_gpu::SourceDev& sd = op.source;
+            float a = h->step < sd.amp.size() ? sd.amp[h->step] : 0.0f;
+            bool hard = sd.kind == EMS_HARD_H;
+            if (!hard && a == 0.0f) continue;
+            k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.i[0], f.i[1], f.i[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_CURRENT && h->step % op.probe.interval == 0) {
+            ems_gpu::ProbeDev& p = op.probe;
+            ems_status st = grow(h, &p.values, p.count, &p.cap, p.count + 1);
+            if (st) return st;
+            k_probe<<<1, 32, 0, s>>>(f.i[0], f.i[1], f.i[2], p.d, p.values + p.count);
+            ++h->launches;
+            ++p.count;
+        }
+    }
+    // pre_e: lumped elements save u^n.
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_LUMPED && (op.lumped.record || op.lumped.has_branch)) {
+            k_lumped_pre_e<<<blocks_for(op.lumped.n_edges, 128), 128, 0, s>>>(f.u[op.lumped.axis], op.lumped.d);
+            ++h->launches;
+        }
+    }
+    k_update_e<<<grd, blk, 0, s>>>(g, f, c);
+    ++h->launches;
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_CPML) {
+            for (const SlabDev& sd : op.cpml) {
+                if (!sd.e_side) continue;
+                dim3 sg(blocks_for(sd.hi[2] - sd.lo[2], 64), (unsigned)(sd.hi[1] - sd.lo[1]), (unsigned)(sd.hi[0] - sd.lo[0]));
+                k_cpml<true><<<sg, 64, 0, s>>>(g, f, c, sd);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_POLES) {
+            if (op.poles.e.n_edges) {
+                k_poles_correct<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.e, true, h->dt);
+                ++h->launches;
+            }
+            if (op.poles.h.n_edges) {
+                k_poles_capture<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, op.poles.h, false);
+                ++h->launches;
+            }
+        }
+    }
+    // Serial post_e hooks in registration order.
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_LUMPED) {
+            ems_gpu::LumpedDev& L = op.lumped;
+            double val = (L.has_src && h->step < L.amp.size()) ? L.amp[h->step] : 0.0;
+            bool active = L.has_src && val != 0.0;
+            size_t idx = L.count;
+            if (L.record) {
+                ems_status st = grow(h, &L.rec, L.count, &L.cap, L.count + 1);
+                if (st) return st;
+                if (L.columns) {
+                    size_t c1 = L.cap, c2 = L.cap;
+                    // Port series share the record's capacity.
+                    st = grow(h, &L.pv, L.count, &c1, L.cap);
+                    if (st) return st;
+                    st = grow(h, &L.pi, L.count, &c2, L.cap);
+                    if (st) return st;
+                }
+            }
+            k_lumped_post_e<<<1, 256, 0, s>>>(f.u[L.axis], L.d, val, active ? 1 : 0, h->dt,
+                                              L.record ? L.rec + idx : nullptr, L.columns ? L.pv + idx : nullptr,
+                                              L.columns ? L.pi + idx : nullptr);
+            ++h->launches;
+            if (L.record) ++L.count;
+        } else if (op.kind == EMS_OP_SOURCE && (op.source.kind == EMS_SOFT_E || op.source.kind == EMS_HARD_E)) {
+            const ems_gpu::SourceDev& sd = op.source;
+            float a = h->step < sd.amp.size() ? sd.amp[h->step] : 0.0f;
+            bool hard = sd.kind == EMS_HARD_E;
+            if (!hard && a == 0.0f) continue;
+            k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_VOLTAGE && h->step % op.probe.interval == 0) {
+            ems_gpu::ProbeDev& p = op.probe;
+            ems_status st = grow(h, &p.values, p.count, &p.cap, p.count + 1);
+            if (st) return st;
+            k_probe<<<1, 32, 0, s>>>(f.u[0], f.u[1], f.u[2], p.d, p.values + p.count);
+            ++h->launches;
+            ++p.count;
+        }
+    }
+    ++h->step;
+    return EMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
+    if (!d || !out) return EMS_ERR_INVALID;
+    *out = nullptr;
+    if (d->nodes[0] < 2 || d->nodes[1] < 2 || d->nodes[2] < 2 || !(d->dt > 0.0)) return EMS_ERR_INVALID;
+    for (int l = 0; l < 12; ++l)
+        if (!d->coeff[l]) return EMS_ERR_INVALID;
+    auto h = std::make_unique<ems_gpu>();
+    h->device = device;
+    if (check(h.get(), cudaSetDevice(device), "cudaSetDevice")) return EMS_ERR_CUDA;
+    if (check(h.get(), cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream")) return EMS_ERR_CUDA;
+    Grid& g = h->g;
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    if (g.np >= (1ull << 32) - 1) return EMS_ERR_INVALID;  // 32-bit device indices
+    h->dt = d->dt;
+    const size_t np = g.np;
+    for (int a = 0; a < 3; ++a) {
+        h->u[a] = h->alloc<float>(np);
+        h->i[a] = h->alloc<float>(np);
+        if (!h->u[a] || !h->i[a]) return EMS_ERR_NOMEM;
+    }
+    // Coefficients: reference rows copied into padded rows (padding zero).
+    for (int l = 0; l < 12; ++l) {
+        h->co[l] = h->alloc<float>(np);
+        if (!h->co[l]) return EMS_ERR_NOMEM;
+        if (check(h.get(), cudaMemcpy2DAsync(h->co[l], g.pitch * sizeof(float), d->coeff[l], g.nz * sizeof(float),
+                                             g.nz * sizeof(float), (size_t)g.nx * g.ny, cudaMemcpyHostToDevice, h->stream),
+                  "coefficient upload"))
+            return EMS_ERR_CUDA;
+    }
+    h->n_partials = (size_t)blocks_for(g.nz, kRowThreads) * g.ny * g.nx;
+    h->partials = h->alloc<double>(h->n_partials);
+    h->d_energy = h->alloc<double>(2);
+    if (!h->partials || !h->d_energy) return EMS_ERR_NOMEM;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        ems_gpu::Op op;
+        op.kind = d->ops[k].kind;
+        const void* t = d->ops[k].table;
+        if (!t) return EMS_ERR_INVALID;
+        switch (op.kind) {
+        case EMS_OP_CPML: {
+            const auto* c = (const ems_cpml*)t;
+            for (size_t q = 0; q < c->n_slabs; ++q) {
+                const ems_cpml_slab& s = c->slabs[q];
+                SlabDev sd{};
+                bool ok = s.comp >= 0 && s.comp < 3 && s.normal >= 0 && s.normal < 3 && s.other >= 0 && s.other < 3;
+                for (int a = 0; ok && a < 3; ++a) ok = s.lo[a] <= s.hi[a] && s.hi[a] <= d->nodes[a];
+                if (ok && !s.e_side) ok = s.hi[s.normal] < d->nodes[s.normal];  // reads node + 1 along normal
+                if (!ok || !s.b || !s.a || !s.k) return EMS_ERR_INVALID;
+                sd.e_side = s.e_side;
+                sd.comp = s.comp;
+                sd.normal = s.normal;
+                sd.other = s.other;
+                sd.sign = s.sign;
+                for (int a = 0; a < 3; ++a) {
+                    sd.lo[a] = (uint32_t)s.lo[a];
+                    sd.hi[a] = (uint32_t)s.hi[a];
+                }
+                size_t depth = s.hi[s.normal] - s.lo[s.normal];
+                size_t len = (size_t)(s.hi[0] - s.lo[0]) * (s.hi[1] - s.lo[1]) * (s.hi[2] - s.lo[2]);
+                if (!len) continue;
+                sd.b = h->upload(s.b, depth);
+                sd.a = h->upload(s.a, depth);
+                sd.k = h->upload(s.k, depth);
+                sd.psi = h->alloc<float>(len);
+                if (!sd.b || !sd.a || !sd.k || !sd.psi) return EMS_ERR_NOMEM;
+                op.cpml.push_back(sd);
+            }
+            break;
+        }
+        case EMS_OP_POLES: {
+            const auto* p = (const ems_poles*)t;
+            ems_status st = make_side(h.get(), p->electric, op.poles.e);
+            if (st) { std::fprintf(stderr, "ems_gpu: %s\n", h->err.c_str()); return st; }
+            st = make_side(h.get(), p->magnetic, op.poles.h);
+            if (st) { std::fprintf(stderr, "ems_gpu: %s\n", h->err.c_str()); return st; }
+            break;
+        }
+        case EMS_OP_LUMPED: {
+            const auto* l = (const ems_lumped*)t;
+            auto& L = op.lumped;
+            size_t ne = l->n_edges;
+            if (l->axis < 0 || l->axis > 2 || !ne || !l->node || !l->cb || !l->g_src || ne > 4096) return EMS_ERR_INVALID;
+            std::vector<uint32_t> node(ne);
+            for (size_t e = 0; e < ne; ++e) {
+                if (l->node[e] >= g.n) return EMS_ERR_INVALID;
+                node[e] = dev_index(g, l->node[e]);
+            }
+            L.axis = l->axis;
+            L.n_edges = ne;
+            L.has_src = l->src_w != nullptr;
+            L.has_branch = l->has_branch != 0;
+            L.record = l->record != 0;
+            L.columns = l->port_columns;
+            if (L.columns && !L.record) return EMS_ERR_INVALID;
+            if (L.has_src) L.amp.assign(l->src_amp, l->src_amp + l->n_src_amp);
+            LumpedDevT& D = L.d;
+            D.n = (uint32_t)ne;
+            D.series = (double)(l->series ? l->series : 1);
+            D.columns = (double)l->port_columns;
+            D.src_in_branch = l->src_in_branch;
+            D.has_branch = l->has_branch;
+            D.record = l->record;
+            D.node = h->upload(node.data(), ne);
+            D.cb = h->upload(l->cb, ne);
+            D.g_src = h->upload(l->g_src, ne);
+            D.src_w = L.has_src ? h->upload(l->src_w, ne) : nullptr;
+            if (L.has_branch) {
+                if (!l->two_l_dt || !l->inv_c || !l->z) return EMS_ERR_INVALID;
+                D.two_l_dt = h->upload(l->two_l_dt, ne);
+                D.inv_c = h->upload(l->inv_c, ne);
+                D.z = h->upload(l->z, ne);
+            }
+            if (L.record) {
+                if (!l->rec_g || !l->rec_c) return EMS_ERR_INVALID;
+                D.rec_g = h->upload(l->rec_g, ne);
+                D.rec_c = h->upload(l->rec_c, ne);
+            }
+            D.v = h->alloc<double>(ne);
+            D.bj = h->alloc<double>(ne);
+            D.bq = h->alloc<double>(ne);
+            D.bu_prev = h->alloc<double>(ne);
+            D.j_avg = h->alloc<double>(ne);
+            D.ru_prev = h->alloc<double>(ne);
+            if (!D.node || !D.cb || !D.g_src || !D.v || !D.bj || !D.bq || !D.bu_prev || !D.j_avg || !D.ru_prev)
+                return EMS_ERR_NOMEM;
+            break;
+        }
+        case EMS_OP_SOURCE: {
+            const auto* sr = (const ems_source*)t;
+            auto& S = op.source;
+            if (sr->kind < 0 || sr->kind > 3) return EMS_ERR_INVALID;
+            S.kind = sr->kind;
+            S.n = sr->n_edges;
+            std::vector<uint32_t> node(S.n);
+            for (size_t e = 0; e < S.n; ++e) {
+                if (sr->node[e] >= g.n || sr->axis[e] > 2) return EMS_ERR_INVALID;
+                node[e] = dev_index(g, sr->node[e]);
+            }
+            // Edges must be distinct: the kernel updates them in parallel.
+            std::vector<uint64_t> key(S.n);
+            for (size_t e = 0; e < S.n; ++e) key[e] = sr->node[e] * 3 + sr->axis[e];
+            std::sort(key.begin(), key.end());
+            if (std::adjacent_find(key.begin(), key.end()) != key.end()) return EMS_ERR_INVALID;
+            S.node = h->upload(node.data(), S.n);
+            S.axis = h->upload(sr->axis, S.n);
+            S.weight = h->upload(sr->weight, S.n);
+            S.amp.assign(sr->amp, sr->amp + sr->n_amp);
+            if (S.n && (!S.node || !S.axis || !S.weight)) return EMS_ERR_NOMEM;
+            break;
+        }
+        case EMS_OP_PROBE: {
+            const auto* pr = (const ems_probe*)t;
+            auto& P = op.probe;
+            if (pr->quantity < 0 || pr->quantity > 1) return EMS_ERR_INVALID;
+            P.quantity = pr->quantity;
+            P.interval = pr->interval ? pr->interval : 1;
+            std::vector<uint32_t> node(pr->n_entries);
+            for (size_t e = 0; e < pr->n_entries; ++e) {
+                if (pr->node[e] >= g.n || pr->axis[e] > 2) return EMS_ERR_INVALID;
+                node[e] = dev_index(g, pr->node[e]);
+            }
+            P.d.n = (uint32_t)pr->n_entries;
+            P.d.f32_sum = pr->f32_sum;
+            P.d.node = h->upload(node.data(), pr->n_entries);
+            P.d.axis = h->upload(pr->axis, pr->n_entries);
+            P.d.weight = h->upload(pr->weight, pr->n_entries);
+            break;
+        }
+        default:
+            return EMS_ERR_INVALID;
+        }
+        h->ops.push_back(std::move(op));
+    }
+    if (check(h.get(), cudaStreamSynchronize(h->stream), "create")) return EMS_ERR_CUDA;
+    *out = h.release();
+    return EMS_OK;
+}
+
+ems_status ems_gpu_destroy(ems_gpu* h) {
+    if (!h) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    h->bufs.clear();
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
+    if (!h) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    for (uint64_t s = 0; s < n; ++s) {
+        ems_status st = run_step(h, false);
+        if (st) return st;
+    }
+    return check(h, cudaGetLastError(), "run");
+}
+
+ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
+    if (!h || !energy) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    // Operator energies of the state before the step (src/engine/mod.rs:819-823).
+    double w_ops = 0.0;
+    for (auto& op : h->ops) {
+        double x = 0.0;
+        if (op.kind == EMS_OP_POLES) {
+            k_pole_energy<<<1, 1024, 0, h->stream>>>(op.poles.e, op.poles.h, h->d_energy + 1);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_LUMPED && op.lumped.has_branch) {
+            k_branch_energy<<<1, 1, 0, h->stream>>>(op.lumped.d, h->dt, h->d_energy + 1);
+            ++h->launches;
+        } else {
+            continue;
+        }
+        if (check(h, cudaMemcpyAsync(&x, h->d_energy + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "energy"))
+            return EMS_ERR_CUDA;
+        if (check(h, cudaStreamSynchronize(h->stream), "energy")) return EMS_ERR_CUDA;
+        w_ops += x;
+    }
+    ems_status st = run_step(h, true);
+    if (st) return st;
+    double w = 0.0;
+    if (check(h, cudaMemcpyAsync(&w, h->d_energy, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "energy"))
+        return EMS_ERR_CUDA;
+    if (check(h, cudaStreamSynchronize(h->stream), "energy")) return EMS_ERR_CUDA;
+    *energy = 0.25 * h->dt * w + w_ops;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_timestep(const ems_gpu* h, uint64_t* n) {
+    if (!h || !n) return EMS_ERR_INVALID;
+    *n = h->step;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_download_field(ems_gpu* h, int field, int axis, float* host) {
+    if (!h || !host || field < 0 || field > 1 || axis < 0 || axis > 2) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    const Grid& g = h->g;
+    float* src = field == 0 ? h->u[axis] : h->i[axis];
+    if (check(h, cudaMemcpy2DAsync(host, g.nz * sizeof(float), src, g.pitch * sizeof(float), g.nz * sizeof(float),
+                                   (size_t)g.nx * g.ny, cudaMemcpyDeviceToHost, h->stream),
+              "download"))
+        return EMS_ERR_CUDA;
+    return check(h, cudaStreamSynchronize(h->stream), "download");
+}
+
+ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* host) {
+    if (!h || !host || field < 0 || field > 1 || axis < 0 || axis > 2) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    const Grid& g = h->g;
+    float* dst = field == 0 ? h->u[axis] : h->i[axis];
+    if (check(h, cudaMemcpy2DAsync(dst, g.pitch * sizeof(float), host, g.nz * sizeof(float), g.nz * sizeof(float),
+                                   (size_t)g.nx * g.ny, cudaMemcpyHostToDevice, h->stream),
+              "upload"))
+        return EMS_ERR_CUDA;
+    return check(h, cudaStreamSynchronize(h->stream), "upload");
+}
+
+ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t cap, size_t* n) {
+    if (!h || !n || op >= h->ops.size()) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    auto& o = h->ops[op];
+    const double* src = nullptr;
+    size_t cnt = 0;
+    if (o.kind == EMS_OP_PROBE && which == 0) {
+        src = o.probe.values;
+        cnt = o.probe.count;
+    } else if (o.kind == EMS_OP_LUMPED && o.lumped.record && which >= 0 && which <= 2) {
+        if (which > 0 && !o.lumped.columns) return EMS_ERR_INVALID;
+        src = which == 0 ? o.lumped.rec : (which == 1 ? o.lumped.pv : o.lumped.pi);
+        cnt = o.lumped.count;
+    } else {
+        return fail(h, EMS_ERR_INVALID, "no such series");
+    }
+    *n = cnt;
+    if (out && cnt && cap) {
+        size_t m = std::min(cap, cnt);
+        if (check(h, cudaMemcpyAsync(out, src, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "samples"))
+            return EMS_ERR_CUDA;
+    }
+    return check(h, cudaStreamSynchronize(h->stream), "samples");
+}
+
+const char* ems_gpu_last_error(const ems_gpu* h) { return h ? h->err.c_str() : "null handle"; }
+
+ems_status ems_gpu_launch_count(const ems_gpu* h, uint64_t* n) {
+    if (!h || !n) return EMS_ERR_INVALID;
+    *n = h->launches;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
+    if (!h || schedule < 0 || schedule > 2) return EMS_ERR_INVALID;
+    h->schedule = schedule;
+    return EMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1056 @@
+// host.cpp — host-side model set-up for the B200 engine (see include/ems_host.h).
+//
+// Restates the reference's set-up arithmetic expression by expression
+// (f64, no contraction: built with -ffp-contract=off) so the tables handed
+// to the engine are the ones the reference's own host would compute.
+#include "../../include/ems_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <tuple>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// src/constants.rs:9-18.
+constexpr double C0 = 299792458.0;
+constexpr double MU0 = 1.25663706127e-6;
+const double EPS0 = 1.0 / (MU0 * C0 * C0);
+const double Z0 = MU0 * C0;
+constexpr double PI = 3.14159265358979323846;
+constexpr double TAU = 6.28318530717958647692;
+constexpr double LN_10 = 2.30258509299404568402;
+
+inline int next_axis(int a) { return (a + 1) % 3; }
+inline int prev_axis(int a) { return (a + 2) % 3; }
+
+struct Material {
+    double eps_r[3], mu_r[3], kappa[3], sigma_m[3];
+};
+
+struct Pole {
+    int kind;  // 0 Lorentz, 1 Drude, 2 Debye
+    double p1, p2, p3;
+    // Pole::scaled (src/engine/dispersive.rs:306-327).
+    Pole scaled(double s) const {
+        Pole q = *this;
+        if (kind == 0 || kind == 1) q.p1 = p1 * std::sqrt(s);
+        else q.p1 = p1 * s;
+        return q;
+    }
+};
+
+struct Entry {
+    int field, axis;
+    uint64_t node[3];
+    Pole pole;
+};
+
+void run_threads(size_t n, const std::function<void(size_t, size_t)>& f);
+
+}  // namespace
+
+struct ems_cellset {
+    uint64_t c[3];
+    std::vector<uint8_t> mask;
+    uint64_t lo[3], hi[3];  // bounding box of the set (cells, half-open)
+    bool any = false;
+    bool at(uint64_t i, uint64_t j, uint64_t k) const { return mask[(i * c[1] + j) * c[2] + k] != 0; }
+    void grow(const uint64_t l[3], const uint64_t h[3]) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = any ? std::min(lo[a], l[a]) : l[a];
+            hi[a] = any ? std::max(hi[a], h[a]) : h[a];
+        }
+        any = true;
+    }
+};
+
+struct ems_dispersive {
+    std::vector<Entry> entries;
+};
+
+namespace {
+
+struct OpStore {
+    int kind = 0;
+    // CPML
+    std::vector<ems_cpml_slab> slabs;
+    std::vector<std::vector<float>> arrays;
+    ems_cpml cpml{};
+    double index[6] = {0, 0, 0, 0, 0, 0};
+    // poles
+    struct Side {
+        std::vector<uint8_t> axis, kind;
+        std::vector<uint64_t> node;
+        std::vector<double> sum_inv_z, a, inv_c, inv_z, half_l;
+        std::vector<uint32_t> pole_end;
+        void fill(ems_pole_side& t) const {
+            t.n_edges = axis.size();
+            t.axis = axis.data();
+            t.node = node.data();
+            t.sum_inv_z = sum_inv_z.data();
+            t.pole_end = pole_end.data();
+            t.n_poles = kind.size();
+            t.kind = kind.data();
+            t.a = a.data();
+            t.inv_c = inv_c.data();
+            t.inv_z = inv_z.data();
+            t.half_l = half_l.data();
+        }
+    } pe, ph;
+    ems_poles poles{};
+    // lumped
+    std::vector<uint64_t> lnode;
+    std::vector<double> lcb, lg, lw, lamp, lrg, lrc;
+    ems_lumped lumped{};
+    // source / probe
+    std::vector<uint8_t> axis;
+    std::vector<uint64_t> node;
+    std::vector<float> fw, famp;
+    std::vector<double> dw;
+    ems_source source{};
+    ems_probe probe{};
+};
+
+}  // namespace
+
+struct ems_model {
+    std::vector<double> lines[3];
+    uint64_t n[3];
+    uint64_t c[3];
+    std::vector<Material> table;
+    std::vector<uint16_t> cell;
+    std::vector<uint8_t> pec[3];
+    int faces[6] = {0, 0, 0, 0, 0, 0};
+    bool built = false;
+    double dt = 0.0;
+    std::vector<float> co[12];
+    std::vector<std::unique_ptr<OpStore>> ops;
+    std::vector<ems_op> op_list;
+    ems_engine_desc desc{};
+    std::string err;
+
+    uint64_t index(uint64_t i, uint64_t j, uint64_t k) const { return (i * n[1] + j) * n[2] + k; }
+    // src/engine/grid.rs:562-597.
+    double delta(int a, uint64_t i) const { return lines[a][i + 1] - lines[a][i]; }
+    double dual_delta(int a, uint64_t i) const {
+        double lo = i > 0 ? delta(a, i - 1) : 0.0;
+        double hi = i + 1 < n[a] ? delta(a, i) : 0.0;
+        return 0.5 * (lo + hi);
+    }
+    double min_delta(int a) const {
+        double m = INFINITY;
+        for (uint64_t i = 0; i + 1 < n[a]; ++i) m = std::fmin(m, delta(a, i));
+        return m;
+    }
+    const Material& mat(uint64_t i, uint64_t j, uint64_t k) const {
+        return table[cell[(i * c[1] + j) * c[2] + k]];
+    }
+    // primary_edge_cg (src/engine/coeffs.rs:264-292).
+    void primary_edge_cg(int a, const uint64_t p[3], double& cap_out, double& cond_out) const {
+        const int b = next_axis(a), cc = prev_axis(a);
+        const double l = delta(a, p[a]);
+        double cap = 0.0, cond = 0.0;
+        for (int db = -1; db <= 0; ++db) {
+            if (p[b] == 0 && db < 0) continue;
+            uint64_t cb = p[b] + db;
+            if (cb >= n[b] - 1) continue;
+            for (int dc = -1; dc <= 0; ++dc) {
+                if (p[cc] == 0 && dc < 0) continue;
+                uint64_t ccell = p[cc] + dc;
+                if (ccell >= n[cc] - 1) continue;
+                uint64_t q[3];
+                q[a] = p[a];
+                q[b] = cb;
+                q[cc] = ccell;
+                double area = 0.25 * delta(b, cb) * delta(cc, ccell);
+                const Material& m = mat(q[0], q[1], q[2]);
+                cap += EPS0 * m.eps_r[a] * area;
+                cond += m.kappa[a] * area;
+            }
+        }
+        cap_out = cap / l;
+        cond_out = cond / l;
+    }
+    // dual_edge_lr (src/engine/coeffs.rs:300-325).
+    void dual_edge_lr(int a, const uint64_t p[3], double& l_out, double& r_out) const {
+        const int b = next_axis(a), cc = prev_axis(a);
+        const double area = delta(b, p[b]) * delta(cc, p[cc]);
+        double inv_l = 0.0, r_over_l2 = 0.0;
+        for (int da = -1; da <= 0; ++da) {
+            if (p[a] == 0 && da < 0) continue;
+            uint64_t ca = p[a] + da;
+            if (ca >= n[a] - 1) continue;
+            uint64_t q[3] = {p[0], p[1], p[2]};
+            q[a] = ca;
+            double half = 0.5 * delta(a, ca);
+            const Material& m = mat(q[0], q[1], q[2]);
+            double lc = MU0 * m.mu_r[a] * area / half;
+            double rc = m.sigma_m[a] * area / half;
+            inv_l += 1.0 / lc;
+            r_over_l2 += rc / (lc * lc);
+        }
+        double l = 1.0 / inv_l;
+        l_out = l;
+        r_out = l * l * r_over_l2;
+    }
+
+    void refresh_desc() {
+        desc.nodes[0] = n[0];
+        desc.nodes[1] = n[1];
+        desc.nodes[2] = n[2];
+        desc.dt = dt;
+        for (int l = 0; l < 12; ++l) desc.coeff[l] = co[l].empty() ? nullptr : co[l].data();
+        op_list.clear();
+        for (auto& o : ops) {
+            ems_op e;
+            e.kind = o->kind;
+            switch (o->kind) {
+            case EMS_OP_CPML: e.table = &o->cpml; break;
+            case EMS_OP_POLES: e.table = &o->poles; break;
+            case EMS_OP_LUMPED: e.table = &o->lumped; break;
+            case EMS_OP_SOURCE: e.table = &o->source; break;
+            default: e.table = &o->probe; break;
+            }
+            op_list.push_back(e);
+        }
+        desc.n_ops = op_list.size();
+        desc.ops = op_list.data();
+    }
+};
+
+namespace {
+
+void run_threads(size_t n, const std::function<void(size_t, size_t)>& f) {
+    unsigned hw = std::thread::hardware_concurrency();
+    size_t t = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, 64));
+    t = std::min(t, n);
+    if (t <= 1) { f(0, n); return; }
+    std::vector<std::thread> th;
+    size_t q = n / t, r = n % t, p = 0;
+    for (size_t s = 0; s < t; ++s) {
+        size_t len = q + (s < r ? 1 : 0);
+        th.emplace_back(f, p, p + len);
+        p += len;
+    }
+    for (auto& x : th) x.join();
+}
+
+// CpmlCoefficients::in_medium (src/engine/boundary/cpml.rs:350-387).
+struct CpmlCo {
+    double b, a, direct;
+};
+CpmlCo cpml_in_medium(double m, double sigma_factor, double kappa_max, double alpha_max, bool linear, double rho,
+                      double delta, double dt, double n) {
+    double g = std::pow(rho, m);
+    double eta = n * Z0;
+    double sigma = sigma_factor * 0.8 * (m + 1.0) / (eta * delta) * g;
+    double kappa = 1.0 + (kappa_max - 1.0) * g;
+    double alpha = alpha_max * (1.0 - rho);
+    double b = std::exp(-(sigma / kappa + alpha) * dt / EPS0);
+    double den = sigma * kappa + kappa * kappa * alpha;
+    double x = (sigma / kappa + alpha) * dt / EPS0;
+    double a, shift;
+    if (!(sigma > 0.0 && den > 0.0)) {
+        a = 0.0;
+        shift = 0.0;
+    } else if (linear && x <= 8.0) {
+        double cdt = sigma * dt / (EPS0 * kappa * kappa);
+        double gg = x < 1e-3 ? 0.5 - x / 3.0 + x * x / 8.0 : (-std::expm1(-x) - x * b) / (x * x);
+        double a1 = -cdt * gg;
+        double a0 = cdt * std::expm1(-x) / x - a1;
+        a = a0 + a1 / b;
+        shift = a1 / b;
+    } else {
+        a = sigma * (b - 1.0) / den;
+        shift = 0.0;
+    }
+    return {b, a, 1.0 / kappa - 1.0 - shift};
+}
+
+// Waveform::Gaussian (src/waveform.rs:241-248, 455-463).
+double gaussian_tau(double fc) { return std::sqrt(LN_10) / (PI * fc); }
+double gaussian_delay(double fc) { return gaussian_tau(fc) * std::sqrt(6.0 * LN_10); }
+
+bool set_err(ems_model* m, const std::string& s) {
+    m->err = s;
+    return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+double ems_const_eps0(void) { return EPS0; }
+double ems_const_mu0(void) { return MU0; }
+double ems_const_c0(void) { return C0; }
+
+double ems_waveform_value(int kind, double f0, double fc, double t, double dt) {
+    (void)dt;
+    if (kind != 0) return 0.0;
+    double delay = gaussian_delay(fc);
+    if (!(t >= 0.0 && t <= 2.0 * delay)) return 0.0;
+    double x = (t - delay) / gaussian_tau(fc);
+    return std::cos(TAU * f0 * (t - delay)) * std::exp(-x * x);
+}
+
+double ems_waveform_duration(int kind, double f0, double fc) {
+    (void)f0;
+    return kind == 0 ? 2.0 * gaussian_delay(fc) : 0.0;
+}
+
+ems_model* ems_model_new(const double* x, size_t nx, const double* y, size_t ny, const double* z, size_t nz) {
+    const double* l[3] = {x, y, z};
+    size_t nn[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        if (!l[a] || nn[a] < 2) return nullptr;
+        for (size_t i = 0; i < nn[a]; ++i)
+            if (!std::isfinite(l[a][i]) || (i && !(l[a][i] > l[a][i - 1]))) return nullptr;
+    }
+    auto* m = new ems_model();
+    for (int a = 0; a < 3; ++a) {
+        m->lines[a].assign(l[a], l[a] + nn[a]);
+        m->n[a] = nn[a];
+        m->c[a] = nn[a] - 1;
+    }
+    m->table.push_back(Material{{1, 1, 1}, {1, 1, 1}, {0, 0, 0}, {0, 0, 0}});
+    m->cell.assign(m->c[0] * m->c[1] * m->c[2], 0);
+    for (int a = 0; a < 3; ++a) m->pec[a].assign(m->n[0] * m->n[1] * m->n[2], 0);
+    m->refresh_desc();
+    return m;
+}
+
+void ems_model_free(ems_model* m) { delete m; }
+const char* ems_model_error(const ems_model* m) { return m ? m->err.c_str() : "null model"; }
+void ems_model_nodes(const ems_model* m, uint64_t nodes[3]) {
+    for (int a = 0; a < 3; ++a) nodes[a] = m->n[a];
+}
+
+int ems_model_material(ems_model* m, const double eps_r[3], const double mu_r[3], const double kappa[3],
+                       const double sigma_m[3]) {
+    Material t;
+    for (int a = 0; a < 3; ++a) {
+        t.eps_r[a] = eps_r[a];
+        t.mu_r[a] = mu_r[a];
+        t.kappa[a] = kappa[a];
+        t.sigma_m[a] = sigma_m[a];
+        // Material::validate (src/engine/material.rs).
+        if (!(std::isfinite(eps_r[a]) && eps_r[a] > 0 && std::isfinite(mu_r[a]) && mu_r[a] > 0 &&
+              std::isfinite(kappa[a]) && kappa[a] >= 0 && std::isfinite(sigma_m[a]) && sigma_m[a] >= 0)) {
+            set_err(m, "invalid material");
+            return -1;
+        }
+    }
+    if (m->table.size() >= 65535) return -1;
+    m->table.push_back(t);
+    return (int)m->table.size() - 1;
+}
+
+ems_cellset* ems_cellset_new(const ems_model* m) {
+    auto* s = new ems_cellset();
+    for (int a = 0; a < 3; ++a) s->c[a] = m->c[a];
+    s->mask.assign(s->c[0] * s->c[1] * s->c[2], 0);
+    return s;
+}
+void ems_cellset_free(ems_cellset* s) { delete s; }
+
+int ems_cellset_box(ems_cellset* s, const uint64_t lo[3], const uint64_t hi[3]) {
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] > hi[a] || hi[a] > s->c[a]) return EMS_ERR_INVALID;
+    if (lo[0] == hi[0] || lo[1] == hi[1] || lo[2] == hi[2]) return EMS_OK;
+    for (uint64_t i = lo[0]; i < hi[0]; ++i)
+        for (uint64_t j = lo[1]; j < hi[1]; ++j)
+            std::memset(&s->mask[(i * s->c[1] + j) * s->c[2] + lo[2]], 1, hi[2] - lo[2]);
+    s->grow(lo, hi);
+    return EMS_OK;
+}
+
+int ems_cellset_sphere(ems_cellset* s, const double ctr[3], double r) {
+    // Cells whose centre (index + 1/2, in cell units) lies within r.
+    uint64_t lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        double l = std::floor(ctr[a] - r - 1.0), h = std::ceil(ctr[a] + r + 1.0);
+        lo[a] = (uint64_t)std::max(0.0, l);
+        hi[a] = (uint64_t)std::min((double)s->c[a], std::max(0.0, h));
+        if (lo[a] >= hi[a]) return EMS_OK;
+    }
+    bool any = false;
+    for (uint64_t i = lo[0]; i < hi[0]; ++i)
+        for (uint64_t j = lo[1]; j < hi[1]; ++j)
+            for (uint64_t k = lo[2]; k < hi[2]; ++k) {
+                double dx = (double)i + 0.5 - ctr[0], dy = (double)j + 0.5 - ctr[1], dz = (double)k + 0.5 - ctr[2];
+                if (dx * dx + dy * dy + dz * dz <= r * r) {
+                    s->mask[(i * s->c[1] + j) * s->c[2] + k] = 1;
+                    any = true;
+                }
+            }
+    if (any) s->grow(lo, hi);
+    return EMS_OK;
+}
+
+uint64_t ems_cellset_count(const ems_cellset* s) {
+    uint64_t n = 0;
+    for (uint8_t v : s->mask) n += v;
+    return n;
+}
+
+int ems_model_fill(ems_model* m, const ems_cellset* s, int mat) {
+    if (mat < 0 || (size_t)mat >= m->table.size() || m->built) return EMS_ERR_INVALID;
+    for (size_t q = 0; q < s->mask.size(); ++q)
+        if (s->mask[q]) m->cell[q] = (uint16_t)mat;
+    return EMS_OK;
+}
+
+int ems_model_pec_edges(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3]) {
+    if (axis < 0 || axis > 2 || m->built) return EMS_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] > hi[a] || hi[a] >= m->n[a]) return EMS_ERR_INVALID;
+    for (uint64_t i = lo[0]; i <= hi[0]; ++i)
+        for (uint64_t j = lo[1]; j <= hi[1]; ++j)
+            for (uint64_t k = lo[2]; k <= hi[2]; ++k) m->pec[axis][m->index(i, j, k)] = 1;
+    return EMS_OK;
+}
+
+int ems_model_faces(ems_model* m, const int faces[6]) {
+    if (m->built) return EMS_ERR_INVALID;
+    for (int f = 0; f < 6; ++f) {
+        if (faces[f] != 0 && faces[f] != 1) return EMS_ERR_INVALID;
+        m->faces[f] = faces[f];
+    }
+    return EMS_OK;
+}
+
+double ems_model_courant_limit(const ems_model* m) {
+    // courant_limit (src/engine/coeffs.rs:254-262).
+    double s = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        double d = m->min_delta(a);
+        s += 1.0 / (d * d);
+    }
+    return 1.0 / (C0 * std::sqrt(s));
+}
+
+int ems_model_build(ems_model* m, double courant, double fixed_dt) {
+    if (m->built) return set_err(m, "model already built"), EMS_ERR_INVALID;
+    // TimeStep::resolve (src/engine/coeffs.rs:220-240).
+    double max = ems_model_courant_limit(m);
+    double dt;
+    if (fixed_dt > 0.0) {
+        if (!(std::isfinite(fixed_dt) && fixed_dt <= max)) return set_err(m, "time step above the stability limit"), EMS_ERR_INVALID;
+        dt = fixed_dt;
+    } else {
+        if (!(std::isfinite(courant) && courant > 0.0 && courant <= 1.0)) return set_err(m, "Courant factor must be in (0, 1]"), EMS_ERR_INVALID;
+        dt = courant * max;
+    }
+    m->dt = dt;
+    const uint64_t N = m->n[0] * m->n[1] * m->n[2];
+    for (int l = 0; l < 12; ++l) m->co[l].assign(N, 0.0f);
+    bool pec_face[3][2];
+    for (int t = 0; t < 3; ++t)
+        for (int s = 0; s < 2; ++s) pec_face[t][s] = m->faces[2 * t + s] == 0;
+    // EdgeMaterials::from_cells + Coefficients::from_edges_rounded (Exact)
+    // (src/engine/edge_material.rs:376-425, src/engine/coeffs.rs:879-966),
+    // one x-plane range per thread.
+    run_threads(m->n[0], [&](size_t i0, size_t i1) {
+        for (uint64_t i = i0; i < i1; ++i)
+            for (uint64_t j = 0; j < m->n[1]; ++j)
+                for (uint64_t k = 0; k < m->n[2]; ++k) {
+                    const uint64_t p[3] = {i, j, k};
+                    const uint64_t idx = m->index(i, j, k);
+                    for (int a = 0; a < 3; ++a) {
+                        const int b = next_axis(a), c = prev_axis(a);
+                        if (p[a] + 1 < m->n[a]) {
+                            bool on_pec_face = false;
+                            for (int t : {b, c})
+                                if ((p[t] == 0 && pec_face[t][0]) || (p[t] == m->n[t] - 1 && pec_face[t][1]))
+                                    on_pec_face = true;
+                            if (!(on_pec_face || m->pec[a][idx])) {
+                                double cap_c, g_c;
+                                m->primary_edge_cg(a, p, cap_c, g_c);
+                                double k_ = m->delta(a, p[a]) / (m->dual_delta(b, p[b]) * m->dual_delta(c, p[c]));
+                                double eps = cap_c * k_ / EPS0;
+                                double kap = g_c * k_;
+                                double geo = m->dual_delta(b, p[b]) * m->dual_delta(c, p[c]) / m->delta(a, p[a]);
+                                double cap = EPS0 * eps * geo;
+                                double g = kap * geo;
+                                double den = cap + 0.5 * g * dt;
+                                m->co[a][idx] = (float)((cap - 0.5 * g * dt) / den);
+                                m->co[3 + a][idx] = (float)(dt / den);
+                            }
+                        }
+                        if (p[b] + 1 < m->n[b] && p[c] + 1 < m->n[c]) {
+                            double l_c, r_c;
+                            m->dual_edge_lr(a, p, l_c, r_c);
+                            double k_ = m->dual_delta(a, p[a]) / (m->delta(b, p[b]) * m->delta(c, p[c]));
+                            double mu = l_c * k_ / MU0;
+                            double sig = r_c * k_;
+                            double geo = m->delta(b, p[b]) * m->delta(c, p[c]) / m->dual_delta(a, p[a]);
+                            double l = MU0 * mu * geo;
+                            double r = sig * geo;
+                            double den = l + 0.5 * r * dt;
+                            m->co[6 + a][idx] = (float)((l - 0.5 * r * dt) / den);
+                            m->co[9 + a][idx] = (float)(dt / den);
+                        }
+                    }
+                }
+    });
+    m->built = true;
+    m->refresh_desc();
+    return EMS_OK;
+}
+
+double ems_model_dt(const ems_model* m) { return m->dt; }
+const float* ems_model_coeff(const ems_model* m, int lane) {
+    if (!m->built || lane < 0 || lane > 11) return nullptr;
+    return m->co[lane].data();
+}
+
+// Mean refractive index of a layer, layer_index (src/engine/boundary/cpml.rs:1056-1120).
+static double layer_index(const ems_model* m, int face, uint64_t cells) {
+    const int p = face / 2;
+    const bool is_max = face % 2 == 1;
+    const uint64_t np = m->n[p];
+    const uint64_t inner = is_max ? np - 1 - cells : cells;
+    const uint64_t l0 = is_max ? inner : 0, l1 = is_max ? np : inner + 1;  // lines
+    const uint64_t c0 = is_max ? inner : 0, c1 = is_max ? np - 1 : inner;  // cells
+    const double dt = m->dt;
+    double we = 0.0, se = 0.0, wh = 0.0, sh = 0.0;
+    const int comps[2] = {next_axis(p), prev_axis(p)};
+    uint64_t lo[3] = {0, 0, 0}, hi[3] = {m->n[0], m->n[1], m->n[2]};
+    lo[p] = std::min(l0, c0);
+    hi[p] = std::max(l1, c1);
+    for (int comp : comps) {
+        const int a = comp, b = next_axis(comp), c = prev_axis(comp);
+        for (uint64_t i = lo[0]; i < hi[0]; ++i)
+            for (uint64_t j = lo[1]; j < hi[1]; ++j)
+                for (uint64_t k = lo[2]; k < hi[2]; ++k) {
+                    const uint64_t node[3] = {i, j, k};
+                    const uint64_t idx = m->index(i, j, k);
+                    const uint64_t along = node[p];
+                    const float ca = m->co[a][idx], cb = m->co[3 + a][idx];
+                    if (along >= l0 && along < l1 && node[a] + 1 < m->n[a] && cb != 0.0f) {
+                        double area = m->dual_delta(b, node[b]) * m->dual_delta(c, node[c]);
+                        double l = m->delta(a, node[a]);
+                        double cap = dt * (1.0 + (double)ca) / (2.0 * (double)cb);
+                        double vol = area * l;
+                        we += vol;
+                        se += vol * cap * l / (EPS0 * area);
+                    }
+                    const float da = m->co[6 + a][idx], db = m->co[9 + a][idx];
+                    if (along >= c0 && along < c1 && node[b] + 1 < m->n[b] && node[c] + 1 < m->n[c] && db != 0.0f) {
+                        double area = m->delta(b, node[b]) * m->delta(c, node[c]);
+                        double l = m->dual_delta(a, node[a]);
+                        double ind = dt * (1.0 + (double)da) / (2.0 * (double)db);
+                        double vol = area * l;
+                        wh += vol;
+                        sh += vol * ind * l / (MU0 * area);
+                    }
+                }
+    }
+    double eps = we > 0.0 ? se / we : 1.0;
+    double mu = wh > 0.0 ? sh / wh : 1.0;
+    double n_r = std::sqrt(eps * mu);
+    if (std::fabs(n_r - 1.0) < 1e-6 || !std::isfinite(n_r) || n_r <= 0.0) return 1.0;
+    return n_r;
+}
+
+int ems_model_add_cpml(ems_model* m, const uint64_t cells[6], double grading, double sigma_factor, double kappa_max,
+                       double alpha_max, int linear) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    // Cpml::validate (src/fdtd.rs:275-295).
+    if (!(std::isfinite(grading) && grading >= 0 && std::isfinite(sigma_factor) && sigma_factor >= 0 &&
+          std::isfinite(kappa_max) && kappa_max >= 1 && std::isfinite(alpha_max) && alpha_max >= 0))
+        return set_err(m, "invalid CPML parameters"), -1;
+    for (int p = 0; p < 3; ++p) {
+        if (cells[2 * p] > m->n[p] - 1 || cells[2 * p + 1] > m->n[p] - 1) return set_err(m, "CPML thicker than the mesh"), -1;
+        if (cells[2 * p] + cells[2 * p + 1] > m->n[p] - 1) return set_err(m, "opposite CPML layers overlap"), -1;
+    }
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_CPML;
+    // CpmlBoundary::build + Layer::new (src/engine/boundary/cpml.rs:979-1035, 1122-1196).
+    for (int face = 0; face < 6; ++face) {
+        const uint64_t c = cells[face];
+        if (c == 0) continue;
+        const int p = face / 2;
+        const bool is_max = face % 2 == 1;
+        const uint64_t np = m->n[p];
+        const double n_face = layer_index(m, face, c);
+        op->index[face] = n_face;
+        const uint64_t inner = is_max ? np - 1 - c : c;
+        auto rho = [&](double x) { return std::min(1.0, std::max(0.0, std::fabs(x - (double)inner) / (double)c)); };
+        std::vector<uint64_t> e_idx, h_idx;
+        if (is_max) {
+            for (uint64_t k = inner + 1; k < np; ++k) e_idx.push_back(k);
+            for (uint64_t k = inner; k < np - 1; ++k) h_idx.push_back(k);
+        } else {
+            for (uint64_t k = 0; k < inner; ++k) e_idx.push_back(k);
+            for (uint64_t k = 0; k < inner; ++k) h_idx.push_back(k);
+        }
+        auto node_delta = [&](uint64_t k) {
+            bool has_lo = k > 0, has_hi = k + 1 < np;
+            if (has_lo && has_hi) return 0.5 * (m->delta(p, k - 1) + m->delta(p, k));
+            return has_lo ? m->delta(p, k - 1) : m->delta(p, k);
+        };
+        std::vector<float> eb, ea, ek, hb, ha, hk;
+        for (uint64_t k : e_idx) {
+            CpmlCo q = cpml_in_medium(grading, sigma_factor, kappa_max, alpha_max, linear != 0, rho((double)k),
+                                      node_delta(k), m->dt, n_face);
+            eb.push_back((float)q.b);
+            ea.push_back((float)q.a);
+            ek.push_back((float)q.direct);
+        }
+        for (uint64_t k : h_idx) {
+            CpmlCo q = cpml_in_medium(grading, sigma_factor, kappa_max, alpha_max, linear != 0, rho((double)k + 0.5),
+                                      m->delta(p, k), m->dt, n_face);
+            hb.push_back((float)q.b);
+            ha.push_back((float)q.a);
+            hk.push_back((float)q.direct);
+        }
+        const int a1 = next_axis(p), a2 = prev_axis(p);
+        auto slab = [&](int comp, bool e_side) {
+            ems_cpml_slab s{};
+            s.e_side = e_side ? 1 : 0;
+            s.comp = comp;
+            s.normal = p;
+            // Slab::new (src/engine/boundary/cpml.rs:412-437).
+            if (p == next_axis(comp)) {
+                s.sign = 1.0f;
+                s.other = prev_axis(comp);
+            } else {
+                s.sign = -1.0f;
+                s.other = next_axis(comp);
+            }
+            for (int t = 0; t < 3; ++t) {
+                s.lo[t] = 0;
+                s.hi[t] = m->n[t];
+            }
+            const auto& idx = e_side ? e_idx : h_idx;
+            if (e_side) {
+                s.hi[comp] = m->n[comp] - 1;
+            } else {
+                int o = comp == a1 ? a2 : a1;
+                s.hi[o] = m->n[o] - 1;
+            }
+            s.lo[p] = idx.empty() ? 0 : idx.front();
+            s.hi[p] = idx.empty() ? 0 : idx.back() + 1;
+            op->arrays.push_back(e_side ? eb : hb);
+            op->arrays.push_back(e_side ? ea : ha);
+            op->arrays.push_back(e_side ? ek : hk);
+            op->slabs.push_back(s);
+        };
+        slab(a1, true);
+        slab(a2, true);
+        slab(a1, false);
+        slab(a2, false);
+    }
+    for (size_t s = 0; s < op->slabs.size(); ++s) {
+        op->slabs[s].b = op->arrays[3 * s].data();
+        op->slabs[s].a = op->arrays[3 * s + 1].data();
+        op->slabs[s].k = op->arrays[3 * s + 2].data();
+    }
+    op->cpml.n_slabs = op->slabs.size();
+    op->cpml.slabs = op->slabs.data();
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+double ems_model_cpml_index(const ems_model* m, int face) {
+    for (auto& o : m->ops)
+        if (o->kind == EMS_OP_CPML && face >= 0 && face < 6) return o->index[face];
+    return 0.0;
+}
+
+ems_dispersive* ems_dispersive_new(void) { return new ems_dispersive(); }
+void ems_dispersive_free(ems_dispersive* d) { delete d; }
+
+int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset* s, int field, size_t n_poles,
+                        const int* kind, const double* p1, const double* p2, const double* p3) {
+    std::vector<Pole> poles;
+    for (size_t q = 0; q < n_poles; ++q) {
+        Pole p{kind[q], p1[q], p2 ? p2[q] : 0.0, p3 ? p3[q] : 0.0};
+        // Pole::validate (src/engine/dispersive.rs:339-358).
+        double v[3] = {p.p1, p.p2, p.kind == 0 ? p.p3 : 0.0};
+        for (double x : v)
+            if (!(std::isfinite(x) && x >= 0.0)) return EMS_ERR_INVALID;
+        if (p.kind < 0 || p.kind > 2) return EMS_ERR_INVALID;
+        poles.push_back(p);
+    }
+    if (!s->any || poles.empty()) return EMS_OK;
+    // Dispersive::fill_cells (src/engine/dispersive.rs:1896-1985) with the
+    // box test replaced by the cell set's membership; edges touching the
+    // set's bounding box, in the reference's axis / node order.
+    for (int axis = 0; axis < 3; ++axis) {
+        const int a = axis, b = next_axis(axis), c = prev_axis(axis);
+        uint64_t lo[3], hi[3];
+        for (int t = 0; t < 3; ++t) {
+            bool along = field == 0 ? t == a : t != a;
+            lo[t] = s->lo[t];
+            hi[t] = along ? s->hi[t] : std::min(s->hi[t] + 1, m->n[t]);
+        }
+        uint64_t node[3];
+        for (node[a] = lo[a]; node[a] < hi[a]; ++node[a])
+            for (node[b] = lo[b]; node[b] < hi[b]; ++node[b])
+                for (node[c] = lo[c]; node[c] < hi[c]; ++node[c]) {
+                    double share;
+                    if (field == 0) {
+                        double w_in = 0.0, w = 0.0;
+                        for (int db = -1; db <= 0; ++db) {
+                            if (node[b] == 0 && db < 0) continue;
+                            uint64_t cb = node[b] + db;
+                            if (cb >= m->n[b] - 1) continue;
+                            for (int dc = -1; dc <= 0; ++dc) {
+                                if (node[c] == 0 && dc < 0) continue;
+                                uint64_t cc = node[c] + dc;
+                                if (cc >= m->n[c] - 1) continue;
+                                double area = m->delta(b, cb) * m->delta(c, cc);
+                                w += area;
+                                uint64_t q[3];
+                                q[a] = node[a];
+                                q[b] = cb;
+                                q[c] = cc;
+                                if (s->at(q[0], q[1], q[2])) w_in += area;
+                            }
+                        }
+                        share = w > 0.0 ? w_in / w : 0.0;
+                    } else {
+                        if (node[b] + 1 >= m->n[b] || node[c] + 1 >= m->n[c]) continue;
+                        double w_in = 0.0, w = 0.0;
+                        for (int da = -1; da <= 0; ++da) {
+                            if (node[a] == 0 && da < 0) continue;
+                            uint64_t ca = node[a] + da;
+                            if (ca >= m->n[a] - 1) continue;
+                            double len = m->delta(a, ca);
+                            w += len;
+                            uint64_t q[3] = {node[0], node[1], node[2]};
+                            q[a] = ca;
+                            if (s->at(q[0], q[1], q[2])) w_in += len;
+                        }
+                        share = w > 0.0 ? w_in / w : 0.0;
+                    }
+                    if (share > 0.0)
+                        for (const Pole& p : poles) {
+                            Pole q = p.scaled(share);
+                            if (q.p1 == 0.0) continue;  // Pole::is_null
+                            d->entries.push_back(Entry{field, axis, {node[0], node[1], node[2]}, q});
+                        }
+                }
+    }
+    return EMS_OK;
+}
+
+int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    for (const Entry& e : d->entries) {
+        bool exists = e.node[0] < m->n[0] && e.node[1] < m->n[1] && e.node[2] < m->n[2];
+        int a = e.axis, b = next_axis(a), c = prev_axis(a);
+        exists = exists && (e.field == 0 ? e.node[a] + 1 < m->n[a] : (e.node[b] + 1 < m->n[b] && e.node[c] + 1 < m->n[c]));
+        if (!exists) return set_err(m, "dispersive edge outside the grid"), -1;
+    }
+    // Dispersive::install (src/engine/dispersive.rs:2054-2300): entries in
+    // edge order (stable: an edge keeps its insertion order), branch
+    // constants from the pole and the edge geometry.
+    std::vector<uint32_t> order(d->entries.size());
+    for (size_t q = 0; q < order.size(); ++q) order[q] = (uint32_t)q;
+    auto key = [&](uint32_t q) {
+        const Entry& e = d->entries[q];
+        return std::make_tuple(e.node[0], e.field, e.axis, e.node[1], e.node[2]);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_POLES;
+    const double dt = m->dt;
+    bool have_last = false;
+    std::tuple<uint64_t, int, int, uint64_t, uint64_t> last;
+    bool skip_edge = false;
+    for (uint32_t q : order) {
+        const Entry& e = d->entries[q];
+        auto k = key(q);
+        const bool new_edge = !have_last || last != k;
+        last = k;
+        have_last = true;
+        const int a = e.axis, b = next_axis(a), c = prev_axis(a);
+        const uint64_t idx = m->index(e.node[0], e.node[1], e.node[2]);
+        double geo, x0;
+        float coef;
+        if (e.field == 0) {
+            coef = m->co[3 + a][idx];
+            x0 = EPS0;
+            geo = m->dual_delta(b, e.node[b]) * m->dual_delta(c, e.node[c]) / m->delta(a, e.node[a]);
+        } else {
+            coef = m->co[9 + a][idx];
+            x0 = MU0;
+            geo = m->delta(b, e.node[b]) * m->delta(c, e.node[c]) / m->dual_delta(a, e.node[a]);
+        }
+        const double mm = x0 * geo;
+        if (new_edge) skip_edge = coef == 0.0f;
+        if (skip_edge) continue;
+        OpStore::Side& side = e.field == 0 ? op->pe : op->ph;
+        if (new_edge) {
+            side.axis.push_back((uint8_t)a);
+            side.node.push_back(idx);
+            side.sum_inv_z.push_back(0.0);
+            side.pole_end.push_back(side.pole_end.empty() ? 0 : side.pole_end.back());
+        }
+        const Pole& p = e.pole;
+        double l = 0.0, r = 0.0, inv_c = 0.0;
+        if (p.kind == 0) {  // Lorentz
+            l = 1.0 / (mm * p.p1 * p.p1);
+            r = p.p3 * l;
+            inv_c = p.p2 * p.p2 * l;
+        } else if (p.kind == 1) {  // Drude (omega_p, gamma)
+            l = 1.0 / (mm * p.p1 * p.p1);
+            r = p.p2 * l;
+            inv_c = 0.0;
+        }
+        if (scheme == 1 && p.kind != 2) {
+            // Pole::leapfrog (src/engine/dispersive.rs:391-407).
+            double dd = l / dt + 0.5 * r;
+            side.kind.push_back(EMS_POLE_LEAPFROG);
+            side.a.push_back((l / dt - 0.5 * r) / dd);
+            side.inv_c.push_back(inv_c);
+            side.inv_z.push_back(1.0 / dd);
+            side.half_l.push_back(0.5 * l);
+        } else {
+            // Pole::branch (src/engine/dispersive.rs:361-384).
+            if (p.kind == 2) {
+                double cc = mm * p.p1;
+                l = 0.0;
+                r = p.p2 / cc;
+                inv_c = 1.0 / cc;
+            }
+            double aa = 2.0 * l / dt;
+            double z = aa + r + 0.5 * dt * inv_c;
+            double inv_z = 1.0 / z;
+            side.kind.push_back(EMS_POLE_TRAPEZOIDAL);
+            side.a.push_back(aa);
+            side.inv_c.push_back(inv_c);
+            side.inv_z.push_back(inv_z);
+            side.half_l.push_back(0.25 * aa * dt);
+            side.sum_inv_z.back() += inv_z;
+        }
+        side.pole_end.back() += 1;
+    }
+    op->pe.fill(op->poles.electric);
+    op->ph.fill(op->poles.magnetic);
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, int wave,
+                              double f0, double fc, double amplitude, uint64_t n_steps) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    if (axis < 0 || axis > 2 || !(r > 0.0) || !std::isfinite(r)) return set_err(m, "invalid lumped port"), -1;
+    // LumpedBox::new / check_fits (src/engine/lumped.rs:145-215).
+    for (int t = 0; t < 3; ++t)
+        if (lo[t] > hi[t] || hi[t] >= m->n[t]) return set_err(m, "lumped box outside the grid"), -1;
+    if (lo[axis] >= hi[axis]) return set_err(m, "lumped box degenerate along its axis"), -1;
+    const int a = axis, b = next_axis(axis), c = prev_axis(axis);
+    std::vector<uint64_t> edges;
+    for (uint64_t pb = lo[b]; pb <= hi[b]; ++pb)
+        for (uint64_t pc = lo[c]; pc <= hi[c]; ++pc)
+            for (uint64_t pa = lo[a]; pa < hi[a]; ++pa) {
+                uint64_t p[3];
+                p[a] = pa;
+                p[b] = pb;
+                p[c] = pc;
+                edges.push_back(m->index(p[0], p[1], p[2]));
+            }
+    const double series = (double)(hi[a] - lo[a]);
+    const double cols = (double)((hi[b] - lo[b] + 1) * (hi[c] - lo[c] + 1));
+    for (uint64_t e : edges)
+        if (m->co[3 + a][e] == 0.0f) return set_err(m, "lumped element edge is PEC"), -1;
+    // LumpedElement::resistor edge_parts: g_e = M/(N·R) (src/engine/lumped.rs:846-852),
+    // folded by fold_parallel (src/engine/lumped.rs:275-282).
+    const double g_e = series / (cols * r);
+    const double dt = m->dt;
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_LUMPED;
+    for (uint64_t e : edges) {
+        double ca = (double)m->co[a][e], cb = (double)m->co[3 + a][e];
+        double cap = dt * (1.0 + ca) / (2.0 * cb) + 0.0;
+        double cond = (1.0 - ca) / cb + g_e;
+        double den = cap + 0.5 * cond * dt;
+        m->co[a][e] = (float)((cap - 0.5 * cond * dt) / den);
+        m->co[3 + a][e] = (float)(dt / den);
+        op->lnode.push_back(e);
+        op->lcb.push_back((double)m->co[3 + a][e]);
+        op->lg.push_back(g_e);
+        op->lw.push_back(1.0 / series);
+        op->lrg.push_back(g_e);
+        op->lrc.push_back(0.0);
+    }
+    // Source value amplitude·w(t) at (n + 1/2)·dt (src/engine/lumped.rs:1136-1148).
+    for (uint64_t s = 0; s < n_steps; ++s)
+        op->lamp.push_back(amplitude * ems_waveform_value(wave, f0, fc, ((double)s + 0.5) * dt, dt));
+    ems_lumped& L = op->lumped;
+    L.axis = a;
+    L.n_edges = edges.size();
+    L.node = op->lnode.data();
+    L.cb = op->lcb.data();
+    L.g_src = op->lg.data();
+    L.series = hi[a] - lo[a];
+    L.src_in_branch = 0;
+    L.src_w = op->lw.data();
+    L.n_src_amp = op->lamp.size();
+    L.src_amp = op->lamp.data();
+    L.has_branch = 0;
+    L.record = 1;
+    L.rec_g = op->lrg.data();
+    L.rec_c = op->lrc.data();
+    L.port_columns = (uint64_t)cols;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+int ems_model_add_source(ems_model* m, int kind, size_t n, const int* axis, const uint64_t* nodes, const double* weight,
+                         int wave, double f0, double fc, uint64_t n_steps) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    if (kind < 0 || kind > 3) return set_err(m, "invalid source kind"), -1;
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_SOURCE;
+    for (size_t e = 0; e < n; ++e) {
+        const uint64_t* p = nodes + 3 * e;
+        if (axis[e] < 0 || axis[e] > 2 || p[0] >= m->n[0] || p[1] >= m->n[1] || p[2] >= m->n[2])
+            return set_err(m, "source edge outside the grid"), -1;
+        op->axis.push_back((uint8_t)axis[e]);
+        op->node.push_back(m->index(p[0], p[1], p[2]));
+        op->fw.push_back((float)weight[e]);
+    }
+    const double dt = m->dt;
+    // Sample time of each kind (src/engine/excite.rs:104-173).
+    for (uint64_t s = 0; s < n_steps; ++s) {
+        double t = kind == EMS_SOFT_E ? ((double)s + 0.5) * dt
+                   : kind == EMS_HARD_E ? ((double)s + 1.0) * dt
+                   : kind == EMS_SOFT_H ? (double)s * dt
+                                        : ((double)s + 0.5) * dt;
+        op->famp.push_back((float)ems_waveform_value(wave, f0, fc, t, dt));
+    }
+    ems_source& S = op->source;
+    S.kind = kind;
+    S.n_edges = n;
+    S.axis = op->axis.data();
+    S.node = op->node.data();
+    S.weight = op->fw.data();
+    S.n_amp = op->famp.size();
+    S.amp = op->famp.data();
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+int ems_model_add_source_table(ems_model* m, int kind, size_t n, const int* axis, const uint64_t* nodes,
+                               const double* weight, const double* amp, uint64_t n_steps) {
+    if (!amp && n_steps) return set_err(m, "missing amplitude table"), -1;
+    int k = ems_model_add_source(m, kind, n, axis, nodes, weight, -1, 0.0, 0.0, 0);
+    if (k < 0) return k;
+    OpStore& op = *m->ops[(size_t)k];
+    // EdgeSource::apply: amplitude(t) as f32 (src/engine/excite.rs:104-106).
+    op.famp.resize(n_steps);
+    for (uint64_t s = 0; s < n_steps; ++s) op.famp[s] = (float)amp[s];
+    op.source.n_amp = op.famp.size();
+    op.source.amp = op.famp.data();
+    m->refresh_desc();
+    return k;
+}
+
+int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, const uint64_t* nodes,
+                        const double* weight, uint64_t interval) {
+    if (quantity < 0 || quantity > 1) return set_err(m, "invalid probe quantity"), -1;
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_PROBE;
+    for (size_t e = 0; e < n; ++e) {
+        const uint64_t* p = nodes + 3 * e;
+        if (axis[e] < 0 || axis[e] > 2 || p[0] >= m->n[0] || p[1] >= m->n[1] || p[2] >= m->n[2])
+            return set_err(m, "probe entry outside the grid"), -1;
+        op->axis.push_back((uint8_t)axis[e]);
+        op->node.push_back(m->index(p[0], p[1], p[2]));
+        op->dw.push_back(weight[e]);
+    }
+    ems_probe& P = op->probe;
+    P.quantity = quantity;
+    P.n_entries = n;
+    P.axis = op->axis.data();
+    P.node = op->node.data();
+    P.weight = op->dw.data();
+    P.interval = interval ? interval : 1;
+    P.f32_sum = 0;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+const ems_engine_desc* ems_model_desc(ems_model* m) {
+    if (!m->built) return nullptr;
+    m->refresh_desc();
+    return &m->desc;
+}
+
+// phase_cycles (src/post/dft.rs:190-203): f·(t0 + n·dt) modulo one cycle.
+static double phase_cycles(double f, double t0, double dt, double n) {
+    double a = f * dt;
+    double p = a * n;
+    double e = std::fma(a, n, -p);
+    double c = f * t0;
+    double x = (p - std::trunc(p)) + e + (c - std::trunc(c));
+    return x - std::trunc(x);
+}
+
+void ems_dft(double t0, double dt, const double* x, size_t n, const double* freqs, size_t nf, double* re, double* im) {
+    for (size_t q = 0; q < nf; ++q) {
+        double sr = 0.0, si = 0.0;
+        for (size_t s = 0; s < n; ++s) {
+            double ph = -TAU * phase_cycles(freqs[q], t0, dt, (double)s);
+            sr += x[s] * std::cos(ph);
+            si += x[s] * std::sin(ph);
+        }
+        re[q] = sr * dt;
+        im[q] = si * dt;
+    }
+}
+
+// drive (src/engine/run.rs:424-540), the invariant measure without a settle test.
+int ems_drive(const ems_stepper* s, const ems_run_limits* lim, ems_run_outcome* out) {
+    if (!s || !lim || !out) return EMS_ERR_INVALID;
+    const uint64_t interval = lim->check_interval ? lim->check_interval : 50;
+    const uint64_t max = lim->max_timesteps;
+    uint64_t steps = 0, checks = 0;
+    double w = 0.0, w_max = 0.0, ratio_db = 0.0;
+    int reason;
+    for (;;) {
+        if (steps >= max) { reason = 1; break; }
+        const uint64_t n = steps;  // timestep of a fresh engine
+        if (s->step_with_energy(s->ctx, &w) != 0) { reason = 3; break; }
+        ++steps;
+        ++checks;
+        w_max = std::max(w_max, w);
+        double ratio = w_max > 0.0 ? w / w_max : 1.0;
+        ratio_db = ratio > 0.0 ? 10.0 * std::log10(ratio) : -INFINITY;
+        double t = (double)n * lim->dt;
+        if (!std::isfinite(w) || w < -1e-12 * w_max) { reason = 2; break; }
+        if (lim->has_end_criteria && (!lim->has_excitation_end || t > lim->excitation_end) && w_max > 0.0 &&
+            ratio < lim->energy_ratio) {
+            reason = 0;
+            break;
+        }
+        uint64_t chunk = std::min(interval - 1, max - steps);
+        if (chunk && s->run(s->ctx, chunk) != 0) { reason = 3; break; }
+        steps += chunk;
+    }
+    out->reason = reason;
+    out->steps = steps;
+    out->energy = w;
+    out->max_energy = w_max;
+    out->ratio_db = ratio_db;
+    out->checks = checks;
+    return EMS_OK;
+}
+
+}  // extern "C"

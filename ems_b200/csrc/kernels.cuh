@@ -1,0 +1,400 @@
+// kernels.cuh — device kernels of the B200 FDTD engine (sm_100a).
+//
+// Every field update uses explicitly rounded IEEE operations (__fmul_rn,
+// __fadd_rn, __fsub_rn and their f64 forms), so no multiply-add is ever
+// contracted and each value is the reference's expression bit for bit.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace emsk {
+
+constexpr unsigned kRowThreads = 128;  // threads of a z-row block
+constexpr uint32_t kMaxPoles = 16;     // poles per edge held in registers
+
+struct Grid {
+    uint32_t nx, ny, nz, pitch;  // pitch: padded z-row length (multiple of 32)
+    uint64_t n, np;              // nodes, padded nodes
+};
+
+struct Fields {
+    float* u[3];
+    float* i[3];
+};
+
+struct Coeffs {
+    const float* c[12];
+};
+
+struct SlabDev {
+    int e_side, comp, normal, other;
+    float sign;
+    uint32_t lo[3], hi[3];
+    const float* b;
+    const float* a;
+    const float* k;
+    float* psi;
+};
+
+struct PoleSideDev {
+    size_t n_edges = 0, n_poles = 0;
+    const uint8_t* axis = nullptr;
+    const uint32_t* node = nullptr;
+    const double* sum_inv_z = nullptr;
+    const uint32_t* pole_end = nullptr;
+    const uint8_t* kind = nullptr;
+    const double* a = nullptr;
+    const double* inv_c = nullptr;
+    const double* inv_z = nullptr;
+    const double* half_l = nullptr;
+    float* prev = nullptr;
+    double* j = nullptr;
+    double* q = nullptr;
+};
+
+struct LumpedDevT {
+    uint32_t n = 0;
+    double series = 1.0, columns = 0.0;
+    int src_in_branch = 0, has_branch = 0, record = 0;
+    const uint32_t* node = nullptr;
+    const double* cb = nullptr;
+    const double* g_src = nullptr;
+    const double* src_w = nullptr;
+    const double* two_l_dt = nullptr;
+    const double* inv_c = nullptr;
+    const double* z = nullptr;
+    const double* rec_g = nullptr;
+    const double* rec_c = nullptr;
+    double* v = nullptr;
+    double* bj = nullptr;
+    double* bq = nullptr;
+    double* bu_prev = nullptr;
+    double* j_avg = nullptr;
+    double* ru_prev = nullptr;
+};
+
+struct ProbeDevT {
+    uint32_t n = 0;
+    int f32_sum = 0;
+    const uint32_t* node = nullptr;
+    const uint8_t* axis = nullptr;
+    const double* weight = nullptr;
+};
+
+// Rounds subnormal results to zero (src/engine/kernel.rs:30-33).
+__device__ __forceinline__ float flush(float x) { return fabsf(x) < FLT_MIN ? 0.0f : x; }
+
+// flush(ca·u + cb·((a − b) − (c − d))) (src/engine/kernel.rs:252-273).
+__device__ __forceinline__ float e_upd(float ca, float u, float cb, float a, float b, float c, float d) {
+    return flush(__fadd_rn(__fmul_rn(ca, u), __fmul_rn(cb, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));
+}
+
+// flush(da·h − db·((a − b) − (c − d))) (src/engine/kernel.rs:58-79).
+__device__ __forceinline__ float h_upd(float da, float h, float db, float a, float b, float c, float d) {
+    return flush(__fsub_rn(__fmul_rn(da, h), __fmul_rn(db, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));
+}
+
+// (1 + a)·p/b, 0 where b = 0 (src/engine/kernel.rs:116-120).
+__device__ __forceinline__ double weight(float a, double p, float b) {
+    return b != 0.0f ? __ddiv_rn(__dmul_rn(__dadd_rn(1.0, (double)a), p), (double)b) : 0.0;
+}
+
+// Block-wide f64 sum in a fixed order; result valid in thread 0.
+template <unsigned THREADS>
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+    const unsigned w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (unsigned q = 0; q < THREADS / 32; ++q) s = __dadd_rn(s, sh[q]);
+    return s;
+}
+
+// H update of every dual edge (src/engine/kernel.rs:447-511, 571-618);
+// with ENERGY each block also writes its share of the energy invariant
+// Σ (1+ca)/cb·u² + Σ (1+da)/db·i_old·i_new in units of dt/4
+// (src/engine/kernel.rs:132-244).
+template <bool ENERGY>
+__global__ void __launch_bounds__(kRowThreads) k_update_h(Grid g, Fields f, Coeffs c, double* partials) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = blockIdx.y, i = blockIdx.z;
+    double w = 0.0;
+    if (k < g.nz) {
+        const uint32_t sj = g.pitch, si = g.ny * g.pitch;
+        const uint32_t idx = i * si + j * sj + k;
+        const float ux = f.u[0][idx], uy = f.u[1][idx], uz = f.u[2][idx];
+        if (ENERGY) {
+            w = __dadd_rn(w, weight(c.c[0][idx], __dmul_rn((double)ux, (double)ux), c.c[3][idx]));
+            w = __dadd_rn(w, weight(c.c[1][idx], __dmul_rn((double)uy, (double)uy), c.c[4][idx]));
+            w = __dadd_rn(w, weight(c.c[2][idx], __dmul_rn((double)uz, (double)uz), c.c[5][idx]));
+        }
+        if (j + 1 < g.ny && k + 1 < g.nz) {
+            const float old = f.i[0][idx];
+            const float da = c.c[6][idx], db = c.c[9][idx];
+            const float nw = h_upd(da, old, db, f.u[2][idx + sj], uz, f.u[1][idx + 1], uy);
+            f.i[0][idx] = nw;
+            if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
+        }
+        if (i + 1 < g.nx && k + 1 < g.nz) {
+            const float old = f.i[1][idx];
+            const float da = c.c[7][idx], db = c.c[10][idx];
+            const float nw = h_upd(da, old, db, f.u[0][idx + 1], ux, f.u[2][idx + si], uz);
+            f.i[1][idx] = nw;
+            if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
+        }
+        if (i + 1 < g.nx && j + 1 < g.ny) {
+            const float old = f.i[2][idx];
+            const float da = c.c[8][idx], db = c.c[11][idx];
+            const float nw = h_upd(da, old, db, f.u[1][idx + si], uy, f.u[0][idx + sj], ux);
+            f.i[2][idx] = nw;
+            if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
+        }
+    }
+    if (ENERGY) {
+        double s = block_sum<kRowThreads>(w);
+        if (threadIdx.x == 0)
+            partials[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// Sums the per-block energy shares in a fixed order.
+__global__ void __launch_bounds__(1024) k_reduce_partials(const double* partials, size_t n, double* out) {
+    double s = 0.0;
+    for (size_t q = threadIdx.x; q < n; q += blockDim.x) s = __dadd_rn(s, partials[q]);
+    double t = block_sum<1024>(s);
+    if (threadIdx.x == 0) out[0] = t;
+}
+
+// E update of every edge (src/engine/kernel.rs:624-697).
+__global__ void __launch_bounds__(kRowThreads) k_update_e(Grid g, Fields f, Coeffs c) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = blockIdx.y, i = blockIdx.z;
+    if (k >= g.nz) return;
+    const uint32_t sj = g.pitch, si = g.ny * g.pitch;
+    const uint32_t idx = i * si + j * sj + k;
+    const float ix = f.i[0][idx], iy = f.i[1][idx], iz = f.i[2][idx];
+    if (i + 1 < g.nx) {
+        const float b = j > 0 ? f.i[2][idx - sj] : 0.0f;
+        const float d = k > 0 ? f.i[1][idx - 1] : 0.0f;
+        f.u[0][idx] = e_upd(c.c[0][idx], f.u[0][idx], c.c[3][idx], iz, b, iy, d);
+    }
+    if (j + 1 < g.ny) {
+        const float b = k > 0 ? f.i[0][idx - 1] : 0.0f;
+        const float d = i > 0 ? f.i[2][idx - si] : 0.0f;
+        f.u[1][idx] = e_upd(c.c[1][idx], f.u[1][idx], c.c[4][idx], ix, b, iz, d);
+    }
+    if (k + 1 < g.nz) {
+        const float b = i > 0 ? f.i[1][idx - si] : 0.0f;
+        const float d = j > 0 ? f.i[0][idx - sj] : 0.0f;
+        f.u[2][idx] = e_upd(c.c[2][idx], f.u[2][idx], c.c[5][idx], iy, b, ix, d);
+    }
+}
+
+// CPML correction of one slab (src/engine/boundary/cpml.rs:445-520, 657-676):
+// s = sign·(h − l); ψ = flush(b·ψ + a·s); t = flush(t + scale·coef·(k·s + ψ)).
+template <bool E_SIDE>
+__global__ void k_cpml(Grid g, Fields f, Coeffs c, SlabDev s) {
+    const uint32_t k = s.lo[2] + blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = s.lo[1] + blockIdx.y, i = s.lo[0] + blockIdx.z;
+    if (k >= s.hi[2]) return;
+    const uint32_t si = g.ny * g.pitch;
+    const uint32_t idx = i * si + j * g.pitch + k;
+    const uint32_t node[3] = {i, j, k};
+    const uint32_t step = s.normal == 0 ? si : (s.normal == 1 ? g.pitch : 1u);
+    const uint32_t d = node[s.normal] - s.lo[s.normal];
+    float h, l;
+    float* t;
+    float coef;
+    if (E_SIDE) {
+        const float* src = f.i[s.other];
+        h = src[idx];
+        l = node[s.normal] == 0 ? 0.0f : src[idx - step];
+        t = f.u[s.comp];
+        coef = c.c[3 + s.comp][idx];
+    } else {
+        const float* src = f.u[s.other];
+        h = src[idx + step];
+        l = src[idx];
+        t = f.i[s.comp];
+        coef = -c.c[9 + s.comp][idx];
+    }
+    const uint32_t n1 = s.hi[1] - s.lo[1], n2 = s.hi[2] - s.lo[2];
+    const uint32_t q = ((i - s.lo[0]) * n1 + (j - s.lo[1])) * n2 + (k - s.lo[2]);
+    const float sv = __fmul_rn(s.sign, __fsub_rn(h, l));
+    const float psi = flush(__fadd_rn(__fmul_rn(s.b[d], s.psi[q]), __fmul_rn(s.a[d], sv)));
+    s.psi[q] = psi;
+    t[idx] = flush(__fadd_rn(t[idx], __fmul_rn(coef, __fadd_rn(__fmul_rn(s.k[d], sv), psi))));
+}
+
+// Dispersive correction of one edge per thread (src/engine/dispersive.rs:1392-1470).
+__global__ void k_poles_correct(Grid g, Fields f, Coeffs c, PoleSideDev p, bool electric, double dt) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n_edges) return;
+    (void)g;
+    const int ax = p.axis[e];
+    const uint32_t idx = p.node[e];
+    float* fld = electric ? f.u[ax] : f.i[ax];
+    const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
+    const uint32_t p0 = e ? p.pole_end[e - 1] : 0u, p1 = p.pole_end[e];
+    const double prev = (double)p.prev[e];
+    const double half_prev = __dmul_rn(0.5, prev);
+    const double u_star = (double)fld[idx];
+    double s = 0.0;
+    double nj[kMaxPoles], nq[kMaxPoles];
+    for (uint32_t q = p0; q < p1; ++q) {
+        const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
+        if (p.kind[q] == 1) {  // leapfrog: j^{n+1/2} from u^n, then q^{n+1}
+            const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
+            nj[q - p0] = jn;
+            nq[q - p0] = __dadd_rn(qq, __dmul_rn(dt, jn));
+            s = __dadd_rn(s, jn);
+        } else {
+            s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
+        }
+    }
+    const float u_new = (float)__ddiv_rn(__dsub_rn(u_star, __dmul_rn(cb, s)),
+                                         __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), p.sum_inv_z[e])));
+    const double half_new = __dmul_rn(0.5, (double)u_new);
+    for (uint32_t q = p0; q < p1; ++q) {
+        if (p.kind[q] == 1) {
+            p.j[q] = nj[q - p0];
+            p.q[q] = nq[q - p0];
+        } else {
+            const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
+            const double kk = __dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev);
+            const double jb = __dmul_rn(__dadd_rn(kk, half_new), iz);
+            p.j[q] = __dsub_rn(__dmul_rn(2.0, jb), jq);
+            p.q[q] = __dadd_rn(qq, __dmul_rn(dt, jb));
+        }
+    }
+    fld[idx] = u_new;
+}
+
+// Saves the field value of every edge (src/engine/dispersive.rs:1173-1180).
+__global__ void k_poles_capture(Fields f, PoleSideDev p, bool electric) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n_edges) return;
+    p.prev[e] = (electric ? f.u[p.axis[e]] : f.i[p.axis[e]])[p.node[e]];
+}
+
+// Edge source (src/engine/excite.rs:104-117): soft adds w·a, hard sets w·a.
+__global__ void k_source(float* f0, float* f1, float* f2, const uint8_t* axis, const uint32_t* node,
+                         const float* weight, size_t n, float a, bool hard) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    float* F = axis[e] == 0 ? f0 : (axis[e] == 1 ? f1 : f2);
+    const float v = __fmul_rn(weight[e], a);
+    F[node[e]] = hard ? v : __fadd_rn(F[node[e]], v);
+}
+
+// Probe sample: Σ w·x in entry order (src/engine/probe.rs:381-392).
+__global__ void k_probe(const float* f0, const float* f1, const float* f2, ProbeDevT p, double* out) {
+    if (threadIdx.x != 0) return;
+    if (p.f32_sum) {
+        float s = 0.0f;
+        for (uint32_t e = 0; e < p.n; ++e) {
+            const float* F = p.axis[e] == 0 ? f0 : (p.axis[e] == 1 ? f1 : f2);
+            s = __fadd_rn(s, __fmul_rn((float)p.weight[e], F[p.node[e]]));
+        }
+        out[0] = (double)s;
+    } else {
+        double s = 0.0;
+        for (uint32_t e = 0; e < p.n; ++e) {
+            const float* F = p.axis[e] == 0 ? f0 : (p.axis[e] == 1 ? f1 : f2);
+            s = __dadd_rn(s, __dmul_rn(p.weight[e], (double)F[p.node[e]]));
+        }
+        out[0] = s;
+    }
+}
+
+// Lumped element pre_e: saves u^n (src/engine/lumped.rs:1106-1121).
+__global__ void k_lumped_pre_e(const float* u, LumpedDevT d) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.n) return;
+    const double x = (double)u[d.node[e]];
+    if (d.has_branch) d.bu_prev[e] = x;
+    if (d.record) d.ru_prev[e] = x;
+}
+
+// Lumped element post_e (src/engine/lumped.rs:1123-1236) and, for a port,
+// V = Σu/columns, I = −record (src/engine/port.rs:276-290). One block: the
+// per-edge updates in parallel, the sums in edge order by thread 0.
+__global__ void __launch_bounds__(256) k_lumped_post_e(float* u, LumpedDevT d, double val, int active, double dt,
+                                                       double* rec_out, double* pv_out, double* pi_out) {
+    for (uint32_t e = threadIdx.x; e < d.n; e += blockDim.x) {
+        const uint32_t idx = d.node[e];
+        if (d.src_w) d.v[e] = active ? __dadd_rn(0.0, __dmul_rn(d.src_w[e], val)) : 0.0;
+        if (active && !d.src_in_branch) {
+            const double add = __dmul_rn(__dmul_rn(d.cb[e], d.g_src[e]), d.v[e]);
+            if (add != 0.0) u[idx] = (float)__dadd_rn((double)u[idx], add);
+        }
+        if (d.has_branch) {
+            const double v_br = (active && d.src_in_branch) ? d.v[e] : 0.0;
+            const double u_star = (double)u[idx];
+            const double kk = __dadd_rn(__dsub_rn(__dsub_rn(__dmul_rn(d.two_l_dt[e], d.bj[e]), __dmul_rn(d.bq[e], d.inv_c[e])), v_br),
+                                        __dmul_rn(0.5, d.bu_prev[e]));
+            const double z = d.z[e], cb = d.cb[e];
+            const double u_new = __ddiv_rn(__dsub_rn(__dmul_rn(z, u_star), __dmul_rn(cb, kk)), __dadd_rn(z, __dmul_rn(0.5, cb)));
+            const double jb = __ddiv_rn(__dadd_rn(kk, __dmul_rn(0.5, u_new)), z);
+            d.bj[e] = __dsub_rn(__dmul_rn(2.0, jb), d.bj[e]);
+            d.bq[e] = __dadd_rn(d.bq[e], __dmul_rn(dt, jb));
+            d.j_avg[e] = jb;
+            u[idx] = (float)u_new;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double rec = 0.0;
+    if (d.record) {
+        double sum = 0.0;
+        for (uint32_t e = 0; e < d.n; ++e) {
+            const double u0 = d.ru_prev[e], u1 = (double)u[d.node[e]];
+            const double v = (active && !d.src_in_branch) ? d.v[e] : 0.0;
+            const double t1 = __dmul_rn(d.rec_g[e], __dsub_rn(__dmul_rn(0.5, __dadd_rn(u0, u1)), v));
+            const double t2 = __ddiv_rn(__dmul_rn(d.rec_c[e], __dsub_rn(u1, u0)), dt);
+            sum = __dadd_rn(sum, __dadd_rn(t1, t2));
+            if (d.has_branch) sum = __dadd_rn(sum, d.j_avg[e]);
+        }
+        rec = __ddiv_rn(sum, d.series);
+        rec_out[0] = rec;
+    }
+    if (pv_out) {
+        pi_out[0] = -rec;
+        double s = 0.0;
+        for (uint32_t e = 0; e < d.n; ++e) s = __dadd_rn(s, (double)u[d.node[e]]);
+        pv_out[0] = __ddiv_rn(s, d.columns);
+    }
+}
+
+// Σ ½·L·j² + ½·q²/C_p of the electric then the magnetic poles
+// (src/engine/dispersive.rs:1488-1506, 2598-2618).
+__global__ void __launch_bounds__(1024) k_pole_energy(PoleSideDev e, PoleSideDev h, double* out) {
+    double s = 0.0;
+    for (int side = 0; side < 2; ++side) {
+        const PoleSideDev& p = side == 0 ? e : h;
+        for (size_t q = threadIdx.x; q < p.n_poles; q += blockDim.x) {
+            const double a = __dmul_rn(__dmul_rn(p.half_l[q], p.j[q]), p.j[q]);
+            const double b = __dmul_rn(__dmul_rn(__dmul_rn(0.5, p.inv_c[q]), p.q[q]), p.q[q]);
+            s = __dadd_rn(s, __dadd_rn(a, b));
+        }
+    }
+    const double t = block_sum<1024>(s);
+    if (threadIdx.x == 0) out[0] = t;
+}
+
+// Σ ½·L_e·j² + ½·q²/C_e of a lumped branch (src/engine/lumped.rs:1066-1077).
+__global__ void k_branch_energy(LumpedDevT d, double dt, double* out) {
+    double s = 0.0;
+    for (uint32_t e = 0; e < d.n; ++e) {
+        const double half_l = __dmul_rn(__dmul_rn(0.25, d.two_l_dt[e]), dt);
+        s = __dadd_rn(s, __dadd_rn(__dmul_rn(__dmul_rn(half_l, d.bj[e]), d.bj[e]),
+                                   __dmul_rn(__dmul_rn(__dmul_rn(0.5, d.inv_c[e]), d.bq[e]), d.bq[e])));
+    }
+    out[0] = s;
+}
+
+}  // namespace emsk

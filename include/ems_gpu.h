@@ -1,0 +1,234 @@
+/*
+ * ems_gpu.h — C ABI of the B200 FDTD time-stepping engine.
+ *
+ * This is the drop-in boundary for the time stepping of the ems FDTD
+ * solver: it replaces `pool::drive` and the per-step work of the operators
+ * that run inside it (src/engine/pool.rs:884-940, src/engine/mod.rs:833-992).
+ * The host keeps everything above it (mesh compilation, coefficient and
+ * operator set-up, ports, post-processing) and hands the engine, once, the
+ * tables those steps produce; the engine then advances the fields on one
+ * GPU and returns probe samples, port series and energies.
+ *
+ * Conventions (those of the reference engine, src/engine/mod.rs:21-62):
+ *  - a node [i, j, k] has the linear index (i*ny + j)*nz + k (z fastest);
+ *    every field and coefficient array has one entry per node;
+ *  - u[a] are the E edge voltages, i[a] the H dual-edge currents of axis a;
+ *  - one step: i^{n-1/2} -> i^{n+1/2} (H), then u^n -> u^{n+1} (E);
+ *  - coefficient lanes: ca 0-2, cb 3-5, da 6-8, db 9-11 (src/engine/coeffs.rs:327-391).
+ *
+ * All tables are copied at ems_gpu_create; the caller keeps ownership of
+ * its buffers. One handle = one CUDA stream; a handle is not thread-safe.
+ * Every call returns an ems_status; the text of the last error of a handle
+ * is ems_gpu_last_error(h).
+ */
+#ifndef EMS_GPU_H
+#define EMS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+typedef enum {
+    EMS_OK = 0,
+    EMS_ERR_INVALID = 1,  /* invalid argument or table                 */
+    EMS_ERR_CUDA = 2,     /* a CUDA call failed                          */
+    EMS_ERR_DIVERGED = 3, /* NaN/Inf found in a checked quantity         */
+    EMS_ERR_TIMEOUT = 4,  /* a bounded device wait ran out               */
+    EMS_ERR_NOMEM = 5     /* device or host allocation failed            */
+} ems_status;
+
+/* Operator kinds, in the order the engine runs their hooks within a
+ * half-step (the registration order of the descriptor decides between
+ * operators of the same hook). */
+typedef enum {
+    EMS_OP_CPML = 1,   /* slab hooks post_h / post_e   (src/engine/boundary/cpml.rs:816-883) */
+    EMS_OP_POLES = 2,  /* slab hooks post_h / post_e   (src/engine/dispersive.rs:1687-1744)  */
+    EMS_OP_LUMPED = 3, /* serial pre_e / post_e        (src/engine/lumped.rs:1123-1236)      */
+    EMS_OP_SOURCE = 4, /* serial post_h or post_e      (src/engine/excite.rs:104-173)        */
+    EMS_OP_PROBE = 5   /* serial post_h or post_e      (src/engine/probe.rs:480-510)         */
+} ems_op_kind;
+
+/* One CPML slab: the correction of one field component in one face layer
+ * (src/engine/boundary/cpml.rs:392-520, Slab). For every node of the box
+ * lo..hi (half-open, node indices):
+ *   s = sign*(h - l)         (derivative of component `other` along `normal`)
+ *   psi = flush(b*psi + a*s)
+ *   t = flush(t + scale*coef*(k*s + psi))
+ * with t = u[comp] (E side, coef = cb, scale = +1, h/l = i[other] at the
+ * node and one node below, zero outside) or t = i[comp] (H side, coef = db,
+ * scale = -1, h/l = u[other] one node above and at the node). b, a, k are
+ * per depth index node[normal] - lo[normal]; psi starts at zero. */
+typedef struct {
+    int32_t e_side;  /* 1: corrects u (after the E update); 0: corrects i   */
+    int32_t comp;    /* corrected component axis (0 x, 1 y, 2 z)            */
+    int32_t normal;  /* layer normal axis                                   */
+    int32_t other;   /* differentiated component axis                       */
+    float sign;      /* +1 if normal == next(comp), else -1                 */
+    uint64_t lo[3];
+    uint64_t hi[3];
+    const float* b;  /* hi[normal]-lo[normal] values each */
+    const float* a;
+    const float* k;  /* 1/kappa - 1 (less a1/b for the linear rule) */
+} ems_cpml_slab;
+
+typedef struct {
+    size_t n_slabs;
+    const ems_cpml_slab* slabs; /* E and H slabs, in layer order */
+} ems_cpml;
+
+/* Pole kinds of one dispersive branch (src/engine/dispersive.rs:961-971). */
+typedef enum { EMS_POLE_TRAPEZOIDAL = 0, EMS_POLE_LEAPFROG = 1 } ems_pole_kind;
+
+/* The poles of one field type (electric: E edges; magnetic: H dual edges)
+ * of a dispersive medium (src/engine/dispersive.rs:973-1041, Side). Edges
+ * are in the reference order (plane, axis, offset); an edge's poles are
+ * [pole_end[e-1], pole_end[e]) in insertion order. Per pole: trapezoidal
+ * (a = 2L/dt, inv_c = 1/C_p, inv_z = 1/z) or leapfrog (a = k_a, inv_c,
+ * inv_z = k_b), half_l = L/2 for the energy. sum_inv_z is the sum of
+ * inv_z over the edge's trapezoidal poles. */
+typedef struct {
+    size_t n_edges;
+    const uint8_t* axis;
+    const uint64_t* node;      /* node index (i*ny+j)*nz+k */
+    const double* sum_inv_z;
+    const uint32_t* pole_end;
+    size_t n_poles;
+    const uint8_t* kind;       /* ems_pole_kind per pole */
+    const double* a;
+    const double* inv_c;
+    const double* inv_z;
+    const double* half_l;
+} ems_pole_side;
+
+typedef struct {
+    ems_pole_side electric;
+    ems_pole_side magnetic;
+} ems_poles;
+
+/* A lumped element on E edges along `axis` (src/engine/lumped.rs:880-1013
+ * install, 1123-1236 post_e). Its resistor and parallel capacitor are
+ * already folded into the uploaded ca/cb. Per edge: cb (the folded edge
+ * coefficient), g_src (conductance in series with the source), src_w
+ * (source weight, V_s share), and with a branch 2L/dt, 1/C, z; with a
+ * current record g and c. src_amp[n] is the source value at (n+1/2)*dt
+ * for step n (n < n_src_amp; 0 beyond). A port (port_columns > 0) also
+ * records V = sum(u)/columns after each step and I = -record. */
+typedef struct {
+    int32_t axis;
+    size_t n_edges;
+    const uint64_t* node;
+    const double* cb;
+    const double* g_src;
+    uint64_t series;            /* M: edges in series */
+    int32_t src_in_branch;      /* series topology: source sits in the branch */
+    const double* src_w;        /* NULL: no source */
+    size_t n_src_amp;
+    const double* src_amp;
+    int32_t has_branch;
+    const double* two_l_dt;
+    const double* inv_c;
+    const double* z;
+    int32_t record;             /* record the terminal current */
+    const double* rec_g;
+    const double* rec_c;
+    uint64_t port_columns;      /* > 0: a lumped port (src/engine/port.rs:262-290) */
+} ems_lumped;
+
+/* Edge source kinds (src/engine/excite.rs:13-40). */
+typedef enum { EMS_SOFT_E = 0, EMS_HARD_E = 1, EMS_SOFT_H = 2, EMS_HARD_H = 3 } ems_source_kind;
+
+/* An edge source: amp[n] = f32(amplitude(t_n)) for step n with t_n the
+ * kind's sample time ((n+1/2)dt soft E, (n+1)dt hard E, n dt soft H,
+ * (n+1/2)dt hard H); 0 for n >= n_amp. */
+typedef struct {
+    int32_t kind;
+    size_t n_edges;
+    const uint8_t* axis;
+    const uint64_t* node;
+    const float* weight;
+    size_t n_amp;
+    const float* amp;
+} ems_source;
+
+/* Probe quantities (src/engine/probe.rs:12-19). */
+typedef enum { EMS_PROBE_VOLTAGE = 0, EMS_PROBE_CURRENT = 1 } ems_probe_quantity;
+
+/* A probe: the weighted sum of field entries, in entry order, every
+ * `interval` steps (steps with n % interval == 0); voltage after the E
+ * update at (n+1)dt, current after the H update at (n+1/2)dt. */
+typedef struct {
+    int32_t quantity;
+    size_t n_entries;
+    const uint8_t* axis;
+    const uint64_t* node;
+    const double* weight;
+    uint64_t interval;
+    int32_t f32_sum;            /* accumulate in f32 (openEMS current probes) */
+} ems_probe;
+
+typedef struct {
+    int32_t kind; /* ems_op_kind */
+    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe* */
+} ems_op;
+
+/* Everything an engine is built from: the grid size, the time step, the
+ * twelve coefficient arrays (reference layout) and the operators in
+ * registration order. */
+typedef struct {
+    uint64_t nodes[3];
+    double dt;
+    const float* coeff[12];
+    size_t n_ops;
+    const ems_op* ops;
+} ems_engine_desc;
+
+typedef struct ems_gpu ems_gpu;
+
+/* Builds an engine on CUDA device `device` (replaces EngineBuilder::build_from
+ * + Engine::add_operator, src/engine/mod.rs:325-381, 549-572). */
+ems_status ems_gpu_create(const ems_engine_desc* desc, int device, ems_gpu** out);
+
+/* Releases all device memory of the engine. */
+ems_status ems_gpu_destroy(ems_gpu* h);
+
+/* Advances n steps (Engine::run, src/engine/mod.rs:826). */
+ems_status ems_gpu_run(ems_gpu* h, uint64_t n);
+
+/* Advances one step and returns in *energy the energy invariant W^n of the
+ * state before the step plus the operators' stored energy
+ * (Engine::step_with_energy, src/engine/mod.rs:819). */
+ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy);
+
+/* Number of completed steps. */
+ems_status ems_gpu_timestep(const ems_gpu* h, uint64_t* n);
+
+/* Copies component `axis` of u (field 0) or i (field 1) to/from `host`
+ * (nx*ny*nz floats, reference layout; Engine::u_component / fields_mut). */
+ems_status ems_gpu_download_field(ems_gpu* h, int field, int axis, float* host);
+ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* host);
+
+/* Samples of operator `op` (index into desc->ops): a probe's values
+ * (which = 0), a lumped element's current record (which = 0) or, for a
+ * port, its voltage (which = 1) and current (which = 2). Writes up to
+ * `cap` values into `out` (may be NULL) and the total count into *n. */
+ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t cap, size_t* n);
+
+/* Text of the last error of handle `h` ("" if none; a static text if h is NULL). */
+const char* ems_gpu_last_error(const ems_gpu* h);
+
+/* Device kernels launched since creation (for bookkeeping). */
+ems_status ems_gpu_launch_count(const ems_gpu* h, uint64_t* n);
+
+/* Selects the step schedule: 0 = automatic, 1 = separate H/E kernels,
+ * 2 = fused single-pass kernel. Results are identical bit for bit. */
+ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMS_GPU_H */

@@ -1,0 +1,164 @@
+/*
+ * ems_host.h — host-side model set-up and run loop of the B200 engine.
+ *
+ * The host side of the drop-in: it restates, in C++, what the reference's
+ * Rust host computes before and around the time stepping — the Cartesian
+ * grid (src/engine/grid.rs), per-cell materials (src/engine/material.rs),
+ * their per-edge averages and the update coefficients
+ * (src/engine/edge_material.rs:376-425, src/engine/coeffs.rs:327-391,
+ * 879-966), the CPML layers (src/engine/boundary/cpml.rs:979-1196), the
+ * dispersive pole tables (src/engine/dispersive.rs:1896-1985, 2054-2470),
+ * lumped ports (src/engine/lumped.rs:880-1013, src/engine/port.rs:102-160),
+ * edge sources, probes, the Gaussian waveform (src/waveform.rs:442-470),
+ * the end-criterion run loop (src/engine/run.rs:424-540) and the DFT /
+ * port analysis (src/post/dft.rs, src/post/port.rs) — and hands the engine
+ * its tables as an ems_engine_desc (include/ems_gpu.h).
+ */
+#ifndef EMS_HOST_H
+#define EMS_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ems_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ems_model ems_model;
+typedef struct ems_cellset ems_cellset;
+typedef struct ems_dispersive ems_dispersive;
+
+/* Physical constants of the reference (src/constants.rs:9-18). */
+double ems_const_eps0(void);
+double ems_const_mu0(void);
+double ems_const_c0(void);
+
+/* A model on the rectilinear grid with the given mesh lines [m]
+ * (Grid::new, src/engine/grid.rs:71-110). NULL on invalid lines. */
+ems_model* ems_model_new(const double* x, size_t nx, const double* y, size_t ny, const double* z, size_t nz);
+void ems_model_free(ems_model* m);
+const char* ems_model_error(const ems_model* m);
+void ems_model_nodes(const ems_model* m, uint64_t nodes[3]);
+
+/* Adds a material (Material, src/engine/material.rs); returns its id (0 is
+ * the vacuum background) or -1. */
+int ems_model_material(ems_model* m, const double eps_r[3], const double mu_r[3], const double kappa[3],
+                       const double sigma_m[3]);
+
+/* Cell sets: a mask over the cells, filled by boxes (cell index ranges
+ * lo..hi, half-open) and spheres (cells whose centre lies inside). */
+ems_cellset* ems_cellset_new(const ems_model* m);
+void ems_cellset_free(ems_cellset* s);
+int ems_cellset_box(ems_cellset* s, const uint64_t lo[3], const uint64_t hi[3]);
+int ems_cellset_sphere(ems_cellset* s, const double centre[3], double radius);
+uint64_t ems_cellset_count(const ems_cellset* s);
+
+/* Assigns material `mat` to the cells of `s` (CellMaterials::fill_box). */
+int ems_model_fill(ems_model* m, const ems_cellset* s, int mat);
+
+/* Marks the E edges along `axis` starting at the nodes of the box lo..hi
+ * (inclusive node ranges) as PEC (CellMaterials PEC mask). */
+int ems_model_pec_edges(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3]);
+
+/* Face conditions in x_min, x_max, y_min, y_max, z_min, z_max order
+ * (0 PEC, 1 PMC); default all PEC (FaceConditions, src/engine/coeffs.rs). */
+int ems_model_faces(ems_model* m, const int faces[6]);
+
+/* Computes dt = courant * courant_limit (TimeStep::Courant) or, with
+ * fixed_dt > 0, takes it (TimeStep::Fixed), then the coefficients
+ * (Coefficients::compute). Must precede the operators. */
+int ems_model_build(ems_model* m, double courant, double fixed_dt);
+double ems_model_dt(const ems_model* m);
+double ems_model_courant_limit(const ems_model* m);
+/* Coefficient lane `lane` (0..11) in reference layout (valid after build). */
+const float* ems_model_coeff(const ems_model* m, int lane);
+
+/* CPML layers (CpmlBoundary::new): cells[f] > 0 puts a layer of that many
+ * cells on face f with grading order m, sigma_factor, kappa_max, alpha_max
+ * and the linear (1) or constant (0) convolution. Returns the op index. */
+int ems_model_add_cpml(ems_model* m, const uint64_t cells[6], double grading, double sigma_factor,
+                       double kappa_max, double alpha_max, int linear);
+/* The refractive index the layer on `face` is tuned for (after add_cpml). */
+double ems_model_cpml_index(const ems_model* m, int face);
+
+/* Dispersive media (Dispersive, src/engine/dispersive.rs). Pole kinds:
+ * 0 Lorentz (omega_p, omega_0, gamma), 1 Drude (omega_p, gamma, -),
+ * 2 Debye (delta_eps, tau, -); frequencies in rad/s. */
+ems_dispersive* ems_dispersive_new(void);
+void ems_dispersive_free(ems_dispersive* d);
+/* Fills the cells of `s` with the poles for `field` (0 electric, 1
+ * magnetic): every edge touching them gets each pole scaled by the share
+ * of its averaging volume inside (Dispersive::fill_cells). */
+int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset* s, int field, size_t n_poles,
+                        const int* kind, const double* p1, const double* p2, const double* p3);
+/* Installs the medium with scheme 0 trapezoidal / 1 leapfrog; op index. */
+int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme);
+
+/* Waveforms: 0 Gaussian (f0, fc; src/waveform.rs Waveform::Gaussian). */
+double ems_waveform_value(int kind, double f0, double fc, double t, double dt);
+double ems_waveform_duration(int kind, double f0, double fc);
+
+/* A lumped port (LumpedPort::new(region, r).excite_waveform(w, amplitude))
+ * along `axis` over the node box lo..hi (inclusive); the source table is
+ * sampled for n_steps steps. Returns the op index. */
+int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r,
+                              int wave, double f0, double fc, double amplitude, uint64_t n_steps);
+
+/* An edge source of `kind` (ems_source_kind) on n edges with the waveform
+ * sampled for n_steps steps. nodes: 3*n indices. Returns the op index. */
+int ems_model_add_source(ems_model* m, int kind, size_t n, const int* axis, const uint64_t* nodes,
+                         const double* weight, int wave, double f0, double fc, uint64_t n_steps);
+
+/* An edge source whose amplitude the caller has sampled: amp[n] is the
+ * amplitude at the kind's sample time of step n (f64, rounded to f32 as
+ * the reference does). Returns the op index. */
+int ems_model_add_source_table(ems_model* m, int kind, size_t n, const int* axis, const uint64_t* nodes,
+                               const double* weight, const double* amp, uint64_t n_steps);
+
+/* A probe (Probe) on n entries; returns the op index. */
+int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, const uint64_t* nodes,
+                        const double* weight, uint64_t interval);
+
+/* The engine descriptor (valid until the model changes or is freed). */
+const ems_engine_desc* ems_model_desc(ems_model* m);
+
+/* DFT X(f) = sum x(t0 + n dt) e^{-j 2 pi f t_n} dt (src/post/dft.rs:218). */
+void ems_dft(double t0, double dt, const double* x, size_t n, const double* freqs, size_t nf, double* re,
+             double* im);
+
+/* The end-criterion run loop (src/engine/run.rs:424-540) over a stepper
+ * given as callbacks. */
+typedef struct {
+    void* ctx;
+    int (*run)(void* ctx, uint64_t n);
+    int (*step_with_energy)(void* ctx, double* energy);
+} ems_stepper;
+
+typedef struct {
+    uint64_t max_timesteps;
+    int has_end_criteria;
+    double energy_ratio;      /* stop when W/W_max < ratio (10^(dB/10)) */
+    uint64_t check_interval;  /* K, default 50 */
+    int has_excitation_end;
+    double excitation_end;    /* checks count only for t > end */
+    double dt;
+} ems_run_limits;
+
+typedef struct {
+    int reason;               /* 0 energy decay, 1 max timesteps, 2 diverged, 3 stepper error */
+    uint64_t steps;
+    double energy;
+    double max_energy;
+    double ratio_db;
+    uint64_t checks;
+} ems_run_outcome;
+
+int ems_drive(const ems_stepper* s, const ems_run_limits* limits, ems_run_outcome* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

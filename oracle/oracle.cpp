@@ -1,0 +1,767 @@
+// oracle.cpp — CPU restatement of the ems engine step (test infrastructure).
+//
+// TEST INFRASTRUCTURE ONLY: the checker of the CUDA engine and the timed
+// CPU baseline. Each function below cites the reference source it restates;
+// the arithmetic follows it expression by expression (f32 fields, f64 branch
+// state, no fused multiply-add: build with -ffp-contract=off), so results are
+// bit-identical to the reference's for the same coefficients, and for any
+// thread count (each value has one writer and one expression).
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// src/engine/kernel.rs:30-33 — subnormal results rounded to zero.
+inline float flush(float x) { return std::fabs(x) < 1.17549435e-38f ? 0.0f : x; }
+
+// src/engine/kernel.rs:116-120 — (1 + a)·p/b, 0 where b = 0.
+inline double weight(float a, double p, float b) {
+    double w = (1.0 + (double)a) * p / (double)b;
+    return b != 0.0f ? w : 0.0;
+}
+
+// Persistent worker pool: the caller runs slab 0, workers slabs 1..n-1
+// (src/engine/pool.rs:1-16, one x-slab per thread, a barrier per phase).
+class Pool {
+public:
+    explicit Pool(int n) : n_(n) {
+        for (int t = 1; t < n; ++t) workers_.emplace_back([this, t] { loop(t); });
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& w : workers_) w.join();
+    }
+    int size() const { return n_; }
+    void run(const std::function<void(int)>& f) {
+        if (n_ == 1) { f(0); return; }
+        {
+            std::lock_guard<std::mutex> g(m_);
+            job_ = &f;
+            done_.store(0);
+            ++gen_;
+        }
+        cv_.notify_all();
+        f(0);
+        while (done_.load(std::memory_order_acquire) != n_ - 1) std::this_thread::yield();
+    }
+
+private:
+    void loop(int t) {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)>* job;
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (stop_) return;
+                job = job_;
+            }
+            (*job)(t);
+            done_.fetch_add(1, std::memory_order_release);
+        }
+    }
+    int n_;
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    const std::function<void(int)>* job_ = nullptr;
+    std::atomic<int> done_{0};
+};
+
+struct CpmlSlab {
+    ems_cpml_slab s;
+    std::vector<float> b, a, k, psi;
+};
+
+struct PoleSide {
+    std::vector<uint8_t> axis;
+    std::vector<uint64_t> node;
+    std::vector<uint32_t> plane;
+    std::vector<double> sum_inv_z;
+    std::vector<uint32_t> pole_end;
+    std::vector<uint8_t> kind;
+    std::vector<double> a, inv_c, inv_z, half_l;
+    std::vector<float> prev;
+    std::vector<double> j, q;
+};
+
+struct Lumped {
+    int axis = 0;
+    std::vector<uint64_t> node;
+    std::vector<double> cb, g_src, src_w, src_amp, two_l_dt, inv_c, z, rec_g, rec_c;
+    uint64_t series = 1;
+    bool src_in_branch = false, has_src = false, has_branch = false, record = false;
+    uint64_t port_columns = 0;
+    std::vector<double> v, bj, bq, bu_prev, j_avg, ru_prev;
+    std::vector<double> rec, port_v, port_i;
+};
+
+struct Source {
+    int kind = 0;
+    std::vector<uint8_t> axis;
+    std::vector<uint64_t> node;
+    std::vector<float> weight, amp;
+};
+
+struct Probe {
+    int quantity = 0;
+    std::vector<uint8_t> axis;
+    std::vector<uint64_t> node;
+    std::vector<double> weight;
+    uint64_t interval = 1;
+    bool f32_sum = false;
+    std::vector<double> values;
+};
+
+struct Op {
+    int kind = 0;
+    std::vector<CpmlSlab> cpml;
+    PoleSide pe, ph;
+    Lumped lumped;
+    Source source;
+    Probe probe;
+};
+
+}  // namespace
+
+struct oracle_engine {
+    size_t nx, ny, nz, plane, n;
+    double dt;
+    std::vector<float> co[12];
+    std::vector<float> u[3], i[3];
+    std::vector<float> zero;
+    std::vector<Op> ops;
+    uint64_t step = 0;
+    std::vector<size_t> slab_start;
+    std::vector<double> plane_w;
+    Pool* pool = nullptr;
+
+    // ---- H update of one x-plane (src/engine/kernel.rs:447-511 h_plane,
+    // 58-79 h_row, 132-174 h_row_energy). Returns the plane's H energy
+    // share in units of dt/4 when ENERGY.
+    template <bool ENERGY>
+    double h_plane(size_t gi) {
+        const size_t base = gi * plane;
+        float* ix = &i[0][base];
+        float* iy = &i[1][base];
+        float* iz = &i[2][base];
+        const float* ux = &u[0][base];
+        const float* uy = &u[1][base];
+        const float* uz = &u[2][base];
+        const bool next = gi + 1 < nx;
+        const float* uyn = next ? &u[1][base + plane] : nullptr;
+        const float* uzn = next ? &u[2][base + plane] : nullptr;
+        double wh = 0.0;
+        // One row: h = flush(da·h − db·((a − b) − (c − d))), energy entry k
+        // into accumulator k & 3 (groups of four, then the tail).
+        auto row = [&](float* h, const float* da, const float* db, const float* a, const float* b,
+                       const float* c, const float* d, size_t m) -> double {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (size_t k = 0; k < m; ++k) {
+                float old = h[k];
+                float nw = flush(da[k] * old - db[k] * ((a[k] - b[k]) - (c[k] - d[k])));
+                if (ENERGY) acc[k & 3] += weight(da[k], (double)old * (double)nw, db[k]);
+                h[k] = nw;
+            }
+            return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        };
+        const size_t m = nz - 1;
+        for (size_t j = 0; j + 1 < ny; ++j) {
+            size_t r = j * nz;
+            double w = row(ix + r, &co[6][base + r], &co[9][base + r], uz + r + nz, uz + r, uy + r + 1,
+                           uy + r, m);
+            if (ENERGY) wh += 1.0 * w;
+        }
+        if (next) {
+            for (size_t j = 0; j < ny; ++j) {
+                size_t r = j * nz;
+                double w = row(iy + r, &co[7][base + r], &co[10][base + r], ux + r + 1, ux + r, uzn + r,
+                               uz + r, m);
+                if (ENERGY) wh += 1.0 * w;
+            }
+            for (size_t j = 0; j + 1 < ny; ++j) {
+                size_t r = j * nz;
+                double w = row(iz + r, &co[8][base + r], &co[11][base + r], uyn + r, uy + r, ux + r + nz,
+                               ux + r, nz);
+                if (ENERGY) wh += w * 1.0;
+            }
+        }
+        return wh;
+    }
+
+    // E part of a plane's energy (src/engine/kernel.rs:211-244
+    // e_energy_row, 393-408 in h_slab): entry with in-plane index r + k into
+    // accumulator (r + k) & 3, per component.
+    double e_energy_plane(size_t gi) {
+        const size_t base = gi * plane;
+        double we = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            const float* uc = &u[a][base];
+            const float* ca = &co[a][base];
+            const float* cb = &co[3 + a][base];
+            for (size_t p = 0; p < plane; ++p) {
+                double x = (double)uc[p];
+                acc[p & 3] += weight(ca[p], x * x, cb[p]);
+            }
+            we += (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        }
+        return we;
+    }
+
+    // ---- E update of one x-plane (src/engine/kernel.rs:624-697 e_rows,
+    // 252-273 e_row): u = flush(ca·u + cb·((a − b) − (c − d))).
+    void e_plane(size_t gi) {
+        const size_t base = gi * plane;
+        float* ux = &u[0][base];
+        float* uy = &u[1][base];
+        float* uz = &u[2][base];
+        const float* ix = &i[0][base];
+        const float* iy = &i[1][base];
+        const float* iz = &i[2][base];
+        const float* iyp = gi == 0 ? zero.data() : &i[1][base - plane];
+        const float* izp = gi == 0 ? zero.data() : &i[2][base - plane];
+        auto e1 = [](float ca, float u0, float cb, float a, float b, float c, float d) {
+            return flush(ca * u0 + cb * ((a - b) - (c - d)));
+        };
+        for (size_t j = 0; j < ny; ++j) {
+            const size_t r = j * nz;
+            if (gi + 1 < nx) {
+                const float* ca = &co[0][base + r];
+                const float* cb = &co[3][base + r];
+                const float* izm = j == 0 ? zero.data() : iz + r - nz;
+                ux[r] = e1(ca[0], ux[r], cb[0], iz[r], izm[0], iy[r], 0.0f);
+                for (size_t k = 1; k < nz; ++k)
+                    ux[r + k] = e1(ca[k], ux[r + k], cb[k], iz[r + k], izm[k], iy[r + k], iy[r + k - 1]);
+            }
+            if (j + 1 < ny) {
+                const float* ca = &co[1][base + r];
+                const float* cb = &co[4][base + r];
+                uy[r] = e1(ca[0], uy[r], cb[0], ix[r], 0.0f, iz[r], izp[r]);
+                for (size_t k = 1; k < nz; ++k)
+                    uy[r + k] = e1(ca[k], uy[r + k], cb[k], ix[r + k], ix[r + k - 1], iz[r + k], izp[r + k]);
+            }
+            {
+                const float* ca = &co[2][base + r];
+                const float* cb = &co[5][base + r];
+                const float* ixm = j == 0 ? zero.data() : ix + r - nz;
+                for (size_t k = 0; k + 1 < nz; ++k)
+                    uz[r + k] = e1(ca[k], uz[r + k], cb[k], iy[r + k], iyp[r + k], ix[r + k], ixm[k]);
+            }
+        }
+    }
+
+    // ---- CPML slab correction on the x-planes [x0, x1)
+    // (src/engine/boundary/cpml.rs:445-520 Slab::apply, 657-676 row_uniform).
+    void cpml_apply(CpmlSlab& c, size_t x0, size_t x1) {
+        const ems_cpml_slab& s = c.s;
+        const size_t lo0 = std::max<size_t>(s.lo[0], x0), hi0 = std::min<size_t>(s.hi[0], x1);
+        if (lo0 >= hi0) return;
+        const bool e = s.e_side != 0;
+        float* t = e ? u[s.comp].data() : i[s.comp].data();
+        const float* src = e ? i[s.other].data() : u[s.other].data();
+        const float* coef = e ? co[3 + s.comp].data() : co[9 + s.comp].data();
+        const float scale = e ? 1.0f : -1.0f;
+        const size_t n1 = s.hi[1] - s.lo[1], n2 = s.hi[2] - s.lo[2];
+        const size_t step_n = s.normal == 0 ? plane : (s.normal == 1 ? nz : 1);
+        for (size_t x = lo0; x < hi0; ++x)
+            for (size_t y = s.lo[1]; y < s.hi[1]; ++y)
+                for (size_t z = s.lo[2]; z < s.hi[2]; ++z) {
+                    const size_t idx = (x * ny + y) * nz + z;
+                    const size_t node[3] = {x, y, z};
+                    const size_t d = node[s.normal] - s.lo[s.normal];
+                    float h, l;
+                    if (e) {
+                        h = src[idx];
+                        l = node[s.normal] == 0 ? 0.0f : src[idx - step_n];
+                    } else {
+                        h = src[idx + step_n];
+                        l = src[idx];
+                    }
+                    const size_t q = ((x - s.lo[0]) * n1 + (y - s.lo[1])) * n2 + (z - s.lo[2]);
+                    const float sv = s.sign * (h - l);
+                    c.psi[q] = flush(c.b[d] * c.psi[q] + c.a[d] * sv);
+                    t[idx] = flush(t[idx] + scale * coef[idx] * (c.k[d] * sv + c.psi[q]));
+                }
+    }
+
+    // ---- dispersive correction of the edges in planes [x0, x1)
+    // (src/engine/dispersive.rs:1392-1470 step_edge, 1183-1343 correct).
+    // Edges of the x-planes [x0, x1) (edges are in plane order).
+    static std::pair<size_t, size_t> edges_in(const PoleSide& p, size_t x0, size_t x1) {
+        auto lo = std::lower_bound(p.plane.begin(), p.plane.end(), (uint32_t)x0);
+        auto hi = std::lower_bound(p.plane.begin(), p.plane.end(), (uint32_t)x1);
+        return {size_t(lo - p.plane.begin()), size_t(hi - p.plane.begin())};
+    }
+
+    void poles_correct(PoleSide& p, bool electric, size_t x0, size_t x1) {
+        const auto [e0, e1] = edges_in(p, x0, x1);
+        for (size_t e = e0; e < e1; ++e) {
+            const int ax = p.axis[e];
+            float* f = electric ? u[ax].data() : i[ax].data();
+            const size_t idx = p.node[e];
+            const double cb = (double)(electric ? co[3 + ax][idx] : co[9 + ax][idx]);
+            const size_t p0 = e ? p.pole_end[e - 1] : 0, p1 = p.pole_end[e];
+            const double prev = (double)p.prev[e];
+            const double half_prev = 0.5 * prev;
+            const double u_star = (double)f[idx];
+            double s = 0.0;
+            double nj[64], nq[64];
+            for (size_t q = p0; q < p1; ++q) {
+                if (p.kind[q] == EMS_POLE_LEAPFROG) {
+                    double jn = p.a[q] * p.j[q] + p.inv_z[q] * (prev - p.q[q] * p.inv_c[q]);
+                    nj[q - p0] = jn;
+                    nq[q - p0] = p.q[q] + dt * jn;
+                    s += jn;
+                } else {
+                    s += (p.a[q] * p.j[q] - p.q[q] * p.inv_c[q] + half_prev) * p.inv_z[q];
+                }
+            }
+            const float u_new = (float)((u_star - cb * s) / (1.0 + 0.5 * cb * p.sum_inv_z[e]));
+            const double half_new = 0.5 * (double)u_new;
+            for (size_t q = p0; q < p1; ++q) {
+                if (p.kind[q] == EMS_POLE_LEAPFROG) {
+                    p.j[q] = nj[q - p0];
+                    p.q[q] = nq[q - p0];
+                } else {
+                    double k = p.a[q] * p.j[q] - p.q[q] * p.inv_c[q] + half_prev;
+                    double jb = (k + half_new) * p.inv_z[q];
+                    p.j[q] = 2.0 * jb - p.j[q];
+                    p.q[q] = p.q[q] + dt * jb;
+                }
+            }
+            f[idx] = u_new;
+        }
+    }
+
+    // Saves the current field value of the edges (src/engine/dispersive.rs:1173-1180).
+    void poles_capture(PoleSide& p, bool electric, size_t x0, size_t x1) {
+        const auto [e0, e1] = edges_in(p, x0, x1);
+        for (size_t e = e0; e < e1; ++e) {
+            p.prev[e] = (electric ? u : i)[p.axis[e]][p.node[e]];
+        }
+    }
+
+    // Σ ½·L·j² + ½·q²/C_p in pole order (src/engine/dispersive.rs:1488-1506).
+    static void pole_energy(const PoleSide& p, double& w) {
+        for (size_t q = 0; q < p.kind.size(); ++q)
+            w += p.half_l[q] * p.j[q] * p.j[q] + 0.5 * p.inv_c[q] * p.q[q] * p.q[q];
+    }
+
+    double operator_energy() const {
+        double w = 0.0;
+        for (const Op& op : ops) {
+            double x = 0.0;
+            if (op.kind == EMS_OP_POLES) {
+                double we = 0.0, wm = 0.0;
+                pole_energy(op.pe, we);
+                pole_energy(op.ph, wm);
+                x = we + wm;
+            } else if (op.kind == EMS_OP_LUMPED && op.lumped.has_branch) {
+                // src/engine/lumped.rs:1066-1077 branch_energy
+                const Lumped& l = op.lumped;
+                for (size_t e = 0; e < l.node.size(); ++e) {
+                    double half_l = 0.25 * l.two_l_dt[e] * dt;
+                    x += half_l * l.bj[e] * l.bj[e] + 0.5 * l.inv_c[e] * l.bq[e] * l.bq[e];
+                }
+            }
+            w += x;
+        }
+        return w;
+    }
+
+    // ---- serial hooks
+    void source_apply(Source& s, bool magnetic_phase) {
+        const bool mag = s.kind == EMS_SOFT_H || s.kind == EMS_HARD_H;
+        if (mag != magnetic_phase) return;
+        const float a = step < s.amp.size() ? s.amp[step] : 0.0f;
+        const bool hard = s.kind == EMS_HARD_E || s.kind == EMS_HARD_H;
+        // src/engine/excite.rs:104-117 apply, 136-150 hooks_at (soft: skipped at 0).
+        if (!hard && a == 0.0f) return;
+        auto& F = mag ? i : u;
+        for (size_t e = 0; e < s.axis.size(); ++e) {
+            float& x = F[s.axis[e]][s.node[e]];
+            if (hard) x = s.weight[e] * a;
+            else x += s.weight[e] * a;
+        }
+    }
+
+    void probe_sample(Probe& p, bool current_phase) {
+        if ((p.quantity == EMS_PROBE_CURRENT) != current_phase) return;
+        if (step % p.interval != 0) return;
+        auto& F = current_phase ? i : u;
+        // src/engine/probe.rs:381-392 (f64 sum in entry order; f32 variant).
+        if (p.f32_sum) {
+            float s = 0.0f;
+            for (size_t e = 0; e < p.axis.size(); ++e) s = s + (float)p.weight[e] * F[p.axis[e]][p.node[e]];
+            p.values.push_back((double)s);
+        } else {
+            double s = 0.0;
+            for (size_t e = 0; e < p.axis.size(); ++e) s += p.weight[e] * (double)F[p.axis[e]][p.node[e]];
+            p.values.push_back(s);
+        }
+    }
+
+    void lumped_pre_e(Lumped& l) {
+        // src/engine/lumped.rs:1106-1121 pre_e_impl.
+        for (size_t e = 0; e < l.node.size(); ++e) {
+            double x = (double)u[l.axis][l.node[e]];
+            if (l.has_branch) l.bu_prev[e] = x;
+            if (l.record) l.ru_prev[e] = x;
+        }
+    }
+
+    void lumped_post_e(Lumped& l) {
+        // src/engine/lumped.rs:1123-1236 post_e_impl (non-openEMS order),
+        // src/engine/port.rs:276-290 LumpedPort::post_e.
+        float* U = u[l.axis].data();
+        const size_t ne = l.node.size();
+        bool active = false;
+        if (l.has_src) {
+            std::fill(l.v.begin(), l.v.end(), 0.0);
+            const double val = step < l.src_amp.size() ? l.src_amp[step] : 0.0;
+            if (val != 0.0) {
+                active = true;
+                for (size_t e = 0; e < ne; ++e) l.v[e] += l.src_w[e] * val;
+            }
+        }
+        if (active && !l.src_in_branch) {
+            for (size_t e = 0; e < ne; ++e) {
+                double add = l.cb[e] * l.g_src[e] * l.v[e];
+                if (add != 0.0) U[l.node[e]] = (float)((double)U[l.node[e]] + add);
+            }
+        }
+        if (l.has_branch) {
+            for (size_t e = 0; e < ne; ++e) {
+                double v_br = (active && l.src_in_branch) ? l.v[e] : 0.0;
+                double u_star = (double)U[l.node[e]];
+                double k = l.two_l_dt[e] * l.bj[e] - l.bq[e] * l.inv_c[e] - v_br + 0.5 * l.bu_prev[e];
+                double z = l.z[e];
+                double cb = l.cb[e];
+                double u_new = (z * u_star - cb * k) / (z + 0.5 * cb);
+                double jb = (k + 0.5 * u_new) / z;
+                l.bj[e] = 2.0 * jb - l.bj[e];
+                l.bq[e] += dt * jb;
+                l.j_avg[e] = jb;
+                U[l.node[e]] = (float)u_new;
+            }
+        }
+        if (l.record) {
+            double sum = 0.0;
+            for (size_t e = 0; e < ne; ++e) {
+                double u0 = l.ru_prev[e], u1 = (double)U[l.node[e]];
+                double v = (active && !l.src_in_branch) ? l.v[e] : 0.0;
+                sum += l.rec_g[e] * (0.5 * (u0 + u1) - v) + l.rec_c[e] * (u1 - u0) / dt;
+                if (l.has_branch) sum += l.j_avg[e];
+            }
+            l.rec.push_back(sum / (double)l.series);
+        }
+        if (l.port_columns > 0) {
+            double i_last = l.rec.empty() ? 0.0 : l.rec.back();
+            l.port_i.push_back(-i_last);
+            double s = 0.0;
+            for (size_t e = 0; e < ne; ++e) s += (double)U[l.node[e]];
+            l.port_v.push_back(s / (double)l.port_columns);
+        }
+    }
+
+    // One step (src/engine/pool.rs Shared::h / Shared::e with the serial
+    // gaps of src/engine/mod.rs:833-992).
+    void one_step(bool energy) {
+        const int ns = pool->size();
+        // H half-step with its slab hooks.
+        pool->run([&](int sl) {
+            const size_t p0 = slab_start[sl], p1 = slab_start[sl + 1];
+            for (size_t gi = p0; gi < p1; ++gi) {
+                if (energy) {
+                    double wh = h_plane<true>(gi);
+                    double we = e_energy_plane(gi);
+                    plane_w[gi] = we + wh;
+                } else {
+                    h_plane<false>(gi);
+                }
+            }
+            for (Op& op : ops) {
+                if (op.kind == EMS_OP_CPML) {
+                    for (CpmlSlab& c : op.cpml)
+                        if (!c.s.e_side) cpml_apply(c, p0, p1);
+                } else if (op.kind == EMS_OP_POLES) {
+                    poles_correct(op.ph, false, p0, p1);
+                    poles_capture(op.pe, true, p0, p1);
+                }
+            }
+        });
+        (void)ns;
+        for (Op& op : ops) {
+            if (op.kind == EMS_OP_SOURCE) source_apply(op.source, true);
+            else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, true);
+        }
+        for (Op& op : ops)
+            if (op.kind == EMS_OP_LUMPED) lumped_pre_e(op.lumped);
+        // E half-step with its slab hooks.
+        pool->run([&](int sl) {
+            const size_t p0 = slab_start[sl], p1 = slab_start[sl + 1];
+            for (size_t gi = p0; gi < p1; ++gi) e_plane(gi);
+            for (Op& op : ops) {
+                if (op.kind == EMS_OP_CPML) {
+                    for (CpmlSlab& c : op.cpml)
+                        if (c.s.e_side) cpml_apply(c, p0, p1);
+                } else if (op.kind == EMS_OP_POLES) {
+                    poles_correct(op.pe, true, p0, p1);
+                    poles_capture(op.ph, false, p0, p1);
+                }
+            }
+        });
+        for (Op& op : ops) {
+            if (op.kind == EMS_OP_LUMPED) lumped_post_e(op.lumped);
+            else if (op.kind == EMS_OP_SOURCE) source_apply(op.source, false);
+            else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, false);
+        }
+        ++step;
+    }
+};
+
+namespace {
+
+int default_threads(size_t nx, size_t cells) {
+    unsigned hw = std::thread::hardware_concurrency();
+    size_t t = hw ? hw : 1;
+    t = std::min<size_t>(t, cells / 4096);
+    t = std::min<size_t>(t, nx / 5);
+    return (int)std::max<size_t>(t, 1);
+}
+
+template <class T>
+std::vector<T> vec(const T* p, size_t n) {
+    return p ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+void load_side(PoleSide& s, const ems_pole_side& t, size_t ny, size_t nz) {
+    s.axis = vec(t.axis, t.n_edges);
+    s.node = vec(t.node, t.n_edges);
+    s.sum_inv_z = vec(t.sum_inv_z, t.n_edges);
+    s.pole_end = vec(t.pole_end, t.n_edges);
+    s.kind = vec(t.kind, t.n_poles);
+    s.a = vec(t.a, t.n_poles);
+    s.inv_c = vec(t.inv_c, t.n_poles);
+    s.inv_z = vec(t.inv_z, t.n_poles);
+    s.half_l = vec(t.half_l, t.n_poles);
+    s.prev.assign(t.n_edges, 0.0f);
+    s.j.assign(t.n_poles, 0.0);
+    s.q.assign(t.n_poles, 0.0);
+    s.plane.resize(t.n_edges);
+    for (size_t e = 0; e < t.n_edges; ++e) s.plane[e] = (uint32_t)(s.node[e] / (ny * nz));
+}
+
+// An edge's poles are at most this many (the per-edge scratch of poles_correct).
+constexpr size_t MAX_POLES = 64;
+
+bool side_ok(const ems_pole_side& t, size_t n) {
+    if (t.n_edges && (!t.axis || !t.node || !t.sum_inv_z || !t.pole_end)) return false;
+    if (t.n_poles && (!t.kind || !t.a || !t.inv_c || !t.inv_z || !t.half_l)) return false;
+    uint32_t prev = 0;
+    for (size_t e = 0; e < t.n_edges; ++e) {
+        if (t.node[e] >= n || t.axis[e] > 2 || t.pole_end[e] < prev || t.pole_end[e] - prev > MAX_POLES)
+            return false;
+        prev = t.pole_end[e];
+    }
+    return prev == t.n_poles;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_create(const ems_engine_desc* d, int threads, oracle_engine** out) {
+    if (!d || !out) return EMS_ERR_INVALID;
+    if (d->nodes[0] < 2 || d->nodes[1] < 2 || d->nodes[2] < 2 || !(d->dt > 0)) return EMS_ERR_INVALID;
+    auto* e = new oracle_engine();
+    e->nx = d->nodes[0];
+    e->ny = d->nodes[1];
+    e->nz = d->nodes[2];
+    e->plane = e->ny * e->nz;
+    e->n = e->nx * e->plane;
+    e->dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (!d->coeff[l]) { delete e; return EMS_ERR_INVALID; }
+        e->co[l].assign(d->coeff[l], d->coeff[l] + e->n);
+    }
+    for (int a = 0; a < 3; ++a) {
+        e->u[a].assign(e->n, 0.0f);
+        e->i[a].assign(e->n, 0.0f);
+    }
+    e->zero.assign(e->plane, 0.0f);
+    e->plane_w.assign(e->nx, 0.0);
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        Op op;
+        op.kind = d->ops[k].kind;
+        const void* t = d->ops[k].table;
+        switch (op.kind) {
+        case EMS_OP_CPML: {
+            const auto* c = (const ems_cpml*)t;
+            for (size_t s = 0; s < c->n_slabs; ++s) {
+                CpmlSlab cs;
+                cs.s = c->slabs[s];
+                size_t depth = cs.s.hi[cs.s.normal] - cs.s.lo[cs.s.normal];
+                cs.b = vec(cs.s.b, depth);
+                cs.a = vec(cs.s.a, depth);
+                cs.k = vec(cs.s.k, depth);
+                size_t len = (cs.s.hi[0] - cs.s.lo[0]) * (cs.s.hi[1] - cs.s.lo[1]) * (cs.s.hi[2] - cs.s.lo[2]);
+                cs.psi.assign(len, 0.0f);
+                op.cpml.push_back(std::move(cs));
+            }
+            break;
+        }
+        case EMS_OP_POLES: {
+            const auto* p = (const ems_poles*)t;
+            if (!side_ok(p->electric, e->n) || !side_ok(p->magnetic, e->n)) { delete e; return EMS_ERR_INVALID; }
+            load_side(op.pe, p->electric, e->ny, e->nz);
+            load_side(op.ph, p->magnetic, e->ny, e->nz);
+            break;
+        }
+        case EMS_OP_LUMPED: {
+            const auto* l = (const ems_lumped*)t;
+            Lumped& L = op.lumped;
+            size_t ne = l->n_edges;
+            L.axis = l->axis;
+            L.node = vec(l->node, ne);
+            L.cb = vec(l->cb, ne);
+            L.g_src = vec(l->g_src, ne);
+            L.series = l->series ? l->series : 1;
+            L.src_in_branch = l->src_in_branch != 0;
+            L.has_src = l->src_w != nullptr;
+            L.src_w = vec(l->src_w, ne);
+            L.src_amp = vec(l->src_amp, l->n_src_amp);
+            L.has_branch = l->has_branch != 0;
+            if (L.has_branch) {
+                L.two_l_dt = vec(l->two_l_dt, ne);
+                L.inv_c = vec(l->inv_c, ne);
+                L.z = vec(l->z, ne);
+            }
+            L.record = l->record != 0;
+            if (L.record) {
+                L.rec_g = vec(l->rec_g, ne);
+                L.rec_c = vec(l->rec_c, ne);
+            }
+            L.port_columns = l->port_columns;
+            L.v.assign(ne, 0.0);
+            L.bj.assign(ne, 0.0);
+            L.bq.assign(ne, 0.0);
+            L.bu_prev.assign(ne, 0.0);
+            L.j_avg.assign(ne, 0.0);
+            L.ru_prev.assign(ne, 0.0);
+            break;
+        }
+        case EMS_OP_SOURCE: {
+            const auto* s = (const ems_source*)t;
+            op.source.kind = s->kind;
+            op.source.axis = vec(s->axis, s->n_edges);
+            op.source.node = vec(s->node, s->n_edges);
+            op.source.weight = vec(s->weight, s->n_edges);
+            op.source.amp = vec(s->amp, s->n_amp);
+            break;
+        }
+        case EMS_OP_PROBE: {
+            const auto* p = (const ems_probe*)t;
+            op.probe.quantity = p->quantity;
+            op.probe.axis = vec(p->axis, p->n_entries);
+            op.probe.node = vec(p->node, p->n_entries);
+            op.probe.weight = vec(p->weight, p->n_entries);
+            op.probe.interval = p->interval ? p->interval : 1;
+            op.probe.f32_sum = p->f32_sum != 0;
+            break;
+        }
+        default:
+            delete e;
+            return EMS_ERR_INVALID;
+        }
+        e->ops.push_back(std::move(op));
+    }
+    size_t cells = (e->nx - 1) * (e->ny - 1) * (e->nz - 1);
+    int nt = threads > 0 ? threads : default_threads(e->nx, cells);
+    nt = (int)std::min<size_t>((size_t)nt, e->nx);
+    // src/engine/fields.rs:38-58 Layout::new — contiguous x-slabs.
+    size_t q = e->nx / nt, r = e->nx % nt, p = 0;
+    for (int s = 0; s < nt; ++s) {
+        e->slab_start.push_back(p);
+        p += q + ((size_t)s < r ? 1 : 0);
+    }
+    e->slab_start.push_back(e->nx);
+    e->pool = new Pool(nt);
+    *out = e;
+    return EMS_OK;
+}
+
+int oracle_destroy(oracle_engine* e) {
+    if (!e) return EMS_ERR_INVALID;
+    delete e->pool;
+    delete e;
+    return EMS_OK;
+}
+
+int oracle_threads(const oracle_engine* e) { return e ? e->pool->size() : 0; }
+
+int oracle_run(oracle_engine* e, uint64_t n) {
+    if (!e) return EMS_ERR_INVALID;
+    for (uint64_t s = 0; s < n; ++s) e->one_step(false);
+    return EMS_OK;
+}
+
+int oracle_step_with_energy(oracle_engine* e, double* energy) {
+    if (!e || !energy) return EMS_ERR_INVALID;
+    // src/engine/mod.rs:819-823 and pool.rs:675-692 (planes summed in order, ×dt/4).
+    double w_ops = e->operator_energy();
+    e->one_step(true);
+    double s = 0.0;
+    for (size_t gi = 0; gi < e->nx; ++gi) s += e->plane_w[gi];
+    *energy = 0.25 * e->dt * s + w_ops;
+    return EMS_OK;
+}
+
+int oracle_download_field(oracle_engine* e, int field, int axis, float* host) {
+    if (!e || !host || axis < 0 || axis > 2 || field < 0 || field > 1) return EMS_ERR_INVALID;
+    const auto& v = field == 0 ? e->u[axis] : e->i[axis];
+    std::memcpy(host, v.data(), v.size() * sizeof(float));
+    return EMS_OK;
+}
+
+int oracle_upload_field(oracle_engine* e, int field, int axis, const float* host) {
+    if (!e || !host || axis < 0 || axis > 2 || field < 0 || field > 1) return EMS_ERR_INVALID;
+    auto& v = field == 0 ? e->u[axis] : e->i[axis];
+    std::memcpy(v.data(), host, v.size() * sizeof(float));
+    return EMS_OK;
+}
+
+int oracle_samples(oracle_engine* e, size_t op, int which, double* out, size_t cap, size_t* n) {
+    if (!e || !n || op >= e->ops.size()) return EMS_ERR_INVALID;
+    const Op& o = e->ops[op];
+    const std::vector<double>* v = nullptr;
+    if (o.kind == EMS_OP_PROBE && which == 0) v = &o.probe.values;
+    else if (o.kind == EMS_OP_LUMPED && which == 0) v = &o.lumped.rec;
+    else if (o.kind == EMS_OP_LUMPED && which == 1) v = &o.lumped.port_v;
+    else if (o.kind == EMS_OP_LUMPED && which == 2) v = &o.lumped.port_i;
+    else return EMS_ERR_INVALID;
+    *n = v->size();
+    if (out) std::memcpy(out, v->data(), std::min(cap, v->size()) * sizeof(double));
+    return EMS_OK;
+}
+
+}  // extern "C"

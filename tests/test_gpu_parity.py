@@ -1,0 +1,141 @@
+"""Parity of the CUDA engine with the oracle (the reference's step restated).
+
+Every test builds one model, runs the CUDA engine (through the C ABI of
+include/ems_gpu.h) and the oracle on the same tables, and requires:
+
+* the six field arrays equal bit for bit (f32 bit patterns);
+* probe, port voltage/current and lumped-current series equal bit for bit
+  (both sum their entries in entry order);
+* energies within 1e-12 relative (a reduction: the GPU sums in another order).
+
+The reference engine itself is bit-identical across thread counts
+(src/engine/mod.rs:64-79), so bit-exact agreement is the bar.
+"""
+import numpy as np
+import pytest
+
+import ems_b200 as E
+from ems_b200 import workloads as W
+from oracle import OracleEngine
+from helpers import assert_fields_equal, mixed_model, small_cavity
+
+pytestmark = pytest.mark.gpu
+
+ENERGY_RTOL = 1e-12
+
+
+def _lockstep(model, steps, energy_every=0, threads=4):
+    g = E.Engine(model)
+    o = OracleEngine(model, threads=threads)
+    eg, eo = [], []
+    s = 0
+    while s < steps:
+        if energy_every and s % energy_every == 0:
+            eg.append(g.step_with_energy())
+            eo.append(o.step_with_energy())
+            s += 1
+        else:
+            n = min(steps - s, (energy_every - s % energy_every) if energy_every else steps)
+            g.run(n)
+            o.run(n)
+            s += n
+    return g, o, np.array(eg), np.array(eo)
+
+
+def _series_equal(g, o, op, which=0):
+    a, b = g.samples(op, which), o.samples(op, which)
+    assert a.shape == b.shape and a.size > 0
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), (op, which, np.max(np.abs(a - b)))
+
+
+def test_vacuum_pec_cavity_bit_exact():
+    m, _ = small_cavity()
+    g, o, eg, eo = _lockstep(m, 300, energy_every=25)
+    assert_fields_equal(g, o, "cavity")
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_lossy_cavity_bit_exact():
+    m, _ = small_cavity(kappa=0.002)
+    g, o, eg, eo = _lockstep(m, 200, energy_every=10)
+    assert_fields_equal(g, o, "lossy cavity")
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+@pytest.mark.parametrize("scheme", [E.TRAPEZOIDAL, E.LEAPFROG])
+def test_every_operator_bit_exact(scheme):
+    m, ops = mixed_model(scheme=scheme, steps=240)
+    g, o, eg, eo = _lockstep(m, 240, energy_every=20)
+    assert_fields_equal(g, o, f"mixed scheme {scheme}")
+    for name in ("pv", "pi", "pe"):
+        _series_equal(g, o, ops[name])
+    for which in (0, 1, 2):
+        _series_equal(g, o, ops["port"], which)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_odd_sizes_and_tile_remainders():
+    # nz = 33 + 1 nodes (a row pitch remainder), ny odd, CPML of 1 cell.
+    m = E.Model.uniform([7, 5, 33], [1e-3, 1.2e-3, 0.9e-3])
+    m.build(courant=0.9)
+    m.add_cpml([1, 1, 1, 1, 1, 1])
+    m.add_source(E.SOFT_E, [(E.Y, (3, 2, 16), 1.0)], 20e9, 15e9, 400)
+    p = m.add_probe(E.VOLTAGE, [(E.Y, (3, 2, 20), 1.0)])
+    g, o, eg, eo = _lockstep(m, 150, energy_every=7)
+    assert_fields_equal(g, o, "odd")
+    _series_equal(g, o, p)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_vacuum_box_configuration_bit_exact():
+    """The plain-method configuration in full: 100³ cells, CPML 8, 2000 steps,
+    4 E_z probes; fields and probe series bit-exact."""
+    w = W.vacuum_box()
+    g, o, _, _ = _lockstep(w.model, w.steps, threads=0)
+    for p in w.probes:
+        _series_equal(g, o, p)
+    assert_fields_equal(g, o, "vacuum box")
+
+
+def test_dispersive_box_small_bit_exact():
+    w = W.dispersive_box(n=48, radius=8, slab=4, cpml=5, steps=300)
+    g, o, eg, eo = _lockstep(w.model, 300, energy_every=30)
+    assert_fields_equal(g, o, "dispersive box")
+    for p in w.probes:
+        _series_equal(g, o, p)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_patch_antenna_port_series_bit_exact():
+    w = W.patch_antenna(scale=0.4, steps=600)
+    g, o, _, _ = _lockstep(w.model, 600, threads=0)
+    for which in (0, 1, 2):
+        _series_equal(g, o, w.port, which)
+    assert_fields_equal(g, o, "patch")
+
+
+def test_field_upload_roundtrip_and_initial_state():
+    m, _ = small_cavity()
+    g = E.Engine(m)
+    o = OracleEngine(m, threads=2)
+    rng = np.random.default_rng(3)
+    for f in (0, 1):
+        for a in range(3):
+            v = (rng.standard_normal(m.nodes) * 1e-3).astype(np.float32)
+            g.set_field(f, a, v)
+            o.set_field(f, a, v)
+            assert np.array_equal(g.field(f, a), v)
+    g.run(37)
+    o.run(37)
+    assert_fields_equal(g, o, "from a random state")
+
+
+def test_invalid_tables_rejected():
+    m, _ = small_cavity()
+    lib = E.gpu_lib()
+    import ctypes as C
+    h = C.c_void_p()
+    assert lib.ems_gpu_create(None, 0, C.byref(h)) == 1
+    g = E.Engine(m)
+    with pytest.raises(E.EngineError):
+        g.samples(99)
