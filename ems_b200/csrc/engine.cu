@@ -72,7 +72,7 @@ struct ems_gpu {
         std::vector<double> amp;   // host copy of the source values (activity test)
         bool has_src = false, record = false, has_branch = false;
         uint64_t columns = 0;
-        size_t count = 0, cap = 0;
+        size_t count = 0, cap = 0, vcap = 0, icap = 0;
         double* rec = nullptr;
         double* pv = nullptr;
         double* pi = nullptr;
@@ -296,11 +296,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
                 ems_status st = grow(h, &L.rec, L.count, &L.cap, L.count + 1);
                 if (st) return st;
                 if (L.columns) {
-                    size_t c1 = L.cap, c2 = L.cap;
-                    // Port series share the record's capacity.
-                    st = grow(h, &L.pv, L.count, &c1, L.cap);
+                    st = grow(h, &L.pv, L.count, &L.vcap, L.count + 1);
                     if (st) return st;
-                    st = grow(h, &L.pi, L.count, &c2, L.cap);
+                    st = grow(h, &L.pi, L.count, &L.icap, L.count + 1);
                     if (st) return st;
                 }
             }
