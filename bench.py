@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the FDTD time stepping: Mcell-updates/s on the large
+dispersive box (512³ cells, 0.5 mm, CPML 10, two-pole Lorentz sphere of
+radius 80 cells, 20-cell Drude slab, soft E_x sheet source, leapfrog ADE),
+with the share of the HBM roofline it reaches.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1): every rank steps its own replica
+of the model (the configuration fits one GPU; there is no data exchange
+between models), so ``scaling`` is weak and ``value`` counts the cell
+updates of all ranks over the slowest rank's device time. Rank 0 prints
+one JSON line.
+
+* ``value``: device time of K steps (CUDA events on the engine's stream,
+  barrier + synchronize on both sides, max over ranks). Inputs (3.2 GB of
+  fields plus coefficients) are far larger than the 126 MB L2, so no flush
+  is needed between steps.
+* ``e2e``: the same metric through the C ABI step by step, as a host that
+  feeds a source and reads a probe every step would: per step the source
+  amplitude goes host→device, the step runs, and the probe's new sample
+  comes back device→host.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  mean launch time (CUDA events around each launch inside the timed
+  region), against the measured HBM copy bandwidth; ``traffic`` is the
+  DRAM bytes of one launch from the committed ncu summary.
+* ``cpu_baseline``: the oracle (the reference engine's step restated in
+  C++, one thread per x-slab like the reference's pool) on a bounded sample
+  of the same model on this host's cores.
+* ``--impl reference`` times that CPU restatement alone (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-updates/s"
+ALGO_BYTES_CELL_FIELDS = 48.0  # read u, i and write u, i (f32 × 6 × 2)
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(cells: int, steps: int):
+    from ems_b200 import workloads as W
+
+    if cells == 512:
+        return W.dispersive_box(steps=steps)
+    # Proportionally scaled box (for small trial runs only).
+    s = cells / 512.0
+    return W.dispersive_box(n=cells, radius=80 * s, slab=max(2, int(round(20 * s))), cpml=max(4, int(round(10 * s))),
+                            steps=steps)
+
+
+def algorithmic_bytes(w) -> dict:
+    """Bytes a step must move at least (per step): fields 48 B per cell, the
+    CPML ψ read and written (8 B per ψ per layer node), the pole state j, q
+    (f64) read and written (32 B per pole) and the prev field value of each
+    pole edge; coefficients count 0 (a handful of distinct rows)."""
+    import ems_b200 as E
+
+    m = w.model
+    nx, ny, nz = m.nodes
+    desc = E.EngineDesc.from_address(m.desc)
+    psi = 0
+    poles = 0
+    pole_edges = 0
+    for k in range(desc.n_ops):
+        op = E.OpEntry.from_address(desc.ops + k * C_sizeof_op())
+        if op.kind == E.OP_CPML:
+            t = E.CpmlTable.from_address(op.table)
+            for q in range(t.n_slabs):
+                sl = E.CpmlSlab.from_address(t.slabs + q * E.C.sizeof(E.CpmlSlab))
+                psi += int(np.prod([sl.hi[a] - sl.lo[a] for a in range(3)]))
+        elif op.kind == E.OP_POLES:
+            t = E.PolesTable.from_address(op.table)
+            poles += t.electric.n_poles + t.magnetic.n_poles
+            pole_edges += t.electric.n_edges + t.magnetic.n_edges
+    cells = (nx - 1) * (ny - 1) * (nz - 1)
+    b_fields = ALGO_BYTES_CELL_FIELDS * cells
+    b_psi = 8.0 * psi
+    b_poles = 32.0 * poles + 8.0 * pole_edges
+    return {"cells": cells, "fields": b_fields, "psi": b_psi, "poles": b_poles, "total": b_fields + b_psi + b_poles,
+            "psi_nodes": psi, "poles_n": poles, "pole_edges": pole_edges}
+
+
+def C_sizeof_op():
+    import ems_b200 as E
+
+    return E.C.sizeof(E.OpEntry)
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` scaled to the full configuration,
+    from the committed ncu summary (profiles/traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(kernel, {}).get("bytes_per_launch_full_config")
+    return float(v) if v is not None else None
+
+
+def cpu_baseline(w, seconds: float = 15.0) -> dict:
+    """The oracle on the same model, timed on this host's cores for about
+    `seconds` (whole steps of the full model)."""
+    from oracle import OracleEngine
+
+    o = OracleEngine(w.model, threads=os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    o.run(1)
+    t1 = time.perf_counter()
+    per = max(t1 - t0, 1e-6)
+    n = max(1, min(200, int(seconds / per)))
+    t0 = time.perf_counter()
+    o.run(n)
+    el = time.perf_counter() - t0
+    v = w.cells * n / el / 1e6
+    th = o.threads
+    o.close()
+    return {"value": round(v, 3), "unit": METRIC, "cores": th, "kind": "port",
+            "sample": f"{n} whole steps of the same {w.name} model after 1 untimed step "
+                      f"(oracle: C++ restatement of the reference step, {th} threads)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = workload(args.cells, max(args.steps + args.warmup + 10, 100))
+    from oracle import OracleEngine
+
+    o = OracleEngine(w.model, threads=os.cpu_count() or 1)
+    o.run(args.warmup)
+    t0 = time.perf_counter()
+    o.run(args.steps)
+    el = time.perf_counter() - t0
+    v = w.cells * args.steps / el / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * el / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config(w, args),
+        "cpu_baseline": {"value": round(v, 3), "unit": METRIC, "cores": o.threads, "kind": "port",
+                         "sample": f"{args.steps} whole steps after {args.warmup} warm-up steps, "
+                                   f"{o.threads} threads (C++ restatement of the reference step)"},
+        "e2e": {"value": round(v, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config(w, args) -> dict:
+    i = w.info
+    return {"workload": f"{w.name}: {i['cells']}^3 cells of {i['cell_m'] * 1e3:g} mm, CPML {i['cpml']}, "
+                        f"2-pole Lorentz sphere r={i['radius']:g} cells (eps_inf 2.0), Drude slab {i['slab']} cells, "
+                        f"soft E_x sheet ({i['sheet_edges']} edges), {i['scheme']} ADE, dt = "
+                        f"{i['courant']} x Courant limit",
+            "cells": w.cells, "seed": "0x5eed",
+            "l2": "inputs larger than L2 (fields alone 3.2 GB at 512^3); no flush between steps",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def run_ours(args):
+    import torch
+
+    import ems_b200 as E
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dev = local if world > 1 else 0
+    total_steps = args.warmup + args.steps
+    w = workload(args.cells, total_steps + 10)
+    eng = E.Engine(w.model, device=dev)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+    eng.run(args.warmup)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # --- timed region
+    eng.profile(True)
+    launches0 = eng.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        eng.run(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    launches = eng.launches - launches0
+    kern = {k: eng.profile_read(k) for k in (0, 1, 2)}
+    eng.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * w.cells * args.steps / (ms * 1e-3) / 1e6
+
+    # --- end to end through the C ABI: per step, amplitude H2D, step, probe sample D2H
+    amp_op = w.source
+    probe_op = w.probes[0]
+    from ems_b200 import waveform_value
+
+    t_src = lambda n: waveform_value(w.info["f0"], w.info["fc"], (n + 0.5) * w.model.dt)  # noqa: E731
+    k_e2e = max(1, min(args.steps, 100))
+    first = eng.timestep
+    host_amp = np.array([t_src(first + q) for q in range(k_e2e)], dtype=np.float64)
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for q in range(k_e2e):
+        eng.source_amplitude(amp_op, first + q, host_amp[q:q + 1])
+        eng.run(1)
+        eng.last_sample(probe_op)
+    el = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([el], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        el = float(t.item())
+    e2e = world * w.cells * k_e2e / el / 1e6
+
+    if rank != 0:
+        eng.close()
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    ab = algorithmic_bytes(w)
+    peaks = measured_peaks()
+    # Dominant kernel: the fused step if it ran, else the H update.
+    if kern[2][1] > 0:
+        kname, (kms, kn) = "fused_step", kern[2]
+        per_launch = ab["total"]
+    else:
+        kname, (kms, kn) = "update_h", kern[0]
+        per_launch = 36.0 * ab["cells"]
+    achieved = per_launch / (kms * 1e-3 / kn) / 1e9 if kn else None
+    step_gbs = ab["total"] / (ms * 1e-3 / args.steps) / 1e9 / (world)
+    traffic = profile_traffic(kname)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 pole state", "data": "synthetic",
+        "config": config(w, args),
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1) if achieved else None,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4) if achieved else None,
+                     "traffic": traffic, "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": per_launch,
+                     "mean_launch_ms": round(kms / kn, 4) if kn else None},
+        "step_roofline": {"algorithmic_bytes_per_step": ab["total"], "bytes_per_cell": round(ab["total"] / ab["cells"], 2),
+                          "achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peaks["hbm_gbs"], 4)},
+        "kernels_ms": {("update_h", "update_e", "fused_step")[k]: {"ms": round(v[0], 3), "launches": v[1]}
+                       for k, v in kern.items() if v[1]},
+        "e2e": {"value": round(e2e, 1), "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8,
+                "steps": k_e2e},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline(w)
+    eng.close()
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -56,6 +56,30 @@ class EngineDesc(C.Structure):
     ]
 
 
+class OpEntry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("table", C.c_void_p)]
+
+
+class CpmlSlab(C.Structure):
+    _fields_ = [("e_side", C.c_int32), ("comp", C.c_int32), ("normal", C.c_int32), ("other", C.c_int32),
+                ("sign", C.c_float), ("lo", C.c_uint64 * 3), ("hi", C.c_uint64 * 3),
+                ("b", C.c_void_p), ("a", C.c_void_p), ("k", C.c_void_p)]
+
+
+class CpmlTable(C.Structure):
+    _fields_ = [("n_slabs", C.c_size_t), ("slabs", C.c_void_p)]
+
+
+class PoleSide(C.Structure):
+    _fields_ = [("n_edges", C.c_size_t), ("axis", C.c_void_p), ("node", C.c_void_p), ("sum_inv_z", C.c_void_p),
+                ("pole_end", C.c_void_p), ("n_poles", C.c_size_t), ("kind", C.c_void_p), ("a", C.c_void_p),
+                ("inv_c", C.c_void_p), ("inv_z", C.c_void_p), ("half_l", C.c_void_p)]
+
+
+class PolesTable(C.Structure):
+    _fields_ = [("electric", PoleSide), ("magnetic", PoleSide)]
+
+
 class Stepper(C.Structure):
     _fields_ = [
         ("ctx", C.c_void_p),
@@ -170,6 +194,11 @@ GPU_SYMBOLS = {
     "ems_gpu_last_error": (C.c_char_p, [C.c_void_p]),
     "ems_gpu_launch_count": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+    "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_last_sample": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
+    "ems_gpu_source_amplitude": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p, C.c_size_t]),
+    "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "ems_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
 }
 
 
@@ -497,6 +526,22 @@ class Engine:
     def set_schedule(self, s: int) -> None:
         self._ck(self._lib.ems_gpu_set_schedule(self._h, s))
 
+    @property
+    def stream(self) -> int:
+        """The engine's cudaStream_t (as an integer address)."""
+        p = C.c_void_p()
+        self._ck(self._lib.ems_gpu_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        self._ck(self._lib.ems_gpu_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self, kernel: int) -> tuple[float, int]:
+        """(device ms, launches) of kernel 0 H update, 1 E update, 2 fused step."""
+        ms, n = C.c_double(), C.c_uint64()
+        self._ck(self._lib.ems_gpu_profile_read(self._h, kernel, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def field(self, field: int, axis: int) -> np.ndarray:
         """``u_component`` (field 0) / ``i_component`` (field 1), shape nodes."""
         out = np.empty(self.nodes, dtype=np.float32)
@@ -514,6 +559,15 @@ class Engine:
         if n.value:
             self._ck(self._lib.ems_gpu_samples(self._h, op, which, out.ctypes.data, n.value, C.byref(n)))
         return out
+
+    def last_sample(self, op: int, which: int = 0) -> float:
+        x = C.c_double()
+        self._ck(self._lib.ems_gpu_last_sample(self._h, op, which, C.byref(x)))
+        return x.value
+
+    def source_amplitude(self, op: int, first: int, values) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._ck(self._lib.ems_gpu_source_amplitude(self._h, op, first, v.ctypes.data, len(v)))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

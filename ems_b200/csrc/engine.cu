@@ -101,6 +101,52 @@ struct ems_gpu {
         ProbeDev probe;
     };
     std::vector<Op> ops;
+    // Kernel timing (ems_gpu_profile): event pairs recorded around the
+    // field-update kernels, per kernel id.
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pairs[3];
+    std::vector<cudaEvent_t> ev_free;
+    double prof_ms[3] = {0, 0, 0};
+    uint64_t prof_n[3] = {0, 0, 0};
+
+    cudaEvent_t take_event() {
+        if (!ev_free.empty()) {
+            cudaEvent_t e = ev_free.back();
+            ev_free.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    // Records the start event of a timed kernel; returns it (or null).
+    cudaEvent_t prof_begin() {
+        if (!profiling) return nullptr;
+        cudaEvent_t a = take_event();
+        cudaEventRecord(a, stream);
+        return a;
+    }
+    void prof_end(int kernel, cudaEvent_t a) {
+        if (!a) return;
+        cudaEvent_t b = take_event();
+        cudaEventRecord(b, stream);
+        ev_pairs[kernel].push_back({a, b});
+        if (ev_pairs[kernel].size() >= 4096) prof_collect();
+    }
+    void prof_collect() {
+        cudaStreamSynchronize(stream);
+        for (int k = 0; k < 3; ++k) {
+            for (auto& pr : ev_pairs[k]) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, pr.first, pr.second);
+                prof_ms[k] += ms;
+                prof_n[k] += 1;
+                ev_free.push_back(pr.first);
+                ev_free.push_back(pr.second);
+            }
+            ev_pairs[k].clear();
+        }
+    }
 
     template <class T>
     T* alloc(size_t n) {
@@ -209,11 +255,13 @@ ems_status run_step(ems_gpu* h, bool energy) {
     for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
     dim3 blk(kRowThreads, 1, 1);
     dim3 grd(blocks_for(g.nz, kRowThreads), (unsigned)g.ny, (unsigned)g.nx);
+    cudaEvent_t ev = h->prof_begin();
     if (energy) {
         k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
     } else {
         k_update_h<false><<<grd, blk, 0, s>>>(g, f, c, nullptr);
     }
+    h->prof_end(0, ev);
     ++h->launches;
     if (energy) {
         k_reduce_partials<<<1, 1024, 0, s>>>(h->partials, h->n_partials, h->d_energy);
@@ -264,7 +312,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
             ++h->launches;
         }
     }
+    ev = h->prof_begin();
     k_update_e<<<grd, blk, 0, s>>>(g, f, c);
+    h->prof_end(1, ev);
     ++h->launches;
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML) {
@@ -518,6 +568,8 @@ ems_status ems_gpu_destroy(ems_gpu* h) {
     if (!h) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
+    h->prof_collect();
+    for (cudaEvent_t e : h->ev_free) cudaEventDestroy(e);
     h->bufs.clear();
     cudaStreamDestroy(h->stream);
     delete h;
@@ -620,12 +672,71 @@ ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t
     return check(h, cudaStreamSynchronize(h->stream), "samples");
 }
 
+ems_status ems_gpu_last_sample(ems_gpu* h, size_t op, int which, double* out) {
+    if (!h || !out || op >= h->ops.size()) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    auto& o = h->ops[op];
+    const double* src = nullptr;
+    size_t cnt = 0;
+    if (o.kind == EMS_OP_PROBE && which == 0) {
+        src = o.probe.values;
+        cnt = o.probe.count;
+    } else if (o.kind == EMS_OP_LUMPED && o.lumped.record && which >= 0 && which <= 2 && (which == 0 || o.lumped.columns)) {
+        src = which == 0 ? o.lumped.rec : (which == 1 ? o.lumped.pv : o.lumped.pi);
+        cnt = o.lumped.count;
+    }
+    if (!src || !cnt) return fail(h, EMS_ERR_INVALID, "no sample");
+    if (check(h, cudaMemcpyAsync(out, src + cnt - 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "sample"))
+        return EMS_ERR_CUDA;
+    return check(h, cudaStreamSynchronize(h->stream), "sample");
+}
+
+ems_status ems_gpu_source_amplitude(ems_gpu* h, size_t op, uint64_t first, const double* values, size_t n) {
+    if (!h || (!values && n) || op >= h->ops.size()) return EMS_ERR_INVALID;
+    auto& o = h->ops[op];
+    if (o.kind == EMS_OP_SOURCE) {
+        if (o.source.amp.size() < first + n) o.source.amp.resize(first + n, 0.0f);
+        for (size_t q = 0; q < n; ++q) o.source.amp[first + q] = (float)values[q];
+    } else if (o.kind == EMS_OP_LUMPED && o.lumped.has_src) {
+        if (o.lumped.amp.size() < first + n) o.lumped.amp.resize(first + n, 0.0);
+        for (size_t q = 0; q < n; ++q) o.lumped.amp[first + q] = values[q];
+    } else {
+        return fail(h, EMS_ERR_INVALID, "not a source");
+    }
+    return EMS_OK;
+}
+
 const char* ems_gpu_last_error(const ems_gpu* h) { return h ? h->err.c_str() : "null handle"; }
 
 ems_status ems_gpu_launch_count(const ems_gpu* h, uint64_t* n) {
     if (!h || !n) return EMS_ERR_INVALID;
     *n = h->launches;
     return EMS_OK;
+}
+
+ems_status ems_gpu_stream(const ems_gpu* h, void** stream) {
+    if (!h || !stream) return EMS_ERR_INVALID;
+    *stream = (void*)h->stream;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_profile(ems_gpu* h, int enable) {
+    if (!h) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    h->prof_collect();
+    h->profiling = enable != 0;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* launches) {
+    if (!h || !ms || !launches || kernel < 0 || kernel > 2) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    h->prof_collect();
+    *ms = h->prof_ms[kernel];
+    *launches = h->prof_n[kernel];
+    h->prof_ms[kernel] = 0.0;
+    h->prof_n[kernel] = 0;
+    return check(h, cudaGetLastError(), "profile");
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {

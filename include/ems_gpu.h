@@ -217,11 +217,33 @@ ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* ho
  * `cap` values into `out` (may be NULL) and the total count into *n. */
 ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t cap, size_t* n);
 
+/* The latest sample of a series of ems_gpu_samples (EMS_ERR_INVALID if the
+ * series is empty): one device-to-host read of 8 bytes. */
+ems_status ems_gpu_last_sample(ems_gpu* h, size_t op, int which, double* out);
+
+/* Overwrites amplitudes [first, first + n) of the source table of operator
+ * `op` (an edge source: f32 values; a lumped element: f64 values given as
+ * the doubles in `values`) from host memory, growing the table as needed:
+ * a host may feed a source step by step instead of tabulating it at
+ * creation. */
+ems_status ems_gpu_source_amplitude(ems_gpu* h, size_t op, uint64_t first, const double* values, size_t n);
+
 /* Text of the last error of handle `h` ("" if none; a static text if h is NULL). */
 const char* ems_gpu_last_error(const ems_gpu* h);
 
 /* Device kernels launched since creation (for bookkeeping). */
 ems_status ems_gpu_launch_count(const ems_gpu* h, uint64_t* n);
+
+/* The CUDA stream (cudaStream_t) all work of the handle runs on, so a host
+ * can order its own work after it or time it with events. */
+ems_status ems_gpu_stream(const ems_gpu* h, void** stream);
+
+/* Kernel timing: with enable != 0 the engine records CUDA events around its
+ * field-update kernels (kernel 0: H update, 1: E update, 2: fused step);
+ * ems_gpu_profile_read returns their summed device time [ms] and launch
+ * count since the last read, and resets them. */
+ems_status ems_gpu_profile(ems_gpu* h, int enable);
+ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* launches);
 
 /* Selects the step schedule: 0 = automatic, 1 = separate H/E kernels,
  * 2 = fused single-pass kernel. Results are identical bit for bit. */
