@@ -195,6 +195,7 @@ GPU_SYMBOLS = {
     "ems_gpu_launch_count": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_last_sample": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
     "ems_gpu_source_amplitude": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p, C.c_size_t]),
     "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),
@@ -524,7 +525,15 @@ class Engine:
         return n.value
 
     def set_schedule(self, s: int) -> None:
+        """0: automatic (fused where the model allows it), 1: separate H and E kernels."""
         self._ck(self._lib.ems_gpu_set_schedule(self._h, s))
+
+    @property
+    def schedule(self) -> int:
+        """The schedule steps run with: 1 separate kernels, 2 fused kernel."""
+        v = C.c_int()
+        self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
+        return v.value
 
     @property
     def stream(self) -> int:

@@ -27,6 +27,10 @@
 
 #include "../../include/ems_gpu.h"
 #include "kernels.cuh"
+#include "fused.cuh"
+
+#include <thread>
+#include <unordered_map>
 
 using namespace emsk;
 
@@ -101,6 +105,21 @@ struct ems_gpu {
         ProbeDev probe;
     };
     std::vector<Op> ops;
+    // ---- the fused single-pass schedule
+    bool fused_ok = false;
+    std::string fused_why;          // why the fused schedule is unavailable
+    int fused_tj = 0;
+    void (*fused_launch)(const emsk::FusedParams&, unsigned, unsigned, size_t, cudaStream_t) = nullptr;
+    size_t fused_smem = 0;
+    unsigned fused_grid = 0;
+    float* u2[3] = {nullptr, nullptr, nullptr};
+    float* i2[3] = {nullptr, nullptr, nullptr};
+    FusedParams fp{};               // everything but the field pointers and ψ_H parity
+    std::vector<std::pair<float*, float*>> psi_h;  // ψ of each H slab: (current, other)
+    std::vector<std::pair<int, int>> psi_h_at;     // its place in fp.slab[0][c][q]
+    uint32_t* counter = nullptr;
+    int* status = nullptr;
+    double* fpartials = nullptr;
     // Kernel timing (ems_gpu_profile): event pairs recorded around the
     // field-update kernels, per kernel id.
     bool profiling = false;
@@ -245,9 +264,309 @@ ems_status make_side(ems_gpu* h, const ems_pole_side& t, PoleSideDev& d) {
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// Pools the rows of one coefficient array (src/engine/coeffs.rs:395-599,
+// Lane::Pooled): the distinct z-rows and a row id per (x, y) row; pooled only
+// when at most a quarter of the rows are distinct.
+struct Pooled {
+    bool pooled = false;
+    std::vector<uint32_t> rid;
+    std::vector<float> rows;  // pitch floats each
+    uint32_t bg = 0;
+};
+
+Pooled pool_lane(const float* a, const Grid& g) {
+    Pooled P;
+    const size_t nrows = (size_t)g.nx * g.ny;
+    const size_t nz = g.nz;
+    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;
+    std::vector<size_t> first;  // source row of each distinct id
+    std::vector<uint32_t> count;
+    P.rid.resize(nrows);
+    for (size_t r = 0; r < nrows; ++r) {
+        const float* row = a + r * nz;
+        uint64_t hsh = 1469598103934665603ull;
+        for (size_t k = 0; k < nz; ++k) {
+            uint32_t b;
+            std::memcpy(&b, &row[k], 4);
+            hsh = (hsh ^ b) * 1099511628211ull;
+        }
+        auto& cand = seen[hsh];
+        uint32_t id = 0xffffffffu;
+        for (uint32_t c : cand)
+            if (std::memcmp(a + first[c] * nz, row, nz * 4) == 0) {
+                id = c;
+                break;
+            }
+        if (id == 0xffffffffu) {
+            id = (uint32_t)first.size();
+            first.push_back(r);
+            count.push_back(0);
+            cand.push_back(id);
+            if (first.size() * 4 > nrows) return P;  // not pooled
+        }
+        count[id]++;
+        P.rid[r] = id;
+    }
+    P.pooled = true;
+    P.rows.assign(first.size() * g.pitch, 0.0f);
+    for (size_t d = 0; d < first.size(); ++d) std::memcpy(&P.rows[d * g.pitch], a + first[d] * nz, nz * 4);
+    P.bg = (uint32_t)(std::max_element(count.begin(), count.end()) - count.begin());
+    return P;
+}
+
+// Fused kernel instances: rows per tile × the thread bound of the launch.
+template <int TJ, int MAXT>
+void launch_fused(const FusedParams& P, unsigned grid, unsigned threads, size_t smem, cudaStream_t s) {
+    k_fused<TJ, MAXT><<<grid, threads, smem, s>>>(P);
+}
+
+using FusedLaunch = void (*)(const FusedParams&, unsigned, unsigned, size_t, cudaStream_t);
+
+template <int TJ, int MAXT>
+bool try_tj(ems_gpu* h, int max_smem) {
+    if (h->g.pitch > (uint32_t)MAXT) return false;
+    const size_t bytes = fused_smem_bytes<TJ>(h->g.pitch);
+    if (bytes > (size_t)max_smem) return false;
+    if (cudaFuncSetAttribute(k_fused<TJ, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+        return false;
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fused<TJ, MAXT>, (int)h->g.pitch, bytes) != cudaSuccess ||
+        bps < 1)
+        return false;
+    h->fused_launch = launch_fused<TJ, MAXT>;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    h->fused_tj = TJ;
+    h->fused_smem = bytes;
+    h->fused_grid = (unsigned)(sms * bps);
+    return true;
+}
+
+// Builds the fused schedule's tables; leaves fused_ok false (with the
+// reason) where the model needs the separate kernels.
+ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
+    const Grid& g = h->g;
+    int n_cpml = 0, n_poles = 0;
+    const ems_pole_side* pe = nullptr;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        const int kind = d->ops[k].kind;
+        if (kind == EMS_OP_CPML) ++n_cpml;
+        if (kind == EMS_OP_POLES) {
+            ++n_poles;
+            const auto* p = (const ems_poles*)d->ops[k].table;
+            if (p->magnetic.n_edges) return (h->fused_why = "magnetic poles", EMS_OK);
+            pe = &p->electric;
+        }
+        if (kind == EMS_OP_SOURCE) {
+            const auto* s = (const ems_source*)d->ops[k].table;
+            if (s->kind == EMS_SOFT_H || s->kind == EMS_HARD_H) return (h->fused_why = "magnetic sources", EMS_OK);
+        }
+    }
+    if (n_cpml > 1 || n_poles > 1) return (h->fused_why = "several CPML or dispersive operators", EMS_OK);
+    if (g.pitch > 1024) return (h->fused_why = "z rows longer than 1024 nodes", EMS_OK);
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (!(try_tj<6, 576>(h, max_smem) || try_tj<4, 576>(h, max_smem) || try_tj<2, 576>(h, max_smem) ||
+          try_tj<4, 1024>(h, max_smem) || try_tj<2, 1024>(h, max_smem)))
+        return (h->fused_why = "shared memory", EMS_OK);
+    FusedParams& P = h->fp;
+    P = FusedParams{};
+    P.g = g;
+    P.dt = h->dt;
+    // Coefficient lanes, pooled on host threads (one per lane).
+    Pooled pl[12];
+    {
+        std::vector<std::thread> th;
+        for (int l = 0; l < 12; ++l) th.emplace_back([&, l] { pl[l] = pool_lane(d->coeff[l], g); });
+        for (auto& t : th) t.join();
+    }
+    for (int l = 0; l < 12; ++l) {
+        if (pl[l].pooled) {
+            P.lane[l].dense = nullptr;
+            P.lane[l].rid = h->upload(pl[l].rid.data(), pl[l].rid.size());
+            P.lane[l].rows = h->upload(pl[l].rows.data(), pl[l].rows.size());
+            P.lane[l].bg = pl[l].bg;
+            if (!P.lane[l].rid || !P.lane[l].rows) return fail(h, EMS_ERR_NOMEM, "pooled coefficients");
+        } else {
+            P.lane[l].dense = h->co[l];
+        }
+    }
+    // CPML slabs in application order per (side, component).
+    int at = 0;
+    for (auto& op : h->ops) {
+        (void)at;
+        if (op.kind != EMS_OP_CPML) continue;
+        for (SlabDev& sd : op.cpml) {
+            const int side = sd.e_side ? 1 : 0;
+            int& n = P.nslab[side][sd.comp];
+            if (n >= 4) return (h->fused_why = "more than four CPML slabs per component", EMS_OK);
+            FSlab& f = P.slab[side][sd.comp][n];
+            for (int a = 0; a < 3; ++a) {
+                f.lo[a] = sd.lo[a];
+                f.hi[a] = sd.hi[a];
+            }
+            f.normal = (uint32_t)sd.normal;
+            f.b = sd.b;
+            f.a = sd.a;
+            f.k = sd.k;
+            f.psi_old = sd.psi;
+            f.psi_new = sd.psi;
+            if (!sd.e_side) {
+                size_t len = (size_t)(sd.hi[0] - sd.lo[0]) * (sd.hi[1] - sd.lo[1]) * (sd.hi[2] - sd.lo[2]);
+                float* other = h->alloc<float>(len);
+                if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
+                h->psi_h.push_back({sd.psi, other});
+                h->psi_h_at.push_back({sd.comp, n});
+            }
+            ++n;
+        }
+    }
+    // Order of the slab hooks: the dispersive medium before the CPML?
+    int pos_cpml = -1, pos_poles = -1;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        if (d->ops[k].kind == EMS_OP_CPML) pos_cpml = (int)k;
+        if (d->ops[k].kind == EMS_OP_POLES) pos_poles = (int)k;
+    }
+    P.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
+    // Electric poles as runs along z (edges are in (plane, axis, y, z) order).
+    if (pe && pe->n_edges) {
+        std::vector<PoleRun> runs;
+        std::vector<double> sets;
+        std::unordered_map<std::string, uint32_t> set_of;
+        std::vector<uint2> row_runs((size_t)g.nx * 3 * g.ny, make_uint2(0, 0));
+        uint64_t last_row = ~0ull;
+        uint32_t last_k = 0;
+        for (size_t e = 0; e < pe->n_edges; ++e) {
+            const uint64_t idx = pe->node[e];
+            const uint64_t kk = idx % g.nz, rr = idx / g.nz;
+            const uint64_t jj = rr % g.ny, ii = rr / g.ny;
+            const uint64_t row_key = (ii * 3 + pe->axis[e]) * g.ny + jj;
+            const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
+            const uint32_t np = p1 - p0;
+            if (np > kMaxPoles || np == 0) return (h->fused_why = "edge pole count", EMS_OK);
+            std::string key((size_t)np * 3 * 8 + 8 + 4, '\0');
+            uint32_t kinds = 0;
+            for (uint32_t q = 0; q < np; ++q) {
+                const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
+                std::memcpy(&key[q * 24], c3, 24);
+                if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
+            }
+            std::memcpy(&key[np * 24], &pe->sum_inv_z[e], 8);
+            std::memcpy(&key[np * 24 + 8], &kinds, 4);
+            auto it = set_of.find(key);
+            uint32_t set;
+            if (it == set_of.end()) {
+                set = (uint32_t)sets.size();
+                for (uint32_t q = 0; q < np; ++q) {
+                    sets.push_back(pe->a[p0 + q]);
+                    sets.push_back(pe->inv_c[p0 + q]);
+                    sets.push_back(pe->inv_z[p0 + q]);
+                }
+                set_of.emplace(key, set);
+            } else {
+                set = it->second;
+            }
+            bool extend = !runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 && runs.back().set == set &&
+                          runs.back().np == np && runs.back().kinds == kinds;
+            if (extend) {
+                runs.back().ke = (uint32_t)kk + 1;
+            } else {
+                if (row_key != last_row) row_runs[row_key] = make_uint2((uint32_t)runs.size(), 0);
+                PoleRun R{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, pe->sum_inv_z[e]};
+                runs.push_back(R);
+                row_runs[row_key].y++;
+            }
+            last_row = row_key;
+            last_k = (uint32_t)kk;
+        }
+        P.has_poles = 1;
+        P.runs = h->upload(runs.data(), runs.size());
+        P.sets = h->upload(sets.data(), sets.size());
+        P.row_runs = h->upload(row_runs.data(), row_runs.size());
+        for (auto& op : h->ops)
+            if (op.kind == EMS_OP_POLES) {
+                P.pj = op.poles.e.j;
+                P.pq = op.poles.e.q;
+            }
+        if (!P.runs || !P.sets || !P.row_runs) return fail(h, EMS_ERR_NOMEM, "pole runs");
+    }
+    // Work items: (row tile, x chunk), about eight per CTA of the persistent grid.
+    P.tiles_j = (g.ny + h->fused_tj - 1) / h->fused_tj;
+    const uint32_t want = 8u * h->fused_grid;
+    uint32_t chunks = std::max<uint32_t>(1, (want + P.tiles_j - 1) / P.tiles_j);
+    uint32_t chunk = std::max<uint32_t>(8, (g.nx + chunks - 1) / chunks);
+    P.chunk = chunk;
+    P.n_chunks = (g.nx + chunk - 1) / chunk;
+    P.n_items = P.tiles_j * P.n_chunks;
+    h->counter = h->alloc<uint32_t>(1);
+    h->status = h->alloc<int>(1);
+    h->fpartials = h->alloc<double>(h->fused_grid);
+    for (int a = 0; a < 3; ++a) {
+        h->u2[a] = h->alloc<float>(g.np);
+        h->i2[a] = h->alloc<float>(g.np);
+        if (!h->u2[a] || !h->i2[a]) return fail(h, EMS_ERR_NOMEM, "second field buffers");
+    }
+    if (!h->counter || !h->status || !h->fpartials) return fail(h, EMS_ERR_NOMEM, "fused schedule");
+    P.counter = h->counter;
+    P.status = h->status;
+    P.partials = h->fpartials;
+    h->fused_ok = true;
+    return EMS_OK;
+}
+
+bool use_fused(const ems_gpu* h) { return h->fused_ok && h->schedule != 1; }
+
+ems_status serial_post_h(ems_gpu* h, const Fields& f);
+ems_status serial_pre_e(ems_gpu* h, const Fields& f);
+ems_status serial_post_e(ems_gpu* h, const Fields& f);
+
+// One step through the fused kernel: lumped pre_e hooks on u^n, the fused
+// H + E pass into the other buffers, then the serial hooks on the new fields.
+ems_status run_step_fused(ems_gpu* h, bool energy) {
+    cudaStream_t s = h->stream;
+    Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    ems_status st = serial_pre_e(h, f);
+    if (st) return st;
+    FusedParams P = h->fp;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = h->u[a];
+        P.io[a] = h->i[a];
+        P.un[a] = h->u2[a];
+        P.in[a] = h->i2[a];
+    }
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        fs.psi_old = h->psi_h[q].first;
+        fs.psi_new = h->psi_h[q].second;
+    }
+    P.energy = energy ? 1 : 0;
+    cudaMemsetAsync(h->counter, 0, sizeof(uint32_t), s);
+    cudaEvent_t ev = h->prof_begin();
+    h->fused_launch(P, h->fused_grid, h->g.pitch, h->fused_smem, s);
+    h->prof_end(2, ev);
+    h->launches += 2;
+    if (energy) {
+        k_reduce_partials<<<1, 1024, 0, s>>>(h->fpartials, h->fused_grid, h->d_energy);
+        ++h->launches;
+    }
+    for (int a = 0; a < 3; ++a) {
+        std::swap(h->u[a], h->u2[a]);
+        std::swap(h->i[a], h->i2[a]);
+    }
+    for (auto& pr : h->psi_h) std::swap(pr.first, pr.second);
+    Fields nf{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    st = serial_post_h(h, nf);
+    if (st) return st;
+    st = serial_post_e(h, nf);
+    if (st) return st;
+    ++h->step;
+    return EMS_OK;
+}
+
 // One step through the separate-kernel schedule; energy: record the
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
+    if (use_fused(h)) return run_step_fused(h, energy);
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
@@ -287,31 +606,10 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         }
     }
-    // Serial post_h hooks: magnetic sources, current probes.
-    for (auto& op : h->ops) {
-        if (op.kind == EMS_OP_SOURCE && (op.source.kind == EMS_SOFT_H || op.source.kind == EMS_HARD_H)) {
-            const ems_gpu::SourceDev& sd = op.source;
-            float a = h->step < sd.amp.size() ? sd.amp[h->step] : 0.0f;
-            bool hard = sd.kind == EMS_HARD_H;
-            if (!hard && a == 0.0f) continue;
-            k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.i[0], f.i[1], f.i[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
-            ++h->launches;
-        } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_CURRENT && h->step % op.probe.interval == 0) {
-            ems_gpu::ProbeDev& p = op.probe;
-            ems_status st = grow(h, &p.values, p.count, &p.cap, p.count + 1);
-            if (st) return st;
-            k_probe<<<1, 32, 0, s>>>(f.i[0], f.i[1], f.i[2], p.d, p.values + p.count);
-            ++h->launches;
-            ++p.count;
-        }
-    }
-    // pre_e: lumped elements save u^n.
-    for (auto& op : h->ops) {
-        if (op.kind == EMS_OP_LUMPED && (op.lumped.record || op.lumped.has_branch)) {
-            k_lumped_pre_e<<<blocks_for(op.lumped.n_edges, 128), 128, 0, s>>>(f.u[op.lumped.axis], op.lumped.d);
-            ++h->launches;
-        }
-    }
+    ems_status st = serial_post_h(h, f);
+    if (st) return st;
+    st = serial_pre_e(h, f);
+    if (st) return st;
     ev = h->prof_begin();
     k_update_e<<<grd, blk, 0, s>>>(g, f, c);
     h->prof_end(1, ev);
@@ -335,7 +633,50 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         }
     }
-    // Serial post_e hooks in registration order.
+    st = serial_post_e(h, f);
+    if (st) return st;
+    ++h->step;
+    return EMS_OK;
+}
+
+// Serial post_h hooks in registration order: magnetic sources, current probes.
+ems_status serial_post_h(ems_gpu* h, const Fields& f) {
+    cudaStream_t s = h->stream;
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_SOURCE && (op.source.kind == EMS_SOFT_H || op.source.kind == EMS_HARD_H)) {
+            const ems_gpu::SourceDev& sd = op.source;
+            float a = h->step < sd.amp.size() ? sd.amp[h->step] : 0.0f;
+            bool hard = sd.kind == EMS_HARD_H;
+            if (!hard && a == 0.0f) continue;
+            k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.i[0], f.i[1], f.i[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_CURRENT && h->step % op.probe.interval == 0) {
+            ems_gpu::ProbeDev& p = op.probe;
+            ems_status st = grow(h, &p.values, p.count, &p.cap, p.count + 1);
+            if (st) return st;
+            k_probe<<<1, 32, 0, s>>>(f.i[0], f.i[1], f.i[2], p.d, p.values + p.count);
+            ++h->launches;
+            ++p.count;
+        }
+    }
+    return EMS_OK;
+}
+
+// pre_e: lumped elements save u^n.
+ems_status serial_pre_e(ems_gpu* h, const Fields& f) {
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_LUMPED && (op.lumped.record || op.lumped.has_branch)) {
+            k_lumped_pre_e<<<blocks_for(op.lumped.n_edges, 128), 128, 0, h->stream>>>(f.u[op.lumped.axis], op.lumped.d);
+            ++h->launches;
+        }
+    }
+    return EMS_OK;
+}
+
+// Serial post_e hooks in registration order: lumped elements, electric
+// sources, voltage probes.
+ems_status serial_post_e(ems_gpu* h, const Fields& f) {
+    cudaStream_t s = h->stream;
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_LUMPED) {
             ems_gpu::LumpedDev& L = op.lumped;
@@ -373,7 +714,6 @@ ems_status run_step(ems_gpu* h, bool energy) {
             ++p.count;
         }
     }
-    ++h->step;
     return EMS_OK;
 }
 
@@ -559,6 +899,10 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
         }
         h->ops.push_back(std::move(op));
     }
+    {
+        ems_status st = setup_fused(h.get(), d);
+        if (st) return st;
+    }
     if (check(h.get(), cudaStreamSynchronize(h->stream), "create")) return EMS_ERR_CUDA;
     *out = h.release();
     return EMS_OK;
@@ -584,6 +928,17 @@ ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
         if (st) return st;
     }
     return check(h, cudaGetLastError(), "run");
+}
+
+// Reads the device status flag of the fused kernel's bounded waits.
+static ems_status device_status(ems_gpu* h) {
+    if (!h->status) return EMS_OK;
+    int st = 0;
+    if (check(h, cudaMemcpyAsync(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status"))
+        return EMS_ERR_CUDA;
+    if (check(h, cudaStreamSynchronize(h->stream), "status")) return EMS_ERR_CUDA;
+    if (st) return fail(h, EMS_ERR_TIMEOUT, "a bounded wait of the fused kernel ran out");
+    return EMS_OK;
 }
 
 ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
@@ -614,7 +969,7 @@ ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
         return EMS_ERR_CUDA;
     if (check(h, cudaStreamSynchronize(h->stream), "energy")) return EMS_ERR_CUDA;
     *energy = 0.25 * h->dt * w + w_ops;
-    return EMS_OK;
+    return device_status(h);
 }
 
 ems_status ems_gpu_timestep(const ems_gpu* h, uint64_t* n) {
@@ -632,18 +987,24 @@ ems_status ems_gpu_download_field(ems_gpu* h, int field, int axis, float* host) 
                                    (size_t)g.nx * g.ny, cudaMemcpyDeviceToHost, h->stream),
               "download"))
         return EMS_ERR_CUDA;
-    return check(h, cudaStreamSynchronize(h->stream), "download");
+    if (check(h, cudaStreamSynchronize(h->stream), "download")) return EMS_ERR_CUDA;
+    return device_status(h);
 }
 
 ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* host) {
     if (!h || !host || field < 0 || field > 1 || axis < 0 || axis > 2) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     const Grid& g = h->g;
-    float* dst = field == 0 ? h->u[axis] : h->i[axis];
-    if (check(h, cudaMemcpy2DAsync(dst, g.pitch * sizeof(float), host, g.nz * sizeof(float), g.nz * sizeof(float),
-                                   (size_t)g.nx * g.ny, cudaMemcpyHostToDevice, h->stream),
-              "upload"))
-        return EMS_ERR_CUDA;
+    // Both buffers of a double-buffered field get the values (the padding
+    // entries the kernels read as zero stay equal in both).
+    float* dsts[2] = {field == 0 ? h->u[axis] : h->i[axis], field == 0 ? h->u2[axis] : h->i2[axis]};
+    for (float* dst : dsts) {
+        if (!dst) continue;
+        if (check(h, cudaMemcpy2DAsync(dst, g.pitch * sizeof(float), host, g.nz * sizeof(float), g.nz * sizeof(float),
+                                       (size_t)g.nx * g.ny, cudaMemcpyHostToDevice, h->stream),
+                  "upload"))
+            return EMS_ERR_CUDA;
+    }
     return check(h, cudaStreamSynchronize(h->stream), "upload");
 }
 
@@ -669,7 +1030,8 @@ ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t
         if (check(h, cudaMemcpyAsync(out, src, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "samples"))
             return EMS_ERR_CUDA;
     }
-    return check(h, cudaStreamSynchronize(h->stream), "samples");
+    if (check(h, cudaStreamSynchronize(h->stream), "samples")) return EMS_ERR_CUDA;
+    return device_status(h);
 }
 
 ems_status ems_gpu_last_sample(ems_gpu* h, size_t op, int which, double* out) {
@@ -740,8 +1102,14 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 2) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 1) return EMS_ERR_INVALID;
     h->schedule = schedule;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {
+    if (!h || !active) return EMS_ERR_INVALID;
+    *active = use_fused(h) ? 2 : 1;
     return EMS_OK;
 }
 

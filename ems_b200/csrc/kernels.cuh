@@ -100,7 +100,8 @@ __device__ __forceinline__ double weight(float a, double p, float b) {
     return b != 0.0f ? __ddiv_rn(__dmul_rn(__dadd_rn(1.0, (double)a), p), (double)b) : 0.0;
 }
 
-// Block-wide f64 sum in a fixed order; result valid in thread 0.
+// Block-wide f64 sum in a fixed order (blockDim.x a multiple of 32, at
+// most THREADS); result valid in thread 0.
 template <unsigned THREADS>
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double sh[THREADS / 32];
@@ -110,7 +111,7 @@ __device__ __forceinline__ double block_sum(double v) {
     __syncthreads();
     double s = 0.0;
     if (threadIdx.x == 0)
-        for (unsigned q = 0; q < THREADS / 32; ++q) s = __dadd_rn(s, sh[q]);
+        for (unsigned q = 0; q < blockDim.x / 32; ++q) s = __dadd_rn(s, sh[q]);
     return s;
 }
 
@@ -203,16 +204,16 @@ __global__ void k_cpml(Grid g, Fields f, Coeffs c, SlabDev s) {
     if (k >= s.hi[2]) return;
     const uint32_t si = g.ny * g.pitch;
     const uint32_t idx = i * si + j * g.pitch + k;
-    const uint32_t node[3] = {i, j, k};
     const uint32_t step = s.normal == 0 ? si : (s.normal == 1 ? g.pitch : 1u);
-    const uint32_t d = node[s.normal] - s.lo[s.normal];
+    const uint32_t along = s.normal == 0 ? i : (s.normal == 1 ? j : k);
+    const uint32_t d = along - s.lo[s.normal];
     float h, l;
     float* t;
     float coef;
     if (E_SIDE) {
         const float* src = f.i[s.other];
         h = src[idx];
-        l = node[s.normal] == 0 ? 0.0f : src[idx - step];
+        l = along == 0 ? 0.0f : src[idx - step];
         t = f.u[s.comp];
         coef = c.c[3 + s.comp][idx];
     } else {
@@ -231,6 +232,8 @@ __global__ void k_cpml(Grid g, Fields f, Coeffs c, SlabDev s) {
 }
 
 // Dispersive correction of one edge per thread (src/engine/dispersive.rs:1392-1470).
+// A leapfrog pole's new state does not depend on the corrected value and is
+// stored at once; a trapezoidal pole's is formed from its old state after it.
 __global__ void k_poles_correct(Grid g, Fields f, Coeffs c, PoleSideDev p, bool electric, double dt) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= p.n_edges) return;
@@ -244,26 +247,25 @@ __global__ void k_poles_correct(Grid g, Fields f, Coeffs c, PoleSideDev p, bool 
     const double half_prev = __dmul_rn(0.5, prev);
     const double u_star = (double)fld[idx];
     double s = 0.0;
-    double nj[kMaxPoles], nq[kMaxPoles];
+    bool trap = false;
     for (uint32_t q = p0; q < p1; ++q) {
         const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
         if (p.kind[q] == 1) {  // leapfrog: j^{n+1/2} from u^n, then q^{n+1}
             const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
-            nj[q - p0] = jn;
-            nq[q - p0] = __dadd_rn(qq, __dmul_rn(dt, jn));
+            p.j[q] = jn;
+            p.q[q] = __dadd_rn(qq, __dmul_rn(dt, jn));
             s = __dadd_rn(s, jn);
         } else {
+            trap = true;
             s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
         }
     }
     const float u_new = (float)__ddiv_rn(__dsub_rn(u_star, __dmul_rn(cb, s)),
                                          __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), p.sum_inv_z[e])));
-    const double half_new = __dmul_rn(0.5, (double)u_new);
-    for (uint32_t q = p0; q < p1; ++q) {
-        if (p.kind[q] == 1) {
-            p.j[q] = nj[q - p0];
-            p.q[q] = nq[q - p0];
-        } else {
+    if (trap) {
+        const double half_new = __dmul_rn(0.5, (double)u_new);
+        for (uint32_t q = p0; q < p1; ++q) {
+            if (p.kind[q] == 1) continue;
             const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
             const double kk = __dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev);
             const double jb = __dmul_rn(__dadd_rn(kk, half_new), iz);

@@ -245,9 +245,13 @@ ems_status ems_gpu_stream(const ems_gpu* h, void** stream);
 ems_status ems_gpu_profile(ems_gpu* h, int enable);
 ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* launches);
 
-/* Selects the step schedule: 0 = automatic, 1 = separate H/E kernels,
- * 2 = fused single-pass kernel. Results are identical bit for bit. */
+/* Selects the step schedule: 0 = automatic (the fused single-pass kernel
+ * where the model allows it), 1 = separate H and E kernels. Results are
+ * identical bit for bit. */
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
+
+/* The schedule steps run with: 1 separate kernels, 2 fused kernel. */
+ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
 #ifdef __cplusplus
 }

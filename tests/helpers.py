@@ -77,7 +77,7 @@ def small_cavity(kappa: float = 0.0, threads_hint: int = 2):
     return m, t_end
 
 
-def mixed_model(n=(18, 16, 14), scheme=E.TRAPEZOIDAL, cpml=3, magnetic=True, lumped=True, steps=200):
+def mixed_model(n=(18, 16, 14), scheme=E.TRAPEZOIDAL, cpml=3, magnetic=True, lumped=True, steps=200, h_source=True):
     """A small model that exercises every operator: graded mesh, materials,
     a PEC box and a PMC face, CPML, electric Lorentz/Drude/Debye and
     magnetic poles, a lumped port, soft/hard E and H sources, voltage and
@@ -108,7 +108,8 @@ def mixed_model(n=(18, 16, 14), scheme=E.TRAPEZOIDAL, cpml=3, magnetic=True, lum
     f, _ = pulse(6e9, 4e9)
     amp = soft_e_table(f, m.dt, steps)
     ops["soft_e"] = m.add_source_table(E.SOFT_E, [(E.Z, (9, 8, 7), 1.0), (E.Y, (6, 5, 9), -0.5)], amp)
-    ops["soft_h"] = m.add_source_table(E.SOFT_H, [(E.X, (12, 10, 9), 1e-3)], 0.5 * amp)
+    if h_source:
+        ops["soft_h"] = m.add_source_table(E.SOFT_H, [(E.X, (12, 10, 9), 1e-3)], 0.5 * amp)
     ops["hard_e"] = m.add_source_table(E.HARD_E, [(E.X, (2, 2, 2), 1.0)], 0.1 * amp)
     ops["pv"] = m.add_probe(E.VOLTAGE, [(E.Z, (9, 8, 8), 1.0), (E.Z, (9, 8, 9), 1.0)])
     ops["pi"] = m.add_probe(E.CURRENT, [(E.X, (9, 8, 7), 1.0), (E.Y, (9, 8, 7), -1.0)], interval=3)

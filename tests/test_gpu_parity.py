@@ -74,6 +74,32 @@ def test_every_operator_bit_exact(scheme):
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
 
 
+@pytest.mark.parametrize("scheme", [E.TRAPEZOIDAL, E.LEAPFROG])
+def test_fused_schedule_bit_exact(scheme):
+    """Without magnetic poles and H sources the fused single-pass kernel
+    runs; it must equal the separate kernels and the oracle bit for bit."""
+    m, ops = mixed_model(scheme=scheme, magnetic=False, h_source=False, steps=240)
+    g, o, eg, eo = _lockstep(m, 240, energy_every=20)
+    assert g.schedule == 2
+    s = E.Engine(m)
+    s.set_schedule(1)
+    assert s.schedule == 1
+    s.run(240)
+    assert_fields_equal(g, o, f"fused vs oracle, scheme {scheme}")
+    assert_fields_equal(g, s, f"fused vs separate, scheme {scheme}")
+    for name in ("pv", "pi", "pe"):
+        _series_equal(g, o, ops[name])
+    for which in (0, 1, 2):
+        _series_equal(g, o, ops["port"], which)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_separate_schedule_where_fused_cannot_run():
+    m, _ = mixed_model(magnetic=True, steps=10)
+    g = E.Engine(m)
+    assert g.schedule == 1
+
+
 def test_odd_sizes_and_tile_remainders():
     # nz = 33 + 1 nodes (a row pitch remainder), ny odd, CPML of 1 cell.
     m = E.Model.uniform([7, 5, 33], [1e-3, 1.2e-3, 0.9e-3])
@@ -92,6 +118,7 @@ def test_vacuum_box_configuration_bit_exact():
     4 E_z probes; fields and probe series bit-exact."""
     w = W.vacuum_box()
     g, o, _, _ = _lockstep(w.model, w.steps, threads=0)
+    assert g.schedule == 2
     for p in w.probes:
         _series_equal(g, o, p)
     assert_fields_equal(g, o, "vacuum box")
@@ -100,6 +127,7 @@ def test_vacuum_box_configuration_bit_exact():
 def test_dispersive_box_small_bit_exact():
     w = W.dispersive_box(n=48, radius=8, slab=4, cpml=5, steps=300)
     g, o, eg, eo = _lockstep(w.model, 300, energy_every=30)
+    assert g.schedule == 2
     assert_fields_equal(g, o, "dispersive box")
     for p in w.probes:
         _series_equal(g, o, p)
@@ -139,3 +167,13 @@ def test_invalid_tables_rejected():
     g = E.Engine(m)
     with pytest.raises(E.EngineError):
         g.samples(99)
+
+
+@pytest.mark.parametrize("n", [40, 67])
+def test_dispersive_box_chunks_and_tiles(n):
+    """Sizes whose rows, tiles and x chunks leave remainders; fused and separate."""
+    w = W.dispersive_box(n=n, radius=n / 6, slab=3, cpml=4, steps=120)
+    g, o, eg, eo = _lockstep(w.model, 120, energy_every=15)
+    assert g.schedule == 2
+    assert_fields_equal(g, o, f"dispersive {n}")
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
