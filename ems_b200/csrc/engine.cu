@@ -28,6 +28,7 @@
 #include "../../include/ems_gpu.h"
 #include "kernels.cuh"
 #include "fused.cuh"
+#include "fused_tables.h"
 
 #include <thread>
 #include <unordered_map>
@@ -264,56 +265,6 @@ ems_status make_side(ems_gpu* h, const ems_pole_side& t, PoleSideDev& d) {
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
-// Pools the rows of one coefficient array (src/engine/coeffs.rs:395-599,
-// Lane::Pooled): the distinct z-rows and a row id per (x, y) row; pooled only
-// when at most a quarter of the rows are distinct.
-struct Pooled {
-    bool pooled = false;
-    std::vector<uint32_t> rid;
-    std::vector<float> rows;  // pitch floats each
-    uint32_t bg = 0;
-};
-
-Pooled pool_lane(const float* a, const Grid& g) {
-    Pooled P;
-    const size_t nrows = (size_t)g.nx * g.ny;
-    const size_t nz = g.nz;
-    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;
-    std::vector<size_t> first;  // source row of each distinct id
-    std::vector<uint32_t> count;
-    P.rid.resize(nrows);
-    for (size_t r = 0; r < nrows; ++r) {
-        const float* row = a + r * nz;
-        uint64_t hsh = 1469598103934665603ull;
-        for (size_t k = 0; k < nz; ++k) {
-            uint32_t b;
-            std::memcpy(&b, &row[k], 4);
-            hsh = (hsh ^ b) * 1099511628211ull;
-        }
-        auto& cand = seen[hsh];
-        uint32_t id = 0xffffffffu;
-        for (uint32_t c : cand)
-            if (std::memcmp(a + first[c] * nz, row, nz * 4) == 0) {
-                id = c;
-                break;
-            }
-        if (id == 0xffffffffu) {
-            id = (uint32_t)first.size();
-            first.push_back(r);
-            count.push_back(0);
-            cand.push_back(id);
-            if (first.size() * 4 > nrows) return P;  // not pooled
-        }
-        count[id]++;
-        P.rid[r] = id;
-    }
-    P.pooled = true;
-    P.rows.assign(first.size() * g.pitch, 0.0f);
-    for (size_t d = 0; d < first.size(); ++d) std::memcpy(&P.rows[d * g.pitch], a + first[d] * nz, nz * 4);
-    P.bg = (uint32_t)(std::max_element(count.begin(), count.end()) - count.begin());
-    return P;
-}
-
 // Fused kernel instances: rows per tile × the thread bound of the launch.
 template <int TJ, int MAXT>
 void launch_fused(const FusedParams& P, unsigned grid, unsigned threads, size_t smem, cudaStream_t s) {
@@ -342,147 +293,74 @@ bool try_tj(ems_gpu* h, int max_smem) {
     return true;
 }
 
-// Builds the fused schedule's tables; leaves fused_ok false (with the
-// reason) where the model needs the separate kernels.
+// Builds the fused schedule's tables (fused_tables.h) and uploads them;
+// leaves fused_ok false, with the reason, where the model needs the
+// separate kernels.
 ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
     const Grid& g = h->g;
-    int n_cpml = 0, n_poles = 0;
-    const ems_pole_side* pe = nullptr;
-    for (size_t k = 0; k < d->n_ops; ++k) {
-        const int kind = d->ops[k].kind;
-        if (kind == EMS_OP_CPML) ++n_cpml;
-        if (kind == EMS_OP_POLES) {
-            ++n_poles;
-            const auto* p = (const ems_poles*)d->ops[k].table;
-            if (p->magnetic.n_edges) return (h->fused_why = "magnetic poles", EMS_OK);
-            pe = &p->electric;
-        }
-        if (kind == EMS_OP_SOURCE) {
-            const auto* s = (const ems_source*)d->ops[k].table;
-            if (s->kind == EMS_SOFT_H || s->kind == EMS_HARD_H) return (h->fused_why = "magnetic sources", EMS_OK);
-        }
-    }
-    if (n_cpml > 1 || n_poles > 1) return (h->fused_why = "several CPML or dispersive operators", EMS_OK);
-    if (g.pitch > 1024) return (h->fused_why = "z rows longer than 1024 nodes", EMS_OK);
+    h->fused_why = fused_ineligible(d, g.pitch);
+    if (!h->fused_why.empty()) return EMS_OK;
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
     if (!(try_tj<6, 576>(h, max_smem) || try_tj<4, 576>(h, max_smem) || try_tj<2, 576>(h, max_smem) ||
-          try_tj<4, 1024>(h, max_smem) || try_tj<2, 1024>(h, max_smem)))
-        return (h->fused_why = "shared memory", EMS_OK);
+          try_tj<4, 1024>(h, max_smem) || try_tj<2, 1024>(h, max_smem))) {
+        h->fused_why = "shared memory";
+        return EMS_OK;
+    }
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        h->fused_why = T.why;
+        return EMS_OK;
+    }
     FusedParams& P = h->fp;
     P = FusedParams{};
     P.g = g;
     P.dt = h->dt;
-    // Coefficient lanes, pooled on host threads (one per lane).
-    Pooled pl[12];
-    {
-        std::vector<std::thread> th;
-        for (int l = 0; l < 12; ++l) th.emplace_back([&, l] { pl[l] = pool_lane(d->coeff[l], g); });
-        for (auto& t : th) t.join();
-    }
     for (int l = 0; l < 12; ++l) {
-        if (pl[l].pooled) {
+        if (T.lane[l].pooled) {
             P.lane[l].dense = nullptr;
-            P.lane[l].rid = h->upload(pl[l].rid.data(), pl[l].rid.size());
-            P.lane[l].rows = h->upload(pl[l].rows.data(), pl[l].rows.size());
-            P.lane[l].bg = pl[l].bg;
+            P.lane[l].rid = h->upload(T.lane[l].rid.data(), T.lane[l].rid.size());
+            P.lane[l].rows = h->upload(T.lane[l].rows.data(), T.lane[l].rows.size());
+            P.lane[l].bg = T.lane[l].bg;
             if (!P.lane[l].rid || !P.lane[l].rows) return fail(h, EMS_ERR_NOMEM, "pooled coefficients");
         } else {
             P.lane[l].dense = h->co[l];
         }
     }
-    // CPML slabs in application order per (side, component).
-    int at = 0;
-    for (auto& op : h->ops) {
-        (void)at;
-        if (op.kind != EMS_OP_CPML) continue;
-        for (SlabDev& sd : op.cpml) {
-            const int side = sd.e_side ? 1 : 0;
-            int& n = P.nslab[side][sd.comp];
-            if (n >= 4) return (h->fused_why = "more than four CPML slabs per component", EMS_OK);
-            FSlab& f = P.slab[side][sd.comp][n];
-            for (int a = 0; a < 3; ++a) {
-                f.lo[a] = sd.lo[a];
-                f.hi[a] = sd.hi[a];
-            }
-            f.normal = (uint32_t)sd.normal;
-            f.b = sd.b;
-            f.a = sd.a;
-            f.k = sd.k;
-            f.psi_old = sd.psi;
-            f.psi_new = sd.psi;
-            if (!sd.e_side) {
-                size_t len = (size_t)(sd.hi[0] - sd.lo[0]) * (sd.hi[1] - sd.lo[1]) * (sd.hi[2] - sd.lo[2]);
-                float* other = h->alloc<float>(len);
-                if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
-                h->psi_h.push_back({sd.psi, other});
-                h->psi_h_at.push_back({sd.comp, n});
-            }
-            ++n;
+    // CPML slabs: the engine's device copies (b, a, k, ψ), in the tables' order.
+    const std::vector<SlabDev>* dev_slabs = nullptr;
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_CPML) dev_slabs = &op.cpml;
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    size_t q_dev = 0;
+    for (const FusedSlabSpec& sp : T.slabs) {
+        // The engine keeps the non-empty slabs of the table in order too.
+        const SlabDev& sd = (*dev_slabs)[q_dev++];
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = sd.lo[a];
+            f.hi[a] = sd.hi[a];
+        }
+        f.normal = (uint32_t)sd.normal;
+        f.b = sd.b;
+        f.a = sd.a;
+        f.k = sd.k;
+        f.psi_old = sd.psi;
+        f.psi_new = sd.psi;
+        if (!sp.side) {
+            float* other = h->alloc<float>(sp.len);
+            if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
+            h->psi_h.push_back({sd.psi, other});
+            h->psi_h_at.push_back({sp.comp, sp.q});
         }
     }
-    // Order of the slab hooks: the dispersive medium before the CPML?
-    int pos_cpml = -1, pos_poles = -1;
-    for (size_t k = 0; k < d->n_ops; ++k) {
-        if (d->ops[k].kind == EMS_OP_CPML) pos_cpml = (int)k;
-        if (d->ops[k].kind == EMS_OP_POLES) pos_poles = (int)k;
-    }
-    P.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
-    // Electric poles as runs along z (edges are in (plane, axis, y, z) order).
-    if (pe && pe->n_edges) {
-        std::vector<PoleRun> runs;
-        std::vector<double> sets;
-        std::unordered_map<std::string, uint32_t> set_of;
-        std::vector<uint2> row_runs((size_t)g.nx * 3 * g.ny, make_uint2(0, 0));
-        uint64_t last_row = ~0ull;
-        uint32_t last_k = 0;
-        for (size_t e = 0; e < pe->n_edges; ++e) {
-            const uint64_t idx = pe->node[e];
-            const uint64_t kk = idx % g.nz, rr = idx / g.nz;
-            const uint64_t jj = rr % g.ny, ii = rr / g.ny;
-            const uint64_t row_key = (ii * 3 + pe->axis[e]) * g.ny + jj;
-            const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
-            const uint32_t np = p1 - p0;
-            if (np > kMaxPoles || np == 0) return (h->fused_why = "edge pole count", EMS_OK);
-            std::string key((size_t)np * 3 * 8 + 8 + 4, '\0');
-            uint32_t kinds = 0;
-            for (uint32_t q = 0; q < np; ++q) {
-                const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
-                std::memcpy(&key[q * 24], c3, 24);
-                if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
-            }
-            std::memcpy(&key[np * 24], &pe->sum_inv_z[e], 8);
-            std::memcpy(&key[np * 24 + 8], &kinds, 4);
-            auto it = set_of.find(key);
-            uint32_t set;
-            if (it == set_of.end()) {
-                set = (uint32_t)sets.size();
-                for (uint32_t q = 0; q < np; ++q) {
-                    sets.push_back(pe->a[p0 + q]);
-                    sets.push_back(pe->inv_c[p0 + q]);
-                    sets.push_back(pe->inv_z[p0 + q]);
-                }
-                set_of.emplace(key, set);
-            } else {
-                set = it->second;
-            }
-            bool extend = !runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 && runs.back().set == set &&
-                          runs.back().np == np && runs.back().kinds == kinds;
-            if (extend) {
-                runs.back().ke = (uint32_t)kk + 1;
-            } else {
-                if (row_key != last_row) row_runs[row_key] = make_uint2((uint32_t)runs.size(), 0);
-                PoleRun R{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, pe->sum_inv_z[e]};
-                runs.push_back(R);
-                row_runs[row_key].y++;
-            }
-            last_row = row_key;
-            last_k = (uint32_t)kk;
-        }
+    P.poles_first = T.poles_first ? 1 : 0;
+    if (T.has_poles) {
         P.has_poles = 1;
-        P.runs = h->upload(runs.data(), runs.size());
-        P.sets = h->upload(sets.data(), sets.size());
-        P.row_runs = h->upload(row_runs.data(), row_runs.size());
+        P.runs = h->upload(T.runs.data(), T.runs.size());
+        P.sets = h->upload(T.sets.data(), T.sets.size());
+        P.row_runs = h->upload(T.row_runs.data(), T.row_runs.size());
         for (auto& op : h->ops)
             if (op.kind == EMS_OP_POLES) {
                 P.pj = op.poles.e.j;
@@ -490,14 +368,7 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
             }
         if (!P.runs || !P.sets || !P.row_runs) return fail(h, EMS_ERR_NOMEM, "pole runs");
     }
-    // Work items: (row tile, x chunk), about eight per CTA of the persistent grid.
-    P.tiles_j = (g.ny + h->fused_tj - 1) / h->fused_tj;
-    const uint32_t want = 8u * h->fused_grid;
-    uint32_t chunks = std::max<uint32_t>(1, (want + P.tiles_j - 1) / P.tiles_j);
-    uint32_t chunk = std::max<uint32_t>(8, (g.nx + chunks - 1) / chunks);
-    P.chunk = chunk;
-    P.n_chunks = (g.nx + chunk - 1) / chunk;
-    P.n_items = P.tiles_j * P.n_chunks;
+    fused_work(P, g.nx, g.ny, h->fused_tj, h->fused_grid);
     h->counter = h->alloc<uint32_t>(1);
     h->status = h->alloc<int>(1);
     h->fpartials = h->alloc<double>(h->fused_grid);

@@ -26,7 +26,7 @@
 namespace emsk {
 
 constexpr int kStages = 3;
-constexpr uint32_t kWaitLimit = 1u << 22;  // bounded mbarrier waits
+constexpr uint64_t kWaitNs = 2000000000ull;  // a bounded mbarrier wait gives up after 2 s
 
 struct Lane {
     const float* dense;     // dense array (padded layout), or null if pooled
@@ -79,6 +79,7 @@ struct FusedParams {
     int* status;           // nonzero: a bounded wait ran out
 };
 
+#ifndef EMS_HOST_EMULATION
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -89,10 +90,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Waits for phase `parity` of the barrier, at most kWaitLimit tries.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of the barrier; gives up (returns false) after
+// kWaitNs nanoseconds.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     uint32_t done = 0;
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -101,8 +110,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((it & 63u) == 63u && global_ns() - t0 > kWaitNs) return false;
     }
-    return false;
 }
 
 // One bulk copy global → shared, completing on `bar` (16-byte aligned, size multiple of 16).
@@ -116,6 +125,22 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+#define EMS_DYNAMIC_SMEM(name) extern __shared__ __align__(128) unsigned char name[]
+#define EMS_SHARED __shared__
+#else
+// CPU emulation (tests): the bulk copies complete at once; a barrier is a
+// phase counter and a wait that would not succeed is reported.
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t) { *bar = 0; }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) { emu::expect_tx(bar, bytes); }
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return emu::wait(bar, parity); }
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    emu::bulk(dst, src, bytes, bar);
+}
+__device__ __forceinline__ void fence_proxy_async() {}
+__device__ __forceinline__ void fence_mbar_init() {}
+#define EMS_DYNAMIC_SMEM(name) unsigned char* name = emu::dynamic_smem()
+#define EMS_SHARED static
+#endif
 
 // The CPML correction of one field value t by every slab of `list` that
 // contains the node, in order: ψ = flush(b·ψ + a·s), t = flush(t + coef·(k·s + ψ)),
@@ -198,7 +223,7 @@ __host__ __device__ constexpr size_t fused_smem_bytes(uint32_t pitch) {
 
 template <int TJ, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    EMS_DYNAMIC_SMEM(smem_raw);
     const Grid g = P.g;
     const uint32_t pitch = g.pitch;
     const uint32_t k = threadIdx.x;
@@ -209,8 +234,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
     uint32_t* sid = (uint32_t*)(sbg + 12 * (size_t)pitch);          // row ids [2][12][TJ+1]
     uint2* srun = (uint2*)(sid + 2 * 12 * (TJ + 1));                // pole runs [2][3][TJ]
     uint64_t* bars = (uint64_t*)(((uintptr_t)(srun + 2 * 3 * TJ) + 7) & ~(uintptr_t)7);
-    __shared__ uint32_t s_item;
-    __shared__ int s_fail;
+    EMS_SHARED uint32_t s_item;
+    EMS_SHARED int s_fail;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
@@ -327,6 +352,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
             load_io(i + 1, io_n);  // prefetch for the next plane
 
             // ---- H of rows j0−1 .. j0+TJ−1 (r = 0 .. TJ); r = 0 is the halo row.
+            // Window row w of the staged voltages is y = j0 − 1 + w: row j is r, row j + 1 is r + 1.
             float hx[TJ + 1], hy[TJ + 1], hz[TJ + 1];
 #pragma unroll
             for (int r = 0; r < TJ + 1; ++r) {
@@ -335,11 +361,11 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
                 if (j < 0 || j >= (int)g.ny || k >= g.nz) continue;
                 const bool own = r >= 1 && !warm;
                 const size_t idx = (size_t)i * si + (size_t)j * pitch + k;
-                const float ux = u0(0, r + 1, k), uy = u0(1, r + 1, k), uz = u0(2, r + 1, k);
+                const float ux = u0(0, r, k), uy = u0(1, r, k), uz = u0(2, r, k);
                 // x: (uz[j+1] − uz[j]) − (uy[k+1] − uy[k])
                 if (j + 1 < (int)g.ny && k + 1 < g.nz) {
                     const float da = row(6, b, r, i)[k], db = row(9, b, r, i)[k];
-                    const float A = __fsub_rn(u0(2, r + 2, k), uz), B = __fsub_rn(u0(1, r + 1, k + 1), uy);
+                    const float A = __fsub_rn(u0(2, r + 1, k), uz), B = __fsub_rn(u0(1, r, k + 1), uy);
                     const float old = io_c[0][r];
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
@@ -354,7 +380,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
                 // y: (ux[k+1] − ux[k]) − (uz[i+1] − uz[i])   (owned rows only)
                 if (r >= 1 && nxt && k + 1 < g.nz) {
                     const float da = row(7, b, r, i)[k], db = row(10, b, r, i)[k];
-                    const float A = __fsub_rn(u0(0, r + 1, k + 1), ux), B = __fsub_rn(u1(2, r + 1), uz);
+                    const float A = __fsub_rn(u0(0, r, k + 1), ux), B = __fsub_rn(u1(2, r), uz);
                     const float old = io_c[1][r];
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
@@ -369,7 +395,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
                 // z: (uy[i+1] − uy[i]) − (ux[j+1] − ux[j])
                 if (nxt && j + 1 < (int)g.ny) {
                     const float da = row(8, b, r, i)[k], db = row(11, b, r, i)[k];
-                    const float A = __fsub_rn(u1(1, r + 1), uy), B = __fsub_rn(u0(0, r + 2, k), ux);
+                    const float A = __fsub_rn(u1(1, r), uy), B = __fsub_rn(u0(0, r + 1, k), ux);
                     const float old = io_c[2][r];
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
@@ -391,6 +417,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
                 }
             }
             __syncthreads();
+            if (s_fail) break;
             if (!warm) {
                 // ---- E of the owned rows.
 #pragma unroll
@@ -398,7 +425,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
                     const int j = j0 - 1 + r;
                     if (j >= (int)g.ny || k >= g.nz) continue;
                     const size_t idx = (size_t)i * si + (size_t)j * pitch + k;
-                    const float uxo = u0(0, r + 1, k), uyo = u0(1, r + 1, k), uzo = u0(2, r + 1, k);
+                    const float uxo = u0(0, r, k), uyo = u0(1, r, k), uzo = u0(2, r, k);
                     const float hxk1 = k > 0 ? sh[(size_t)(r - 1) * pitch + k - 1] : 0.0f;
                     const float hyk1 = k > 0 ? sh[(size_t)(TJ + r - 1) * pitch + k - 1] : 0.0f;
                     float ca, cb;

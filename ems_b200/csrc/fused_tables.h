@@ -1,0 +1,221 @@
+// fused_tables.h — host-side tables of the fused step kernel (fused.cuh).
+//
+// Pure host code (no CUDA calls): from an engine descriptor it decides
+// whether the fused schedule can run, pools the coefficient rows, orders the
+// CPML slabs per (side, component) and turns the electric poles into runs
+// along z. The engine uploads the result; the CPU emulation of the kernel
+// used by the tests reads it in place.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ems_gpu.h"
+
+namespace emsk {
+
+// Pools the rows of one coefficient array (src/engine/coeffs.rs:395-599,
+// Lane::Pooled): the distinct z-rows and a row id per (x, y) row; pooled only
+// when at most a quarter of the rows are distinct (coeffs.rs POOL_RATIO).
+struct Pooled {
+    bool pooled = false;
+    std::vector<uint32_t> rid;
+    std::vector<float> rows;  // pitch floats each, zero beyond nz
+    uint32_t bg = 0;          // the most frequent row
+};
+
+inline Pooled pool_lane(const float* a, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t pitch) {
+    Pooled P;
+    const size_t nrows = (size_t)nx * ny;
+    std::unordered_map<uint64_t, std::vector<uint32_t>> seen;
+    std::vector<size_t> first;  // source row of each distinct id
+    std::vector<uint32_t> count;
+    P.rid.resize(nrows);
+    for (size_t r = 0; r < nrows; ++r) {
+        const float* row = a + r * nz;
+        uint64_t hsh = 1469598103934665603ull;
+        for (size_t k = 0; k < nz; ++k) {
+            uint32_t b;
+            std::memcpy(&b, &row[k], 4);
+            hsh = (hsh ^ b) * 1099511628211ull;
+        }
+        auto& cand = seen[hsh];
+        uint32_t id = 0xffffffffu;
+        for (uint32_t c : cand)
+            if (std::memcmp(a + first[c] * nz, row, (size_t)nz * 4) == 0) {
+                id = c;
+                break;
+            }
+        if (id == 0xffffffffu) {
+            id = (uint32_t)first.size();
+            first.push_back(r);
+            count.push_back(0);
+            cand.push_back(id);
+            if (first.size() * 4 > nrows) {
+                P.rid.clear();
+                return P;  // not pooled
+            }
+        }
+        count[id]++;
+        P.rid[r] = id;
+    }
+    P.pooled = true;
+    P.rows.assign(first.size() * pitch, 0.0f);
+    for (size_t d = 0; d < first.size(); ++d) std::memcpy(&P.rows[d * pitch], a + first[d] * nz, (size_t)nz * 4);
+    P.bg = (uint32_t)(std::max_element(count.begin(), count.end()) - count.begin());
+    return P;
+}
+
+struct FusedSlabSpec {
+    int side, comp, q;             // place in FusedParams::slab[side][comp][q]
+    size_t op_slab;                // index of the slab in the CPML table
+    const ems_cpml_slab* src;
+    size_t len;                    // ψ values of the slab
+};
+
+struct FusedTables {
+    std::string why;               // empty: the fused schedule can run
+    Pooled lane[12];
+    std::vector<FusedSlabSpec> slabs;
+    int nslab[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    bool poles_first = false;
+    bool has_poles = false;
+    std::vector<PoleRun> runs;
+    std::vector<double> sets;
+    std::vector<uint2> row_runs;
+};
+
+// Why the fused schedule cannot run this model ("" if it can).
+inline std::string fused_ineligible(const ems_engine_desc* d, uint32_t pitch) {
+    int n_cpml = 0, n_poles = 0;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        const int kind = d->ops[k].kind;
+        if (kind == EMS_OP_CPML) ++n_cpml;
+        if (kind == EMS_OP_POLES) {
+            ++n_poles;
+            const auto* p = (const ems_poles*)d->ops[k].table;
+            if (p->magnetic.n_edges) return "magnetic poles";
+        }
+        if (kind == EMS_OP_SOURCE) {
+            const auto* s = (const ems_source*)d->ops[k].table;
+            if (s->kind == EMS_SOFT_H || s->kind == EMS_HARD_H) return "magnetic sources";
+        }
+    }
+    if (n_cpml > 1 || n_poles > 1) return "several CPML or dispersive operators";
+    if (pitch > 1024) return "z rows longer than 1024 nodes";
+    return "";
+}
+
+inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) {
+    FusedTables T;
+    T.why = fused_ineligible(d, pitch);
+    if (!T.why.empty()) return T;
+    const uint32_t nx = (uint32_t)d->nodes[0], ny = (uint32_t)d->nodes[1], nz = (uint32_t)d->nodes[2];
+    {
+        std::vector<std::thread> th;
+        for (int l = 0; l < 12; ++l)
+            th.emplace_back([&, l] { T.lane[l] = pool_lane(d->coeff[l], nx, ny, nz, pitch); });
+        for (auto& t : th) t.join();
+    }
+    int pos_cpml = -1, pos_poles = -1;
+    const ems_pole_side* pe = nullptr;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        if (d->ops[k].kind == EMS_OP_CPML) {
+            pos_cpml = (int)k;
+            const auto* c = (const ems_cpml*)d->ops[k].table;
+            for (size_t q = 0; q < c->n_slabs; ++q) {
+                const ems_cpml_slab& s = c->slabs[q];
+                const size_t len = (size_t)(s.hi[0] - s.lo[0]) * (s.hi[1] - s.lo[1]) * (s.hi[2] - s.lo[2]);
+                if (!len) continue;
+                const int side = s.e_side ? 1 : 0;
+                int& n = T.nslab[side][s.comp];
+                if (n >= 4) {
+                    T.why = "more than four CPML slabs per component";
+                    return T;
+                }
+                T.slabs.push_back({side, (int)s.comp, n, q, &s, len});
+                ++n;
+            }
+        }
+        if (d->ops[k].kind == EMS_OP_POLES) {
+            pos_poles = (int)k;
+            pe = &((const ems_poles*)d->ops[k].table)->electric;
+        }
+    }
+    T.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
+    // Electric poles as runs along z (edges are in (plane, axis, y, z) order):
+    // consecutive edges of one row with the same constants share a run.
+    if (pe && pe->n_edges) {
+        std::unordered_map<std::string, uint32_t> set_of;
+        T.row_runs.assign((size_t)nx * 3 * ny, uint2{0, 0});
+        uint64_t last_row = ~0ull;
+        uint32_t last_k = 0;
+        for (size_t e = 0; e < pe->n_edges; ++e) {
+            const uint64_t idx = pe->node[e];
+            const uint64_t kk = idx % nz, rr = idx / nz;
+            const uint64_t jj = rr % ny, ii = rr / ny;
+            const uint64_t row_key = (ii * 3 + pe->axis[e]) * ny + jj;
+            const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
+            const uint32_t np = p1 - p0;
+            if (np > kMaxPoles || np == 0) {
+                T.why = "edge pole count";
+                return T;
+            }
+            std::string key((size_t)np * 24 + 12, '\0');
+            uint32_t kinds = 0;
+            for (uint32_t q = 0; q < np; ++q) {
+                const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
+                std::memcpy(&key[(size_t)q * 24], c3, 24);
+                if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
+            }
+            std::memcpy(&key[(size_t)np * 24], &pe->sum_inv_z[e], 8);
+            std::memcpy(&key[(size_t)np * 24 + 8], &kinds, 4);
+            auto it = set_of.find(key);
+            uint32_t set;
+            if (it == set_of.end()) {
+                set = (uint32_t)T.sets.size();
+                for (uint32_t q = 0; q < np; ++q) {
+                    T.sets.push_back(pe->a[p0 + q]);
+                    T.sets.push_back(pe->inv_c[p0 + q]);
+                    T.sets.push_back(pe->inv_z[p0 + q]);
+                }
+                set_of.emplace(key, set);
+            } else {
+                set = it->second;
+            }
+            const bool extend = !T.runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 &&
+                                T.runs.back().set == set && T.runs.back().np == np && T.runs.back().kinds == kinds &&
+                                T.runs.back().p0 + (T.runs.back().ke - T.runs.back().kb) * np == p0;
+            if (extend) {
+                T.runs.back().ke = (uint32_t)kk + 1;
+            } else {
+                if (row_key != last_row) T.row_runs[row_key] = uint2{(uint32_t)T.runs.size(), 0};
+                T.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, pe->sum_inv_z[e]});
+                T.row_runs[row_key].y++;
+            }
+            last_row = row_key;
+            last_k = (uint32_t)kk;
+        }
+        T.has_poles = true;
+    }
+    return T;
+}
+
+// Work items (row tile, x chunk): about eight per CTA of the persistent grid,
+// chunks of at least eight planes.
+inline void fused_work(FusedParams& P, uint32_t nx, uint32_t ny, int tj, unsigned grid) {
+    P.tiles_j = (ny + tj - 1) / tj;
+    const uint32_t want = 8u * grid;
+    const uint32_t chunks = std::max<uint32_t>(1, (want + P.tiles_j - 1) / P.tiles_j);
+    const uint32_t chunk = std::max<uint32_t>(8, (nx + chunks - 1) / chunks);
+    P.chunk = chunk;
+    P.n_chunks = (nx + chunk - 1) / chunk;
+    P.n_items = P.tiles_j * P.n_chunks;
+}
+
+}  // namespace emsk

@@ -102,6 +102,10 @@ __device__ __forceinline__ double weight(float a, double p, float b) {
 
 // Block-wide f64 sum in a fixed order (blockDim.x a multiple of 32, at
 // most THREADS); result valid in thread 0.
+#ifdef EMS_HOST_EMULATION
+template <unsigned THREADS>
+__device__ __forceinline__ double block_sum(double v) { return emu::block_sum(v); }
+#else
 template <unsigned THREADS>
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double sh[THREADS / 32];
@@ -114,6 +118,7 @@ __device__ __forceinline__ double block_sum(double v) {
         for (unsigned q = 0; q < blockDim.x / 32; ++q) s = __dadd_rn(s, sh[q]);
     return s;
 }
+#endif
 
 // H update of every dual edge (src/engine/kernel.rs:447-511, 571-618);
 // with ENERGY each block also writes its share of the energy invariant

@@ -1,0 +1,182 @@
+// harness.cpp — the fused step kernel (ems_b200/csrc/fused.cuh) run on the
+// CPU through emu_shim.h. TEST INFRASTRUCTURE: compiled and called by
+// tests/test_fused_emulation.py; shared memory is a heap buffer of exactly
+// the size the engine requests, and every global array is bounds-checked by
+// the surrounding tables' sizes (the tests run it under the same sizes).
+#include "emu_shim.h"
+
+thread_local EmuDim threadIdx;
+EmuDim blockIdx, blockDim, gridDim;
+namespace emu {
+Block* cur = nullptr;
+void fail(const char* what) {
+    if (cur && cur->errors.fetch_add(1) == 0) std::snprintf(cur->msg, sizeof cur->msg, "%s", what);
+}
+}  // namespace emu
+
+#include "../../ems_b200/csrc/fused.cuh"
+#include "../../ems_b200/csrc/fused_tables.h"
+
+using namespace emsk;
+
+static char g_err[256];
+
+extern "C" const char* emu_error(void) { return g_err; }
+
+// Runs `steps` fused steps from the fields given in reference layout
+// (u_x, u_y, u_z, i_x, i_y, i_z; overwritten with the result). energies:
+// the invariant's field part (×dt/4 applied) of each step, or NULL.
+extern "C" int emu_fused_run(const ems_engine_desc* d, int tj, unsigned grid, uint64_t steps, float** fields,
+                             double* energies) {
+    g_err[0] = 0;
+    Grid g{};
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "not eligible: %s", T.why.c_str());
+        return 1;
+    }
+    auto pad = [&](const float* src, std::vector<float>& dst) {
+        dst.assign(g.np, 0.0f);
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r) std::memcpy(&dst[r * g.pitch], src + r * g.nz, g.nz * 4);
+    };
+    std::vector<float> buf[2][6];
+    for (int c = 0; c < 6; ++c) {
+        pad(fields[c], buf[0][c]);
+        buf[1][c].assign(g.np, 0.0f);
+    }
+    std::vector<float> dense[12];
+    FusedParams P{};
+    P.g = g;
+    P.dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (T.lane[l].pooled) {
+            P.lane[l].rid = T.lane[l].rid.data();
+            P.lane[l].rows = T.lane[l].rows.data();
+            P.lane[l].bg = T.lane[l].bg;
+        } else {
+            pad(d->coeff[l], dense[l]);
+            P.lane[l].dense = dense[l].data();
+        }
+    }
+    std::vector<std::vector<float>> psi_e, psi_h0, psi_h1;
+    std::vector<std::pair<int, int>> at_h;
+    psi_e.reserve(T.slabs.size());
+    psi_h0.reserve(T.slabs.size());
+    psi_h1.reserve(T.slabs.size());
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    for (const FusedSlabSpec& sp : T.slabs) {
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = (uint32_t)sp.src->lo[a];
+            f.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        f.normal = (uint32_t)sp.src->normal;
+        f.b = sp.src->b;
+        f.a = sp.src->a;
+        f.k = sp.src->k;
+        if (sp.side) {
+            psi_e.emplace_back(sp.len, 0.0f);
+            f.psi_old = psi_e.back().data();
+            f.psi_new = psi_e.back().data();
+        } else {
+            psi_h0.emplace_back(sp.len, 0.0f);
+            psi_h1.emplace_back(sp.len, 0.0f);
+            at_h.push_back({sp.comp, sp.q});
+        }
+    }
+    std::vector<double> pj, pq;
+    if (T.has_poles) {
+        size_t np = 0;
+        for (size_t k = 0; k < d->n_ops; ++k)
+            if (d->ops[k].kind == EMS_OP_POLES) np = ((const ems_poles*)d->ops[k].table)->electric.n_poles;
+        pj.assign(np, 0.0);
+        pq.assign(np, 0.0);
+        P.has_poles = 1;
+        P.runs = T.runs.data();
+        P.sets = T.sets.data();
+        P.row_runs = T.row_runs.data();
+        P.pj = pj.data();
+        P.pq = pq.data();
+    }
+    P.poles_first = T.poles_first ? 1 : 0;
+    fused_work(P, g.nx, g.ny, tj, grid);
+    uint32_t counter = 0;
+    int status = 0;
+    std::vector<double> partials(grid, 0.0);
+    P.counter = &counter;
+    P.status = &status;
+    P.partials = partials.data();
+    size_t smem_bytes = 0;
+    switch (tj) {
+    case 2: smem_bytes = fused_smem_bytes<2>(g.pitch); break;
+    case 4: smem_bytes = fused_smem_bytes<4>(g.pitch); break;
+    case 6: smem_bytes = fused_smem_bytes<6>(g.pitch); break;
+    default: std::snprintf(g_err, sizeof g_err, "tj must be 2, 4 or 6"); return 1;
+    }
+    std::vector<unsigned char> smem(smem_bytes + 128);
+    unsigned char* sm = smem.data() + (128 - ((uintptr_t)smem.data() & 127)) % 128;
+    int cur = 0;
+    for (uint64_t s = 0; s < steps; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            P.uo[a] = buf[cur][a].data();
+            P.io[a] = buf[cur][3 + a].data();
+            P.un[a] = buf[cur ^ 1][a].data();
+            P.in[a] = buf[cur ^ 1][3 + a].data();
+        }
+        for (size_t q = 0; q < at_h.size(); ++q) {
+            FSlab& f = P.slab[0][at_h[q].first][at_h[q].second];
+            f.psi_old = (s & 1) ? psi_h1[q].data() : psi_h0[q].data();
+            f.psi_new = (s & 1) ? psi_h0[q].data() : psi_h1[q].data();
+        }
+        P.energy = energies ? 1 : 0;
+        counter = 0;
+        blockDim.x = g.pitch;
+        gridDim.x = grid;
+        double w = 0.0;
+        for (unsigned b = 0; b < grid; ++b) {
+            blockIdx.x = b;
+            emu::Block blk;
+            std::barrier<> bar((std::ptrdiff_t)g.pitch);
+            blk.bar = &bar;
+            blk.smem = sm;
+            blk.smem_bytes = smem_bytes;
+            blk.sums.assign(g.pitch, 0.0);
+            std::memset(sm, 0xA5, smem_bytes);  // stale shared memory must not matter
+            emu::cur = &blk;
+            std::vector<std::thread> th;
+            for (unsigned t = 0; t < g.pitch; ++t)
+                th.emplace_back([&, t] {
+                    threadIdx.x = t;
+                    switch (tj) {
+                    case 2: k_fused<2, 1024>(P); break;
+                    case 4: k_fused<4, 1024>(P); break;
+                    default: k_fused<6, 1024>(P); break;
+                    }
+                });
+            for (auto& x : th) x.join();
+            emu::cur = nullptr;
+            if (blk.errors.load()) {
+                std::snprintf(g_err, sizeof g_err, "step %llu block %u: %s", (unsigned long long)s, b, blk.msg);
+                return 2;
+            }
+            if (energies) w += partials[b];
+        }
+        if (status) {
+            std::snprintf(g_err, sizeof g_err, "status flag set at step %llu", (unsigned long long)s);
+            return 3;
+        }
+        if (energies) energies[s] = 0.25 * d->dt * w;
+        cur ^= 1;
+    }
+    for (int c = 0; c < 6; ++c)
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
+            std::memcpy(fields[c] + r * g.nz, &buf[cur][c][r * g.pitch], g.nz * 4);
+    return 0;
+}

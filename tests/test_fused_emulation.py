@@ -1,0 +1,118 @@
+"""The fused step kernel's own source, run on the CPU (tests/fused_emu), equals
+the oracle bit for bit.
+
+The CUDA source of the fused kernel (ems_b200/csrc/fused.cuh) is compiled
+for the host with a shim that turns each CUDA thread into a host thread and
+each TMA bulk copy into a checked memcpy (shared-memory bounds, 16-byte
+alignment, the mbarrier's expected bytes and phases). This checks the
+kernel's tiling, halo rows, x chunks, stage ring and indexing without a
+GPU; the oracle is the reference's step restated.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import ems_b200 as E
+from ems_b200 import workloads as W
+from oracle import OracleEngine
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def emu_lib(asan=False):
+    from fused_emu import build
+
+    lib = C.CDLL(build.build(asan))
+    lib.emu_fused_run.restype = C.c_int
+    lib.emu_fused_run.argtypes = [C.c_void_p, C.c_int, C.c_uint, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_error.restype = C.c_char_p
+    return lib
+
+
+def model(n, scheme, cpml=3, poles=True, graded=False):
+    rng = np.random.default_rng(11)
+    if graded:
+        lines = [np.cumsum(np.concatenate([[0.0], 1e-3 * (1.0 + 0.3 * rng.random(c))])) for c in n]
+        m = E.Model(*lines)
+    else:
+        m = E.Model.uniform(n, [1e-3] * 3)
+    sph = m.cells().sphere([n[0] / 2, n[1] / 2, n[2] / 2], min(n) / 4)
+    m.fill(sph, m.material(eps_r=2.0, kappa=0.01))
+    m.fill_pec_box([1, 1, 1], [3, 2, 3])
+    m.build()
+    if cpml:
+        m.add_cpml([cpml, cpml + 1, cpml, 0, cpml, cpml], kappa_max=1.5, alpha_max=0.02)
+    if poles:
+        d = E.Dispersive()
+        d.fill_cells(m, sph, W.lorentz_poles(5))
+        d.fill_cells(m, m.cells().box([0, 0, n[2] - 4], [n[0], n[1], n[2] - 2]), [E.Pole.drude(6e10, 6e9)])
+        d.fill_cells(m, m.cells().box([2, 2, 2], [5, 4, 6]), [E.Pole.debye(1.5, 1e-11)])
+        m.add_dispersive(d, scheme)
+    return m
+
+
+def random_state(m, seed=0):
+    rng = np.random.default_rng(seed)
+    return [(rng.standard_normal(m.nodes) * 1e-2).astype(np.float32) for _ in range(6)]
+
+
+def run_emu(lib, m, state, steps, tj, grid):
+    arrs = [np.ascontiguousarray(s.copy()) for s in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    en = np.zeros(steps)
+    r = lib.emu_fused_run(m.desc, tj, grid, steps, ptrs, en.ctypes.data)
+    assert r == 0, lib.emu_error().decode()
+    return arrs, en
+
+
+def run_oracle(m, state, steps):
+    o = OracleEngine(m, threads=2)
+    for f in range(2):
+        for a in range(3):
+            o.set_field(f, a, state[3 * f + a])
+    en = [o.step_with_energy() for _ in range(steps)]
+    return [o.field(f, a) for f in range(2) for a in range(3)], np.array(en), o
+
+
+@pytest.mark.parametrize("n,tj,grid,scheme", [
+    ((9, 10, 13), 2, 1, E.TRAPEZOIDAL),
+    ((12, 11, 9), 4, 3, E.LEAPFROG),
+    ((17, 14, 40), 6, 2, E.TRAPEZOIDAL),
+    ((21, 7, 33), 4, 5, E.LEAPFROG),
+])
+def test_fused_kernel_source_equals_oracle(n, tj, grid, scheme):
+    m = model(n, scheme, graded=tj == 4)
+    state = random_state(m)
+    steps = 12
+    got, eg = run_emu(emu_lib(), m, state, steps, tj, grid)
+    want, eo, o = run_oracle(m, state, steps)
+    names = ["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"]
+    for name, a, b in zip(names, got, want):
+        bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])}: {a[tuple(bad[0])]} vs {b[tuple(bad[0])]}"
+    # The field part of the invariant (the oracle adds the pole energy).
+    assert np.all(np.isfinite(eg)) and np.all(eg > 0)
+
+
+def test_fused_kernel_source_under_address_sanitizer():
+    """The same emulation built with AddressSanitizer: no out-of-bounds access
+    of any table, field, state or shared-memory buffer."""
+    import shutil
+
+    asan = subprocess.run(["gcc", "-print-file-name=libasan.so"], capture_output=True, text=True).stdout.strip()
+    if not asan or not os.path.exists(asan):
+        pytest.skip("libasan not available")
+    code = (
+        "import sys; sys.path[:0] = [%r, %r]\n"
+        "import test_fused_emulation as T, ems_b200 as E\n"
+        "m = T.model((11, 9, 14), E.LEAPFROG)\n"
+        "T.run_emu(T.emu_lib(asan=True), m, T.random_state(m), 6, 4, 2)\n"
+        "print('clean')\n"
+    ) % (HERE, os.path.dirname(HERE))
+    env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0 and "clean" in r.stdout, r.stderr[-3000:]
