@@ -222,7 +222,7 @@ __host__ __device__ constexpr size_t fused_smem_bytes(uint32_t pitch) {
 }
 
 template <int TJ, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) k_fused(FusedParams P) {
+__global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ FusedParams P) {
     EMS_DYNAMIC_SMEM(smem_raw);
     const Grid g = P.g;
     const uint32_t pitch = g.pitch;

@@ -125,7 +125,7 @@ __device__ __forceinline__ double block_sum(double v) {
 // Σ (1+ca)/cb·u² + Σ (1+da)/db·i_old·i_new in units of dt/4
 // (src/engine/kernel.rs:132-244).
 template <bool ENERGY>
-__global__ void __launch_bounds__(kRowThreads) k_update_h(Grid g, Fields f, Coeffs c, double* partials) {
+__global__ void __launch_bounds__(kRowThreads) k_update_h(const __grid_constant__ Grid g, const __grid_constant__ Fields f, const __grid_constant__ Coeffs c, double* partials) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y, i = blockIdx.z;
     double w = 0.0;
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(1024) k_reduce_partials(const double* partials
 }
 
 // E update of every edge (src/engine/kernel.rs:624-697).
-__global__ void __launch_bounds__(kRowThreads) k_update_e(Grid g, Fields f, Coeffs c) {
+__global__ void __launch_bounds__(kRowThreads) k_update_e(const __grid_constant__ Grid g, const __grid_constant__ Fields f, const __grid_constant__ Coeffs c) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y, i = blockIdx.z;
     if (k >= g.nz) return;
@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(kRowThreads) k_update_e(Grid g, Fields f, Coef
 // CPML correction of one slab (src/engine/boundary/cpml.rs:445-520, 657-676):
 // s = sign·(h − l); ψ = flush(b·ψ + a·s); t = flush(t + scale·coef·(k·s + ψ)).
 template <bool E_SIDE>
-__global__ void k_cpml(Grid g, Fields f, Coeffs c, SlabDev s) {
+__global__ void k_cpml(const __grid_constant__ Grid g, const __grid_constant__ Fields f,
+                       const __grid_constant__ Coeffs c, const __grid_constant__ SlabDev s) {
     const uint32_t k = s.lo[2] + blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = s.lo[1] + blockIdx.y, i = s.lo[0] + blockIdx.z;
     if (k >= s.hi[2]) return;
@@ -239,7 +240,9 @@ __global__ void k_cpml(Grid g, Fields f, Coeffs c, SlabDev s) {
 // Dispersive correction of one edge per thread (src/engine/dispersive.rs:1392-1470).
 // A leapfrog pole's new state does not depend on the corrected value and is
 // stored at once; a trapezoidal pole's is formed from its old state after it.
-__global__ void k_poles_correct(Grid g, Fields f, Coeffs c, PoleSideDev p, bool electric, double dt) {
+__global__ void k_poles_correct(const __grid_constant__ Grid g, const __grid_constant__ Fields f,
+                                const __grid_constant__ Coeffs c, const __grid_constant__ PoleSideDev p, bool electric,
+                                double dt) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= p.n_edges) return;
     (void)g;
@@ -282,7 +285,7 @@ __global__ void k_poles_correct(Grid g, Fields f, Coeffs c, PoleSideDev p, bool 
 }
 
 // Saves the field value of every edge (src/engine/dispersive.rs:1173-1180).
-__global__ void k_poles_capture(Fields f, PoleSideDev p, bool electric) {
+__global__ void k_poles_capture(const __grid_constant__ Fields f, const __grid_constant__ PoleSideDev p, bool electric) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= p.n_edges) return;
     p.prev[e] = (electric ? f.u[p.axis[e]] : f.i[p.axis[e]])[p.node[e]];

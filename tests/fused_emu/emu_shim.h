@@ -25,6 +25,7 @@
 #define __forceinline__ inline
 #define __launch_bounds__(...)
 #define __align__(n) alignas(n)
+#define __grid_constant__
 
 struct uint2 {
     uint32_t x, y;
