@@ -525,12 +525,12 @@ class Engine:
         return n.value
 
     def set_schedule(self, s: int) -> None:
-        """0: automatic (fused where the model allows it), 1: separate H and E kernels."""
+        """0 automatic, 1 per-operator kernels, 2 fused single pass, 3 two kernels."""
         self._ck(self._lib.ems_gpu_set_schedule(self._h, s))
 
     @property
     def schedule(self) -> int:
-        """The schedule steps run with: 1 separate kernels, 2 fused kernel."""
+        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels."""
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value

@@ -29,6 +29,7 @@
 #include "kernels.cuh"
 #include "fused.cuh"
 #include "fused_tables.h"
+#include "separate.cuh"
 
 #include <thread>
 #include <unordered_map>
@@ -108,7 +109,11 @@ struct ems_gpu {
     std::vector<Op> ops;
     // ---- the fused single-pass schedule
     bool fused_ok = false;
+    bool tables_ok = false;         // the table-driven two-kernel schedule can run
     std::string fused_why;          // why the fused schedule is unavailable
+    std::string tables_why;         // why the two-kernel schedule is unavailable
+    double* spartials = nullptr;    // energy shares of the two-kernel H update
+    size_t n_spartials = 0;
     int fused_tj = 0;
     void (*fused_launch)(const emsk::FusedParams&, unsigned, unsigned, size_t, cudaStream_t) = nullptr;
     size_t fused_smem = 0;
@@ -293,25 +298,16 @@ bool try_tj(ems_gpu* h, int max_smem) {
     return true;
 }
 
-// Builds the fused schedule's tables (fused_tables.h) and uploads them;
-// leaves fused_ok false, with the reason, where the model needs the
-// separate kernels.
+// Builds the tables of the table-driven schedules (fused_tables.h) and
+// uploads them: the two-kernel schedule runs every model whose CPML and
+// dispersive operators are single; the fused kernel in addition needs no
+// magnetic poles, no magnetic sources and shared memory for its tile.
 ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
     const Grid& g = h->g;
-    h->fused_why = fused_ineligible(d, g.pitch);
-    if (!h->fused_why.empty()) return EMS_OK;
-    int max_smem = 0;
-    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    if (!(try_tj<6, 576>(h, max_smem) || try_tj<4, 576>(h, max_smem) || try_tj<2, 576>(h, max_smem) ||
-          try_tj<4, 1024>(h, max_smem) || try_tj<2, 1024>(h, max_smem))) {
-        h->fused_why = "shared memory";
-        return EMS_OK;
-    }
     FusedTables T = build_fused_tables(d, g.pitch);
-    if (!T.why.empty()) {
-        h->fused_why = T.why;
-        return EMS_OK;
-    }
+    h->tables_why = T.why;
+    h->fused_why = T.why.empty() ? T.fused_why : T.why;
+    if (!T.why.empty()) return EMS_OK;
     FusedParams& P = h->fp;
     P = FusedParams{};
     P.g = g;
@@ -327,7 +323,8 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
             P.lane[l].dense = h->co[l];
         }
     }
-    // CPML slabs: the engine's device copies (b, a, k, ψ), in the tables' order.
+    // CPML slabs: the engine's device copies (b, a, k, ψ), in the tables' order
+    // (both keep the non-empty slabs of the table in order).
     const std::vector<SlabDev>* dev_slabs = nullptr;
     for (auto& op : h->ops)
         if (op.kind == EMS_OP_CPML) dev_slabs = &op.cpml;
@@ -335,7 +332,6 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
     size_t q_dev = 0;
     for (const FusedSlabSpec& sp : T.slabs) {
-        // The engine keeps the non-empty slabs of the table in order too.
         const SlabDev& sd = (*dev_slabs)[q_dev++];
         FSlab& f = P.slab[sp.side][sp.comp][sp.q];
         for (int a = 0; a < 3; ++a) {
@@ -349,24 +345,57 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         f.psi_old = sd.psi;
         f.psi_new = sd.psi;
         if (!sp.side) {
-            float* other = h->alloc<float>(sp.len);
-            if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
-            h->psi_h.push_back({sd.psi, other});
+            h->psi_h.push_back({sd.psi, nullptr});
             h->psi_h_at.push_back({sp.comp, sp.q});
         }
     }
     P.poles_first = T.poles_first ? 1 : 0;
+    PoleSideDev* pe_dev = nullptr;
+    PoleSideDev* ph_dev = nullptr;
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_POLES) {
+            pe_dev = &op.poles.e;
+            ph_dev = &op.poles.h;
+        }
     if (T.has_poles) {
         P.has_poles = 1;
         P.runs = h->upload(T.runs.data(), T.runs.size());
         P.sets = h->upload(T.sets.data(), T.sets.size());
         P.row_runs = h->upload(T.row_runs.data(), T.row_runs.size());
-        for (auto& op : h->ops)
-            if (op.kind == EMS_OP_POLES) {
-                P.pj = op.poles.e.j;
-                P.pq = op.poles.e.q;
-            }
+        P.pj = pe_dev->j;
+        P.pq = pe_dev->q;
         if (!P.runs || !P.sets || !P.row_runs) return fail(h, EMS_ERR_NOMEM, "pole runs");
+    }
+    if (T.has_poles_h) {
+        P.has_poles_h = 1;
+        P.runs_h = h->upload(T.h.runs.data(), T.h.runs.size());
+        P.sets_h = h->upload(T.h.sets.data(), T.h.sets.size());
+        P.row_runs_h = h->upload(T.h.row_runs.data(), T.h.row_runs.size());
+        P.pj_h = ph_dev->j;
+        P.pq_h = ph_dev->q;
+        P.prev_h = ph_dev->prev;
+        if (!P.runs_h || !P.sets_h || !P.row_runs_h) return fail(h, EMS_ERR_NOMEM, "pole runs");
+    }
+    h->n_spartials = (size_t)blocks_for(g.nz, kSepK) * blocks_for(g.ny, kSepJ) * g.nx;
+    h->spartials = h->alloc<double>(h->n_spartials);
+    if (!h->spartials) return fail(h, EMS_ERR_NOMEM, "energy shares");
+    h->tables_ok = true;
+    // The fused kernel.
+    if (!h->fused_why.empty()) return EMS_OK;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (!(try_tj<6, 576>(h, max_smem) || try_tj<4, 576>(h, max_smem) || try_tj<2, 576>(h, max_smem) ||
+          try_tj<4, 1024>(h, max_smem) || try_tj<2, 1024>(h, max_smem))) {
+        h->fused_why = "shared memory";
+        return EMS_OK;
+    }
+    for (size_t q = 0; q < T.slabs.size(); ++q) (void)q;
+    size_t qh = 0;
+    for (const FusedSlabSpec& sp : T.slabs) {
+        if (sp.side) continue;
+        float* other = h->alloc<float>(sp.len);
+        if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
+        h->psi_h[qh++].second = other;
     }
     fused_work(P, g.nx, g.ny, h->fused_tj, h->fused_grid);
     h->counter = h->alloc<uint32_t>(1);
@@ -385,7 +414,17 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
     return EMS_OK;
 }
 
-bool use_fused(const ems_gpu* h) { return h->fused_ok && h->schedule != 1; }
+// The schedule a step runs: 2 fused, 3 two kernels, 1 the per-operator kernels.
+int active_schedule(const ems_gpu* h) {
+    switch (h->schedule) {
+    case 1: return 1;
+    case 2: return h->fused_ok ? 2 : (h->tables_ok ? 3 : 1);
+    case 3: return h->tables_ok ? 3 : 1;
+    default: return h->fused_ok ? 2 : (h->tables_ok ? 3 : 1);
+    }
+}
+
+bool use_fused(const ems_gpu* h) { return active_schedule(h) == 2; }
 
 ems_status serial_post_h(ems_gpu* h, const Fields& f);
 ems_status serial_pre_e(ems_gpu* h, const Fields& f);
@@ -434,10 +473,61 @@ ems_status run_step_fused(ems_gpu* h, bool energy) {
     return EMS_OK;
 }
 
-// One step through the separate-kernel schedule; energy: record the
+// One step through the two-kernel schedule (separate.cuh), in place.
+ems_status run_step_two(ems_gpu* h, bool energy) {
+    cudaStream_t s = h->stream;
+    const Grid& g = h->g;
+    Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    FusedParams P = h->fp;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = P.un[a] = h->u[a];
+        P.io[a] = P.in[a] = h->i[a];
+    }
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        fs.psi_old = fs.psi_new = h->psi_h[q].first;
+    }
+    P.partials = h->spartials;
+    dim3 blk(kSepK, kSepJ, 1);
+    dim3 grd(blocks_for(g.nz, kSepK), blocks_for(g.ny, kSepJ), g.nx);
+    cudaEvent_t ev = h->prof_begin();
+    if (energy) {
+        k_step_h<true><<<grd, blk, 0, s>>>(P);
+    } else {
+        k_step_h<false><<<grd, blk, 0, s>>>(P);
+    }
+    h->prof_end(0, ev);
+    ++h->launches;
+    if (energy) {
+        k_reduce_partials<<<1, 1024, 0, s>>>(h->spartials, h->n_spartials, h->d_energy);
+        ++h->launches;
+    }
+    ems_status st = serial_post_h(h, f);
+    if (st) return st;
+    st = serial_pre_e(h, f);
+    if (st) return st;
+    ev = h->prof_begin();
+    k_step_e<<<grd, blk, 0, s>>>(P);
+    h->prof_end(1, ev);
+    ++h->launches;
+    // Magnetic-pole edges save i^{n+1/2} after the E update (src/engine/dispersive.rs:1730-1744).
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_POLES && op.poles.h.n_edges) {
+            k_poles_capture<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, op.poles.h, false);
+            ++h->launches;
+        }
+    st = serial_post_e(h, f);
+    if (st) return st;
+    ++h->step;
+    return EMS_OK;
+}
+
+// One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
-    if (use_fused(h)) return run_step_fused(h, energy);
+    const int sch = active_schedule(h);
+    if (sch == 2) return run_step_fused(h, energy);
+    if (sch == 3) return run_step_two(h, energy);
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
@@ -973,14 +1063,16 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 1) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 3) return EMS_ERR_INVALID;
+    if (schedule == 2 && !h->fused_ok) return fail(h, EMS_ERR_INVALID, "fused schedule unavailable: " + h->fused_why);
+    if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
     h->schedule = schedule;
     return EMS_OK;
 }
 
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {
     if (!h || !active) return EMS_ERR_INVALID;
-    *active = use_fused(h) ? 2 : 1;
+    *active = active_schedule(h);
     return EMS_OK;
 }
 

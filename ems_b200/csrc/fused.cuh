@@ -52,6 +52,8 @@ struct PoleRun {
     uint32_t set;      // offset of the run's constants (np poles × {a, inv_c, inv_z})
     uint32_t np;       // poles per edge
     uint32_t kinds;    // bit q set: pole q is a leapfrog pole
+    uint32_t e0;       // edge index of the run's first edge (in the side's table)
+    uint32_t pad;
     double sum_inv_z;
 };
 
@@ -70,6 +72,13 @@ struct FusedParams {
     double* pj;
     double* pq;
     int has_poles;
+    const uint2* row_runs_h; // magnetic poles (two-kernel schedule only)
+    const PoleRun* runs_h;
+    const double* sets_h;
+    double* pj_h;
+    double* pq_h;
+    const float* prev_h;   // saved i^{n−½} of each magnetic-pole edge
+    int has_poles_h;
     int poles_first;       // the dispersive medium was registered before the CPML
     double dt;
     uint32_t tiles_j, chunk, n_chunks, n_items;
@@ -146,8 +155,8 @@ __device__ __forceinline__ void fence_mbar_init() {}
 // contains the node, in order: ψ = flush(b·ψ + a·s), t = flush(t + coef·(k·s + ψ)),
 // s the derivative term along the slab's normal (sA along next(c), sB along prev(c)).
 template <bool WRITE>
-__device__ __forceinline__ float cpml_apply(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c,
-                                            float t, float coef, float sA, float sB) {
+__device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c, float t,
+                                        float coef, float sA, float sB) {
     const int na = (c + 1) % 3;
     for (int q = 0; q < n; ++q) {
         const FSlab& s = list[q];
@@ -162,28 +171,49 @@ __device__ __forceinline__ float cpml_apply(const FSlab* list, int n, uint32_t i
     return t;
 }
 
+// Whether any slab of `list` contains the node (inline; the correction itself
+// is out of line, as most nodes lie in no layer).
+__device__ __forceinline__ bool in_slabs(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k) {
+    bool in = false;
+    for (int q = 0; q < n; ++q) {
+        const FSlab& s = list[q];
+        in |= i >= s.lo[0] && i < s.hi[0] && j >= s.lo[1] && j < s.hi[1] && k >= s.lo[2] && k < s.hi[2];
+    }
+    return in;
+}
+
+template <bool WRITE>
+__device__ __forceinline__ float cpml_apply(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c,
+                                            float t, float coef, float sA, float sB) {
+    if (n == 0 || !in_slabs(list, n, i, j, k)) return t;
+    return cpml_body<WRITE>(list, n, i, j, k, c, t, coef, sA, sB);
+}
+
 // Electric-pole correction of the E edge (axis a, row (i, j), node k)
 // (src/engine/dispersive.rs:1392-1470), if the edge has poles. A leapfrog
 // pole's new state does not depend on the corrected voltage and is stored
 // at once; a trapezoidal pole's is formed from its old state after it.
-__device__ __forceinline__ float poles_apply(const FusedParams& P, const uint2 rr, uint32_t k, float u_star,
-                                             float prev_f, float cb_f) {
+__device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets, double* pj, double* pq, double dt,
+                                        const uint2 rr, uint32_t k, float u_star, float prev_f, float cb_f,
+                                        const float* prev_arr) {
     for (uint32_t q = 0; q < rr.y; ++q) {
-        const PoleRun R = P.runs[rr.x + q];
+        const PoleRun R = runs[rr.x + q];
         if (k < R.kb || k >= R.ke) continue;
         const uint32_t p0 = R.p0 + (k - R.kb) * R.np;
-        const double* cs = P.sets + R.set;
+        const double* cs = sets + R.set;
         const double cb = (double)cb_f;
-        const double prev = (double)prev_f;
+        // The field value the update starts from: the one given, or the
+        // edge's saved value (magnetic poles, src/engine/dispersive.rs:1173).
+        const double prev = (double)(prev_arr ? prev_arr[R.e0 + (k - R.kb)] : prev_f);
         const double half_prev = __dmul_rn(0.5, prev);
         double s = 0.0;
         for (uint32_t p = 0; p < R.np; ++p) {
             const double a = cs[3 * p], ic = cs[3 * p + 1], iz = cs[3 * p + 2];
-            const double jq = P.pj[p0 + p], qq = P.pq[p0 + p];
+            const double jq = pj[p0 + p], qq = pq[p0 + p];
             if ((R.kinds >> p) & 1u) {
                 const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
-                P.pj[p0 + p] = jn;
-                P.pq[p0 + p] = __dadd_rn(qq, __dmul_rn(P.dt, jn));
+                pj[p0 + p] = jn;
+                pq[p0 + p] = __dadd_rn(qq, __dmul_rn(dt, jn));
                 s = __dadd_rn(s, jn);
             } else {
                 s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
@@ -196,16 +226,24 @@ __device__ __forceinline__ float poles_apply(const FusedParams& P, const uint2 r
             for (uint32_t p = 0; p < R.np; ++p) {
                 if ((R.kinds >> p) & 1u) continue;
                 const double a = cs[3 * p], ic = cs[3 * p + 1], iz = cs[3 * p + 2];
-                const double jq = P.pj[p0 + p], qq = P.pq[p0 + p];
+                const double jq = pj[p0 + p], qq = pq[p0 + p];
                 const double kk = __dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev);
                 const double jb = __dmul_rn(__dadd_rn(kk, half_new), iz);
-                P.pj[p0 + p] = __dsub_rn(__dmul_rn(2.0, jb), jq);
-                P.pq[p0 + p] = __dadd_rn(qq, __dmul_rn(P.dt, jb));
+                pj[p0 + p] = __dsub_rn(__dmul_rn(2.0, jb), jq);
+                pq[p0 + p] = __dadd_rn(qq, __dmul_rn(dt, jb));
             }
         }
         return u_new;
     }
     return u_star;
+}
+
+// The pole correction of one edge, if its row has runs (the common case,
+// no runs, stays inline).
+__device__ __forceinline__ float poles_apply(const FusedParams& P, const uint2 rr, uint32_t k, float u_star,
+                                             float prev_f, float cb_f) {
+    if (rr.y == 0) return u_star;
+    return poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, u_star, prev_f, cb_f, nullptr);
 }
 
 // Shared memory layout of the fused kernel (floats unless noted):

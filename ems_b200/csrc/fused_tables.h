@@ -78,26 +78,90 @@ struct FusedSlabSpec {
     size_t len;                    // ψ values of the slab
 };
 
+struct PoleRuns {
+    std::vector<PoleRun> runs;
+    std::vector<double> sets;
+    std::vector<uint2> row_runs;  // per (x*3 + axis)*ny + y
+};
+
+// The poles of one side as runs along z (edges are in (plane, axis, y, z)
+// order): consecutive edges of one row with the same constants share a run.
+// Returns "" or why the side cannot be held as runs.
+inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, uint32_t nz, PoleRuns& R) {
+    std::unordered_map<std::string, uint32_t> set_of;
+    R.row_runs.assign((size_t)nx * 3 * ny, uint2{0, 0});
+    uint64_t last_row = ~0ull;
+    uint32_t last_k = 0;
+    for (size_t e = 0; e < pe->n_edges; ++e) {
+        const uint64_t idx = pe->node[e];
+        const uint64_t kk = idx % nz, rr = idx / nz;
+        const uint64_t jj = rr % ny, ii = rr / ny;
+        const uint64_t row_key = (ii * 3 + pe->axis[e]) * ny + jj;
+        if (last_row != ~0ull && row_key < last_row) return "pole edges out of order";
+        const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
+        const uint32_t np = p1 - p0;
+        if (np > kMaxPoles || np == 0) return "more than 16 poles on an edge";
+        std::string key((size_t)np * 24 + 12, '\0');
+        uint32_t kinds = 0;
+        for (uint32_t q = 0; q < np; ++q) {
+            const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
+            std::memcpy(&key[(size_t)q * 24], c3, 24);
+            if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
+        }
+        std::memcpy(&key[(size_t)np * 24], &pe->sum_inv_z[e], 8);
+        std::memcpy(&key[(size_t)np * 24 + 8], &kinds, 4);
+        auto it = set_of.find(key);
+        uint32_t set;
+        if (it == set_of.end()) {
+            set = (uint32_t)R.sets.size();
+            for (uint32_t q = 0; q < np; ++q) {
+                R.sets.push_back(pe->a[p0 + q]);
+                R.sets.push_back(pe->inv_c[p0 + q]);
+                R.sets.push_back(pe->inv_z[p0 + q]);
+            }
+            set_of.emplace(key, set);
+        } else {
+            set = it->second;
+        }
+        const bool extend = !R.runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 &&
+                            R.runs.back().set == set && R.runs.back().np == np && R.runs.back().kinds == kinds &&
+                            R.runs.back().p0 + (R.runs.back().ke - R.runs.back().kb) * np == p0 &&
+                            R.runs.back().e0 + (R.runs.back().ke - R.runs.back().kb) == e;
+        if (extend) {
+            R.runs.back().ke = (uint32_t)kk + 1;
+        } else {
+            if (row_key != last_row) R.row_runs[row_key] = uint2{(uint32_t)R.runs.size(), 0};
+            R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, 0, pe->sum_inv_z[e]});
+            R.row_runs[row_key].y++;
+        }
+        last_row = row_key;
+        last_k = (uint32_t)kk;
+    }
+    return "";
+}
+
+// Tables of the table-driven schedules (the fused kernel and the two-kernel
+// schedule): pooled coefficient rows, CPML slabs per (side, component) in
+// application order, poles as runs.
 struct FusedTables {
-    std::string why;               // empty: the fused schedule can run
+    std::string why;               // why the table-driven schedules cannot run ("" if they can)
+    std::string fused_why;         // why the fused kernel cannot run ("" if it can)
     Pooled lane[12];
     std::vector<FusedSlabSpec> slabs;
     int nslab[2][3] = {{0, 0, 0}, {0, 0, 0}};
     bool poles_first = false;
-    bool has_poles = false;
+    bool has_poles = false, has_poles_h = false;
     std::vector<PoleRun> runs;
     std::vector<double> sets;
     std::vector<uint2> row_runs;
+    PoleRuns h;                    // magnetic poles
 };
 
 // Why the fused schedule cannot run this model ("" if it can).
 inline std::string fused_ineligible(const ems_engine_desc* d, uint32_t pitch) {
-    int n_cpml = 0, n_poles = 0;
     for (size_t k = 0; k < d->n_ops; ++k) {
         const int kind = d->ops[k].kind;
-        if (kind == EMS_OP_CPML) ++n_cpml;
         if (kind == EMS_OP_POLES) {
-            ++n_poles;
             const auto* p = (const ems_poles*)d->ops[k].table;
             if (p->magnetic.n_edges) return "magnetic poles";
         }
@@ -106,15 +170,22 @@ inline std::string fused_ineligible(const ems_engine_desc* d, uint32_t pitch) {
             if (s->kind == EMS_SOFT_H || s->kind == EMS_HARD_H) return "magnetic sources";
         }
     }
-    if (n_cpml > 1 || n_poles > 1) return "several CPML or dispersive operators";
     if (pitch > 1024) return "z rows longer than 1024 nodes";
     return "";
 }
 
 inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) {
     FusedTables T;
-    T.why = fused_ineligible(d, pitch);
-    if (!T.why.empty()) return T;
+    int n_cpml = 0, n_poles = 0;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        n_cpml += d->ops[k].kind == EMS_OP_CPML;
+        n_poles += d->ops[k].kind == EMS_OP_POLES;
+    }
+    if (n_cpml > 1 || n_poles > 1) {
+        T.why = T.fused_why = "several CPML or dispersive operators";
+        return T;
+    }
+    T.fused_why = fused_ineligible(d, pitch);
     const uint32_t nx = (uint32_t)d->nodes[0], ny = (uint32_t)d->nodes[1], nz = (uint32_t)d->nodes[2];
     {
         std::vector<std::thread> th;
@@ -123,7 +194,7 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
         for (auto& t : th) t.join();
     }
     int pos_cpml = -1, pos_poles = -1;
-    const ems_pole_side* pe = nullptr;
+    const ems_poles* poles = nullptr;
     for (size_t k = 0; k < d->n_ops; ++k) {
         if (d->ops[k].kind == EMS_OP_CPML) {
             pos_cpml = (int)k;
@@ -135,7 +206,7 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
                 const int side = s.e_side ? 1 : 0;
                 int& n = T.nslab[side][s.comp];
                 if (n >= 4) {
-                    T.why = "more than four CPML slabs per component";
+                    T.why = T.fused_why = "more than four CPML slabs per component";
                     return T;
                 }
                 T.slabs.push_back({side, (int)s.comp, n, q, &s, len});
@@ -144,64 +215,29 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
         }
         if (d->ops[k].kind == EMS_OP_POLES) {
             pos_poles = (int)k;
-            pe = &((const ems_poles*)d->ops[k].table)->electric;
+            poles = (const ems_poles*)d->ops[k].table;
         }
     }
     T.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
-    // Electric poles as runs along z (edges are in (plane, axis, y, z) order):
-    // consecutive edges of one row with the same constants share a run.
-    if (pe && pe->n_edges) {
-        std::unordered_map<std::string, uint32_t> set_of;
-        T.row_runs.assign((size_t)nx * 3 * ny, uint2{0, 0});
-        uint64_t last_row = ~0ull;
-        uint32_t last_k = 0;
-        for (size_t e = 0; e < pe->n_edges; ++e) {
-            const uint64_t idx = pe->node[e];
-            const uint64_t kk = idx % nz, rr = idx / nz;
-            const uint64_t jj = rr % ny, ii = rr / ny;
-            const uint64_t row_key = (ii * 3 + pe->axis[e]) * ny + jj;
-            const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
-            const uint32_t np = p1 - p0;
-            if (np > kMaxPoles || np == 0) {
-                T.why = "edge pole count";
-                return T;
-            }
-            std::string key((size_t)np * 24 + 12, '\0');
-            uint32_t kinds = 0;
-            for (uint32_t q = 0; q < np; ++q) {
-                const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
-                std::memcpy(&key[(size_t)q * 24], c3, 24);
-                if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
-            }
-            std::memcpy(&key[(size_t)np * 24], &pe->sum_inv_z[e], 8);
-            std::memcpy(&key[(size_t)np * 24 + 8], &kinds, 4);
-            auto it = set_of.find(key);
-            uint32_t set;
-            if (it == set_of.end()) {
-                set = (uint32_t)T.sets.size();
-                for (uint32_t q = 0; q < np; ++q) {
-                    T.sets.push_back(pe->a[p0 + q]);
-                    T.sets.push_back(pe->inv_c[p0 + q]);
-                    T.sets.push_back(pe->inv_z[p0 + q]);
-                }
-                set_of.emplace(key, set);
-            } else {
-                set = it->second;
-            }
-            const bool extend = !T.runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 &&
-                                T.runs.back().set == set && T.runs.back().np == np && T.runs.back().kinds == kinds &&
-                                T.runs.back().p0 + (T.runs.back().ke - T.runs.back().kb) * np == p0;
-            if (extend) {
-                T.runs.back().ke = (uint32_t)kk + 1;
-            } else {
-                if (row_key != last_row) T.row_runs[row_key] = uint2{(uint32_t)T.runs.size(), 0};
-                T.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, pe->sum_inv_z[e]});
-                T.row_runs[row_key].y++;
-            }
-            last_row = row_key;
-            last_k = (uint32_t)kk;
+    if (poles && poles->electric.n_edges) {
+        PoleRuns R;
+        std::string w = pole_runs(&poles->electric, nx, ny, nz, R);
+        if (!w.empty()) {
+            T.why = T.fused_why = w;
+            return T;
         }
+        T.runs = std::move(R.runs);
+        T.sets = std::move(R.sets);
+        T.row_runs = std::move(R.row_runs);
         T.has_poles = true;
+    }
+    if (poles && poles->magnetic.n_edges) {
+        std::string w = pole_runs(&poles->magnetic, nx, ny, nz, T.h);
+        if (!w.empty()) {
+            T.why = T.fused_why = w;
+            return T;
+        }
+        T.has_poles_h = true;
     }
     return T;
 }

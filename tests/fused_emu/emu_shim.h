@@ -23,6 +23,7 @@
 #define __device__
 #define __host__
 #define __forceinline__ inline
+#define __noinline__ __attribute__((noinline))
 #define __launch_bounds__(...)
 #define __align__(n) alignas(n)
 #define __grid_constant__
@@ -35,6 +36,7 @@ inline uint2 make_uint2(uint32_t x, uint32_t y) { return uint2{x, y}; }
 struct EmuDim {
     unsigned x = 0, y = 0, z = 0;
 };
+inline uint2 make_uint2(uint32_t x, uint32_t y);
 extern thread_local EmuDim threadIdx;
 extern EmuDim blockIdx, blockDim, gridDim;
 

@@ -16,6 +16,7 @@ void fail(const char* what) {
 
 #include "../../ems_b200/csrc/fused.cuh"
 #include "../../ems_b200/csrc/fused_tables.h"
+#include "../../ems_b200/csrc/separate.cuh"
 
 using namespace emsk;
 
@@ -178,5 +179,149 @@ extern "C" int emu_fused_run(const ems_engine_desc* d, int tj, unsigned grid, ui
     for (int c = 0; c < 6; ++c)
         for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
             std::memcpy(fields[c] + r * g.nz, &buf[cur][c][r * g.pitch], g.nz * 4);
+    return 0;
+}
+
+// Runs `steps` steps of the two-kernel schedule (separate.cuh) in place from
+// the given fields (reference layout, overwritten). energies as above.
+extern "C" int emu_two_run(const ems_engine_desc* d, uint64_t steps, float** fields, double* energies) {
+    g_err[0] = 0;
+    Grid g{};
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "not eligible: %s", T.why.c_str());
+        return 1;
+    }
+    auto pad = [&](const float* src, std::vector<float>& dst) {
+        dst.assign(g.np, 0.0f);
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r) std::memcpy(&dst[r * g.pitch], src + r * g.nz, g.nz * 4);
+    };
+    std::vector<float> buf[6];
+    for (int c = 0; c < 6; ++c) pad(fields[c], buf[c]);
+    std::vector<float> dense[12];
+    FusedParams P{};
+    P.g = g;
+    P.dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (T.lane[l].pooled) {
+            P.lane[l].rid = T.lane[l].rid.data();
+            P.lane[l].rows = T.lane[l].rows.data();
+            P.lane[l].bg = T.lane[l].bg;
+        } else {
+            pad(d->coeff[l], dense[l]);
+            P.lane[l].dense = dense[l].data();
+        }
+    }
+    std::vector<std::vector<float>> psi;
+    psi.reserve(T.slabs.size());
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    for (const FusedSlabSpec& sp : T.slabs) {
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = (uint32_t)sp.src->lo[a];
+            f.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        f.normal = (uint32_t)sp.src->normal;
+        f.b = sp.src->b;
+        f.a = sp.src->a;
+        f.k = sp.src->k;
+        psi.emplace_back(sp.len, 0.0f);
+        f.psi_old = f.psi_new = psi.back().data();
+    }
+    std::vector<double> pj, pq, pjh, pqh;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind == EMS_OP_POLES) {
+            const auto* p = (const ems_poles*)d->ops[k].table;
+            pj.assign(p->electric.n_poles, 0.0);
+            pq.assign(p->electric.n_poles, 0.0);
+            pjh.assign(p->magnetic.n_poles, 0.0);
+            pqh.assign(p->magnetic.n_poles, 0.0);
+        }
+    if (T.has_poles) {
+        P.has_poles = 1;
+        P.runs = T.runs.data();
+        P.sets = T.sets.data();
+        P.row_runs = T.row_runs.data();
+        P.pj = pj.data();
+        P.pq = pq.data();
+    }
+    std::vector<float> prev_h;
+    const ems_pole_side* mside = nullptr;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind == EMS_OP_POLES) mside = &((const ems_poles*)d->ops[k].table)->magnetic;
+    if (T.has_poles_h) {
+        P.has_poles_h = 1;
+        P.runs_h = T.h.runs.data();
+        P.sets_h = T.h.sets.data();
+        P.row_runs_h = T.h.row_runs.data();
+        P.pj_h = pjh.data();
+        P.pq_h = pqh.data();
+        prev_h.assign(mside->n_edges, 0.0f);
+        P.prev_h = prev_h.data();
+    }
+    P.poles_first = T.poles_first ? 1 : 0;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = P.un[a] = buf[a].data();
+        P.io[a] = P.in[a] = buf[3 + a].data();
+    }
+    const unsigned gx = (g.nz + kSepK - 1) / kSepK, gy = (g.ny + kSepJ - 1) / kSepJ, gz = g.nx;
+    std::vector<double> partials((size_t)gx * gy * gz, 0.0);
+    P.partials = partials.data();
+    auto launch = [&](auto body) -> bool {
+        blockDim = EmuDim{kSepK, kSepJ, 1};
+        gridDim = EmuDim{gx, gy, gz};
+        for (unsigned bz = 0; bz < gz; ++bz)
+            for (unsigned by = 0; by < gy; ++by)
+                for (unsigned bx = 0; bx < gx; ++bx) {
+                    blockIdx = EmuDim{bx, by, bz};
+                    emu::Block blk;
+                    std::barrier<> bar((std::ptrdiff_t)(kSepK * kSepJ));
+                    blk.bar = &bar;
+                    blk.sums.assign(kSepK * kSepJ, 0.0);
+                    emu::cur = &blk;
+                    std::vector<std::thread> th;
+                    for (unsigned ty = 0; ty < kSepJ; ++ty)
+                        for (unsigned tx = 0; tx < kSepK; ++tx)
+                            th.emplace_back([&, tx, ty] {
+                                threadIdx.x = tx;
+                                threadIdx.y = ty;
+                                body();
+                            });
+                    for (auto& x : th) x.join();
+                    emu::cur = nullptr;
+                    if (blk.errors.load()) {
+                        std::snprintf(g_err, sizeof g_err, "%s", blk.msg);
+                        return false;
+                    }
+                }
+        return true;
+    };
+    for (uint64_t s = 0; s < steps; ++s) {
+        bool ok = energies ? launch([&] { k_step_h<true>(P); }) : launch([&] { k_step_h<false>(P); });
+        if (!ok) return 2;
+        if (energies) {
+            double w = 0.0;
+            for (double x : partials) w += x;
+            energies[s] = 0.25 * d->dt * w;
+        }
+        if (!launch([&] { k_step_e(P); })) return 2;
+        // The magnetic-pole edges save their current after the E update.
+        if (T.has_poles_h)
+            for (size_t e = 0; e < mside->n_edges; ++e) {
+                const uint64_t idx = mside->node[e];
+                const uint64_t k = idx % g.nz, r = idx / g.nz;
+                prev_h[e] = buf[3 + mside->axis[e]][r * g.pitch + k];
+            }
+    }
+    for (int c = 0; c < 6; ++c)
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
+            std::memcpy(fields[c] + r * g.nz, &buf[c][r * g.pitch], g.nz * 4);
     return 0;
 }

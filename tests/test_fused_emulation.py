@@ -29,11 +29,13 @@ def emu_lib(asan=False):
     lib = C.CDLL(build.build(asan))
     lib.emu_fused_run.restype = C.c_int
     lib.emu_fused_run.argtypes = [C.c_void_p, C.c_int, C.c_uint, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_two_run.restype = C.c_int
+    lib.emu_two_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_error.restype = C.c_char_p
     return lib
 
 
-def model(n, scheme, cpml=3, poles=True, graded=False):
+def model(n, scheme, cpml=3, poles=True, graded=False, magnetic=False):
     rng = np.random.default_rng(11)
     if graded:
         lines = [np.cumsum(np.concatenate([[0.0], 1e-3 * (1.0 + 0.3 * rng.random(c))])) for c in n]
@@ -51,6 +53,9 @@ def model(n, scheme, cpml=3, poles=True, graded=False):
         d.fill_cells(m, sph, W.lorentz_poles(5))
         d.fill_cells(m, m.cells().box([0, 0, n[2] - 4], [n[0], n[1], n[2] - 2]), [E.Pole.drude(6e10, 6e9)])
         d.fill_cells(m, m.cells().box([2, 2, 2], [5, 4, 6]), [E.Pole.debye(1.5, 1e-11)])
+        if magnetic:
+            d.fill_cells(m, m.cells().box([1, 3, 2], [6, 7, 5]), [E.Pole.lorentz(3e10, 2e10, 1e9)], field=1)
+            d.fill_cells(m, m.cells().box([2, 1, 4], [5, 5, 8]), [E.Pole.drude(2e10, 3e9)], field=1)
         m.add_dispersive(d, scheme)
     return m
 
@@ -98,6 +103,26 @@ def test_fused_kernel_source_equals_oracle(n, tj, grid, scheme):
     assert np.all(np.isfinite(eg)) and np.all(eg > 0)
 
 
+@pytest.mark.parametrize("n,scheme,magnetic", [
+    ((9, 10, 13), E.TRAPEZOIDAL, True),
+    ((12, 11, 35), E.LEAPFROG, True),
+    ((10, 9, 8), E.LEAPFROG, False),
+])
+def test_two_kernel_source_equals_oracle(n, scheme, magnetic):
+    m = model(n, scheme, magnetic=magnetic)
+    state = random_state(m, seed=1)
+    steps = 10
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    en = np.zeros(steps)
+    lib = emu_lib()
+    assert lib.emu_two_run(m.desc, steps, ptrs, en.ctypes.data) == 0, lib.emu_error().decode()
+    want, _, _ = run_oracle(m, state, steps)
+    for name, a, b in zip(["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"], arrs, want):
+        bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])}"
+
+
 def test_fused_kernel_source_under_address_sanitizer():
     """The same emulation built with AddressSanitizer: no out-of-bounds access
     of any table, field, state or shared-memory buffer."""
@@ -111,6 +136,11 @@ def test_fused_kernel_source_under_address_sanitizer():
         "import test_fused_emulation as T, ems_b200 as E\n"
         "m = T.model((11, 9, 14), E.LEAPFROG)\n"
         "T.run_emu(T.emu_lib(asan=True), m, T.random_state(m), 6, 4, 2)\n"
+        "import ctypes as C, numpy as np\n"
+        "m2 = T.model((9, 10, 13), E.TRAPEZOIDAL, magnetic=True)\n"
+        "st = [np.ascontiguousarray(x) for x in T.random_state(m2)]\n"
+        "p = (C.c_void_p * 6)(*[a.ctypes.data for a in st])\n"
+        "assert T.emu_lib(asan=True).emu_two_run(m2.desc, 4, p, None) == 0\n"
         "print('clean')\n"
     ) % (HERE, os.path.dirname(HERE))
     env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")

@@ -24,8 +24,9 @@ pytestmark = pytest.mark.gpu
 ENERGY_RTOL = 1e-12
 
 
-def _lockstep(model, steps, energy_every=0, threads=4):
+def _lockstep(model, steps, energy_every=0, threads=4, schedule=0):
     g = E.Engine(model)
+    g.set_schedule(schedule)
     o = OracleEngine(model, threads=threads)
     eg, eo = [], []
     s = 0
@@ -63,10 +64,14 @@ def test_lossy_cavity_bit_exact():
 
 
 @pytest.mark.parametrize("scheme", [E.TRAPEZOIDAL, E.LEAPFROG])
-def test_every_operator_bit_exact(scheme):
+@pytest.mark.parametrize("schedule", [1, 3])
+def test_every_operator_bit_exact(scheme, schedule):
+    """Every operator at once (magnetic poles and an H source included), on
+    the per-operator kernels (1) and the two-kernel schedule (3)."""
     m, ops = mixed_model(scheme=scheme, steps=240)
-    g, o, eg, eo = _lockstep(m, 240, energy_every=20)
-    assert_fields_equal(g, o, f"mixed scheme {scheme}")
+    g, o, eg, eo = _lockstep(m, 240, energy_every=20, schedule=schedule)
+    assert g.schedule == schedule
+    assert_fields_equal(g, o, f"mixed scheme {scheme} schedule {schedule}")
     for name in ("pv", "pi", "pe"):
         _series_equal(g, o, ops[name])
     for which in (0, 1, 2):
@@ -81,12 +86,13 @@ def test_fused_schedule_bit_exact(scheme):
     m, ops = mixed_model(scheme=scheme, magnetic=False, h_source=False, steps=240)
     g, o, eg, eo = _lockstep(m, 240, energy_every=20)
     assert g.schedule == 2
-    s = E.Engine(m)
-    s.set_schedule(1)
-    assert s.schedule == 1
-    s.run(240)
     assert_fields_equal(g, o, f"fused vs oracle, scheme {scheme}")
-    assert_fields_equal(g, s, f"fused vs separate, scheme {scheme}")
+    for sch in (1, 3):
+        s = E.Engine(m)
+        s.set_schedule(sch)
+        assert s.schedule == sch
+        s.run(240)
+        assert_fields_equal(g, s, f"fused vs schedule {sch}, scheme {scheme}")
     for name in ("pv", "pi", "pe"):
         _series_equal(g, o, ops[name])
     for which in (0, 1, 2):
@@ -94,10 +100,12 @@ def test_fused_schedule_bit_exact(scheme):
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
 
 
-def test_separate_schedule_where_fused_cannot_run():
+def test_two_kernel_schedule_where_fused_cannot_run():
     m, _ = mixed_model(magnetic=True, steps=10)
     g = E.Engine(m)
-    assert g.schedule == 1
+    assert g.schedule == 3
+    with pytest.raises(E.EngineError):
+        g.set_schedule(2)
 
 
 def test_odd_sizes_and_tile_remainders():
@@ -170,10 +178,11 @@ def test_invalid_tables_rejected():
 
 
 @pytest.mark.parametrize("n", [40, 67])
-def test_dispersive_box_chunks_and_tiles(n):
-    """Sizes whose rows, tiles and x chunks leave remainders; fused and separate."""
+@pytest.mark.parametrize("schedule", [2, 3])
+def test_dispersive_box_chunks_and_tiles(n, schedule):
+    """Sizes whose rows, tiles and x chunks leave remainders."""
     w = W.dispersive_box(n=n, radius=n / 6, slab=3, cpml=4, steps=120)
-    g, o, eg, eo = _lockstep(w.model, 120, energy_every=15)
-    assert g.schedule == 2
+    g, o, eg, eo = _lockstep(w.model, 120, energy_every=15, schedule=schedule)
+    assert g.schedule == schedule
     assert_fields_equal(g, o, f"dispersive {n}")
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
