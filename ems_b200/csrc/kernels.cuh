@@ -100,8 +100,8 @@ __device__ __forceinline__ double weight(float a, double p, float b) {
     return b != 0.0f ? __ddiv_rn(__dmul_rn(__dadd_rn(1.0, (double)a), p), (double)b) : 0.0;
 }
 
-// Block-wide f64 sum in a fixed order (blockDim.x a multiple of 32, at
-// most THREADS); result valid in thread 0.
+// Block-wide f64 sum in a fixed order (blockDim.x·blockDim.y a multiple of
+// 32, at most THREADS); result valid in thread (0, 0).
 #ifdef EMS_HOST_EMULATION
 template <unsigned THREADS>
 __device__ __forceinline__ double block_sum(double v) { return emu::block_sum(v); }
@@ -110,12 +110,14 @@ template <unsigned THREADS>
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double sh[THREADS / 32];
     for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
-    const unsigned w = threadIdx.x / 32, l = threadIdx.x % 32;
-    if (l == 0) sh[w] = v;
+    // Linear thread index (blocks may be 2-D); warps of 32 consecutive ids.
+    const unsigned t = threadIdx.x + blockDim.x * threadIdx.y;
+    const unsigned n = blockDim.x * blockDim.y;
+    if (t % 32 == 0) sh[t / 32] = v;
     __syncthreads();
     double s = 0.0;
-    if (threadIdx.x == 0)
-        for (unsigned q = 0; q < blockDim.x / 32; ++q) s = __dadd_rn(s, sh[q]);
+    if (t == 0)
+        for (unsigned q = 0; q < n / 32; ++q) s = __dadd_rn(s, sh[q]);
     return s;
 }
 #endif

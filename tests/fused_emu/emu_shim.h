@@ -99,11 +99,12 @@ inline bool wait(uint64_t* bar, uint32_t parity) {
 }
 
 inline double block_sum(double v) {
-    cur->sums[threadIdx.x] = v;
+    const unsigned t = threadIdx.x + blockDim.x * threadIdx.y;
+    cur->sums[t] = v;
     cur->bar->arrive_and_wait();
     double s = 0.0;
-    if (threadIdx.x == 0)
-        for (unsigned q = 0; q < blockDim.x; ++q) s += cur->sums[q];
+    if (t == 0)
+        for (unsigned q = 0; q < blockDim.x * blockDim.y; ++q) s += cur->sums[q];
     cur->bar->arrive_and_wait();
     return s;
 }

@@ -138,11 +138,11 @@ extern "C" int emu_fused_run(const ems_engine_desc* d, int tj, unsigned grid, ui
         }
         P.energy = energies ? 1 : 0;
         counter = 0;
-        blockDim.x = g.pitch;
-        gridDim.x = grid;
+        blockDim = EmuDim{g.pitch, 1, 1};
+        gridDim = EmuDim{grid, 1, 1};
         double w = 0.0;
         for (unsigned b = 0; b < grid; ++b) {
-            blockIdx.x = b;
+            blockIdx = EmuDim{b, 0, 0};
             emu::Block blk;
             std::barrier<> bar((std::ptrdiff_t)g.pitch);
             blk.bar = &bar;
