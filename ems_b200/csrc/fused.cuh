@@ -66,13 +66,13 @@ struct FusedParams {
     Lane lane[12];
     FSlab slab[2][3][4];   // [side: 0 H, 1 E][component][application order]
     int nslab[2][3];
-    const uint2* row_runs; // electric poles: per (x*3 + axis)*ny + y: (first run, count)
+    const uint4* row_runs; // electric poles: per (x*3 + axis)*ny + y: (first run, count, z min, z end)
     const PoleRun* runs;
     const double* sets;
     double* pj;
     double* pq;
     int has_poles;
-    const uint2* row_runs_h; // magnetic poles (two-kernel schedule only)
+    const uint4* row_runs_h; // magnetic poles (two-kernel schedule only)
     const PoleRun* runs_h;
     const double* sets_h;
     double* pj_h;
@@ -171,22 +171,26 @@ __device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, ui
     return t;
 }
 
-// Whether any slab of `list` contains the node (inline; the correction itself
-// is out of line, as most nodes lie in no layer).
-__device__ __forceinline__ bool in_slabs(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k) {
-    bool in = false;
-    for (int q = 0; q < n; ++q) {
-        const FSlab& s = list[q];
-        in |= i >= s.lo[0] && i < s.hi[0] && j >= s.lo[1] && j < s.hi[1] && k >= s.lo[2] && k < s.hi[2];
+// The CPML correction of component C on side SIDE (0 H, 1 E): the slab
+// membership tests read the slab boxes straight from the kernel parameters
+// (most nodes lie in no layer); the correction itself is out of line. A node
+// of an updated edge lies in a slab exactly when its index along the slab's
+// normal is in the slab's range (the slab boxes leave out only padding).
+template <bool WRITE, int SIDE, int C>
+__device__ __forceinline__ float cpml_apply(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k, float t,
+                                            float coef, float sA, float sB) {
+    const int n = P.nslab[SIDE][C];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (q >= n) break;
+        const FSlab& s = P.slab[SIDE][C][q];
+        const uint32_t nrm = s.normal;
+        const uint32_t x = nrm == 0 ? i : (nrm == 1 ? j : k);
+        if (x >= s.lo[nrm] && x < s.hi[nrm] && i >= s.lo[0] && i < s.hi[0] && j >= s.lo[1] && j < s.hi[1] &&
+            k >= s.lo[2] && k < s.hi[2])
+            t = cpml_body<WRITE>(&P.slab[SIDE][C][q], 1, i, j, k, C, t, coef, sA, sB);
     }
-    return in;
-}
-
-template <bool WRITE>
-__device__ __forceinline__ float cpml_apply(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c,
-                                            float t, float coef, float sA, float sB) {
-    if (n == 0 || !in_slabs(list, n, i, j, k)) return t;
-    return cpml_body<WRITE>(list, n, i, j, k, c, t, coef, sA, sB);
+    return t;
 }
 
 // Electric-pole correction of the E edge (axis a, row (i, j), node k)
@@ -194,7 +198,7 @@ __device__ __forceinline__ float cpml_apply(const FSlab* list, int n, uint32_t i
 // pole's new state does not depend on the corrected voltage and is stored
 // at once; a trapezoidal pole's is formed from its old state after it.
 __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets, double* pj, double* pq, double dt,
-                                        const uint2 rr, uint32_t k, float u_star, float prev_f, float cb_f,
+                                        const uint4 rr, uint32_t k, float u_star, float prev_f, float cb_f,
                                         const float* prev_arr) {
     for (uint32_t q = 0; q < rr.y; ++q) {
         const PoleRun R = runs[rr.x + q];
@@ -240,9 +244,9 @@ __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets,
 
 // The pole correction of one edge, if its row has runs (the common case,
 // no runs, stays inline).
-__device__ __forceinline__ float poles_apply(const FusedParams& P, const uint2 rr, uint32_t k, float u_star,
+__device__ __forceinline__ float poles_apply(const FusedParams& P, const uint4 rr, uint32_t k, float u_star,
                                              float prev_f, float cb_f) {
-    if (rr.y == 0) return u_star;
+    if (k < rr.z || k >= rr.w) return u_star;
     return poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, u_star, prev_f, cb_f, nullptr);
 }
 
@@ -251,12 +255,12 @@ __device__ __forceinline__ float poles_apply(const FusedParams& P, const uint2 r
 //   H tile:   2 × TJ × pitch            (i_x, i_y of the owned rows, for the k−1 neighbour)
 //   bg rows:  12 × pitch                (each lane's background row)
 //   ids:      2 × 12 × (TJ + 1) u32     (row ids, current / next plane)
-//   runs:     2 × 3 × TJ uint2          (pole runs of the owned rows)
+//   runs:     2 × 3 × TJ uint4          (pole runs of the owned rows, 16-byte aligned)
 //   bars:     kStages u64
 template <int TJ>
 __host__ __device__ constexpr size_t fused_smem_bytes(uint32_t pitch) {
     return sizeof(float) * ((size_t)kStages * 3 * (TJ + 2) * pitch + 2 * (size_t)TJ * pitch + 12 * (size_t)pitch) +
-           sizeof(uint32_t) * 2 * 12 * (TJ + 1) + sizeof(uint2) * 2 * 3 * TJ + 8 * kStages + 64;
+           sizeof(uint32_t) * 2 * 12 * (TJ + 1) + 16 + sizeof(uint4) * 2 * 3 * TJ + 8 * kStages + 64;
 }
 
 template <int TJ, int MAXT>
@@ -270,8 +274,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
     float* sh = su + (size_t)kStages * 3 * (TJ + 2) * pitch;        // H tile
     float* sbg = sh + 2 * (size_t)TJ * pitch;                       // background rows
     uint32_t* sid = (uint32_t*)(sbg + 12 * (size_t)pitch);          // row ids [2][12][TJ+1]
-    uint2* srun = (uint2*)(sid + 2 * 12 * (TJ + 1));                // pole runs [2][3][TJ]
-    uint64_t* bars = (uint64_t*)(((uintptr_t)(srun + 2 * 3 * TJ) + 7) & ~(uintptr_t)7);
+    uint4* srun = (uint4*)(((uintptr_t)(sid + 2 * 12 * (TJ + 1)) + 15) & ~(uintptr_t)15);  // pole runs [2][3][TJ]
+    uint64_t* bars = (uint64_t*)(srun + 2 * 3 * TJ);
     EMS_SHARED uint32_t s_item;
     EMS_SHARED int s_fail;
 
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     const uint32_t q = t - 12 * (TJ + 1);
                     const int a = (int)(q / TJ), r = (int)(q % TJ);
                     const int j = j0 + r;
-                    uint2 v = make_uint2(0, 0);
+                    uint4 v = make_uint4(0, 0, 0, 0);
                     if (P.has_poles && p < g.nx && j < (int)g.ny) v = P.row_runs[((size_t)p * 3 + a) * g.ny + j];
                     srun[(b * 3 + a) * TJ + r] = v;
                 }
@@ -409,8 +413,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
                     if (P.nslab[0][0]) {
-                        t = own ? cpml_apply<true>(P.slab[0][0], P.nslab[0][0], i, j, k, 0, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false>(P.slab[0][0], P.nslab[0][0], i, j, k, 0, t, -db, A, __fmul_rn(-1.0f, B));
+                        t = own ? cpml_apply<true, 0, 0>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 0>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hx[r] = t;
                     if (own) P.in[0][idx] = t;
@@ -424,8 +428,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
                     if (P.nslab[0][1]) {
-                        t = own ? cpml_apply<true>(P.slab[0][1], P.nslab[0][1], i, j, k, 1, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false>(P.slab[0][1], P.nslab[0][1], i, j, k, 1, t, -db, A, __fmul_rn(-1.0f, B));
+                        t = own ? cpml_apply<true, 0, 1>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 1>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hy[r] = t;
                     if (own) P.in[1][idx] = t;
@@ -439,8 +443,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
                     if (P.nslab[0][2]) {
-                        t = own ? cpml_apply<true>(P.slab[0][2], P.nslab[0][2], i, j, k, 2, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false>(P.slab[0][2], P.nslab[0][2], i, j, k, 2, t, -db, A, __fmul_rn(-1.0f, B));
+                        t = own ? cpml_apply<true, 0, 2>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 2>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hz[r] = t;
                     if (own) P.in[2][idx] = t;
@@ -481,7 +485,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hz[r], hz[r - 1]), B = __fsub_rn(hy[r], hyk1);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uxo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 0) * TJ + r - 1], k, t, uxo, cb);
-                        if (P.nslab[1][0]) t = cpml_apply<true>(P.slab[1][0], P.nslab[1][0], i, j, k, 0, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (P.nslab[1][0]) t = cpml_apply<true, 1, 0>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 0) * TJ + r - 1], k, t, uxo, cb);
                         P.un[0][idx] = t;
                     }
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hx[r], hxk1), B = __fsub_rn(hz[r], hz_prev[r - 1]);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uyo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 1) * TJ + r - 1], k, t, uyo, cb);
-                        if (P.nslab[1][1]) t = cpml_apply<true>(P.slab[1][1], P.nslab[1][1], i, j, k, 1, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (P.nslab[1][1]) t = cpml_apply<true, 1, 1>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 1) * TJ + r - 1], k, t, uyo, cb);
                         P.un[1][idx] = t;
                     }
@@ -503,7 +507,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hy[r], hy_prev[r - 1]), B = __fsub_rn(hx[r], hx[r - 1]);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uzo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 2) * TJ + r - 1], k, t, uzo, cb);
-                        if (P.nslab[1][2]) t = cpml_apply<true>(P.slab[1][2], P.nslab[1][2], i, j, k, 2, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (P.nslab[1][2]) t = cpml_apply<true, 1, 2>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 2) * TJ + r - 1], k, t, uzo, cb);
                         P.un[2][idx] = t;
                     }

@@ -81,7 +81,7 @@ struct FusedSlabSpec {
 struct PoleRuns {
     std::vector<PoleRun> runs;
     std::vector<double> sets;
-    std::vector<uint2> row_runs;  // per (x*3 + axis)*ny + y
+    std::vector<uint4> row_runs;  // per (x*3 + axis)*ny + y: first run, count, z min, z end
 };
 
 // The poles of one side as runs along z (edges are in (plane, axis, y, z)
@@ -89,7 +89,7 @@ struct PoleRuns {
 // Returns "" or why the side cannot be held as runs.
 inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, uint32_t nz, PoleRuns& R) {
     std::unordered_map<std::string, uint32_t> set_of;
-    R.row_runs.assign((size_t)nx * 3 * ny, uint2{0, 0});
+    R.row_runs.assign((size_t)nx * 3 * ny, uint4{0, 0, 0, 0});
     uint64_t last_row = ~0ull;
     uint32_t last_k = 0;
     for (size_t e = 0; e < pe->n_edges; ++e) {
@@ -130,10 +130,11 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
         if (extend) {
             R.runs.back().ke = (uint32_t)kk + 1;
         } else {
-            if (row_key != last_row) R.row_runs[row_key] = uint2{(uint32_t)R.runs.size(), 0};
+            if (row_key != last_row) R.row_runs[row_key] = uint4{(uint32_t)R.runs.size(), 0, (uint32_t)kk, 0};
             R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, 0, pe->sum_inv_z[e]});
             R.row_runs[row_key].y++;
         }
+        R.row_runs[row_key].w = (uint32_t)kk + 1;  // the row's edges are in z order
         last_row = row_key;
         last_k = (uint32_t)kk;
     }
@@ -153,7 +154,7 @@ struct FusedTables {
     bool has_poles = false, has_poles_h = false;
     std::vector<PoleRun> runs;
     std::vector<double> sets;
-    std::vector<uint2> row_runs;
+    std::vector<uint4> row_runs;
     PoleRuns h;                    // magnetic poles
 };
 

@@ -28,19 +28,22 @@ __device__ __forceinline__ const float* lane_row(const FusedParams& P, int l, si
 template <bool H>
 __device__ __forceinline__ float hooks(const FusedParams& P, int c, uint32_t i, uint32_t j, uint32_t k, float t,
                                        float coef, float A, float B, float prev) {
-    const int side = H ? 0 : 1;
-    const uint2 rr = H ? (P.has_poles_h ? P.row_runs_h[((size_t)i * 3 + c) * P.g.ny + j] : make_uint2(0, 0))
-                       : (P.has_poles ? P.row_runs[((size_t)i * 3 + c) * P.g.ny + j] : make_uint2(0, 0));
+    constexpr int side = H ? 0 : 1;
+    const uint4 rr = H ? (P.has_poles_h ? P.row_runs_h[((size_t)i * 3 + c) * P.g.ny + j] : make_uint4(0, 0, 0, 0))
+                       : (P.has_poles ? P.row_runs[((size_t)i * 3 + c) * P.g.ny + j] : make_uint4(0, 0, 0, 0));
+    const bool in_runs = k >= rr.z && k < rr.w;
     // The pole correction's coefficient is the edge's cb (E) or db (H).
     const float pc = H ? -coef : coef;
     // Electric poles start from u^n (the voltage this thread read before
     // updating it); magnetic poles from the current saved after the last
     // E update (zero before the first), as the reference does.
-    if (P.poles_first && rr.y)
+    if (P.poles_first && in_runs)
         t = H ? poles_run(P.runs_h, P.sets_h, P.pj_h, P.pq_h, P.dt, rr, k, t, prev, pc, P.prev_h)
               : poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, t, prev, pc, nullptr);
-    t = cpml_apply<true>(P.slab[side][c], P.nslab[side][c], i, j, k, c, t, coef, A, __fmul_rn(-1.0f, B));
-    if (!P.poles_first && rr.y)
+    t = c == 0 ? cpml_apply<true, side, 0>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
+               : (c == 1 ? cpml_apply<true, side, 1>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
+                         : cpml_apply<true, side, 2>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B)));
+    if (!P.poles_first && in_runs)
         t = H ? poles_run(P.runs_h, P.sets_h, P.pj_h, P.pq_h, P.dt, rr, k, t, prev, pc, P.prev_h)
               : poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, t, prev, pc, nullptr);
     return t;

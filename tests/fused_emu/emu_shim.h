@@ -31,6 +31,10 @@
 struct uint2 {
     uint32_t x, y;
 };
+struct alignas(16) uint4 {
+    uint32_t x, y, z, w;
+};
+inline uint4 make_uint4(uint32_t x, uint32_t y, uint32_t z, uint32_t w) { return uint4{x, y, z, w}; }
 inline uint2 make_uint2(uint32_t x, uint32_t y) { return uint2{x, y}; }
 
 struct EmuDim {
