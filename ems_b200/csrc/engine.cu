@@ -349,6 +349,10 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
             h->psi_h_at.push_back({sp.comp, sp.q});
         }
     }
+    for (int a = 0; a < 3; ++a) {
+        P.cmask[a] = h->upload(T.cmask[a].data(), T.cmask[a].size());
+        if (!P.cmask[a]) return fail(h, EMS_ERR_NOMEM, "CPML masks");
+    }
     P.poles_first = T.poles_first ? 1 : 0;
     PoleSideDev* pe_dev = nullptr;
     PoleSideDev* ph_dev = nullptr;

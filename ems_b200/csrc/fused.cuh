@@ -66,6 +66,10 @@ struct FusedParams {
     Lane lane[12];
     FSlab slab[2][3][4];   // [side: 0 H, 1 E][component][application order]
     int nslab[2][3];
+    // Per axis and node index: bit side·12 + component·4 + q is set where the
+    // index lies in the normal range of slab [side][component][q] (a slab
+    // spans the grid on its other axes, so that decides membership).
+    const uint32_t* cmask[3];
     const uint4* row_runs; // electric poles: per (x*3 + axis)*ny + y: (first run, count, z min, z end)
     const PoleRun* runs;
     const double* sets;
@@ -171,24 +175,22 @@ __device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, ui
     return t;
 }
 
-// The CPML correction of component C on side SIDE (0 H, 1 E): the slab
-// membership tests read the slab boxes straight from the kernel parameters
-// (most nodes lie in no layer); the correction itself is out of line. A node
-// of an updated edge lies in a slab exactly when its index along the slab's
-// normal is in the slab's range (the slab boxes leave out only padding).
+// The CPML slabs containing node (i, j, k): one bit per slab (cmask).
+__device__ __forceinline__ uint32_t cpml_bits(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k) {
+    return P.cmask[0][i] | P.cmask[1][j] | P.cmask[2][k];
+}
+
+// The CPML correction of component C on side SIDE (0 H, 1 E) by the slabs
+// whose bits are set in `bits`, in application order; out of line, as most
+// nodes lie in no layer.
 template <bool WRITE, int SIDE, int C>
-__device__ __forceinline__ float cpml_apply(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k, float t,
-                                            float coef, float sA, float sB) {
-    const int n = P.nslab[SIDE][C];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (q >= n) break;
-        const FSlab& s = P.slab[SIDE][C][q];
-        const uint32_t nrm = s.normal;
-        const uint32_t x = nrm == 0 ? i : (nrm == 1 ? j : k);
-        if (x >= s.lo[nrm] && x < s.hi[nrm] && i >= s.lo[0] && i < s.hi[0] && j >= s.lo[1] && j < s.hi[1] &&
-            k >= s.lo[2] && k < s.hi[2])
-            t = cpml_body<WRITE>(&P.slab[SIDE][C][q], 1, i, j, k, C, t, coef, sA, sB);
+__device__ __forceinline__ float cpml_apply(const FusedParams& P, uint32_t bits, uint32_t i, uint32_t j, uint32_t k,
+                                            float t, float coef, float sA, float sB) {
+    uint32_t m = (bits >> (SIDE * 12 + C * 4)) & 15u;
+    while (m) {
+        const int q = __ffs(m) - 1;
+        m &= m - 1;
+        t = cpml_body<WRITE>(&P.slab[SIDE][C][q], 1, i, j, k, C, t, coef, sA, sB);
     }
     return t;
 }
@@ -403,6 +405,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                 if (j < 0 || j >= (int)g.ny || k >= g.nz) continue;
                 const bool own = r >= 1 && !warm;
                 const size_t idx = (size_t)i * si + (size_t)j * pitch + k;
+                const uint32_t cbits = cpml_bits(P, i, j, k);
                 const float ux = u0(0, r, k), uy = u0(1, r, k), uz = u0(2, r, k);
                 // x: (uz[j+1] − uz[j]) − (uy[k+1] − uy[k])
                 if (j + 1 < (int)g.ny && k + 1 < g.nz) {
@@ -412,9 +415,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
-                    if (P.nslab[0][0]) {
-                        t = own ? cpml_apply<true, 0, 0>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false, 0, 0>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
+                    if (cbits) {
+                        t = own ? cpml_apply<true, 0, 0>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 0>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hx[r] = t;
                     if (own) P.in[0][idx] = t;
@@ -427,9 +430,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
-                    if (P.nslab[0][1]) {
-                        t = own ? cpml_apply<true, 0, 1>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false, 0, 1>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
+                    if (cbits) {
+                        t = own ? cpml_apply<true, 0, 1>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 1>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hy[r] = t;
                     if (own) P.in[1][idx] = t;
@@ -442,9 +445,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
                     if (P.energy && own) w_acc = __dadd_rn(w_acc, weight(da, __dmul_rn((double)old, (double)nw), db));
                     float t = nw;
-                    if (P.nslab[0][2]) {
-                        t = own ? cpml_apply<true, 0, 2>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
-                                : cpml_apply<false, 0, 2>(P, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
+                    if (cbits) {
+                        t = own ? cpml_apply<true, 0, 2>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B))
+                                : cpml_apply<false, 0, 2>(P, cbits, i, j, k, t, -db, A, __fmul_rn(-1.0f, B));
                     }
                     hz[r] = t;
                     if (own) P.in[2][idx] = t;
@@ -468,6 +471,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                     if (j >= (int)g.ny || k >= g.nz) continue;
                     const size_t idx = (size_t)i * si + (size_t)j * pitch + k;
                     const float uxo = u0(0, r, k), uyo = u0(1, r, k), uzo = u0(2, r, k);
+                    const uint32_t cbits = cpml_bits(P, i, j, k);
                     const float hxk1 = k > 0 ? sh[(size_t)(r - 1) * pitch + k - 1] : 0.0f;
                     const float hyk1 = k > 0 ? sh[(size_t)(TJ + r - 1) * pitch + k - 1] : 0.0f;
                     float ca, cb;
@@ -485,7 +489,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hz[r], hz[r - 1]), B = __fsub_rn(hy[r], hyk1);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uxo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 0) * TJ + r - 1], k, t, uxo, cb);
-                        if (P.nslab[1][0]) t = cpml_apply<true, 1, 0>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (cbits) t = cpml_apply<true, 1, 0>(P, cbits, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 0) * TJ + r - 1], k, t, uxo, cb);
                         P.un[0][idx] = t;
                     }
@@ -496,7 +500,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hx[r], hxk1), B = __fsub_rn(hz[r], hz_prev[r - 1]);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uyo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 1) * TJ + r - 1], k, t, uyo, cb);
-                        if (P.nslab[1][1]) t = cpml_apply<true, 1, 1>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (cbits) t = cpml_apply<true, 1, 1>(P, cbits, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 1) * TJ + r - 1], k, t, uyo, cb);
                         P.un[1][idx] = t;
                     }
@@ -507,7 +511,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_fused(const __grid_constant__ Fused
                         const float A = __fsub_rn(hy[r], hy_prev[r - 1]), B = __fsub_rn(hx[r], hx[r - 1]);
                         float t = flush(__fadd_rn(__fmul_rn(ca, uzo), __fmul_rn(cb, __fsub_rn(A, B))));
                         if (P.has_poles && P.poles_first) t = poles_apply(P, srun[(b * 3 + 2) * TJ + r - 1], k, t, uzo, cb);
-                        if (P.nslab[1][2]) t = cpml_apply<true, 1, 2>(P, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
+                        if (cbits) t = cpml_apply<true, 1, 2>(P, cbits, i, j, k, t, cb, A, __fmul_rn(-1.0f, B));
                         if (P.has_poles && !P.poles_first) t = poles_apply(P, srun[(b * 3 + 2) * TJ + r - 1], k, t, uzo, cb);
                         P.un[2][idx] = t;
                     }

@@ -150,6 +150,7 @@ struct FusedTables {
     Pooled lane[12];
     std::vector<FusedSlabSpec> slabs;
     int nslab[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    std::vector<uint32_t> cmask[3];  // per axis and node index: the slabs whose normal range holds it
     bool poles_first = false;
     bool has_poles = false, has_poles_h = false;
     std::vector<PoleRun> runs;
@@ -210,6 +211,20 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
                     T.why = T.fused_why = "more than four CPML slabs per component";
                     return T;
                 }
+                // The kernels test a node's membership along the normal only:
+                // the slab must span the grid on its other axes (as the
+                // reference's layers do, less the padding index).
+                for (int a = 0; a < 3; ++a) {
+                    if (a == s.normal) continue;
+                    if (s.lo[a] != 0 || s.hi[a] + 1 < d->nodes[a]) {
+                        T.why = T.fused_why = "a CPML slab that does not span the grid";
+                        return T;
+                    }
+                }
+                if (T.cmask[0].empty())
+                    for (int a = 0; a < 3; ++a) T.cmask[a].assign(d->nodes[a], 0u);
+                for (uint64_t x = s.lo[s.normal]; x < s.hi[s.normal]; ++x)
+                    T.cmask[s.normal][x] |= 1u << (side * 12 + s.comp * 4 + n);
                 T.slabs.push_back({side, (int)s.comp, n, q, &s, len});
                 ++n;
             }
@@ -219,6 +234,8 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
             poles = (const ems_poles*)d->ops[k].table;
         }
     }
+    if (T.cmask[0].empty())
+        for (int a = 0; a < 3; ++a) T.cmask[a].assign(d->nodes[a], 0u);
     T.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
     if (poles && poles->electric.n_edges) {
         PoleRuns R;

@@ -26,8 +26,8 @@ __device__ __forceinline__ const float* lane_row(const FusedParams& P, int l, si
 // The slab hooks of one edge in registration order: CPML then poles, or
 // poles then CPML.
 template <bool H>
-__device__ __forceinline__ float hooks(const FusedParams& P, int c, uint32_t i, uint32_t j, uint32_t k, float t,
-                                       float coef, float A, float B, float prev) {
+__device__ __forceinline__ float hooks(const FusedParams& P, uint32_t cbits, int c, uint32_t i, uint32_t j, uint32_t k,
+                                       float t, float coef, float A, float B, float prev) {
     constexpr int side = H ? 0 : 1;
     const uint4 rr = H ? (P.has_poles_h ? P.row_runs_h[((size_t)i * 3 + c) * P.g.ny + j] : make_uint4(0, 0, 0, 0))
                        : (P.has_poles ? P.row_runs[((size_t)i * 3 + c) * P.g.ny + j] : make_uint4(0, 0, 0, 0));
@@ -40,9 +40,10 @@ __device__ __forceinline__ float hooks(const FusedParams& P, int c, uint32_t i, 
     if (P.poles_first && in_runs)
         t = H ? poles_run(P.runs_h, P.sets_h, P.pj_h, P.pq_h, P.dt, rr, k, t, prev, pc, P.prev_h)
               : poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, t, prev, pc, nullptr);
-    t = c == 0 ? cpml_apply<true, side, 0>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
-               : (c == 1 ? cpml_apply<true, side, 1>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
-                         : cpml_apply<true, side, 2>(P, i, j, k, t, coef, A, __fmul_rn(-1.0f, B)));
+    if (cbits)
+        t = c == 0 ? cpml_apply<true, side, 0>(P, cbits, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
+                   : (c == 1 ? cpml_apply<true, side, 1>(P, cbits, i, j, k, t, coef, A, __fmul_rn(-1.0f, B))
+                             : cpml_apply<true, side, 2>(P, cbits, i, j, k, t, coef, A, __fmul_rn(-1.0f, B)));
     if (!P.poles_first && in_runs)
         t = H ? poles_run(P.runs_h, P.sets_h, P.pj_h, P.pq_h, P.dt, rr, k, t, prev, pc, P.prev_h)
               : poles_run(P.runs, P.sets, P.pj, P.pq, P.dt, rr, k, t, prev, pc, nullptr);
@@ -61,6 +62,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_h(const __grid_constant__
         const uint32_t idx = i * si + j * g.pitch + k;
         const size_t row = (size_t)i * g.ny + j;
         const float ux = P.un[0][idx], uy = P.un[1][idx], uz = P.un[2][idx];
+        const uint32_t cbits = cpml_bits(P, i, j, k);
         if (ENERGY) {
             w = __dadd_rn(w, weight(lane_row(P, 0, row)[k], __dmul_rn((double)ux, (double)ux), lane_row(P, 3, row)[k]));
             w = __dadd_rn(w, weight(lane_row(P, 1, row)[k], __dmul_rn((double)uy, (double)uy), lane_row(P, 4, row)[k]));
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_h(const __grid_constant__
             const float old = P.in[0][idx];
             const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
-            P.in[0][idx] = hooks<true>(P, 0, i, j, k, nw, -db, A, B, old);
+            P.in[0][idx] = hooks<true>(P, cbits, 0, i, j, k, nw, -db, A, B, old);
         }
         // y: (ux[k+1] − ux[k]) − (uz[i+1] − uz[i])
         if (i + 1 < g.nx && k + 1 < g.nz) {
@@ -82,7 +84,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_h(const __grid_constant__
             const float old = P.in[1][idx];
             const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
-            P.in[1][idx] = hooks<true>(P, 1, i, j, k, nw, -db, A, B, old);
+            P.in[1][idx] = hooks<true>(P, cbits, 1, i, j, k, nw, -db, A, B, old);
         }
         // z: (uy[i+1] − uy[i]) − (ux[j+1] − ux[j])
         if (i + 1 < g.nx && j + 1 < g.ny) {
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_h(const __grid_constant__
             const float old = P.in[2][idx];
             const float nw = flush(__fsub_rn(__fmul_rn(da, old), __fmul_rn(db, __fsub_rn(A, B))));
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
-            P.in[2][idx] = hooks<true>(P, 2, i, j, k, nw, -db, A, B, old);
+            P.in[2][idx] = hooks<true>(P, cbits, 2, i, j, k, nw, -db, A, B, old);
         }
     }
     if (ENERGY) {
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_e(const __grid_constant__
     const uint32_t idx = i * si + j * g.pitch + k;
     const size_t row = (size_t)i * g.ny + j;
     const float ix = P.in[0][idx], iy = P.in[1][idx], iz = P.in[2][idx];
+    const uint32_t cbits = cpml_bits(P, i, j, k);
     // x: (iz[j] − iz[j−1]) − (iy[k] − iy[k−1])
     if (i + 1 < g.nx) {
         const float ca = lane_row(P, 0, row)[k], cb = lane_row(P, 3, row)[k];
@@ -117,7 +120,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_e(const __grid_constant__
         const float B = __fsub_rn(iy, k > 0 ? P.in[1][idx - 1] : 0.0f);
         const float old = P.un[0][idx];
         const float t = flush(__fadd_rn(__fmul_rn(ca, old), __fmul_rn(cb, __fsub_rn(A, B))));
-        P.un[0][idx] = hooks<false>(P, 0, i, j, k, t, cb, A, B, old);
+        P.un[0][idx] = hooks<false>(P, cbits, 0, i, j, k, t, cb, A, B, old);
     }
     // y: (ix[k] − ix[k−1]) − (iz[i] − iz[i−1])
     if (j + 1 < g.ny) {
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_e(const __grid_constant__
         const float B = __fsub_rn(iz, i > 0 ? P.in[2][idx - si] : 0.0f);
         const float old = P.un[1][idx];
         const float t = flush(__fadd_rn(__fmul_rn(ca, old), __fmul_rn(cb, __fsub_rn(A, B))));
-        P.un[1][idx] = hooks<false>(P, 1, i, j, k, t, cb, A, B, old);
+        P.un[1][idx] = hooks<false>(P, cbits, 1, i, j, k, t, cb, A, B, old);
     }
     // z: (iy[i] − iy[i−1]) − (ix[j] − ix[j−1])
     if (k + 1 < g.nz) {
@@ -135,7 +138,7 @@ __global__ void __launch_bounds__(kSepK* kSepJ) k_step_e(const __grid_constant__
         const float B = __fsub_rn(ix, j > 0 ? P.in[0][idx - g.pitch] : 0.0f);
         const float old = P.un[2][idx];
         const float t = flush(__fadd_rn(__fmul_rn(ca, old), __fmul_rn(cb, __fsub_rn(A, B))));
-        P.un[2][idx] = hooks<false>(P, 2, i, j, k, t, cb, A, B, old);
+        P.un[2][idx] = hooks<false>(P, cbits, 2, i, j, k, t, cb, A, B, old);
     }
 }
 

@@ -107,6 +107,7 @@ extern "C" int emu_fused_run(const ems_engine_desc* d, int tj, unsigned grid, ui
         P.pq = pq.data();
     }
     P.poles_first = T.poles_first ? 1 : 0;
+    for (int a = 0; a < 3; ++a) P.cmask[a] = T.cmask[a].data();
     fused_work(P, g.nx, g.ny, tj, grid);
     uint32_t counter = 0;
     int status = 0;
@@ -267,6 +268,7 @@ extern "C" int emu_two_run(const ems_engine_desc* d, uint64_t steps, float** fie
         P.prev_h = prev_h.data();
     }
     P.poles_first = T.poles_first ? 1 : 0;
+    for (int a = 0; a < 3; ++a) P.cmask[a] = T.cmask[a].data();
     for (int a = 0; a < 3; ++a) {
         P.uo[a] = P.un[a] = buf[a].data();
         P.io[a] = P.in[a] = buf[3 + a].data();
