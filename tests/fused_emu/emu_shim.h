@@ -31,6 +31,10 @@
 struct uint2 {
     uint32_t x, y;
 };
+struct alignas(16) float4 {
+    float x, y, z, w;
+};
+inline float4 make_float4(float x, float y, float z, float w) { return float4{x, y, z, w}; }
 struct alignas(16) uint4 {
     uint32_t x, y, z, w;
 };
