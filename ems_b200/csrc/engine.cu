@@ -380,7 +380,7 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         P.prev_h = ph_dev->prev;
         if (!P.runs_h || !P.sets_h || !P.row_runs_h) return fail(h, EMS_ERR_NOMEM, "pole runs");
     }
-    h->n_spartials = (size_t)blocks_for(g.nz, kSepK * kVec) * blocks_for(g.ny, kSepJ) * g.nx;
+    h->n_spartials = (size_t)blocks_for(g.nz, kSepJ * kSeg) * blocks_for(g.ny, kSepK) * g.nx;
     h->spartials = h->alloc<double>(h->n_spartials);
     if (!h->spartials) return fail(h, EMS_ERR_NOMEM, "energy shares");
     h->tables_ok = true;
@@ -493,7 +493,7 @@ ems_status run_step_two(ems_gpu* h, bool energy) {
     }
     P.partials = h->spartials;
     dim3 blk(kSepK, kSepJ, 1);
-    dim3 grd(blocks_for(g.nz, kSepK * kVec), blocks_for(g.ny, kSepJ), g.nx);
+    dim3 grd(blocks_for(g.nz, kSepJ * kSeg), blocks_for(g.ny, kSepK), g.nx);
     cudaEvent_t ev = h->prof_begin();
     if (energy) {
         k_step_h<true><<<grd, blk, 0, s>>>(P);

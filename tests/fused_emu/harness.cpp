@@ -273,7 +273,7 @@ extern "C" int emu_two_run(const ems_engine_desc* d, uint64_t steps, float** fie
         P.uo[a] = P.un[a] = buf[a].data();
         P.io[a] = P.in[a] = buf[3 + a].data();
     }
-    const unsigned gx = (g.nz + kSepK * kVec - 1) / (kSepK * kVec), gy = (g.ny + kSepJ - 1) / kSepJ, gz = g.nx;
+    const unsigned gx = (g.nz + kSepJ * kSeg - 1) / (kSepJ * kSeg), gy = (g.ny + kSepK - 1) / kSepK, gz = g.nx;
     std::vector<double> partials((size_t)gx * gy * gz, 0.0);
     P.partials = partials.data();
     auto launch = [&](auto body) -> bool {
