@@ -196,6 +196,8 @@ GPU_SYMBOLS = {
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_energy_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
     "ems_gpu_last_sample": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
     "ems_gpu_source_amplitude": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p, C.c_size_t]),
     "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),

@@ -8,6 +8,8 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "arith.cuh"
+
 namespace emsk {
 
 constexpr unsigned kRowThreads = 128;  // threads of a z-row block
@@ -81,46 +83,6 @@ struct ProbeDevT {
     const uint8_t* axis = nullptr;
     const double* weight = nullptr;
 };
-
-// Rounds subnormal results to zero (src/engine/kernel.rs:30-33).
-__device__ __forceinline__ float flush(float x) { return fabsf(x) < FLT_MIN ? 0.0f : x; }
-
-// flush(ca·u + cb·((a − b) − (c − d))) (src/engine/kernel.rs:252-273).
-__device__ __forceinline__ float e_upd(float ca, float u, float cb, float a, float b, float c, float d) {
-    return flush(__fadd_rn(__fmul_rn(ca, u), __fmul_rn(cb, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));
-}
-
-// flush(da·h − db·((a − b) − (c − d))) (src/engine/kernel.rs:58-79).
-__device__ __forceinline__ float h_upd(float da, float h, float db, float a, float b, float c, float d) {
-    return flush(__fsub_rn(__fmul_rn(da, h), __fmul_rn(db, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));
-}
-
-// (1 + a)·p/b, 0 where b = 0 (src/engine/kernel.rs:116-120).
-__device__ __forceinline__ double weight(float a, double p, float b) {
-    return b != 0.0f ? __ddiv_rn(__dmul_rn(__dadd_rn(1.0, (double)a), p), (double)b) : 0.0;
-}
-
-// Block-wide f64 sum in a fixed order (blockDim.x·blockDim.y a multiple of
-// 32, at most THREADS); result valid in thread (0, 0).
-#ifdef EMS_HOST_EMULATION
-template <unsigned THREADS>
-__device__ __forceinline__ double block_sum(double v) { return emu::block_sum(v); }
-#else
-template <unsigned THREADS>
-__device__ __forceinline__ double block_sum(double v) {
-    __shared__ double sh[THREADS / 32];
-    for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
-    // Linear thread index (blocks may be 2-D); warps of 32 consecutive ids.
-    const unsigned t = threadIdx.x + blockDim.x * threadIdx.y;
-    const unsigned n = blockDim.x * blockDim.y;
-    if (t % 32 == 0) sh[t / 32] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (t == 0)
-        for (unsigned q = 0; q < n / 32; ++q) s = __dadd_rn(s, sh[q]);
-    return s;
-}
-#endif
 
 // H update of every dual edge (src/engine/kernel.rs:447-511, 571-618);
 // with ENERGY each block also writes its share of the energy invariant

@@ -228,6 +228,28 @@ ems_status ems_gpu_last_sample(ems_gpu* h, size_t op, int which, double* out);
  * creation. */
 ems_status ems_gpu_source_amplitude(ems_gpu* h, size_t op, uint64_t first, const double* values, size_t n);
 
+/* The energy invariant W^n of a field state, for callers that cannot
+ * allocate device memory when they need it (a framework that owns all
+ * device memory through its own pool, a real-time loop that must not
+ * allocate after start-up). It has no counterpart in the reference: there
+ * the engine evaluates W^n on its own fields (Engine::energy).
+ *
+ * u, i: the six field arrays, i holding i^{n-1/2}; coeff: the twelve
+ * coefficient arrays; all device arrays in the reference layout
+ * ((i*ny + j)*nz + k, nx*ny*nz floats each). Writes
+ * W^n = dt/4 * [sum (1+ca)/cb u^2 + sum (1+da)/db i^{n-1/2} i^{n+1/2}]
+ * (i^{n+1/2} the H update's value, not stored; no operator energies) to the
+ * device double `energy`, in stream `stream` (a cudaStream_t; NULL: the
+ * legacy default stream), asynchronously. It calls no allocator: its working
+ * memory is a file-scope device array of 2048 doubles (16 KiB) that every
+ * GPU which loads the library holds until the process exits. At most
+ * 2^31 - 1 nodes (EMS_ERR_INVALID beyond). The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress, with the device current)
+ * and should come before any stream capture. All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+ems_status ems_energy_noalloc(const uint64_t nodes[3], double dt, const float* const u[3], const float* const i[3],
+                              const float* const coeff[12], double* energy, void* stream);
+
 /* Text of the last error of handle `h` ("" if none; a static text if h is NULL). */
 const char* ems_gpu_last_error(const ems_gpu* h);
 
