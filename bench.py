@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
-    ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels")
+    ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split")
     return ap.parse_args()
 
 
@@ -333,9 +333,11 @@ def run_ours(args):
 
     ab = algorithmic_bytes(w)
     peaks = measured_peaks()
-    # Dominant kernel: the fused step if it ran; else the H update of the
+    # Dominant kernel: the fused step if it ran; else the H update: of the
     # two-kernel schedule (H update, CPML H, magnetic poles: reads u, reads
-    # and writes i, reads and writes the H half of ψ).
+    # and writes i, reads and writes the H half of ψ), or the streaming H
+    # update of the split and per-operator schedules (reads u, reads and
+    # writes i: 36 B per cell).
     schedule = eng.schedule
     if kern[2][1] > 0:
         kname, (kms, kn) = "fused_step", kern[2]
@@ -361,7 +363,7 @@ def run_ours(args):
                           "achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peaks["hbm_gbs"], 4)},
         "kernels_ms": {("h_update", "e_update", "fused_step")[k]: {"ms": round(v[0], 3), "launches": v[1]}
                        for k, v in kern.items() if v[1]},
-        "schedule": {1: "per-operator kernels", 2: "fused single pass", 3: "two kernels"}[schedule],
+        "schedule": {1: "per-operator kernels", 2: "fused single pass", 3: "two kernels", 4: "split"}[schedule],
         "e2e": {"value": round(e2e, 1), "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8,
                 "steps": k_e2e},
         "gpu_launches": launches,

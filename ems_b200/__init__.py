@@ -532,7 +532,7 @@ class Engine:
 
     @property
     def schedule(self) -> int:
-        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels."""
+        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels, 4 split."""
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value

@@ -53,7 +53,7 @@ def _run(cmd: list[str]) -> None:
 
 def build_gpu(force: bool = False) -> str:
     srcs = [os.path.join(CSRC, f) for f in ("engine.cu", "noalloc.cu", "arith.cuh", "kernels.cuh", "fused.cuh", "separate.cuh",
-                                             "fused_tables.h")]
+                                             "split.cuh", "fused_tables.h")]
     srcs = [s for s in srcs if os.path.exists(s)] + [os.path.join(INCLUDE, "ems_gpu.h")]
     if force or _stale(GPU_LIB, srcs):
         tmp = GPU_LIB + ".tmp"

@@ -30,6 +30,7 @@
 #include "fused.cuh"
 #include "fused_tables.h"
 #include "separate.cuh"
+#include "split.cuh"
 
 #include <thread>
 #include <unordered_map>
@@ -123,6 +124,11 @@ struct ems_gpu {
     FusedParams fp{};               // everything but the field pointers and ψ_H parity
     std::vector<std::pair<float*, float*>> psi_h;  // ψ of each H slab: (current, other)
     std::vector<std::pair<int, int>> psi_h_at;     // its place in fp.slab[0][c][q]
+    // The split schedule: CPML layer shell segments per side (0 H, 1 E).
+    ShellDev shell[2] = {};
+    const uint32_t* run_of[2] = {nullptr, nullptr};  // per pole edge its run: electric, magnetic
+    double* qpartials = nullptr;    // energy shares of the split H update
+    size_t n_qpartials = 0;
     uint32_t* counter = nullptr;
     int* status = nullptr;
     double* fpartials = nullptr;
@@ -368,7 +374,8 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         P.row_runs = h->upload(T.row_runs.data(), T.row_runs.size());
         P.pj = pe_dev->j;
         P.pq = pe_dev->q;
-        if (!P.runs || !P.sets || !P.row_runs) return fail(h, EMS_ERR_NOMEM, "pole runs");
+        h->run_of[0] = h->upload(T.run_of.data(), T.run_of.size());
+        if (!P.runs || !P.sets || !P.row_runs || !h->run_of[0]) return fail(h, EMS_ERR_NOMEM, "pole runs");
     }
     if (T.has_poles_h) {
         P.has_poles_h = 1;
@@ -378,8 +385,29 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         P.pj_h = ph_dev->j;
         P.pq_h = ph_dev->q;
         P.prev_h = ph_dev->prev;
-        if (!P.runs_h || !P.sets_h || !P.row_runs_h) return fail(h, EMS_ERR_NOMEM, "pole runs");
+        h->run_of[1] = h->upload(T.h.run_of.data(), T.h.run_of.size());
+        if (!P.runs_h || !P.sets_h || !P.row_runs_h || !h->run_of[1]) return fail(h, EMS_ERR_NOMEM, "pole runs");
     }
+    if (g.nz >= (1u << 24)) {
+        h->tables_why = h->fused_why = "z rows of 2^24 nodes or more";
+        return EMS_OK;
+    }
+    for (int side = 0; side < 2; ++side) {
+        const ShellTables st = shell_tables(T.cmask, g.nx, g.ny, g.nz, side);
+        ShellDev& S = h->shell[side];
+        S = ShellDev{};
+        S.n_seg = (uint32_t)st.seg.size();
+        S.blocks_a = (S.n_seg + kShellWarps - 1) / kShellWarps;
+        S.n_b = (uint32_t)st.rows_b.size();
+        S.n_kz = (uint32_t)st.kz.size();
+        if (S.n_seg) S.seg = h->upload(st.seg.data(), st.seg.size());
+        if (S.n_b) S.rows_b = h->upload(st.rows_b.data(), st.rows_b.size());
+        if (S.n_kz) S.kz = h->upload(st.kz.data(), st.kz.size());
+        if ((S.n_seg && !S.seg) || (S.n_b && !S.rows_b) || (S.n_kz && !S.kz)) return fail(h, EMS_ERR_NOMEM, "CPML shell");
+    }
+    h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
+    h->qpartials = h->alloc<double>(h->n_qpartials);
+    if (!h->qpartials) return fail(h, EMS_ERR_NOMEM, "energy shares");
     h->n_spartials = (size_t)blocks_for(g.nz, kSepJ * kSeg) * blocks_for(g.ny, kSepK) * g.nx;
     h->spartials = h->alloc<double>(h->n_spartials);
     if (!h->spartials) return fail(h, EMS_ERR_NOMEM, "energy shares");
@@ -418,13 +446,16 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
     return EMS_OK;
 }
 
-// The schedule a step runs: 2 fused, 3 two kernels, 1 the per-operator kernels.
+// The schedule a step runs: 1 the per-operator kernels, 2 fused, 3 two
+// kernels, 4 split. Automatic: split, which measures fastest on B200, where
+// the tables allow it.
 int active_schedule(const ems_gpu* h) {
     switch (h->schedule) {
     case 1: return 1;
     case 2: return h->fused_ok ? 2 : (h->tables_ok ? 3 : 1);
     case 3: return h->tables_ok ? 3 : 1;
-    default: return h->fused_ok ? 2 : (h->tables_ok ? 3 : 1);
+    case 4: return h->tables_ok ? 4 : 1;
+    default: return h->tables_ok ? 4 : 1;
     }
 }
 
@@ -532,15 +563,38 @@ ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
     if (sch == 2) return run_step_fused(h, energy);
     if (sch == 3) return run_step_two(h, energy);
+    // Schedules 1 and 4 share the hook sequence; split (4) runs the table
+    // kernels of split.cuh for the updates and one shell kernel per CPML side.
+    const bool split = sch == 4;
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
     Coeffs c;
     for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
+    FusedParams P;
+    if (split) {
+        P = h->fp;
+        for (int a = 0; a < 3; ++a) {
+            P.uo[a] = P.un[a] = h->u[a];
+            P.io[a] = P.in[a] = h->i[a];
+        }
+        for (size_t q = 0; q < h->psi_h.size(); ++q) {
+            FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+            fs.psi_old = fs.psi_new = h->psi_h[q].first;
+        }
+        P.partials = h->qpartials;
+    }
     dim3 blk(kRowThreads, 1, 1);
     dim3 grd(blocks_for(g.nz, kRowThreads), (unsigned)g.ny, (unsigned)g.nx);
+    const dim3 qgrd(split_blocks_x(g), g.nx, 1);
     cudaEvent_t ev = h->prof_begin();
-    if (energy) {
+    if (split) {
+        if (energy) {
+            k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P);
+        } else {
+            k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P);
+        }
+    } else if (energy) {
         k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
     } else {
         k_update_h<false><<<grd, blk, 0, s>>>(g, f, c, nullptr);
@@ -548,12 +602,21 @@ ems_status run_step(ems_gpu* h, bool energy) {
     h->prof_end(0, ev);
     ++h->launches;
     if (energy) {
-        k_reduce_partials<<<1, 1024, 0, s>>>(h->partials, h->n_partials, h->d_energy);
+        if (split) {
+            k_reduce_partials<<<1, 1024, 0, s>>>(h->qpartials, h->n_qpartials, h->d_energy);
+        } else {
+            k_reduce_partials<<<1, 1024, 0, s>>>(h->partials, h->n_partials, h->d_energy);
+        }
         ++h->launches;
     }
     // Slab hooks after the H update, in registration order.
     for (auto& op : h->ops) {
-        if (op.kind == EMS_OP_CPML) {
+        if (op.kind == EMS_OP_CPML && split) {
+            if (const uint32_t nb = shell_blocks(h->shell[0])) {
+                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[0]);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_CPML) {
             for (const SlabDev& sd : op.cpml) {
                 if (sd.e_side) continue;
                 dim3 sg(blocks_for(sd.hi[2] - sd.lo[2], 64), (unsigned)(sd.hi[1] - sd.lo[1]), (unsigned)(sd.hi[0] - sd.lo[0]));
@@ -561,7 +624,11 @@ ems_status run_step(ems_gpu* h, bool energy) {
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_POLES) {
-            if (op.poles.h.n_edges) {
+            if (op.poles.h.n_edges && split) {
+                k_poles_runs<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, c, op.poles.h, P.runs_h, P.sets_h,
+                                                                                h->run_of[1], 0, h->dt);
+                ++h->launches;
+            } else if (op.poles.h.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.h, false, h->dt);
                 ++h->launches;
             }
@@ -576,11 +643,20 @@ ems_status run_step(ems_gpu* h, bool energy) {
     st = serial_pre_e(h, f);
     if (st) return st;
     ev = h->prof_begin();
-    k_update_e<<<grd, blk, 0, s>>>(g, f, c);
+    if (split) {
+        k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P);
+    } else {
+        k_update_e<<<grd, blk, 0, s>>>(g, f, c);
+    }
     h->prof_end(1, ev);
     ++h->launches;
     for (auto& op : h->ops) {
-        if (op.kind == EMS_OP_CPML) {
+        if (op.kind == EMS_OP_CPML && split) {
+            if (const uint32_t nb = shell_blocks(h->shell[1])) {
+                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[1]);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_CPML) {
             for (const SlabDev& sd : op.cpml) {
                 if (!sd.e_side) continue;
                 dim3 sg(blocks_for(sd.hi[2] - sd.lo[2], 64), (unsigned)(sd.hi[1] - sd.lo[1]), (unsigned)(sd.hi[0] - sd.lo[0]));
@@ -588,7 +664,11 @@ ems_status run_step(ems_gpu* h, bool energy) {
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_POLES) {
-            if (op.poles.e.n_edges) {
+            if (op.poles.e.n_edges && split) {
+                k_poles_runs<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, c, op.poles.e, P.runs, P.sets,
+                                                                                h->run_of[0], 1, h->dt);
+                ++h->launches;
+            } else if (op.poles.e.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.e, true, h->dt);
                 ++h->launches;
             }
@@ -1067,9 +1147,10 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 3) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 4) return EMS_ERR_INVALID;
     if (schedule == 2 && !h->fused_ok) return fail(h, EMS_ERR_INVALID, "fused schedule unavailable: " + h->fused_why);
     if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
+    if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
     h->schedule = schedule;
     return EMS_OK;
 }

@@ -82,6 +82,7 @@ struct PoleRuns {
     std::vector<PoleRun> runs;
     std::vector<double> sets;
     std::vector<uint4> row_runs;  // per (x*3 + axis)*ny + y: first run, count, z min, z end
+    std::vector<uint32_t> run_of; // per edge: its run
 };
 
 // The poles of one side as runs along z (edges are in (plane, axis, y, z)
@@ -134,6 +135,7 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
             R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, 0, pe->sum_inv_z[e]});
             R.row_runs[row_key].y++;
         }
+        R.run_of.push_back((uint32_t)R.runs.size() - 1);
         R.row_runs[row_key].w = (uint32_t)kk + 1;  // the row's edges are in z order
         last_row = row_key;
         last_k = (uint32_t)kk;
@@ -156,6 +158,7 @@ struct FusedTables {
     std::vector<PoleRun> runs;
     std::vector<double> sets;
     std::vector<uint4> row_runs;
+    std::vector<uint32_t> run_of;  // electric poles: per edge, its run
     PoleRuns h;                    // magnetic poles
 };
 
@@ -247,6 +250,7 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
         T.runs = std::move(R.runs);
         T.sets = std::move(R.sets);
         T.row_runs = std::move(R.row_runs);
+        T.run_of = std::move(R.run_of);
         T.has_poles = true;
     }
     if (poles && poles->magnetic.n_edges) {
@@ -258,6 +262,35 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
         T.has_poles_h = true;
     }
     return T;
+}
+
+// The CPML layer shell of one side (0 H, 1 E). Part A: the rows that an x or
+// y layer of the side holds, whole, as warp segments of at most 32 z-nodes
+// (row i*ny + j, first z | count << 24). Part B: every other row, each with
+// the z-indices that a z layer of the side holds (kz, shared by all rows).
+// Requires nz < 2^24.
+struct ShellTables {
+    std::vector<uint2> seg;
+    std::vector<uint32_t> rows_b;
+    std::vector<uint32_t> kz;
+};
+
+inline ShellTables shell_tables(const std::vector<uint32_t> cmask[3], uint32_t nx, uint32_t ny, uint32_t nz, int side) {
+    const uint32_t m = 0xfffu << (side * 12);
+    ShellTables S;
+    if (cmask[0].empty()) return S;
+    for (uint32_t k = 0; k < nz; ++k)
+        if (cmask[2][k] & m) S.kz.push_back(k);
+    for (uint32_t i = 0; i < nx; ++i)
+        for (uint32_t j = 0; j < ny; ++j) {
+            const uint32_t row = i * ny + j;
+            if ((cmask[0][i] | cmask[1][j]) & m) {
+                for (uint32_t k = 0; k < nz; k += 32) S.seg.push_back(uint2{row, k | (std::min(32u, nz - k) << 24)});
+            } else if (!S.kz.empty()) {
+                S.rows_b.push_back(row);
+            }
+        }
+    return S;
 }
 
 // Work items (row tile, x chunk): about eight per CTA of the persistent grid,

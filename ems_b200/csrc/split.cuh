@@ -1,0 +1,331 @@
+// split.cuh — the split step of the B200 FDTD engine (sm_100a).
+//
+// The H and E updates run as plain streaming kernels: four z-nodes per
+// thread in 16-byte loads and stores, nothing in them but the Yee update of
+// the three components, every load issued before any arithmetic and every
+// store after it, so a warp keeps all of its loads in flight at once. Coefficients come from the pooled
+// rows (a z-row's coefficient is one broadcast row id and one L2-resident
+// row); in the common case of a uniform background that makes each update
+// move 36 bytes per node (three components read, three read and written).
+//
+// The CPML correction of each side runs after its update as one kernel over
+// the layer shell, listed once at set-up: the rows inside an x or y layer as
+// warp segments of 32 z-nodes, every other row's z-layer nodes one per
+// thread; a node applies every slab that holds it in the slabs' order. Dispersive, lumped, source and probe hooks run as
+// in the per-operator schedule. All expressions are the reference's, so the
+// results equal it bit for bit.
+#pragma once
+
+#include "separate.cuh"
+
+namespace emsk {
+
+constexpr unsigned kSplitThreads = 128;  // quads (4 z-nodes) per block
+constexpr unsigned kShellWarps = 8;      // shell segments per block
+
+// Four consecutive z-nodes as registers (the element 4 of a 5-array is the
+// z-neighbour beyond them, or below them for the E update).
+struct Q4 {
+    float v[4];
+};
+__device__ __forceinline__ Q4 ldq(const float* p) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ Q4 ldq_rw(const float* p) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ void stq(float* p, const Q4& q) {
+    *reinterpret_cast<float4*>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+}
+__device__ __forceinline__ Q4 zq() { return Q4{{0.0f, 0.0f, 0.0f, 0.0f}}; }
+
+// The quad a thread owns: plane i = blockIdx.y; quad q of the plane's
+// ny·pitch/4 (rows are padded to a multiple of 32 floats, so a quad never
+// straddles two rows). False for a quad that lies beyond the plane or in
+// a row's padding.
+__device__ __forceinline__ bool quad_of(const Grid& g, uint32_t& j, uint32_t& k0) {
+    const uint32_t qpr = g.pitch >> 2;
+    const uint32_t q = blockIdx.x * kSplitThreads + threadIdx.x;
+    if (q >= g.ny * qpr) return false;
+    j = q / qpr;
+    k0 = (q - j * qpr) * 4u;
+    return k0 < g.nz;
+}
+
+// H update of every dual edge (src/engine/kernel.rs:447-511, 571-618), four
+// z-nodes per thread; with ENERGY each block writes its share of the energy
+// invariant in units of dt/4 (src/engine/kernel.rs:132-244). Entries the
+// update does not write (edges that do not exist, row padding) are stored
+// back as read. Grid: (quads of a plane / kSplitThreads, nx).
+template <bool ENERGY>
+__global__ void __launch_bounds__(kSplitThreads) k_split_h(const __grid_constant__ FusedParams P) {
+    const Grid& g = P.g;
+    const uint32_t i = blockIdx.y;
+    uint32_t j = 0, k0 = 0;
+    double w = 0.0;
+    if (quad_of(g, j, k0)) {
+        const uint32_t sj = g.pitch, si = g.ny * g.pitch;
+        const uint32_t idx = i * si + j * sj + k0;
+        const uint32_t row = i * g.ny + j;
+        const bool jn = j + 1 < g.ny, in_ = i + 1 < g.nx;
+        // Neighbour offsets; 0 where the neighbour does not exist (the value
+        // read is then unused).
+        const uint32_t oj = jn ? sj : 0u, oi = in_ ? si : 0u, o4 = k0 + 4 < g.nz ? 4u : 0u;
+        const Q4 ux = ldq(P.un[0] + idx), uy = ldq(P.un[1] + idx), uz = ldq(P.un[2] + idx);
+        const Q4 uzj = ldq(P.un[2] + idx + oj), uxj = ldq(P.un[0] + idx + oj);
+        const Q4 uzi = ldq(P.un[2] + idx + oi), uyi = ldq(P.un[1] + idx + oi);
+        const float uy4 = __ldg(P.un[1] + idx + o4), ux4 = __ldg(P.un[0] + idx + o4);
+        const Q4 hx = ldq_rw(P.in[0] + idx), hy = ldq_rw(P.in[1] + idx), hz = ldq_rw(P.in[2] + idx);
+        const Q4 dax = ldq(lane_row(P, 6, row) + k0), dbx = ldq(lane_row(P, 9, row) + k0);
+        const Q4 day = ldq(lane_row(P, 7, row) + k0), dby = ldq(lane_row(P, 10, row) + k0);
+        const Q4 daz = ldq(lane_row(P, 8, row) + k0), dbz = ldq(lane_row(P, 11, row) + k0);
+        Q4 nx_ = hx, ny_ = hy, nz_ = hz;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t k = k0 + e;
+            const bool kn = k + 1 < g.nz;
+            const float uy1 = e < 3 ? uy.v[e + 1] : uy4, ux1 = e < 3 ? ux.v[e + 1] : ux4;
+            if (jn && kn) nx_.v[e] = h_upd(dax.v[e], hx.v[e], dbx.v[e], uzj.v[e], uz.v[e], uy1, uy.v[e]);
+            if (in_ && kn) ny_.v[e] = h_upd(day.v[e], hy.v[e], dby.v[e], ux1, ux.v[e], uzi.v[e], uz.v[e]);
+            if (in_ && jn && k < g.nz) nz_.v[e] = h_upd(daz.v[e], hz.v[e], dbz.v[e], uyi.v[e], uy.v[e], uxj.v[e], ux.v[e]);
+        }
+        if (ENERGY) {
+            const Q4 ca0 = ldq(lane_row(P, 0, row) + k0), cb0 = ldq(lane_row(P, 3, row) + k0);
+            const Q4 ca1 = ldq(lane_row(P, 1, row) + k0), cb1 = ldq(lane_row(P, 4, row) + k0);
+            const Q4 ca2 = ldq(lane_row(P, 2, row) + k0), cb2 = ldq(lane_row(P, 5, row) + k0);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t k = k0 + e;
+                if (k >= g.nz) break;
+                const bool kn = k + 1 < g.nz;
+                const double x = ux.v[e], y = uy.v[e], z = uz.v[e];
+                w = __dadd_rn(w, weight(ca0.v[e], __dmul_rn(x, x), cb0.v[e]));
+                w = __dadd_rn(w, weight(ca1.v[e], __dmul_rn(y, y), cb1.v[e]));
+                w = __dadd_rn(w, weight(ca2.v[e], __dmul_rn(z, z), cb2.v[e]));
+                if (jn && kn) w = __dadd_rn(w, weight(dax.v[e], __dmul_rn((double)hx.v[e], (double)nx_.v[e]), dbx.v[e]));
+                if (in_ && kn) w = __dadd_rn(w, weight(day.v[e], __dmul_rn((double)hy.v[e], (double)ny_.v[e]), dby.v[e]));
+                if (in_ && jn) w = __dadd_rn(w, weight(daz.v[e], __dmul_rn((double)hz.v[e], (double)nz_.v[e]), dbz.v[e]));
+            }
+        }
+        if (jn) stq(P.in[0] + idx, nx_);
+        if (in_) stq(P.in[1] + idx, ny_);
+        if (in_ && jn) stq(P.in[2] + idx, nz_);
+    }
+    if (ENERGY) {
+        const double s = block_sum<kSplitThreads>(w);
+        if (threadIdx.x == 0) P.partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// E update of every edge (src/engine/kernel.rs:624-697), four z-nodes per
+// thread. Grid: (quads of a plane / kSplitThreads, nx).
+__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P) {
+    const Grid& g = P.g;
+    const uint32_t i = blockIdx.y;
+    uint32_t j = 0, k0 = 0;
+    if (!quad_of(g, j, k0)) return;
+    const uint32_t sj = g.pitch, si = g.ny * g.pitch;
+    const uint32_t idx = i * si + j * sj + k0;
+    const uint32_t row = i * g.ny + j;
+    const Q4 ix = ldq(P.in[0] + idx), iy = ldq(P.in[1] + idx), iz = ldq(P.in[2] + idx);
+    // Neighbours below the node; zero on the low faces (no edge there).
+    const Q4 izj = j > 0 ? ldq(P.in[2] + idx - sj) : zq(), ixj = j > 0 ? ldq(P.in[0] + idx - sj) : zq();
+    const Q4 izi = i > 0 ? ldq(P.in[2] + idx - si) : zq(), iyi = i > 0 ? ldq(P.in[1] + idx - si) : zq();
+    const float iym = k0 > 0 ? __ldg(P.in[1] + idx - 1) : 0.0f, ixm = k0 > 0 ? __ldg(P.in[0] + idx - 1) : 0.0f;
+    const Q4 ex = ldq_rw(P.un[0] + idx), ey = ldq_rw(P.un[1] + idx), ez = ldq_rw(P.un[2] + idx);
+    const Q4 cax = ldq(lane_row(P, 0, row) + k0), cbx = ldq(lane_row(P, 3, row) + k0);
+    const Q4 cay = ldq(lane_row(P, 1, row) + k0), cby = ldq(lane_row(P, 4, row) + k0);
+    const Q4 caz = ldq(lane_row(P, 2, row) + k0), cbz = ldq(lane_row(P, 5, row) + k0);
+    const bool xi = i + 1 < g.nx, yj = j + 1 < g.ny;
+    Q4 nx_ = ex, ny_ = ey, nz_ = ez;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const uint32_t k = k0 + e;
+        if (k >= g.nz) break;
+        const float iy0 = e > 0 ? iy.v[e - 1] : iym, ix0 = e > 0 ? ix.v[e - 1] : ixm;
+        if (xi) nx_.v[e] = e_upd(cax.v[e], ex.v[e], cbx.v[e], iz.v[e], izj.v[e], iy.v[e], iy0);
+        if (yj) ny_.v[e] = e_upd(cay.v[e], ey.v[e], cby.v[e], ix.v[e], ix0, iz.v[e], izi.v[e]);
+        if (k + 1 < g.nz) nz_.v[e] = e_upd(caz.v[e], ez.v[e], cbz.v[e], iy.v[e], iyi.v[e], ix.v[e], ixj.v[e]);
+    }
+    if (xi) stq(P.un[0] + idx, nx_);
+    if (yj) stq(P.un[1] + idx, ny_);
+    stq(P.un[2] + idx, nz_);
+}
+
+// Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.
+__host__ __device__ inline uint32_t split_blocks_x(const Grid& g) {
+    return (g.ny * (g.pitch >> 2) + kSplitThreads - 1) / kSplitThreads;
+}
+
+// The layer shell of one side, as the shell kernel reads it: part A, the
+// rows an x or y layer holds whole, as warp segments (row i*ny + j, first z |
+// count << 24); part B, every other row (rows_b) times the z-indices a z
+// layer holds (kz), one thread per node.
+struct ShellDev {
+    const uint2* seg;
+    uint32_t n_seg, blocks_a;
+    const uint32_t* rows_b;
+    const uint32_t* kz;
+    uint32_t n_b, n_kz;
+};
+
+// The CPML chain of one field value: every slab of component C on side
+// SIDE whose bit is set and which holds the node, in order (the arithmetic
+// of cpml_body, inline).
+template <int SIDE, int C>
+__device__ __forceinline__ float shell_chain(const FusedParams& P, uint32_t bits, uint32_t i, uint32_t j, uint32_t k,
+                                             float t, float coef, float sA, float sB) {
+    constexpr uint32_t na = (C + 1) % 3;
+    uint32_t m = (bits >> (SIDE * 12 + C * 4)) & 15u;
+    while (m) {
+        const int q = __ffs(m) - 1;
+        m &= m - 1;
+        const FSlab& s = P.slab[SIDE][C][q];
+        if (i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1] || k < s.lo[2] || k >= s.hi[2]) continue;
+        const uint32_t d = s.normal == 0 ? i - s.lo[0] : (s.normal == 1 ? j - s.lo[1] : k - s.lo[2]);
+        const uint32_t at = ((i - s.lo[0]) * (s.hi[1] - s.lo[1]) + (j - s.lo[1])) * (s.hi[2] - s.lo[2]) + (k - s.lo[2]);
+        const float sv = s.normal == na ? sA : sB;
+        const float psi = flush(__fadd_rn(__fmul_rn(__ldg(s.b + d), s.psi_old[at]), __fmul_rn(__ldg(s.a + d), sv)));
+        s.psi_new[at] = psi;
+        t = flush(__fadd_rn(t, __fmul_rn(coef, __fadd_rn(__fmul_rn(__ldg(s.k + d), sv), psi))));
+    }
+    return t;
+}
+
+// CPML correction of the node (i, j, k) on one side (0: H edges after the
+// H update, 1: E edges after the E update) (src/engine/boundary/cpml.rs:
+// 445-520, 657-676). The curl differences are those of the update: A along
+// next(c), B along prev(c); a slab takes s = A or −B by its normal.
+template <int SIDE>
+__device__ __forceinline__ void shell_node(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k) {
+    const Grid& g = P.g;
+    const uint32_t bits = P.cmask[0][i] | P.cmask[1][j] | P.cmask[2][k];
+    const uint32_t sb = bits >> (SIDE * 12);  // this side's bits: component c at 4c
+    if (!(sb & 0xfffu)) return;
+    const uint32_t sj = g.pitch, si = g.ny * g.pitch;
+    const uint32_t idx = i * si + j * sj + k, row = i * g.ny + j;
+    if (SIDE == 0) {
+        const float *ux = P.un[0], *uy = P.un[1], *uz = P.un[2];
+        if ((sb & 0xfu) && j + 1 < g.ny && k + 1 < g.nz) {
+            const float A = __fsub_rn(uz[idx + sj], uz[idx]), B = __fsub_rn(uy[idx + 1], uy[idx]);
+            const float db = lane_row(P, 9, row)[k];
+            P.in[0][idx] = shell_chain<0, 0>(P, bits, i, j, k, P.in[0][idx], -db, A, __fmul_rn(-1.0f, B));
+        }
+        if ((sb & 0xf0u) && i + 1 < g.nx && k + 1 < g.nz) {
+            const float A = __fsub_rn(ux[idx + 1], ux[idx]), B = __fsub_rn(uz[idx + si], uz[idx]);
+            const float db = lane_row(P, 10, row)[k];
+            P.in[1][idx] = shell_chain<0, 1>(P, bits, i, j, k, P.in[1][idx], -db, A, __fmul_rn(-1.0f, B));
+        }
+        if ((sb & 0xf00u) && i + 1 < g.nx && j + 1 < g.ny) {
+            const float A = __fsub_rn(uy[idx + si], uy[idx]), B = __fsub_rn(ux[idx + sj], ux[idx]);
+            const float db = lane_row(P, 11, row)[k];
+            P.in[2][idx] = shell_chain<0, 2>(P, bits, i, j, k, P.in[2][idx], -db, A, __fmul_rn(-1.0f, B));
+        }
+    } else {
+        const float *ix = P.in[0], *iy = P.in[1], *iz = P.in[2];
+        if ((sb & 0xfu) && i + 1 < g.nx) {
+            const float A = __fsub_rn(iz[idx], j > 0 ? iz[idx - sj] : 0.0f);
+            const float B = __fsub_rn(iy[idx], k > 0 ? iy[idx - 1] : 0.0f);
+            const float cb = lane_row(P, 3, row)[k];
+            P.un[0][idx] = shell_chain<1, 0>(P, bits, i, j, k, P.un[0][idx], cb, A, __fmul_rn(-1.0f, B));
+        }
+        if ((sb & 0xf0u) && j + 1 < g.ny) {
+            const float A = __fsub_rn(ix[idx], k > 0 ? ix[idx - 1] : 0.0f);
+            const float B = __fsub_rn(iz[idx], i > 0 ? iz[idx - si] : 0.0f);
+            const float cb = lane_row(P, 4, row)[k];
+            P.un[1][idx] = shell_chain<1, 1>(P, bits, i, j, k, P.un[1][idx], cb, A, __fmul_rn(-1.0f, B));
+        }
+        if ((sb & 0xf00u) && k + 1 < g.nz) {
+            const float A = __fsub_rn(iy[idx], i > 0 ? iy[idx - si] : 0.0f);
+            const float B = __fsub_rn(ix[idx], j > 0 ? ix[idx - sj] : 0.0f);
+            const float cb = lane_row(P, 5, row)[k];
+            P.un[2][idx] = shell_chain<1, 2>(P, bits, i, j, k, P.un[2][idx], cb, A, __fmul_rn(-1.0f, B));
+        }
+    }
+}
+
+// CPML correction of one side over its layer shell: blocks [0, blocks_a)
+// take part A (one warp per segment), the rest part B (one thread per node).
+template <int SIDE>
+__global__ void __launch_bounds__(32 * kShellWarps) k_shell(const __grid_constant__ FusedParams P,
+                                                            const __grid_constant__ ShellDev S) {
+    const Grid& g = P.g;
+    uint32_t row, k;
+    if (blockIdx.x < S.blocks_a) {
+        const uint32_t w = blockIdx.x * kShellWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+        if (w >= S.n_seg) return;
+        const uint2 sg = S.seg[w];
+        if (lane >= (sg.y >> 24)) return;
+        row = sg.x;
+        k = (sg.y & 0xffffffu) + lane;
+    } else {
+        const uint32_t t = (blockIdx.x - S.blocks_a) * (32 * kShellWarps) + threadIdx.x;
+        if (t >= S.n_b * S.n_kz) return;
+        const uint32_t r = t / S.n_kz;
+        row = S.rows_b[r];
+        k = S.kz[t - r * S.n_kz];
+    }
+    const uint32_t i = row / g.ny;
+    shell_node<SIDE>(P, i, row - i * g.ny, k);
+}
+
+// Blocks of the shell kernel for a side.
+__host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
+    const uint32_t tb = 32 * kShellWarps;
+    return S.blocks_a + (uint32_t)(((uint64_t)S.n_b * S.n_kz + tb - 1) / tb);
+}
+
+// Dispersive correction of one side, one edge per thread, the constants
+// read from the edge's run (shared by consecutive edges of a row with equal
+// poles) instead of per pole (src/engine/dispersive.rs:1392-1470). A
+// leapfrog pole's new state does not depend on the corrected value and is
+// stored at once; a trapezoidal pole's is formed from its old state after it.
+__global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
+                                                    const __grid_constant__ PoleSideDev p, const PoleRun* runs,
+                                                    const double* sets, const uint32_t* run_of, int electric,
+                                                    double dt) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n_edges) return;
+    const PoleRun R = runs[run_of[e]];
+    const uint32_t p0 = R.p0 + (e - R.e0) * R.np;
+    const int ax = p.axis[e];
+    const uint32_t idx = p.node[e];
+    float* fld = electric ? f.u[ax] : f.i[ax];
+    const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
+    const double prev = (double)p.prev[e];
+    const double half_prev = __dmul_rn(0.5, prev);
+    const double u_star = (double)fld[idx];
+    const double* cs = sets + R.set;
+    double s = 0.0;
+    for (uint32_t q = 0; q < R.np; ++q) {
+        const double a = cs[3 * q], ic = cs[3 * q + 1], iz = cs[3 * q + 2];
+        const double jq = p.j[p0 + q], qq = p.q[p0 + q];
+        if ((R.kinds >> q) & 1u) {
+            const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
+            p.j[p0 + q] = jn;
+            p.q[p0 + q] = __dadd_rn(qq, __dmul_rn(dt, jn));
+            s = __dadd_rn(s, jn);
+        } else {
+            s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
+        }
+    }
+    const float u_new = (float)__ddiv_rn(__dsub_rn(u_star, __dmul_rn(cb, s)),
+                                         __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
+    if (R.kinds != (1u << R.np) - 1u) {
+        const double half_new = __dmul_rn(0.5, (double)u_new);
+        for (uint32_t q = 0; q < R.np; ++q) {
+            if ((R.kinds >> q) & 1u) continue;
+            const double a = cs[3 * q], ic = cs[3 * q + 1], iz = cs[3 * q + 2];
+            const double jq = p.j[p0 + q], qq = p.q[p0 + q];
+            const double kk = __dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev);
+            const double jb = __dmul_rn(__dadd_rn(kk, half_new), iz);
+            p.j[p0 + q] = __dsub_rn(__dmul_rn(2.0, jb), jq);
+            p.q[p0 + q] = __dadd_rn(qq, __dmul_rn(dt, jb));
+        }
+    }
+    fld[idx] = u_new;
+}
+
+}  // namespace emsk

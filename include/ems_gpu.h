@@ -267,14 +267,15 @@ ems_status ems_gpu_stream(const ems_gpu* h, void** stream);
 ems_status ems_gpu_profile(ems_gpu* h, int enable);
 ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* launches);
 
-/* Selects the step schedule: 0 = automatic (the best one the model
+/* Selects the step schedule: 0 = automatic (the fastest one the model
  * allows), 1 = one kernel per field update and operator, 2 = the fused
  * single-pass kernel, 3 = two kernels (H with its slab hooks, E with its
- * slab hooks). Results are identical bit for bit. Asking for a schedule the
- * model cannot run returns EMS_ERR_INVALID. */
+ * slab hooks), 4 = split (streaming H and E updates, one CPML shell kernel
+ * per side, the other hooks per operator). Results are identical bit for
+ * bit. Asking for a schedule the model cannot run returns EMS_ERR_INVALID. */
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 
-/* The schedule steps run with (1, 2 or 3 as above). */
+/* The schedule steps run with (1 to 4 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
 #ifdef __cplusplus

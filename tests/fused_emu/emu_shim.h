@@ -57,6 +57,8 @@ inline double __dsub_rn(double a, double b) { return a - b; }
 inline double __ddiv_rn(double a, double b) { return a / b; }
 inline uint32_t min(uint32_t a, uint32_t b) { return a < b ? a : b; }
 inline int __ffs(uint32_t x) { return __builtin_ffs((int)x); }
+template <class T>
+inline T __ldg(const T* p) { return *p; }
 
 inline unsigned atomicAdd(uint32_t* p, uint32_t v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
 inline int atomicExch(int* p, int v) { return __atomic_exchange_n(p, v, __ATOMIC_SEQ_CST); }

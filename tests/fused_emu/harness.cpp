@@ -17,6 +17,7 @@ void fail(const char* what) {
 #include "../../ems_b200/csrc/fused.cuh"
 #include "../../ems_b200/csrc/fused_tables.h"
 #include "../../ems_b200/csrc/separate.cuh"
+#include "../../ems_b200/csrc/split.cuh"
 
 using namespace emsk;
 
@@ -321,6 +322,138 @@ extern "C" int emu_two_run(const ems_engine_desc* d, uint64_t steps, float** fie
                 const uint64_t k = idx % g.nz, r = idx / g.nz;
                 prev_h[e] = buf[3 + mside->axis[e]][r * g.pitch + k];
             }
+    }
+    for (int c = 0; c < 6; ++c)
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
+            std::memcpy(fields[c] + r * g.nz, &buf[c][r * g.pitch], g.nz * 4);
+    return 0;
+}
+
+// Runs a kernel body over a grid (gx, gy, gz) of blocks of (bx, by) threads,
+// one host thread per CUDA thread. False (and g_err set) on a shim error.
+template <class F>
+static bool emu_launch(unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsigned by, F body) {
+    blockDim = EmuDim{bx, by, 1};
+    gridDim = EmuDim{gx, gy, gz};
+    for (unsigned z = 0; z < gz; ++z)
+        for (unsigned y = 0; y < gy; ++y)
+            for (unsigned x = 0; x < gx; ++x) {
+                blockIdx = EmuDim{x, y, z};
+                emu::Block blk;
+                std::barrier<> bar((std::ptrdiff_t)(bx * by));
+                blk.bar = &bar;
+                blk.sums.assign(bx * by, 0.0);
+                emu::cur = &blk;
+                std::vector<std::thread> th;
+                for (unsigned ty = 0; ty < by; ++ty)
+                    for (unsigned tx = 0; tx < bx; ++tx)
+                        th.emplace_back([&, tx, ty] {
+                            threadIdx.x = tx;
+                            threadIdx.y = ty;
+                            body();
+                        });
+                for (auto& t : th) t.join();
+                emu::cur = nullptr;
+                if (blk.errors.load()) {
+                    std::snprintf(g_err, sizeof g_err, "%s", blk.msg);
+                    return false;
+                }
+            }
+    return true;
+}
+
+// Runs `steps` steps of the split schedule (split.cuh: streaming H and E
+// updates, one CPML shell kernel per side) from the fields given in reference
+// layout (overwritten with the result); models without dispersive media,
+// lumped elements or sources (those hooks are the per-operator kernels).
+extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** fields, double* energies) {
+    g_err[0] = 0;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE) {
+            std::snprintf(g_err, sizeof g_err, "only CPML and probes are emulated");
+            return 1;
+        }
+    Grid g{};
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "not eligible: %s", T.why.c_str());
+        return 1;
+    }
+    auto pad = [&](const float* src, std::vector<float>& dst) {
+        dst.assign(g.np, 0.0f);
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r) std::memcpy(&dst[r * g.pitch], src + r * g.nz, g.nz * 4);
+    };
+    std::vector<float> buf[6];
+    for (int c = 0; c < 6; ++c) pad(fields[c], buf[c]);
+    std::vector<float> dense[12];
+    FusedParams P{};
+    P.g = g;
+    P.dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (T.lane[l].pooled) {
+            P.lane[l].rid = T.lane[l].rid.data();
+            P.lane[l].rows = T.lane[l].rows.data();
+        } else {
+            pad(d->coeff[l], dense[l]);
+            P.lane[l].dense = dense[l].data();
+        }
+    }
+    std::vector<std::vector<float>> psi;
+    psi.reserve(T.slabs.size());
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    for (const FusedSlabSpec& sp : T.slabs) {
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = (uint32_t)sp.src->lo[a];
+            f.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        f.normal = (uint32_t)sp.src->normal;
+        f.b = sp.src->b;
+        f.a = sp.src->a;
+        f.k = sp.src->k;
+        psi.emplace_back(sp.len, 0.0f);
+        f.psi_old = f.psi_new = psi.back().data();
+    }
+    for (int a = 0; a < 3; ++a) P.cmask[a] = T.cmask[a].data();
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = P.un[a] = buf[a].data();
+        P.io[a] = P.in[a] = buf[3 + a].data();
+    }
+    ShellTables st[2];
+    ShellDev sd[2];
+    for (int side = 0; side < 2; ++side) {
+        st[side] = shell_tables(T.cmask, g.nx, g.ny, g.nz, side);
+        sd[side] = ShellDev{st[side].seg.data(), (uint32_t)st[side].seg.size(),
+                            (uint32_t)((st[side].seg.size() + kShellWarps - 1) / kShellWarps), st[side].rows_b.data(),
+                            st[side].kz.data(), (uint32_t)st[side].rows_b.size(), (uint32_t)st[side].kz.size()};
+    }
+    const unsigned gx = split_blocks_x(g);
+    std::vector<double> partials((size_t)gx * g.nx, 0.0);
+    P.partials = partials.data();
+    auto shell = [&](int side) -> bool {
+        const uint32_t blocks = shell_blocks(sd[side]);
+        if (!blocks) return true;
+        const ShellDev S = sd[side];
+        return side ? emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<1>(P, S); })
+                    : emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<0>(P, S); });
+    };
+    for (uint64_t s = 0; s < steps; ++s) {
+        bool ok = energies ? emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<true>(P); })
+                           : emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P); });
+        if (!ok || !shell(0)) return 2;
+        if (energies) {
+            double w = 0.0;
+            for (double x : partials) w += x;
+            energies[s] = 0.25 * d->dt * w;
+        }
+        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P); }) || !shell(1)) return 2;
     }
     for (int c = 0; c < 6; ++c)
         for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)

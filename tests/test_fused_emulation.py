@@ -31,6 +31,8 @@ def emu_lib(asan=False):
     lib.emu_fused_run.argtypes = [C.c_void_p, C.c_int, C.c_uint, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_two_run.restype = C.c_int
     lib.emu_two_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_split_run.restype = C.c_int
+    lib.emu_split_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_error.restype = C.c_char_p
     return lib
 
@@ -141,6 +143,25 @@ def test_two_kernel_energy_equals_oracle():
     np.testing.assert_allclose(eg, eo, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("n,graded", [((10, 9, 12), False), ((12, 11, 35), True), ((9, 14, 40), False)])
+def test_split_source_equals_oracle(n, graded):
+    """The split schedule's update and CPML shell kernels: fields bit-exact,
+    energy within 1e-12 (a sum in another order)."""
+    m = model(n, E.TRAPEZOIDAL, poles=False, graded=graded)
+    state = random_state(m, seed=3)
+    steps = 6
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    en = np.zeros(steps)
+    lib = emu_lib()
+    assert lib.emu_split_run(m.desc, steps, ptrs, en.ctypes.data) == 0, lib.emu_error().decode()
+    want, eo, _ = run_oracle(m, state, steps)
+    for name, a, b in zip(["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"], arrs, want):
+        bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])}"
+    np.testing.assert_allclose(en, eo, rtol=1e-12, atol=0)
+
+
 def test_fused_kernel_source_under_address_sanitizer():
     """The same emulation built with AddressSanitizer: no out-of-bounds access
     of any table, field, state or shared-memory buffer."""
@@ -159,6 +180,10 @@ def test_fused_kernel_source_under_address_sanitizer():
         "st = [np.ascontiguousarray(x) for x in T.random_state(m2)]\n"
         "p = (C.c_void_p * 6)(*[a.ctypes.data for a in st])\n"
         "assert T.emu_lib(asan=True).emu_two_run(m2.desc, 4, p, None) == 0\n"
+        "m3 = T.model((10, 9, 12), E.TRAPEZOIDAL, poles=False)\n"
+        "st = [np.ascontiguousarray(x) for x in T.random_state(m3)]\n"
+        "p = (C.c_void_p * 6)(*[a.ctypes.data for a in st])\n"
+        "assert T.emu_lib(asan=True).emu_split_run(m3.desc, 3, p, None) == 0\n"
         "print('clean')\n"
     ) % (HERE, os.path.dirname(HERE))
     env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")

@@ -64,10 +64,11 @@ def test_lossy_cavity_bit_exact():
 
 
 @pytest.mark.parametrize("scheme", [E.TRAPEZOIDAL, E.LEAPFROG])
-@pytest.mark.parametrize("schedule", [1, 3])
+@pytest.mark.parametrize("schedule", [1, 3, 4])
 def test_every_operator_bit_exact(scheme, schedule):
     """Every operator at once (magnetic poles and an H source included), on
-    the per-operator kernels (1) and the two-kernel schedule (3)."""
+    the per-operator kernels (1), the two-kernel schedule (3) and the split
+    schedule (4)."""
     m, ops = mixed_model(scheme=scheme, steps=240)
     g, o, eg, eo = _lockstep(m, 240, energy_every=20, schedule=schedule)
     assert g.schedule == schedule
@@ -84,10 +85,10 @@ def test_fused_schedule_bit_exact(scheme):
     """Without magnetic poles and H sources the fused single-pass kernel
     runs; it must equal the separate kernels and the oracle bit for bit."""
     m, ops = mixed_model(scheme=scheme, magnetic=False, h_source=False, steps=240)
-    g, o, eg, eo = _lockstep(m, 240, energy_every=20)
+    g, o, eg, eo = _lockstep(m, 240, energy_every=20, schedule=2)
     assert g.schedule == 2
     assert_fields_equal(g, o, f"fused vs oracle, scheme {scheme}")
-    for sch in (1, 3):
+    for sch in (1, 3, 4):
         s = E.Engine(m)
         s.set_schedule(sch)
         assert s.schedule == sch
@@ -103,9 +104,13 @@ def test_fused_schedule_bit_exact(scheme):
 def test_two_kernel_schedule_where_fused_cannot_run():
     m, _ = mixed_model(magnetic=True, steps=10)
     g = E.Engine(m)
+    assert g.schedule == 4
+    g.set_schedule(3)
     assert g.schedule == 3
     with pytest.raises(E.EngineError):
         g.set_schedule(2)
+    with pytest.raises(E.EngineError):
+        g.set_schedule(5)
 
 
 def test_odd_sizes_and_tile_remainders():
@@ -126,7 +131,7 @@ def test_vacuum_box_configuration_bit_exact():
     4 E_z probes; fields and probe series bit-exact."""
     w = W.vacuum_box()
     g, o, _, _ = _lockstep(w.model, w.steps, threads=0)
-    assert g.schedule == 2
+    assert g.schedule == 4
     for p in w.probes:
         _series_equal(g, o, p)
     assert_fields_equal(g, o, "vacuum box")
@@ -135,7 +140,7 @@ def test_vacuum_box_configuration_bit_exact():
 def test_dispersive_box_small_bit_exact():
     w = W.dispersive_box(n=48, radius=8, slab=4, cpml=5, steps=300)
     g, o, eg, eo = _lockstep(w.model, 300, energy_every=30)
-    assert g.schedule == 2
+    assert g.schedule == 4
     assert_fields_equal(g, o, "dispersive box")
     for p in w.probes:
         _series_equal(g, o, p)
@@ -178,7 +183,7 @@ def test_invalid_tables_rejected():
 
 
 @pytest.mark.parametrize("n", [40, 67])
-@pytest.mark.parametrize("schedule", [2, 3])
+@pytest.mark.parametrize("schedule", [2, 3, 4])
 def test_dispersive_box_chunks_and_tiles(n, schedule):
     """Sizes whose rows, tiles and x chunks leave remainders."""
     w = W.dispersive_box(n=n, radius=n / 6, slab=3, cpml=4, steps=120)
