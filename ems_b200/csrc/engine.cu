@@ -127,6 +127,12 @@ struct ems_gpu {
     // The split schedule: CPML layer shell segments per side (0 H, 1 E).
     ShellDev shell[2] = {};
     const uint32_t* run_of[2] = {nullptr, nullptr};  // per pole edge its run: electric, magnetic
+    // The split schedule's pole kernels store the corrected value as the
+    // saved value of the side (electric, magnetic) instead of a capture
+    // kernel (pole_prev_fold); the electric one is current only after a split
+    // step with no field upload since.
+    bool fold_prev[2] = {false, false};
+    bool prev_e_valid = false;
     double* qpartials = nullptr;    // energy shares of the split H update
     size_t n_qpartials = 0;
     uint32_t* counter = nullptr;
@@ -405,6 +411,8 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         if (S.n_kz) S.kz = h->upload(st.kz.data(), st.kz.size());
         if ((S.n_seg && !S.seg) || (S.n_b && !S.rows_b) || (S.n_kz && !S.kz)) return fail(h, EMS_ERR_NOMEM, "CPML shell");
     }
+    h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
+    h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);
     h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
     h->qpartials = h->alloc<double>(h->n_qpartials);
     if (!h->qpartials) return fail(h, EMS_ERR_NOMEM, "energy shares");
@@ -561,6 +569,8 @@ ems_status run_step_two(ems_gpu* h, bool energy) {
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
+    // Only the per-operator and split steps keep the electric saved values.
+    if (sch != 4) h->prev_e_valid = false;
     if (sch == 2) return run_step_fused(h, energy);
     if (sch == 3) return run_step_two(h, energy);
     // Schedules 1 and 4 share the hook sequence; split (4) runs the table
@@ -626,13 +636,14 @@ ems_status run_step(ems_gpu* h, bool energy) {
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.h.n_edges && split) {
                 k_poles_runs<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, c, op.poles.h, P.runs_h, P.sets_h,
-                                                                                h->run_of[1], 0, h->dt);
+                                                                                h->run_of[1], 0, h->dt,
+                                                                                h->fold_prev[1] ? 1 : 0);
                 ++h->launches;
             } else if (op.poles.h.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.h, false, h->dt);
                 ++h->launches;
             }
-            if (op.poles.e.n_edges) {
+            if (op.poles.e.n_edges && !(split && h->fold_prev[0] && h->prev_e_valid)) {
                 k_poles_capture<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, op.poles.e, true);
                 ++h->launches;
             }
@@ -666,13 +677,14 @@ ems_status run_step(ems_gpu* h, bool energy) {
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.e.n_edges && split) {
                 k_poles_runs<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, c, op.poles.e, P.runs, P.sets,
-                                                                                h->run_of[0], 1, h->dt);
+                                                                                h->run_of[0], 1, h->dt,
+                                                                                h->fold_prev[0] ? 1 : 0);
                 ++h->launches;
             } else if (op.poles.e.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.e, true, h->dt);
                 ++h->launches;
             }
-            if (op.poles.h.n_edges) {
+            if (op.poles.h.n_edges && !(split && h->fold_prev[1])) {
                 k_poles_capture<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, op.poles.h, false);
                 ++h->launches;
             }
@@ -680,6 +692,7 @@ ems_status run_step(ems_gpu* h, bool energy) {
     }
     st = serial_post_e(h, f);
     if (st) return st;
+    if (split) h->prev_e_valid = h->fold_prev[0];
     ++h->step;
     return EMS_OK;
 }
@@ -1040,6 +1053,7 @@ ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* ho
     if (!h || !host || field < 0 || field > 1 || axis < 0 || axis > 2) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     const Grid& g = h->g;
+    if (field == 0) h->prev_e_valid = false;  // the saved electric values are captured again
     // Both buffers of a double-buffered field get the values (the padding
     // entries the kernels read as zero stay equal in both).
     float* dsts[2] = {field == 0 ? h->u[axis] : h->i[axis], field == 0 ? h->u2[axis] : h->i2[axis]};

@@ -53,6 +53,8 @@ struct PoleRun {
     uint32_t np;       // poles per edge
     uint32_t kinds;    // bit q set: pole q is a leapfrog pole
     uint32_t e0;       // edge index of the run's first edge (in the side's table)
+    uint32_t axis;     // the edges' axis
+    uint32_t node0;    // padded node index of the run's first edge
     uint32_t pad;
     double sum_inv_z;
 };

@@ -88,7 +88,8 @@ struct PoleRuns {
 // The poles of one side as runs along z (edges are in (plane, axis, y, z)
 // order): consecutive edges of one row with the same constants share a run.
 // Returns "" or why the side cannot be held as runs.
-inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, uint32_t nz, PoleRuns& R) {
+inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t pitch,
+                             PoleRuns& R) {
     std::unordered_map<std::string, uint32_t> set_of;
     R.row_runs.assign((size_t)nx * 3 * ny, uint4{0, 0, 0, 0});
     uint64_t last_row = ~0ull;
@@ -132,7 +133,8 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
             R.runs.back().ke = (uint32_t)kk + 1;
         } else {
             if (row_key != last_row) R.row_runs[row_key] = uint4{(uint32_t)R.runs.size(), 0, (uint32_t)kk, 0};
-            R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, 0, pe->sum_inv_z[e]});
+            R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, (uint32_t)pe->axis[e],
+                                     (uint32_t)((ii * ny + jj) * pitch + kk), 0, pe->sum_inv_z[e]});
             R.row_runs[row_key].y++;
         }
         R.run_of.push_back((uint32_t)R.runs.size() - 1);
@@ -242,7 +244,7 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
     T.poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
     if (poles && poles->electric.n_edges) {
         PoleRuns R;
-        std::string w = pole_runs(&poles->electric, nx, ny, nz, R);
+        std::string w = pole_runs(&poles->electric, nx, ny, nz, pitch, R);
         if (!w.empty()) {
             T.why = T.fused_why = w;
             return T;
@@ -254,7 +256,7 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
         T.has_poles = true;
     }
     if (poles && poles->magnetic.n_edges) {
-        std::string w = pole_runs(&poles->magnetic, nx, ny, nz, T.h);
+        std::string w = pole_runs(&poles->magnetic, nx, ny, nz, pitch, T.h);
         if (!w.empty()) {
             T.why = T.fused_why = w;
             return T;
@@ -291,6 +293,70 @@ inline ShellTables shell_tables(const std::vector<uint32_t> cmask[3], uint32_t n
             }
         }
     return S;
+}
+
+// Whether a side's dispersive correction may store its corrected value as
+// the edge's saved field value, in place of the capture the reference makes
+// one hook later (E edges: after the next H update; H edges: after the E
+// update; src/engine/dispersive.rs:1173-1180, 1730-1744). True when nothing
+// that runs between the correction and that capture writes a pole edge of
+// the side: no lumped element or source of that field on one, and, when the
+// CPML hooks run after the dispersive ones, no CPML slab of that side over
+// one. The side's edges are in (plane, axis, row, z) order, so membership is
+// a binary search.
+inline bool pole_prev_fold(const ems_engine_desc* d, bool electric, bool poles_first) {
+    const ems_pole_side* ps = nullptr;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind == EMS_OP_POLES) {
+            const auto* p = (const ems_poles*)d->ops[k].table;
+            ps = electric ? &p->electric : &p->magnetic;
+        }
+    if (!ps || !ps->n_edges) return false;
+    const uint64_t ny = d->nodes[1], nz = d->nodes[2];
+    auto key = [&](uint64_t node, uint64_t axis) {
+        const uint64_t k = node % nz, r = node / nz, j = r % ny, i = r / ny;
+        return ((i * 3 + axis) * ny + j) * nz + k;
+    };
+    auto is_pole_edge = [&](uint64_t node, uint64_t axis) {
+        const uint64_t want = key(node, axis);
+        size_t lo = 0, hi = ps->n_edges;
+        while (lo < hi) {
+            const size_t mid = lo + (hi - lo) / 2;
+            const uint64_t k = key(ps->node[mid], ps->axis[mid]);
+            if (k == want) return true;
+            if (k < want) lo = mid + 1;
+            else hi = mid;
+        }
+        return false;
+    };
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        const int kind = d->ops[k].kind;
+        if (kind == EMS_OP_LUMPED && electric) {
+            const auto* l = (const ems_lumped*)d->ops[k].table;
+            for (size_t e = 0; e < l->n_edges; ++e)
+                if (is_pole_edge(l->node[e], (uint64_t)l->axis)) return false;
+        } else if (kind == EMS_OP_SOURCE) {
+            const auto* sr = (const ems_source*)d->ops[k].table;
+            const bool e_src = sr->kind == EMS_SOFT_E || sr->kind == EMS_HARD_E;
+            if (e_src != electric) continue;
+            for (size_t e = 0; e < sr->n_edges; ++e)
+                if (is_pole_edge(sr->node[e], sr->axis[e])) return false;
+        } else if (kind == EMS_OP_CPML && poles_first) {
+            const auto* c = (const ems_cpml*)d->ops[k].table;
+            for (size_t q = 0; q < c->n_slabs; ++q) {
+                const ems_cpml_slab& sl = c->slabs[q];
+                if ((sl.e_side != 0) != electric) continue;
+                for (size_t e = 0; e < ps->n_edges; ++e) {
+                    if ((int)ps->axis[e] != sl.comp) continue;
+                    const uint64_t n = ps->node[e], kk = n % nz, r = n / nz, jj = r % ny, ii = r / ny;
+                    if (ii >= sl.lo[0] && ii < sl.hi[0] && jj >= sl.lo[1] && jj < sl.hi[1] && kk >= sl.lo[2] &&
+                        kk < sl.hi[2])
+                        return false;
+                }
+            }
+        }
+    }
+    return true;
 }
 
 // Work items (row tile, x chunk): about eight per CTA of the persistent grid,

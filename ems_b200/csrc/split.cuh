@@ -60,7 +60,7 @@ __device__ __forceinline__ bool quad_of(const Grid& g, uint32_t& j, uint32_t& k0
 // update does not write (edges that do not exist, row padding) are stored
 // back as read. Grid: (quads of a plane / kSplitThreads, nx).
 template <bool ENERGY>
-__global__ void __launch_bounds__(kSplitThreads) k_split_h(const __grid_constant__ FusedParams P) {
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P) {
     const Grid& g = P.g;
     const uint32_t i = blockIdx.y;
     uint32_t j = 0, k0 = 0;
@@ -282,16 +282,18 @@ __host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
 // poles) instead of per pole (src/engine/dispersive.rs:1392-1470). A
 // leapfrog pole's new state does not depend on the corrected value and is
 // stored at once; a trapezoidal pole's is formed from its old state after it.
+// save_prev: also store the corrected value as the edge's saved value (the
+// capture it replaces would read the same value; pole_prev_fold).
 __global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
                                                     const __grid_constant__ PoleSideDev p, const PoleRun* runs,
                                                     const double* sets, const uint32_t* run_of, int electric,
-                                                    double dt) {
+                                                    double dt, int save_prev) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= p.n_edges) return;
     const PoleRun R = runs[run_of[e]];
     const uint32_t p0 = R.p0 + (e - R.e0) * R.np;
-    const int ax = p.axis[e];
-    const uint32_t idx = p.node[e];
+    const int ax = (int)R.axis;
+    const uint32_t idx = R.node0 + (e - R.e0);
     float* fld = electric ? f.u[ax] : f.i[ax];
     const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
     const double prev = (double)p.prev[e];
@@ -326,6 +328,7 @@ __global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fiel
         }
     }
     fld[idx] = u_new;
+    if (save_prev) p.prev[e] = u_new;
 }
 
 }  // namespace emsk

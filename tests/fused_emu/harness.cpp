@@ -460,3 +460,15 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
             std::memcpy(fields[c] + r * g.nz, &buf[c][r * g.pitch], g.nz * 4);
     return 0;
 }
+
+// pole_prev_fold of fused_tables.h for a model (1: the side's pole kernel
+// may store its saved values itself).
+extern "C" int emu_pole_prev_fold(const ems_engine_desc* d, int electric) {
+    int pos_cpml = -1, pos_poles = -1;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        if (d->ops[k].kind == EMS_OP_CPML) pos_cpml = (int)k;
+        if (d->ops[k].kind == EMS_OP_POLES) pos_poles = (int)k;
+    }
+    const bool poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
+    return pole_prev_fold(d, electric != 0, poles_first) ? 1 : 0;
+}

@@ -20,6 +20,8 @@ import ems_b200 as E
 from ems_b200 import workloads as W
 from oracle import OracleEngine
 
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -33,6 +35,8 @@ def emu_lib(asan=False):
     lib.emu_two_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_split_run.restype = C.c_int
     lib.emu_split_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_pole_prev_fold.restype = C.c_int
+    lib.emu_pole_prev_fold.argtypes = [C.c_void_p, C.c_int]
     lib.emu_error.restype = C.c_char_p
     return lib
 
@@ -160,6 +164,40 @@ def test_split_source_equals_oracle(n, graded):
         bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
         assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])}"
     np.testing.assert_allclose(en, eo, rtol=1e-12, atol=0)
+
+
+def test_pole_capture_fold_decision():
+    """The split schedule lets a pole kernel store the saved field values
+    itself only when nothing between the correction and the reference's
+    capture writes a pole edge: a source on a pole edge, or CPML applied after
+    the dispersive hooks over a pole edge, keeps the capture kernel."""
+    from helpers import mixed_model
+
+    lib = emu_lib()
+    m, _ = mixed_model(h_source=True)  # soft E source at the sphere's centre, soft H in the magnetic box
+    assert lib.emu_pole_prev_fold(m.desc, 1) == 0
+    assert lib.emu_pole_prev_fold(m.desc, 0) == 0
+    m, _ = mixed_model(h_source=False)
+    assert lib.emu_pole_prev_fold(m.desc, 1) == 0
+    assert lib.emu_pole_prev_fold(m.desc, 0) == 1
+    w = W.dispersive_box(n=40, radius=6, slab=3, cpml=4, steps=10)
+    assert lib.emu_pole_prev_fold(w.model.desc, 1) == 1
+    assert lib.emu_pole_prev_fold(w.model.desc, 0) == 0  # no magnetic poles
+    # Dispersive medium registered before the CPML, its slab through the layers.
+    m = E.Model.uniform([16, 16, 16], [1e-3] * 3)
+    m.build()
+    d = E.Dispersive()
+    d.fill_cells(m, m.cells().box([0, 0, 6], [16, 16, 9]), [E.Pole.drude(6e10, 6e9)])
+    m.add_dispersive(d, E.LEAPFROG)
+    m.add_cpml([3] * 6)
+    assert lib.emu_pole_prev_fold(m.desc, 1) == 0
+    m = E.Model.uniform([16, 16, 16], [1e-3] * 3)
+    m.build()
+    d = E.Dispersive()
+    d.fill_cells(m, m.cells().box([6, 6, 6], [9, 9, 9]), [E.Pole.drude(6e10, 6e9)])
+    m.add_dispersive(d, E.LEAPFROG)
+    m.add_cpml([3] * 6)
+    assert lib.emu_pole_prev_fold(m.desc, 1) == 1
 
 
 def test_fused_kernel_source_under_address_sanitizer():

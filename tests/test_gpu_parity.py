@@ -191,3 +191,43 @@ def test_dispersive_box_chunks_and_tiles(n, schedule):
     assert g.schedule == schedule
     assert_fields_equal(g, o, f"dispersive {n}")
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_split_saved_values_across_uploads_and_schedule_switches():
+    """The split schedule's pole kernels store the saved field values
+    themselves where that is exact; a field upload or a step on another
+    schedule makes the next split step capture them again."""
+    w = W.dispersive_box(n=40, radius=6, slab=3, cpml=4, steps=200)
+    m = w.model
+    g = E.Engine(m)
+    o = OracleEngine(m, threads=4)
+    assert g.schedule == 4
+    rng = np.random.default_rng(5)
+    for sch, n in ((4, 25), (1, 7), (4, 9), (3, 5), (4, 11)):
+        g.set_schedule(sch)
+        g.run(n)
+        o.run(n)
+        if sch == 4:
+            v = (rng.standard_normal(m.nodes) * 1e-3).astype(np.float32)
+            g.set_field(0, 0, v)
+            o.set_field(0, 0, v)
+    g.set_schedule(4)
+    g.run(30)
+    o.run(30)
+    assert_fields_equal(g, o, "split with uploads and switches")
+    for p in w.probes:
+        _series_equal(g, o, p)
+
+
+@pytest.mark.parametrize("h_source", [True, False])
+def test_split_magnetic_poles(h_source):
+    """Magnetic poles on the split schedule, with (capture kernel) and
+    without (saved values stored by the pole kernel) an H source on a pole
+    edge."""
+    m, ops = mixed_model(scheme=E.LEAPFROG, h_source=h_source, steps=160)
+    g, o, eg, eo = _lockstep(m, 160, energy_every=16, schedule=4)
+    assert g.schedule == 4
+    assert_fields_equal(g, o, f"split, magnetic poles, H source {h_source}")
+    for which in (0, 1, 2):
+        _series_equal(g, o, ops["port"], which)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
