@@ -1,0 +1,536 @@
+"""The oracle against the reference's own known-answer tests.
+
+The oracle (a C++ restatement of the reference step) is the checker of the
+CUDA engine; these tests pin it to the answers the reference's own test
+suite holds for the engine, restated on the oracle with the same models,
+sources, probes and thresholds:
+
+* PEC cavity resonances on uniform, graded and anisotropic-dielectric grids
+  (tests/engine.rs:1-188);
+* the lossless energy invariant, lossy decay at κ/ε0, and the run loop's
+  energy-decay stop (tests/engine.rs:189-410);
+* determinism across thread counts (tests/engine.rs:412-520);
+* CPML reflection at normal incidence (uniform, graded, CFS, dielectric
+  background), a 3-D point source, and late-time stability
+  (tests/cpml.rs:1-300);
+* energy conservation, dissipation, boundedness and thread determinism with
+  dispersive poles (tests/validation_dispersive.rs:377-562).
+
+They run on the CPU (the oracle only), so they are not marked gpu.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import ems_b200 as E
+from helpers import graded, pulse, soft_e_table, small_cavity
+from oracle import OracleEngine
+
+C0 = E.c0()
+EPS0 = E.eps0()
+
+
+# --------------------------------------------------------------------------
+# Spectral helpers of tests/engine.rs:25-70.
+
+def spectrum(times, values, t_start, f):
+    """|DFT| at f of the Hann-windowed samples with t >= t_start (engine.rs:25-38)."""
+    first = int(np.argmax(times >= t_start))
+    t, v = times[first:], values[first:]
+    n = len(t)
+    w = 0.5 - 0.5 * np.cos(2.0 * math.pi * np.arange(n) / (n - 1.0))
+    ph = -2.0 * math.pi * f * t
+    return float(np.hypot(np.sum(w * v * np.cos(ph)), np.sum(w * v * np.sin(ph))))
+
+
+def peak(times, values, t_start, lo, hi):
+    """Spectral peak in [lo, hi]: coarse scan, golden-section refinement (engine.rs:40-64)."""
+    s = lambda f: spectrum(times, values, t_start, f)  # noqa: E731
+    n = 200
+    step = (hi - lo) / n
+    best = max(range(n + 1), key=lambda q: s(lo + q * step))
+    a, b = lo + (best - 1) * step, lo + (best + 1) * step
+    g = (math.sqrt(5.0) - 1.0) / 2.0
+    for _ in range(60):
+        c = b - g * (b - a)
+        d = a + g * (b - a)
+        if s(c) > s(d):
+            b = d
+        else:
+            a = c
+    f = 0.5 * (a + b)
+    return f, s(f)
+
+
+DIMS = (0.10, 0.045, 0.07)
+
+
+def cavity_freq(m, n, p, eps_r):
+    return C0 / (2.0 * math.sqrt(eps_r)) * math.sqrt((m / DIMS[0]) ** 2 + (n / DIMS[1]) ** 2 + (p / DIMS[2]) ** 2)
+
+
+def run_cavity(lines, eps_r, steps, scale):
+    """tests/engine.rs:92-136: E_y source near (0.3a, 0.3b, 0.4c), E_y probe
+    near (0.7a, 0.5b, 0.6c), pulse(3.2 GHz·scale, 2.5 GHz·scale)."""
+    m = E.Model(*lines)
+    if eps_r is not None:
+        m.fill(m.cells().box([0, 0, 0], [len(l) - 1 for l in lines]), m.material(eps_r=eps_r))
+    m.build()
+    nearest = lambda a, x: int(np.argmin(np.abs(np.asarray(lines[a]) - x)))  # noqa: E731
+    src = (nearest(0, 0.3 * DIMS[0]), nearest(1, 0.3 * DIMS[1]), nearest(2, 0.4 * DIMS[2]))
+    prb = (nearest(0, 0.7 * DIMS[0]), nearest(1, 0.5 * DIMS[1]), nearest(2, 0.6 * DIMS[2]))
+    f, t_end = pulse(3.2e9 * scale, 2.5e9 * scale)
+    m.add_source_table(E.SOFT_E, [(E.Y, src, 1.0)], soft_e_table(f, m.dt, steps))
+    p = m.add_probe(E.VOLTAGE, [(E.Y, prb, 1.0)])
+    o = OracleEngine(m, threads=4)
+    o.run(steps)
+    v = o.samples(p)
+    times = (np.arange(len(v)) + 1.0) * m.dt  # voltage samples at (n+1)·dt
+    return times, v, t_end
+
+
+def check_modes(times, values, t_start, eps_r, tol):
+    """tests/engine.rs:138-158: modes (1,0,1) and (2,0,1) within tol, clear peaks."""
+    for mnp in ((1.0, 0.0, 1.0), (2.0, 0.0, 1.0)):
+        fa = cavity_freq(*mnp, eps_r)
+        f, mag = peak(times, values, t_start, 0.95 * fa, 1.05 * fa)
+        err = (f - fa) / fa
+        assert abs(err) < tol, f"mode {mnp} off by {100 * err:.3f}%"
+        assert 0.96 * fa < f < 1.04 * fa
+        off = spectrum(times, values, t_start, 0.9 * fa)
+        assert mag > 20.0 * off, f"no clear peak for {mnp}"
+
+
+def test_pec_cavity_uniform():
+    d = 0.005
+    lines = [np.arange(n + 1) * d for n in (20, 9, 14)]
+    t, v, t0 = run_cavity(lines, None, 3000, 1.0)
+    check_modes(t, v, t0, 1.0, 0.005)
+
+
+def test_pec_cavity_graded():
+    lines = [graded(DIMS[0], 22, 0.3), graded(DIMS[1], 10, 0.2), graded(DIMS[2], 16, 0.3)]
+    t, v, t0 = run_cavity(lines, None, 4000, 1.0)
+    check_modes(t, v, t0, 1.0, 0.005)
+
+
+def test_dielectric_cavity_scales():
+    """Only E_y exists in the (m, 0, p) modes: an anisotropic fill with
+    ε_y = 2.25 scales them by 1/1.5 (tests/engine.rs:178-188)."""
+    d = 0.005
+    lines = [np.arange(n + 1) * d for n in (20, 9, 14)]
+    t, v, t0 = run_cavity(lines, (4.0, 2.25, 9.0), 4500, 1.0 / 1.5)
+    check_modes(t, v, t0, 2.25, 0.005)
+
+
+# --------------------------------------------------------------------------
+# Energy invariant (tests/engine.rs:205-320).
+
+def invariant_drift(o, dt, t_end, steps, interval):
+    """Runs past the source, then samples W every `interval` steps; the
+    largest |W/W0 − 1| (tests/engine.rs:205-230)."""
+    o.run(int(math.ceil(t_end / dt)) + 1)
+    w0 = o.step_with_energy()
+    assert w0 > 0.0
+    o.run(interval - 1)
+    dev = 0.0
+    for _ in range(steps // interval - 1):
+        w = o.step_with_energy()
+        dev = max(dev, abs(w / w0 - 1.0))
+        o.run(interval - 1)
+    return dev
+
+
+def test_lossless_energy_conserved_uniform():
+    m, t_end = small_cavity()
+    o = OracleEngine(m, threads=2)
+    dev = invariant_drift(o, m.dt, t_end, 10_000, 10)
+    assert dev < 1e-4, f"lossless invariant drifted by {dev:e}"
+
+
+def test_lossless_energy_conserved_graded_dielectric():
+    """tests/engine.rs:253-280: graded grid, dielectric and anisotropic
+    magnetic blocks, a PEC box, a PMC y_max face."""
+    m = E.Model(graded(0.1, 15, 0.3), graded(0.07, 11, 0.2), graded(0.05, 9, 0.25))
+    m.fill(m.cells().box([3, 2, 1], [9, 8, 6]), m.material(eps_r=4.0))
+    m.fill(m.cells().box([9, 0, 4], [14, 11, 9]), m.material(eps_r=(2.0, 3.0, 1.5), mu_r=1.5))
+    m.fill_pec_box([11, 3, 2], [12, 8, 7])
+    m.faces([E.PEC, E.PEC, E.PEC, E.PMC, E.PEC, E.PEC])
+    m.build()
+    f, t_end = pulse(3e9, 2e9)
+    n = int(math.ceil(t_end / m.dt)) + 4
+    m.add_source_table(E.SOFT_E, [(E.Z, (5, 4, 3), 1.0), (E.Y, (10, 5, 6), 0.7)], soft_e_table(f, m.dt, n))
+    o = OracleEngine(m, threads=3)
+    dev = invariant_drift(o, m.dt, t_end, 8000, 50)
+    assert dev < 1e-4, f"lossless invariant drifted by {dev:e}"
+
+
+def test_lossy_energy_decays_at_kappa_over_eps0():
+    """tests/engine.rs:282-320: W non-increasing, decay rate κ/ε0 within 2 %."""
+    kappa = 0.002
+    m, t_end = small_cavity(kappa=kappa)
+    o = OracleEngine(m, threads=2)
+    dt = m.dt
+    o.run(int(math.ceil(t_end / dt)) + 1)
+    step = int(math.ceil(t_end / dt)) + 1
+    prev = o.step_with_energy()
+    step += 1
+    w1, t1 = prev, (step - 1) * dt
+    for _ in range(500):
+        w = o.step_with_energy()
+        step += 1
+        assert w <= prev, f"lossy energy grew: {prev} -> {w}"
+        prev = w
+
+    def avg():
+        nonlocal step
+        s = 0.0
+        for _ in range(100):
+            s += o.step_with_energy()
+            step += 1
+        return s / 100.0, step * dt - 50.5 * dt
+
+    wa, ta = avg()
+    o.run(400)
+    step += 400
+    wb, tb = avg()
+    assert wb < wa < w1 and t1 < ta
+    rate = math.log(wa / wb) / (tb - ta)
+    want = kappa / EPS0
+    assert abs(rate / want - 1.0) < 0.02, f"decay rate {rate} vs {want}"
+
+
+def test_run_until_energy_decay_stops_at_the_predicted_time():
+    """tests/engine.rs:322-375: −30 dB energy decay checked every 20 steps
+    stops where the free decay W(t) = W(ta)·exp(−κ/ε0·(t − ta)) crosses
+    ratio·W_max."""
+    kappa = 0.002
+    m, t_end = small_cavity(kappa=kappa)
+    o = OracleEngine(m, threads=2)
+    db = -30.0
+    lim = E.energy_decay_limits(100_000, db, m.dt, excitation_end=t_end, interval=20)
+    trace = []
+
+    class Rec:
+        """The oracle, recording (time, energy) at each check."""
+
+        def __init__(self):
+            self.n = 0
+
+        def run(self, n):
+            o.run(n)
+            self.n += n
+
+        def step_with_energy(self):
+            w = o.step_with_energy()
+            trace.append((self.n * m.dt, w))
+            self.n += 1
+            return w
+
+    r = Rec()
+    out = E.run_until(r, lim)
+    assert out.reason == 0, out.reason  # energy decay
+    assert db - 1.0 < out.ratio_db < db
+    assert out.energy / out.max_energy < lim.energy_ratio
+    w_max = max(w for _, w in trace)
+    assert out.max_energy == w_max
+    # The deciding check is the last one; the first check after the excitation.
+    ta, wa = next((t, w) for t, w in trace if t > t_end)
+    t_stop = trace[-1][0]
+    rate = kappa / EPS0
+    want = ta + math.log(wa / (lim.energy_ratio * w_max)) / rate
+    window = 0.01 * (want - ta) + 20.0 * m.dt
+    assert abs(t_stop - want) < window, (t_stop, want, window)
+
+
+def test_run_until_max_timesteps():
+    """tests/engine.rs:377-395: lossless, so the run hits max_timesteps."""
+    m, t_end = small_cavity()
+    o = OracleEngine(m, threads=2)
+    lim = E.energy_decay_limits(1234, -60.0, m.dt, excitation_end=t_end)
+    out = E.run_until(o, lim)
+    assert out.reason == 1 and out.steps == 1234
+    assert 0.0 < out.energy <= out.max_energy
+
+
+# --------------------------------------------------------------------------
+# Determinism across threads (tests/engine.rs:460-500).
+
+def _det_model():
+    m = E.Model(graded(0.1, 13, 0.2), graded(0.08, 9, 0.1), graded(0.06, 7, 0.0))
+    m.fill(m.cells().box([2, 1, 2], [6, 5, 6]), m.material(eps_r=3.0, kappa=0.02))
+    m.fill(m.cells().box([7, 0, 0], [12, 9, 3]), m.material(mu_r=2.0, sigma_m=50.0))
+    m.fill_pec_box([9, 2, 1], [10, 7, 6])
+    m.faces([E.PEC, E.PMC, E.PEC, E.PEC, E.PMC, E.PEC])
+    m.build(courant=0.95)
+    f, _ = pulse(5e9, 4e9)
+    m.add_source_table(E.SOFT_E, [(E.Z, (4, 4, 3), 1.0)], soft_e_table(f, m.dt, 300))
+    p = m.add_probe(E.CURRENT, [(E.X, (5, 3, 3), 1.0)], interval=3)
+    return m, p
+
+
+def test_deterministic_across_threads():
+    m, p = _det_model()
+    runs = []
+    for t in (1, 2, 3, 4):
+        o = OracleEngine(m, threads=t)
+        o.run(300)
+        arrays = [o.field(f, a).view(np.uint32).copy() for f in (0, 1) for a in range(3)]
+        runs.append((arrays, o.samples(p).view(np.uint64).copy(), o.step_with_energy()))
+    a1, p1, w1 = runs[0]
+    assert w1 > 0.0
+    for a, pv, w in runs[1:]:
+        for x, y in zip(a1, a):
+            assert np.array_equal(x, y)
+        assert np.array_equal(p1, pv)
+        assert w == w1
+
+
+# --------------------------------------------------------------------------
+# CPML (tests/cpml.rs).
+
+DZ = 1e-3
+
+
+def sine_pulse(f0, bw):
+    """tests/cpml.rs:16-24 (the same pulse as tests/engine.rs, without t_end)."""
+    return pulse(f0, bw)[0]
+
+
+def dgauss(tau):
+    """Derivative-of-Gaussian pulse (tests/cpml.rs:26-34)."""
+    t0 = 4.0 * tau
+
+    def f(t):
+        x = (t - t0) / tau
+        return -2.0 * x * np.exp(-x * x)
+
+    return f
+
+
+def db(x):
+    return 20.0 * math.log10(x)
+
+
+def rel_err(a, b):
+    """max |a − b| / max |b| (tests/cpml.rs:40-50)."""
+    assert len(a) == len(b)
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def line_run(z, eps_r, pml, lead, src, prb, steps):
+    """Quasi-1-D TEM line along z (tests/cpml.rs:57-95): one 10 mm cell in x
+    and y, PEC x walls, PMC y walls; `pml` = (cells, kwargs) on both z faces."""
+    m = E.Model([0.0, 0.01], [0.0, 0.01], z)
+    m.faces([E.PEC, E.PEC, E.PMC, E.PMC, E.PEC, E.PEC])
+    nz = len(z) - 1
+    m.fill(m.cells().box([0, 0, 0], [1, 1, nz]), m.material(eps_r=eps_r))
+    m.build()
+    if pml is not None:
+        cells, kw = pml
+        m.add_cpml([0, 0, 0, 0, cells, cells], **kw)
+    f = sine_pulse(10e9 / math.sqrt(eps_r), 10e9 / math.sqrt(eps_r))
+    ks = lead + src
+    m.add_source_table(E.SOFT_E, [(E.X, (0, 0, ks), 1.0), (E.X, (0, 1, ks), 1.0)], soft_e_table(f, m.dt, steps))
+    p = m.add_probe(E.VOLTAGE, [(E.X, (0, 0, lead + prb), 1.0)])
+    o = OracleEngine(m, threads=1)
+    o.run(steps)
+    return o.samples(p)
+
+
+def normal_reflection(pml_cells, eps_r=1.0, **kw):
+    """Reflection from a CPML of the given cell sizes (interface outwards)
+    against a long PEC-ended reference line (tests/cpml.rs:97-128)."""
+    n = len(pml_cells)
+    interior, src, prb = 150, 30, 100
+    z = [0.0]
+    for d in reversed(pml_cells):
+        z.append(z[-1] + d)
+    zi = z[-1]
+    z.extend(zi + DZ * np.arange(1, interior + 1))
+    for d in pml_cells:
+        z.append(z[-1] + d)
+    steps = int(900.0 * math.sqrt(eps_r))
+    test = line_run(np.array(z), eps_r, (n, kw), n, src, prb, steps)
+    pad = 1000
+    zr = np.arange(interior + 2 * pad + 1) * DZ
+    ref = line_run(zr, eps_r, None, pad, src, prb, steps)
+    return rel_err(test, ref)
+
+
+def test_cpml_normal_incidence_uniform():
+    r = normal_reflection([DZ] * 8)
+    assert db(r) < -70.0, f"reflection {db(r):.1f} dB"
+    r0 = normal_reflection([DZ] * 8, sigma_factor=0.0)
+    assert db(r0) > -1.0, f"window misses the echo: {db(r0):.1f} dB"
+
+
+def test_cpml_normal_incidence_graded_mesh():
+    r = normal_reflection([DZ * 1.25 ** q for q in range(8)])
+    assert db(r) < -45.0, f"graded 1.25x: {db(r):.1f} dB"
+    r = normal_reflection([DZ * 1.1 ** q for q in range(8)])
+    assert db(r) < -50.0, f"graded 1.1x: {db(r):.1f} dB"
+
+
+def test_cpml_normal_incidence_cfs():
+    r = normal_reflection([DZ] * 8, kappa_max=3.0, alpha_max=0.02)
+    assert db(r) < -60.0, f"reflection {db(r):.1f} dB"
+
+
+@pytest.mark.parametrize("eps", [4.0, 12.0])
+def test_cpml_normal_incidence_dielectric_background(eps):
+    """σ_max is tuned to the layer's index: as good as in vacuum, and better
+    than the vacuum σ_max by more than 3 dB (tests/cpml.rs:159-178)."""
+    r = normal_reflection([DZ] * 8, eps_r=eps)
+    assert db(r) < -80.0, f"eps_r {eps}: {db(r):.1f} dB"
+    v = normal_reflection([DZ] * 8, eps_r=eps, sigma_factor=math.sqrt(eps))
+    assert db(v) > db(r) + 3.0, (db(v), db(r))
+
+
+def box_run(interior, pml, cpml_kw, probes, steps):
+    """tests/cpml.rs:180-218: cubic box of 2 mm cells, E_z derivative-of-
+    Gaussian soft source at the centre, E_z probes at offsets."""
+    d = 2e-3
+    n = interior + 2 * pml
+    m = E.Model.uniform([n] * 3, [d] * 3)
+    m.build()
+    if cpml_kw is not None:
+        m.add_cpml([pml] * 6, **cpml_kw)
+    c = n // 2
+    m.add_source_table(E.SOFT_E, [(E.Z, (c, c, c), 1.0)], soft_e_table(dgauss(25e-12), m.dt, steps))
+    ps = [m.add_probe(E.VOLTAGE, [(E.Z, tuple(c + v for v in o), 1.0)]) for o in probes]
+    o = OracleEngine(m, threads=4)
+    o.run(steps)
+    return [o.samples(p) for p in ps]
+
+
+def test_cpml_point_source_3d():
+    """tests/cpml.rs:220-265: 12³ interior + 8-cell CPML against a box with
+    22 cells of padding, 80 steps: every probe below −60 dB; a lossless layer
+    shows in the window (above −25 dB)."""
+    interior, steps, pad = 12, 80, 22
+    h = interior // 2
+    probes = [(h - 3, 0, 0), (h - 3, h - 3, 0), (h - 3, h - 3, h - 4)]
+    ref = box_run(interior, pad, None, probes, steps)
+    test = box_run(interior, 8, {}, probes, steps)
+    errs = [rel_err(t, r) for t, r in zip(test, ref)]
+    assert all(db(e) < -60.0 for e in errs), [db(e) for e in errs]
+    lossless = box_run(interior, 8, {"sigma_factor": 0.0}, probes, steps)
+    errs = [rel_err(t, r) for t, r in zip(lossless, ref)]
+    assert all(db(e) > -25.0 for e in errs), [db(e) for e in errs]
+
+
+def test_cpml_energy_decays_and_stays_small():
+    """tests/cpml.rs:267-300: interior 2 cells + CPML 3 per face, 20 000
+    steps: W after 1000 steps below 1e-5·W_max, no late-time growth."""
+    p, interior, steps = 3, 2, 20_000
+    n = interior + 2 * p
+    m = E.Model.uniform([n] * 3, [2e-3] * 3)
+    m.build()
+    m.add_cpml([p] * 6)
+    c = n // 2
+    m.add_source_table(E.SOFT_E, [(E.Z, (c, c, c), 1.0)], soft_e_table(dgauss(25e-12), m.dt, 1000))
+    o = OracleEngine(m, threads=1)
+    w_max = 0.0
+    for _ in range(400):
+        w_max = max(w_max, o.step_with_energy())
+    o.run(600)
+    w1 = o.step_with_energy()
+    assert w1 < 1e-5 * w_max, (w1, w_max)
+    o.run(steps - 1001)
+    w2 = o.step_with_energy()
+    assert math.isfinite(w2) and w2 <= max(w1, 1e-12 * w_max), (w1, w2)
+
+
+# --------------------------------------------------------------------------
+# Dispersive media (tests/validation_dispersive.rs:377-531).
+
+def _disp_cavity(lossless, magnetic, threads=1):
+    """tests/validation_dispersive.rs:377-425: 10×8×6 cells of 1 mm, a
+    block of ε 1.5 with a Lorentz, a Drude and a Debye electric pole (and a
+    magnetic Lorentz pole), four nodes of u set to 1..4; trapezoidal (the
+    engine's default scheme)."""
+    m = E.Model.uniform([10, 8, 6], [1e-3] * 3)
+    m.fill(m.cells().box([2, 1, 1], [8, 6, 5]), m.material(eps_r=1.5))
+    m.build()
+    gam = 0.0 if lossless else 3e9
+    w = 2.0 * math.pi * 20e9
+    d = E.Dispersive()
+    d.fill_cells(m, m.cells().box([2, 1, 1], [8, 6, 5]),
+                 [E.Pole.lorentz(w, w, gam), E.Pole.drude(0.7 * w, gam), E.Pole.debye(2.0, 0.0 if lossless else 5e-12)])
+    if magnetic:
+        d.fill_cells(m, m.cells().box([2, 1, 1], [8, 6, 5]), [E.Pole.lorentz(0.5 * w, 1.5 * w, gam)], field=1)
+    m.add_dispersive(d, E.TRAPEZOIDAL)
+    o = OracleEngine(m, threads=threads)
+    for q, n in enumerate([(3, 3, 2), (5, 2, 3), (1, 4, 2), (6, 5, 3)]):
+        u = o.field(0, q % 3)
+        u[n] = 1.0 + q
+        o.set_field(0, q % 3, u)
+    return m, o
+
+
+def _energy_drift(steps, magnetic):
+    """(max − min)/W0 of W sampled every 50 steps after 10 (validation_dispersive.rs:431-447)."""
+    _, o = _disp_cavity(True, magnetic)
+    o.run(10)
+    w0 = o.step_with_energy()
+    lo = hi = w0
+    for _ in range(steps // 50):
+        o.run(49)
+        w = o.step_with_energy()
+        lo, hi = min(lo, w), max(hi, w)
+    return (hi - lo) / w0
+
+
+@pytest.mark.parametrize("magnetic", [False, True])
+def test_lossless_poles_conserve_energy(magnetic):
+    """Lossless Lorentz + Drude + Debye(τ = 0) block (and magnetic Lorentz
+    poles): field plus pole energy conserved to 1e-5 over 4000 steps
+    (validation_dispersive.rs:449-476)."""
+    drift = _energy_drift(4000, magnetic)
+    assert drift < 1e-5, drift
+
+
+def test_lossy_poles_dissipate():
+    """validation_dispersive.rs:487-503: never increases, halves in 2000 steps."""
+    _, o = _disp_cavity(False, False)
+    o.run(2)
+    w = w0 = o.step_with_energy()
+    for _ in range(200):
+        o.run(9)
+        wn = o.step_with_energy()
+        assert wn <= w * (1.0 + 1e-6), (wn, w)
+        w = wn
+    assert w < 0.5 * w0
+
+
+@pytest.mark.parametrize("lossless", [True, False])
+def test_magnetic_poles_stay_bounded(lossless):
+    """validation_dispersive.rs:505-530: bounded within 5 %, non-increasing with losses."""
+    _, o = _disp_cavity(lossless, True)
+    o.run(2)
+    w0 = w = o.step_with_energy()
+    wmax = 0.0
+    for _ in range(60):
+        o.run(49)
+        wn = o.step_with_energy()
+        if not lossless:
+            assert wn <= w * (1.0 + 1e-6), (wn, w)
+        w = wn
+        wmax = max(wmax, wn)
+    assert wmax < 1.05 * w0, (wmax, w0)
+
+
+def test_dispersive_deterministic_across_threads():
+    """validation_dispersive.rs:532-562: 1 and 4 threads bit-identical with
+    electric and magnetic poles crossing the slab boundaries."""
+    out = []
+    for t in (1, 4):
+        _, o = _disp_cavity(False, True, threads=t)
+        o.run(300)
+        out.append([o.field(f, a).view(np.uint32).copy() for f in (0, 1) for a in range(3)])
+    for x, y in zip(*out):
+        assert np.array_equal(x, y)
