@@ -88,6 +88,16 @@ class Stepper(C.Structure):
     ]
 
 
+class BatchStepper(C.Structure):
+    _fields_ = [
+        ("ctx", C.c_void_p),
+        ("n_models", C.c_size_t),
+        ("run", C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)),
+        ("step_with_energy", C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double))),
+        ("set_active", C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_int)),
+    ]
+
+
 class RunLimits(C.Structure):
     """``RunLimits`` (src/engine/run.rs:24-53) for :func:`run_until`."""
 
@@ -170,6 +180,7 @@ def host_lib() -> C.CDLL:
             "ems_model_desc": (p, [p]),
             "ems_dft": (None, [d, d, p, sz, p, sz, p, p]),
             "ems_drive": (i, [p, p, p]),
+            "ems_batch_drive": (i, [p, p, p]),
             "ems_const_eps0": (d, []),
             "ems_const_mu0": (d, []),
             "ems_const_c0": (d, []),
@@ -202,6 +213,17 @@ GPU_SYMBOLS = {
     "ems_gpu_source_amplitude": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p, C.c_size_t]),
     "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
+    "ems_batch_destroy": (C.c_int, [C.c_void_p]),
+    "ems_batch_run": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ems_batch_step_with_energy": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_batch_set_active": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int]),
+    "ems_batch_timestep": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),
+    "ems_batch_samples": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_int, C.c_void_p, C.c_size_t,
+                                    C.c_void_p]),
+    "ems_batch_download_field": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p]),
+    "ems_batch_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_batch_last_error": (C.c_char_p, [C.c_void_p]),
 }
 
 
@@ -589,6 +611,70 @@ class Engine:
         self.close()
 
 
+class Batch:
+    """Many built :class:`Model` s stepping together on one device
+    (``ems_batch_*``): one launch per kernel kind over all models, one CUDA
+    graph per step; a frozen model keeps its state."""
+
+    def __init__(self, models: Sequence[Model], device: int = 0, max_steps: int = 100_000):
+        self._lib = gpu_lib()
+        self._models = list(models)
+        arr = (C.c_void_p * len(self._models))(*[m.desc for m in self._models])
+        h = C.c_void_p()
+        st = self._lib.ems_batch_create(arr, len(self._models), device, max_steps, C.byref(h))
+        if st != 0:
+            raise EngineError(st, "ems_batch_create failed")
+        self._h = h
+        self.n = len(self._models)
+
+    def _ck(self, st: int) -> None:
+        if st != 0:
+            raise EngineError(st, self._lib.ems_batch_last_error(self._h).decode())
+
+    def run(self, n: int) -> None:
+        self._ck(self._lib.ems_batch_run(self._h, n))
+
+    def step_with_energy(self) -> np.ndarray:
+        w = np.zeros(self.n, dtype=np.float64)
+        self._ck(self._lib.ems_batch_step_with_energy(self._h, w.ctypes.data))
+        return w
+
+    def set_active(self, model: int, active: bool) -> None:
+        self._ck(self._lib.ems_batch_set_active(self._h, model, 1 if active else 0))
+
+    def timestep(self, model: int) -> int:
+        n = C.c_uint64()
+        self._ck(self._lib.ems_batch_timestep(self._h, model, C.byref(n)))
+        return n.value
+
+    def samples(self, model: int, op: int, which: int = 0) -> np.ndarray:
+        n = C.c_size_t()
+        self._ck(self._lib.ems_batch_samples(self._h, model, op, which, None, 0, C.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        if n.value:
+            self._ck(self._lib.ems_batch_samples(self._h, model, op, which, out.ctypes.data, n.value, C.byref(n)))
+        return out
+
+    def field(self, model: int, field: int, axis: int) -> np.ndarray:
+        out = np.empty(self._models[model].nodes, dtype=np.float32)
+        self._ck(self._lib.ems_batch_download_field(self._h, model, field, axis, out.ctypes.data))
+        return out
+
+    @property
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._ck(self._lib.ems_batch_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ems_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 def run_until(stepper, limits: RunLimits) -> RunOutcome:
     """``Engine::run_until`` (src/engine/run.rs:221-540) over any object with
     ``run(n)`` and ``step_with_energy()``, driven by the host's run loop."""
@@ -619,6 +705,55 @@ def run_until(stepper, limits: RunLimits) -> RunOutcome:
     if err:
         raise err[0]
     return out
+
+
+def run_until_batch(batch, limits: Sequence[RunLimits]) -> list[RunOutcome]:
+    """The run loop over a batch (``ems_batch_drive``): every model gets the
+    outcome ``run_until`` would give it alone; a model that stops is frozen.
+    ``batch`` has ``n``, ``run(n)``, ``step_with_energy()`` (one value per
+    model) and ``set_active(model, active)``."""
+    lib = host_lib()
+    err: list[BaseException] = []
+    n = batch.n
+
+    @C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
+    def _run(_ctx, k):
+        try:
+            batch.run(k)
+            return 0
+        except BaseException as e:
+            err.append(e)
+            return 1
+
+    @C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double))
+    def _swe(_ctx, w):
+        try:
+            v = batch.step_with_energy()
+            for q in range(n):
+                w[q] = float(v[q])
+            return 0
+        except BaseException as e:
+            err.append(e)
+            return 1
+
+    @C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_int)
+    def _act(_ctx, m, a):
+        try:
+            batch.set_active(m, bool(a))
+            return 0
+        except BaseException as e:
+            err.append(e)
+            return 1
+
+    s = BatchStepper(None, n, _run, _swe, _act)
+    lims = (RunLimits * n)(*limits)
+    outs = (RunOutcome * n)()
+    st = lib.ems_batch_drive(C.byref(s), lims, outs)
+    if err:
+        raise err[0]
+    if st != 0:
+        raise ValueError("ems_batch_drive: invalid limits (check intervals differ?)")
+    return list(outs)
 
 
 def energy_decay_limits(max_steps: int, db: float, dt: float, excitation_end: float | None = None,

@@ -31,6 +31,7 @@
 #include "fused_tables.h"
 #include "separate.cuh"
 #include "split.cuh"
+#include "batch.cuh"
 
 #include <thread>
 #include <unordered_map>
@@ -1174,5 +1175,434 @@ ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {
     *active = active_schedule(h);
     return EMS_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches (batch.cuh): many models stepping together, one CUDA graph per step.
+
+struct ems_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<ems_gpu*> models;            // owned
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    uint64_t max_steps = 0;
+    std::vector<uint32_t> start[BK_KINDS];   // host copies of the prefix sums
+    BatchTable T{};
+    std::vector<int> active;
+    int* d_active = nullptr;
+    uint32_t* d_steps = nullptr;
+    BatchSource* d_src[2] = {nullptr, nullptr};  // [0] H sources, [1] E sources
+    uint32_t n_src[2] = {0, 0};
+    BatchProbe* d_probe[2] = {nullptr, nullptr}; // [0] current, [1] voltage
+    uint32_t n_probe[2] = {0, 0};
+    BatchLumped* d_lumped = nullptr;
+    uint32_t n_lumped = 0;
+    bool any_cpml = false, any_poles_e = false, any_poles_h = false, poles_first = false;
+    double* partials = nullptr;
+    double* ops_energy = nullptr;
+    double* energies = nullptr;
+    // Sample series: (model, op) → device buffer, interval (0: per step), which.
+    struct Series {
+        size_t model, op;
+        int which;
+        uint32_t interval, cap;
+        double* dev;
+    };
+    std::vector<Series> series;
+    unsigned grid[BK_KINDS] = {0, 0, 0, 0, 0};  // persistent grid per kind
+    cudaGraphExec_t step_graph = nullptr, energy_graph = nullptr;
+
+    template <class T_>
+    T_* alloc(size_t n) {
+        auto b = std::make_unique<DevBuf>();
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T_);
+        if (cudaMalloc(&b->p, bytes) != cudaSuccess) return nullptr;
+        cudaMemsetAsync(b->p, 0, bytes, stream);
+        b->bytes = bytes;
+        T_* p = (T_*)b->p;
+        bufs.push_back(std::move(b));
+        return p;
+    }
+    template <class T_>
+    T_* upload(const T_* h, size_t n) {
+        T_* d = alloc<T_>(n);
+        if (d && n && h) cudaMemcpyAsync(d, h, n * sizeof(T_), cudaMemcpyHostToDevice, stream);
+        return d;
+    }
+};
+
+namespace {
+
+ems_status bfail(ems_batch* b, ems_status s, const std::string& m) {
+    if (b) b->err = m;
+    return s;
+}
+
+// The whole step of every active model, in the hook order of the split
+// schedule (run_step), each kernel over all models at once.
+void batch_enqueue_step(ems_batch* b, bool energy) {
+    cudaStream_t s = b->stream;
+    const BatchTable& T = b->T;
+    const uint32_t nm = T.n;
+    if (energy) k_batch_ops_energy<<<nm, 1024, 0, s>>>(T, b->d_lumped, b->n_lumped, b->ops_energy);
+    if (b->grid[BK_SPLIT]) {
+        if (energy) k_batch_h<true><<<b->grid[BK_SPLIT], kSplitThreads, 0, s>>>(T, b->partials);
+        else k_batch_h<false><<<b->grid[BK_SPLIT], kSplitThreads, 0, s>>>(T, nullptr);
+    }
+    auto shell = [&](int side) {
+        if (!b->grid[BK_SHELL_H + side]) return;
+        if (side) k_batch_shell<1><<<b->grid[BK_SHELL_E], 32 * kShellWarps, 0, s>>>(T);
+        else k_batch_shell<0><<<b->grid[BK_SHELL_H], 32 * kShellWarps, 0, s>>>(T);
+    };
+    auto poles_h = [&] {
+        if (b->grid[BK_POLES_H]) k_batch_poles<0><<<b->grid[BK_POLES_H], 256, 0, s>>>(T);
+        if (b->grid[BK_POLES_E]) k_batch_capture<1><<<b->grid[BK_POLES_E], 256, 0, s>>>(T);
+    };
+    auto poles_e = [&] {
+        if (b->grid[BK_POLES_E]) k_batch_poles<1><<<b->grid[BK_POLES_E], 256, 0, s>>>(T);
+        if (b->grid[BK_POLES_H]) k_batch_capture<0><<<b->grid[BK_POLES_H], 256, 0, s>>>(T);
+    };
+    // Slab hooks after H, in registration order; then serial post_h.
+    if (b->poles_first) { poles_h(); shell(0); } else { shell(0); poles_h(); }
+    if (b->n_src[0]) k_batch_sources<0><<<blocks_for(b->n_src[0], 256), 256, 0, s>>>(T, b->d_src[0], b->n_src[0]);
+    if (b->n_probe[0]) k_batch_probes<0><<<blocks_for(b->n_probe[0], 128), 128, 0, s>>>(T, b->d_probe[0], b->n_probe[0]);
+    if (b->n_lumped) k_batch_lumped_pre<<<b->n_lumped, 128, 0, s>>>(T, b->d_lumped, b->n_lumped);
+    if (b->grid[BK_SPLIT]) k_batch_e<<<b->grid[BK_SPLIT], kSplitThreads, 0, s>>>(T);
+    if (b->poles_first) { poles_e(); shell(1); } else { shell(1); poles_e(); }
+    if (b->n_lumped) k_batch_lumped_post<<<b->n_lumped, 256, 0, s>>>(T, b->d_lumped, b->n_lumped);
+    if (b->n_src[1]) k_batch_sources<1><<<blocks_for(b->n_src[1], 256), 256, 0, s>>>(T, b->d_src[1], b->n_src[1]);
+    if (b->n_probe[1]) k_batch_probes<1><<<blocks_for(b->n_probe[1], 128), 128, 0, s>>>(T, b->d_probe[1], b->n_probe[1]);
+    if (energy) k_batch_energy<<<nm, 1024, 0, s>>>(T, b->partials, b->ops_energy, b->energies);
+    k_batch_advance<<<blocks_for(nm, 128), 128, 0, s>>>(T, b->d_steps);
+}
+
+ems_status batch_capture(ems_batch* b, bool energy, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bfail(b, EMS_ERR_CUDA, "graph capture");
+    batch_enqueue_step(b, energy);
+    if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess || !g) return bfail(b, EMS_ERR_CUDA, "graph capture");
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return bfail(b, EMS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return EMS_OK;
+}
+
+// Checks the operator order a batch can run: per model, the serial post_h
+// hooks are H sources then current probes, the serial post_e hooks lumped
+// elements then E sources then voltage probes (the order the batched
+// kernels run them in), and no two sources (or lumped elements) of a model
+// share an edge (they are applied in parallel).
+std::string batch_ineligible(const ems_engine_desc* d) {
+    int phase_e = 0, phase_h = 0;
+    std::vector<uint64_t> ke, kh, kl;
+    for (size_t k = 0; k < d->n_ops; ++k) {
+        const int kind = d->ops[k].kind;
+        int pe = -1, ph = -1;
+        if (kind == EMS_OP_LUMPED) {
+            pe = 0;
+            const auto* l = (const ems_lumped*)d->ops[k].table;
+            for (size_t e = 0; e < l->n_edges; ++e) kl.push_back(l->node[e]);
+        } else if (kind == EMS_OP_SOURCE) {
+            const auto* sr = (const ems_source*)d->ops[k].table;
+            const bool e_side = sr->kind == EMS_SOFT_E || sr->kind == EMS_HARD_E;
+            (e_side ? pe : ph) = e_side ? 1 : 0;
+            for (size_t e = 0; e < sr->n_edges; ++e) (e_side ? ke : kh).push_back(sr->node[e] * 3 + sr->axis[e]);
+        } else if (kind == EMS_OP_PROBE) {
+            const auto* pr = (const ems_probe*)d->ops[k].table;
+            if (pr->quantity == EMS_PROBE_VOLTAGE) pe = 2;
+            else ph = 1;
+        }
+        if (pe >= 0) {
+            if (pe < phase_e) return "post_e hooks not in the order lumped, E sources, voltage probes";
+            phase_e = pe;
+        }
+        if (ph >= 0) {
+            if (ph < phase_h) return "post_h hooks not in the order H sources, current probes";
+            phase_h = ph;
+        }
+    }
+    for (auto* v : {&ke, &kh, &kl}) {
+        std::sort(v->begin(), v->end());
+        if (std::adjacent_find(v->begin(), v->end()) != v->end()) return "two sources or lumped elements share an edge";
+    }
+    return "";
+}
+
+}  // namespace
+
+extern "C" {
+
+ems_status ems_batch_create(const ems_engine_desc* const* descs, size_t n_models, int device, uint64_t max_steps,
+                            ems_batch** out) {
+    if (!descs || !out || !n_models || n_models > kMaxBatch || max_steps == 0 || max_steps >= (1ull << 31))
+        return EMS_ERR_INVALID;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return EMS_ERR_CUDA;
+    // Everything made so far is released on every early return.
+    struct Guard {
+        ems_batch* b;
+        ~Guard() {
+            if (b) ems_batch_destroy(b);
+        }
+    } guard{new ems_batch};
+    ems_batch* b = guard.b;
+    b->device = device;
+    b->max_steps = max_steps;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return EMS_ERR_CUDA;
+    std::vector<BatchModel> hm(n_models);
+    std::vector<BatchSource> src[2];
+    std::vector<BatchProbe> prb[2];
+    std::vector<BatchLumped> lum;
+    for (int k = 0; k < BK_KINDS; ++k) b->start[k].assign(1, 0u);
+    int pf = -1;
+    for (size_t m = 0; m < n_models; ++m) {
+        const ems_engine_desc* d = descs[m];
+        if (!d) return EMS_ERR_INVALID;
+        std::string why = batch_ineligible(d);
+        if (!why.empty()) {
+            std::fprintf(stderr, "ems_batch: model %zu: %s\n", m, why.c_str());
+            return EMS_ERR_INVALID;
+        }
+        ems_gpu* h = nullptr;
+        ems_status st = ems_gpu_create(d, device, &h);
+        if (st) return st;
+        b->models.push_back(h);
+        if (!h->tables_ok) {
+            std::fprintf(stderr, "ems_batch: model %zu: %s\n", m, h->tables_why.c_str());
+            return EMS_ERR_INVALID;
+        }
+        const Grid& g = h->g;
+        BatchModel& M = hm[m];
+        M = BatchModel{};
+        M.P = h->fp;
+        for (int a = 0; a < 3; ++a) {
+            M.P.uo[a] = M.P.un[a] = h->u[a];
+            M.P.io[a] = M.P.in[a] = h->i[a];
+            M.f.u[a] = h->u[a];
+            M.f.i[a] = h->i[a];
+        }
+        for (size_t q = 0; q < h->psi_h.size(); ++q) {
+            FSlab& fs = M.P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+            fs.psi_old = fs.psi_new = h->psi_h[q].first;
+        }
+        for (int l = 0; l < 12; ++l) M.c.c[l] = h->co[l];
+        M.shell[0] = h->shell[0];
+        M.shell[1] = h->shell[1];
+        M.run_of[0] = h->run_of[0];
+        M.run_of[1] = h->run_of[1];
+        M.dt = h->dt;
+        M.bx = split_blocks_x(g);
+        bool has_cpml = false, has_poles = false;
+        for (auto& op : h->ops) {
+            if (op.kind == EMS_OP_CPML) has_cpml = true;
+            if (op.kind == EMS_OP_POLES) {
+                has_poles = true;
+                M.pe = op.poles.e;
+                M.ph = op.poles.h;
+            }
+        }
+        if (has_cpml && has_poles) {
+            if (pf >= 0 && pf != h->fp.poles_first) return EMS_ERR_INVALID;
+            pf = h->fp.poles_first;
+        }
+        b->any_cpml |= has_cpml;
+        b->any_poles_e |= M.pe.n_edges > 0;
+        b->any_poles_h |= M.ph.n_edges > 0;
+        const uint32_t blocks[BK_KINDS] = {M.bx * g.nx, shell_blocks(M.shell[0]), shell_blocks(M.shell[1]),
+                                           (uint32_t)blocks_for(M.pe.n_edges, 256),
+                                           (uint32_t)blocks_for(M.ph.n_edges, 256)};
+        for (int k = 0; k < BK_KINDS; ++k) {
+            const uint64_t next = (uint64_t)b->start[k].back() + blocks[k];
+            if (next >= (1ull << 32)) return EMS_ERR_INVALID;
+            b->start[k].push_back((uint32_t)next);
+        }
+        // Serial hooks: sources, probes, lumped elements (device tables).
+        size_t op_i = 0;
+        for (auto& op : h->ops) {
+            const size_t op_index = op_i++;
+            if (op.kind == EMS_OP_SOURCE) {
+                const auto* sr = (const ems_source*)d->ops[op_index].table;
+                const bool e_side = sr->kind == EMS_SOFT_E || sr->kind == EMS_HARD_E;
+                const bool hard = sr->kind == EMS_HARD_E || sr->kind == EMS_HARD_H;
+                const float* amp = op.source.amp.empty() ? nullptr : b->upload(op.source.amp.data(), op.source.amp.size());
+                for (size_t e = 0; e < sr->n_edges; ++e)
+                    src[e_side ? 1 : 0].push_back(BatchSource{(uint32_t)m, dev_index(g, sr->node[e]), sr->axis[e],
+                                                              hard ? 1u : 0u, sr->weight[e],
+                                                              (uint32_t)op.source.amp.size(), amp});
+            } else if (op.kind == EMS_OP_PROBE) {
+                const ems_gpu::ProbeDev& P = op.probe;
+                const uint32_t interval = (uint32_t)std::min<uint64_t>(P.interval, max_steps);
+                const uint32_t cap = (uint32_t)((max_steps - 1) / interval + 1);
+                double* v = b->alloc<double>(cap);
+                if (!v) return EMS_ERR_NOMEM;
+                prb[P.quantity == EMS_PROBE_VOLTAGE ? 1 : 0].push_back(BatchProbe{(uint32_t)m, interval, cap, P.d, v});
+                b->series.push_back({m, op_index, 0, interval, cap, v});
+            } else if (op.kind == EMS_OP_LUMPED) {
+                const ems_gpu::LumpedDev& L = op.lumped;
+                BatchLumped bl{};
+                bl.model = (uint32_t)m;
+                bl.axis = (uint32_t)L.axis;
+                bl.cap = (uint32_t)max_steps;
+                bl.has_src = L.has_src ? 1u : 0u;
+                bl.d = L.d;
+                bl.n_amp = (uint32_t)L.amp.size();
+                bl.amp = L.amp.empty() ? nullptr : b->upload(L.amp.data(), L.amp.size());
+                if (L.record) {
+                    bl.rec = b->alloc<double>(max_steps);
+                    if (!bl.rec) return EMS_ERR_NOMEM;
+                    b->series.push_back({m, op_index, 0, 1, (uint32_t)max_steps, bl.rec});
+                }
+                if (L.columns) {
+                    bl.pv = b->alloc<double>(max_steps);
+                    bl.pi = b->alloc<double>(max_steps);
+                    if (!bl.pv || !bl.pi) return EMS_ERR_NOMEM;
+                    b->series.push_back({m, op_index, 1, 1, (uint32_t)max_steps, bl.pv});
+                    b->series.push_back({m, op_index, 2, 1, (uint32_t)max_steps, bl.pi});
+                }
+                lum.push_back(bl);
+            }
+        }
+    }
+    b->poles_first = pf == 1;
+    b->active.assign(n_models, 1);
+    BatchTable& T = b->T;
+    T.n = (uint32_t)n_models;
+    T.models = b->upload(hm.data(), n_models);
+    for (int k = 0; k < BK_KINDS; ++k) T.start[k] = b->upload(b->start[k].data(), b->start[k].size());
+    b->d_active = b->upload(b->active.data(), n_models);
+    b->d_steps = b->alloc<uint32_t>(n_models);
+    T.active = b->d_active;
+    T.steps = b->d_steps;
+    for (int sd = 0; sd < 2; ++sd) {
+        b->n_src[sd] = (uint32_t)src[sd].size();
+        b->d_src[sd] = b->upload(src[sd].data(), src[sd].size());
+        b->n_probe[sd] = (uint32_t)prb[sd].size();
+        b->d_probe[sd] = b->upload(prb[sd].data(), prb[sd].size());
+    }
+    b->n_lumped = (uint32_t)lum.size();
+    b->d_lumped = b->upload(lum.data(), lum.size());
+    b->partials = b->alloc<double>(b->start[BK_SPLIT].back());
+    b->ops_energy = b->alloc<double>(n_models);
+    b->energies = b->alloc<double>(n_models);
+    if (!T.models || !b->d_active || !b->d_steps || !b->partials || !b->ops_energy || !b->energies)
+        return EMS_ERR_NOMEM;
+    // Persistent grids: as many blocks as are resident at once (at most the
+    // work), so each block walks the packed index with a stride.
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int occ[BK_KINDS] = {8, 6, 6, 8, 8};
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[BK_SPLIT], k_batch_e, kSplitThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[BK_SHELL_H], k_batch_shell<0>, 32 * kShellWarps, 0);
+    occ[BK_SHELL_E] = occ[BK_SHELL_H];
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[BK_POLES_E], k_batch_poles<1>, 256, 0);
+    occ[BK_POLES_H] = occ[BK_POLES_E];
+    for (int k = 0; k < BK_KINDS; ++k) {
+        const uint64_t work = b->start[k].back();
+        const uint64_t resident = (uint64_t)sms * std::max(1, occ[k]);
+        b->grid[k] = (unsigned)std::min<uint64_t>(work, resident);
+    }
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return EMS_ERR_CUDA;
+    ems_status st = batch_capture(b, false, &b->step_graph);
+    if (st) return st;
+    st = batch_capture(b, true, &b->energy_graph);
+    if (st) return st;
+    guard.b = nullptr;
+    *out = b;
+    return EMS_OK;
+}
+
+ems_status ems_batch_destroy(ems_batch* b) {
+    if (!b) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->step_graph) cudaGraphExecDestroy(b->step_graph);
+    if (b->energy_graph) cudaGraphExecDestroy(b->energy_graph);
+    b->bufs.clear();
+    for (ems_gpu* h : b->models) ems_gpu_destroy(h);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return EMS_OK;
+}
+
+ems_status ems_batch_run(ems_batch* b, uint64_t n) {
+    if (!b) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    for (uint64_t q = 0; q < n; ++q)
+        if (cudaGraphLaunch(b->step_graph, b->stream) != cudaSuccess) return bfail(b, EMS_ERR_CUDA, "graph launch");
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? EMS_OK : bfail(b, EMS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+ems_status ems_batch_step_with_energy(ems_batch* b, double* energies) {
+    if (!b || !energies) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    const size_t n = b->models.size();
+    if (cudaMemsetAsync(b->energies, 0, n * sizeof(double), b->stream) != cudaSuccess ||
+        cudaGraphLaunch(b->energy_graph, b->stream) != cudaSuccess ||
+        cudaMemcpyAsync(energies, b->energies, n * sizeof(double), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return bfail(b, EMS_ERR_CUDA, "energy step");
+    return EMS_OK;
+}
+
+ems_status ems_batch_set_active(ems_batch* b, size_t model, int active) {
+    if (!b || model >= b->models.size()) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    b->active[model] = active ? 1 : 0;
+    // Ordered with the graph launches on the batch's stream.
+    if (cudaMemcpyAsync(b->d_active + model, &b->active[model], sizeof(int), cudaMemcpyHostToDevice, b->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return bfail(b, EMS_ERR_CUDA, "set active");
+    return EMS_OK;
+}
+
+ems_status ems_batch_timestep(ems_batch* b, size_t model, uint64_t* n) {
+    if (!b || !n || model >= b->models.size()) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    uint32_t v = 0;
+    if (cudaMemcpyAsync(&v, b->d_steps + model, sizeof(v), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return bfail(b, EMS_ERR_CUDA, "timestep");
+    *n = v;
+    return EMS_OK;
+}
+
+ems_status ems_batch_samples(ems_batch* b, size_t model, size_t op, int which, double* out, size_t cap, size_t* n) {
+    if (!b || !n || model >= b->models.size()) return EMS_ERR_INVALID;
+    uint64_t steps = 0;
+    ems_status st = ems_batch_timestep(b, model, &steps);
+    if (st) return st;
+    for (const auto& sr : b->series) {
+        if (sr.model != model || sr.op != op || sr.which != which) continue;
+        const uint64_t count = std::min<uint64_t>(steps ? (steps - 1) / sr.interval + 1 : 0, sr.cap);
+        *n = (size_t)count;
+        if (!out) return EMS_OK;
+        const size_t k = std::min<size_t>(cap, (size_t)count);
+        if (k && (cudaMemcpyAsync(out, sr.dev, k * sizeof(double), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
+                  cudaStreamSynchronize(b->stream) != cudaSuccess))
+            return bfail(b, EMS_ERR_CUDA, "samples");
+        return EMS_OK;
+    }
+    return bfail(b, EMS_ERR_INVALID, "no such series");
+}
+
+ems_status ems_batch_download_field(ems_batch* b, size_t model, int field, int axis, float* host) {
+    if (!b || model >= b->models.size()) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, EMS_ERR_CUDA, "download");
+    return ems_gpu_download_field(b->models[model], field, axis, host);
+}
+
+ems_status ems_batch_stream(const ems_batch* b, void** stream) {
+    if (!b || !stream) return EMS_ERR_INVALID;
+    *stream = (void*)b->stream;
+    return EMS_OK;
+}
+
+const char* ems_batch_last_error(const ems_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 }  // extern "C"

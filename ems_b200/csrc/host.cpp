@@ -1053,4 +1053,84 @@ int ems_drive(const ems_stepper* s, const ems_run_limits* lim, ems_run_outcome* 
     return EMS_OK;
 }
 
+// drive for a batch: ems_drive's loop per model, the models stepping
+// together; a model whose loop ends is frozen and the rest go on.
+int ems_batch_drive(const ems_batch_stepper* s, const ems_run_limits* lim, ems_run_outcome* out) {
+    if (!s || !lim || !out || !s->n_models) return EMS_ERR_INVALID;
+    const size_t n = s->n_models;
+    const uint64_t interval = lim[0].check_interval ? lim[0].check_interval : 50;
+    for (size_t m = 0; m < n; ++m)
+        if ((lim[m].check_interval ? lim[m].check_interval : 50) != interval) return EMS_ERR_INVALID;
+    struct State {
+        bool done = false;
+        double w = 0.0, w_max = 0.0, ratio_db = 0.0;
+        uint64_t checks = 0;
+    };
+    std::vector<State> st(n);
+    std::vector<double> e(n, 0.0);
+    uint64_t steps = 0;
+    size_t left = n;
+    auto finish = [&](size_t m, int reason) {
+        State& x = st[m];
+        x.done = true;
+        --left;
+        out[m].reason = reason;
+        out[m].steps = steps;
+        out[m].energy = x.w;
+        out[m].max_energy = x.w_max;
+        out[m].ratio_db = x.ratio_db;
+        out[m].checks = x.checks;
+        s->set_active(s->ctx, m, 0);
+    };
+    auto finish_maxed = [&] {
+        for (size_t m = 0; m < n; ++m)
+            if (!st[m].done && steps >= lim[m].max_timesteps) finish(m, 1);
+    };
+    auto fail_all = [&] {
+        for (size_t m = 0; m < n; ++m)
+            if (!st[m].done) finish(m, 3);
+    };
+    for (;;) {
+        finish_maxed();
+        if (!left) break;
+        const uint64_t t_step = steps;  // timestep of every active model
+        if (s->step_with_energy(s->ctx, e.data()) != 0) {
+            fail_all();
+            break;
+        }
+        ++steps;
+        for (size_t m = 0; m < n; ++m) {
+            State& x = st[m];
+            if (x.done) continue;
+            x.w = e[m];
+            ++x.checks;
+            x.w_max = std::max(x.w_max, x.w);
+            const double ratio = x.w_max > 0.0 ? x.w / x.w_max : 1.0;
+            x.ratio_db = ratio > 0.0 ? 10.0 * std::log10(ratio) : -INFINITY;
+            const double t = (double)t_step * lim[m].dt;
+            if (!std::isfinite(x.w) || x.w < -1e-12 * x.w_max) {
+                finish(m, 2);
+            } else if (lim[m].has_end_criteria && (!lim[m].has_excitation_end || t > lim[m].excitation_end) &&
+                       x.w_max > 0.0 && ratio < lim[m].energy_ratio) {
+                finish(m, 0);
+            }
+        }
+        // The steps up to the next check, stopping at each model's limit.
+        uint64_t remaining = interval - 1;
+        while (remaining && left) {
+            uint64_t c = remaining;
+            for (size_t m = 0; m < n; ++m)
+                if (!st[m].done) c = std::min(c, lim[m].max_timesteps - std::min(lim[m].max_timesteps, steps));
+            if (c && s->run(s->ctx, c) != 0) {
+                fail_all();
+                break;
+            }
+            steps += c;
+            remaining -= c;
+            finish_maxed();
+        }
+    }
+    return EMS_OK;
+}
+
 }  // extern "C"

@@ -266,8 +266,8 @@ __global__ void k_source(float* f0, float* f1, float* f2, const uint8_t* axis, c
 }
 
 // Probe sample: Σ w·x in entry order (src/engine/probe.rs:381-392).
-__global__ void k_probe(const float* f0, const float* f1, const float* f2, ProbeDevT p, double* out) {
-    if (threadIdx.x != 0) return;
+__device__ __forceinline__ void probe_sample(const float* f0, const float* f1, const float* f2, const ProbeDevT& p,
+                                             double* out) {
     if (p.f32_sum) {
         float s = 0.0f;
         for (uint32_t e = 0; e < p.n; ++e) {
@@ -285,20 +285,29 @@ __global__ void k_probe(const float* f0, const float* f1, const float* f2, Probe
     }
 }
 
+__global__ void k_probe(const float* f0, const float* f1, const float* f2, ProbeDevT p, double* out) {
+    if (threadIdx.x != 0) return;
+    probe_sample(f0, f1, f2, p, out);
+}
+
 // Lumped element pre_e: saves u^n (src/engine/lumped.rs:1106-1121).
-__global__ void k_lumped_pre_e(const float* u, LumpedDevT d) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= d.n) return;
+__device__ __forceinline__ void lumped_pre_e_edge(const float* u, const LumpedDevT& d, uint32_t e) {
     const double x = (double)u[d.node[e]];
     if (d.has_branch) d.bu_prev[e] = x;
     if (d.record) d.ru_prev[e] = x;
 }
 
+__global__ void k_lumped_pre_e(const float* u, LumpedDevT d) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.n) return;
+    lumped_pre_e_edge(u, d, e);
+}
+
 // Lumped element post_e (src/engine/lumped.rs:1123-1236) and, for a port,
 // V = Σu/columns, I = −record (src/engine/port.rs:276-290). One block: the
 // per-edge updates in parallel, the sums in edge order by thread 0.
-__global__ void __launch_bounds__(256) k_lumped_post_e(float* u, LumpedDevT d, double val, int active, double dt,
-                                                       double* rec_out, double* pv_out, double* pi_out) {
+__device__ __forceinline__ void lumped_post_e_block(float* u, const LumpedDevT& d, double val, int active, double dt,
+                                                    double* rec_out, double* pv_out, double* pi_out) {
     for (uint32_t e = threadIdx.x; e < d.n; e += blockDim.x) {
         const uint32_t idx = d.node[e];
         if (d.src_w) d.v[e] = active ? __dadd_rn(0.0, __dmul_rn(d.src_w[e], val)) : 0.0;
@@ -323,7 +332,7 @@ __global__ void __launch_bounds__(256) k_lumped_post_e(float* u, LumpedDevT d, d
     __syncthreads();
     if (threadIdx.x != 0) return;
     double rec = 0.0;
-    if (d.record) {
+    if (d.record && rec_out) {
         double sum = 0.0;
         for (uint32_t e = 0; e < d.n; ++e) {
             const double u0 = d.ru_prev[e], u1 = (double)u[d.node[e]];
@@ -344,8 +353,27 @@ __global__ void __launch_bounds__(256) k_lumped_post_e(float* u, LumpedDevT d, d
     }
 }
 
+__global__ void __launch_bounds__(256) k_lumped_post_e(float* u, LumpedDevT d, double val, int active, double dt,
+                                                       double* rec_out, double* pv_out, double* pi_out) {
+    lumped_post_e_block(u, d, val, active, dt, rec_out, pv_out, pi_out);
+}
+
 // Σ ½·L·j² + ½·q²/C_p of the electric then the magnetic poles
 // (src/engine/dispersive.rs:1488-1506, 2598-2618).
+template <unsigned THREADS>
+__device__ __forceinline__ double pole_energy_block(const PoleSideDev& e, const PoleSideDev& h) {
+    double s = 0.0;
+    for (int side = 0; side < 2; ++side) {
+        const PoleSideDev& p = side == 0 ? e : h;
+        for (size_t q = threadIdx.x; q < p.n_poles; q += blockDim.x) {
+            const double a = __dmul_rn(__dmul_rn(p.half_l[q], p.j[q]), p.j[q]);
+            const double b = __dmul_rn(__dmul_rn(__dmul_rn(0.5, p.inv_c[q]), p.q[q]), p.q[q]);
+            s = __dadd_rn(s, __dadd_rn(a, b));
+        }
+    }
+    return block_sum<THREADS>(s);
+}
+
 __global__ void __launch_bounds__(1024) k_pole_energy(PoleSideDev e, PoleSideDev h, double* out) {
     double s = 0.0;
     for (int side = 0; side < 2; ++side) {
@@ -361,6 +389,16 @@ __global__ void __launch_bounds__(1024) k_pole_energy(PoleSideDev e, PoleSideDev
 }
 
 // Σ ½·L_e·j² + ½·q²/C_e of a lumped branch (src/engine/lumped.rs:1066-1077).
+__device__ __forceinline__ double branch_energy(const LumpedDevT& d, double dt) {
+    double s = 0.0;
+    for (uint32_t e = 0; e < d.n; ++e) {
+        const double half_l = __dmul_rn(__dmul_rn(0.25, d.two_l_dt[e]), dt);
+        s = __dadd_rn(s, __dadd_rn(__dmul_rn(__dmul_rn(half_l, d.bj[e]), d.bj[e]),
+                                   __dmul_rn(__dmul_rn(__dmul_rn(0.5, d.inv_c[e]), d.bq[e]), d.bq[e])));
+    }
+    return s;
+}
+
 __global__ void k_branch_energy(LumpedDevT d, double dt, double* out) {
     double s = 0.0;
     for (uint32_t e = 0; e < d.n; ++e) {

@@ -45,9 +45,8 @@ __device__ __forceinline__ Q4 zq() { return Q4{{0.0f, 0.0f, 0.0f, 0.0f}}; }
 // ny·pitch/4 (rows are padded to a multiple of 32 floats, so a quad never
 // straddles two rows). False for a quad that lies beyond the plane or in
 // a row's padding.
-__device__ __forceinline__ bool quad_of(const Grid& g, uint32_t& j, uint32_t& k0) {
+__device__ __forceinline__ bool quad_of(const Grid& g, uint32_t q, uint32_t& j, uint32_t& k0) {
     const uint32_t qpr = g.pitch >> 2;
-    const uint32_t q = blockIdx.x * kSplitThreads + threadIdx.x;
     if (q >= g.ny * qpr) return false;
     j = q / qpr;
     k0 = (q - j * qpr) * 4u;
@@ -60,12 +59,11 @@ __device__ __forceinline__ bool quad_of(const Grid& g, uint32_t& j, uint32_t& k0
 // update does not write (edges that do not exist, row padding) are stored
 // back as read. Grid: (quads of a plane / kSplitThreads, nx).
 template <bool ENERGY>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P) {
+__device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
-    const uint32_t i = blockIdx.y;
     uint32_t j = 0, k0 = 0;
     double w = 0.0;
-    if (quad_of(g, j, k0)) {
+    if (quad_of(g, q, j, k0)) {
         const uint32_t sj = g.pitch, si = g.ny * g.pitch;
         const uint32_t idx = i * si + j * sj + k0;
         const uint32_t row = i * g.ny + j;
@@ -113,6 +111,12 @@ __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const
         if (in_) stq(P.in[1] + idx, ny_);
         if (in_ && jn) stq(P.in[2] + idx, nz_);
     }
+    return w;
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P) {
+    const double w = split_h_quad<ENERGY>(P, blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
         if (threadIdx.x == 0) P.partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
@@ -121,11 +125,10 @@ __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const
 
 // E update of every edge (src/engine/kernel.rs:624-697), four z-nodes per
 // thread. Grid: (quads of a plane / kSplitThreads, nx).
-__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P) {
+__device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
-    const uint32_t i = blockIdx.y;
     uint32_t j = 0, k0 = 0;
-    if (!quad_of(g, j, k0)) return;
+    if (!quad_of(g, q, j, k0)) return;
     const uint32_t sj = g.pitch, si = g.ny * g.pitch;
     const uint32_t idx = i * si + j * sj + k0;
     const uint32_t row = i * g.ny + j;
@@ -152,6 +155,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant
     if (xi) stq(P.un[0] + idx, nx_);
     if (yj) stq(P.un[1] + idx, ny_);
     stq(P.un[2] + idx, nz_);
+}
+
+__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P) {
+    split_e_quad(P, blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
 }
 
 // Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.
@@ -249,19 +256,18 @@ __device__ __forceinline__ void shell_node(const FusedParams& P, uint32_t i, uin
 // CPML correction of one side over its layer shell: blocks [0, blocks_a)
 // take part A (one warp per segment), the rest part B (one thread per node).
 template <int SIDE>
-__global__ void __launch_bounds__(32 * kShellWarps) k_shell(const __grid_constant__ FusedParams P,
-                                                            const __grid_constant__ ShellDev S) {
+__device__ __forceinline__ void shell_item(const FusedParams& P, const ShellDev& S, uint32_t block, uint32_t tid) {
     const Grid& g = P.g;
     uint32_t row, k;
-    if (blockIdx.x < S.blocks_a) {
-        const uint32_t w = blockIdx.x * kShellWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    if (block < S.blocks_a) {
+        const uint32_t w = block * kShellWarps + (tid >> 5), lane = tid & 31u;
         if (w >= S.n_seg) return;
         const uint2 sg = S.seg[w];
         if (lane >= (sg.y >> 24)) return;
         row = sg.x;
         k = (sg.y & 0xffffffu) + lane;
     } else {
-        const uint32_t t = (blockIdx.x - S.blocks_a) * (32 * kShellWarps) + threadIdx.x;
+        const uint32_t t = (block - S.blocks_a) * (32 * kShellWarps) + tid;
         if (t >= S.n_b * S.n_kz) return;
         const uint32_t r = t / S.n_kz;
         row = S.rows_b[r];
@@ -269,6 +275,12 @@ __global__ void __launch_bounds__(32 * kShellWarps) k_shell(const __grid_constan
     }
     const uint32_t i = row / g.ny;
     shell_node<SIDE>(P, i, row - i * g.ny, k);
+}
+
+template <int SIDE>
+__global__ void __launch_bounds__(32 * kShellWarps) k_shell(const __grid_constant__ FusedParams P,
+                                                            const __grid_constant__ ShellDev S) {
+    shell_item<SIDE>(P, S, blockIdx.x, threadIdx.x);
 }
 
 // Blocks of the shell kernel for a side.
@@ -284,11 +296,9 @@ __host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
 // stored at once; a trapezoidal pole's is formed from its old state after it.
 // save_prev: also store the corrected value as the edge's saved value (the
 // capture it replaces would read the same value; pole_prev_fold).
-__global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
-                                                    const __grid_constant__ PoleSideDev p, const PoleRun* runs,
-                                                    const double* sets, const uint32_t* run_of, int electric,
-                                                    double dt, int save_prev) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, const PoleSideDev& p, const PoleRun* runs,
+                                           const double* sets, const uint32_t* run_of, int electric, double dt,
+                                           int save_prev, uint32_t e) {
     if (e >= p.n_edges) return;
     const PoleRun R = runs[run_of[e]];
     const uint32_t p0 = R.p0 + (e - R.e0) * R.np;
@@ -329,6 +339,13 @@ __global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fiel
     }
     fld[idx] = u_new;
     if (save_prev) p.prev[e] = u_new;
+}
+
+__global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
+                                                    const __grid_constant__ PoleSideDev p, const PoleRun* runs,
+                                                    const double* sets, const uint32_t* run_of, int electric,
+                                                    double dt, int save_prev) {
+    poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace emsk

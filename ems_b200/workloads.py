@@ -163,3 +163,45 @@ def patch_antenna(scale: float = 1.0, seed: int = 0x5EED, steps: int = 30000, cp
     n = m.nodes
     return Workload(f"patch_antenna_{n[0] - 1}x{n[1] - 1}x{n[2] - 1}", m, steps, port=port,
                     info={"nodes": n, "port_node": (px, py), "substrate_cells": kh, "courant": courant})
+
+
+def patch_variant(seed: int, cells: tuple[int, int] = (60, 160), steps: int = 60000, cpml: int = 8,
+                  courant: float = 0.99) -> Workload:
+    """One seeded patch-antenna variant of the batched sweep: patch side
+    8–30 mm, substrate ε_r 2.2–10.2 and thickness 0.8–3.2 mm, port offset
+    2–10 mm from the patch centre, PEC ground at z_min, CPML on the other
+    five faces, 50 Ω port with a Gaussian f0 = 2 GHz, fc = 1.5 GHz; meshed to
+    its own size, N × N × N/2 cells with N drawn from `cells` (graded in z:
+    the substrate finer than the air)."""
+    mm = 1e-3
+    rng = np.random.default_rng(seed)
+    side = rng.uniform(8.0, 30.0) * mm
+    eps = rng.uniform(2.2, 10.2)
+    h = rng.uniform(0.8, 3.2) * mm
+    off = rng.uniform(2.0, 10.0) * mm
+    n = int(rng.integers(cells[0], cells[1] + 1))
+    sub = 2.2 * side + 10 * mm
+    lx = sub + 2 * 12.0 * mm
+    d = lx / n
+    xl = np.arange(n + 1) * d
+    nz = max(12, n // 2)
+    nsub = max(3, min(nz // 4, int(round(h / (0.5 * d)))))
+    air = (nz - nsub) * d * 1.2
+    zl = np.concatenate([np.linspace(0.0, h, nsub + 1), h + np.linspace(0.0, air, nz - nsub + 1)[1:]])
+    m = E.Model(xl, xl, zl)
+    c = lx / 2
+    near = lambda lines, v: int(np.argmin(np.abs(lines - v)))  # noqa: E731
+    i0, i1 = near(xl, c - sub / 2), near(xl, c + sub / 2)
+    m.fill(m.cells().box([i0, i0, 0], [i1, i1, nsub]), m.material(eps_r=eps))
+    p0, p1 = near(xl, c - side / 2), near(xl, c + side / 2)
+    m.pec_edges(E.X, [p0, p0, nsub], [p1 - 1, p1, nsub])
+    m.pec_edges(E.Y, [p0, p0, nsub], [p1, p1 - 1, nsub])
+    m.faces([E.PEC] * 6)
+    m.build(courant=courant)
+    m.add_cpml([cpml, cpml, cpml, cpml, 0, cpml])
+    px, py = near(xl, c + off), near(xl, c)
+    port = m.add_lumped_port(E.Z, [px, py, 0], [px, py, nsub], 50.0, 2e9, 1.5e9, 1.0, steps)
+    nn = m.nodes
+    return Workload(f"patch_variant_{seed}_{nn[0] - 1}x{nn[1] - 1}x{nn[2] - 1}", m, steps, port=port,
+                    info={"seed": seed, "side_mm": side / mm, "eps_r": eps, "h_mm": h / mm, "offset_mm": off / mm,
+                          "cells": (nn[0] - 1) * (nn[1] - 1) * (nn[2] - 1), "f0": 2e9, "fc": 1.5e9})

@@ -278,6 +278,53 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 /* The schedule steps run with (1 to 4 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
+/* ---- Batches: many models stepping together.
+ *
+ * No counterpart in the reference, where a parameter sweep runs
+ * Simulation::run (src/sim/mod.rs:1044) once per model. A batch builds
+ * every model as ems_gpu_create does and steps them together on one device:
+ * each kernel kind of the split schedule runs once per step over all models
+ * (a packed per-model block table walked by a persistent grid), the serial
+ * hooks run batched from device-side step counters, and a whole step is one
+ * CUDA graph. Each model's fields, probe and port series equal those of the
+ * same model run alone bit for bit. A model needs the split schedule's
+ * tables, its post_e hooks in the order lumped elements, E sources, voltage
+ * probes and its post_h hooks in the order H sources, current probes, and
+ * no two sources (or lumped elements) on one edge; otherwise creation
+ * returns EMS_ERR_INVALID. max_steps (< 2^31) bounds the recorded series. */
+typedef struct ems_batch ems_batch;
+
+ems_status ems_batch_create(const ems_engine_desc* const* descs, size_t n_models, int device, uint64_t max_steps,
+                            ems_batch** out);
+ems_status ems_batch_destroy(ems_batch* b);
+
+/* Advances every active model n steps. */
+ems_status ems_batch_run(ems_batch* b, uint64_t n);
+
+/* Advances every active model one step and writes each model's energy
+ * invariant W^n of the state before the step (as ems_gpu_step_with_energy)
+ * to energies[model]; 0 for inactive models. */
+ems_status ems_batch_step_with_energy(ems_batch* b, double* energies);
+
+/* Freezes (active = 0) or resumes a model: a frozen model keeps its state
+ * and takes no steps (its end criterion has been met). */
+ems_status ems_batch_set_active(ems_batch* b, size_t model, int active);
+
+/* Completed steps of a model. */
+ems_status ems_batch_timestep(ems_batch* b, size_t model, uint64_t* n);
+
+/* A model's series as ems_gpu_samples (op: index into its descriptor's ops). */
+ems_status ems_batch_samples(ems_batch* b, size_t model, size_t op, int which, double* out, size_t cap, size_t* n);
+
+/* A model's field component in reference layout. */
+ems_status ems_batch_download_field(ems_batch* b, size_t model, int field, int axis, float* host);
+
+/* The batch's CUDA stream (cudaStream_t). */
+ems_status ems_batch_stream(const ems_batch* b, void** stream);
+
+/* Text of the batch's last error. */
+const char* ems_batch_last_error(const ems_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -157,6 +157,21 @@ typedef struct {
 
 int ems_drive(const ems_stepper* s, const ems_run_limits* limits, ems_run_outcome* out);
 
+/* The same run loop for n models stepping together (an ems_batch): each
+ * model gets exactly the checks, stop reason and step count ems_drive gives
+ * it alone; a model that stops is frozen (set_active 0) while the others go
+ * on. All limits must share check_interval. No counterpart in the
+ * reference, which drives one engine at a time. */
+typedef struct {
+    void* ctx;
+    size_t n_models;
+    int (*run)(void* ctx, uint64_t n);
+    int (*step_with_energy)(void* ctx, double* energies); /* n_models values */
+    int (*set_active)(void* ctx, size_t model, int active);
+} ems_batch_stepper;
+
+int ems_batch_drive(const ems_batch_stepper* s, const ems_run_limits* limits, ems_run_outcome* out);
+
 #ifdef __cplusplus
 }
 #endif
