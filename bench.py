@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
     ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split")
+    ap.add_argument("--workload", choices=["box", "sweep"], default="box",
+                    help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant sweep")
+    ap.add_argument("--models", type=int, default=64, help="sweep: number of patch variants")
+    ap.add_argument("--sweep-cells", type=int, nargs=2, default=[60, 160], help="sweep: N range (N x N x N/2 cells)")
+    ap.add_argument("--max-steps", type=int, default=40000, help="sweep: step limit per model")
     return ap.parse_args()
 
 
@@ -378,10 +383,61 @@ def run_ours(args):
     return 0
 
 
+def run_sweep(args):
+    """The batched sweep: seeded patch variants of uneven sizes run to the
+    −40 dB energy criterion (checked every 50 steps), batched (one graph per
+    step over all models, models frozen as they stop) and one at a time on
+    the same GPU; both must give every model the same outcome."""
+    import torch
+
+    import ems_b200 as E
+    from ems_b200 import workloads as W
+
+    ws = [W.patch_variant(s, cells=tuple(args.sweep_cells), steps=args.max_steps) for s in range(args.models)]
+    t_exc = E.waveform_duration(2e9, 1.5e9)
+    lims = [E.energy_decay_limits(args.max_steps, -40.0, w.model.dt, excitation_end=t_exc, interval=50) for w in ws]
+    cells = [w.info["cells"] for w in ws]
+    t0 = time.perf_counter()
+    b = E.Batch([w.model for w in ws], max_steps=args.max_steps)
+    t1 = time.perf_counter()
+    outs_b = E.run_until_batch(b, lims)
+    torch.cuda.synchronize(0)
+    t2 = time.perf_counter()
+    b.close()
+    upd_b = sum(c * o.steps for c, o in zip(cells, outs_b))
+    t_one, outs_1 = 0.0, []
+    for w, lim in zip(ws, lims):
+        g = E.Engine(w.model)
+        ta = time.perf_counter()
+        outs_1.append(E.run_until(g, lim))
+        torch.cuda.synchronize(0)
+        t_one += time.perf_counter() - ta
+        g.close()
+    same = all((x.reason, x.steps) == (y.reason, y.steps) for x, y in zip(outs_b, outs_1))
+    line = {
+        "metric": "sweep wall time", "value": round(t2 - t1, 3), "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "data": "synthetic",
+        "config": {"workload": f"{args.models} seeded patch variants, N x N x N/2 cells, N in {args.sweep_cells}, "
+                               f"-40 dB energy criterion every 50 steps, max {args.max_steps} steps",
+                   "total_cells": sum(cells)},
+        "batched": {"s": round(t2 - t1, 3), "create_s": round(t1 - t0, 3),
+                    "mcell_updates_per_s": round(upd_b / (t2 - t1) / 1e6, 1)},
+        "one_at_a_time": {"s": round(t_one, 3), "mcell_updates_per_s": round(upd_b / t_one / 1e6, 1)},
+        "speedup": round(t_one / (t2 - t1), 3),
+        "steps": {"min": min(o.steps for o in outs_b), "max": max(o.steps for o in outs_b),
+                  "reasons": sorted({o.reason for o in outs_b})},
+        "same_outcomes": same,
+    }
+    print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "sweep":
+        return run_sweep(args)
     return run_ours(args)
 
 

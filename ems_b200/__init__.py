@@ -213,6 +213,8 @@ GPU_SYMBOLS = {
     "ems_gpu_source_amplitude": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p, C.c_size_t]),
     "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ems_gpu_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ems_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
     "ems_batch_destroy": (C.c_int, [C.c_void_p]),
     "ems_batch_run": (C.c_int, [C.c_void_p, C.c_uint64]),
@@ -559,6 +561,11 @@ class Engine:
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value
 
+    def autotune(self, cache_path: str) -> None:
+        """Schedule autotuning (``ems_gpu_autotune``): cached pick, or timed
+        over the next steps ``run`` takes."""
+        self._ck(self._lib.ems_gpu_autotune(self._h, os.fsencode(cache_path)))
+
     @property
     def stream(self) -> int:
         """The engine's cudaStream_t (as an integer address)."""
@@ -641,6 +648,10 @@ class Batch:
 
     def set_active(self, model: int, active: bool) -> None:
         self._ck(self._lib.ems_batch_set_active(self._h, model, 1 if active else 0))
+
+    def autotune(self, cache_path: str) -> None:
+        """Persistent-grid autotuning (``ems_batch_autotune``)."""
+        self._ck(self._lib.ems_batch_autotune(self._h, os.fsencode(cache_path)))
 
     def timestep(self, model: int) -> int:
         n = C.c_uint64()

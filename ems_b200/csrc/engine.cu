@@ -59,6 +59,17 @@ struct ems_gpu {
     uint64_t launches = 0;
     int schedule = 0;
     std::string err;
+    // Autotuning (ems_gpu_autotune): candidate schedules timed over real
+    // steps (every schedule gives the same bits), the pick cached by key.
+    struct Tune {
+        bool active = false;
+        std::string cache, key;
+        std::vector<int> cand;
+        std::vector<double> ms;
+        size_t at = 0;       // candidate being timed
+        int done = 0;        // steps of it run (the first is a warm-up)
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+    } tune;
     std::vector<std::unique_ptr<DevBuf>> bufs;
     float* u[3] = {nullptr, nullptr, nullptr};
     float* i[3] = {nullptr, nullptr, nullptr};
@@ -979,14 +990,103 @@ ems_status ems_gpu_destroy(ems_gpu* h) {
     return EMS_OK;
 }
 
+// Autotune cache: text lines "<key> <value> <ms>"; the last line of a key wins.
+static bool tune_lookup(const std::string& path, const std::string& key, int* value) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[512];
+    bool found = false;
+    while (std::fgets(line, sizeof line, f)) {
+        std::string l(line);
+        while (!l.empty() && (l.back() == '\n' || l.back() == ' ')) l.pop_back();
+        const size_t p2 = l.rfind(' ');                                   // before <ms>
+        if (p2 == std::string::npos || p2 == 0) continue;
+        const size_t p1 = l.rfind(' ', p2 - 1);                           // before <value>
+        if (p1 == std::string::npos || p1 != key.size() || l.compare(0, p1, key) != 0) continue;
+        *value = std::atoi(l.c_str() + p1 + 1);
+        found = true;
+    }
+    std::fclose(f);
+    return found;
+}
+
+static void tune_record(const std::string& path, const std::string& key, int value, double ms) {
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %.6f\n", key.c_str(), value, ms);
+    std::fclose(f);
+}
+
+constexpr int kTuneSteps = 4;  // per candidate: one warm-up step and three timed
+
+// One step of a tuning engine: the current candidate's schedule, timed.
+static ems_status tune_step(ems_gpu* h) {
+    auto& T = h->tune;
+    h->schedule = T.cand[T.at];
+    const bool timed = T.done > 0;
+    if (timed) cudaEventRecord(T.e0, h->stream);
+    ems_status st = run_step(h, false);
+    if (st) return st;
+    if (timed) {
+        cudaEventRecord(T.e1, h->stream);
+        cudaEventSynchronize(T.e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, T.e0, T.e1);
+        T.ms[T.at] += ms;
+    }
+    if (++T.done == kTuneSteps) {
+        T.done = 0;
+        if (++T.at == T.cand.size()) {
+            size_t best = 0;
+            for (size_t q = 1; q < T.cand.size(); ++q)
+                if (T.ms[q] < T.ms[best]) best = q;
+            h->schedule = T.cand[best];
+            tune_record(T.cache, T.key, T.cand[best], T.ms[best] / (kTuneSteps - 1));
+            T.active = false;
+            cudaEventDestroy(T.e0);
+            cudaEventDestroy(T.e1);
+        }
+    }
+    return EMS_OK;
+}
+
 ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
     if (!h) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     for (uint64_t s = 0; s < n; ++s) {
-        ems_status st = run_step(h, false);
+        ems_status st = h->tune.active ? tune_step(h) : run_step(h, false);
         if (st) return st;
     }
     return check(h, cudaGetLastError(), "run");
+}
+
+ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
+    if (!h || !cache_path) return EMS_ERR_INVALID;
+    auto& T = h->tune;
+    char key[256];
+    std::snprintf(key, sizeof key, "engine %ux%ux%u ops=%zu tables=%d", h->g.nx, h->g.ny, h->g.nz, h->ops.size(),
+                  h->tables_ok ? 1 : 0);
+    std::string k(key);
+    for (auto& op : h->ops) k += "," + std::to_string(op.kind);
+    T.key = k;
+    T.cache = cache_path;
+    int v = 0;
+    if (tune_lookup(T.cache, T.key, &v) && (v == 1 || ((v == 3 || v == 4) && h->tables_ok))) {
+        h->schedule = v;
+        return EMS_OK;
+    }
+    // In-place schedules only (the per-operator, two-kernel and split ones
+    // share the CPML state buffers).
+    T.cand.clear();
+    if (h->tables_ok) T.cand = {4, 3};
+    T.cand.push_back(1);
+    T.ms.assign(T.cand.size(), 0.0);
+    T.at = 0;
+    T.done = 0;
+    if (check(h, cudaEventCreate(&T.e0), "autotune") || check(h, cudaEventCreate(&T.e1), "autotune"))
+        return EMS_ERR_CUDA;
+    T.active = true;
+    return EMS_OK;
 }
 
 // Reads the device status flag of the fused kernel's bounded waits.
@@ -1212,7 +1312,20 @@ struct ems_batch {
     };
     std::vector<Series> series;
     unsigned grid[BK_KINDS] = {0, 0, 0, 0, 0};  // persistent grid per kind
+    uint64_t resident[BK_KINDS] = {0, 0, 0, 0, 0};  // blocks resident at once per kind
     cudaGraphExec_t step_graph = nullptr, energy_graph = nullptr;
+    // Autotuning of the persistent grids (ems_batch_autotune): code 0 one
+    // block per work item, 1 the resident blocks, 2 half of them.
+    struct Tune {
+        bool active = false;
+        std::string cache, key;
+        std::vector<int> cand;
+        std::vector<double> ms;
+        size_t at = 0;
+        int done = 0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+    } tune;
+    int grid_code = 1;
 
     template <class T_>
     T_* alloc(size_t n) {
@@ -1276,6 +1389,30 @@ void batch_enqueue_step(ems_batch* b, bool energy) {
     if (b->n_probe[1]) k_batch_probes<1><<<blocks_for(b->n_probe[1], 128), 128, 0, s>>>(T, b->d_probe[1], b->n_probe[1]);
     if (energy) k_batch_energy<<<nm, 1024, 0, s>>>(T, b->partials, b->ops_energy, b->energies);
     k_batch_advance<<<blocks_for(nm, 128), 128, 0, s>>>(T, b->d_steps);
+}
+
+// The persistent grid of each kernel kind for grid code `code`.
+void batch_grids(ems_batch* b, int code) {
+    for (int k = 0; k < BK_KINDS; ++k) {
+        const uint64_t work = b->start[k].back();
+        uint64_t g = work;
+        if (code == 1) g = std::min<uint64_t>(work, b->resident[k]);
+        if (code == 2) g = std::min<uint64_t>(work, std::max<uint64_t>(1, b->resident[k] / 2));
+        b->grid[k] = (unsigned)g;
+    }
+    b->grid_code = code;
+}
+
+ems_status batch_capture(ems_batch* b, bool energy, cudaGraphExec_t* out);
+
+// Captures the step and energy-step graphs for the current grids.
+ems_status batch_graphs(ems_batch* b) {
+    if (b->step_graph) cudaGraphExecDestroy(b->step_graph);
+    if (b->energy_graph) cudaGraphExecDestroy(b->energy_graph);
+    b->step_graph = b->energy_graph = nullptr;
+    ems_status st = batch_capture(b, false, &b->step_graph);
+    if (st) return st;
+    return batch_capture(b, true, &b->energy_graph);
 }
 
 ems_status batch_capture(ems_batch* b, bool energy, cudaGraphExec_t* out) {
@@ -1499,15 +1636,10 @@ ems_status ems_batch_create(const ems_engine_desc* const* descs, size_t n_models
     occ[BK_SHELL_E] = occ[BK_SHELL_H];
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[BK_POLES_E], k_batch_poles<1>, 256, 0);
     occ[BK_POLES_H] = occ[BK_POLES_E];
-    for (int k = 0; k < BK_KINDS; ++k) {
-        const uint64_t work = b->start[k].back();
-        const uint64_t resident = (uint64_t)sms * std::max(1, occ[k]);
-        b->grid[k] = (unsigned)std::min<uint64_t>(work, resident);
-    }
+    for (int k = 0; k < BK_KINDS; ++k) b->resident[k] = (uint64_t)sms * std::max(1, occ[k]);
+    batch_grids(b, 1);
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return EMS_ERR_CUDA;
-    ems_status st = batch_capture(b, false, &b->step_graph);
-    if (st) return st;
-    st = batch_capture(b, true, &b->energy_graph);
+    ems_status st = batch_graphs(b);
     if (st) return st;
     guard.b = nullptr;
     *out = b;
@@ -1527,13 +1659,83 @@ ems_status ems_batch_destroy(ems_batch* b) {
     return EMS_OK;
 }
 
+// One step of a tuning batch: the current candidate's graph, timed.
+static ems_status batch_tune_step(ems_batch* b) {
+    auto& T = b->tune;
+    if (b->grid_code != T.cand[T.at]) {
+        batch_grids(b, T.cand[T.at]);
+        ems_status st = batch_graphs(b);
+        if (st) return st;
+    }
+    const bool timed = T.done > 0;
+    if (timed) cudaEventRecord(T.e0, b->stream);
+    if (cudaGraphLaunch(b->step_graph, b->stream) != cudaSuccess) return bfail(b, EMS_ERR_CUDA, "graph launch");
+    if (timed) {
+        cudaEventRecord(T.e1, b->stream);
+        cudaEventSynchronize(T.e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, T.e0, T.e1);
+        T.ms[T.at] += ms;
+    }
+    if (++T.done == kTuneSteps) {
+        T.done = 0;
+        if (++T.at == T.cand.size()) {
+            size_t best = 0;
+            for (size_t q = 1; q < T.cand.size(); ++q)
+                if (T.ms[q] < T.ms[best]) best = q;
+            tune_record(T.cache, T.key, T.cand[best], T.ms[best] / (kTuneSteps - 1));
+            T.active = false;
+            cudaEventDestroy(T.e0);
+            cudaEventDestroy(T.e1);
+            if (b->grid_code != T.cand[best]) {
+                batch_grids(b, T.cand[best]);
+                return batch_graphs(b);
+            }
+        }
+    }
+    return EMS_OK;
+}
+
 ems_status ems_batch_run(ems_batch* b, uint64_t n) {
     if (!b) return EMS_ERR_INVALID;
     cudaSetDevice(b->device);
-    for (uint64_t q = 0; q < n; ++q)
-        if (cudaGraphLaunch(b->step_graph, b->stream) != cudaSuccess) return bfail(b, EMS_ERR_CUDA, "graph launch");
+    for (uint64_t q = 0; q < n; ++q) {
+        if (b->tune.active) {
+            ems_status st = batch_tune_step(b);
+            if (st) return st;
+        } else if (cudaGraphLaunch(b->step_graph, b->stream) != cudaSuccess) {
+            return bfail(b, EMS_ERR_CUDA, "graph launch");
+        }
+    }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? EMS_OK : bfail(b, EMS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+ems_status ems_batch_autotune(ems_batch* b, const char* cache_path) {
+    if (!b || !cache_path) return EMS_ERR_INVALID;
+    cudaSetDevice(b->device);
+    auto& T = b->tune;
+    char key[256];
+    std::snprintf(key, sizeof key, "batch n=%zu blocks=%u,%u,%u,%u,%u", b->models.size(), b->start[0].back(),
+                  b->start[1].back(), b->start[2].back(), b->start[3].back(), b->start[4].back());
+    T.key = key;
+    T.cache = cache_path;
+    int v = 0;
+    if (tune_lookup(T.cache, T.key, &v) && v >= 0 && v <= 2) {
+        if (v != b->grid_code) {
+            batch_grids(b, v);
+            return batch_graphs(b);
+        }
+        return EMS_OK;
+    }
+    T.cand = {1, 0, 2};
+    T.ms.assign(T.cand.size(), 0.0);
+    T.at = 0;
+    T.done = 0;
+    if (cudaEventCreate(&T.e0) != cudaSuccess || cudaEventCreate(&T.e1) != cudaSuccess)
+        return bfail(b, EMS_ERR_CUDA, "autotune");
+    T.active = true;
+    return EMS_OK;
 }
 
 ems_status ems_batch_step_with_energy(ems_batch* b, double* energies) {

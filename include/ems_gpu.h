@@ -278,6 +278,15 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 /* The schedule steps run with (1 to 4 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
+/* Picks the fastest in-place schedule (4, 3 or 1) for this model's grid
+ * shape and operators: from `cache_path` (a text file of earlier picks,
+ * lines "<key> <schedule> <ms>") if it holds the key, else by timing each
+ * candidate over the next steps ems_gpu_run takes (four steps each, the
+ * first untimed; the results do not depend on the schedule, so these are
+ * ordinary steps) and appending the pick to the file. No counterpart in
+ * the reference, whose CPU engine has a single code path. */
+ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path);
+
 /* ---- Batches: many models stepping together.
  *
  * No counterpart in the reference, where a parameter sweep runs
@@ -318,6 +327,13 @@ ems_status ems_batch_samples(ems_batch* b, size_t model, size_t op, int which, d
 
 /* A model's field component in reference layout. */
 ems_status ems_batch_download_field(ems_batch* b, size_t model, int field, int axis, float* host);
+
+/* Picks the persistent grid of the batched kernels (one block per work
+ * item, the resident blocks, or half of them) for this batch's shape: from
+ * `cache_path` if it holds the key, else by timing each candidate over the
+ * next steps ems_batch_run takes (results do not depend on the grid) and
+ * appending the pick to the file. No counterpart in the reference. */
+ems_status ems_batch_autotune(ems_batch* b, const char* cache_path);
 
 /* The batch's CUDA stream (cudaStream_t). */
 ems_status ems_batch_stream(const ems_batch* b, void** stream);

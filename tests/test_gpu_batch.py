@@ -105,3 +105,33 @@ def test_batch_rejects_models_it_cannot_order():
     m.add_source(E.SOFT_E, [(E.Z, (4, 4, 4), 1.0)], 10e9, 5e9, 100)  # a probe before a source
     with pytest.raises(E.EngineError):
         E.Batch([m], max_steps=100)
+
+
+def test_autotune_picks_and_caches_without_changing_results():
+    import os
+
+    cache = os.path.join(os.path.dirname(os.path.abspath(__file__)), ".cache", "autotune.txt")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    if os.path.exists(cache):
+        os.remove(cache)
+    m, _ = mixed_model(scheme=E.TRAPEZOIDAL, steps=60)
+    g, ref = E.Engine(m), E.Engine(m)
+    g.autotune(cache)
+    g.run(40)  # 3 candidates × 4 steps tuned, the rest on the pick
+    ref.run(40)
+    assert_fields_equal(g, ref, "autotuned engine")
+    lines = open(cache).read().splitlines()
+    assert len(lines) == 1 and lines[0].startswith("engine ")
+    pick = int(lines[0].split()[-2])
+    assert g.schedule == pick
+    h = E.Engine(m)
+    h.autotune(cache)  # from the cache: no tuning steps
+    assert h.schedule == pick
+    models, _ = _models()
+    b, singles = E.Batch(models, max_steps=100), [E.Engine(x) for x in models]
+    b.autotune(cache)
+    b.run(30)
+    for q, x in enumerate(singles):
+        x.run(30)
+        assert_fields_equal(Alone(b, q), x, f"autotuned batch model {q}")
+    assert any(l.startswith("batch ") for l in open(cache).read().splitlines())
