@@ -57,12 +57,37 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
     ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split")
-    ap.add_argument("--workload", choices=["box", "sweep"], default="box",
-                    help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant sweep")
+    ap.add_argument("--workload", choices=["box", "sweep", "learned"], default="box",
+                    help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
+                         "sweep; learned: training and held-out evaluation of the learned early stop")
     ap.add_argument("--models", type=int, default=64, help="sweep: number of patch variants")
     ap.add_argument("--sweep-cells", type=int, nargs=2, default=[60, 160], help="sweep: N range (N x N x N/2 cells)")
     ap.add_argument("--max-steps", type=int, default=40000, help="sweep: step limit per model")
+    ap.add_argument("--train", type=int, default=2000, help="learned: training variants")
+    ap.add_argument("--test", type=int, default=256, help="learned: held-out variants")
+    ap.add_argument("--learn-cells", type=int, nargs=2, default=[30, 50], help="learned: N range of the variants")
+    ap.add_argument("--epochs", type=int, default=60, help="learned: training epochs")
+    ap.add_argument("--threshold", type=float, default=0.1, help="learned: window residual threshold")
     return ap.parse_args()
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The largest x over the ranks (the slowest rank's time): an all-reduce
+    of one f64 on the process group (NCCL on the GPU, gloo on the CPU)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(world: int, cells: int, steps: int, seconds: float) -> float:
+    """Whole-job Mcell-updates/s: every rank steps its own replica, so the
+    job updates world × cells × steps cells in the slowest rank's time."""
+    return world * cells * steps / seconds / 1e6
 
 
 def dist_env():
@@ -301,11 +326,8 @@ def run_ours(args):
     launches = eng.launches - launches0
     kern = {k: eng.profile_read(k) for k in (0, 1, 2)}
     eng.profile(False)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * w.cells * args.steps / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(ms, world, f"cuda:{dev}")
+    value = aggregate(world, w.cells, args.steps, ms * 1e-3)
 
     # --- end to end through the C ABI: per step, amplitude H2D, step, probe sample D2H
     amp_op = w.source
@@ -324,11 +346,8 @@ def run_ours(args):
         eng.run(1)
         eng.last_sample(probe_op)
     el = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([el], device=f"cuda:{dev}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        el = float(t.item())
-    e2e = world * w.cells * k_e2e / el / 1e6
+    el = max_over_ranks(el, world, f"cuda:{dev}")
+    e2e = aggregate(world, w.cells, k_e2e, el)
 
     if rank != 0:
         eng.close()
@@ -432,12 +451,123 @@ def run_sweep(args):
     return 0 if same else 1
 
 
+def run_learned(args):
+    """The learned early stop: train the network on port records of seeded
+    patch variants generated by the batched solver, then run held-out
+    variants to the −40 dB criterion plainly and with the learned stop (both
+    batched); report steps saved, sweep times and the |S11| error over
+    1-3 GHz of the stopped runs against the plain ones (and, for contrast,
+    of stopping at the same step without the network's tail)."""
+    import torch
+
+    import ems_b200 as E
+    from ems_b200 import learn as Lr
+    from ems_b200 import workloads as W
+
+    cells = tuple(args.learn_cells)
+    t0 = time.perf_counter()
+    X, Y = [], []
+    phase = {"build_s": 0.0, "create_s": 0.0, "run_s": 0.0, "extract_s": 0.0}
+    for c0 in range(0, args.train, 1000):
+        ta = time.perf_counter()
+        ws = [W.patch_variant(10_000 + q, cells=cells, steps=args.max_steps) for q in range(c0, min(args.train, c0 + 1000))]
+        L = max(Lr.steps_needed(w.model.dt) for w in ws)
+        tb_ = time.perf_counter()
+        bb = E.Batch([w.model for w in ws], max_steps=L)
+        tc = time.perf_counter()
+        bb.run(L)
+        torch.cuda.synchronize()
+        td = time.perf_counter()
+        for q, w in enumerate(ws):
+            x, y = Lr.example(bb.samples(q, w.port, 1), bb.samples(q, w.port, 2), w.model.dt)
+            X.append(x)
+            Y.append(y)
+        bb.close()
+        te = time.perf_counter()
+        for k, v in zip(phase, (tb_ - ta, tc - tb_, td - tc, te - td)):
+            phase[k] += v
+        del ws
+    t_data = time.perf_counter() - t0
+    Xd, Yd = torch.from_numpy(np.stack(X)).cuda(), torch.from_numpy(np.stack(Y)).cuda()
+    net = Lr.Net(seed=0)
+    t1 = time.perf_counter()
+    hist = Lr.train(net, Xd, Yd, epochs=args.epochs, batch=64, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+
+    ws = [W.patch_variant(20_000 + q, cells=cells, steps=args.max_steps) for q in range(args.test)]
+    models, ports = [w.model for w in ws], [w.port for w in ws]
+    t_exc = E.waveform_duration(2e9, 1.5e9)
+    lims = [E.energy_decay_limits(args.max_steps, -40.0, m.dt, excitation_end=t_exc, interval=50) for m in models]
+    b = E.Batch(models, max_steps=args.max_steps)
+    ta = time.perf_counter()
+    plain = E.run_until_batch(b, lims)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - ta
+    recs = [(b.samples(q, ports[q], 1), b.samples(q, ports[q], 2)) for q in range(len(models))]
+    b.close()
+    b = E.Batch(models, max_steps=args.max_steps)
+    ls = Lr.LearnedStop(b, ports, [m.dt for m in models], net, threshold=args.threshold)
+    tb = time.perf_counter()
+    learned = E.run_until_batch(ls, lims)
+    torch.cuda.synchronize()
+    t_learned = time.perf_counter() - tb
+    lrecs = [(b.samples(q, ports[q], 1), b.samples(q, ports[q], 2)) for q in range(len(models))]
+    b.close()
+
+    freqs = np.linspace(1e9, 3e9, 81)
+    err, err_cut, steps_l, fallback_same = [], [], [], True
+    for q, m in enumerate(models):
+        v, i = recs[q]
+        full = Lr.s11_db(np.arange(len(v)), v, i, m.dt, freqs)
+        if q in ls.stopped:
+            stop = ls.stopped[q]
+            st, vv, ii = Lr.spliced(lrecs[q][0], lrecs[q][1], ls.pred[q], stop, m.dt)
+            err.append(float(np.max(np.abs(Lr.s11_db(st, vv, ii, m.dt, freqs) - full))))
+            cut = Lr.s11_db(np.arange(stop), lrecs[q][0][:stop], lrecs[q][1][:stop], m.dt, freqs)
+            err_cut.append(float(np.max(np.abs(cut - full))))
+            steps_l.append(stop)
+        else:
+            steps_l.append(learned[q].steps)
+            fallback_same &= learned[q].steps == plain[q].steps and np.array_equal(lrecs[q][0], v)
+    steps_p = [o.steps for o in plain]
+    upd = lambda st: sum(w.info["cells"] * n for w, n in zip(ws, st))  # noqa: E731
+    e = np.array(err) if err else np.zeros(0)
+    line = {
+        "metric": "sweep wall time, learned stop vs plain", "value": round(t_learned, 3), "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+        "config": {"workload": f"patch variants N x N x N/2, N in {list(cells)}; {args.train} training and "
+                               f"{args.test} held-out variants; -40 dB criterion every 50 steps, max {args.max_steps}",
+                   "k_in": Lr.K_IN, "t_out": Lr.T_OUT, "stride": Lr.STRIDE, "window": Lr.WINDOW,
+                   "dt_ref_ps": Lr.DT_REF * 1e12,
+                   "threshold": args.threshold, "params": int(net.p.numel()), "dtype": "bf16 GEMM, f32 accumulate"},
+        "plain": {"s": round(t_plain, 3), "steps": int(sum(steps_p)), "mcell_updates": round(upd(steps_p) / 1e6, 1)},
+        "learned": {"s": round(t_learned, 3), "steps": int(sum(steps_l)), "stopped": len(ls.stopped),
+                    "fallback": args.test - len(ls.stopped), "fallback_identical": bool(fallback_same)},
+        "speedup": round(t_plain / t_learned, 3),
+        "steps_saved": round(1.0 - sum(steps_l) / max(1, sum(steps_p)), 4),
+        "s11_err_db": {"median": round(float(np.median(e)), 4) if e.size else None,
+                       "p90": round(float(np.percentile(e, 90)), 4) if e.size else None,
+                       "max": round(float(e.max()), 4) if e.size else None,
+                       "within_0.5dB": round(float(np.mean(e <= 0.5)), 4) if e.size else None},
+        "s11_err_db_truncated_without_net": {"median": round(float(np.median(err_cut)), 4) if err_cut else None,
+                                             "max": round(float(np.max(err_cut)), 4) if err_cut else None},
+        "training": {"data_s": round(t_data, 2), "data_phases_s": {k: round(v, 2) for k, v in phase.items()},
+                     "train_s": round(t_train, 2), "loss_first": round(hist[0], 6),
+                     "loss_last": round(hist[-1], 6), "epochs": args.epochs},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "sweep":
         return run_sweep(args)
+    if args.workload == "learned":
+        return run_learned(args)
     return run_ours(args)
 
 

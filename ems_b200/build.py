@@ -1,7 +1,8 @@
 """Builds the engine's shared libraries in-tree.
 
 * ``ems_b200/libems_gpu.so``  — the CUDA engine (include/ems_gpu.h), sm_100a;
-* ``ems_b200/libems_host.so`` — host-side set-up and run loop (include/ems_host.h).
+* ``ems_b200/libems_host.so`` — host-side set-up and run loop (include/ems_host.h);
+* ``ems_b200/libems_learn.so`` — the learned early stop's kernels (include/ems_learn.h).
 
 The CUDA sources are compiled without fused multiply-add contraction and
 with IEEE denormals, division and square root, which the engine's bit-exact
@@ -28,6 +29,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-Wal
 
 GPU_LIB = os.path.join(HERE, "libems_gpu.so")
 HOST_LIB = os.path.join(HERE, "libems_host.so")
+LEARN_LIB = os.path.join(HERE, "libems_learn.so")
 
 
 def _nvcc() -> str:
@@ -63,6 +65,17 @@ def build_gpu(force: bool = False) -> str:
     return GPU_LIB
 
 
+def build_learn(force: bool = False) -> str:
+    """The learned early stop's kernels (include/ems_learn.h)."""
+    srcs = [os.path.join(CSRC, "learn.cu"), os.path.join(INCLUDE, "ems_learn.h")]
+    if force or _stale(LEARN_LIB, srcs):
+        tmp = LEARN_LIB + ".tmp"
+        _run([_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-I", INCLUDE,
+              "-o", tmp, os.path.join(CSRC, "learn.cu")])
+        os.replace(tmp, LEARN_LIB)
+    return LEARN_LIB
+
+
 def build_host(force: bool = False) -> str:
     srcs = [os.path.join(CSRC, "host.cpp"), os.path.join(INCLUDE, "ems_host.h"), os.path.join(INCLUDE, "ems_gpu.h")]
     if force or _stale(HOST_LIB, srcs):
@@ -75,9 +88,11 @@ def build_host(force: bool = False) -> str:
 def build(force: bool = False) -> None:
     build_host(force)
     build_gpu(force)
+    build_learn(force)
 
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv)
     print(HOST_LIB)
     print(GPU_LIB)
+    print(LEARN_LIB)

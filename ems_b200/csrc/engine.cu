@@ -43,6 +43,7 @@ namespace {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool chunk = false;  // an arena chunk: freed only with the engine
     ~DevBuf() {
         if (p) cudaFree(p);
     }
@@ -197,10 +198,34 @@ struct ems_gpu {
         }
     }
 
+    // Small tables come out of 4 MiB arena chunks (256-byte aligned), so an
+    // engine of a batch costs a few cudaMalloc calls rather than a hundred;
+    // arrays of 1 MiB and more get their own allocation. Everything is
+    // zeroed and lives until ems_gpu_destroy.
+    static constexpr size_t kArenaChunk = 4u << 20, kArenaMax = 1u << 20;
+    char* arena = nullptr;
+    size_t arena_used = 0;
+
     template <class T>
     T* alloc(size_t n) {
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        if (bytes < kArenaMax) {
+            const size_t need = (bytes + 255) & ~(size_t)255;
+            if (!arena || arena_used + need > kArenaChunk) {
+                auto b = std::make_unique<DevBuf>();
+                if (cudaMalloc(&b->p, kArenaChunk) != cudaSuccess) return nullptr;
+                cudaMemsetAsync(b->p, 0, kArenaChunk, stream);
+                b->bytes = kArenaChunk;
+                b->chunk = true;
+                arena = (char*)b->p;
+                arena_used = 0;
+                bufs.push_back(std::move(b));
+            }
+            T* p = (T*)(arena + arena_used);
+            arena_used += need;
+            return p;
+        }
         auto b = std::make_unique<DevBuf>();
-        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
         if (cudaMalloc(&b->p, bytes) != cudaSuccess) return nullptr;
         cudaMemsetAsync(b->p, 0, bytes, stream);
         b->bytes = bytes;
@@ -216,7 +241,7 @@ struct ems_gpu {
     }
     void release(void* p) {
         for (size_t k = 0; k < bufs.size(); ++k)
-            if (bufs[k]->p == p) {
+            if (bufs[k]->p == p && !bufs[k]->chunk) {
                 bufs.erase(bufs.begin() + k);
                 return;
             }
