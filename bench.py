@@ -471,11 +471,17 @@ def run_learned(args):
     for c0 in range(0, args.train, 1000):
         ta = time.perf_counter()
         ws = [W.patch_variant(10_000 + q, cells=cells, steps=args.max_steps) for q in range(c0, min(args.train, c0 + 1000))]
-        L = max(Lr.steps_needed(w.model.dt) for w in ws)
+        need = [Lr.steps_needed(w.model.dt) for w in ws]
         tb_ = time.perf_counter()
-        bb = E.Batch([w.model for w in ws], max_steps=L)
+        bb = E.Batch([w.model for w in ws], max_steps=max(need))
         tc = time.perf_counter()
-        bb.run(L)
+        done = 0
+        for target in sorted(set(need)):  # each model runs the steps its record needs, then is frozen
+            bb.run(target - done)
+            done = target
+            for q, nq in enumerate(need):
+                if nq == target:
+                    bb.set_active(q, False)
         torch.cuda.synchronize()
         td = time.perf_counter()
         for q, w in enumerate(ws):

@@ -436,17 +436,14 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         return EMS_OK;
     }
     for (int side = 0; side < 2; ++side) {
-        const ShellTables st = shell_tables(T.cmask, g.nx, g.ny, g.nz, side);
+        uint32_t total = 0;
+        const std::vector<ShellBox> boxes = shell_boxes(T, d->nodes, side, &total);
         ShellDev& S = h->shell[side];
         S = ShellDev{};
-        S.n_seg = (uint32_t)st.seg.size();
-        S.blocks_a = (S.n_seg + kShellWarps - 1) / kShellWarps;
-        S.n_b = (uint32_t)st.rows_b.size();
-        S.n_kz = (uint32_t)st.kz.size();
-        if (S.n_seg) S.seg = h->upload(st.seg.data(), st.seg.size());
-        if (S.n_b) S.rows_b = h->upload(st.rows_b.data(), st.rows_b.size());
-        if (S.n_kz) S.kz = h->upload(st.kz.data(), st.kz.size());
-        if ((S.n_seg && !S.seg) || (S.n_b && !S.rows_b) || (S.n_kz && !S.kz)) return fail(h, EMS_ERR_NOMEM, "CPML shell");
+        S.n_box = (uint32_t)boxes.size();
+        S.total = total;
+        if (S.n_box) S.box = h->upload(boxes.data(), boxes.size());
+        if (S.n_box && !S.box) return fail(h, EMS_ERR_NOMEM, "CPML shell");
     }
     h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
     h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);

@@ -46,6 +46,16 @@ struct FSlab {
     float* psi_new;
 };
 
+// A box of the CPML layer shell in which every node has the same CPML
+// slabs per component (split schedule): first node, extent, the index of its
+// first node in the side's flat node list, and per component c the slabs in
+// application order, list[c] = count | q0 << 4 | q1 << 8 | q2 << 12 | q3 << 16.
+struct ShellBox {
+    uint32_t lo[3], n[3];
+    uint32_t start;
+    uint32_t list[3];
+};
+
 struct PoleRun {
     uint32_t kb, ke;   // z range of the run's edges
     uint32_t p0;       // state index of the run's first pole

@@ -266,33 +266,70 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
     return T;
 }
 
-// The CPML layer shell of one side (0 H, 1 E). Part A: the rows that an x or
-// y layer of the side holds, whole, as warp segments of at most 32 z-nodes
-// (row i*ny + j, first z | count << 24). Part B: every other row, each with
-// the z-indices that a z layer of the side holds (kz, shared by all rows).
-// Requires nz < 2^24.
-struct ShellTables {
-    std::vector<uint2> seg;
-    std::vector<uint32_t> rows_b;
-    std::vector<uint32_t> kz;
-};
-
-inline ShellTables shell_tables(const std::vector<uint32_t> cmask[3], uint32_t nx, uint32_t ny, uint32_t nz, int side) {
-    const uint32_t m = 0xfffu << (side * 12);
-    ShellTables S;
-    if (cmask[0].empty()) return S;
-    for (uint32_t k = 0; k < nz; ++k)
-        if (cmask[2][k] & m) S.kz.push_back(k);
-    for (uint32_t i = 0; i < nx; ++i)
-        for (uint32_t j = 0; j < ny; ++j) {
-            const uint32_t row = i * ny + j;
-            if ((cmask[0][i] | cmask[1][j]) & m) {
-                for (uint32_t k = 0; k < nz; k += 32) S.seg.push_back(uint2{row, k | (std::min(32u, nz - k) << 24)});
-            } else if (!S.kz.empty()) {
-                S.rows_b.push_back(row);
-            }
+// The CPML layer shell of one side (0 H, 1 E) as boxes with one slab set
+// per component each. Along every axis the slabs' bounds and n − 1, n cut the
+// grid into intervals; in a product of intervals every node lies in the same
+// slabs and has the same components (a component is missing on the high
+// faces, as in the update), so a box needs no per-node test. Boxes with no
+// correction are dropped. Returns the boxes and the total node count.
+inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t nodes[3], int side, uint32_t* total) {
+    std::vector<uint32_t> bp[3];
+    for (int a = 0; a < 3; ++a) bp[a] = {0u, (uint32_t)nodes[a] - 1u, (uint32_t)nodes[a]};
+    for (const FusedSlabSpec& sp : T.slabs) {
+        if (sp.side != side) continue;
+        for (int a = 0; a < 3; ++a) {
+            bp[a].push_back((uint32_t)sp.src->lo[a]);
+            bp[a].push_back((uint32_t)sp.src->hi[a]);
         }
-    return S;
+    }
+    for (int a = 0; a < 3; ++a) {
+        std::sort(bp[a].begin(), bp[a].end());
+        bp[a].erase(std::unique(bp[a].begin(), bp[a].end()), bp[a].end());
+    }
+    // Slabs of this side per component, in application order.
+    std::vector<const FusedSlabSpec*> by[3];
+    for (int c = 0; c < 3; ++c) by[c].assign(T.nslab[side][c], nullptr);
+    for (const FusedSlabSpec& sp : T.slabs)
+        if (sp.side == side) by[sp.comp][sp.q] = &sp;
+    std::vector<ShellBox> out;
+    uint64_t sum = 0;
+    for (size_t xi = 0; xi + 1 < bp[0].size(); ++xi)
+        for (size_t yi = 0; yi + 1 < bp[1].size(); ++yi)
+            for (size_t zi = 0; zi + 1 < bp[2].size(); ++zi) {
+                const uint32_t lo[3] = {bp[0][xi], bp[1][yi], bp[2][zi]};
+                const uint32_t hi[3] = {bp[0][xi + 1], bp[1][yi + 1], bp[2][zi + 1]};
+                ShellBox B{};
+                bool any = false;
+                for (int c = 0; c < 3; ++c) {
+                    // The component exists in the box (the update's conditions:
+                    // E_c needs index c + 1 < n_c, H_c both other indices + 1 < n;
+                    // n − 1 is a cut, so lo decides for the whole box).
+                    const int p1 = (c + 1) % 3, p2 = (c + 2) % 3;
+                    const bool valid = side ? lo[c] + 1 < nodes[c]
+                                            : (lo[p1] + 1 < nodes[p1]) && (lo[p2] + 1 < nodes[p2]);
+                    uint32_t cnt = 0, list = 0;
+                    for (int q = 0; valid && q < (int)by[c].size(); ++q) {
+                        const ems_cpml_slab* sl = by[c][q]->src;
+                        bool in = true;
+                        for (int a = 0; a < 3; ++a) in = in && sl->lo[a] <= lo[a] && hi[a] <= sl->hi[a];
+                        if (!in) continue;
+                        list |= (uint32_t)q << (4 + 4 * cnt);
+                        ++cnt;
+                    }
+                    B.list[c] = list | cnt;
+                    any = any || cnt;
+                }
+                if (!any) continue;
+                for (int a = 0; a < 3; ++a) {
+                    B.lo[a] = lo[a];
+                    B.n[a] = hi[a] - lo[a];
+                }
+                B.start = (uint32_t)sum;
+                sum += (uint64_t)B.n[0] * B.n[1] * B.n[2];
+                out.push_back(B);
+            }
+    *total = (uint32_t)sum;
+    return out;
 }
 
 // Whether a side's dispersive correction may store its corrected value as

@@ -9,9 +9,9 @@
 // move 36 bytes per node (three components read, three read and written).
 //
 // The CPML correction of each side runs after its update as one kernel over
-// the layer shell, listed once at set-up: the rows inside an x or y layer as
-// warp segments of 32 z-nodes, every other row's z-layer nodes one per
-// thread; a node applies every slab that holds it in the slabs' order. Dispersive, lumped, source and probe hooks run as
+// the layer shell, cut once at set-up into boxes whose nodes all lie in the
+// same slabs: a thread takes one node and applies its box's slabs in the
+// slabs' order, with no per-node membership test. Dispersive, lumped, source and probe hooks run as
 // in the per-operator schedule. All expressions are the reference's, so the
 // results equal it bit for bit.
 #pragma once
@@ -166,31 +166,25 @@ __host__ __device__ inline uint32_t split_blocks_x(const Grid& g) {
     return (g.ny * (g.pitch >> 2) + kSplitThreads - 1) / kSplitThreads;
 }
 
-// The layer shell of one side, as the shell kernel reads it: part A, the
-// rows an x or y layer holds whole, as warp segments (row i*ny + j, first z |
-// count << 24); part B, every other row (rows_b) times the z-indices a z
-// layer holds (kz), one thread per node.
+// The layer shell of one side as the shell kernel reads it: boxes with one
+// slab set per component (ShellBox), their nodes numbered box by box (z
+// fastest), one thread per node.
 struct ShellDev {
-    const uint2* seg;
-    uint32_t n_seg, blocks_a;
-    const uint32_t* rows_b;
-    const uint32_t* kz;
-    uint32_t n_b, n_kz;
+    const ShellBox* box;
+    uint32_t n_box, total;
 };
 
-// The CPML chain of one field value: every slab of component C on side
-// SIDE whose bit is set and which holds the node, in order (the arithmetic
-// of cpml_body, inline).
+// The CPML chain of one field value over the slabs of `list` (count | q…),
+// in order: ψ = flush(b·ψ + a·s), t = flush(t + coef·(k·s + ψ)), with s = sA
+// or sB by the slab's normal (the arithmetic of cpml_body; every listed
+// slab holds the node).
 template <int SIDE, int C>
-__device__ __forceinline__ float shell_chain(const FusedParams& P, uint32_t bits, uint32_t i, uint32_t j, uint32_t k,
+__device__ __forceinline__ float shell_chain(const FusedParams& P, uint32_t list, uint32_t i, uint32_t j, uint32_t k,
                                              float t, float coef, float sA, float sB) {
     constexpr uint32_t na = (C + 1) % 3;
-    uint32_t m = (bits >> (SIDE * 12 + C * 4)) & 15u;
-    while (m) {
-        const int q = __ffs(m) - 1;
-        m &= m - 1;
-        const FSlab& s = P.slab[SIDE][C][q];
-        if (i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1] || k < s.lo[2] || k >= s.hi[2]) continue;
+    const uint32_t cnt = list & 15u;
+    for (uint32_t e = 0; e < cnt; ++e) {
+        const FSlab& s = P.slab[SIDE][C][(list >> (4 + 4 * e)) & 15u];
         const uint32_t d = s.normal == 0 ? i - s.lo[0] : (s.normal == 1 ? j - s.lo[1] : k - s.lo[2]);
         const uint32_t at = ((i - s.lo[0]) * (s.hi[1] - s.lo[1]) + (j - s.lo[1])) * (s.hi[2] - s.lo[2]) + (k - s.lo[2]);
         const float sv = s.normal == na ? sA : sB;
@@ -201,80 +195,77 @@ __device__ __forceinline__ float shell_chain(const FusedParams& P, uint32_t bits
     return t;
 }
 
-// CPML correction of the node (i, j, k) on one side (0: H edges after the
-// H update, 1: E edges after the E update) (src/engine/boundary/cpml.rs:
-// 445-520, 657-676). The curl differences are those of the update: A along
-// next(c), B along prev(c); a slab takes s = A or −B by its normal.
+// CPML correction of the node (i, j, k) of box B on one side (0: H edges
+// after the H update, 1: E edges after the E update)
+// (src/engine/boundary/cpml.rs:445-520, 657-676). The curl differences are
+// those of the update: A along next(c), B along prev(c); a slab takes s = A
+// or −B by its normal.
 template <int SIDE>
-__device__ __forceinline__ void shell_node(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k) {
+__device__ __forceinline__ void shell_node(const FusedParams& P, const ShellBox& Bx, uint32_t i, uint32_t j,
+                                           uint32_t k) {
     const Grid& g = P.g;
-    const uint32_t bits = P.cmask[0][i] | P.cmask[1][j] | P.cmask[2][k];
-    const uint32_t sb = bits >> (SIDE * 12);  // this side's bits: component c at 4c
-    if (!(sb & 0xfffu)) return;
     const uint32_t sj = g.pitch, si = g.ny * g.pitch;
     const uint32_t idx = i * si + j * sj + k, row = i * g.ny + j;
+    const uint32_t l0 = Bx.list[0], l1 = Bx.list[1], l2 = Bx.list[2];
     if (SIDE == 0) {
         const float *ux = P.un[0], *uy = P.un[1], *uz = P.un[2];
-        if ((sb & 0xfu) && j + 1 < g.ny && k + 1 < g.nz) {
+        if (l0 & 15u) {
             const float A = __fsub_rn(uz[idx + sj], uz[idx]), B = __fsub_rn(uy[idx + 1], uy[idx]);
             const float db = lane_row(P, 9, row)[k];
-            P.in[0][idx] = shell_chain<0, 0>(P, bits, i, j, k, P.in[0][idx], -db, A, __fmul_rn(-1.0f, B));
+            P.in[0][idx] = shell_chain<0, 0>(P, l0, i, j, k, P.in[0][idx], -db, A, __fmul_rn(-1.0f, B));
         }
-        if ((sb & 0xf0u) && i + 1 < g.nx && k + 1 < g.nz) {
+        if (l1 & 15u) {
             const float A = __fsub_rn(ux[idx + 1], ux[idx]), B = __fsub_rn(uz[idx + si], uz[idx]);
             const float db = lane_row(P, 10, row)[k];
-            P.in[1][idx] = shell_chain<0, 1>(P, bits, i, j, k, P.in[1][idx], -db, A, __fmul_rn(-1.0f, B));
+            P.in[1][idx] = shell_chain<0, 1>(P, l1, i, j, k, P.in[1][idx], -db, A, __fmul_rn(-1.0f, B));
         }
-        if ((sb & 0xf00u) && i + 1 < g.nx && j + 1 < g.ny) {
+        if (l2 & 15u) {
             const float A = __fsub_rn(uy[idx + si], uy[idx]), B = __fsub_rn(ux[idx + sj], ux[idx]);
             const float db = lane_row(P, 11, row)[k];
-            P.in[2][idx] = shell_chain<0, 2>(P, bits, i, j, k, P.in[2][idx], -db, A, __fmul_rn(-1.0f, B));
+            P.in[2][idx] = shell_chain<0, 2>(P, l2, i, j, k, P.in[2][idx], -db, A, __fmul_rn(-1.0f, B));
         }
     } else {
         const float *ix = P.in[0], *iy = P.in[1], *iz = P.in[2];
-        if ((sb & 0xfu) && i + 1 < g.nx) {
+        if (l0 & 15u) {
             const float A = __fsub_rn(iz[idx], j > 0 ? iz[idx - sj] : 0.0f);
             const float B = __fsub_rn(iy[idx], k > 0 ? iy[idx - 1] : 0.0f);
             const float cb = lane_row(P, 3, row)[k];
-            P.un[0][idx] = shell_chain<1, 0>(P, bits, i, j, k, P.un[0][idx], cb, A, __fmul_rn(-1.0f, B));
+            P.un[0][idx] = shell_chain<1, 0>(P, l0, i, j, k, P.un[0][idx], cb, A, __fmul_rn(-1.0f, B));
         }
-        if ((sb & 0xf0u) && j + 1 < g.ny) {
+        if (l1 & 15u) {
             const float A = __fsub_rn(ix[idx], k > 0 ? ix[idx - 1] : 0.0f);
             const float B = __fsub_rn(iz[idx], i > 0 ? iz[idx - si] : 0.0f);
             const float cb = lane_row(P, 4, row)[k];
-            P.un[1][idx] = shell_chain<1, 1>(P, bits, i, j, k, P.un[1][idx], cb, A, __fmul_rn(-1.0f, B));
+            P.un[1][idx] = shell_chain<1, 1>(P, l1, i, j, k, P.un[1][idx], cb, A, __fmul_rn(-1.0f, B));
         }
-        if ((sb & 0xf00u) && k + 1 < g.nz) {
+        if (l2 & 15u) {
             const float A = __fsub_rn(iy[idx], i > 0 ? iy[idx - si] : 0.0f);
             const float B = __fsub_rn(ix[idx], j > 0 ? ix[idx - sj] : 0.0f);
             const float cb = lane_row(P, 5, row)[k];
-            P.un[2][idx] = shell_chain<1, 2>(P, bits, i, j, k, P.un[2][idx], cb, A, __fmul_rn(-1.0f, B));
+            P.un[2][idx] = shell_chain<1, 2>(P, l2, i, j, k, P.un[2][idx], cb, A, __fmul_rn(-1.0f, B));
         }
     }
 }
 
-// CPML correction of one side over its layer shell: blocks [0, blocks_a)
-// take part A (one warp per segment), the rest part B (one thread per node).
+// Node `block·256 + tid` of the side's shell: its box by binary search over
+// the boxes' first nodes, then its (i, j, k) in the box (z fastest).
 template <int SIDE>
 __device__ __forceinline__ void shell_item(const FusedParams& P, const ShellDev& S, uint32_t block, uint32_t tid) {
-    const Grid& g = P.g;
-    uint32_t row, k;
-    if (block < S.blocks_a) {
-        const uint32_t w = block * kShellWarps + (tid >> 5), lane = tid & 31u;
-        if (w >= S.n_seg) return;
-        const uint2 sg = S.seg[w];
-        if (lane >= (sg.y >> 24)) return;
-        row = sg.x;
-        k = (sg.y & 0xffffffu) + lane;
-    } else {
-        const uint32_t t = (block - S.blocks_a) * (32 * kShellWarps) + tid;
-        if (t >= S.n_b * S.n_kz) return;
-        const uint32_t r = t / S.n_kz;
-        row = S.rows_b[r];
-        k = S.kz[t - r * S.n_kz];
+    const uint32_t t = block * (32 * kShellWarps) + tid;
+    if (t >= S.total) return;
+    uint32_t lo = 0, hi = S.n_box;  // box[lo].start <= t < box[hi].start
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&S.box[mid].start) <= t) lo = mid;
+        else hi = mid;
     }
-    const uint32_t i = row / g.ny;
-    shell_node<SIDE>(P, i, row - i * g.ny, k);
+    const ShellBox& Bx = S.box[lo];
+    const uint32_t local = t - Bx.start;
+    const uint32_t r = local / Bx.n[2];
+    const uint32_t k = Bx.lo[2] + (local - r * Bx.n[2]);
+    const uint32_t i = Bx.lo[0] + r / Bx.n[1];
+    const uint32_t j = Bx.lo[1] + (r - (r / Bx.n[1]) * Bx.n[1]);
+    shell_node<SIDE>(P, Bx, i, j, k);
 }
 
 template <int SIDE>
@@ -286,7 +277,7 @@ __global__ void __launch_bounds__(32 * kShellWarps) k_shell(const __grid_constan
 // Blocks of the shell kernel for a side.
 __host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
     const uint32_t tb = 32 * kShellWarps;
-    return S.blocks_a + (uint32_t)(((uint64_t)S.n_b * S.n_kz + tb - 1) / tb);
+    return (S.total + tb - 1) / tb;
 }
 
 // Dispersive correction of one side, one edge per thread, the constants

@@ -391,14 +391,23 @@ def s11_db(steps: np.ndarray, v: np.ndarray, i: np.ndarray, dt: float, freqs: np
 # ---------------------------------------------------------------------------
 # Runs: records from the batched solver, training, and the early-stop driver.
 
-def port_records(models, ports, steps: int, device: int = 0):
-    """Port V and I series of every model after `steps` steps, stepped as
-    one batch: list of (v, i) float64 arrays of length `steps`."""
+def port_records(models, ports, steps, device: int = 0):
+    """Port V and I series of every model, stepped as one batch: model q
+    runs steps[q] steps (an int: all the same) and is frozen there while the
+    others go on. List of (v, i) float64 arrays of length steps[q]."""
     from ems_b200 import Batch
 
-    b = Batch(models, device=device, max_steps=steps)
-    b.run(steps)
-    out = [(b.samples(q, ports[q], 1), b.samples(q, ports[q], 2)) for q in range(len(models))]
+    n = len(models)
+    need = [int(steps)] * n if np.isscalar(steps) else [int(x) for x in steps]
+    b = Batch(models, device=device, max_steps=max(need))
+    done = 0
+    for target in sorted(set(need)):
+        b.run(target - done)
+        done = target
+        for q in range(n):
+            if need[q] == target:
+                b.set_active(q, False)
+    out = [(b.samples(q, ports[q], 1), b.samples(q, ports[q], 2)) for q in range(n)]
     b.close()
     return out
 

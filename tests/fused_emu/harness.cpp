@@ -426,13 +426,12 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
         P.uo[a] = P.un[a] = buf[a].data();
         P.io[a] = P.in[a] = buf[3 + a].data();
     }
-    ShellTables st[2];
+    std::vector<ShellBox> st[2];
     ShellDev sd[2];
     for (int side = 0; side < 2; ++side) {
-        st[side] = shell_tables(T.cmask, g.nx, g.ny, g.nz, side);
-        sd[side] = ShellDev{st[side].seg.data(), (uint32_t)st[side].seg.size(),
-                            (uint32_t)((st[side].seg.size() + kShellWarps - 1) / kShellWarps), st[side].rows_b.data(),
-                            st[side].kz.data(), (uint32_t)st[side].rows_b.size(), (uint32_t)st[side].kz.size()};
+        uint32_t total = 0;
+        st[side] = shell_boxes(T, d->nodes, side, &total);
+        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total};
     }
     const unsigned gx = split_blocks_x(g);
     std::vector<double> partials((size_t)gx * g.nx, 0.0);
