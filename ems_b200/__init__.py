@@ -46,6 +46,21 @@ class EngineError(RuntimeError):
 # ctypes declarations of include/ems_gpu.h and include/ems_host.h
 
 
+class FreqDumpSpec(C.Structure):
+    """``ems_freq_dump`` (include/ems_gpu.h)."""
+
+    _fields_ = [
+        ("field", C.c_int32),
+        ("lo", C.c_uint64 * 3),
+        ("hi", C.c_uint64 * 3),
+        ("stride", C.c_uint64 * 3),
+        ("inv_len", C.c_void_p * 3),
+        ("n_freqs", C.c_size_t),
+        ("freqs", C.c_void_p),
+        ("interval", C.c_uint64),
+    ]
+
+
 class EngineDesc(C.Structure):
     _fields_ = [
         ("nodes", C.c_uint64 * 3),
@@ -214,6 +229,8 @@ GPU_SYMBOLS = {
     "ems_gpu_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "ems_gpu_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "ems_gpu_freq_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ems_gpu_freq_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t]),
     "ems_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
     "ems_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -382,6 +399,22 @@ class Model:
 
     def cells(self) -> CellSet:
         return CellSet(self)
+
+    def inv_edge_lengths(self, axis: int, dual: bool = False) -> np.ndarray:
+        """1/length of the edges along `axis` per node index: primary edges
+        (``Grid::delta``; 0 at the last node, which starts no edge) or dual
+        edges (``Grid::dual_delta``: half a cell on the outer nodes)."""
+        x = self._keep[axis]
+        d = np.diff(x)
+        n = len(x)
+        if dual:
+            dd = np.empty(n)
+            dd[0], dd[-1] = 0.5 * d[0], 0.5 * d[-1]
+            dd[1:-1] = 0.5 * (d[:-1] + d[1:])
+            return 1.0 / dd
+        out = np.zeros(n)
+        out[:-1] = 1.0 / d
+        return out
 
     def fill(self, cells: CellSet, mat: int) -> "Model":
         self._check(self._lib.ems_model_fill(self._p, cells._p, mat), "fill!")
@@ -560,6 +593,31 @@ class Engine:
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value
+
+    def add_freq_dump(self, field: int, lo, hi, freqs, stride=(1, 1, 1), interval: int = 1) -> int:
+        """A running DFT of E (field 0) or H (field 1) over the node box
+        lo..hi (inclusive) on the device (``ems_gpu_freq_dump_add``); the
+        edge lengths come from the model's lines. Returns the dump id."""
+        m = self._model
+        inv = [m.inv_edge_lengths(a, dual=field == 1) for a in range(3)]
+        fr = np.ascontiguousarray(freqs, dtype=np.float64)
+        spec = FreqDumpSpec(field, (C.c_uint64 * 3)(*lo), (C.c_uint64 * 3)(*hi), (C.c_uint64 * 3)(*stride),
+                            (C.c_void_p * 3)(*[x.ctypes.data for x in inv]), len(fr), fr.ctypes.data, interval)
+        i = C.c_size_t()
+        self._ck(self._lib.ems_gpu_freq_dump_add(self._h, C.byref(spec), C.byref(i)))
+        dims = [(hi[a] - lo[a]) // stride[a] + 1 for a in range(3)]
+        self._dumps = getattr(self, "_dumps", {})
+        self._dumps[i.value] = (dims, len(fr))
+        return i.value
+
+    def freq_dump(self, dump: int, k: int) -> np.ndarray:
+        """The transform at frequency index k: complex (nx, ny, nz, 3)."""
+        dims, _ = self._dumps[dump]
+        n = int(np.prod(dims))
+        out = np.empty(n * 6, dtype=np.float64)
+        self._ck(self._lib.ems_gpu_freq_dump_read(self._h, dump, k, out.ctypes.data, out.size))
+        c = out[0::2] + 1j * out[1::2]
+        return c.reshape(*dims, 3)
 
     def autotune(self, cache_path: str) -> None:
         """Schedule autotuning (``ems_gpu_autotune``): cached pick, or timed

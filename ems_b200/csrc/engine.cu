@@ -121,6 +121,14 @@ struct ems_gpu {
         ProbeDev probe;
     };
     std::vector<Op> ops;
+    // Frequency-domain dumps (ems_gpu_freq_dump_add).
+    struct FreqDump {
+        DumpDev d;
+        int field = 0;
+        uint64_t interval = 1;
+        bool started = false;
+    };
+    std::vector<FreqDump> dumps;
     // ---- the fused single-pass schedule
     bool fused_ok = false;
     bool tables_ok = false;         // the table-driven two-kernel schedule can run
@@ -1072,14 +1080,88 @@ static ems_status tune_step(ems_gpu* h) {
     return EMS_OK;
 }
 
+// Samples state m (the state after m steps) into every dump that is due.
+static void dumps_sample(ems_gpu* h, uint64_t m, bool first) {
+    for (auto& D : h->dumps) {
+        if (first == D.started) continue;
+        D.started = true;
+        if (m % D.interval) continue;
+        DumpDev d = D.d;
+        for (int a = 0; a < 3; ++a) d.f[a] = D.field ? h->i[a] : h->u[a];
+        k_dump<<<blocks_for(d.npts, 256), 256, 0, h->stream>>>(d, (double)m);
+        ++h->launches;
+    }
+}
+
+// One step with the dumps: the first sample of a new dump is the state the
+// step starts from (src/engine/dump.rs Cursor::pre_h), then the state after
+// every step (Cursor::post_e).
+static ems_status step_dumped(ems_gpu* h, bool energy) {
+    if (!h->dumps.empty()) dumps_sample(h, h->step, true);
+    ems_status st = (!energy && h->tune.active) ? tune_step(h) : run_step(h, energy);
+    if (st) return st;
+    if (!h->dumps.empty()) dumps_sample(h, h->step, false);
+    return EMS_OK;
+}
+
 ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
     if (!h) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     for (uint64_t s = 0; s < n; ++s) {
-        ems_status st = h->tune.active ? tune_step(h) : run_step(h, false);
+        ems_status st = step_dumped(h, false);
         if (st) return st;
     }
     return check(h, cudaGetLastError(), "run");
+}
+
+ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* id) {
+    if (!h || !spec || !id || spec->field < 0 || spec->field > 1 || !spec->freqs || !spec->n_freqs) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    const Grid& g = h->g;
+    const uint32_t nn[3] = {g.nx, g.ny, g.nz};
+    ems_gpu::FreqDump D;
+    DumpDev& d = D.d;
+    d = DumpDev{};
+    uint64_t npts = 1;
+    for (int a = 0; a < 3; ++a) {
+        const uint64_t st = spec->stride[a] ? spec->stride[a] : 1;
+        if (spec->lo[a] > spec->hi[a] || spec->hi[a] >= nn[a] || !spec->inv_len[a]) return EMS_ERR_INVALID;
+        d.lo[a] = (uint32_t)spec->lo[a];
+        d.st[a] = (uint32_t)st;
+        d.n[a] = (uint32_t)((spec->hi[a] - spec->lo[a]) / st + 1);
+        npts *= d.n[a];
+        d.inv_len[a] = h->upload(spec->inv_len[a], nn[a]);
+        if (!d.inv_len[a]) return fail(h, EMS_ERR_NOMEM, "dump");
+    }
+    if (npts * spec->n_freqs * 6 >= (1ull << 34)) return fail(h, EMS_ERR_INVALID, "dump too large");
+    d.pitch = g.pitch;
+    d.ny = g.ny;
+    d.npts = (uint32_t)npts;
+    d.nf = (uint32_t)spec->n_freqs;
+    d.freqs = h->upload(spec->freqs, spec->n_freqs);
+    d.dt = h->dt;
+    d.t0 = spec->field ? -0.5 * h->dt : 0.0;
+    d.acc = h->alloc<double>(npts * spec->n_freqs * 6);
+    if (!d.freqs || !d.acc) return fail(h, EMS_ERR_NOMEM, "dump");
+    D.field = spec->field;
+    D.interval = spec->interval ? spec->interval : 1;
+    h->dumps.push_back(D);
+    *id = h->dumps.size() - 1;
+    return check(h, cudaStreamSynchronize(h->stream), "dump");
+}
+
+ems_status ems_gpu_freq_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap) {
+    if (!h || !out || id >= h->dumps.size()) return EMS_ERR_INVALID;
+    const auto& D = h->dumps[id];
+    if (k >= D.d.nf || cap < (size_t)D.d.npts * 6) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (check(h, cudaMemcpyAsync(out, D.d.acc + (size_t)k * D.d.npts * 6, (size_t)D.d.npts * 6 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, h->stream), "dump read") ||
+        check(h, cudaStreamSynchronize(h->stream), "dump read"))
+        return EMS_ERR_CUDA;
+    const double s = (double)D.interval * h->dt;
+    for (size_t q = 0; q < (size_t)D.d.npts * 6; ++q) out[q] *= s;
+    return EMS_OK;
 }
 
 ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
@@ -1143,7 +1225,7 @@ ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
         if (check(h, cudaStreamSynchronize(h->stream), "energy")) return EMS_ERR_CUDA;
         w_ops += x;
     }
-    ems_status st = run_step(h, true);
+    ems_status st = step_dumped(h, true);
     if (st) return st;
     double w = 0.0;
     if (check(h, cudaMemcpyAsync(&w, h->d_energy, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "energy"))

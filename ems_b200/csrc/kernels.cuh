@@ -409,4 +409,47 @@ __global__ void k_branch_energy(LumpedDevT d, double dt, double* out) {
     out[0] = s;
 }
 
+// Frequency-domain dump (src/engine/dump.rs:1420-1700): one running-DFT
+// update of every point of the box with the field of state m. The phase is
+// f·(t0 + m·dt) reduced modulo one cycle with the product's exact rounding
+// error (src/post/dft.rs:196-203), the phasor e^{−j2π·phase}.
+struct DumpDev {
+    const float* f[3];
+    const double* inv_len[3];
+    uint32_t lo[3], st[3], n[3];
+    uint32_t pitch, ny, npts, nf;
+    const double* freqs;
+    double dt, t0;
+    double* acc;  // [nf][npts][3] complex, re and im interleaved
+};
+
+__device__ __forceinline__ double frac_toward_zero(double x) { return x - trunc(x); }
+
+__global__ void __launch_bounds__(256) k_dump(const __grid_constant__ DumpDev d, double m) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= d.npts) return;
+    const uint32_t iz = p % d.n[2], r = p / d.n[2], iy = r % d.n[1], ix = r / d.n[1];
+    const uint32_t i = d.lo[0] + ix * d.st[0], j = d.lo[1] + iy * d.st[1], k = d.lo[2] + iz * d.st[2];
+    const size_t idx = ((size_t)i * d.ny + j) * d.pitch + k;
+    const double x[3] = {__dmul_rn((double)d.f[0][idx], d.inv_len[0][i]),
+                         __dmul_rn((double)d.f[1][idx], d.inv_len[1][j]),
+                         __dmul_rn((double)d.f[2][idx], d.inv_len[2][k])};
+    for (uint32_t q = 0; q < d.nf; ++q) {
+        const double fq = d.freqs[q];
+        const double a = __dmul_rn(fq, d.dt);
+        const double pr = __dmul_rn(a, m);
+        const double e = __fma_rn(a, m, -pr);
+        const double c = __dmul_rn(fq, d.t0);
+        const double ph = frac_toward_zero(__dadd_rn(__dadd_rn(frac_toward_zero(pr), e), frac_toward_zero(c)));
+        double sn, cs;
+        sincospi(__dmul_rn(2.0, ph), &sn, &cs);
+        double* a6 = d.acc + ((size_t)q * d.npts + p) * 6;
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            a6[2 * cc] = __dadd_rn(a6[2 * cc], __dmul_rn(x[cc], cs));
+            a6[2 * cc + 1] = __dsub_rn(a6[2 * cc + 1], __dmul_rn(x[cc], sn));
+        }
+    }
+}
+
 }  // namespace emsk

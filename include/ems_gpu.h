@@ -287,6 +287,35 @@ ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
  * the reference, whose CPU engine has a single code path. */
 ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path);
 
+/* ---- Frequency-domain field dumps (src/engine/dump.rs:1420-1700,
+ * FreqDump with DumpPosition::Native and DumpTiming::State): a running DFT
+ * on the device of one field over a box of nodes.
+ *
+ * field 0 samples E = u/len (primary edge length), field 1 H = i/len (dual
+ * edge length), each component at the edge that starts at the node (raw,
+ * not interpolated); inv_len[c] holds 1/len of the component-c edges per
+ * node index along axis c (nodes[c] values, 0 where no edge). Points are
+ * the nodes lo + q*stride <= hi of the box (inclusive), z fastest. The
+ * states m = 0, 1, 2, ... (the state after m steps; the first sampled is
+ * the state when the dump is added) with m % interval == 0 are accumulated
+ * as X(f) = sum x(t_m) e^{-j 2 pi f t_m} * interval*dt, t_m = m*dt (E) or
+ * (m - 1/2)*dt (H), the phase reduced exactly (post/dft.rs phase_cycles). */
+typedef struct {
+    int32_t field;
+    uint64_t lo[3], hi[3], stride[3];
+    const double* inv_len[3];
+    size_t n_freqs;
+    const double* freqs;
+    uint64_t interval;
+} ems_freq_dump;
+
+/* Adds a dump (before or between runs); *id is its index. */
+ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* id);
+
+/* The transform at frequency index k: 3 complex values (re, im
+ * interleaved: 6 doubles) per point, z fastest; cap in doubles. */
+ems_status ems_gpu_freq_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap);
+
 /* ---- Batches: many models stepping together.
  *
  * No counterpart in the reference, where a parameter sweep runs

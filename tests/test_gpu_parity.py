@@ -231,3 +231,43 @@ def test_split_magnetic_poles(h_source):
     for which in (0, 1, 2):
         _series_equal(g, o, ops["port"], which)
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_freq_dump_equals_the_dft_of_the_oracle_states():
+    """Device frequency dumps (src/engine/dump.rs FreqDump, native values,
+    state timing) against X(f) = Σ_m x(t_m)·e^{−j2πf·t_m}·K·dt over the
+    oracle's states m = 0, K, 2K, … (E at m·dt, H at (m − ½)·dt), E = u/Δ,
+    H = i/Δ*."""
+    m, _ = small_cavity()
+    freqs = [1.5e9, 3.0e9, 4.2e9]
+    g = E.Engine(m)
+    de = g.add_freq_dump(0, (1, 1, 1), (8, 6, 5), freqs, stride=(2, 1, 2), interval=1)
+    dh = g.add_freq_dump(1, (0, 2, 0), (10, 2, 6), freqs, interval=3)
+    o = OracleEngine(m, threads=2)
+    steps = 90
+    want_e = np.zeros((len(freqs), 4, 6, 3, 3), dtype=complex)
+    want_h = np.zeros((len(freqs), 11, 1, 7, 3), dtype=complex)
+    inv_e = [m.inv_edge_lengths(a) for a in range(3)]
+    inv_h = [m.inv_edge_lengths(a, dual=True) for a in range(3)]
+    ie, je, ke = np.arange(1, 9, 2), np.arange(1, 7), np.arange(1, 6, 2)
+    for s in range(steps + 1):
+        if s:
+            o.run(1)
+        u = [o.field(0, a)[np.ix_(ie, je, ke)] for a in range(3)]
+        xe = np.stack([u[0] * inv_e[0][ie][:, None, None], u[1] * inv_e[1][je][None, :, None],
+                       u[2] * inv_e[2][ke][None, None, :]], axis=-1)
+        for q, f in enumerate(freqs):
+            want_e[q] += xe * np.exp(-2j * np.pi * f * s * m.dt) * m.dt
+        if s % 3 == 0:
+            ih, jh, kh = np.arange(0, 11), np.array([2]), np.arange(0, 7)
+            i_ = [o.field(1, a)[np.ix_(ih, jh, kh)] for a in range(3)]
+            xh = np.stack([i_[0] * inv_h[0][ih][:, None, None], i_[1] * inv_h[1][jh][None, :, None],
+                           i_[2] * inv_h[2][kh][None, None, :]], axis=-1)
+            for q, f in enumerate(freqs):
+                want_h[q] += xh * np.exp(-2j * np.pi * f * (s - 0.5) * m.dt) * 3 * m.dt
+    g.run(steps)
+    for q in range(len(freqs)):
+        ge, gh = g.freq_dump(de, q), g.freq_dump(dh, q)
+        assert np.abs(ge).max() > 0 and np.abs(gh).max() > 0
+        assert np.abs(ge - want_e[q]).max() <= 1e-9 * np.abs(want_e[q]).max()
+        assert np.abs(gh - want_h[q]).max() <= 1e-9 * np.abs(want_h[q]).max()
