@@ -19,7 +19,7 @@ Layers (channels-last activations, weights W[out][fan_in]):
     dense 1792→64, SiLU
     dense 64→2·T_OUT                       (V then I)
 
-about 0.26 M parameters. Every layer runs on the kernels of
+about 0.25 M parameters. Every layer runs on the kernels of
 libems_learn.so (include/ems_learn.h): im2col, the bf16 tensor-core GEMM
 (f32 accumulation), bias + activation, their adjoints, MSE and Adam; the
 f32 master weights are copied to bf16 for the GEMMs. torch only holds the
@@ -37,7 +37,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 K_IN = 1024      # samples of V and I the network reads
-T_OUT = 256      # predicted samples per signal
+T_OUT = 384      # predicted samples per signal
 DT_REF = 6.4e-12  # [s] spacing of the input samples
 STRIDE = 16      # spacing of the predicted samples, in DT_REF
 WINDOW = 4 * STRIDE  # verification window after the input, in DT_REF
@@ -336,18 +336,26 @@ class Decision:
     residual: float  # relative misfit over the window
 
 
+TAIL_FLOOR = 0.02  # the prediction must decay below this (of the input's end amplitude)
+
+
 def verify(pred: np.ndarray, v: np.ndarray, i: np.ndarray, dt: float, k_in: int = K_IN, t_out: int = T_OUT,
-           stride: int = STRIDE, window: int = WINDOW, threshold: float = 0.1) -> Decision:
-    """Compares the prediction with the live samples of the window after
-    the input (records of at least decision_step(dt) steps): relative L2
-    misfit of the predicted points inside the window, V and I together."""
+           stride: int = STRIDE, window: int = WINDOW, threshold: float = 0.1,
+           floor: float = TAIL_FLOOR) -> Decision:
+    """Whether a run may stop on its prediction: the predicted points inside
+    the window after the input agree with the live samples (relative L2
+    misfit of V and I together at most `threshold`; records of at least
+    decision_step(dt) steps), and the predicted ring-down has died out
+    within the horizon (RMS of its last 32 points below `floor`), so the
+    reported record holds the whole decay."""
     _, (sv, si) = example_input(v, i, dt, k_in)
     n = window // stride
     tt = tail_times(k_in, t_out, stride)[:n]
     live = np.concatenate([_at(v, dt, False, tt) / sv, _at(i, dt, True, tt) / si])
     want = np.concatenate([pred[:n], pred[t_out:t_out + n]])
     r = float(np.linalg.norm(live - want) / max(np.linalg.norm(live), 1e-12))
-    return Decision(r <= threshold, r)
+    end = max(float(np.sqrt(np.mean(pred[t_out - 32:t_out] ** 2))), float(np.sqrt(np.mean(pred[-32:] ** 2))))
+    return Decision(r <= threshold and end <= floor, r)
 
 
 def spliced(v: np.ndarray, i: np.ndarray, pred: np.ndarray, stop: int, dt: float, k_in: int = K_IN,
