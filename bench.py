@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
-    ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split")
+    ap.add_argument("--schedule", type=int, default=0, help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split, 5 sweep")
     ap.add_argument("--workload", choices=["box", "sweep", "learned"], default="box",
                     help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
                          "sweep; learned: training and held-out evaluation of the learned early stop")
@@ -366,6 +366,11 @@ def run_ours(args):
     if kern[2][1] > 0:
         kname, (kms, kn) = "fused_step", kern[2]
         per_launch = ab["total"]
+    elif schedule == 5:
+        # The sweep: one timed span per step over all chunks' updates and
+        # slab hooks (everything but the serial hooks).
+        kname, (kms, kn) = "sweep_chunks", kern[0]
+        per_launch = ab["total"]
     else:
         kname, (kms, kn) = ("step_h" if schedule == 3 else "update_h"), kern[0]
         per_launch = 36.0 * ab["cells"] + (0.5 * ab["psi"] if schedule == 3 else 0.0)
@@ -387,7 +392,8 @@ def run_ours(args):
                           "achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peaks["hbm_gbs"], 4)},
         "kernels_ms": {("h_update", "e_update", "fused_step")[k]: {"ms": round(v[0], 3), "launches": v[1]}
                        for k, v in kern.items() if v[1]},
-        "schedule": {1: "per-operator kernels", 2: "fused single pass", 3: "two kernels", 4: "split"}[schedule],
+        "schedule": {1: "per-operator kernels", 2: "fused single pass", 3: "two kernels", 4: "split",
+                     5: "sweep"}[schedule],
         "e2e": {"value": round(e2e, 1), "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8,
                 "steps": k_e2e},
         "gpu_launches": launches,

@@ -230,6 +230,7 @@ GPU_SYMBOLS = {
     "ems_gpu_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "ems_gpu_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_gpu_freq_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ems_gpu_set_sweep_planes": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ems_gpu_freq_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t]),
     "ems_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
@@ -589,10 +590,14 @@ class Engine:
 
     @property
     def schedule(self) -> int:
-        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels, 4 split."""
+        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels, 4 split, 5 sweep."""
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value
+
+    def set_sweep_planes(self, planes: int) -> None:
+        """Chunk size of the sweep schedule (5), in x-planes."""
+        self._ck(self._lib.ems_gpu_set_sweep_planes(self._h, planes))
 
     def add_freq_dump(self, field: int, lo, hi, freqs, stride=(1, 1, 1), interval: int = 1) -> int:
         """A running DFT of E (field 0) or H (field 1) over the node box

@@ -147,6 +147,19 @@ struct ems_gpu {
     std::vector<std::pair<int, int>> psi_h_at;     // its place in fp.slab[0][c][q]
     // The split schedule: CPML layer shell segments per side (0 H, 1 E).
     ShellDev shell[2] = {};
+    // The sweep schedule: x chunks of sweep_planes planes, each chunk's
+    // shell boxes (first box, first node) and pole edges (first edge) per
+    // side; entry [chunks] closes the last range.
+    uint32_t sweep_planes = 0;
+    bool sweep_ok = false;
+    std::vector<uint32_t> chunk_box[2], chunk_node[2], chunk_edge[2];
+    std::vector<SlabGeo> slab_geo;       // to re-cut the shell for another chunk size
+    // The chunk loop of a sweep step as a CUDA graph ([0] plain, [1] energy
+    // step), captured on first use; rebuilt when the chunks change.
+    cudaGraphExec_t sweep_graph[2] = {nullptr, nullptr};
+    uint64_t sweep_graph_launches[2] = {0, 0};
+    int nslab[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    std::vector<uint32_t> pole_plane[2]; // plane of every pole edge: electric, magnetic
     const uint32_t* run_of[2] = {nullptr, nullptr};  // per pole edge its run: electric, magnetic
     // The split schedule's pole kernels store the corrected value as the
     // saved value of the side (electric, magnetic) instead of a capture
@@ -355,6 +368,56 @@ bool try_tj(ems_gpu* h, int max_smem) {
     return true;
 }
 
+// The sweep schedule's chunks of S planes: the CPML shell of each side cut
+// into boxes that never straddle a chunk (the split schedule uses the same
+// boxes), each chunk's box and node range, and its pole edges.
+ems_status build_chunks(ems_gpu* h, uint32_t S) {
+    const Grid& g = h->g;
+    const uint64_t nodes[3] = {g.nx, g.ny, g.nz};
+    h->sweep_planes = S;
+    for (auto& gx : h->sweep_graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    std::vector<uint32_t> cuts;
+    for (uint32_t x = S; x < g.nx; x += S) cuts.push_back(x);
+    for (int side = 0; side < 2; ++side) {
+        uint32_t total = 0;
+        const std::vector<ShellBox> boxes = shell_boxes(h->slab_geo, h->nslab[side], nodes, side, &total, cuts);
+        ShellDev& Sd = h->shell[side];
+        Sd = ShellDev{};
+        Sd.n_box = (uint32_t)boxes.size();
+        Sd.total = total;
+        if (Sd.n_box) {
+            Sd.box = h->upload(boxes.data(), boxes.size());
+            if (!Sd.box) return fail(h, EMS_ERR_NOMEM, "CPML shell");
+        }
+        auto& cb = h->chunk_box[side];
+        auto& cn = h->chunk_node[side];
+        cb.clear();
+        cn.clear();
+        size_t q = 0;
+        for (uint32_t a0 = 0; a0 < g.nx; a0 += S) {
+            while (q < boxes.size() && boxes[q].lo[0] < a0) ++q;
+            cb.push_back((uint32_t)q);
+            cn.push_back(q < boxes.size() ? boxes[q].start : total);
+        }
+        cb.push_back((uint32_t)boxes.size());
+        cn.push_back(total);
+        auto& ce = h->chunk_edge[side];
+        ce.clear();
+        const auto& pl = h->pole_plane[side];
+        size_t e = 0;
+        for (uint32_t a0 = 0; a0 < g.nx; a0 += S) {
+            while (e < pl.size() && pl[e] < a0) ++e;
+            ce.push_back((uint32_t)e);
+        }
+        ce.push_back((uint32_t)pl.size());
+    }
+    return EMS_OK;
+}
+
 // Builds the tables of the table-driven schedules (fused_tables.h) and
 // uploads them: the two-kernel schedule runs every model whose CPML and
 // dispersive operators are single; the fused kernel in addition needs no
@@ -443,16 +506,36 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         h->tables_why = h->fused_why = "z rows of 2^24 nodes or more";
         return EMS_OK;
     }
+    h->slab_geo = slab_geometry(T);
+    for (int sd = 0; sd < 2; ++sd)
+        for (int c = 0; c < 3; ++c) h->nslab[sd][c] = T.nslab[sd][c];
+    // The plane of every pole edge (a side's edges are in plane order).
     for (int side = 0; side < 2; ++side) {
-        uint32_t total = 0;
-        const std::vector<ShellBox> boxes = shell_boxes(T, d->nodes, side, &total);
-        ShellDev& S = h->shell[side];
-        S = ShellDev{};
-        S.n_box = (uint32_t)boxes.size();
-        S.total = total;
-        if (S.n_box) S.box = h->upload(boxes.data(), boxes.size());
-        if (S.n_box && !S.box) return fail(h, EMS_ERR_NOMEM, "CPML shell");
+        h->pole_plane[side].clear();
+        for (size_t k = 0; k < d->n_ops; ++k)
+            if (d->ops[k].kind == EMS_OP_POLES) {
+                const auto* pp = (const ems_poles*)d->ops[k].table;
+                const ems_pole_side* ps = side ? &pp->magnetic : &pp->electric;
+                const uint64_t per_plane = (uint64_t)g.ny * g.nz;
+                for (size_t e = 0; e < ps->n_edges; ++e) h->pole_plane[side].push_back((uint32_t)(ps->node[e] / per_plane));
+            }
     }
+    {
+        int l2 = 0;
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device);
+        const double plane = 6.0 * g.ny * g.pitch * 4.0;
+        const uint32_t S = (uint32_t)std::max(2.0, std::min(64.0, std::floor(0.45 * (l2 > 0 ? l2 : 50 << 20) / plane)));
+        ems_status st = build_chunks(h, S);
+        if (st) return st;
+    }
+    // The sweep needs no magnetic sources (their serial hook would sit
+    // between a chunk's H and E updates).
+    h->sweep_ok = true;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind == EMS_OP_SOURCE) {
+            const auto* sr = (const ems_source*)d->ops[k].table;
+            if (sr->kind == EMS_SOFT_H || sr->kind == EMS_HARD_H) h->sweep_ok = false;
+        }
     h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
     h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);
     h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
@@ -505,6 +588,7 @@ int active_schedule(const ems_gpu* h) {
     case 2: return h->fused_ok ? 2 : (h->tables_ok ? 3 : 1);
     case 3: return h->tables_ok ? 3 : 1;
     case 4: return h->tables_ok ? 4 : 1;
+    case 5: return h->tables_ok ? (h->sweep_ok ? 5 : 4) : 1;
     default: return h->tables_ok ? 4 : 1;
     }
 }
@@ -519,6 +603,13 @@ ems_status serial_post_e(ems_gpu* h, const Fields& f);
 // H + E pass into the other buffers, then the serial hooks on the new fields.
 ems_status run_step_fused(ems_gpu* h, bool energy) {
     cudaStream_t s = h->stream;
+    // The fused step swaps the field and ψ buffers: a captured sweep graph
+    // would point at the old ones.
+    for (auto& gx : h->sweep_graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
     ems_status st = serial_pre_e(h, f);
     if (st) return st;
@@ -607,14 +698,125 @@ ems_status run_step_two(ems_gpu* h, bool energy) {
     return EMS_OK;
 }
 
+// One step through the sweep schedule: the split kernels run chunk by
+// chunk along x (H update, its slab hooks, E update, its slab hooks for the
+// chunk's planes), so the fields a chunk's E update reads were just touched
+// by its H update and come from L2. Order is the reference's per node: the E
+// update of plane i needs H of planes i and i − 1 (this chunk and the last,
+// both final) and changes only u of its own planes, which no later H update
+// reads. Lumped elements save u^n before the first chunk (u is unchanged
+// until the E updates); current probes sample after the last chunk (nothing
+// changes i after its slab hooks); magnetic sources are excluded (sweep_ok).
+ems_status run_step_sweep(ems_gpu* h, bool energy) {
+    const Grid& g = h->g;
+    cudaStream_t s = h->stream;
+    Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    Coeffs c;
+    for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
+    FusedParams P = h->fp;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = P.un[a] = h->u[a];
+        P.io[a] = P.in[a] = h->i[a];
+    }
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        fs.psi_old = fs.psi_new = h->psi_h[q].first;
+    }
+    P.partials = h->qpartials;
+    ems_status st = serial_pre_e(h, f);
+    if (st) return st;
+    const ems_gpu::Op* cpml = nullptr;
+    const ems_gpu::Op* poles = nullptr;
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_CPML) cpml = &op;
+        if (op.kind == EMS_OP_POLES) poles = &op;
+    }
+    const bool pf = h->fp.poles_first != 0;
+    // The electric saved values u^n, unless the pole kernel kept them.
+    if (poles && poles->poles.e.n_edges && !(h->fold_prev[0] && h->prev_e_valid)) {
+        k_poles_capture<<<blocks_for(poles->poles.e.n_edges, 256), 256, 0, s>>>(f, poles->poles.e, true);
+        ++h->launches;
+    }
+    const uint32_t bx = split_blocks_x(g), S = h->sweep_planes;
+    auto shell = [&](int side, size_t ch) {
+        const uint32_t n0 = h->chunk_node[side][ch], n1 = h->chunk_node[side][ch + 1];
+        if (!cpml || n1 == n0) return;
+        ShellDev sd = h->shell[side];
+        sd.total = n1 - n0;
+        sd.base = n0;
+        const uint32_t nb = (sd.total + 32 * kShellWarps - 1) / (32 * kShellWarps);
+        if (side) k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, sd);
+        else k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, sd);
+        ++h->launches;
+    };
+    auto pole = [&](int side, size_t ch) {  // side 0 electric, 1 magnetic
+        if (!poles) return;
+        const PoleSideDev& ps = side ? poles->poles.h : poles->poles.e;
+        const uint32_t e0 = h->chunk_edge[side][ch], e1 = h->chunk_edge[side][ch + 1];
+        if (!ps.n_edges || e1 == e0) return;
+        k_poles_runs<<<blocks_for(e1 - e0, 256), 256, 0, s>>>(f, c, ps, side ? P.runs_h : P.runs, side ? P.sets_h : P.sets,
+                                                             h->run_of[side], side ? 0 : 1, h->dt,
+                                                             h->fold_prev[side] ? 1 : 0, e0, e1);
+        ++h->launches;
+    };
+    // The chunk loop (and the energy sum) depends on nothing the host
+    // changes between steps: it is captured once as a CUDA graph, so its
+    // hundreds of small launches cost one graph launch per step.
+    const int gi = energy ? 1 : 0;
+    if (!h->sweep_graph[gi]) {
+        const uint64_t before = h->launches;
+        cudaGraph_t graph = nullptr;
+        if (check(h, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "sweep capture")) return EMS_ERR_CUDA;
+        size_t ch = 0;
+        for (uint32_t a0 = 0; a0 < g.nx; a0 += S, ++ch) {
+            const uint32_t np = std::min(S, g.nx - a0);
+            const dim3 grd(bx, np, 1);
+            if (energy) k_split_h<true><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            else k_split_h<false><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            ++h->launches;
+            if (pf) { pole(1, ch); shell(0, ch); } else { shell(0, ch); pole(1, ch); }
+            k_split_e<<<grd, kSplitThreads, 0, s>>>(P, a0);
+            ++h->launches;
+            if (pf) { pole(0, ch); shell(1, ch); } else { shell(1, ch); pole(0, ch); }
+        }
+        if (energy) {
+            k_reduce_partials<<<1, 1024, 0, s>>>(h->qpartials, h->n_qpartials, h->d_energy);
+            ++h->launches;
+        }
+        if (check(h, cudaStreamEndCapture(s, &graph), "sweep capture")) return EMS_ERR_CUDA;
+        const cudaError_t e = cudaGraphInstantiate(&h->sweep_graph[gi], graph, 0);
+        cudaGraphDestroy(graph);
+        if (check(h, e, "sweep graph")) return EMS_ERR_CUDA;
+        h->sweep_graph_launches[gi] = h->launches - before;
+        h->launches = before;
+    }
+    cudaEvent_t ev = h->prof_begin();
+    if (check(h, cudaGraphLaunch(h->sweep_graph[gi], s), "sweep graph launch")) return EMS_ERR_CUDA;
+    h->launches += h->sweep_graph_launches[gi];
+    h->prof_end(0, ev);
+    // The magnetic saved values (i after the E update), unless kept.
+    if (poles && poles->poles.h.n_edges && !h->fold_prev[1]) {
+        k_poles_capture<<<blocks_for(poles->poles.h.n_edges, 256), 256, 0, s>>>(f, poles->poles.h, false);
+        ++h->launches;
+    }
+    st = serial_post_h(h, f);
+    if (st) return st;
+    st = serial_post_e(h, f);
+    if (st) return st;
+    h->prev_e_valid = h->fold_prev[0];
+    ++h->step;
+    return EMS_OK;
+}
+
 // One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
-    // Only the per-operator and split steps keep the electric saved values.
-    if (sch != 4) h->prev_e_valid = false;
+    // Only the per-operator, split and sweep steps keep the electric saved values.
+    if (sch != 4 && sch != 5) h->prev_e_valid = false;
     if (sch == 2) return run_step_fused(h, energy);
     if (sch == 3) return run_step_two(h, energy);
+    if (sch == 5) return run_step_sweep(h, energy);
     // Schedules 1 and 4 share the hook sequence; split (4) runs the table
     // kernels of split.cuh for the updates and one shell kernel per CPML side.
     const bool split = sch == 4;
@@ -642,9 +844,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
     cudaEvent_t ev = h->prof_begin();
     if (split) {
         if (energy) {
-            k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P);
+            k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
         } else {
-            k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P);
+            k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
         }
     } else if (energy) {
         k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
@@ -677,9 +879,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.h.n_edges && split) {
-                k_poles_runs<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, c, op.poles.h, P.runs_h, P.sets_h,
-                                                                                h->run_of[1], 0, h->dt,
-                                                                                h->fold_prev[1] ? 1 : 0);
+                k_poles_runs<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(
+                    f, c, op.poles.h, P.runs_h, P.sets_h, h->run_of[1], 0, h->dt, h->fold_prev[1] ? 1 : 0, 0u,
+                    (uint32_t)op.poles.h.n_edges);
                 ++h->launches;
             } else if (op.poles.h.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.h, false, h->dt);
@@ -697,7 +899,7 @@ ems_status run_step(ems_gpu* h, bool energy) {
     if (st) return st;
     ev = h->prof_begin();
     if (split) {
-        k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P);
+        k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
     } else {
         k_update_e<<<grd, blk, 0, s>>>(g, f, c);
     }
@@ -718,9 +920,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.e.n_edges && split) {
-                k_poles_runs<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, c, op.poles.e, P.runs, P.sets,
-                                                                                h->run_of[0], 1, h->dt,
-                                                                                h->fold_prev[0] ? 1 : 0);
+                k_poles_runs<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(
+                    f, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, h->fold_prev[0] ? 1 : 0, 0u,
+                    (uint32_t)op.poles.e.n_edges);
                 ++h->launches;
             } else if (op.poles.e.n_edges) {
                 k_poles_correct<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(g, f, c, op.poles.e, true, h->dt);
@@ -1012,6 +1214,8 @@ ems_status ems_gpu_destroy(ems_gpu* h) {
     if (!h) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
+    for (auto& gx : h->sweep_graph)
+        if (gx) cudaGraphExecDestroy(gx);
     h->prof_collect();
     for (cudaEvent_t e : h->ev_free) cudaEventDestroy(e);
     h->bufs.clear();
@@ -1175,7 +1379,8 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     T.key = k;
     T.cache = cache_path;
     int v = 0;
-    if (tune_lookup(T.cache, T.key, &v) && (v == 1 || ((v == 3 || v == 4) && h->tables_ok))) {
+    if (tune_lookup(T.cache, T.key, &v) &&
+        (v == 1 || ((v == 3 || v == 4) && h->tables_ok) || (v == 5 && h->tables_ok && h->sweep_ok))) {
         h->schedule = v;
         return EMS_OK;
     }
@@ -1183,6 +1388,7 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     // share the CPML state buffers).
     T.cand.clear();
     if (h->tables_ok) T.cand = {4, 3};
+    if (h->tables_ok && h->sweep_ok) T.cand.push_back(5);
     T.cand.push_back(1);
     T.ms.assign(T.cand.size(), 0.0);
     T.at = 0;
@@ -1366,12 +1572,23 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 4) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 5) return EMS_ERR_INVALID;
     if (schedule == 2 && !h->fused_ok) return fail(h, EMS_ERR_INVALID, "fused schedule unavailable: " + h->fused_why);
     if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
     if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
+    if (schedule == 5 && !(h->tables_ok && h->sweep_ok))
+        return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources") : h->tables_why));
     h->schedule = schedule;
     return EMS_OK;
+}
+
+ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes) {
+    if (!h || !planes || !h->tables_ok) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (check(h, cudaStreamSynchronize(h->stream), "sweep planes")) return EMS_ERR_CUDA;
+    ems_status st = build_chunks(h, std::min(planes, h->g.nx));
+    if (st) return st;
+    return check(h, cudaStreamSynchronize(h->stream), "sweep planes");
 }
 
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {

@@ -271,15 +271,39 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
 // grid into intervals; in a product of intervals every node lies in the same
 // slabs and has the same components (a component is missing on the high
 // faces, as in the update), so a box needs no per-node test. Boxes with no
-// correction are dropped. Returns the boxes and the total node count.
-inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t nodes[3], int side, uint32_t* total) {
+// correction are dropped; they come x-interval by x-interval, so the boxes
+// of an x range between two cuts are consecutive. Returns the boxes and the
+// total node count.
+// A slab's place and extent, kept by the engine to re-cut the shell.
+struct SlabGeo {
+    int side, comp, q;
+    uint32_t lo[3], hi[3];
+};
+
+inline std::vector<SlabGeo> slab_geometry(const FusedTables& T) {
+    std::vector<SlabGeo> out;
+    for (const FusedSlabSpec& sp : T.slabs) {
+        SlabGeo g{sp.side, sp.comp, sp.q, {}, {}};
+        for (int a = 0; a < 3; ++a) {
+            g.lo[a] = (uint32_t)sp.src->lo[a];
+            g.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        out.push_back(g);
+    }
+    return out;
+}
+
+inline std::vector<ShellBox> shell_boxes(const std::vector<SlabGeo>& slabs, const int nslab[3],
+                                         const uint64_t nodes[3], int side, uint32_t* total,
+                                         const std::vector<uint32_t>& xcuts = {}) {
     std::vector<uint32_t> bp[3];
     for (int a = 0; a < 3; ++a) bp[a] = {0u, (uint32_t)nodes[a] - 1u, (uint32_t)nodes[a]};
-    for (const FusedSlabSpec& sp : T.slabs) {
+    bp[0].insert(bp[0].end(), xcuts.begin(), xcuts.end());  // extra cuts: no box straddles an x chunk
+    for (const SlabGeo& sp : slabs) {
         if (sp.side != side) continue;
         for (int a = 0; a < 3; ++a) {
-            bp[a].push_back((uint32_t)sp.src->lo[a]);
-            bp[a].push_back((uint32_t)sp.src->hi[a]);
+            bp[a].push_back(sp.lo[a]);
+            bp[a].push_back(sp.hi[a]);
         }
     }
     for (int a = 0; a < 3; ++a) {
@@ -287,9 +311,9 @@ inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t no
         bp[a].erase(std::unique(bp[a].begin(), bp[a].end()), bp[a].end());
     }
     // Slabs of this side per component, in application order.
-    std::vector<const FusedSlabSpec*> by[3];
-    for (int c = 0; c < 3; ++c) by[c].assign(T.nslab[side][c], nullptr);
-    for (const FusedSlabSpec& sp : T.slabs)
+    std::vector<const SlabGeo*> by[3];
+    for (int c = 0; c < 3; ++c) by[c].assign(nslab[c], nullptr);
+    for (const SlabGeo& sp : slabs)
         if (sp.side == side) by[sp.comp][sp.q] = &sp;
     std::vector<ShellBox> out;
     uint64_t sum = 0;
@@ -309,7 +333,7 @@ inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t no
                                             : (lo[p1] + 1 < nodes[p1]) && (lo[p2] + 1 < nodes[p2]);
                     uint32_t cnt = 0, list = 0;
                     for (int q = 0; valid && q < (int)by[c].size(); ++q) {
-                        const ems_cpml_slab* sl = by[c][q]->src;
+                        const SlabGeo* sl = by[c][q];
                         bool in = true;
                         for (int a = 0; a < 3; ++a) in = in && sl->lo[a] <= lo[a] && hi[a] <= sl->hi[a];
                         if (!in) continue;
@@ -330,6 +354,11 @@ inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t no
             }
     *total = (uint32_t)sum;
     return out;
+}
+
+inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t nodes[3], int side, uint32_t* total,
+                                         const std::vector<uint32_t>& xcuts = {}) {
+    return shell_boxes(slab_geometry(T), T.nslab[side], nodes, side, total, xcuts);
 }
 
 // Whether a side's dispersive correction may store its corrected value as

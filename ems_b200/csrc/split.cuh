@@ -114,12 +114,15 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
     return w;
 }
 
+// Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
 template <bool ENERGY>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P) {
-    const double w = split_h_quad<ENERGY>(P, blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P,
+                                                                         uint32_t i0) {
+    const uint32_t i = i0 + blockIdx.y;
+    const double w = split_h_quad<ENERGY>(P, i, blockIdx.x * kSplitThreads + threadIdx.x);
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
-        if (threadIdx.x == 0) P.partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+        if (threadIdx.x == 0) P.partials[(size_t)i * gridDim.x + blockIdx.x] = s;
     }
 }
 
@@ -157,8 +160,8 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
     stq(P.un[2] + idx, nz_);
 }
 
-__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P) {
-    split_e_quad(P, blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
+__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
+    split_e_quad(P, i0 + blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
 }
 
 // Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.
@@ -171,7 +174,8 @@ __host__ __device__ inline uint32_t split_blocks_x(const Grid& g) {
 // fastest), one thread per node.
 struct ShellDev {
     const ShellBox* box;
-    uint32_t n_box, total;
+    uint32_t n_box, total;  // boxes, and the nodes this launch covers
+    uint32_t base;          // the first node of the launch (box starts count from 0)
 };
 
 // The CPML chain of one field value over the slabs of `list` (count | q…),
@@ -251,8 +255,9 @@ __device__ __forceinline__ void shell_node(const FusedParams& P, const ShellBox&
 // the boxes' first nodes, then its (i, j, k) in the box (z fastest).
 template <int SIDE>
 __device__ __forceinline__ void shell_item(const FusedParams& P, const ShellDev& S, uint32_t block, uint32_t tid) {
-    const uint32_t t = block * (32 * kShellWarps) + tid;
-    if (t >= S.total) return;
+    const uint32_t t0 = block * (32 * kShellWarps) + tid;
+    if (t0 >= S.total) return;
+    const uint32_t t = S.base + t0;
     uint32_t lo = 0, hi = S.n_box;  // box[lo].start <= t < box[hi].start
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -332,11 +337,14 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
     if (save_prev) p.prev[e] = u_new;
 }
 
+// Edges [e0, e1) of the side.
 __global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
                                                     const __grid_constant__ PoleSideDev p, const PoleRun* runs,
                                                     const double* sets, const uint32_t* run_of, int electric,
-                                                    double dt, int save_prev) {
-    poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, blockIdx.x * blockDim.x + threadIdx.x);
+                                                    double dt, int save_prev, uint32_t e0, uint32_t e1) {
+    const uint32_t e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= e1) return;
+    poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e);
 }
 
 }  // namespace emsk

@@ -271,14 +271,20 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
  * allows), 1 = one kernel per field update and operator, 2 = the fused
  * single-pass kernel, 3 = two kernels (H with its slab hooks, E with its
  * slab hooks), 4 = split (streaming H and E updates, one CPML shell kernel
- * per side, the other hooks per operator). Results are identical bit for
+ * per side, the other hooks per operator), 5 = sweep (the split kernels
+ * chunk by chunk along x, so each chunk's E update reads what its H update
+ * left in L2; not with magnetic sources). Results are identical bit for
  * bit. Asking for a schedule the model cannot run returns EMS_ERR_INVALID. */
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 
-/* The schedule steps run with (1 to 4 as above). */
+/* The schedule steps run with (1 to 5 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
-/* Picks the fastest in-place schedule (4, 3 or 1) for this model's grid
+/* The sweep schedule's chunk size in x-planes (set at creation so that a
+ * chunk's fields take under half of L2; larger than nx: one chunk). */
+ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes);
+
+/* Picks the fastest in-place schedule (4, 3, 5 or 1) for this model's grid
  * shape and operators: from `cache_path` (a text file of earlier picks,
  * lines "<key> <schedule> <ms>") if it holds the key, else by timing each
  * candidate over the next steps ems_gpu_run takes (four steps each, the

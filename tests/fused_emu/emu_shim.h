@@ -59,6 +59,12 @@ inline uint32_t min(uint32_t a, uint32_t b) { return a < b ? a : b; }
 inline int __ffs(uint32_t x) { return __builtin_ffs((int)x); }
 template <class T>
 inline T __ldg(const T* p) { return *p; }
+inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
+// Host stand-in (the emulated kernels here do not use it for parity).
+inline void sincospi(double x, double* s, double* c) {
+    *s = std::sin(3.14159265358979323846 * x);
+    *c = std::cos(3.14159265358979323846 * x);
+}
 
 inline unsigned atomicAdd(uint32_t* p, uint32_t v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
 inline int atomicExch(int* p, int v) { return __atomic_exchange_n(p, v, __ATOMIC_SEQ_CST); }

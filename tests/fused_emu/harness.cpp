@@ -431,7 +431,7 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
     for (int side = 0; side < 2; ++side) {
         uint32_t total = 0;
         st[side] = shell_boxes(T, d->nodes, side, &total);
-        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total};
+        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u};
     }
     const unsigned gx = split_blocks_x(g);
     std::vector<double> partials((size_t)gx * g.nx, 0.0);
@@ -444,15 +444,15 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
                     : emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<0>(P, S); });
     };
     for (uint64_t s = 0; s < steps; ++s) {
-        bool ok = energies ? emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<true>(P); })
-                           : emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P); });
+        bool ok = energies ? emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<true>(P, 0u); })
+                           : emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P, 0u); });
         if (!ok || !shell(0)) return 2;
         if (energies) {
             double w = 0.0;
             for (double x : partials) w += x;
             energies[s] = 0.25 * d->dt * w;
         }
-        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P); }) || !shell(1)) return 2;
+        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P, 0u); }) || !shell(1)) return 2;
     }
     for (int c = 0; c < 6; ++c)
         for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)

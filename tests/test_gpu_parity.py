@@ -271,3 +271,48 @@ def test_freq_dump_equals_the_dft_of_the_oracle_states():
         assert np.abs(ge).max() > 0 and np.abs(gh).max() > 0
         assert np.abs(ge - want_e[q]).max() <= 1e-9 * np.abs(want_e[q]).max()
         assert np.abs(gh - want_h[q]).max() <= 1e-9 * np.abs(want_h[q]).max()
+
+
+@pytest.mark.parametrize("planes", [3, 7, 64])
+def test_sweep_schedule_bit_exact(planes):
+    """The sweep schedule (chunks of `planes` x-planes, each chunk's H
+    update, hooks, E update and hooks in turn) on every operator but magnetic
+    sources, against the oracle; chunk edges fall inside the CPML layers,
+    the dispersive blocks and the port."""
+    m, ops = mixed_model(scheme=E.LEAPFROG, h_source=False, steps=160)
+    g = E.Engine(m)
+    g.set_sweep_planes(planes)
+    g.set_schedule(5)
+    assert g.schedule == 5
+    o = OracleEngine(m, threads=4)
+    eg, eo = [], []
+    for s in range(160):
+        if s % 16 == 0:
+            eg.append(g.step_with_energy())
+            eo.append(o.step_with_energy())
+        else:
+            g.run(1)
+            o.run(1)
+    assert_fields_equal(g, o, f"sweep, {planes} planes")
+    for name in ("pv", "pi", "pe"):
+        _series_equal(g, o, ops[name])
+    for which in (0, 1, 2):
+        _series_equal(g, o, ops["port"], which)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+
+
+def test_sweep_schedule_dispersive_box_and_refusals():
+    w = W.dispersive_box(n=40, radius=6, slab=3, cpml=4, steps=200)
+    g = E.Engine(w.model)
+    g.set_sweep_planes(5)
+    g.set_schedule(5)
+    o = OracleEngine(w.model, threads=4)
+    g.run(90)
+    o.run(90)
+    assert_fields_equal(g, o, "sweep dispersive box")
+    for p in w.probes:
+        _series_equal(g, o, p)
+    m, _ = mixed_model(h_source=True, steps=10)
+    h = E.Engine(m)
+    with pytest.raises(E.EngineError):
+        h.set_schedule(5)  # magnetic sources
