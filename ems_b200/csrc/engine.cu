@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -1609,7 +1610,8 @@ struct ems_batch {
     std::vector<ems_gpu*> models;            // owned
     std::vector<std::unique_ptr<DevBuf>> bufs;
     uint64_t max_steps = 0;
-    std::vector<uint32_t> start[BK_KINDS];   // host copies of the prefix sums
+    std::vector<uint32_t> start[BK_KINDS];   // host copies of the prefix sums (frozen models count 0)
+    std::vector<std::array<uint32_t, BK_KINDS>> blocks;  // each model's blocks per kernel kind
     BatchTable T{};
     std::vector<int> active;
     int* d_active = nullptr;
@@ -1715,7 +1717,10 @@ void batch_enqueue_step(ems_batch* b, bool energy) {
 // The persistent grid of each kernel kind for grid code `code`.
 void batch_grids(ems_batch* b, int code) {
     for (int k = 0; k < BK_KINDS; ++k) {
-        const uint64_t work = b->start[k].back();
+        // All models' work, frozen or not: a graph keeps every kernel a
+        // model may need when it is resumed.
+        uint64_t work = 0;
+        for (const auto& mb : b->blocks) work += mb[k];
         uint64_t g = work;
         if (code == 1) g = std::min<uint64_t>(work, b->resident[k]);
         if (code == 2) g = std::min<uint64_t>(work, std::max<uint64_t>(1, b->resident[k] / 2));
@@ -1877,6 +1882,7 @@ ems_status ems_batch_create(const ems_engine_desc* const* descs, size_t n_models
             if (next >= (1ull << 32)) return EMS_ERR_INVALID;
             b->start[k].push_back((uint32_t)next);
         }
+        b->blocks.push_back({blocks[0], blocks[1], blocks[2], blocks[3], blocks[4]});
         // Serial hooks: sources, probes, lumped elements (device tables).
         size_t op_i = 0;
         for (auto& op : h->ops) {
@@ -2075,11 +2081,21 @@ ems_status ems_batch_set_active(ems_batch* b, size_t model, int active) {
     if (!b || model >= b->models.size()) return EMS_ERR_INVALID;
     cudaSetDevice(b->device);
     b->active[model] = active ? 1 : 0;
+    // The packed block table shrinks to the active models (a frozen model's
+    // range becomes empty), so the persistent grids walk only live work;
+    // the graphs read the table from device memory and need no re-capture.
+    const size_t n = b->models.size();
+    for (int k = 0; k < BK_KINDS; ++k) {
+        auto& st = b->start[k];
+        for (size_t m = 0; m < n; ++m) st[m + 1] = st[m] + (b->active[m] ? b->blocks[m][k] : 0u);
+    }
     // Ordered with the graph launches on the batch's stream.
-    if (cudaMemcpyAsync(b->d_active + model, &b->active[model], sizeof(int), cudaMemcpyHostToDevice, b->stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(b->stream) != cudaSuccess)
-        return bfail(b, EMS_ERR_CUDA, "set active");
+    bool ok = cudaMemcpyAsync(b->d_active + model, &b->active[model], sizeof(int), cudaMemcpyHostToDevice,
+                              b->stream) == cudaSuccess;
+    for (int k = 0; ok && k < BK_KINDS; ++k)
+        ok = cudaMemcpyAsync((void*)b->T.start[k], b->start[k].data(), (n + 1) * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, b->stream) == cudaSuccess;
+    if (!ok || cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, EMS_ERR_CUDA, "set active");
     return EMS_OK;
 }
 
