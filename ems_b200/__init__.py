@@ -31,7 +31,9 @@ LORENTZ, DRUDE, DEBYE = 0, 1, 2
 TRAPEZOIDAL, LEAPFROG = 0, 1
 GAUSSIAN = 0
 
-OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE = 1, 2, 3, 4, 5
+OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR = 1, 2, 3, 4, 5, 6
+# Mur options (MurBoundary::openems_order / openems_corners / count_energy).
+MUR_OPENEMS_ORDER, MUR_OPENEMS_CORNERS, MUR_COUNT_ENERGY = 1, 2, 4
 
 
 class EngineError(RuntimeError):
@@ -141,6 +143,14 @@ class RunOutcome(C.Structure):
     ]
 
 
+class MurTable(C.Structure):
+    """``ems_mur`` (include/ems_gpu.h)."""
+
+    _fields_ = [("n", C.c_size_t), ("n_edges", C.c_size_t), ("axis", C.c_void_p), ("node", C.c_void_p),
+                ("inner", C.c_void_p), ("k", C.c_void_p), ("hold", C.c_void_p), ("cap", C.c_void_p),
+                ("openems_order", C.c_int32), ("openems_corners", C.c_int32), ("count_energy", C.c_int32)]
+
+
 _host = None
 _gpu = None
 
@@ -192,6 +202,7 @@ def host_lib() -> C.CDLL:
             "ems_model_add_source": (i, [p, i, sz, p, p, p, i, d, d, u]),
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
+            "ems_model_add_mur": (i, [p, p, p, p, i]),
             "ems_model_desc": (p, [p]),
             "ems_dft": (None, [d, d, p, sz, p, sz, p, p]),
             "ems_drive": (i, [p, p, p]),
@@ -518,6 +529,28 @@ class Model:
         self.ops.append((OP_SOURCE, "source"))
         return k
 
+    def add_mur(self, faces, hold: dict | None = None, flags: int = 0) -> int:
+        """``MurBoundary::with_faces_in(engine, faces, materials)``
+        (src/engine/boundary/mur.rs:355-401): ``faces`` maps a face (index or
+        name) to its phase velocity in m/s, or to None for each edge's local
+        medium speed; ``hold`` maps faces to the step before which their
+        edges are not updated (``hold_faces``); flags: MUR_* bits."""
+        mode = (C.c_int * 6)()
+        vel = (C.c_double * 6)()
+        for f, v in dict(faces).items():
+            f = FACES.index(f) if isinstance(f, str) else int(f)
+            mode[f] = 2 if v is None else 1
+            vel[f] = 0.0 if v is None else float(v)
+        held = None
+        if hold:
+            h = [0] * 6
+            for f, until in hold.items():
+                h[FACES.index(f) if isinstance(f, str) else int(f)] = int(until)
+            held = _u64(h)
+        k = self._check(self._lib.ems_model_add_mur(self._p, mode, vel, held, int(flags)), "add_mur")
+        self.ops.append((OP_MUR, "mur"))
+        return k
+
     def add_probe(self, quantity: int, entries: Sequence[tuple[int, Sequence[int], float]], interval: int = 1) -> int:
         """``Probe::new(quantity).entry(axis, node, w)...interval(n)`` (src/engine/probe.rs)."""
         n = len(entries)
@@ -535,6 +568,36 @@ class Model:
         if not p:
             raise ValueError("model not built")
         return p
+
+    def mur_table(self, op: int) -> dict:
+        """The Mur operator ``op``'s entries as handed to the engine (copies):
+        axis, node/inner as (i, j, k), k (2 per entry), hold, cap, and the
+        number of face edges (the rest are edges shared by two faces)."""
+        d = EngineDesc.from_address(self.desc)
+        ops = (OpEntry * d.n_ops).from_address(d.ops) if d.n_ops else []
+        if not 0 <= op < d.n_ops or ops[op].kind != OP_MUR:
+            raise ValueError("not a Mur operator")
+        t = MurTable.from_address(ops[op].table)
+        n = int(t.n)
+        ny, nz = self.nodes[1], self.nodes[2]
+
+        def arr(ptr, ctype, count, dtype):
+            if not ptr or not count:
+                return np.zeros(count, dtype=dtype)
+            return np.ctypeslib.as_array((ctype * count).from_address(ptr)).astype(dtype)
+
+        def ijk(flat):
+            return np.stack([flat // (ny * nz), (flat // nz) % ny, flat % nz], axis=-1)
+
+        return {
+            "n_edges": int(t.n_edges),
+            "axis": arr(t.axis, C.c_uint8, n, np.int64),
+            "node": ijk(arr(t.node, C.c_uint64, n, np.int64)),
+            "inner": ijk(arr(t.inner, C.c_uint64, 2 * n, np.int64)).reshape(n, 2, 3),
+            "k": arr(t.k, C.c_float, 2 * n, np.float32).reshape(n, 2),
+            "hold": arr(t.hold, C.c_uint64, n, np.int64),
+            "cap": arr(t.cap, C.c_double, n, np.float64),
+        }
 
     def __del__(self):
         if getattr(self, "_p", None):

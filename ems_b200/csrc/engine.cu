@@ -120,6 +120,8 @@ struct ems_gpu {
         LumpedDev lumped;
         SourceDev source;
         ProbeDev probe;
+        MurDevT mur;
+        bool mur_energy = false;
     };
     std::vector<Op> ops;
     // Frequency-domain dumps (ems_gpu_freq_dump_add).
@@ -965,23 +967,37 @@ ems_status serial_post_h(ems_gpu* h, const Fields& f) {
     return EMS_OK;
 }
 
-// pre_e: lumped elements save u^n.
+// pre_e: lumped elements and Mur boundaries save u^n.
 ems_status serial_pre_e(ems_gpu* h, const Fields& f) {
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_LUMPED && (op.lumped.record || op.lumped.has_branch)) {
             k_lumped_pre_e<<<blocks_for(op.lumped.n_edges, 128), 128, 0, h->stream>>>(f.u[op.lumped.axis], op.lumped.d);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_MUR && op.mur.n) {
+            k_mur_save<<<blocks_for(op.mur.n, 256), 256, 0, h->stream>>>(f.u[0], f.u[1], f.u[2], op.mur);
             ++h->launches;
         }
     }
     return EMS_OK;
 }
 
-// Serial post_e hooks in registration order: lumped elements, electric
-// sources, voltage probes.
+// Serial post_e hooks in registration order: lumped elements, Mur
+// boundaries, electric sources, voltage probes.
 ems_status serial_post_e(ems_gpu* h, const Fields& f) {
     cudaStream_t s = h->stream;
     for (auto& op : h->ops) {
-        if (op.kind == EMS_OP_LUMPED) {
+        if (op.kind == EMS_OP_MUR) {
+            const MurDevT& m = op.mur;
+            if (m.n_edges) {
+                k_mur_update<<<blocks_for(m.n_edges, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], m, h->step, 0u, m.n_edges);
+                ++h->launches;
+            }
+            if (m.n > m.n_edges) {
+                k_mur_update<<<blocks_for(m.n - m.n_edges, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], m, h->step,
+                                                                               m.n_edges, m.n);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_LUMPED) {
             ems_gpu::LumpedDev& L = op.lumped;
             double val = (L.has_src && h->step < L.amp.size()) ? L.amp[h->step] : 0.0;
             bool active = L.has_src && val != 0.0;
@@ -1195,6 +1211,64 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
             P.d.node = h->upload(node.data(), pr->n_entries);
             P.d.axis = h->upload(pr->axis, pr->n_entries);
             P.d.weight = h->upload(pr->weight, pr->n_entries);
+            break;
+        }
+        case EMS_OP_MUR: {
+            const auto* m = (const ems_mur*)t;
+            MurDevT& M = op.mur;
+            const size_t n = m->n;
+            auto fail = [](ems_gpu*, ems_status st, const char* why) {
+                std::fprintf(stderr, "ems_gpu: %s\n", why);
+                return st;
+            };
+            if (m->n_edges > n || n >= (1ull << 31) || (n && (!m->axis || !m->node || !m->inner || !m->k)) ||
+                (m->count_energy && n && !m->cap))
+                return fail(h.get(), EMS_ERR_INVALID, "Mur boundary: inconsistent table");
+            std::vector<uint32_t> node(n), inner(2 * n, 0);
+            for (size_t e = 0; e < n; ++e) {
+                const size_t nb = e < m->n_edges ? 1 : 2;
+                if (m->axis[e] > 2 || m->node[e] >= g.n) return fail(h.get(), EMS_ERR_INVALID, "Mur boundary: entry out of range");
+                node[e] = dev_index(g, m->node[e]);
+                for (size_t q = 0; q < nb; ++q) {
+                    if (m->inner[2 * e + q] >= g.n) return fail(h.get(), EMS_ERR_INVALID, "Mur boundary: entry out of range");
+                    inner[2 * e + q] = dev_index(g, m->inner[2 * e + q]);
+                }
+            }
+            // The entries of one launch run in parallel: within the face
+            // edges (and within the shared edges) every entry is distinct
+            // and none reads another's edge.
+            for (int phase = 0; phase < 2; ++phase) {
+                const size_t a0 = phase ? m->n_edges : 0, a1 = phase ? n : m->n_edges, nb = phase ? 2 : 1;
+                std::vector<uint64_t> w, r;
+                for (size_t e = a0; e < a1; ++e) {
+                    w.push_back(m->node[e] * 3 + m->axis[e]);
+                    for (size_t q = 0; q < nb; ++q) r.push_back(m->inner[2 * e + q] * 3 + m->axis[e]);
+                }
+                std::sort(w.begin(), w.end());
+                if (std::adjacent_find(w.begin(), w.end()) != w.end())
+                    return fail(h.get(), EMS_ERR_INVALID, "Mur boundary: an edge listed twice");
+                for (uint64_t x : r)
+                    if (std::binary_search(w.begin(), w.end(), x))
+                        return fail(h.get(), EMS_ERR_INVALID, "Mur boundary: an edge reads another edge of its launch");
+            }
+            M.n = (uint32_t)n;
+            M.n_edges = (uint32_t)m->n_edges;
+            M.openems_order = m->openems_order != 0;
+            M.openems_corners = m->openems_corners != 0;
+            op.mur_energy = m->count_energy != 0 && n;
+            if (n) {
+                M.axis = h->upload(m->axis, n);
+                M.node = h->upload(node.data(), n);
+                M.inner = h->upload(inner.data(), 2 * n);
+                M.k = h->upload(m->k, 2 * n);
+                M.hold = m->hold ? h->upload(m->hold, n) : nullptr;
+                M.cap = op.mur_energy ? h->upload(m->cap, n) : nullptr;
+                M.saved = h->alloc<float>(3 * n);
+                M.last = h->alloc<float>(n);
+                if (!M.axis || !M.node || !M.inner || !M.k || !M.saved || !M.last || (m->hold && !M.hold) ||
+                    (op.mur_energy && !M.cap))
+                    return EMS_ERR_NOMEM;
+            }
             break;
         }
         default:
@@ -1423,6 +1497,9 @@ ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
             ++h->launches;
         } else if (op.kind == EMS_OP_LUMPED && op.lumped.has_branch) {
             k_branch_energy<<<1, 1, 0, h->stream>>>(op.lumped.d, h->dt, h->d_energy + 1);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_MUR && op.mur_energy) {
+            k_mur_energy<<<1, 1024, 0, h->stream>>>(op.mur, h->d_energy + 1);
             ++h->launches;
         } else {
             continue;
@@ -1778,6 +1855,7 @@ std::string batch_ineligible(const ems_engine_desc* d) {
             if (pr->quantity == EMS_PROBE_VOLTAGE) pe = 2;
             else ph = 1;
         }
+        if (kind == EMS_OP_MUR) return "Mur boundaries";
         if (pe >= 0) {
             if (pe < phase_e) return "post_e hooks not in the order lumped, E sources, voltage probes";
             phase_e = pe;

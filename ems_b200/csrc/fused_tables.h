@@ -366,7 +366,8 @@ inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t no
 // one hook later (E edges: after the next H update; H edges: after the E
 // update; src/engine/dispersive.rs:1173-1180, 1730-1744). True when nothing
 // that runs between the correction and that capture writes a pole edge of
-// the side: no lumped element or source of that field on one, and, when the
+// the side: no lumped element, Mur boundary edge or source of that field on
+// one, and, when the
 // CPML hooks run after the dispersive ones, no CPML slab of that side over
 // one. The side's edges are in (plane, axis, row, z) order, so membership is
 // a binary search.
@@ -401,6 +402,10 @@ inline bool pole_prev_fold(const ems_engine_desc* d, bool electric, bool poles_f
             const auto* l = (const ems_lumped*)d->ops[k].table;
             for (size_t e = 0; e < l->n_edges; ++e)
                 if (is_pole_edge(l->node[e], (uint64_t)l->axis)) return false;
+        } else if (kind == EMS_OP_MUR && electric) {
+            const auto* m = (const ems_mur*)d->ops[k].table;
+            for (size_t e = 0; e < m->n; ++e)
+                if (is_pole_edge(m->node[e], m->axis[e])) return false;
         } else if (kind == EMS_OP_SOURCE) {
             const auto* sr = (const ems_source*)d->ops[k].table;
             const bool e_src = sr->kind == EMS_SOFT_E || sr->kind == EMS_HARD_E;

@@ -6,6 +6,7 @@
 #include "../../include/ems_host.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -115,6 +116,11 @@ struct OpStore {
     std::vector<double> dw;
     ems_source source{};
     ems_probe probe{};
+    // Mur
+    std::vector<uint64_t> inner, hold;
+    std::vector<float> mk;
+    std::vector<double> mcap;
+    ems_mur mur{};
 };
 
 }  // namespace
@@ -215,6 +221,7 @@ struct ems_model {
             case EMS_OP_POLES: e.table = &o->poles; break;
             case EMS_OP_LUMPED: e.table = &o->lumped; break;
             case EMS_OP_SOURCE: e.table = &o->source; break;
+            case EMS_OP_MUR: e.table = &o->mur; break;
             default: e.table = &o->probe; break;
             }
             op_list.push_back(e);
@@ -982,6 +989,176 @@ int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, c
     P.weight = op->dw.data();
     P.interval = interval ? interval : 1;
     P.f32_sum = 0;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+// MurBoundary::build (src/engine/boundary/mur.rs:403-604), hold_faces
+// (619-637), openems_order / openems_corners / count_energy (649-679).
+int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6], const uint64_t hold_until[6],
+                      int flags) {
+    if (!m->built) return set_err(m, "build the model before adding operators"), -1;
+    const uint64_t* n = m->n;
+    const double dt = m->dt;
+    // MurBoundary::coefficient (mur.rs:725-727).
+    auto coefficient = [](double v, double dt_, double delta) { return (v * dt_ - delta) / (v * dt_ + delta); };
+    auto face_delta = [&](int f) {
+        const int a = f / 2;
+        return (f & 1) ? m->delta(a, n[a] - 2) : m->delta(a, 0);
+    };
+    bool on[6] = {};
+    float k_face[6] = {};
+    for (int f = 0; f < 6; ++f) {
+        if (mode[f] == 0) continue;
+        if (mode[f] != 1 && mode[f] != 2) return set_err(m, "Mur boundary: face mode must be 0, 1 or 2"), -1;
+        const int a = f / 2;
+        if (mode[f] == 1) {
+            const double v = velocity[f];
+            if (!(std::isfinite(v) && v > 0.0))
+                return set_err(m, "Mur boundary: phase velocity must be finite and > 0"), -1;
+            k_face[f] = (float)coefficient(v, dt, face_delta(f));
+        }
+        if (n[a] < 3) return set_err(m, "Mur boundary: needs at least 3 mesh lines along the face normal"), -1;
+        on[f] = true;
+    }
+    auto plane = [&](int f) -> uint64_t { return (f & 1) ? n[f / 2] - 1 : 0; };
+    auto inner_of = [&](int f, std::array<uint64_t, 3> p) {
+        const int a = f / 2;
+        p[a] = (f & 1) ? p[a] - 1 : p[a] + 1;
+        return p;
+    };
+    auto idx = [&](const std::array<uint64_t, 3>& p) { return m->index(p[0], p[1], p[2]); };
+    // Local phase velocity c0/sqrt(eps_r mu_r) of the edge along t at node on
+    // face f: eps_r of the interior neighbour edge, mu_r of the H face
+    // between them (mur.rs:487-510), both the per-edge values of
+    // EdgeMaterials::from_cells (src/engine/edge_material.rs:376-413).
+    std::string bad;
+    auto local = [&](int f, int t, int o, const std::array<uint64_t, 3>& node) -> float {
+        const int a = f / 2;
+        const auto in = inner_of(f, node);
+        auto hf = node;
+        hf[a] = std::min(node[a], in[a]);
+        const uint64_t pi[3] = {in[0], in[1], in[2]};
+        double cap = 0.0, cond = 0.0;
+        m->primary_edge_cg(t, pi, cap, cond);
+        const int tb = next_axis(t), tc = prev_axis(t);
+        const double eps = cap * (m->delta(t, in[t]) / (m->dual_delta(tb, in[tb]) * m->dual_delta(tc, in[tc]))) / EPS0;
+        const uint64_t ph[3] = {hf[0], hf[1], hf[2]};
+        double l = 0.0, r = 0.0;
+        m->dual_edge_lr(o, ph, l, r);
+        const int ob = next_axis(o), oc = prev_axis(o);
+        const double mu = l * (m->dual_delta(o, hf[o]) / (m->delta(ob, hf[ob]) * m->delta(oc, hf[oc]))) / MU0;
+        const double v = C0 / std::sqrt(eps * mu);
+        if (!(std::isfinite(v) && v > 0.0)) {
+            bad = "Mur boundary: local phase velocity must be finite and > 0";
+            return 0.0f;
+        }
+        return (float)coefficient(v, dt, face_delta(f));
+    };
+    auto coef = [&](int f, int t, int o, const std::array<uint64_t, 3>& node) {
+        return mode[f] == 1 ? k_face[f] : local(f, t, o, node);
+    };
+    // Capacitance of a boundary edge with full dual cells on the outer
+    // planes (mur.rs:469-482), from the interior neighbour's ca, cb
+    // (Coefficients::capacitance, src/engine/coeffs.rs:1066-1076).
+    auto full_c = [&](int t, const std::array<uint64_t, 3>& node, const std::array<uint64_t, 3>& in) {
+        const size_t i = idx(in);
+        const float ca = m->co[t][i], cb = m->co[3 + t][i];
+        const double c = cb == 0.0f ? 0.0 : dt * (1.0 + (double)ca) / (2.0 * (double)cb);
+        double fac = 1.0;
+        for (int b = 0; b < 3; ++b) {
+            if (b == t) continue;
+            const uint64_t k = node[b], ki = in[b], nb = n[b];
+            if (k == 0 || k + 1 == nb) {
+                const double cell = m->delta(b, k == 0 ? 0 : nb - 2);
+                fac *= cell / m->dual_delta(b, ki);
+            }
+        }
+        return std::isfinite(c) ? c * fac : 0.0;
+    };
+    struct Ent {
+        int t;
+        std::array<uint64_t, 3> node, in0, in1;
+        float k0, k1;
+        double c;
+        bool corner;
+    };
+    std::vector<Ent> edges, corners;
+    for (int f = 0; f < 6; ++f) {
+        if (!on[f]) continue;
+        const int a = f / 2;
+        for (int t = 0; t < 3; ++t) {
+            if (t == a) continue;
+            const int o = 3 - a - t;
+            const float* ca = m->co[t].data();
+            const float* cb = m->co[3 + t].data();
+            for (uint64_t p = 0; p + 1 < n[t]; ++p) {
+                for (uint64_t q = 0; q < n[o]; ++q) {
+                    std::array<uint64_t, 3> node{};
+                    node[a] = plane(f);
+                    node[t] = p;
+                    node[o] = q;
+                    const size_t id = idx(node);
+                    if (ca[id] != 0.0f || cb[id] != 0.0f)
+                        return set_err(m, "Mur boundary: the face must be PEC (its tangential edges have ca = cb = 0)"), -1;
+                    int g = -1;
+                    for (int mx = 0; mx < 2; ++mx)
+                        if (on[2 * o + mx] && plane(2 * o + mx) == q) {
+                            g = 2 * o + mx;
+                            break;
+                        }
+                    if (g < 0) {
+                        const auto in = inner_of(f, node);
+                        edges.push_back({t, node, in, in, coef(f, t, o, node), 0.0f, full_c(t, node, in), false});
+                    } else if (f < g) {
+                        const auto i0 = inner_of(f, node), i1 = inner_of(g, node);
+                        corners.push_back({t, node, i0, i1, coef(f, t, o, node), coef(g, t, a, node),
+                                           full_c(t, node, inner_of(g, i0)), true});
+                    }
+                    if (!bad.empty()) return set_err(m, bad.c_str()), -1;
+                }
+            }
+        }
+    }
+    // hold_faces: an entry whose node-to-neighbour step crosses a held
+    // face's plane is held (mur.rs:619-637).
+    auto held = [&](const std::array<uint64_t, 3>& node, const std::array<uint64_t, 3>& in) -> uint64_t {
+        uint64_t until = 0;
+        if (!hold_until) return 0;
+        for (int f = 0; f < 6; ++f) {
+            if (!hold_until[f]) continue;
+            const int a = f / 2;
+            if (node[a] != in[a] && (node[a] == 0) != ((f & 1) != 0)) until = std::max(until, hold_until[f]);
+        }
+        return until;
+    };
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_MUR;
+    for (const auto* list : {&edges, &corners}) {
+        for (const Ent& e : *list) {
+            op->axis.push_back((uint8_t)e.t);
+            op->node.push_back(idx(e.node));
+            op->inner.push_back(idx(e.in0));
+            op->inner.push_back(e.corner ? idx(e.in1) : idx(e.in0));
+            op->mk.push_back(e.k0);
+            op->mk.push_back(e.k1);
+            op->mcap.push_back(e.c);
+            op->hold.push_back(e.corner ? std::max(held(e.node, e.in0), held(e.node, e.in1)) : held(e.node, e.in0));
+        }
+    }
+    ems_mur& M = op->mur;
+    M.n = op->node.size();
+    M.n_edges = edges.size();
+    M.axis = op->axis.data();
+    M.node = op->node.data();
+    M.inner = op->inner.data();
+    M.k = op->mk.data();
+    M.hold = hold_until ? op->hold.data() : nullptr;
+    M.count_energy = (flags & 4) ? 1 : 0;
+    M.cap = M.count_energy ? op->mcap.data() : nullptr;
+    M.openems_order = (flags & 1) ? 1 : 0;
+    M.openems_corners = (flags & 2) ? 1 : 0;
     m->ops.push_back(std::move(op));
     m->refresh_desc();
     return (int)m->ops.size() - 1;

@@ -409,6 +409,72 @@ __global__ void k_branch_energy(LumpedDevT d, double dt, double* out) {
     out[0] = s;
 }
 
+// A Mur boundary on the device (src/engine/boundary/mur.rs:103-139):
+// entries [0, n_edges) face edges, [n_edges, n) edges shared by two faces;
+// inner and k 2 per entry, saved 3 per entry (u_b^n, u_1^n of each
+// neighbour), last the value after the last update (energy).
+struct MurDevT {
+    uint32_t n = 0, n_edges = 0;
+    int openems_order = 0, openems_corners = 0;
+    const uint8_t* axis = nullptr;
+    const uint32_t* node = nullptr;
+    const uint32_t* inner = nullptr;
+    const float* k = nullptr;
+    const uint64_t* hold = nullptr;  // null: no holds
+    const double* cap = nullptr;     // null: energy not counted
+    float* saved = nullptr;
+    float* last = nullptr;
+};
+
+// src/engine/boundary/mur.rs:252-259 mur_1d, rounded step by step.
+__device__ __forceinline__ float mur_1d(float i, float k, float x, float b, int openems) {
+    return openems ? __fadd_rn(__fsub_rn(i, __fmul_rn(k, b)), __fmul_rn(k, x)) : __fadd_rn(i, __fmul_rn(k, __fsub_rn(x, b)));
+}
+
+// pre_e (src/engine/boundary/mur.rs:781-808): u_b^n, u_1^n of every entry.
+__global__ void k_mur_save(float* f0, float* f1, float* f2, MurDevT m) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.n) return;
+    const float* F = m.axis[e] == 0 ? f0 : (m.axis[e] == 1 ? f1 : f2);
+    m.saved[3 * e] = F[m.node[e]];
+    m.saved[3 * e + 1] = F[m.inner[2 * e]];
+    if (e >= m.n_edges) m.saved[3 * e + 2] = F[m.inner[2 * e + 1]];
+}
+
+// post_e (src/engine/boundary/mur.rs:812-843) of the entries [e0, e1): the
+// face edges in one launch, then the shared edges, whose neighbours are
+// face edges, in a second one.
+__global__ void k_mur_update(float* f0, float* f1, float* f2, MurDevT m, uint64_t step, uint32_t e0, uint32_t e1) {
+    const uint32_t e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= e1) return;
+    if (m.hold && step < m.hold[e]) return;
+    float* F = m.axis[e] == 0 ? f0 : (m.axis[e] == 1 ? f1 : f2);
+    const float b = m.saved[3 * e], i0 = m.saved[3 * e + 1];
+    float v;
+    if (e < m.n_edges) {
+        v = mur_1d(i0, m.k[2 * e], F[m.inner[2 * e]], b, m.openems_order);
+    } else if (m.openems_corners) {
+        v = __fsub_rn(i0, __fmul_rn(m.k[2 * e], b));
+    } else {
+        const float v0 = mur_1d(i0, m.k[2 * e], F[m.inner[2 * e]], b, m.openems_order);
+        const float v1 = mur_1d(m.saved[3 * e + 2], m.k[2 * e + 1], F[m.inner[2 * e + 1]], b, m.openems_order);
+        v = __fmul_rn(0.5f, __fadd_rn(v0, v1));
+    }
+    F[m.node[e]] = v;
+    m.last[e] = v;
+}
+
+// Σ ½·C_e·u_e² over the last written values (src/engine/boundary/mur.rs:683-704).
+__global__ void __launch_bounds__(1024) k_mur_energy(MurDevT m, double* out) {
+    double s = 0.0;
+    for (uint32_t e = threadIdx.x; e < m.n; e += blockDim.x) {
+        const double x = (double)m.last[e];
+        s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(0.5, m.cap[e]), x), x));
+    }
+    const double t = block_sum<1024>(s);
+    if (threadIdx.x == 0) out[0] = t;
+}
+
 // Frequency-domain dump (src/engine/dump.rs:1420-1700): one running-DFT
 // update of every point of the box with the field of state m. The phase is
 // f·(t0 + m·dt) reduced modulo one cycle with the product's exact rounding

@@ -49,7 +49,8 @@ typedef enum {
     EMS_OP_POLES = 2,  /* slab hooks post_h / post_e   (src/engine/dispersive.rs:1687-1744)  */
     EMS_OP_LUMPED = 3, /* serial pre_e / post_e        (src/engine/lumped.rs:1123-1236)      */
     EMS_OP_SOURCE = 4, /* serial post_h or post_e      (src/engine/excite.rs:104-173)        */
-    EMS_OP_PROBE = 5   /* serial post_h or post_e      (src/engine/probe.rs:480-510)         */
+    EMS_OP_PROBE = 5,  /* serial post_h or post_e      (src/engine/probe.rs:480-510)         */
+    EMS_OP_MUR = 6     /* serial pre_e / post_e        (src/engine/boundary/mur.rs:781-843)  */
 } ems_op_kind;
 
 /* One CPML slab: the correction of one field component in one face layer
@@ -170,9 +171,38 @@ typedef struct {
     int32_t f32_sum;            /* accumulate in f32 (openEMS current probes) */
 } ems_probe;
 
+/* A first-order Mur absorbing boundary (src/engine/boundary/mur.rs:103-139
+ * Edge and Corner, 249-299 the update). Entries [0, n_edges) are face
+ * edges with one 1-D update, entries [n_edges, n) edges shared by two Mur
+ * faces, updated after every face edge as the mean of two 1-D updates.
+ * Per entry: the E edge along axis[e] at node[e], its interior neighbours
+ * inner[2e] (and inner[2e+1] for a shared edge) and coefficients k[2e]
+ * (k[2e+1]), hold[e] (no update before that step; NULL: none) and cap[e]
+ * (capacitance counted by the energy with count_energy).
+ *   pre_e:  b = u[node], i0 = u[inner0] (i1 = u[inner1])  (u^n)
+ *   post_e: face edge   u[node] = i0 + k0*(u[inner0] - b)
+ *                       (openems_order: (i0 - k0*b) + k0*u[inner0])
+ *           shared edge u[node] = 0.5*(v0 + v1), each v the face update
+ *                       along its own normal (openems_corners: i0 - k0*b)
+ * All in f32. No face edge may be another face edge's neighbour, no
+ * shared edge another shared edge's (the updates run in parallel). */
+typedef struct {
+    size_t n;
+    size_t n_edges;
+    const uint8_t* axis;
+    const uint64_t* node;
+    const uint64_t* inner;     /* 2 per entry (the second unused for face edges) */
+    const float* k;            /* 2 per entry */
+    const uint64_t* hold;      /* NULL: every entry updates from step 0 */
+    const double* cap;         /* NULL unless count_energy */
+    int32_t openems_order;
+    int32_t openems_corners;
+    int32_t count_energy;      /* energy: sum of 1/2 cap u^2 over the last written values */
+} ems_mur;
+
 typedef struct {
     int32_t kind; /* ems_op_kind */
-    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe* */
+    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe*, ems_mur* */
 } ems_op;
 
 /* Everything an engine is built from: the grid size, the time step, the

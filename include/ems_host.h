@@ -121,6 +121,18 @@ int ems_model_add_source_table(ems_model* m, int kind, size_t n, const int* axis
 int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, const uint64_t* nodes,
                         const double* weight, uint64_t interval);
 
+/* A first-order Mur absorbing boundary (MurBoundary::with_faces /
+ * with_faces_in, src/engine/boundary/mur.rs:355-604) on the faces f with
+ * mode[f] = 1 (phase velocity velocity[f] m/s) or 2 (each edge's local
+ * medium speed c0/sqrt(eps_r mu_r)); 0 leaves the face alone. Mur faces
+ * must be PEC. hold_until (NULL: none): no update of the edges at face f
+ * before step hold_until[f] (MurBoundary::hold_faces). flags: 1 openEMS
+ * operation order, 2 openEMS shared-edge update, 4 count the boundary
+ * edges' energy. Edges on two Mur faces take the mean of both updates.
+ * Returns the op index or -1. */
+int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6], const uint64_t hold_until[6],
+                      int flags);
+
 /* The engine descriptor (valid until the model changes or is freed). */
 const ems_engine_desc* ems_model_desc(ems_model* m);
 

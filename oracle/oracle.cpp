@@ -137,6 +137,19 @@ struct Probe {
     std::vector<double> values;
 };
 
+// A Mur boundary (src/engine/boundary/mur.rs:103-139): face edges first,
+// then the edges shared by two Mur faces.
+struct Mur {
+    size_t n_edges = 0;
+    std::vector<uint8_t> axis;
+    std::vector<uint64_t> node, inner, hold;  // inner: 2 per entry
+    std::vector<float> k;                     // 2 per entry
+    std::vector<double> cap;
+    bool openems_order = false, openems_corners = false, count_energy = false;
+    std::vector<float> saved;                 // 3 per entry: u_b^n, u_1^n (both neighbours)
+    std::vector<float> last;                  // value after the last update
+};
+
 struct Op {
     int kind = 0;
     std::vector<CpmlSlab> cpml;
@@ -144,7 +157,14 @@ struct Op {
     Lumped lumped;
     Source source;
     Probe probe;
+    Mur mur;
 };
+
+// src/engine/boundary/mur.rs:252-259 mur_1d: u_b^{n+1} from u_1^n (i),
+// k, u_1^{n+1} (x) and u_b^n (b), in ems's or openEMS's order.
+inline float mur_1d(float i, float k, float x, float b, bool openems) {
+    return openems ? (i - k * b) + k * x : i + k * (x - b);
+}
 
 }  // namespace
 
@@ -381,6 +401,11 @@ struct oracle_engine {
                 pole_energy(op.pe, we);
                 pole_energy(op.ph, wm);
                 x = we + wm;
+            } else if (op.kind == EMS_OP_MUR && op.mur.count_energy) {
+                // src/engine/boundary/mur.rs:683-704 boundary_energy, in entry order.
+                const Mur& m = op.mur;
+                for (size_t e = 0; e < m.node.size(); ++e)
+                    x += 0.5 * m.cap[e] * (double)m.last[e] * (double)m.last[e];
             } else if (op.kind == EMS_OP_LUMPED && op.lumped.has_branch) {
                 // src/engine/lumped.rs:1066-1077 branch_energy
                 const Lumped& l = op.lumped;
@@ -423,6 +448,39 @@ struct oracle_engine {
             double s = 0.0;
             for (size_t e = 0; e < p.axis.size(); ++e) s += p.weight[e] * (double)F[p.axis[e]][p.node[e]];
             p.values.push_back(s);
+        }
+    }
+
+    // src/engine/boundary/mur.rs:781-808 pre_e: u_b^n and u_1^n.
+    void mur_pre_e(Mur& m) {
+        for (size_t e = 0; e < m.node.size(); ++e) {
+            const std::vector<float>& f = u[m.axis[e]];
+            m.saved[3 * e] = f[m.node[e]];
+            m.saved[3 * e + 1] = f[m.inner[2 * e]];
+            if (e >= m.n_edges) m.saved[3 * e + 2] = f[m.inner[2 * e + 1]];
+        }
+    }
+
+    // src/engine/boundary/mur.rs:812-843 post_e: the face edges, then the
+    // shared edges, whose neighbours are face edges updated just before.
+    void mur_post_e(Mur& m) {
+        for (size_t e = 0; e < m.node.size(); ++e) {
+            if (step < m.hold[e]) continue;
+            std::vector<float>& f = u[m.axis[e]];
+            const float b = m.saved[3 * e], i0 = m.saved[3 * e + 1];
+            float v;
+            if (e < m.n_edges) {
+                v = mur_1d(i0, m.k[2 * e], f[m.inner[2 * e]], b, m.openems_order);
+            } else if (m.openems_corners) {
+                v = i0 - m.k[2 * e] * b;
+            } else {
+                const float i1 = m.saved[3 * e + 2];
+                const float v0 = mur_1d(i0, m.k[2 * e], f[m.inner[2 * e]], b, m.openems_order);
+                const float v1 = mur_1d(i1, m.k[2 * e + 1], f[m.inner[2 * e + 1]], b, m.openems_order);
+                v = 0.5f * (v0 + v1);
+            }
+            f[m.node[e]] = v;
+            m.last[e] = v;
         }
     }
 
@@ -520,8 +578,10 @@ struct oracle_engine {
             if (op.kind == EMS_OP_SOURCE) source_apply(op.source, true);
             else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, true);
         }
-        for (Op& op : ops)
+        for (Op& op : ops) {
             if (op.kind == EMS_OP_LUMPED) lumped_pre_e(op.lumped);
+            else if (op.kind == EMS_OP_MUR) mur_pre_e(op.mur);
+        }
         // E half-step with its slab hooks.
         pool->run([&](int sl) {
             const size_t p0 = slab_start[sl], p1 = slab_start[sl + 1];
@@ -538,6 +598,7 @@ struct oracle_engine {
         });
         for (Op& op : ops) {
             if (op.kind == EMS_OP_LUMPED) lumped_post_e(op.lumped);
+            else if (op.kind == EMS_OP_MUR) mur_post_e(op.mur);
             else if (op.kind == EMS_OP_SOURCE) source_apply(op.source, false);
             else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, false);
         }
@@ -693,6 +754,33 @@ int oracle_create(const ems_engine_desc* d, int threads, oracle_engine** out) {
             op.probe.weight = vec(p->weight, p->n_entries);
             op.probe.interval = p->interval ? p->interval : 1;
             op.probe.f32_sum = p->f32_sum != 0;
+            break;
+        }
+        case EMS_OP_MUR: {
+            const auto* m = (const ems_mur*)t;
+            Mur& M = op.mur;
+            if (m->n_edges > m->n || (m->n && (!m->axis || !m->node || !m->inner || !m->k)) ||
+                (m->count_energy && !m->cap)) {
+                delete e;
+                return EMS_ERR_INVALID;
+            }
+            for (size_t q = 0; q < m->n; ++q) {
+                bool ok = m->axis[q] < 3 && m->node[q] < e->n && m->inner[2 * q] < e->n;
+                if (q >= m->n_edges) ok = ok && m->inner[2 * q + 1] < e->n;
+                if (!ok) { delete e; return EMS_ERR_INVALID; }
+            }
+            M.n_edges = m->n_edges;
+            M.axis = vec(m->axis, m->n);
+            M.node = vec(m->node, m->n);
+            M.inner = vec(m->inner, 2 * m->n);
+            M.k = vec(m->k, 2 * m->n);
+            M.hold = m->hold ? vec(m->hold, m->n) : std::vector<uint64_t>(m->n, 0);
+            M.cap = m->count_energy ? vec(m->cap, m->n) : std::vector<double>(m->n, 0.0);
+            M.openems_order = m->openems_order != 0;
+            M.openems_corners = m->openems_corners != 0;
+            M.count_energy = m->count_energy != 0;
+            M.saved.assign(3 * m->n, 0.0f);
+            M.last.assign(m->n, 0.0f);
             break;
         }
         default:
