@@ -187,6 +187,9 @@ def host_lib() -> C.CDLL:
             "ems_model_pec_edges": (i, [p, i, p, p]),
             "ems_model_faces": (i, [p, p]),
             "ems_model_build": (i, [p, d, d]),
+            "ems_model_build_bound": (i, [p, d, i]),
+            "ems_model_openems_timestep": (d, [p, i]),
+            "ems_model_zero_edges": (i, [p, i, i, p, p]),
             "ems_model_dt": (d, [p]),
             "ems_model_courant_limit": (d, [p]),
             "ems_model_coeff": (p, [p, i]),
@@ -203,6 +206,7 @@ def host_lib() -> C.CDLL:
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
             "ems_model_add_mur": (i, [p, p, p, p, i]),
+            "ems_model_probe_f32": (i, [p, i, i]),
             "ems_model_desc": (p, [p]),
             "ems_dft": (None, [d, d, p, sz, p, sz, p, p]),
             "ems_drive": (i, [p, p, p]),
@@ -454,6 +458,28 @@ class Model:
         self._check(self._lib.ems_model_build(self._p, courant, dt or 0.0), "build!")
         return self
 
+    def build_bound(self, dt: float, openems_rounding: bool = False, openems_sigma_m: bool = False) -> "Model":
+        """Builds with ``dt`` as given (``TimeStep::Bound``), the exact or
+        openEMS coefficient rounding (``CoeffRounding``) and csx's or
+        openEMS's average of the magnetic conductivity."""
+        flags = (1 if openems_rounding else 0) | (2 if openems_sigma_m else 0)
+        self._check(self._lib.ems_model_build_bound(self._p, dt, flags), "build_bound!")
+        return self
+
+    def openems_timestep(self, method: int = 3) -> float:
+        """openEMS's time step (``TimeStepMethod`` 3 Rennings, 1 CFL) of
+        the grid and materials (src/engine/timestep.rs)."""
+        dt = self._lib.ems_model_openems_timestep(self._p, method)
+        if not dt > 0.0:
+            raise ValueError(f"unknown time-step method {method}")
+        return dt
+
+    def zero_edges(self, field: int, axis: int, lo: Sequence[int], hi: Sequence[int]) -> "Model":
+        """Zeroes the coefficients of the E (field 0) or H (1) edges along
+        ``axis`` at the nodes of the inclusive box lo..hi (after build)."""
+        self._check(self._lib.ems_model_zero_edges(self._p, field, axis, _u64(lo), _u64(hi)), "zero_edges!")
+        return self
+
     @property
     def dt(self) -> float:
         return self._lib.ems_model_dt(self._p)
@@ -551,14 +577,18 @@ class Model:
         self.ops.append((OP_MUR, "mur"))
         return k
 
-    def add_probe(self, quantity: int, entries: Sequence[tuple[int, Sequence[int], float]], interval: int = 1) -> int:
-        """``Probe::new(quantity).entry(axis, node, w)...interval(n)`` (src/engine/probe.rs)."""
+    def add_probe(self, quantity: int, entries: Sequence[tuple[int, Sequence[int], float]], interval: int = 1,
+                  f32_sum: bool = False) -> int:
+        """``Probe::new(quantity).entry(axis, node, w)...interval(n)`` (src/engine/probe.rs);
+        ``f32_sum``: entries summed in f32, as openEMS's current probes."""
         n = len(entries)
         axis = (C.c_int * n)(*[e[0] for e in entries])
         nodes = _u64([c for e in entries for c in e[1]])
         w = _f64([e[2] for e in entries])
         k = self._check(self._lib.ems_model_add_probe(self._p, quantity, n, axis, nodes, w, interval), "add_probe")
         self.ops.append((OP_PROBE, "probe"))
+        if f32_sum:
+            self._check(self._lib.ems_model_probe_f32(self._p, k, 1), "probe_f32!")
         return k
 
     @property

@@ -22,6 +22,9 @@ namespace {
 constexpr double C0 = 299792458.0;
 constexpr double MU0 = 1.25663706127e-6;
 const double EPS0 = 1.0 / (MU0 * C0 * C0);
+// openEMS's vacuum constants (src/constants.rs OPENEMS_EPS0, OPENEMS_MU0).
+constexpr double OE_EPS0 = 8.85418781762e-12;
+constexpr double OE_MU0 = 1.256637062e-6;
 const double Z0 = MU0 * C0;
 constexpr double PI = 3.14159265358979323846;
 constexpr double TAU = 6.28318530717958647692;
@@ -442,27 +445,72 @@ double ems_model_courant_limit(const ems_model* m) {
     return 1.0 / (C0 * std::sqrt(s));
 }
 
-int ems_model_build(ems_model* m, double courant, double fixed_dt) {
-    if (m->built) return set_err(m, "model already built"), EMS_ERR_INVALID;
-    // TimeStep::resolve (src/engine/coeffs.rs:220-240).
-    double max = ems_model_courant_limit(m);
-    double dt;
-    if (fixed_dt > 0.0) {
-        if (!(std::isfinite(fixed_dt) && fixed_dt <= max)) return set_err(m, "time step above the stability limit"), EMS_ERR_INVALID;
-        dt = fixed_dt;
-    } else {
-        if (!(std::isfinite(courant) && courant > 0.0 && courant <= 1.0)) return set_err(m, "Courant factor must be in (0, 1]"), EMS_ERR_INVALID;
-        dt = courant * max;
+// EdgeMaterials::from_cells (src/engine/edge_material.rs:376-413): eps_r
+// and kappa of the E edge along a at p, mu_r and sigma_m of the H dual edge
+// along a through p (vacuum where the edge does not exist).
+static void edge_eps(const ems_model* m, int a, const uint64_t p[3], double& eps, double& kap) {
+    eps = 1.0;
+    kap = 0.0;
+    if (p[a] + 1 >= m->n[a]) return;
+    const int b = next_axis(a), c = prev_axis(a);
+    double cap_c, g_c;
+    m->primary_edge_cg(a, p, cap_c, g_c);
+    const double k_ = m->delta(a, p[a]) / (m->dual_delta(b, p[b]) * m->dual_delta(c, p[c]));
+    eps = cap_c * k_ / EPS0;
+    kap = g_c * k_;
+}
+
+static void edge_mu(const ems_model* m, int a, const uint64_t p[3], double& mu, double& sig) {
+    mu = 1.0;
+    sig = 0.0;
+    const int b = next_axis(a), c = prev_axis(a);
+    if (p[b] + 1 >= m->n[b] || p[c] + 1 >= m->n[c]) return;
+    double l_c, r_c;
+    m->dual_edge_lr(a, p, l_c, r_c);
+    const double k_ = m->dual_delta(a, p[a]) / (m->delta(b, p[b]) * m->delta(c, p[c]));
+    mu = l_c * k_ / MU0;
+    sig = r_c * k_;
+}
+
+// openEMS's magnetic conductivity of the H dual edge along a through p
+// (openems_sigma_m and sigma_m_average, src/compile/openems.rs:580-650):
+// the length-weighted harmonic mean of the two half cells along a, 0 when
+// the upper half is lossless, a lossless lower half left out.
+static double oe_sigma_m(const ems_model* m, int a, const uint64_t p[3]) {
+    const int b = next_axis(a), c = prev_axis(a);
+    uint64_t q[3] = {p[0], p[1], p[2]};
+    double len = 0.0, inv = 0.0;
+    bool hi_zero = false;
+    for (int side = 0; side < 2; ++side) {
+        if (side == 0 && p[a] == 0) continue;
+        if (side == 1 && p[a] + 1 >= m->n[a]) continue;
+        q[a] = side == 0 ? p[a] - 1 : p[a];
+        q[b] = p[b];
+        q[c] = p[c];
+        const double h = 0.5 * m->delta(a, q[a]);
+        const double sg = m->mat(q[0], q[1], q[2]).sigma_m[a];
+        len += h;
+        if (sg != 0.0) inv += h / sg;
+        else if (side == 1) hi_zero = true;
     }
-    m->dt = dt;
+    if (hi_zero || inv == 0.0) return 0.0;
+    return len / inv;
+}
+
+// Coefficients::from_edges_rounded (src/engine/coeffs.rs:879-966) from the
+// per-edge materials of EdgeMaterials::from_cells; `openems`: the circuit
+// quantities C, G, L, R rounded to f32 and formed with openEMS's vacuum
+// constants (CoeffRounding::OpenEms, coeffs.rs:705-760); `oe_sigma`: the
+// magnetic conductivities by openEMS's average (oe_sigma_m). One x-plane
+// range per thread.
+static void compute_coefficients(ems_model* m, double dt, bool openems, bool oe_sigma = false) {
     const uint64_t N = m->n[0] * m->n[1] * m->n[2];
     for (int l = 0; l < 12; ++l) m->co[l].assign(N, 0.0f);
     bool pec_face[3][2];
     for (int t = 0; t < 3; ++t)
         for (int s = 0; s < 2; ++s) pec_face[t][s] = m->faces[2 * t + s] == 0;
-    // EdgeMaterials::from_cells + Coefficients::from_edges_rounded (Exact)
-    // (src/engine/edge_material.rs:376-425, src/engine/coeffs.rs:879-966),
-    // one x-plane range per thread.
+    const double eps0 = openems ? OE_EPS0 : EPS0, mu0 = openems ? OE_MU0 : MU0;
+    auto store = [openems](double x) { return openems ? (double)(float)x : x; };
     run_threads(m->n[0], [&](size_t i0, size_t i1) {
         for (uint64_t i = i0; i < i1; ++i)
             for (uint64_t j = 0; j < m->n[1]; ++j)
@@ -477,28 +525,23 @@ int ems_model_build(ems_model* m, double courant, double fixed_dt) {
                                 if ((p[t] == 0 && pec_face[t][0]) || (p[t] == m->n[t] - 1 && pec_face[t][1]))
                                     on_pec_face = true;
                             if (!(on_pec_face || m->pec[a][idx])) {
-                                double cap_c, g_c;
-                                m->primary_edge_cg(a, p, cap_c, g_c);
-                                double k_ = m->delta(a, p[a]) / (m->dual_delta(b, p[b]) * m->dual_delta(c, p[c]));
-                                double eps = cap_c * k_ / EPS0;
-                                double kap = g_c * k_;
+                                double eps, kap;
+                                edge_eps(m, a, p, eps, kap);
                                 double geo = m->dual_delta(b, p[b]) * m->dual_delta(c, p[c]) / m->delta(a, p[a]);
-                                double cap = EPS0 * eps * geo;
-                                double g = kap * geo;
+                                double cap = store(eps0 * eps * geo);
+                                double g = store(kap * geo);
                                 double den = cap + 0.5 * g * dt;
                                 m->co[a][idx] = (float)((cap - 0.5 * g * dt) / den);
                                 m->co[3 + a][idx] = (float)(dt / den);
                             }
                         }
                         if (p[b] + 1 < m->n[b] && p[c] + 1 < m->n[c]) {
-                            double l_c, r_c;
-                            m->dual_edge_lr(a, p, l_c, r_c);
-                            double k_ = m->dual_delta(a, p[a]) / (m->delta(b, p[b]) * m->delta(c, p[c]));
-                            double mu = l_c * k_ / MU0;
-                            double sig = r_c * k_;
+                            double mu, sig;
+                            edge_mu(m, a, p, mu, sig);
+                            if (oe_sigma) sig = oe_sigma_m(m, a, p);
                             double geo = m->delta(b, p[b]) * m->delta(c, p[c]) / m->dual_delta(a, p[a]);
-                            double l = MU0 * mu * geo;
-                            double r = sig * geo;
+                            double l = store(mu0 * mu * geo);
+                            double r = store(sig * geo);
                             double den = l + 0.5 * r * dt;
                             m->co[6 + a][idx] = (float)((l - 0.5 * r * dt) / den);
                             m->co[9 + a][idx] = (float)(dt / den);
@@ -506,8 +549,192 @@ int ems_model_build(ems_model* m, double courant, double fixed_dt) {
                     }
                 }
     });
+    m->dt = dt;
     m->built = true;
     m->refresh_desc();
+}
+
+int ems_model_build(ems_model* m, double courant, double fixed_dt) {
+    if (m->built) return set_err(m, "model already built"), EMS_ERR_INVALID;
+    // TimeStep::resolve (src/engine/coeffs.rs:220-240).
+    double max = ems_model_courant_limit(m);
+    double dt;
+    if (fixed_dt > 0.0) {
+        if (!(std::isfinite(fixed_dt) && fixed_dt <= max)) return set_err(m, "time step above the stability limit"), EMS_ERR_INVALID;
+        dt = fixed_dt;
+    } else {
+        if (!(std::isfinite(courant) && courant > 0.0 && courant <= 1.0)) return set_err(m, "Courant factor must be in (0, 1]"), EMS_ERR_INVALID;
+        dt = courant * max;
+    }
+    compute_coefficients(m, dt, false);
+    return EMS_OK;
+}
+
+int ems_model_build_bound(ems_model* m, double dt, int flags) {
+    if (m->built) return set_err(m, "model already built"), EMS_ERR_INVALID;
+    // TimeStep::Bound (src/engine/coeffs.rs:233-236): any positive step.
+    if (!(std::isfinite(dt) && dt > 0.0)) return set_err(m, "time step must be positive and finite"), EMS_ERR_INVALID;
+    if (flags & ~3) return set_err(m, "unknown build flags"), EMS_ERR_INVALID;
+    compute_coefficients(m, dt, (flags & 1) != 0, (flags & 2) != 0);
+    return EMS_OK;
+}
+
+namespace {
+
+// openEMS's time-step criteria (src/engine/timestep.rs:127-320): the
+// circuit values C (E edges) and L (H dual edges) in f32 with openEMS's
+// constants and full dual lengths at the boundary; a lookup clamps every
+// index into its table.
+struct OeCircuit {
+    uint64_t n[3];
+    uint64_t dc[3][3], dl[3][3];
+    std::vector<float> c[3], l[3];
+    float get(const std::vector<float>& v, const uint64_t* d, const int64_t q[3]) const {
+        uint64_t k[3];
+        for (int a = 0; a < 3; ++a) k[a] = (uint64_t)std::min<int64_t>(std::max<int64_t>(q[a], 0), (int64_t)d[a] - 1);
+        return v[(k[0] * d[1] + k[1]) * d[2] + k[2]];
+    }
+    float C(int a, const int64_t q[3]) const { return get(c[a], dc[a], q); }
+    float L(int a, const int64_t q[3]) const { return get(l[a], dl[a], q); }
+};
+
+OeCircuit oe_circuit(const ems_model* m) {
+    OeCircuit cir;
+    std::vector<double> pl[3], dl[3];
+    for (int a = 0; a < 3; ++a) {
+        cir.n[a] = m->n[a];
+        const uint64_t na = m->n[a];
+        if (na < 2) pl[a] = {1.0};
+        else for (uint64_t i = 0; i + 1 < na; ++i) pl[a].push_back(m->delta(a, i));
+        for (uint64_t i = 0; i < na; ++i) {
+            const bool lo = i >= 1 && i - 1 < pl[a].size(), hi = i < pl[a].size() && na >= 2 && i + 1 < na;
+            if (lo && hi) dl[a].push_back(0.5 * (pl[a][i - 1] + pl[a][i]));
+            else if (lo) dl[a].push_back(pl[a][i - 1]);
+            else if (i < pl[a].size()) dl[a].push_back(pl[a][i]);
+            else dl[a].push_back(1.0);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        const int b = (a + 1) % 3, c = (a + 2) % 3;
+        for (int edge = 1; edge >= 0; --edge) {
+            uint64_t* d = edge ? cir.dc[a] : cir.dl[a];
+            for (int q = 0; q < 3; ++q)
+                d[q] = ((q == a) == (edge != 0)) ? std::max<uint64_t>(m->n[q] - 1, 1) : m->n[q];
+            std::vector<float>& v = edge ? cir.c[a] : cir.l[a];
+            v.resize(d[0] * d[1] * d[2]);
+            for (uint64_t i = 0; i < d[0]; ++i)
+                for (uint64_t j = 0; j < d[1]; ++j)
+                    for (uint64_t k = 0; k < d[2]; ++k) {
+                        const uint64_t q[3] = {i, j, k};
+                        double x;
+                        if (edge) {
+                            double eps, kap;
+                            edge_eps(m, a, q, eps, kap);
+                            const double geo = dl[b][q[b]] * dl[c][q[c]] / pl[a][q[a]];
+                            x = OE_EPS0 * eps * geo;
+                        } else {
+                            double mu, sig;
+                            edge_mu(m, a, q, mu, sig);
+                            const double geo = pl[b][q[b]] * pl[c][q[c]] / dl[a][q[a]];
+                            x = OE_MU0 * mu * geo;
+                        }
+                        v[(i * d[1] + j) * d[2] + k] = (float)x;
+                    }
+        }
+    }
+    return cir;
+}
+
+inline float oe_x(float c, float l) { return 1.0f / (c * l); }
+
+}  // namespace
+
+double ems_model_openems_timestep(const ems_model* m, int method) {
+    if (method != 1 && method != 3) return 0.0;
+    const OeCircuit cir = oe_circuit(m);
+    const uint64_t* n = m->n;
+    double w2max = 0.0;
+    auto sh = [](const int64_t q[3], int a, int64_t k, int64_t out[3]) {
+        out[0] = q[0];
+        out[1] = q[1];
+        out[2] = q[2];
+        out[a] += k;
+    };
+    for (int a = 0; a < 3; ++a) {
+        for (uint64_t i = 0; i < n[0]; ++i)
+            for (uint64_t j = 0; j < n[1]; ++j)
+                for (uint64_t k = 0; k < n[2]; ++k) {
+                    const int64_t q[3] = {(int64_t)i, (int64_t)j, (int64_t)k};
+                    int64_t t0[3], t1[3];
+                    if (method == 1) {
+                        // gershgorin (timestep.rs:225-246).
+                        if ((uint64_t)q[a] + 1 >= n[a]) continue;
+                        const int b = (a + 1) % 3, c = (a + 2) % 3;
+                        float s = 0.0f;
+                        for (int t : {c, b}) {
+                            const int o = 3 - a - t;
+                            s += 1.0f / cir.L(o, q);
+                            sh(q, t, -1, t0);
+                            s += 1.0f / cir.L(o, t0);
+                        }
+                        w2max = std::max(w2max, (double)s / (double)cir.C(a, q));
+                        continue;
+                    }
+                    // rennings (timestep.rs:248-287).
+                    const int bs[2] = {(a + 1) % 3, (a + 2) % 3};
+                    double tt[2];
+                    float lm[2], l0[2];
+                    for (int slot = 0; slot < 2; ++slot) {
+                        const int b = bs[slot], c = 3 - a - b;
+                        sh(q, b, -1, t0);
+                        lm[slot] = cir.L(c, t0);
+                        l0[slot] = cir.L(c, q);
+                        float below;
+                        if ((b + 3 - a) % 3 == 2) {
+                            int64_t f[3];
+                            sh(t0, c, -1, f);
+                            const float lb = cir.L(c, f);
+                            sh(q, c, -1, t1);
+                            below = oe_x(cir.C(a, f), lb) + oe_x(cir.C(a, t1), lb);
+                        } else {
+                            below = oe_x(cir.C(a, t0), lm[slot]) + oe_x(cir.C(a, q), lm[slot]);
+                        }
+                        sh(q, b, 1, t1);
+                        const float above = oe_x(cir.C(a, q), l0[slot]) + oe_x(cir.C(a, t1), l0[slot]);
+                        tt[slot] = 0.25 * ((double)below + (double)above);
+                    }
+                    double own = 0.0;
+                    for (int e = 0; e < 2; ++e) {
+                        int64_t mm[3];
+                        sh(q, a, e, mm);
+                        const float c0 = cir.C(bs[0], mm), c1 = cir.C(bs[1], mm);
+                        const double x0m = oe_x(c0, lm[0]), x00 = oe_x(c0, l0[0]);
+                        const double x1m = oe_x(c1, lm[1]), x10 = oe_x(c1, l0[1]);
+                        const double lc0 = 0.5 * (x0m + x00), dc0 = 0.5 * (x0m - x00);
+                        const double lc1 = 0.5 * (x1m + x10), dc1 = 0.5 * (x1m - x10);
+                        own += std::max(lc1 + std::fabs(dc0), lc0 + std::fabs(dc1));
+                    }
+                    w2max = std::max(w2max, tt[0] + tt[1] + 0.5 * own);
+                }
+    }
+    if (method == 1) return (double)(1.0f / std::sqrt((float)w2max));
+    return 1.0 / std::sqrt(w2max);
+}
+
+int ems_model_zero_edges(ems_model* m, int field, int axis, const uint64_t lo[3], const uint64_t hi[3]) {
+    if (!m->built) return set_err(m, "build the model first"), EMS_ERR_INVALID;
+    if ((field != 0 && field != 1) || axis < 0 || axis > 2) return set_err(m, "invalid field or axis"), EMS_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] > hi[a] || hi[a] >= m->n[a]) return set_err(m, "box outside the grid"), EMS_ERR_INVALID;
+    std::vector<float>& c0 = m->co[(field ? 6 : 0) + axis];
+    std::vector<float>& c1 = m->co[(field ? 9 : 3) + axis];
+    for (uint64_t i = lo[0]; i <= hi[0]; ++i)
+        for (uint64_t j = lo[1]; j <= hi[1]; ++j)
+            for (uint64_t k = lo[2]; k <= hi[2]; ++k) {
+                const uint64_t idx = m->index(i, j, k);
+                c0[idx] = 0.0f;
+                c1[idx] = 0.0f;
+            }
     return EMS_OK;
 }
 
@@ -1162,6 +1389,13 @@ int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6],
     m->ops.push_back(std::move(op));
     m->refresh_desc();
     return (int)m->ops.size() - 1;
+}
+
+int ems_model_probe_f32(ems_model* m, int op, int on) {
+    if (op < 0 || (size_t)op >= m->ops.size() || m->ops[(size_t)op]->kind != EMS_OP_PROBE)
+        return set_err(m, "not a probe"), EMS_ERR_INVALID;
+    m->ops[(size_t)op]->probe.f32_sum = on ? 1 : 0;
+    return EMS_OK;
 }
 
 const ems_engine_desc* ems_model_desc(ems_model* m) {

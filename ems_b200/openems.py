@@ -1,0 +1,939 @@
+"""openEMS XML models on the engine (a subset of the reference's file path).
+
+Reads an openEMS ``model.xml`` and sets it up the way the reference does
+for files (``Simulation::from_xml`` with ``Fdtd::openems_run``; src/sim/
+mod.rs:55-190, src/sim/map.rs, src/compile/mod.rs, src/fdtd.rs), runs it on
+the CUDA engine (or any engine with the same interface) and writes
+openEMS's probe files and excitation signal files (``et``/``ht``).
+
+Restated from the reference:
+
+* the time step: openEMS's criterion (``TimeStepMethod`` 3 Rennings or 1
+  Gershgorin, src/engine/timestep.rs), times ``TimeStepFactor``, or
+  ``TimeStep``; a sinusoid's period split into whole steps
+  (periodic_timestep, timestep.rs:292-296); the run length
+  ``NumberOfTimesteps`` cut by ``MaxTime``;
+* the coefficients with openEMS's rounding (``CoeffRounding::OpenEms``);
+* the signals (src/waveform.rs:442-518, src/io/openems/signal.rs):
+  openEMS's Gaussian (τ = 3/(2π·fc), delay 3τ, sample 0 zero), sinusoid
+  (period repeated), Dirac, step and custom expressions; openEMS's timing
+  (src/sim/map.rs:270-307: the field value at time T gets the sample at
+  T − dt − ⌊Delay/dt⌋·dt);
+* PEC, PMC (openEMS's half-cell PMC, src/compile/mod.rs:1556-1626) and
+  first-order Mur faces (openEMS's options, the hold of faces that carry an
+  E excitation, src/compile/mod.rs:1439-1476);
+* isotropic or anisotropic materials and metal on box primitives;
+* E and H excitations (soft, hard) with ``Excite`` and ``Delay``;
+* probes (src/sim/map.rs:1150-1380, 1683-1870): voltage along the
+  staircase path, current around a loop in the nearest dual plane
+  (openEMS's snapping, entry order and f32 sum), native E and H field
+  components; openEMS's skip rules; time-domain files every
+  ⌊N/OverSampling⌋ steps (N the Nyquist interval), ``FD_Samples`` files,
+  H-type files with the sample after the last step.
+
+Not restated: csx's general discretisation (primitives other than boxes,
+weighting functions, transformations), PML, dispersive materials, lumped
+elements, dumps, cylindrical grids, the openEMS energy measure for
+``endCriteria`` (runs go to their step limit; refused where a criterion
+above 1e-30 could stop them), probe time windows.
+"""
+from __future__ import annotations
+
+import math
+import os
+import re
+import xml.etree.ElementTree as ET
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import probe_files as PF
+
+C0 = 299792458.0
+TWO_PI = 2.0 * math.pi
+FACE_NAMES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+PEC_FACE, PMC_FACE, MUR_FACE = 0, 1, 2
+
+
+# ---------------------------------------------------------------------------
+# Custom signal expressions (openEMS's function parser syntax, a subset).
+
+_FUNCS = {"exp": math.exp, "cos": math.cos, "sin": math.sin, "tan": math.tan, "sqrt": math.sqrt,
+          "abs": abs, "log": math.log, "log10": math.log10, "atan": math.atan, "cosh": math.cosh,
+          "sinh": math.sinh, "tanh": math.tanh}
+_TOKEN = re.compile(r"\s*(?:(\d+\.?\d*(?:[eE][-+]?\d+)?|\.\d+(?:[eE][-+]?\d+)?)|([A-Za-z_]\w*)|(.))")
+
+
+class Expression:
+    """A signal ``f(t)`` in openEMS's expression syntax: numbers, ``t``,
+    ``pi``, + − * / ^, parentheses, unary minus and the functions of
+    ``_FUNCS`` (parsed once into a tree; no evaluation of arbitrary code)."""
+
+    def __init__(self, text: str):
+        self.text = text
+        self._tok = [(m.group(1), m.group(2), m.group(3)) for m in _TOKEN.finditer(text) if any(m.groups())]
+        self._i = 0
+        self._tree = self._sum()
+        if self._i != len(self._tok):
+            raise ValueError(f"expression {text!r}: unexpected {self._tok[self._i]}")
+
+    def _peek(self):
+        return self._tok[self._i] if self._i < len(self._tok) else (None, None, None)
+
+    def _take(self, op):
+        if self._peek()[2] == op:
+            self._i += 1
+            return True
+        return False
+
+    def _sum(self):
+        node = self._product()
+        while True:
+            if self._take("+"):
+                node = ("+", node, self._product())
+            elif self._take("-"):
+                node = ("-", node, self._product())
+            else:
+                return node
+
+    def _product(self):
+        node = self._unary()
+        while True:
+            if self._take("*"):
+                node = ("*", node, self._unary())
+            elif self._take("/"):
+                node = ("/", node, self._unary())
+            else:
+                return node
+
+    def _unary(self):
+        if self._take("-"):
+            return ("neg", self._unary())
+        if self._take("+"):
+            return self._unary()
+        return self._power()
+
+    def _power(self):
+        base = self._atom()
+        if self._take("^"):
+            return ("^", base, self._unary())
+        return base
+
+    def _atom(self):
+        num, name, op = self._peek()
+        if num is not None:
+            self._i += 1
+            return ("num", float(num))
+        if name is not None:
+            self._i += 1
+            if name in _FUNCS:
+                if not self._take("("):
+                    raise ValueError(f"expression {self.text!r}: {name} needs (")
+                arg = self._sum()
+                if not self._take(")"):
+                    raise ValueError(f"expression {self.text!r}: missing )")
+                return ("fn", name, arg)
+            if name == "t":
+                return ("t",)
+            if name == "pi":
+                return ("num", math.pi)
+            raise ValueError(f"expression {self.text!r}: unknown name {name}")
+        if self._take("("):
+            node = self._sum()
+            if not self._take(")"):
+                raise ValueError(f"expression {self.text!r}: missing )")
+            return node
+        raise ValueError(f"expression {self.text!r}: unexpected {op!r}")
+
+    def __call__(self, t: float) -> float:
+        def ev(n):
+            k = n[0]
+            if k == "num":
+                return n[1]
+            if k == "t":
+                return t
+            if k == "neg":
+                return -ev(n[1])
+            if k == "fn":
+                return _FUNCS[n[1]](ev(n[2]))
+            a, b = ev(n[1]), ev(n[2])
+            return {"+": a + b, "-": a - b, "*": a * b, "/": a / b if b != 0 else math.inf}.get(k) \
+                if k != "^" else a ** b
+        return float(ev(self._tree))
+
+
+# ---------------------------------------------------------------------------
+# Signals (src/waveform.rs:442-518).
+
+@dataclass
+class Signal:
+    """openEMS excitation signal: kind 0 Gaussian (f0, fc), 1 sinusoid
+    (f0), 2 Dirac, 3 step, 10 custom expression (f0 for the Nyquist rate)."""
+
+    kind: int
+    f0: float = 0.0
+    fc: float = 0.0
+    expr: Expression | None = None
+
+    @property
+    def tau(self) -> float:
+        return 3.0 / (TWO_PI * self.fc)
+
+    @property
+    def delay(self) -> float:
+        return 3.0 * self.tau if self.kind == 0 else 0.0
+
+    def value(self, t: float, dt: float) -> float:
+        """Waveform::value with openEMS's sampling convention: sample
+        k = ⌊t/dt + ¼⌋ on the E or H grid."""
+        k = math.floor(t / dt + 0.25 + 1e-9)
+        if self.kind == 0:
+            T = self.delay
+            if not (k >= 1 and k <= math.floor(2.0 * T / dt + 1e-9)):
+                return 0.0
+            x = (t - T) / self.tau
+            return math.cos(TWO_PI * self.f0 * (t - T)) * math.exp(-x * x)
+        if self.kind == 1:
+            return math.sin(TWO_PI * self.f0 * t) if (k >= 1 and not self._sine_wrap(dt, k)) else 0.0
+        if self.kind == 2:
+            return 1.0 if k == 1 else 0.0
+        if self.kind == 3:
+            return 1.0 if k >= 0 else 0.0
+        return self.expr(t)
+
+    def _sine_wrap(self, dt, k):
+        p = 1.0 / (self.f0 * dt)
+        n = round(p)
+        return n >= 1 and abs(p - n) <= 1e-6 * n and (k % n) == 0
+
+    def nyquist_frequency(self):
+        if self.kind == 0:
+            return self.f0 + self.fc
+        if self.kind in (1, 10) and self.f0 > 0:
+            return self.f0
+        return None
+
+    def nyquist_interval(self, dt: float) -> int:
+        f = self.nyquist_frequency()
+        if not f or not math.isfinite(f) or f <= 0:
+            return 1
+        k = math.floor(1.0 / (2.0 * f * dt))
+        return int(k) if k >= 1 else 1
+
+    def length(self, dt: float, max_steps: int) -> int:
+        """Rows of the ``et``/``ht`` files (src/io/openems/signal.rs:77-104)."""
+        if self.kind == 0:
+            return min(int(math.floor(2.0 * self.delay / dt)) + 1, max_steps)
+        if self.kind == 1:
+            return 2 * max(1, round(1.0 / (self.f0 * dt)))
+        if self.kind in (2, 3):
+            return 2
+        return max_steps
+
+    def signal_text(self, dt: float, max_steps: int, offset: float) -> str:
+        rows = []
+        for k in range(self.length(dt, max_steps)):
+            t = (k + offset) * dt
+            rows.append(f"{PF.fmt_g(t, 6)}\t{PF.fmt_g(self.value(t, dt), 6)}")
+        return "\n".join(rows) + "\n"
+
+
+# ---------------------------------------------------------------------------
+# The file.
+
+@dataclass
+class Box:
+    p1: tuple
+    p2: tuple
+    priority: int = 0
+
+
+@dataclass
+class Prop:
+    kind: str            # Material, Metal, Excitation, ProbeBox
+    name: str
+    attrs: dict
+    prop: dict = field(default_factory=dict)
+    boxes: list = field(default_factory=list)
+    fd: list = field(default_factory=list)
+    order: int = 0
+
+
+@dataclass
+class OpenEmsFile:
+    lines: list          # drawing units, per axis
+    unit: float
+    max_steps: int
+    end_criteria: float
+    max_time: float | None
+    timestep: float | None
+    timestep_factor: float
+    timestep_method: int
+    oversampling: int
+    signal: Signal
+    faces: list          # per face (kind, parameter)
+    mur_velocity: float | None
+    props: list
+    background: dict | None = None
+
+
+def _f(x, default=None):
+    return default if x is None else float(x)
+
+
+def _vec3(text, default, isotropic=True):
+    """A material value: isotropic materials take the first number for all
+    three axes; anisotropic ones (Isotropy="0") take the numbers given for
+    x, y, z in turn, the missing ones the default."""
+    if text is None:
+        return [default] * 3
+    v = [float(x) for x in text.split(",")]
+    if isotropic:
+        return [v[0]] * 3
+    return (v + [default] * 3)[:3]
+
+
+def parse(text: str) -> OpenEmsFile:
+    root = ET.fromstring(text)
+    fd = root.find("FDTD")
+    if fd is None:
+        raise ValueError("no <FDTD> element")
+    ex = fd.find("Excitation")
+    if ex is None:
+        raise ValueError("no excitation signal")
+    kind = int(float(ex.get("Type", "0")))
+    if kind == 0:
+        sig = Signal(0, float(ex.get("f0")), float(ex.get("fc")))
+    elif kind == 1:
+        sig = Signal(1, float(ex.get("f0")))
+    elif kind in (2, 3):
+        sig = Signal(kind)
+    elif kind == 10:
+        sig = Signal(10, _f(ex.get("f0"), 0.0), expr=Expression(ex.get("Function")))
+    else:
+        raise NotImplementedError(f"excitation signal type {kind}")
+    bc = fd.find("BoundaryCond")
+    faces = []
+    for name in FACE_NAMES:
+        v = (bc.get(name) if bc is not None else None) or "PEC"
+        u = v.upper()
+        if u in ("PEC", "0"):
+            faces.append((PEC_FACE, None))
+        elif u in ("PMC", "1"):
+            faces.append((PMC_FACE, None))
+        elif u in ("MUR", "2"):
+            faces.append((MUR_FACE, None))
+        else:
+            raise NotImplementedError(f"boundary {v!r} on {name}")
+    mur_v = _f(bc.get("MUR_PhaseVelocity")) if bc is not None else None
+    cs = root.find("ContinuousStructure")
+    grid = cs.find("RectilinearGrid")
+    if int(float(grid.get("CoordSystem", cs.get("CoordSystem", "0")))) != 0:
+        raise NotImplementedError("cylindrical grids")
+    unit = float(grid.get("DeltaUnit", "1"))
+    lines = []
+    for tag in ("XLines", "YLines", "ZLines"):
+        v = sorted(float(x) for x in grid.find(tag).text.split(","))
+        lines.append(v)
+    props = []
+    pr = cs.find("Properties")
+    for q, el in enumerate(list(pr) if pr is not None else []):
+        boxes = []
+        prims = el.find("Primitives")
+        for b in (list(prims) if prims is not None else []):
+            if b.tag != "Box":
+                raise NotImplementedError(f"primitive {b.tag} in {el.get('Name')!r}")
+            if b.find("Transformation") is not None:
+                raise NotImplementedError("transformed primitives")
+            p1, p2 = b.find("P1"), b.find("P2")
+            boxes.append(Box(tuple(float(p1.get(c)) for c in "XYZ"), tuple(float(p2.get(c)) for c in "XYZ"),
+                             int(float(b.get("Priority", "0")))))
+        if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox"):
+            raise NotImplementedError(f"property {el.tag}")
+        if el.tag == "ProbeBox" and len(boxes) > 1:
+            raise NotImplementedError(f"probe {el.get('Name')!r} with several primitives")
+        if el.find("Weight") is not None:
+            raise NotImplementedError(f"weighting functions ({el.get('Name')!r})")
+        sub = el.find("Property")
+        fds = el.find("FD_Samples")
+        props.append(Prop(el.tag, el.get("Name", ""), dict(el.attrib), dict(sub.attrib) if sub is not None else {},
+                          boxes, [float(x) for x in fds.text.split(",")] if fds is not None and fds.text else [], q))
+    # src/fdtd/convert.rs:32-47: OverSampling below 2 → 4; endCriteria
+    # absent or 0 → openEMS's default, negative → none; TimeStepFactor
+    # outside (0, 1] → 1 and TimeStepMethod other than 1 or 3 → 1 (what
+    # openEMS does).
+    os_ = int(float(fd.get("OverSampling", "4")))
+    end = float(fd.get("endCriteria", "0"))
+    end = 1e-5 if end == 0.0 else (None if end < 0 else end)
+    factor = float(fd.get("TimeStepFactor", "1"))
+    method = int(float(fd.get("TimeStepMethod", "3")))
+    bg = cs.find("BackgroundMaterial")
+    for el in cs:
+        if el.tag not in ("Properties", "RectilinearGrid", "BackgroundMaterial"):
+            raise NotImplementedError(f"<{el.tag}> in the structure")
+    return OpenEmsFile(lines, unit, int(float(fd.get("NumberOfTimesteps", "0"))), end,
+                       _f(fd.get("MaxTime")), _f(fd.get("TimeStep")),
+                       factor if 0.0 < factor <= 1.0 else 1.0, method if method in (1, 3) else 1,
+                       os_ if os_ >= 2 else 4, sig, faces, mur_v, props,
+                       dict(bg.attrib) if bg is not None else None)
+
+
+# ---------------------------------------------------------------------------
+# Snapping (src/sim/map.rs:1816-1870).
+
+def snap_lower(lines, x):
+    best = 0
+    for i in range(1, len(lines)):
+        tol = 1e-9 * abs(lines[i] - lines[i - 1])
+        if abs(lines[i] - x) < abs(lines[best] - x) - tol:
+            best = i
+    return best
+
+
+def snap_upper(lines, x):
+    best = 0
+    for i in range(1, len(lines)):
+        tol = 1e-9 * abs(lines[i] - lines[i - 1])
+        if abs(lines[i] - x) <= abs(lines[best] - x) + tol:
+            best = i
+    return best
+
+
+def snap_cell(lines, x):
+    if len(lines) < 2:
+        return 0
+    i = 0
+    for k in range(1, len(lines) - 1):
+        tol = 1e-9 * abs(lines[k + 1] - lines[k - 1])
+        if lines[k] < x - tol:
+            i = k
+    return i
+
+
+def voltage_path(start, stop):
+    """src/sim/map.rs:1683-1702: x, then y, then z; reversed edges −1."""
+    out, p = [], list(start)
+    for a in range(3):
+        lo, hi = p[a], stop[a]
+        if lo <= hi:
+            for i in range(lo, hi):
+                p[a] = i
+                out.append((a, tuple(p), 1.0))
+        else:
+            for i in range(lo - 1, hi - 1, -1):
+                p[a] = i
+                out.append((a, tuple(p), -1.0))
+        p[a] = hi
+    return out
+
+
+def loop_entries(n, lo, hi, layer):
+    """−∮H around the E edges along n with transverse nodes in lo..hi
+    (src/engine/port.rs:231-260)."""
+    b, c = (n + 1) % 3, (n + 2) % 3
+
+    def node(pb, pc):
+        p = [0, 0, 0]
+        p[n], p[b], p[c] = layer, pb, pc
+        return tuple(p)
+
+    v = []
+    for pc in range(lo[c], hi[c] + 1):
+        v.append((c, node(hi[b], pc), -1.0))
+        if lo[b] > 0:
+            v.append((c, node(lo[b] - 1, pc), 1.0))
+    for pb in range(lo[b], hi[b] + 1):
+        v.append((b, node(pb, hi[c]), 1.0))
+        if lo[c] > 0:
+            v.append((b, node(pb, lo[c] - 1), -1.0))
+    return v
+
+
+def openems_loop_order(entries, n, lo, hi):
+    """src/sim/map.rs:1776-1805."""
+    b, c = (n + 1) % 3, (n + 2) % 3
+
+    def key(e):
+        a, p, _ = e
+        if a == b and p[c] < lo[c]:
+            return (0, p[b])
+        if a == c and p[b] >= hi[b]:
+            return (1, p[c])
+        if a == b:
+            return (2, p[b])
+        return (3, p[c])
+
+    return sorted(entries, key=key)
+
+
+# ---------------------------------------------------------------------------
+# Set-up.
+
+@dataclass
+class ProbeSpec:
+    name: str
+    kind: str            # voltage, current, efield, hfield
+    ops: list            # engine op indices (one, or three for field probes)
+    location: tuple
+    fd: list
+    oversampling: int | None = None
+    start_time: float = 0.0
+    stop_time: float = 0.0
+
+
+class Setup:
+    """A parsed file mapped onto a built ``ems_b200.Model``: ``model``,
+    ``dt``, ``steps`` (the run length), ``probes`` and ``warnings``."""
+
+    def __init__(self, f: OpenEmsFile):
+        from . import PEC, PMC, Model
+        self.file = f
+        self.warnings: list[str] = []
+        u = f.unit
+        lines_m = [np.array(v) * u for v in f.lines]
+        n = [len(v) for v in f.lines]
+        self.nodes = n
+        m = Model(*lines_m)
+        self.lines_m = lines_m
+        m.faces([PMC if k == PMC_FACE else PEC for k, _ in f.faces])
+        self._materials(m)
+        # Time step: openEMS's criterion, TimeStepFactor, or TimeStep.
+        if f.timestep is not None:
+            base = f.timestep
+        else:
+            base = m.openems_timestep(f.timestep_method)
+        dt = f.timestep_factor * base
+        if f.signal.kind == 1 and f.signal.f0 > 0:
+            period = 1.0 / f.signal.f0
+            dt = period / (math.floor(period / dt) + 1.0)
+        m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
+        self.dt = dt
+        self._pmc_half_cell(m)
+        steps = f.max_steps
+        if f.max_time is not None and f.max_time > 0:
+            steps = min(steps, int(math.floor(f.max_time / dt)))
+        self.steps = steps
+        if f.end_criteria is not None and f.end_criteria > 1e-30 and \
+                (any(k == MUR_FACE for k, _ in f.faces) or self._lossy()):
+            raise NotImplementedError("energy end criteria (openEMS's measure) in a model that loses energy")
+        self.model = m
+        self.excited = self._excitation_edges()
+        self._mur(m)
+        self._excitations(m)
+        self.probes: list[ProbeSpec] = []
+        self._probes(m)
+
+    # -- geometry helpers (drawing units)
+    def _inside(self, a, x, lo, hi):
+        tol = 1e-9 * max(1.0, abs(hi - lo), abs(self.file.lines[a][-1] - self.file.lines[a][0]))
+        return lo - tol <= x <= hi + tol
+
+    def _materials(self, m):
+        f = self.file
+        mats = [p for p in f.props if p.kind in ("Material", "Metal")]
+        # Paint in priority order; at equal priority the property defined
+        # first wins (it is painted last).
+        items = []
+        for p in mats:
+            for b in p.boxes:
+                items.append((b.priority, -p.order, p, b))
+        items.sort(key=lambda t: (t[0], t[1]))
+        lines = f.lines
+        if f.background:
+            n = self.nodes
+            m.fill(m.cells().box([0, 0, 0], [n[0] - 1, n[1] - 1, n[2] - 1]), self._material(m, f.background))
+        cen = [0.5 * (np.array(v[1:]) + np.array(v[:-1])) for v in lines]
+        for _, _, p, b in items:
+            lo = [min(b.p1[a], b.p2[a]) for a in range(3)]
+            hi = [max(b.p1[a], b.p2[a]) for a in range(3)]
+            if p.kind == "Metal":
+                # Edges whose midpoint lies in the closed box, unless a
+                # material of higher priority (or of equal priority defined
+                # earlier) holds the midpoint too.
+                over = [(ob, op) for (_, _, op, ob) in items if op.kind == "Material" and
+                        (ob.priority > b.priority or (ob.priority == b.priority and op.order < p.order))]
+                for a in range(3):
+                    rng = []
+                    for q in range(3):
+                        pts = cen[q] if q == a else np.array(lines[q])
+                        rng.append([i for i, x in enumerate(pts) if self._inside(q, x, lo[q], hi[q])])
+                    if not all(rng):
+                        continue
+                    for i in rng[0]:
+                        for j in rng[1]:
+                            run = []
+                            for k in rng[2] + [None]:
+                                keep = k is not None
+                                if keep and over:
+                                    mid = [cen[q][x] if q == a else lines[q][x] for q, x in enumerate((i, j, k))]
+                                    keep = not any(all(self._inside(q, mid[q], min(ob.p1[q], ob.p2[q]),
+                                                                    max(ob.p1[q], ob.p2[q])) for q in range(3))
+                                                   for ob, _ in over)
+                                if keep and run and k == run[-1] + 1:
+                                    run.append(k)
+                                    continue
+                                if run:
+                                    m.pec_edges(a, [i, j, run[0]], [i, j, run[-1]])
+                                run = [k] if keep else []
+                continue
+            cells = [[i for i, x in enumerate(cen[a]) if self._inside(a, x, lo[a], hi[a])] for a in range(3)]
+            if not all(cells):
+                continue
+            mat = self._material(m, p.prop, p.attrs.get("Isotropy", "1") != "0")
+            cs = m.cells().box([c[0] for c in cells], [c[-1] + 1 for c in cells])
+            m.fill(cs, mat)
+
+    @staticmethod
+    def _material(m, prop, isotropic=True):
+        eps = _vec3(prop.get("Epsilon"), 1.0, isotropic)
+        mu = _vec3(prop.get("Mue"), 1.0, isotropic)
+        kap = _vec3(prop.get("Kappa"), 0.0, isotropic)
+        sig = _vec3(prop.get("Sigma"), 0.0, isotropic)
+        return m.material(eps_r=tuple(eps), mu_r=tuple(mu), kappa=tuple(kap), sigma_m=tuple(sig))
+
+    def _lossy(self):
+        f = self.file
+        props = [p.prop for p in f.props if p.kind == "Material"] + ([f.background] if f.background else [])
+        return any(any(float(x) != 0.0 for x in (pr.get(k) or "0").split(","))
+                   for pr in props for k in ("Kappa", "Sigma"))
+
+    def _pmc_half_cell(self, m):
+        """openEMS's PMC (src/compile/mod.rs:1556-1626): the tangential H of
+        the dual layer next to the face, the tangential E and the normal H
+        on the face are never updated."""
+        n = self.nodes
+        for face, (k, _) in enumerate(self.file.faces):
+            if k != PMC_FACE:
+                continue
+            t, is_max = face // 2, face % 2 == 1
+            h_layer, e_layer = (n[t] - 2, n[t] - 1) if is_max else (0, 0)
+            for a in range(3):
+                todo = [(1, e_layer)] if a == t else [(1, h_layer), (0, e_layer)]
+                for field_, layer in todo:
+                    lo, hi = [0, 0, 0], [n[0] - 1, n[1] - 1, n[2] - 1]
+                    lo[t] = hi[t] = layer
+                    m.zero_edges(field_, a, lo, hi)
+
+    def _excitation_edges(self):
+        """(E?, axis, node, weight per unit amplitude, property) of every
+        driven edge: E edges whose both nodes lie in the closed box, H dual
+        edges whose midpoint does; weight = Excite × (dual) edge length."""
+        out = []
+        f = self.file
+        n = self.nodes
+        lines = f.lines
+        for p in f.props:
+            if p.kind != "Excitation" or p.attrs.get("Enabled", "1") == "0":
+                continue
+            typ = int(float(p.attrs.get("Type", "0")))
+            if typ not in (0, 1, 2, 3):
+                raise NotImplementedError(f"excitation type {typ}")
+            e_type = typ in (0, 1)
+            exc = _vec3(p.attrs.get("Excite"), 0.0, isotropic=False)
+            for b in p.boxes:
+                lo = [min(b.p1[a], b.p2[a]) for a in range(3)]
+                hi = [max(b.p1[a], b.p2[a]) for a in range(3)]
+                for a in range(3):
+                    if exc[a] == 0.0:
+                        continue
+                    rng = []
+                    for q in range(3):
+                        if e_type:
+                            pts = [i for i in range(n[q] - (1 if q == a else 0))
+                                   if self._inside(q, lines[q][i], lo[q], hi[q])
+                                   and (q != a or self._inside(q, lines[q][i + 1], lo[q], hi[q]))]
+                        else:
+                            if q == a:
+                                pts = [i for i in range(n[q]) if self._inside(q, lines[q][i], lo[q], hi[q])]
+                            else:
+                                pts = [i for i in range(n[q] - 1)
+                                       if self._inside(q, 0.5 * (lines[q][i] + lines[q][i + 1]), lo[q], hi[q])]
+                        rng.append(pts)
+                    for i in rng[0]:
+                        for j in rng[1]:
+                            for k in rng[2]:
+                                node = (i, j, k)
+                                if e_type:
+                                    length = self.model_delta(a, node[a])
+                                else:
+                                    length = self.model_dual(a, node[a])
+                                out.append((e_type, typ, a, node, exc[a] * length, p))
+        return out
+
+    def model_delta(self, a, i):
+        return float(self.lines_m[a][i + 1] - self.lines_m[a][i])
+
+    def model_dual(self, a, i):
+        v = self.lines_m[a]
+        lo = v[i] - v[i - 1] if i > 0 else 0.0
+        hi = v[i + 1] - v[i] if i + 1 < len(v) else 0.0
+        return float(0.5 * (lo + hi))
+
+    def _mur(self, m):
+        f = self.file
+        faces = {fc: f.mur_velocity for fc, (k, _) in enumerate(f.faces) if k == MUR_FACE}
+        if not faces:
+            return
+        from . import MUR_COUNT_ENERGY, MUR_OPENEMS_CORNERS, MUR_OPENEMS_ORDER
+        hold = None
+        if f.signal.kind == 0:
+            n = self.nodes
+            held = set()
+            for e_type, _, a, node, _, _ in self.excited:
+                if not e_type:
+                    continue
+                for fc in faces:
+                    fa = fc // 2
+                    plane = n[fa] - 1 if fc % 2 else 0
+                    if fa != a and node[fa] == plane:
+                        held.add(fc)
+            if held:
+                steps = int(math.floor(2.0 * f.signal.delay / self.dt)) + 1
+                hold = {fc: steps + 10 for fc in held}
+        m.add_mur(faces, hold=hold, flags=MUR_COUNT_ENERGY | MUR_OPENEMS_CORNERS | MUR_OPENEMS_ORDER)
+
+    def _excitations(self, m):
+        from . import HARD_E, HARD_H, SOFT_E, SOFT_H
+        f, dt, steps = self.file, self.dt, self.steps + 1
+        kinds = {0: SOFT_E, 1: HARD_E, 2: SOFT_H, 3: HARD_H}
+        by_prop = {}
+        for e_type, typ, a, node, w, p in self.excited:
+            by_prop.setdefault(p.order, (typ, p, []))[2].append((a, node, w))
+        for order in sorted(by_prop):
+            typ, p, edges = by_prop[order]
+            kind = kinds[typ]
+            hard = typ in (1, 3)
+            lag = dt if hard else 0.5 * dt
+            delay = _f(p.attrs.get("Delay"), 0.0)
+            shift = lag + (math.floor(delay / dt) if delay > 0 else 0) * dt
+            # The kind's sample time of step n (SourceKind).
+            t_of = {SOFT_E: lambda s: (s + 0.5) * dt, HARD_E: lambda s: (s + 1.0) * dt,
+                    SOFT_H: lambda s: s * dt, HARD_H: lambda s: (s + 0.5) * dt}[kind]
+            amp = np.zeros(steps)
+            for s in range(steps):
+                tau = t_of(s) - shift
+                amp[s] = 0.0 if tau < -0.25 * dt else f.signal.value(tau, dt)
+            m.add_source_table(kind, edges, amp)
+
+    def _probes(self, m):
+        from . import CURRENT, VOLTAGE
+        f = self.file
+        n = self.nodes
+        lines = f.lines
+        at = lambda idx: tuple(float(self.lines_m[a][idx[a]]) for a in range(3))  # noqa: E731
+        for p in f.props:
+            if p.kind != "ProbeBox" or not p.boxes:
+                continue
+            typ = int(float(p.attrs.get("Type", "0")))
+            weight = float(p.attrs.get("Weight", "1"))
+            c0, c1 = p.boxes[0].p1, p.boxes[0].p2
+            window = (_f(p.attrs.get("StartTime"), 0.0), _f(p.attrs.get("StopTime"), 0.0))
+            os_attr = p.attrs.get("OverSampling")
+            os_ = int(float(os_attr)) if os_attr is not None else None
+            if typ not in (0, 1, 2, 3):
+                self.warnings.append(f"probe {p.name!r}: type {typ} not supported; ignored")
+                continue
+            extent = [a for a in range(3) if c0[a] != c1[a]]
+            norm = p.attrs.get("NormDir")
+            norm = int(float(norm)) if norm is not None else None
+            if typ == 0 and len(extent) != 1:
+                self.warnings.append(f"probe {p.name!r}: its box is not a line; ignored, as openEMS does")
+                continue
+            if typ == 1 and ((norm is not None and norm in extent) or (norm is None and len(extent) == 3)):
+                self.warnings.append(f"probe {p.name!r}: not flat along its normal; ignored, as openEMS does")
+                continue
+            prim = lambda c: [snap_lower(lines[a], c[a]) for a in range(3)]  # noqa: E731
+            dual = lambda c: [snap_cell(lines[a], c[a]) for a in range(3)]  # noqa: E731
+            if typ == 0:
+                start, stop = prim(c0), prim(c1)
+                path = voltage_path(start, stop)
+                k = m.add_probe(VOLTAGE, [(a, nd, w * weight) for a, nd, w in path]) if path else \
+                    m.add_probe(VOLTAGE, [(0, (0, 0, 0), 0.0)])
+                self.probes.append(ProbeSpec(p.name, "voltage", [k], ((at(start), start), (at(stop), stop)),
+                                             p.fd, os_, *window))
+            elif typ == 1:
+                start = [snap_lower(lines[a], c0[a]) for a in range(3)]
+                stop = [snap_lower(lines[a], c1[a]) for a in range(3)]
+                if norm is None:
+                    flat = [a for a in range(3) if start[a] == stop[a]]
+                    if len(flat) != 1:
+                        self.warnings.append(f"probe {p.name!r}: no normal direction; ignored")
+                        continue
+                    norm = flat[0]
+                nn = norm
+                crossed = [False] * 3
+                for a in range(3):
+                    if a == nn:
+                        continue
+                    r0, r1 = c0[a], c1[a]
+                    lo = snap_upper(lines[a], min(r0, r1))
+                    hi = snap_lower(lines[a], max(r0, r1))
+                    crossed[a] = lo > hi
+                    start[a], stop[a] = (lo, hi) if r0 <= r1 else (hi, lo)
+                flat_layer = dual(c0)[nn] if start[nn] == stop[nn] else None
+                lo = [min(start[a], stop[a]) for a in range(3)]
+                hi = [max(start[a], stop[a]) for a in range(3)]
+                if flat_layer is not None:
+                    layer = min(flat_layer, n[nn] - 2)
+                elif lo[nn] == hi[nn]:
+                    layer = min(lo[nn], n[nn] - 2)
+                else:
+                    layer = lo[nn] + (hi[nn] - lo[nn] - 1) // 2
+                sign = 1.0 if start[nn] <= stop[nn] else -1.0
+                entries = [(a, nd, -w * sign) for a, nd, w in loop_entries(nn, lo, hi, layer)]
+                entries = openems_loop_order(entries, nn, start, stop)
+                llo, lhi = [0, 0, 0], [0, 0, 0]
+                for d in range(3):
+                    if d == nn:
+                        llo[d] = lhi[d] = layer
+                    else:
+                        a_, b_ = min(start[d], stop[d]), max(start[d], stop[d])
+                        if crossed[d]:
+                            a_, b_ = b_, a_
+                        llo[d], lhi[d] = max(a_ - 1, 0), min(b_, max(n[d] - 2, 0))
+                if any(crossed):
+                    entries = []
+                if entries:
+                    k = m.add_probe(CURRENT, [(a, nd, w * weight) for a, nd, w in entries], f32_sum=True)
+                else:
+                    k = m.add_probe(CURRENT, [(0, (0, 0, 0), 0.0)])
+                self.probes.append(ProbeSpec(p.name, "current", [k], ((at(llo), llo), (at(lhi), lhi)), p.fd, os_,
+                                             *window))
+            else:
+                e = typ == 2
+                idx = prim(c0) if e else dual(c0)
+                loc = ((at(prim(c0)), prim(c0)), (at(prim(c1)), prim(c1))) if e else \
+                    ((at(idx), idx), (at(dual(c1)), dual(c1)))
+                ks = []
+                for a in range(3):
+                    ok = all((idx[b] + 1 < n[b]) if ((b == a) == e) else True for b in range(3))
+                    length = 0.0
+                    if ok:
+                        length = self.model_delta(a, idx[a]) if e else self.model_dual(a, idx[a])
+                    q = VOLTAGE if e else CURRENT
+                    if ok and length > 0:
+                        ks.append(m.add_probe(q, [(a, tuple(idx), weight / length)]))
+                    else:
+                        ks.append(m.add_probe(q, [(a, (0, 0, 0), 0.0)]))
+                self.probes.append(ProbeSpec(p.name, "efield" if e else "hfield", ks, loc, p.fd, os_, *window))
+
+    # -- running and output
+    def run(self, engine) -> "Results":
+        """Runs ``engine`` (built on ``self.model``) for the run length plus
+        one step, whose H update gives the H-type probes' sample after the
+        last step, and collects the probe series."""
+        engine.run(self.steps + 1)
+        series = {}
+        for p in self.probes:
+            cols = [np.asarray(engine.samples(k)) for k in p.ops]
+            v = np.stack(cols, axis=1)
+            magnetic = p.kind in PF.MAGNETIC
+            series[p.name] = v[: self.steps + 1] if magnetic else v[: self.steps]
+        return Results(self, series)
+
+
+
+@dataclass
+class Results:
+    setup: Setup
+    series: dict
+
+    def rows(self, p: ProbeSpec) -> list:
+        """(step, time, values) of every sample of probe ``p`` in its
+        StartTime/StopTime window (src/sim/mod.rs:1135-1150: E-type samples
+        with start − dt ≤ t ≤ stop + dt, H-type start ≤ t ≤ stop + dt; stop
+        ≤ 0: no limit); E-type series start with the initial state at t = 0,
+        H-type ones end with the sample after the last step."""
+        s = self.setup
+        dt = s.dt
+        v = self.series[p.name]
+        width = v.shape[1] if v.ndim == 2 else 1
+        if p.kind in PF.MAGNETIC or len(v):
+            rows = PF.samples(p.kind, v, dt, 1)
+        else:
+            rows = [(0, 0.0, [0.0] * width)]  # a run of no steps: the initial state
+        eps = 1e-9 * dt
+        lo = p.start_time - (0.0 if p.kind in PF.MAGNETIC else dt) - eps
+        return [r for r in rows if r[1] >= lo and (p.stop_time <= 0.0 or r[1] <= p.stop_time + dt + eps)]
+
+    def files(self) -> dict:
+        """File name → text of every probe file openEMS writes: the
+        time-domain rows every ⌊N/OverSampling⌋ steps and, with
+        FD_Samples, the frequency-domain file over the rows every N steps
+        (N the Nyquist interval)."""
+        s = self.setup
+        dt = s.dt
+        nyq = s.file.signal.nyquist_interval(dt)
+        out = {}
+        for p in s.probes:
+            os_ = p.oversampling if (p.oversampling or 0) >= 2 else s.file.oversampling
+            kt = max(1, nyq // os_)
+            rows = self.rows(p)
+            out[p.name] = PF.ProbeFile("time", p.kind, [[t] + list(x) for st, t, x in rows if st % kt == 0],
+                                       p.location, PF.generator_text()).to_text()
+            if p.fd:
+                picked = [(t, np.asarray(x)) for st, t, x in rows if st % nyq == 0]
+                w = 2.0 * nyq * dt
+                fd_rows = []
+                for f in p.fd:
+                    acc = np.zeros(len(picked[0][1]) if picked else len(PF.COLUMNS[p.kind]), dtype=np.complex128)
+                    for t, x in picked:
+                        acc += w * np.exp(-2j * math.pi * f * t) * x
+                    r = [float(f)]
+                    for a in acc:
+                        r += [a.real, a.imag]
+                    fd_rows.append(r)
+                out[p.name + "_FD"] = PF.ProbeFile("frequency", p.kind, fd_rows, p.location,
+                                                   PF.generator_text()).to_text()
+        return out
+
+    def signal_files(self) -> dict:
+        s = self.setup
+        return {"et": s.file.signal.signal_text(s.dt, s.steps, 0.0),
+                "ht": s.file.signal.signal_text(s.dt, s.steps, 0.5)}
+
+    def write(self, directory: str) -> list:
+        os.makedirs(directory, exist_ok=True)
+        out = []
+        for name, text in {**self.files(), **self.signal_files()}.items():
+            path = os.path.join(directory, name)
+            with open(path, "w") as h:
+                h.write(text)
+            out.append(path)
+        return out
+
+
+def load(path: str) -> Setup:
+    with open(path) as h:
+        return Setup(parse(h.read()))
+
+
+def loads(text: str) -> Setup:
+    return Setup(parse(text))
+
+
+def main(argv=None) -> int:
+    """``python -m ems_b200.openems model.xml OUTDIR [--device N]``: runs an
+    openEMS file on the CUDA engine and writes openEMS's probe files and
+    ``et``/``ht`` into OUTDIR (the ems CLI's ``--openems`` output)."""
+    import argparse
+
+    from . import Engine
+
+    ap = argparse.ArgumentParser(prog="python -m ems_b200.openems", description=main.__doc__)
+    ap.add_argument("model")
+    ap.add_argument("outdir")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    s = load(a.model)
+    for w in s.warnings:
+        print("warning:", w)
+    eng = Engine(s.model, device=a.device)
+    r = s.run(eng)
+    paths = r.write(a.outdir)
+    print(f"{len(paths)} files in {a.outdir}: {s.steps} steps of {s.dt:.6g} s")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -70,6 +70,24 @@ int ems_model_faces(ems_model* m, const int faces[6]);
  * fixed_dt > 0, takes it (TimeStep::Fixed), then the coefficients
  * (Coefficients::compute). Must precede the operators. */
 int ems_model_build(ems_model* m, double courant, double fixed_dt);
+/* Builds with the time step dt taken as given (TimeStep::Bound,
+ * src/engine/coeffs.rs:233-236: a step established elsewhere, such as
+ * openEMS's criterion below). flags: 1 openEMS's coefficient rounding (C,
+ * G, L, R rounded to f32 and formed with openEMS's vacuum constants;
+ * CoeffRounding, src/engine/coeffs.rs:705-760), 2 openEMS's average of the
+ * magnetic conductivity over the two halves of a dual edge (openems_sigma_m,
+ * src/compile/openems.rs:580-650). */
+int ems_model_build_bound(ems_model* m, double dt, int flags);
+/* openEMS's time step of the model's grid and materials by TimeStepMethod
+ * `method` (3 Rennings, openEMS's default; 1 the Gershgorin "CFL" bound),
+ * before any TimeStepFactor (openems_timestep, src/engine/timestep.rs:
+ * 213-287). 0 for an unknown method. */
+double ems_model_openems_timestep(const ems_model* m, int method);
+/* Zeroes the update coefficients of the E edges (field 0: ca, cb) or H
+ * dual edges (field 1: da, db) along `axis` at the nodes of the inclusive
+ * box lo..hi, after build (openEMS's PMC half cell, pmc_half_cell,
+ * src/compile/mod.rs:1556-1626, is made of such boxes). */
+int ems_model_zero_edges(ems_model* m, int field, int axis, const uint64_t lo[3], const uint64_t hi[3]);
 double ems_model_dt(const ems_model* m);
 double ems_model_courant_limit(const ems_model* m);
 /* Coefficient lane `lane` (0..11) in reference layout (valid after build). */
@@ -132,6 +150,10 @@ int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, c
  * Returns the op index or -1. */
 int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6], const uint64_t hold_until[6],
                       int flags);
+
+/* Sums probe `op`'s entries in f32 (openEMS's current probes, the
+ * `f32_sum` of Probe, src/engine/probe.rs:381-392) when `on`. */
+int ems_model_probe_f32(ems_model* m, int op, int on);
 
 /* The engine descriptor (valid until the model changes or is freed). */
 const ems_engine_desc* ems_model_desc(ems_model* m);

@@ -1,0 +1,147 @@
+"""openEMS XML models on the CUDA engine against the oracle.
+
+Models written for this test in openEMS's XML (graded meshes, PEC, PMC and
+Mur faces, anisotropic lossy materials with magnetic conductivity, metal
+under a higher-priority material, soft and hard E and H excitations with
+every signal type and a delay, voltage, current, E and H field probes with
+FD samples, a time window and a probe oversampling) are set up by
+ems_b200/openems.py and run on the CUDA engine (every schedule that can
+run them) and on the oracle: every probe series, every written probe file
+and the final fields agree bit for bit. The oracle itself is checked
+against openEMS's own output for the same features in
+test_openems_fixtures.py. Also the command-line entry point.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ems_b200 as E
+from ems_b200 import openems as OE
+from helpers import assert_fields_equal
+from oracle import OracleEngine
+
+pytestmark = pytest.mark.gpu
+
+
+def _lines(v):
+    return ",".join(f"{x:g}" for x in v)
+
+
+X = [0, 1, 2, 3, 4, 5, 5.5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16]
+Y = [0, 1, 2, 3, 4, 4.6, 5.2, 6, 7, 8, 9, 10, 11, 12, 13]
+Z = [0, 1.2, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12]
+
+BOX = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="420" endCriteria="1e-30" OverSampling="3">
+    <Excitation Type="0" f0="4e9" fc="3e9"/>
+    <BoundaryCond xmin="PEC" xmax="MUR" ymin="PMC" ymax="PEC" zmin="MUR" zmax="PEC" MUR_PhaseVelocity="2.6e8"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <Material Name="aniso" Isotropy="0"><Property Epsilon="2,3.5,2.5" Mue="1,1.4,1.2" Kappa="0.01,0.005,0.02" Sigma="80,0,40"/>
+        <Primitives><Box Priority="1"><P1 X="9" Y="2" Z="2"/><P2 X="14" Y="9" Z="7"/></Box></Primitives></Material>
+      <Metal Name="block"><Primitives><Box Priority="2"><P1 X="10" Y="4" Z="3"/><P2 X="12" Y="6" Z="5"/></Box></Primitives></Metal>
+      <Material Name="over"><Property Epsilon="4" Kappa="0.01"/>
+        <Primitives><Box Priority="3"><P1 X="10" Y="4" Z="5"/><P2 X="12" Y="6" Z="6"/></Box></Primitives></Material>
+      <Excitation Name="soft" Type="0" Excite="0.3,0,1"><Primitives><Box Priority="0"><P1 X="4" Y="7" Z="5"/><P2 X="5" Y="7" Z="7"/></Box></Primitives></Excitation>
+      <Excitation Name="hard" Type="1" Excite="0,0.5,0"><Primitives><Box Priority="0"><P1 X="15" Y="10" Z="9"/><P2 X="15" Y="11" Z="9"/></Box></Primitives></Excitation>
+      <ProbeBox Name="ut" Type="0"><FD_Samples>2e9,4e9,6e9</FD_Samples><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="4"/><P2 X="7" Y="7" Z="8.4"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="ur" Type="0" Weight="-2"><Primitives><Box Priority="0"><P1 X="13" Y="8" Z="3"/><P2 X="9.6" Y="8" Z="3"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="it" Type="1" NormDir="2"><FD_Samples>3e9</FD_Samples><Primitives><Box Priority="0"><P1 X="3" Y="5.2" Z="6.3"/><P2 X="6" Y="9" Z="6.3"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="ix" Type="1"><Primitives><Box Priority="0"><P1 X="8" Y="3" Z="2"/><P2 X="8" Y="10" Z="9"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="ef" Type="2" StartTime="1e-10" StopTime="5e-10"><Primitives><Box Priority="0"><P1 X="8" Y="7" Z="6"/><P2 X="8" Y="7" Z="6"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="hf" Type="3" OverSampling="6"><FD_Samples>4e9</FD_Samples><Primitives><Box Priority="0"><P1 X="5.5" Y="6.5" Z="6"/><P2 X="5.5" Y="6.5" Z="6"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+SINE = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="300" endCriteria="-1" TimeStepFactor="0.9">
+    <Excitation Type="1" f0="3e9"/>
+    <BoundaryCond xmin="PMC" xmax="PEC" ymin="PEC" ymax="PMC" zmin="PEC" zmax="MUR"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <BackgroundMaterial Epsilon="1.5" Mue="1.1"/>
+    <Properties>
+      <Excitation Name="h" Type="2" Excite="0,0,1" Delay="1.3e-10"><Primitives><Box Priority="0"><P1 X="6.5" Y="5.5" Z="6"/><P2 X="7.5" Y="6.5" Z="6"/></Box></Primitives></Excitation>
+      <Excitation Name="off" Type="0" Excite="1,0,0" Enabled="0"><Primitives><Box Priority="0"><P1 X="2" Y="2" Z="2"/><P2 X="3" Y="2" Z="2"/></Box></Primitives></Excitation>
+      <ProbeBox Name="hz" Type="3"><FD_Samples>3e9</FD_Samples><Primitives><Box Priority="0"><P1 X="8.5" Y="6.5" Z="6.5"/><P2 X="8.5" Y="6.5" Z="6.5"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="ue" Type="0"><Primitives><Box Priority="0"><P1 X="9" Y="4" Z="6"/><P2 X="9" Y="8" Z="6"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+PULSES = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="90" endCriteria="1e-30" TimeStepMethod="1">
+    <Excitation Type="10" f0="5e9" Function="exp(-((t-6e-11)/2e-11)^2)*sin(2*pi*5e9*t)"/>
+    <BoundaryCond xmin="PEC" xmax="PEC" ymin="PEC" ymax="PEC" zmin="PEC" zmax="PEC"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <Excitation Name="hh" Type="3" Excite="0,1,0"><Primitives><Box Priority="0"><P1 X="5.5" Y="6" Z="5.5"/><P2 X="5.5" Y="6" Z="5.5"/></Box></Primitives></Excitation>
+      <Excitation Name="se" Type="0" Excite="0,0,-1"><Primitives><Box Priority="0"><P1 X="9" Y="8" Z="3"/><P2 X="9" Y="8" Z="6"/></Box></Primitives></Excitation>
+      <ProbeBox Name="e" Type="2"><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="5"/><P2 X="8" Y="8" Z="6"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="i" Type="1" NormDir="1"><Primitives><Box Priority="0"><P1 X="4" Y="6.4" Z="4"/><P2 X="7" Y="6.4" Z="7"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+
+def _both(text, schedule=0):
+    s = OE.loads(text)
+    g = E.Engine(s.model)
+    g.set_schedule(schedule)
+    o = OracleEngine(s.model, threads=2)
+    return s, g, s.run(g), o, s.run(o)
+
+
+# Schedules 2 (fused) and 5 (sweep) do not run magnetic sources.
+@pytest.mark.parametrize("name,text,schedule", [
+    ("box", BOX, 0), ("box", BOX, 1), ("box", BOX, 2), ("box", BOX, 3), ("box", BOX, 5),
+    ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1)])
+def test_openems_models_bit_exact(name, text, schedule):
+    s, g, rg, o, ro = _both(text, schedule)
+    assert s.steps > 0 and s.probes
+    for p in s.probes:
+        a, b = rg.series[p.name], ro.series[p.name]
+        assert a.shape == b.shape and a.size
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), (name, p.name)
+    assert rg.files().keys() == ro.files().keys()
+    for k, text_g in rg.files().items():
+        assert text_g.splitlines()[1:] == ro.files()[k].splitlines()[1:], (name, k)
+    assert_fields_equal(g, o, f"openEMS model {name}")
+    assert any(np.any(v != 0) for v in rg.series.values())
+
+
+def test_openems_command_line(tmp_path):
+    path = tmp_path / "model.xml"
+    path.write_text(BOX)
+    assert OE.main([str(path), str(tmp_path / "out")]) == 0
+    s = OE.loads(BOX)
+    ro = s.run(OracleEngine(s.model, threads=2))
+    want = {**ro.files(), **ro.signal_files()}
+    assert sorted(os.listdir(tmp_path / "out")) == sorted(want)
+    for k, text in want.items():
+        assert (tmp_path / "out" / k).read_text().splitlines()[1:] == text.splitlines()[1:], k
