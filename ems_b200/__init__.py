@@ -235,6 +235,7 @@ GPU_SYMBOLS = {
     "ems_gpu_last_error": (C.c_char_p, [C.c_void_p]),
     "ems_gpu_launch_count": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+    "ems_gpu_set_curl_order": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_energy_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -676,6 +677,11 @@ class Engine:
         n = C.c_uint64()
         self._ck(self._lib.ems_gpu_launch_count(self._h, C.byref(n)))
         return n.value
+
+    def set_curl_order(self, order: int) -> None:
+        """0 the reference's default summation order of the curl, 1
+        openEMS's (``CurlOrder``; per-operator, split and sweep schedules)."""
+        self._ck(self._lib.ems_gpu_set_curl_order(self._h, order))
 
     def set_schedule(self, s: int) -> None:
         """0 automatic, 1 per-operator kernels, 2 fused single pass, 3 two kernels."""

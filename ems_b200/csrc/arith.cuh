@@ -23,6 +23,28 @@ __device__ __forceinline__ float h_upd(float da, float h, float db, float a, flo
     return flush(__fsub_rn(__fmul_rn(da, h), __fmul_rn(db, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));
 }
 
+// openEMS's summation order with every operation flushed (CurlOrder::OpenEms,
+// src/engine/kernel.rs:35-50): h = da·h − db·(((a − b) + d) − c) and
+// u = ca·u + cb·(((a − b) − c) + d).
+__device__ __forceinline__ float h_upd_oe(float da, float h, float db, float a, float b, float c, float d) {
+    const float curl = flush(__fsub_rn(flush(__fadd_rn(flush(__fsub_rn(a, b)), d)), c));
+    return flush(__fsub_rn(flush(__fmul_rn(da, h)), flush(__fmul_rn(db, curl))));
+}
+__device__ __forceinline__ float e_upd_oe(float ca, float u, float cb, float a, float b, float c, float d) {
+    const float curl = flush(__fadd_rn(flush(__fsub_rn(flush(__fsub_rn(a, b)), c)), d));
+    return flush(__fadd_rn(flush(__fmul_rn(ca, u)), flush(__fmul_rn(cb, curl))));
+}
+
+// The update in the summation order OE selects (false: the reference's).
+template <bool OE>
+__device__ __forceinline__ float h_upd_t(float da, float h, float db, float a, float b, float c, float d) {
+    return OE ? h_upd_oe(da, h, db, a, b, c, d) : h_upd(da, h, db, a, b, c, d);
+}
+template <bool OE>
+__device__ __forceinline__ float e_upd_t(float ca, float u, float cb, float a, float b, float c, float d) {
+    return OE ? e_upd_oe(ca, u, cb, a, b, c, d) : e_upd(ca, u, cb, a, b, c, d);
+}
+
 // (1 + a)·p/b, 0 where b = 0 (src/engine/kernel.rs:116-120).
 __device__ __forceinline__ double weight(float a, double p, float b) {
     return b != 0.0f ? __ddiv_rn(__dmul_rn(__dadd_rn(1.0, (double)a), p), (double)b) : 0.0;

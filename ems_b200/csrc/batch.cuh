@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_batch_h(const
         const BatchModel& M = T.models[m];
         const uint32_t lb = gb - T.start[BK_SPLIT][m];
         const uint32_t i = lb / M.bx, bx = lb - i * M.bx;
-        const double w = split_h_quad<ENERGY>(M.P, i, bx * kSplitThreads + threadIdx.x);
+        const double w = split_h_quad<ENERGY, false>(M.P, i, bx * kSplitThreads + threadIdx.x);
         if (ENERGY) {
             const double s = block_sum<kSplitThreads>(w);
             if (threadIdx.x == 0) partials[gb] = s;
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_batch_e(const __grid_constant
         const BatchModel& M = T.models[m];
         const uint32_t lb = gb - T.start[BK_SPLIT][m];
         const uint32_t i = lb / M.bx, bx = lb - i * M.bx;
-        split_e_quad(M.P, i, bx * kSplitThreads + threadIdx.x);
+        split_e_quad<false>(M.P, i, bx * kSplitThreads + threadIdx.x);
     }
 }
 

@@ -60,6 +60,7 @@ struct ems_gpu {
     uint64_t step = 0;
     uint64_t launches = 0;
     int schedule = 0;
+    bool oe_curl = false;  // openEMS's summation order of the curl (ems_gpu_set_curl_order)
     std::string err;
     // Autotuning (ems_gpu_autotune): candidate schedules timed over real
     // steps (every schedule gives the same bits), the pick cached by key.
@@ -774,11 +775,18 @@ ems_status run_step_sweep(ems_gpu* h, bool energy) {
         for (uint32_t a0 = 0; a0 < g.nx; a0 += S, ++ch) {
             const uint32_t np = std::min(S, g.nx - a0);
             const dim3 grd(bx, np, 1);
-            if (energy) k_split_h<true><<<grd, kSplitThreads, 0, s>>>(P, a0);
-            else k_split_h<false><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            if (h->oe_curl) {
+                if (energy) k_split_h<true, true><<<grd, kSplitThreads, 0, s>>>(P, a0);
+                else k_split_h<false, true><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            } else if (energy) {
+                k_split_h<true><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            } else {
+                k_split_h<false><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            }
             ++h->launches;
             if (pf) { pole(1, ch); shell(0, ch); } else { shell(0, ch); pole(1, ch); }
-            k_split_e<<<grd, kSplitThreads, 0, s>>>(P, a0);
+            if (h->oe_curl) k_split_e<true><<<grd, kSplitThreads, 0, s>>>(P, a0);
+            else k_split_e<<<grd, kSplitThreads, 0, s>>>(P, a0);
             ++h->launches;
             if (pf) { pole(0, ch); shell(1, ch); } else { shell(1, ch); pole(0, ch); }
         }
@@ -845,16 +853,21 @@ ems_status run_step(ems_gpu* h, bool energy) {
     dim3 grd(blocks_for(g.nz, kRowThreads), (unsigned)g.ny, (unsigned)g.nx);
     const dim3 qgrd(split_blocks_x(g), g.nx, 1);
     cudaEvent_t ev = h->prof_begin();
+    const bool oe = h->oe_curl;
     if (split) {
         if (energy) {
-            k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+            if (oe) k_split_h<true, true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+            else k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
         } else {
-            k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+            if (oe) k_split_h<false, true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+            else k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
         }
     } else if (energy) {
-        k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
+        if (oe) k_update_h<true, true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
+        else k_update_h<true><<<grd, blk, 0, s>>>(g, f, c, h->partials);
     } else {
-        k_update_h<false><<<grd, blk, 0, s>>>(g, f, c, nullptr);
+        if (oe) k_update_h<false, true><<<grd, blk, 0, s>>>(g, f, c, nullptr);
+        else k_update_h<false><<<grd, blk, 0, s>>>(g, f, c, nullptr);
     }
     h->prof_end(0, ev);
     ++h->launches;
@@ -902,9 +915,11 @@ ems_status run_step(ems_gpu* h, bool energy) {
     if (st) return st;
     ev = h->prof_begin();
     if (split) {
-        k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+        if (oe) k_split_e<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+        else k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
     } else {
-        k_update_e<<<grd, blk, 0, s>>>(g, f, c);
+        if (oe) k_update_e<true><<<grd, blk, 0, s>>>(g, f, c);
+        else k_update_e<<<grd, blk, 0, s>>>(g, f, c);
     }
     h->prof_end(1, ev);
     ++h->launches;
@@ -1447,22 +1462,22 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     if (!h || !cache_path) return EMS_ERR_INVALID;
     auto& T = h->tune;
     char key[256];
-    std::snprintf(key, sizeof key, "engine %ux%ux%u ops=%zu tables=%d", h->g.nx, h->g.ny, h->g.nz, h->ops.size(),
-                  h->tables_ok ? 1 : 0);
+    std::snprintf(key, sizeof key, "engine %ux%ux%u ops=%zu tables=%d curl=%d", h->g.nx, h->g.ny, h->g.nz,
+                  h->ops.size(), h->tables_ok ? 1 : 0, h->oe_curl ? 1 : 0);
     std::string k(key);
     for (auto& op : h->ops) k += "," + std::to_string(op.kind);
     T.key = k;
     T.cache = cache_path;
     int v = 0;
     if (tune_lookup(T.cache, T.key, &v) &&
-        (v == 1 || ((v == 3 || v == 4) && h->tables_ok) || (v == 5 && h->tables_ok && h->sweep_ok))) {
+        (v == 1 || ((v == 4 || (v == 3 && !h->oe_curl)) && h->tables_ok) || (v == 5 && h->tables_ok && h->sweep_ok))) {
         h->schedule = v;
         return EMS_OK;
     }
     // In-place schedules only (the per-operator, two-kernel and split ones
     // share the CPML state buffers).
     T.cand.clear();
-    if (h->tables_ok) T.cand = {4, 3};
+    if (h->tables_ok) T.cand = h->oe_curl ? std::vector<int>{4} : std::vector<int>{4, 3};
     if (h->tables_ok && h->sweep_ok) T.cand.push_back(5);
     T.cand.push_back(1);
     T.ms.assign(T.cand.size(), 0.0);
@@ -1651,12 +1666,28 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
     if (!h || schedule < 0 || schedule > 5) return EMS_ERR_INVALID;
+    if (h->oe_curl && (schedule == 2 || schedule == 3))
+        return fail(h, EMS_ERR_INVALID, "the fused and two-kernel schedules sum the curl in the default order only");
     if (schedule == 2 && !h->fused_ok) return fail(h, EMS_ERR_INVALID, "fused schedule unavailable: " + h->fused_why);
     if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
     if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
     if (schedule == 5 && !(h->tables_ok && h->sweep_ok))
         return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources") : h->tables_why));
     h->schedule = schedule;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_set_curl_order(ems_gpu* h, int order) {
+    if (!h || order < 0 || order > 1) return EMS_ERR_INVALID;
+    if (order == 1 && (h->schedule == 2 || h->schedule == 3))
+        return fail(h, EMS_ERR_INVALID, "the fused and two-kernel schedules sum the curl in the default order only");
+    h->oe_curl = order == 1;
+    // A captured sweep step holds the other kernels.
+    for (auto& gx : h->sweep_graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
     return EMS_OK;
 }
 

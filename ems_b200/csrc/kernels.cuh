@@ -87,8 +87,8 @@ struct ProbeDevT {
 // H update of every dual edge (src/engine/kernel.rs:447-511, 571-618);
 // with ENERGY each block also writes its share of the energy invariant
 // Σ (1+ca)/cb·u² + Σ (1+da)/db·i_old·i_new in units of dt/4
-// (src/engine/kernel.rs:132-244).
-template <bool ENERGY>
+// (src/engine/kernel.rs:132-244). OE: openEMS's summation order.
+template <bool ENERGY, bool OE = false>
 __global__ void __launch_bounds__(kRowThreads) k_update_h(const __grid_constant__ Grid g, const __grid_constant__ Fields f, const __grid_constant__ Coeffs c, double* partials) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y, i = blockIdx.z;
@@ -105,21 +105,21 @@ __global__ void __launch_bounds__(kRowThreads) k_update_h(const __grid_constant_
         if (j + 1 < g.ny && k + 1 < g.nz) {
             const float old = f.i[0][idx];
             const float da = c.c[6][idx], db = c.c[9][idx];
-            const float nw = h_upd(da, old, db, f.u[2][idx + sj], uz, f.u[1][idx + 1], uy);
+            const float nw = h_upd_t<OE>(da, old, db, f.u[2][idx + sj], uz, f.u[1][idx + 1], uy);
             f.i[0][idx] = nw;
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
         }
         if (i + 1 < g.nx && k + 1 < g.nz) {
             const float old = f.i[1][idx];
             const float da = c.c[7][idx], db = c.c[10][idx];
-            const float nw = h_upd(da, old, db, f.u[0][idx + 1], ux, f.u[2][idx + si], uz);
+            const float nw = h_upd_t<OE>(da, old, db, f.u[0][idx + 1], ux, f.u[2][idx + si], uz);
             f.i[1][idx] = nw;
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
         }
         if (i + 1 < g.nx && j + 1 < g.ny) {
             const float old = f.i[2][idx];
             const float da = c.c[8][idx], db = c.c[11][idx];
-            const float nw = h_upd(da, old, db, f.u[1][idx + si], uy, f.u[0][idx + sj], ux);
+            const float nw = h_upd_t<OE>(da, old, db, f.u[1][idx + si], uy, f.u[0][idx + sj], ux);
             f.i[2][idx] = nw;
             if (ENERGY) w = __dadd_rn(w, weight(da, __dmul_rn((double)old, (double)nw), db));
         }
@@ -139,7 +139,9 @@ __global__ void __launch_bounds__(1024) k_reduce_partials(const double* partials
     if (threadIdx.x == 0) out[0] = t;
 }
 
-// E update of every edge (src/engine/kernel.rs:624-697).
+// E update of every edge (src/engine/kernel.rs:624-697); OE: openEMS's
+// summation order.
+template <bool OE = false>
 __global__ void __launch_bounds__(kRowThreads) k_update_e(const __grid_constant__ Grid g, const __grid_constant__ Fields f, const __grid_constant__ Coeffs c) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y, i = blockIdx.z;
@@ -150,17 +152,17 @@ __global__ void __launch_bounds__(kRowThreads) k_update_e(const __grid_constant_
     if (i + 1 < g.nx) {
         const float b = j > 0 ? f.i[2][idx - sj] : 0.0f;
         const float d = k > 0 ? f.i[1][idx - 1] : 0.0f;
-        f.u[0][idx] = e_upd(c.c[0][idx], f.u[0][idx], c.c[3][idx], iz, b, iy, d);
+        f.u[0][idx] = e_upd_t<OE>(c.c[0][idx], f.u[0][idx], c.c[3][idx], iz, b, iy, d);
     }
     if (j + 1 < g.ny) {
         const float b = k > 0 ? f.i[0][idx - 1] : 0.0f;
         const float d = i > 0 ? f.i[2][idx - si] : 0.0f;
-        f.u[1][idx] = e_upd(c.c[1][idx], f.u[1][idx], c.c[4][idx], ix, b, iz, d);
+        f.u[1][idx] = e_upd_t<OE>(c.c[1][idx], f.u[1][idx], c.c[4][idx], ix, b, iz, d);
     }
     if (k + 1 < g.nz) {
         const float b = i > 0 ? f.i[1][idx - si] : 0.0f;
         const float d = j > 0 ? f.i[0][idx - sj] : 0.0f;
-        f.u[2][idx] = e_upd(c.c[2][idx], f.u[2][idx], c.c[5][idx], iy, b, ix, d);
+        f.u[2][idx] = e_upd_t<OE>(c.c[2][idx], f.u[2][idx], c.c[5][idx], iy, b, ix, d);
     }
 }
 

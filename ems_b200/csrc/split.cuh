@@ -57,8 +57,9 @@ __device__ __forceinline__ bool quad_of(const Grid& g, uint32_t q, uint32_t& j, 
 // z-nodes per thread; with ENERGY each block writes its share of the energy
 // invariant in units of dt/4 (src/engine/kernel.rs:132-244). Entries the
 // update does not write (edges that do not exist, row padding) are stored
-// back as read. Grid: (quads of a plane / kSplitThreads, nx).
-template <bool ENERGY>
+// back as read. OE: openEMS's summation order. Grid: (quads of a plane /
+// kSplitThreads, nx).
+template <bool ENERGY, bool OE>
 __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
@@ -85,9 +86,10 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
             const uint32_t k = k0 + e;
             const bool kn = k + 1 < g.nz;
             const float uy1 = e < 3 ? uy.v[e + 1] : uy4, ux1 = e < 3 ? ux.v[e + 1] : ux4;
-            if (jn && kn) nx_.v[e] = h_upd(dax.v[e], hx.v[e], dbx.v[e], uzj.v[e], uz.v[e], uy1, uy.v[e]);
-            if (in_ && kn) ny_.v[e] = h_upd(day.v[e], hy.v[e], dby.v[e], ux1, ux.v[e], uzi.v[e], uz.v[e]);
-            if (in_ && jn && k < g.nz) nz_.v[e] = h_upd(daz.v[e], hz.v[e], dbz.v[e], uyi.v[e], uy.v[e], uxj.v[e], ux.v[e]);
+            if (jn && kn) nx_.v[e] = h_upd_t<OE>(dax.v[e], hx.v[e], dbx.v[e], uzj.v[e], uz.v[e], uy1, uy.v[e]);
+            if (in_ && kn) ny_.v[e] = h_upd_t<OE>(day.v[e], hy.v[e], dby.v[e], ux1, ux.v[e], uzi.v[e], uz.v[e]);
+            if (in_ && jn && k < g.nz)
+                nz_.v[e] = h_upd_t<OE>(daz.v[e], hz.v[e], dbz.v[e], uyi.v[e], uy.v[e], uxj.v[e], ux.v[e]);
         }
         if (ENERGY) {
             const Q4 ca0 = ldq(lane_row(P, 0, row) + k0), cb0 = ldq(lane_row(P, 3, row) + k0);
@@ -115,11 +117,11 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
 }
 
 // Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
-template <bool ENERGY>
+template <bool ENERGY, bool OE = false>
 __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P,
                                                                          uint32_t i0) {
     const uint32_t i = i0 + blockIdx.y;
-    const double w = split_h_quad<ENERGY>(P, i, blockIdx.x * kSplitThreads + threadIdx.x);
+    const double w = split_h_quad<ENERGY, OE>(P, i, blockIdx.x * kSplitThreads + threadIdx.x);
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
         if (threadIdx.x == 0) P.partials[(size_t)i * gridDim.x + blockIdx.x] = s;
@@ -127,7 +129,9 @@ __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const
 }
 
 // E update of every edge (src/engine/kernel.rs:624-697), four z-nodes per
-// thread. Grid: (quads of a plane / kSplitThreads, nx).
+// thread; OE: openEMS's summation order. Grid: (quads of a plane /
+// kSplitThreads, nx).
+template <bool OE>
 __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
@@ -151,17 +155,18 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
         const uint32_t k = k0 + e;
         if (k >= g.nz) break;
         const float iy0 = e > 0 ? iy.v[e - 1] : iym, ix0 = e > 0 ? ix.v[e - 1] : ixm;
-        if (xi) nx_.v[e] = e_upd(cax.v[e], ex.v[e], cbx.v[e], iz.v[e], izj.v[e], iy.v[e], iy0);
-        if (yj) ny_.v[e] = e_upd(cay.v[e], ey.v[e], cby.v[e], ix.v[e], ix0, iz.v[e], izi.v[e]);
-        if (k + 1 < g.nz) nz_.v[e] = e_upd(caz.v[e], ez.v[e], cbz.v[e], iy.v[e], iyi.v[e], ix.v[e], ixj.v[e]);
+        if (xi) nx_.v[e] = e_upd_t<OE>(cax.v[e], ex.v[e], cbx.v[e], iz.v[e], izj.v[e], iy.v[e], iy0);
+        if (yj) ny_.v[e] = e_upd_t<OE>(cay.v[e], ey.v[e], cby.v[e], ix.v[e], ix0, iz.v[e], izi.v[e]);
+        if (k + 1 < g.nz) nz_.v[e] = e_upd_t<OE>(caz.v[e], ez.v[e], cbz.v[e], iy.v[e], iyi.v[e], ix.v[e], ixj.v[e]);
     }
     if (xi) stq(P.un[0] + idx, nx_);
     if (yj) stq(P.un[1] + idx, ny_);
     stq(P.un[2] + idx, nz_);
 }
 
+template <bool OE = false>
 __global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
-    split_e_quad(P, i0 + blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
+    split_e_quad<OE>(P, i0 + blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
 }
 
 // Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.

@@ -13,7 +13,9 @@ Restated from the reference:
   ``TimeStep``; a sinusoid's period split into whole steps
   (periodic_timestep, timestep.rs:292-296); the run length
   ``NumberOfTimesteps`` cut by ``MaxTime``;
-* the coefficients with openEMS's rounding (``CoeffRounding::OpenEms``);
+* the coefficients with openEMS's rounding (``CoeffRounding::OpenEms``)
+  and magnetic-conductivity average, the curl summed in openEMS's order
+  (``CurlOrder::OpenEms``);
 * the signals (src/waveform.rs:442-518, src/io/openems/signal.rs):
   openEMS's Gaussian (τ = 3/(2π·fc), delay 3τ, sample 0 zero), sinusoid
   (period repeated), Dirac, step and custom expressions; openEMS's timing
@@ -818,10 +820,14 @@ class Setup:
                 self.probes.append(ProbeSpec(p.name, "efield" if e else "hfield", ks, loc, p.fd, os_, *window))
 
     # -- running and output
-    def run(self, engine) -> "Results":
+    def run(self, engine, curl_order: int = 1) -> "Results":
         """Runs ``engine`` (built on ``self.model``) for the run length plus
         one step, whose H update gives the H-type probes' sample after the
-        last step, and collects the probe series."""
+        last step, and collects the probe series. ``curl_order`` 1 sums the
+        curl in openEMS's order, as the reference does for files (its
+        fields then equal openEMS's where the coefficients do), 0 in the
+        engine's default order."""
+        engine.set_curl_order(curl_order)
         engine.run(self.steps + 1)
         series = {}
         for p in self.probes:

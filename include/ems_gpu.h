@@ -310,6 +310,16 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 /* The schedule steps run with (1 to 5 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
+/* The order in which the H and E updates sum the four terms of an edge's
+ * circulation (CurlOrder, src/engine/kernel.rs:81-108): 0 the reference's
+ * default (a - b) - (c - d); 1 openEMS's, ((a - b) + d) - c for H and
+ * ((a - b) - c) + d for E with every operation's subnormal result flushed,
+ * which openEMS files use (their fields then equal openEMS's where the
+ * coefficients do). Order 1 runs on the per-operator, split and sweep
+ * schedules; it is refused while the fused or two-kernel schedule is set,
+ * and those are refused while it is on. */
+ems_status ems_gpu_set_curl_order(ems_gpu* h, int order);
+
 /* The sweep schedule's chunk size in x-planes (set at creation so that a
  * chunk's fields take under half of L2; larger than nx: one chunk). */
 ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes);

@@ -27,6 +27,7 @@ def lib() -> C.CDLL:
             "oracle_create": [p, C.c_int, p],
             "oracle_destroy": [p],
             "oracle_threads": [p],
+            "oracle_set_curl_order": [p, C.c_int],
             "oracle_run": [p, C.c_uint64],
             "oracle_step_with_energy": [p, p],
             "oracle_download_field": [p, C.c_int, C.c_int, p],
@@ -57,6 +58,11 @@ class OracleEngine:
     @property
     def threads(self) -> int:
         return self._lib.oracle_threads(self._h)
+
+    def set_curl_order(self, order: int) -> None:
+        """0 the reference's default summation order, 1 openEMS's."""
+        if self._lib.oracle_set_curl_order(self._h, order) != 0:
+            raise ValueError(f"invalid curl order {order}")
 
     def run(self, n: int) -> None:
         if self._lib.oracle_run(self._h, n) != 0:

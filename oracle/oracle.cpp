@@ -33,6 +33,17 @@ namespace {
 // src/engine/kernel.rs:30-33 — subnormal results rounded to zero.
 inline float flush(float x) { return std::fabs(x) < 1.17549435e-38f ? 0.0f : x; }
 
+// openEMS's summation order with every operation flushed (CurlOrder::OpenEms,
+// src/engine/kernel.rs:35-50 oe_h, oe_e).
+inline float oe_h(float da, float h, float db, float a, float b, float c, float d) {
+    const float curl = flush(flush(flush(a - b) + d) - c);
+    return flush(flush(da * h) - flush(db * curl));
+}
+inline float oe_e(float ca, float u, float cb, float a, float b, float c, float d) {
+    const float curl = flush(flush(flush(a - b) - c) + d);
+    return flush(flush(ca * u) + flush(cb * curl));
+}
+
 // src/engine/kernel.rs:116-120 — (1 + a)·p/b, 0 where b = 0.
 inline double weight(float a, double p, float b) {
     double w = (1.0 + (double)a) * p / (double)b;
@@ -182,6 +193,7 @@ struct oracle_engine {
     std::vector<size_t> slab_start;
     std::vector<double> plane_w;
     Pool* pool = nullptr;
+    bool oe = false;  // CurlOrder::OpenEms
 
     // ---- H update of one x-plane (src/engine/kernel.rs:447-511 h_plane,
     // 58-79 h_row, 132-174 h_row_energy). Returns the plane's H energy
@@ -206,7 +218,8 @@ struct oracle_engine {
             double acc[4] = {0.0, 0.0, 0.0, 0.0};
             for (size_t k = 0; k < m; ++k) {
                 float old = h[k];
-                float nw = flush(da[k] * old - db[k] * ((a[k] - b[k]) - (c[k] - d[k])));
+                float nw = oe ? oe_h(da[k], old, db[k], a[k], b[k], c[k], d[k])
+                              : flush(da[k] * old - db[k] * ((a[k] - b[k]) - (c[k] - d[k])));
                 if (ENERGY) acc[k & 3] += weight(da[k], (double)old * (double)nw, db[k]);
                 h[k] = nw;
             }
@@ -268,8 +281,9 @@ struct oracle_engine {
         const float* iz = &i[2][base];
         const float* iyp = gi == 0 ? zero.data() : &i[1][base - plane];
         const float* izp = gi == 0 ? zero.data() : &i[2][base - plane];
-        auto e1 = [](float ca, float u0, float cb, float a, float b, float c, float d) {
-            return flush(ca * u0 + cb * ((a - b) - (c - d)));
+        const bool o = oe;
+        auto e1 = [o](float ca, float u0, float cb, float a, float b, float c, float d) {
+            return o ? oe_e(ca, u0, cb, a, b, c, d) : flush(ca * u0 + cb * ((a - b) - (c - d)));
         };
         for (size_t j = 0; j < ny; ++j) {
             const size_t r = j * nz;
@@ -815,6 +829,12 @@ int oracle_destroy(oracle_engine* e) {
 }
 
 int oracle_threads(const oracle_engine* e) { return e ? e->pool->size() : 0; }
+
+int oracle_set_curl_order(oracle_engine* e, int order) {
+    if (!e || order < 0 || order > 1) return EMS_ERR_INVALID;
+    e->oe = order == 1;
+    return EMS_OK;
+}
 
 int oracle_run(oracle_engine* e, uint64_t n) {
     if (!e) return EMS_ERR_INVALID;

@@ -31,6 +31,9 @@ typedef struct oracle_engine oracle_engine;
 int oracle_create(const ems_engine_desc* desc, int threads, oracle_engine** out);
 int oracle_destroy(oracle_engine* e);
 int oracle_threads(const oracle_engine* e);
+/* 0: the reference's default curl order (a - b) - (c - d); 1: openEMS's
+ * order with every operation flushed (CurlOrder, src/engine/kernel.rs:81-108). */
+int oracle_set_curl_order(oracle_engine* e, int order);
 int oracle_run(oracle_engine* e, uint64_t n);
 int oracle_step_with_energy(oracle_engine* e, double* energy);
 int oracle_download_field(oracle_engine* e, int field, int axis, float* host);

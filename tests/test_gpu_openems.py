@@ -110,11 +110,14 @@ PULSES = f"""<?xml version="1.0" encoding="UTF-8"?>
 
 
 def _both(text, schedule=0):
+    """Both engines on the model, in openEMS's curl order except on the
+    fused and two-kernel schedules, which have only the default one."""
     s = OE.loads(text)
     g = E.Engine(s.model)
     g.set_schedule(schedule)
     o = OracleEngine(s.model, threads=2)
-    return s, g, s.run(g), o, s.run(o)
+    order = 0 if schedule in (2, 3) else 1
+    return s, g, s.run(g, order), o, s.run(o, order)
 
 
 # Schedules 2 (fused) and 5 (sweep) do not run magnetic sources.
@@ -133,6 +136,32 @@ def test_openems_models_bit_exact(name, text, schedule):
         assert text_g.splitlines()[1:] == ro.files()[k].splitlines()[1:], (name, k)
     assert_fields_equal(g, o, f"openEMS model {name}")
     assert any(np.any(v != 0) for v in rg.series.values())
+
+
+@pytest.mark.parametrize("schedule", [1, 4, 5])
+def test_openems_curl_order_with_every_operator(schedule):
+    """openEMS's summation order on a model with every operator (CPML,
+    electric poles, lumped port, sources, probes): bit for bit with the
+    oracle; and it differs from the default order."""
+    from helpers import mixed_model
+
+    m, ops = mixed_model(magnetic=False, h_source=False, steps=200)
+    g = E.Engine(m)
+    g.set_schedule(schedule)
+    g.set_curl_order(1)
+    with pytest.raises(E.EngineError):
+        g.set_schedule(3)
+    o = OracleEngine(m, threads=3)
+    o.set_curl_order(1)
+    g.run(200)
+    o.run(200)
+    assert_fields_equal(g, o, f"openEMS order, schedule {schedule}")
+    for k in (ops["pv"], ops["pe"]):
+        assert np.array_equal(g.samples(k).view(np.uint64), o.samples(k).view(np.uint64))
+    d = E.Engine(m)
+    d.set_schedule(schedule)
+    d.run(200)
+    assert not np.array_equal(d.field(0, E.Z), g.field(0, E.Z))
 
 
 def test_openems_command_line(tmp_path):

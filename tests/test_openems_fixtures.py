@@ -8,11 +8,12 @@ its model.xml, run on the oracle, written the openEMS way and compared as
 the reference's own tests/openems_core.rs and tests/openems_sweep.rs do:
 the same set of probe files, the coordinate header lines exactly, the
 sample times (1e-6 relative), the values (relative L2 difference over all
-value columns below the tolerance), the excitation signals (first period of
-a sinusoid). The tolerance here is 1e-4 (the reference's core default): the
-engine sums the curl in its own order, so the fields differ from openEMS's
-by f32 round-off (measured 1e-7 ... 1e-5, up to 1.8e-4 on one
-frequency-domain file whose openEMS values are themselves round-off).
+value columns), the excitation signals (first period of a sinusoid). With
+openEMS's summation order of the curl (``CurlOrder::OpenEms``, what the
+reference uses for files) every value of every file equals openEMS's to
+all 12 printed digits, so the bar is 1e-12 (the reference's own tests
+allow 1e-6); in the engine's default order the same runs agree to
+round-off, 1e-7 ... 1.8e-4 (checked below on a few cases at 2.5e-4).
 
 Also the openEMS time step against the values openEMS printed, restated
 from the reference's unit tests (src/engine/timestep.rs:327-420), and the
@@ -38,14 +39,14 @@ have = pytest.mark.skipif(not os.path.isdir(FIXTURES), reason="reference fixture
 
 # (case, tolerance): the cases whose features the front end restates.
 CASES = [
-    ("gauss_soft_e", 1e-4), ("dirac_hard_e", 1e-4), ("sine_delay_soft_h", 1e-4), ("step_hard_h", 1e-4),
-    ("current_probes", 1e-4), ("probe_skip", 1e-4), ("cfl_method", 1e-4), ("max_time", 1e-4),
-    ("pmc_mur", 1e-4), ("cell_constant_material", 1e-4), ("adv_msl_nonuniform", 1e-4),
-    ("sweep_bg_material", 1e-4), ("sweep_exc_disabled", 1e-4), ("sweep_fdtd_odd", 1e-4),
-    ("sweep_fdtd_ts_and_steps0", 1e-30), ("sweep_grid_deltaunit_m", 1e-4), ("sweep_mat_aniso", 1e-4),
-    ("sweep_mat_aniso_single", 1e-4), ("sweep_mat_aniso_two", 1e-4), ("sweep_mat_mue_sigma", 1e-4),
-    ("sweep_prio_metal_in_mat", 1e-4), ("sweep_prio_overlap", 1e-4), ("sweep_probe_e_box", 1e-4),
-    ("sweep_probe_fd", 2.5e-4), ("sweep_probe_times", 1e-4),
+    ("gauss_soft_e", 1e-12), ("dirac_hard_e", 1e-12), ("sine_delay_soft_h", 1e-12), ("step_hard_h", 1e-12),
+    ("current_probes", 1e-12), ("probe_skip", 1e-12), ("cfl_method", 1e-12), ("max_time", 1e-12),
+    ("pmc_mur", 1e-12), ("cell_constant_material", 1e-12), ("adv_msl_nonuniform", 1e-12),
+    ("sweep_bg_material", 1e-12), ("sweep_exc_disabled", 1e-12), ("sweep_fdtd_odd", 1e-12),
+    ("sweep_fdtd_ts_and_steps0", 1e-12), ("sweep_grid_deltaunit_m", 1e-12), ("sweep_mat_aniso", 1e-12),
+    ("sweep_mat_aniso_single", 1e-12), ("sweep_mat_aniso_two", 1e-12), ("sweep_mat_mue_sigma", 1e-12),
+    ("sweep_prio_metal_in_mat", 1e-12), ("sweep_prio_overlap", 1e-12), ("sweep_probe_e_box", 1e-12),
+    ("sweep_probe_fd", 1e-12), ("sweep_probe_times", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -78,10 +79,10 @@ def probe_diff(a_text, b_text, dt):
     return math.sqrt(num) if den == 0.0 else math.sqrt(num / den)
 
 
-def run_case(case):
+def run_case(case, curl_order=1):
     s = OE.load(os.path.join(FIXTURES, case, "model.xml"))
     o = OracleEngine(s.model, threads=1)
-    return s, s.run(o)
+    return s, s.run(o, curl_order)
 
 
 @have
@@ -123,6 +124,18 @@ def test_fixture(case, tol):
             tk = (k + offset) * s.dt
             assert abs(t - tk) <= 1e-5 * max(tk, s.dt) and abs(tg - t) <= 1e-5 * max(tk, s.dt)
             assert abs(vg - v) <= 2e-5 * max(peak, 1e-30) + 1e-6 * abs(v), (name, k, vg, v)
+
+
+@have
+@pytest.mark.parametrize("case", ["gauss_soft_e", "pmc_mur", "sweep_mat_mue_sigma", "sweep_probe_fd"])
+def test_fixture_in_default_curl_order(case):
+    """The engine's default summation order: round-off away from openEMS."""
+    s, r = run_case(case, curl_order=0)
+    d = os.path.join(FIXTURES, case)
+    files = r.files()
+    keep = meta(case, "keep") or sorted(set(os.listdir(d)) - NOT_PROBES)
+    worst = max(probe_diff(open(os.path.join(d, n)).read(), files[n], s.dt) for n in keep)
+    assert 0.0 < worst < 2.5e-4, worst
 
 
 @have
