@@ -31,13 +31,13 @@ Restated from the reference:
   (openEMS's snapping, entry order and f32 sum), native E and H field
   components; openEMS's skip rules; time-domain files every
   ⌊N/OverSampling⌋ steps (N the Nyquist interval), ``FD_Samples`` files,
-  H-type files with the sample after the last step.
+  H-type files with the sample after the last step;
+* the end criterion: openEMS's energy measure checked every Nyquist
+  interval and after half a Gaussian's length (src/sim/mod.rs:892-930).
 
 Not restated: csx's general discretisation (primitives other than boxes,
 weighting functions, transformations), PML, dispersive materials, lumped
-elements, dumps, cylindrical grids, the openEMS energy measure for
-``endCriteria`` (runs go to their step limit; refused where a criterion
-above 1e-30 could stop them), probe time windows.
+elements, dumps, cylindrical grids.
 """
 from __future__ import annotations
 
@@ -515,10 +515,9 @@ class Setup:
         if f.max_time is not None and f.max_time > 0:
             steps = min(steps, int(math.floor(f.max_time / dt)))
         self.steps = steps
-        if f.end_criteria is not None and f.end_criteria > 1e-30 and \
-                (any(k == MUR_FACE for k, _ in f.faces) or self._lossy()):
-            raise NotImplementedError("energy end criteria (openEMS's measure) in a model that loses energy")
+        self.criterion = f.end_criteria
         self.model = m
+        self.h_sources = []
         self.excited = self._excitation_edges()
         self._mur(m)
         self._excitations(m)
@@ -716,6 +715,8 @@ class Setup:
                 tau = t_of(s) - shift
                 amp[s] = 0.0 if tau < -0.25 * dt else f.signal.value(tau, dt)
             m.add_source_table(kind, edges, amp)
+            if typ in (2, 3):
+                self.h_sources.append((typ == 3, edges, amp.astype(np.float32)))
 
     def _probes(self, m):
         from . import CURRENT, VOLTAGE
@@ -820,21 +821,105 @@ class Setup:
                 self.probes.append(ProbeSpec(p.name, "efield" if e else "hfield", ks, loc, p.fd, os_, *window))
 
     # -- running and output
+    def energy(self, engine, step: int, curl_order: int = 1) -> float:
+        """openEMS's energy measure of the engine's state
+        (EnergyMeasure::OpenEms, src/engine/run.rs:66-76, kernel.rs:364-414,
+        dump.rs:1735-1785): ε0·Σu² over the E edges but those on the three
+        upper faces, plus μ0·Σ w·h² over the H dual edges with h the next H
+        update evaluated from the state (the H sources of the next step
+        included) and w = 4 on the outer planes normal to the edge."""
+        n = self.nodes
+        u = [engine.field(0, a).astype(np.float32) for a in range(3)]
+        i = [engine.field(1, a).astype(np.float32) for a in range(3)]
+        co = [self.model.coeff(lane) for lane in range(12)]
+        we = sum(float(np.sum(np.square(u[a][:-1, :-1, :-1].astype(np.float64)))) for a in range(3))
+        tiny = np.float32(np.finfo(np.float32).tiny)
+
+        def fl(x):
+            return np.where(np.abs(x) < tiny, np.float32(0.0), x).astype(np.float32)
+
+        def upd(da, h, db, a, b, c, d):
+            if curl_order:
+                curl = fl(fl(fl(a - b) + d) - c)
+                return fl(fl(da * h) - fl(db * curl))
+            return fl(da * h - db * ((a - b) - (c - d)))
+
+        z = np.zeros_like(u[0])
+        sh = lambda x, ax: np.concatenate([x.take(range(1, x.shape[ax]), axis=ax),  # noqa: E731
+                                           z.take([0], axis=ax)], axis=ax)
+        hn = [upd(co[6], i[0], co[9], sh(u[2], 1), u[2], sh(u[1], 2), u[1]),
+              upd(co[7], i[1], co[10], sh(u[0], 2), u[0], sh(u[2], 0), u[2]),
+              upd(co[8], i[2], co[11], sh(u[1], 0), u[1], sh(u[0], 1), u[0])]
+        for hard, edges, amp in self.h_sources:
+            a_ = amp[step] if step < len(amp) else np.float32(0.0)
+            for ax, node, w in edges:
+                v = np.float32(np.float32(w) * a_)
+                hn[ax][node] = v if hard else np.float32(hn[ax][node] + v)
+        valid = [(slice(None), slice(0, n[1] - 1), slice(0, n[2] - 1)),
+                 (slice(0, n[0] - 1), slice(None), slice(0, n[2] - 1)),
+                 (slice(0, n[0] - 1), slice(0, n[1] - 1), slice(None))]
+        wh = 0.0
+        for a in range(3):
+            x = hn[a].astype(np.float64) ** 2
+            wgt = np.ones(n[a])
+            wgt[0] = wgt[-1] = 4.0
+            shape = [1, 1, 1]
+            shape[a] = n[a]
+            wh += float(np.sum((x * wgt.reshape(shape))[valid[a]]))
+        from . import eps0, mu0
+        return eps0() * we + mu0() * wh
+
+    def _drive(self, engine, curl_order) -> int:
+        """The reference's run loop for files (src/engine/run.rs:424-540
+        with check_after_interval, src/sim/mod.rs:910-930): openEMS's energy
+        measure every Nyquist interval and once after half the Gaussian's
+        length; stops when it falls below endCriteria times its maximum."""
+        k = self.file.signal.nyquist_interval(self.dt)
+        extra = None
+        if self.file.signal.kind == 0:
+            extra = self.file.signal.length(self.dt, self.steps) // 2
+        steps, w_max = 0, 0.0
+        self.stopped, self.last_ratio_db = False, None
+        while steps < self.steps:
+            regular = (steps // k + 1) * k
+            nxt = extra if (extra is not None and steps < extra < regular) else regular
+            nxt = min(nxt, self.steps)
+            engine.run(nxt - steps)
+            steps = nxt
+            if steps % k and steps != extra:
+                continue
+            w = self.energy(engine, steps, curl_order)
+            w_max = max(w_max, w)
+            if not math.isfinite(w) or w < -1e-12 * w_max:
+                self.warnings.append("diverged")
+                break
+            self.last_ratio_db = 10.0 * math.log10(w / w_max) if w > 0.0 and w_max > 0.0 else -math.inf
+            if w_max > 0.0 and w / w_max < self.criterion:
+                self.stopped = True
+                break
+        return steps
+
     def run(self, engine, curl_order: int = 1) -> "Results":
-        """Runs ``engine`` (built on ``self.model``) for the run length plus
-        one step, whose H update gives the H-type probes' sample after the
-        last step, and collects the probe series. ``curl_order`` 1 sums the
-        curl in openEMS's order, as the reference does for files (its
-        fields then equal openEMS's where the coefficients do), 0 in the
-        engine's default order."""
+        """Runs ``engine`` (built on ``self.model``) to the end criterion or
+        the run length, then one step more, whose H update gives the H-type
+        probes' sample after the last step, and collects the probe series.
+        ``curl_order`` 1 sums the curl in openEMS's order, as the reference
+        does for files (its fields then equal openEMS's where the
+        coefficients do), 0 in the engine's default order."""
         engine.set_curl_order(curl_order)
-        engine.run(self.steps + 1)
+        if self.criterion is None:
+            engine.run(self.steps + 1)
+            self.steps_run = self.steps
+        else:
+            self.steps_run = self._drive(engine, curl_order)
+            engine.run(1)
+        n = self.steps_run
         series = {}
         for p in self.probes:
             cols = [np.asarray(engine.samples(k)) for k in p.ops]
             v = np.stack(cols, axis=1)
             magnetic = p.kind in PF.MAGNETIC
-            series[p.name] = v[: self.steps + 1] if magnetic else v[: self.steps]
+            series[p.name] = v[: n + 1] if magnetic else v[:n]
         return Results(self, series)
 
 
