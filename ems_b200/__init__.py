@@ -199,6 +199,8 @@ def host_lib() -> C.CDLL:
             "ems_dispersive_free": (None, [p]),
             "ems_dispersive_fill": (i, [p, p, p, i, sz, p, p, p, p]),
             "ems_model_add_dispersive": (i, [p, p, i]),
+            "ems_dispersive_add_edge": (i, [p, i, i, p, i, d, d, d]),
+            "ems_model_edge_material": (i, [p, i, i, p, p]),
             "ems_waveform_value": (d, [i, d, d, d, d]),
             "ems_waveform_duration": (d, [i, d, d]),
             "ems_model_add_lumped_port": (i, [p, i, p, p, d, i, d, d, d, u]),
@@ -366,6 +368,14 @@ class Dispersive:
         r = self._lib.ems_dispersive_fill(self._p, model._p, cells._p, field, n, kinds,
                                           _f64([p.p1 for p in poles]), _f64([p.p2 for p in poles]),
                                           _f64([p.p3 for p in poles]))
+        if r != 0:
+            raise ValueError("invalid dispersive pole")
+        return self
+
+    def add_edge(self, field: int, axis: int, node: Sequence[int], pole: "Pole") -> "Dispersive":
+        """One full (unscaled) pole on the E edge (field 0) or H dual edge
+        (field 1) along ``axis`` at ``node``."""
+        r = self._lib.ems_dispersive_add_edge(self._p, field, axis, _u64(node), pole.kind, pole.p1, pole.p2, pole.p3)
         if r != 0:
             raise ValueError("invalid dispersive pole")
         return self
@@ -599,6 +609,14 @@ class Model:
         if not p:
             raise ValueError("model not built")
         return p
+
+    def edge_material(self, field: int, axis: int, node: Sequence[int]) -> tuple[float, float]:
+        """(eps_r, kappa) of an E edge (field 0) or (mu_r, sigma_m) of an H
+        dual edge (field 1), averaged over its cells (EdgeMaterials)."""
+        out = (C.c_double * 2)()
+        if self._lib.ems_model_edge_material(self._p, field, axis, _u64(node), out) != 0:
+            raise ValueError("edge outside the grid")
+        return out[0], out[1]
 
     def mur_table(self, op: int) -> dict:
         """The Mur operator ``op``'s entries as handed to the engine (copies):

@@ -978,6 +978,26 @@ int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset
     return EMS_OK;
 }
 
+int ems_dispersive_add_edge(ems_dispersive* d, int field, int axis, const uint64_t node[3], int kind, double p1,
+                            double p2, double p3) {
+    if ((field != 0 && field != 1) || axis < 0 || axis > 2 || kind < 0 || kind > 2) return EMS_ERR_INVALID;
+    const double v[3] = {p1, p2, kind == 0 ? p3 : 0.0};
+    for (double x : v)
+        if (!(std::isfinite(x) && x >= 0.0)) return EMS_ERR_INVALID;
+    if (p1 == 0.0) return EMS_OK;  // Pole::is_null
+    d->entries.push_back(Entry{field, axis, {node[0], node[1], node[2]}, Pole{kind, p1, p2, p3}});
+    return EMS_OK;
+}
+
+int ems_model_edge_material(const ems_model* m, int field, int axis, const uint64_t node[3], double out[2]) {
+    if ((field != 0 && field != 1) || axis < 0 || axis > 2) return EMS_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (node[a] >= m->n[a]) return EMS_ERR_INVALID;
+    if (field == 0) edge_eps(m, axis, node, out[0], out[1]);
+    else edge_mu(m, axis, node, out[0], out[1]);
+    return EMS_OK;
+}
+
 int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
     if (!m->built) return set_err(m, "build the model first"), -1;
     for (const Entry& e : d->entries) {

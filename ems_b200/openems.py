@@ -25,6 +25,8 @@ Restated from the reference:
   first-order Mur faces (openEMS's options, the hold of faces that carry an
   E excitation, src/compile/mod.rs:1439-1476);
 * isotropic or anisotropic materials and metal on box primitives;
+  Lorentz, Drude and Debye materials as per-edge leapfrog poles with
+  openEMS's edge rule (src/compile/dispersive.rs:1-130);
 * E and H excitations (soft, hard) with ``Excite`` and ``Delay``;
 * probes (src/sim/map.rs:1150-1380, 1683-1870): voltage along the
   staircase path, current around a loop in the nearest dual plane
@@ -36,8 +38,9 @@ Restated from the reference:
   interval and after half a Gaussian's length (src/sim/mod.rs:892-930).
 
 Not restated: csx's general discretisation (primitives other than boxes,
-weighting functions, transformations), PML, dispersive materials, lumped
-elements, dumps, cylindrical grids.
+weighting functions, transformations), PML, openEMS's f32 pole arithmetic,
+Mur faces with dispersive media, lumped elements, dumps, cylindrical
+grids.
 """
 from __future__ import annotations
 
@@ -55,6 +58,7 @@ C0 = 299792458.0
 TWO_PI = 2.0 * math.pi
 FACE_NAMES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
 PEC_FACE, PMC_FACE, MUR_FACE = 0, 1, 2
+MATERIALS = ("Material", "LorentzMaterial", "DebyeMaterial")
 
 
 # ---------------------------------------------------------------------------
@@ -350,7 +354,7 @@ def parse(text: str) -> OpenEmsFile:
             p1, p2 = b.find("P1"), b.find("P2")
             boxes.append(Box(tuple(float(p1.get(c)) for c in "XYZ"), tuple(float(p2.get(c)) for c in "XYZ"),
                              int(float(b.get("Priority", "0")))))
-        if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox"):
+        if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial"):
             raise NotImplementedError(f"property {el.tag}")
         if el.tag == "ProbeBox" and len(boxes) > 1:
             raise NotImplementedError(f"probe {el.get('Name')!r} with several primitives")
@@ -510,6 +514,7 @@ class Setup:
             dt = period / (math.floor(period / dt) + 1.0)
         m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
         self.dt = dt
+        self._dispersive(m)
         self._pmc_half_cell(m)
         steps = f.max_steps
         if f.max_time is not None and f.max_time > 0:
@@ -531,7 +536,7 @@ class Setup:
 
     def _materials(self, m):
         f = self.file
-        mats = [p for p in f.props if p.kind in ("Material", "Metal")]
+        mats = [p for p in f.props if p.kind in ("Metal",) + MATERIALS]
         # Paint in priority order; at equal priority the property defined
         # first wins (it is painted last).
         items = []
@@ -551,7 +556,7 @@ class Setup:
                 # Edges whose midpoint lies in the closed box, unless a
                 # material of higher priority (or of equal priority defined
                 # earlier) holds the midpoint too.
-                over = [(ob, op) for (_, _, op, ob) in items if op.kind == "Material" and
+                over = [(ob, op) for (_, _, op, ob) in items if op.kind in MATERIALS and
                         (ob.priority > b.priority or (ob.priority == b.priority and op.order < p.order))]
                 for a in range(3):
                     rng = []
@@ -584,6 +589,107 @@ class Setup:
             cs = m.cells().box([c[0] for c in cells], [c[-1] + 1 for c in cells])
             m.fill(cs, mat)
 
+    def _winner(self, pt):
+        """The property holding point ``pt`` (drawing units) by openEMS's
+        priority (closed bounds; at equal priority the one defined first),
+        among materials and metal; None for the background."""
+        best = None
+        for p in self.file.props:
+            if p.kind not in MATERIALS + ("Metal",):
+                continue
+            for b in p.boxes:
+                if all(self._inside(q, pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
+                    key = (b.priority, -p.order)
+                    if best is None or key > best[0]:
+                        best = (key, p)
+        return best[1] if best else None
+
+    def _dispersive(self, m):
+        """Lorentz, Drude and Debye poles the openEMS way (src/compile/
+        dispersive.rs:1-130): every E edge (H dual edge) gets the full poles
+        of the dispersive property winning at its midpoint (the centre of
+        the face it pierces), ω_p = 2π·f_plasma·√ε_e with the edge's own
+        averaged static ε_e (μ_e), ω_0 = 2π·f_Lor, γ = 1/τ; Debye Δε, τ as
+        given, dropped below three time steps; integrated with the leapfrog
+        scheme."""
+        from . import LEAPFROG, Dispersive, Pole
+        f = self.file
+        disp = [p for p in f.props if p.kind in ("LorentzMaterial", "DebyeMaterial")]
+        if not disp:
+            return
+        if any(k == MUR_FACE for k, _ in f.faces):
+            raise NotImplementedError("Mur faces with dispersive materials (openEMS's Mur reads before the poles)")
+        lines, n = f.lines, self.nodes
+        co = [m.coeff(lane) for lane in (3, 4, 5, 9, 10, 11)]
+        d = Dispersive()
+        count = 0
+        for field_ in (0, 1):
+            for a in range(3):
+                b, c = (a + 1) % 3, (a + 2) % 3
+                # Candidate nodes: inside the dispersive boxes' bounding box.
+                lo = [min(min(bx.p1[q], bx.p2[q]) for p in disp for bx in p.boxes) for q in range(3)]
+                hi = [max(max(bx.p1[q], bx.p2[q]) for p in disp for bx in p.boxes) for q in range(3)]
+                rng = []
+                for q in range(3):
+                    along = (q == a) == (field_ == 0)
+                    last = n[q] - 1 if along else n[q]
+                    rng.append([i for i in range(last)
+                                if (along and lines[q][i + 1] >= lo[q] - 1e-9 and lines[q][i] <= hi[q] + 1e-9)
+                                or (not along and lo[q] - 1e-9 <= lines[q][i] <= hi[q] + 1e-9)
+                                or (not along and field_ == 1 and False)])
+                if field_ == 1:
+                    # H dual edge along a through node: midpoint at the node
+                    # line along a, cell centres across.
+                    rng = [([i for i in range(n[q]) if lo[q] - 1e-9 <= lines[q][i] <= hi[q] + 1e-9] if q == a else
+                            [i for i in range(n[q] - 1) if lines[q][i + 1] >= lo[q] - 1e-9 and lines[q][i] <= hi[q] + 1e-9])
+                           for q in range(3)]
+                for i in rng[0]:
+                    for j in rng[1]:
+                        for k in rng[2]:
+                            node = (i, j, k)
+                            if field_ == 0:
+                                if node[a] + 1 >= n[a] or co[a][node] == 0.0:
+                                    continue
+                                pt = [0.5 * (lines[q][node[q]] + lines[q][node[q] + 1]) if q == a else lines[q][node[q]]
+                                      for q in range(3)]
+                            else:
+                                if node[b] + 1 >= n[b] or node[c] + 1 >= n[c] or co[3 + a][node] == 0.0:
+                                    continue
+                                pt = [lines[q][node[q]] if q == a else 0.5 * (lines[q][node[q]] + lines[q][node[q] + 1])
+                                      for q in range(3)]
+                            w = self._winner(pt)
+                            if w is None or w.kind not in ("LorentzMaterial", "DebyeMaterial"):
+                                continue
+                            inf = m.edge_material(field_, a, node)[0]
+                            for pole in self._poles(w, field_, a, inf):
+                                d.add_edge(field_, a, node, pole)
+                                count += 1
+        if count:
+            m.add_dispersive(d, LEAPFROG)
+
+    def _poles(self, p, field_, a, inf):
+        from . import Pole
+        iso = p.attrs.get("Isotropy", "1") != "0"
+        order = int(float(p.attrs.get("Order", "1")))
+        pre = "Epsilon" if field_ == 0 else "Mue"
+        out = []
+        for q in range(1, order + 1):
+            get = lambda name: _vec3(p.prop.get(f"{pre}{name}_{q}"), 0.0, iso)[a]  # noqa: E731
+            if p.kind == "DebyeMaterial":
+                if field_ == 1:
+                    continue
+                de, tau = get("Delta"), get("RelaxTime")
+                if de != 0.0 and tau >= 3.0 * self.dt:
+                    out.append(Pole.debye(de, tau))
+                continue
+            fp, fl, tau = get("PlasmaFrequency"), get("LorPoleFrequency"), get("RelaxTime")
+            gamma = 1.0 / tau if tau > 0.0 else 0.0
+            wp = TWO_PI * fp * math.sqrt(max(inf, 0.0))
+            if wp == 0.0:
+                continue
+            out.append(Pole.drude(wp, gamma) if fl == 0.0 else Pole.lorentz(wp, TWO_PI * fl, gamma))
+        return out
+
     @staticmethod
     def _material(m, prop, isotropic=True):
         eps = _vec3(prop.get("Epsilon"), 1.0, isotropic)
@@ -594,7 +700,7 @@ class Setup:
 
     def _lossy(self):
         f = self.file
-        props = [p.prop for p in f.props if p.kind == "Material"] + ([f.background] if f.background else [])
+        props = [p.prop for p in f.props if p.kind in MATERIALS] + ([f.background] if f.background else [])
         return any(any(float(x) != 0.0 for x in (pr.get(k) or "0").split(","))
                    for pr in props for k in ("Kappa", "Sigma"))
 

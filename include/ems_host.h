@@ -111,6 +111,16 @@ void ems_dispersive_free(ems_dispersive* d);
  * of its averaging volume inside (Dispersive::fill_cells). */
 int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset* s, int field, size_t n_poles,
                         const int* kind, const double* p1, const double* p2, const double* p3);
+/* Adds one pole of `kind` (parameters as for ems_dispersive_fill), unscaled,
+ * to the E edge (field 0) or H dual edge (field 1) along `axis` at `node`
+ * (Dispersive::push of an EdgePole, src/engine/dispersive.rs:474-507): the
+ * openEMS files' rule of full poles per edge. */
+int ems_dispersive_add_edge(ems_dispersive* d, int field, int axis, const uint64_t node[3], int kind, double p1,
+                            double p2, double p3);
+/* The averaged static material of the E edge (field 0: eps_r, kappa) or H
+ * dual edge (field 1: mu_r, sigma_m) along `axis` at `node`
+ * (EdgeMaterials::from_cells, src/engine/edge_material.rs:376-413). */
+int ems_model_edge_material(const ems_model* m, int field, int axis, const uint64_t node[3], double out[2]);
 /* Installs the medium with scheme 0 trapezoidal / 1 leapfrog; op index. */
 int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme);
 

@@ -2,9 +2,10 @@
 
 Models written for this test in openEMS's XML (graded meshes, PEC, PMC and
 Mur faces, anisotropic lossy materials with magnetic conductivity, metal
-under a higher-priority material, soft and hard E and H excitations with
-every signal type and a delay, voltage, current, E and H field probes with
-FD samples, a time window and a probe oversampling) are set up by
+under a higher-priority material, Lorentz, Drude, magnetic and Debye
+poles, soft and hard E and H excitations with every signal type and a
+delay, voltage, current, E and H field probes with FD samples, a time
+window and a probe oversampling, an energy end criterion) are set up by
 ems_b200/openems.py and run on the CUDA engine (every schedule that can
 run them) and on the oracle: every probe series, every written probe file
 and the final fields agree bit for bit. The oracle itself is checked
@@ -109,6 +110,34 @@ PULSES = f"""<?xml version="1.0" encoding="UTF-8"?>
 """
 
 
+DISP = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="360" endCriteria="1e-4" f_max="10e9">
+    <Excitation Type="0" f0="5e9" fc="4e9"/>
+    <BoundaryCond xmin="PEC" xmax="PEC" ymin="PMC" ymax="PMC" zmin="PEC" zmax="PEC"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <LorentzMaterial Name="lor" Order="2">
+        <Property Epsilon="2" Mue="1.2" EpsilonPlasmaFrequency_1="5e9" EpsilonLorPoleFrequency_1="7e9" EpsilonRelaxTime_1="1e-9"
+                  EpsilonPlasmaFrequency_2="3e9" EpsilonRelaxTime_2="2e-10" MuePlasmaFrequency_2="2e9" MueRelaxTime_2="5e-10"/>
+        <Primitives><Box Priority="1"><P1 X="8" Y="2" Z="2"/><P2 X="12.5" Y="9" Z="8"/></Box></Primitives></LorentzMaterial>
+      <DebyeMaterial Name="deb" Order="1"><Property Epsilon="1.5" EpsilonDelta_1="2" EpsilonRelaxTime_1="3e-11"/>
+        <Primitives><Box Priority="2"><P1 X="11" Y="4" Z="3"/><P2 X="14" Y="7" Z="6"/></Box></Primitives></DebyeMaterial>
+      <Excitation Name="soft" Type="0" Excite="0,0,1"><Primitives><Box Priority="0"><P1 X="4" Y="6" Z="4"/><P2 X="4" Y="6" Z="7"/></Box></Primitives></Excitation>
+      <ProbeBox Name="ut" Type="0"><Primitives><Box Priority="0"><P1 X="10" Y="6" Z="3"/><P2 X="10" Y="6" Z="7"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="it" Type="1" NormDir="0"><Primitives><Box Priority="0"><P1 X="13" Y="3" Z="2"/><P2 X="13" Y="9" Z="8"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -120,10 +149,12 @@ def _both(text, schedule=0):
     return s, g, s.run(g, order), o, s.run(o, order)
 
 
-# Schedules 2 (fused) and 5 (sweep) do not run magnetic sources.
+# Schedules 2 (fused) and 5 (sweep) do not run magnetic sources, 2 not
+# magnetic poles.
 @pytest.mark.parametrize("name,text,schedule", [
     ("box", BOX, 0), ("box", BOX, 1), ("box", BOX, 2), ("box", BOX, 3), ("box", BOX, 5),
-    ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1)])
+    ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1),
+    ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes

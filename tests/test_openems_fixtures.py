@@ -49,6 +49,12 @@ CASES = [
     ("sweep_probe_fd", 1e-12), ("sweep_probe_times", 1e-12), ("end_criteria", 1e-12),
     ("end_criteria_half", 1e-12), ("end_criteria_mur", 1e-12), ("end_criteria_tem", 1e-12),
     ("adv_mur_dielectric", 1e-12),
+    # Dispersive slabs: the engine's own f64 leapfrog poles, where openEMS
+    # runs its f32 pole arithmetic (the reference measured ~1.5e-6 before
+    # restating it; here 5e-7 ... 1.9e-6).
+    ("adv_drude_slab", 3e-6), ("adv_lorentz_slab", 3e-6), ("adv_lorentz2_slab", 3e-6),
+    ("adv_lorentz_mag_slab", 3e-6), ("adv_debye_slab", 3e-6), ("adv_debye2_slab", 3e-6),
+    ("adv_debye_offgrid", 3e-6), ("adv_lorentz_coarse", 3e-6),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -100,13 +106,13 @@ def test_fixture(case, tol):
         assert abs(s.dt / dt_oe - 1.0) < 6e-6
     files = r.files()
     written = set(files)
-    listed = meta(case, "files")
+    listed, keep = meta(case, "files"), meta(case, "keep")
     if listed is not None:  # sweep cases: the files openEMS wrote
         assert written == set(listed), (written, listed)
-        keep = meta(case, "keep")
-    else:
+    elif keep is None:  # core cases: every file openEMS wrote is kept
         keep = sorted(set(os.listdir(d)) - NOT_PROBES)
         assert written == set(keep), (written, keep)
+    assert set(keep) <= written
     worst = 0.0
     for name in keep:
         worst = max(worst, probe_diff(open(os.path.join(d, name)).read(), files[name], s.dt))
@@ -169,7 +175,7 @@ def test_probe_skip_warnings():
 @have
 @pytest.mark.parametrize("case,why", [
     ("nonuniform_materials", "weighting"), ("lumped_port", "LumpedElement"), ("pml", "PML"),
-    ("adv_lorentz_slab", "LorentzMaterial")])
+    ("sweep_exc_sphere", "Sphere")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
         OE.load(os.path.join(FIXTURES, case, "model.xml"))
