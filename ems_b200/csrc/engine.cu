@@ -395,7 +395,9 @@ ems_status build_chunks(ems_gpu* h, uint32_t S) {
         Sd.total = total;
         if (Sd.n_box) {
             Sd.box = h->upload(boxes.data(), boxes.size());
-            if (!Sd.box) return fail(h, EMS_ERR_NOMEM, "CPML shell");
+            const std::vector<uint32_t> win = shell_windows(boxes, total);
+            Sd.first_box = h->upload(win.data(), win.size());
+            if (!Sd.box || !Sd.first_box) return fail(h, EMS_ERR_NOMEM, "CPML shell");
         }
         auto& cb = h->chunk_box[side];
         auto& cn = h->chunk_node[side];

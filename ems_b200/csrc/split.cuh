@@ -17,6 +17,7 @@
 #pragma once
 
 #include "separate.cuh"
+#include <vector>
 
 namespace emsk {
 
@@ -181,7 +182,25 @@ struct ShellDev {
     const ShellBox* box;
     uint32_t n_box, total;  // boxes, and the nodes this launch covers
     uint32_t base;          // the first node of the launch (box starts count from 0)
+    // Per window of kShellWindow nodes (node t in window t / kShellWindow),
+    // the box holding the window's first node; null: binary search.
+    const uint32_t* first_box = nullptr;
 };
+
+constexpr uint32_t kShellWindowLog = 8, kShellWindow = 1u << kShellWindowLog;
+
+// The first_box table of a shell's boxes (sorted by start) covering `total`
+// nodes.
+inline std::vector<uint32_t> shell_windows(const std::vector<ShellBox>& boxes, uint32_t total) {
+    std::vector<uint32_t> w((total + kShellWindow - 1) / kShellWindow + 1, 0);
+    uint32_t q = 0;
+    for (size_t b = 0; b < w.size(); ++b) {
+        const uint64_t t = (uint64_t)b * kShellWindow;
+        while (q + 1 < boxes.size() && boxes[q + 1].start <= t) ++q;
+        w[b] = q;
+    }
+    return w;
+}
 
 // The CPML chain of one field value over the slabs of `list` (count | q…),
 // in order: ψ = flush(b·ψ + a·s), t = flush(t + coef·(k·s + ψ)), with s = sA
@@ -263,11 +282,18 @@ __device__ __forceinline__ void shell_item(const FusedParams& P, const ShellDev&
     const uint32_t t0 = block * (32 * kShellWarps) + tid;
     if (t0 >= S.total) return;
     const uint32_t t = S.base + t0;
-    uint32_t lo = 0, hi = S.n_box;  // box[lo].start <= t < box[hi].start
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(&S.box[mid].start) <= t) lo = mid;
-        else hi = mid;
+    uint32_t lo = 0;  // box[lo].start <= t < box[lo + 1].start
+    if (S.first_box) {
+        // The window's first box, then forward (a window spans few boxes).
+        lo = __ldg(&S.first_box[t >> kShellWindowLog]);
+        while (lo + 1 < S.n_box && __ldg(&S.box[lo + 1].start) <= t) ++lo;
+    } else {
+        uint32_t hi = S.n_box;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(&S.box[mid].start) <= t) lo = mid;
+            else hi = mid;
+        }
     }
     const ShellBox& Bx = S.box[lo];
     const uint32_t local = t - Bx.start;
@@ -301,20 +327,27 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
                                            const double* sets, const uint32_t* run_of, int electric, double dt,
                                            int save_prev, uint32_t e) {
     if (e >= p.n_edges) return;
-    const PoleRun R = runs[run_of[e]];
-    const uint32_t p0 = R.p0 + (e - R.e0) * R.np;
-    const int ax = (int)R.axis;
-    const uint32_t idx = R.node0 + (e - R.e0);
-    float* fld = electric ? f.u[ax] : f.i[ax];
-    const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
+    // The edge's own tables first (independent of each other, so their
+    // latencies overlap): its run, node, axis, first pole and saved value;
+    // then the field, its coefficient and the first pole's state, which
+    // need only those. The run (shared by many edges, from L1) gives the
+    // pole count and constants.
+    const uint32_t r = __ldg(run_of + e);
+    const uint32_t idx = __ldg(p.node + e);
+    const int ax = (int)__ldg(p.axis + e);
+    const uint32_t p0 = e ? __ldg(p.pole_end + e - 1) : 0u;
     const double prev = (double)p.prev[e];
-    const double half_prev = __dmul_rn(0.5, prev);
+    float* fld = electric ? f.u[ax] : f.i[ax];
     const double u_star = (double)fld[idx];
+    const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
+    const double j0 = p.j[p0], q0 = p.q[p0];
+    const PoleRun R = runs[r];
+    const double half_prev = __dmul_rn(0.5, prev);
     const double* cs = sets + R.set;
     double s = 0.0;
     for (uint32_t q = 0; q < R.np; ++q) {
         const double a = cs[3 * q], ic = cs[3 * q + 1], iz = cs[3 * q + 2];
-        const double jq = p.j[p0 + q], qq = p.q[p0 + q];
+        const double jq = q ? p.j[p0 + q] : j0, qq = q ? p.q[p0 + q] : q0;
         if ((R.kinds >> q) & 1u) {
             const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
             p.j[p0 + q] = jn;

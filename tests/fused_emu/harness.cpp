@@ -427,11 +427,13 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
         P.io[a] = P.in[a] = buf[3 + a].data();
     }
     std::vector<ShellBox> st[2];
+    std::vector<uint32_t> win[2];
     ShellDev sd[2];
     for (int side = 0; side < 2; ++side) {
         uint32_t total = 0;
         st[side] = shell_boxes(T, d->nodes, side, &total);
-        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u};
+        win[side] = shell_windows(st[side], total);
+        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u, win[side].data()};
     }
     const unsigned gx = split_blocks_x(g);
     std::vector<double> partials((size_t)gx * g.nx, 0.0);
