@@ -63,6 +63,13 @@ class FreqDumpSpec(C.Structure):
     ]
 
 
+class TimeDumpSpec(C.Structure):
+    """``ems_time_dump`` (include/ems_gpu.h)."""
+
+    _fields_ = [("field", C.c_int32), ("lo", C.c_uint64 * 3), ("hi", C.c_uint64 * 3), ("stride", C.c_uint64 * 3),
+                ("inv_len", C.c_void_p * 3), ("interval", C.c_uint64)]
+
+
 class EngineDesc(C.Structure):
     _fields_ = [
         ("nodes", C.c_uint64 * 3),
@@ -238,6 +245,9 @@ GPU_SYMBOLS = {
     "ems_gpu_launch_count": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_set_curl_order": (C.c_int, [C.c_void_p, C.c_int]),
+    "ems_gpu_time_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ems_gpu_time_dump_count": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),
+    "ems_gpu_time_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_energy_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -731,6 +741,36 @@ class Engine:
         self._dumps = getattr(self, "_dumps", {})
         self._dumps[i.value] = (dims, len(fr))
         return i.value
+
+    def add_time_dump(self, field: int, lo, hi, stride=(1, 1, 1), interval: int = 1) -> int:
+        """Time-domain snapshots of E (field 0) or H (field 1) over the node
+        box lo..hi every ``interval`` states, kept on the device
+        (``ems_gpu_time_dump_add``). Returns the dump id."""
+        m = self._model
+        inv = [m.inv_edge_lengths(a, dual=field == 1) for a in range(3)]
+        spec = TimeDumpSpec(field, (C.c_uint64 * 3)(*lo), (C.c_uint64 * 3)(*hi), (C.c_uint64 * 3)(*stride),
+                            (C.c_void_p * 3)(*[x.ctypes.data for x in inv]), interval)
+        self._inv_keep = getattr(self, "_inv_keep", []) + [inv]
+        i = C.c_size_t()
+        self._ck(self._lib.ems_gpu_time_dump_add(self._h, C.byref(spec), C.byref(i)))
+        self._tdumps = getattr(self, "_tdumps", {})
+        self._tdumps[i.value] = [(hi[a] - lo[a]) // stride[a] + 1 for a in range(3)]
+        return i.value
+
+    def time_dump(self, dump: int) -> tuple[np.ndarray, np.ndarray]:
+        """(states, values): the state m of every snapshot and the values,
+        shape (snapshots, nx, ny, nz, 3)."""
+        dims = self._tdumps[dump]
+        n = C.c_size_t()
+        self._ck(self._lib.ems_gpu_time_dump_count(self._h, dump, C.byref(n)))
+        pts = int(np.prod(dims))
+        vals = np.empty((n.value, pts * 3), dtype=np.float64)
+        states = np.empty(n.value, dtype=np.uint64)
+        st = C.c_uint64()
+        for k in range(n.value):
+            self._ck(self._lib.ems_gpu_time_dump_read(self._h, dump, k, vals[k].ctypes.data, pts * 3, C.byref(st)))
+            states[k] = st.value
+        return states, vals.reshape(n.value, *dims, 3)
 
     def freq_dump(self, dump: int, k: int) -> np.ndarray:
         """The transform at frequency index k: complex (nx, ny, nz, 3)."""

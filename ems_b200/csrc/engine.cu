@@ -133,6 +133,18 @@ struct ems_gpu {
         bool started = false;
     };
     std::vector<FreqDump> dumps;
+    // Time-domain snapshots (ems_gpu_time_dump_add): the sampled states
+    // stored one after another on the device.
+    struct TimeDump {
+        DumpDev d;
+        int field = 0;
+        uint64_t interval = 1;
+        bool started = false;
+        double* buf = nullptr;
+        size_t used = 0, cap = 0;     // doubles
+        std::vector<uint64_t> states; // the state m of each snapshot
+    };
+    std::vector<TimeDump> tdumps;
     // ---- the fused single-pass schedule
     bool fused_ok = false;
     bool tables_ok = false;         // the table-driven two-kernel schedule can run
@@ -1377,7 +1389,21 @@ static ems_status tune_step(ems_gpu* h) {
 }
 
 // Samples state m (the state after m steps) into every dump that is due.
-static void dumps_sample(ems_gpu* h, uint64_t m, bool first) {
+static ems_status dumps_sample(ems_gpu* h, uint64_t m, bool first) {
+    for (auto& T : h->tdumps) {
+        if (first == T.started) continue;
+        T.started = true;
+        if (m % T.interval) continue;
+        const size_t n = (size_t)T.d.npts * 3;
+        ems_status st = grow(h, &T.buf, T.used, &T.cap, T.used + n);
+        if (st) return st;
+        DumpDev d = T.d;
+        for (int a = 0; a < 3; ++a) d.f[a] = T.field ? h->i[a] : h->u[a];
+        k_snapshot<<<blocks_for(d.npts, 256), 256, 0, h->stream>>>(d, T.buf + T.used);
+        ++h->launches;
+        T.used += n;
+        T.states.push_back(m);
+    }
     for (auto& D : h->dumps) {
         if (first == D.started) continue;
         D.started = true;
@@ -1387,17 +1413,19 @@ static void dumps_sample(ems_gpu* h, uint64_t m, bool first) {
         k_dump<<<blocks_for(d.npts, 256), 256, 0, h->stream>>>(d, (double)m);
         ++h->launches;
     }
+    return EMS_OK;
 }
 
 // One step with the dumps: the first sample of a new dump is the state the
 // step starts from (src/engine/dump.rs Cursor::pre_h), then the state after
 // every step (Cursor::post_e).
 static ems_status step_dumped(ems_gpu* h, bool energy) {
-    if (!h->dumps.empty()) dumps_sample(h, h->step, true);
-    ems_status st = (!energy && h->tune.active) ? tune_step(h) : run_step(h, energy);
+    const bool any = !h->dumps.empty() || !h->tdumps.empty();
+    ems_status st = any ? dumps_sample(h, h->step, true) : EMS_OK;
     if (st) return st;
-    if (!h->dumps.empty()) dumps_sample(h, h->step, false);
-    return EMS_OK;
+    st = (!energy && h->tune.active) ? tune_step(h) : run_step(h, energy);
+    if (st) return st;
+    return any ? dumps_sample(h, h->step, false) : EMS_OK;
 }
 
 ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
@@ -1444,6 +1472,56 @@ ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* 
     h->dumps.push_back(D);
     *id = h->dumps.size() - 1;
     return check(h, cudaStreamSynchronize(h->stream), "dump");
+}
+
+ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* id) {
+    if (!h || !spec || !id || spec->field < 0 || spec->field > 1) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    const Grid& g = h->g;
+    const uint32_t nn[3] = {g.nx, g.ny, g.nz};
+    ems_gpu::TimeDump T;
+    DumpDev& d = T.d;
+    d = DumpDev{};
+    uint64_t npts = 1;
+    for (int a = 0; a < 3; ++a) {
+        const uint64_t st = spec->stride[a] ? spec->stride[a] : 1;
+        if (spec->lo[a] > spec->hi[a] || spec->hi[a] >= nn[a] || !spec->inv_len[a]) return EMS_ERR_INVALID;
+        d.lo[a] = (uint32_t)spec->lo[a];
+        d.st[a] = (uint32_t)st;
+        d.n[a] = (uint32_t)((spec->hi[a] - spec->lo[a]) / st + 1);
+        npts *= d.n[a];
+        d.inv_len[a] = h->upload(spec->inv_len[a], nn[a]);
+        if (!d.inv_len[a]) return fail(h, EMS_ERR_NOMEM, "time dump");
+    }
+    if (npts >= (1ull << 31)) return fail(h, EMS_ERR_INVALID, "time dump too large");
+    d.pitch = g.pitch;
+    d.ny = g.ny;
+    d.npts = (uint32_t)npts;
+    T.field = spec->field;
+    T.interval = spec->interval ? spec->interval : 1;
+    h->tdumps.push_back(std::move(T));
+    *id = h->tdumps.size() - 1;
+    return check(h, cudaStreamSynchronize(h->stream), "time dump");
+}
+
+ems_status ems_gpu_time_dump_count(const ems_gpu* h, size_t id, size_t* n) {
+    if (!h || !n || id >= h->tdumps.size()) return EMS_ERR_INVALID;
+    *n = h->tdumps[id].states.size();
+    return EMS_OK;
+}
+
+ems_status ems_gpu_time_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap, uint64_t* state) {
+    if (!h || !out || id >= h->tdumps.size()) return EMS_ERR_INVALID;
+    const auto& T = h->tdumps[id];
+    const size_t n = (size_t)T.d.npts * 3;
+    if (k >= T.states.size() || cap < n) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (check(h, cudaMemcpyAsync(out, T.buf + k * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+              "time dump read") ||
+        check(h, cudaStreamSynchronize(h->stream), "time dump read"))
+        return EMS_ERR_CUDA;
+    if (state) *state = T.states[k];
+    return EMS_OK;
 }
 
 ems_status ems_gpu_freq_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap) {

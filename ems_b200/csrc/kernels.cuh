@@ -491,6 +491,20 @@ struct DumpDev {
     double* acc;  // [nf][npts][3] complex, re and im interleaved
 };
 
+// Time-domain snapshot (src/engine/dump.rs TimeDump with native positions):
+// the field values E = u/Δ or H = i/Δ* of every point of the box, in f64,
+// into out[p·3 + component].
+__global__ void __launch_bounds__(256) k_snapshot(const __grid_constant__ DumpDev d, double* out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= d.npts) return;
+    const uint32_t iz = p % d.n[2], r = p / d.n[2], iy = r % d.n[1], ix = r / d.n[1];
+    const uint32_t i = d.lo[0] + ix * d.st[0], j = d.lo[1] + iy * d.st[1], k = d.lo[2] + iz * d.st[2];
+    const size_t idx = ((size_t)i * d.ny + j) * d.pitch + k;
+    out[3 * (size_t)p] = __dmul_rn((double)d.f[0][idx], d.inv_len[0][i]);
+    out[3 * (size_t)p + 1] = __dmul_rn((double)d.f[1][idx], d.inv_len[1][j]);
+    out[3 * (size_t)p + 2] = __dmul_rn((double)d.f[2][idx], d.inv_len[2][k]);
+}
+
 __device__ __forceinline__ double frac_toward_zero(double x) { return x - trunc(x); }
 
 __global__ void __launch_bounds__(256) k_dump(const __grid_constant__ DumpDev d, double m) {

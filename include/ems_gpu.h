@@ -358,6 +358,26 @@ typedef struct {
 /* Adds a dump (before or between runs); *id is its index. */
 ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* id);
 
+/* A time-domain dump (TimeDump with native positions, src/engine/dump.rs:
+ * 1-80, Schedule::Every): snapshots of E = u/len or H = i/len* (f64, len
+ * from inv_len as in ems_freq_dump) at the nodes lo + q*stride <= hi of the
+ * box, z fastest, of the states m (the state after m steps: E at m*dt, H
+ * at (m - 1/2)*dt; the first sampled is the state when the dump is added)
+ * with m % interval == 0, kept on the device until read. */
+typedef struct {
+    int32_t field;
+    uint64_t lo[3], hi[3], stride[3];
+    const double* inv_len[3];
+    uint64_t interval;
+} ems_time_dump;
+
+ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* id);
+/* Number of snapshots taken so far. */
+ems_status ems_gpu_time_dump_count(const ems_gpu* h, size_t id, size_t* n);
+/* Snapshot k: 3 values per point (x, y, z components) into out (cap >= 3 *
+ * points); *state (if not NULL) the state m it shows. */
+ems_status ems_gpu_time_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap, uint64_t* state);
+
 /* The transform at frequency index k: 3 complex values (re, im
  * interleaved: 6 doubles) per point, z fastest; cap in doubles. */
 ems_status ems_gpu_freq_dump_read(ems_gpu* h, size_t id, size_t k, double* out, size_t cap);

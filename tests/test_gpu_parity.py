@@ -273,6 +273,44 @@ def test_freq_dump_equals_the_dft_of_the_oracle_states():
         assert np.abs(gh - want_h[q]).max() <= 1e-9 * np.abs(want_h[q]).max()
 
 
+def test_time_dump_equals_the_oracle_states():
+    """Device time-domain dumps (src/engine/dump.rs TimeDump, native values,
+    state timing, every K states): E = u/Δ and H = i/Δ* of the oracle's
+    states m = 0, K, 2K, ... bit for bit, with dumps added before the run
+    and between runs, across buffer growth."""
+    m, _ = small_cavity()
+    g = E.Engine(m)
+    de = g.add_time_dump(0, (1, 1, 1), (8, 6, 5), stride=(2, 1, 2), interval=2)
+    o = OracleEngine(m, threads=2)
+    inv_e = [m.inv_edge_lengths(a) for a in range(3)]
+    inv_h = [m.inv_edge_lengths(a, dual=True) for a in range(3)]
+    ie, je, ke = np.arange(1, 9, 2), np.arange(1, 7), np.arange(1, 6, 2)
+    ih, jh, kh = np.arange(0, 11), np.array([2]), np.arange(0, 7)
+    want_e, want_h = [], []
+    steps = 300
+    for s in range(steps + 1):
+        if s:
+            o.run(1)
+        if s % 2 == 0:
+            u = [o.field(0, a)[np.ix_(ie, je, ke)].astype(np.float64) for a in range(3)]
+            want_e.append(np.stack([u[0] * inv_e[0][ie][:, None, None], u[1] * inv_e[1][je][None, :, None],
+                                    u[2] * inv_e[2][ke][None, None, :]], axis=-1))
+        if s >= 100 and s % 7 == 0:
+            i_ = [o.field(1, a)[np.ix_(ih, jh, kh)].astype(np.float64) for a in range(3)]
+            want_h.append((s, np.stack([i_[0] * inv_h[0][ih][:, None, None], i_[1] * inv_h[1][jh][None, :, None],
+                                        i_[2] * inv_h[2][kh][None, None, :]], axis=-1)))
+    g.run(100)
+    dh = g.add_time_dump(1, (0, 2, 0), (10, 2, 6), interval=7)
+    g.run(steps - 100)
+    se, ve = g.time_dump(de)
+    assert list(se) == list(range(0, steps + 1, 2))
+    assert np.array_equal(ve.view(np.uint64), np.stack(want_e).view(np.uint64))
+    sh, vh = g.time_dump(dh)
+    assert list(sh) == [s for s, _ in want_h]
+    assert np.array_equal(vh.view(np.uint64), np.stack([v for _, v in want_h]).view(np.uint64))
+    assert np.abs(vh).max() > 0
+
+
 @pytest.mark.parametrize("planes", [3, 7, 64])
 def test_sweep_schedule_bit_exact(planes):
     """The sweep schedule (chunks of `planes` x-planes, each chunk's H
