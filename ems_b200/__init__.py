@@ -197,6 +197,7 @@ def host_lib() -> C.CDLL:
             "ems_model_build_bound": (i, [p, d, i]),
             "ems_model_openems_timestep": (d, [p, i]),
             "ems_model_zero_edges": (i, [p, i, i, p, p]),
+            "ems_model_set_edge_circuit": (i, [p, i, p, d, d]),
             "ems_model_dt": (d, [p]),
             "ems_model_courant_limit": (d, [p]),
             "ems_model_coeff": (p, [p, i]),
@@ -494,6 +495,12 @@ class Model:
         if not dt > 0.0:
             raise ValueError(f"unknown time-step method {method}")
         return dt
+
+    def set_edge_circuit(self, axis: int, node: Sequence[int], cap: float = -1.0, cond: float = -1.0) -> "Model":
+        """Replaces an E edge's capacitance and/or conductance (negative:
+        the medium's) after build."""
+        self._check(self._lib.ems_model_set_edge_circuit(self._p, axis, _u64(node), cap, cond), "set_edge_circuit!")
+        return self
 
     def zero_edges(self, field: int, axis: int, lo: Sequence[int], hi: Sequence[int]) -> "Model":
         """Zeroes the coefficients of the E (field 0) or H (1) edges along

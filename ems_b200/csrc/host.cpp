@@ -137,6 +137,7 @@ struct ems_model {
     std::vector<uint8_t> pec[3];
     int faces[6] = {0, 0, 0, 0, 0, 0};
     bool built = false;
+    bool oe_round = false;  // built with openEMS's coefficient rounding
     double dt = 0.0;
     std::vector<float> co[12];
     std::vector<std::unique_ptr<OpStore>> ops;
@@ -576,6 +577,7 @@ int ems_model_build_bound(ems_model* m, double dt, int flags) {
     if (!(std::isfinite(dt) && dt > 0.0)) return set_err(m, "time step must be positive and finite"), EMS_ERR_INVALID;
     if (flags & ~3) return set_err(m, "unknown build flags"), EMS_ERR_INVALID;
     compute_coefficients(m, dt, (flags & 1) != 0, (flags & 2) != 0);
+    m->oe_round = (flags & 1) != 0;
     return EMS_OK;
 }
 
@@ -719,6 +721,32 @@ double ems_model_openems_timestep(const ems_model* m, int method) {
     }
     if (method == 1) return (double)(1.0f / std::sqrt((float)w2max));
     return 1.0 / std::sqrt(w2max);
+}
+
+int ems_model_set_edge_circuit(ems_model* m, int axis, const uint64_t node[3], double cap, double cond) {
+    if (!m->built) return set_err(m, "build the model first"), EMS_ERR_INVALID;
+    if (axis < 0 || axis > 2) return set_err(m, "invalid axis"), EMS_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (node[a] >= m->n[a] || (a == axis && node[a] + 1 >= m->n[a]))
+            return set_err(m, "edge outside the grid"), EMS_ERR_INVALID;
+    // replace_medium (src/sim/map.rs:1525-1606): the element's C and 1/R
+    // replace the medium's, each rounded like the model's circuit values;
+    // e_coefficients (src/engine/coeffs.rs:395-410).
+    const bool oe = m->oe_round;
+    auto store = [oe](double x) { return oe ? (double)(float)x : x; };
+    const int b = next_axis(axis), c = prev_axis(axis);
+    double eps, kap;
+    edge_eps(m, axis, node, eps, kap);
+    const double geo = m->dual_delta(b, node[b]) * m->dual_delta(c, node[c]) / m->delta(axis, node[axis]);
+    const double C = cap >= 0.0 ? store(cap) : store((oe ? OE_EPS0 : EPS0) * eps * geo);
+    const double G = cond >= 0.0 ? store(cond) : store(kap * geo);
+    if (!(C > 0.0 && std::isfinite(C) && G >= 0.0 && std::isfinite(G)))
+        return set_err(m, "edge circuit must have C > 0 and G >= 0"), EMS_ERR_INVALID;
+    const double dt = m->dt, den = C + 0.5 * G * dt;
+    const uint64_t idx = m->index(node[0], node[1], node[2]);
+    m->co[axis][idx] = (float)((C - 0.5 * G * dt) / den);
+    m->co[3 + axis][idx] = (float)(dt / den);
+    return EMS_OK;
 }
 
 int ems_model_zero_edges(ems_model* m, int field, int axis, const uint64_t lo[3], const uint64_t hi[3]) {

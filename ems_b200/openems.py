@@ -354,7 +354,8 @@ def parse(text: str) -> OpenEmsFile:
             p1, p2 = b.find("P1"), b.find("P2")
             boxes.append(Box(tuple(float(p1.get(c)) for c in "XYZ"), tuple(float(p2.get(c)) for c in "XYZ"),
                              int(float(b.get("Priority", "0")))))
-        if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial"):
+        if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
+                          "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
         if el.tag == "ProbeBox" and len(boxes) > 1:
             raise NotImplementedError(f"probe {el.get('Name')!r} with several primitives")
@@ -514,8 +515,9 @@ class Setup:
             dt = period / (math.floor(period / dt) + 1.0)
         m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
         self.dt = dt
-        self._dispersive(m)
         self._pmc_half_cell(m)
+        self._lumped(m)
+        self._dispersive(m)
         steps = f.max_steps
         if f.max_time is not None and f.max_time > 0:
             steps = min(steps, int(math.floor(f.max_time / dt)))
@@ -588,6 +590,75 @@ class Setup:
             mat = self._material(m, p.prop, p.attrs.get("Isotropy", "1") != "0")
             cs = m.cells().box([c[0] for c in cells], [c[-1] + 1 for c in cells])
             m.fill(cs, mat)
+
+    def _lumped(self, m):
+        """Parallel R/C lumped elements the openEMS way (src/sim/map.rs:
+        46-255, 1525-1680): spread like a homogeneous material over their
+        E edges (G_e = g_e·S/R, C_e = g_e·C·S with g_e the edge's dual
+        face over its length, outer lines counting full cells, and
+        S = Σ over positions along the element of 1/Σ g_e), their R and C
+        replacing the medium's conductance and capacitance, and PEC caps
+        on the two end planes (Caps, the default)."""
+        f = self.file
+        n, lines = self.nodes, f.lines
+        for p in f.props:
+            if p.kind != "LumpedElement":
+                continue
+            a = int(float(p.attrs.get("Direction", "0")))
+            r = _f(p.attrs.get("R"))
+            c = _f(p.attrs.get("C"))
+            if p.attrs.get("L") is not None or p.attrs.get("LEtype", "0") not in ("0", "-1"):
+                raise NotImplementedError(f"lumped element {p.name!r}: inductors and series elements")
+            r = r if r is not None and r > 0 and math.isfinite(r) else None
+            c = c if c is not None and c > 0 and math.isfinite(c) else None
+            edges = []
+            for b in p.boxes:
+                lo = [min(b.p1[q], b.p2[q]) for q in range(3)]
+                hi = [max(b.p1[q], b.p2[q]) for q in range(3)]
+                rng = [[i for i in range(n[q] - (1 if q == a else 0))
+                        if self._inside(q, lines[q][i], lo[q], hi[q])
+                        and (q != a or self._inside(q, lines[q][i + 1], lo[q], hi[q]))] for q in range(3)]
+                edges += [(i, j, k) for i in rng[0] for j in rng[1] for k in rng[2]]
+            cb = m.coeff(3 + a)
+            kept = []
+            for e in edges:
+                if cb[e] == 0.0:
+                    self.warnings.append(f"lumped element {p.name!r}: edge {e} is PEC (shorted); ignored")
+                else:
+                    kept.append(e)
+            if not kept or (r is None and c is None):
+                continue
+
+            # openems_edge_geometry (src/sim/map.rs:164-218).
+            def geo(e):
+                area = 1.0
+                for t in range(3):
+                    if t == a:
+                        continue
+                    area *= self.model_dual(t, e[t]) * (2.0 if e[t] in (0, n[t] - 1) else 1.0)
+                return area / self.model_delta(a, e[a])
+
+            w = {e: geo(e) for e in kept}
+            per = {}
+            for e in kept:
+                per[e[a]] = per.get(e[a], 0.0) + w[e]
+            S = sum(1.0 / x for x in per.values())
+            for e in kept:
+                m.set_edge_circuit(a, e, cap=c * w[e] * S if c is not None else -1.0,
+                                   cond=1.0 / (r / (w[e] * S)) if r is not None else -1.0)
+            if p.attrs.get("Caps", "1") != "0":
+                lo = [min(e[q] for e in kept) for q in range(3)]
+                hi = [max(e[q] + (1 if q == a else 0) for e in kept) for q in range(3)]
+                for t in range(3):
+                    if t == a or hi[t] == lo[t]:
+                        continue
+                    o = 3 - a - t
+                    for plane in (lo[a], hi[a]):
+                        blo, bhi = [0, 0, 0], [0, 0, 0]
+                        blo[a] = bhi[a] = plane
+                        blo[t], bhi[t] = lo[t], hi[t] - 1
+                        blo[o], bhi[o] = lo[o], hi[o]
+                        m.zero_edges(0, t, blo, bhi)
 
     def _winner(self, pt):
         """The property holding point ``pt`` (drawing units) by openEMS's
@@ -674,7 +745,13 @@ class Setup:
         pre = "Epsilon" if field_ == 0 else "Mue"
         out = []
         for q in range(1, order + 1):
-            get = lambda name: _vec3(p.prop.get(f"{pre}{name}_{q}"), 0.0, iso)[a]  # noqa: E731
+            def get(name, q=q):
+                # "<name>_<order>", or for the first order also "<name>".
+                v = p.prop.get(f"{pre}{name}_{q}")
+                if v is None and q == 1:
+                    v = p.prop.get(f"{pre}{name}")
+                return _vec3(v, 0.0, iso)[a]
+
             if p.kind == "DebyeMaterial":
                 if field_ == 1:
                     continue

@@ -83,6 +83,12 @@ int ems_model_build_bound(ems_model* m, double dt, int flags);
  * before any TimeStepFactor (openems_timestep, src/engine/timestep.rs:
  * 213-287). 0 for an unknown method. */
 double ems_model_openems_timestep(const ems_model* m, int method);
+/* Replaces the circuit of the E edge along `axis` at `node` after build: its
+ * capacitance `cap` [F] and conductance `cond` [S] (a negative value keeps
+ * the medium's), rounded like the model's circuit values, give its ca, cb
+ * (replace_medium, src/sim/map.rs:1525-1606: how openEMS folds a parallel
+ * R/C lumped element into its edges). */
+int ems_model_set_edge_circuit(ems_model* m, int axis, const uint64_t node[3], double cap, double cond);
 /* Zeroes the update coefficients of the E edges (field 0: ca, cb) or H
  * dual edges (field 1: da, db) along `axis` at the nodes of the inclusive
  * box lo..hi, after build (openEMS's PMC half cell, pmc_half_cell,

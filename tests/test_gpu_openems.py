@@ -2,7 +2,7 @@
 
 Models written for this test in openEMS's XML (graded meshes, PEC, PMC and
 Mur faces, anisotropic lossy materials with magnetic conductivity, metal
-under a higher-priority material, Lorentz, Drude, magnetic and Debye
+under a higher-priority material, a parallel R/C lumped element, Lorentz, Drude, magnetic and Debye
 poles, soft and hard E and H excitations with every signal type and a
 delay, voltage, current, E and H field probes with FD samples, a time
 window and a probe oversampling, an energy end criterion) are set up by
@@ -46,6 +46,7 @@ BOX = f"""<?xml version="1.0" encoding="UTF-8"?>
       <Metal Name="block"><Primitives><Box Priority="2"><P1 X="10" Y="4" Z="3"/><P2 X="12" Y="6" Z="5"/></Box></Primitives></Metal>
       <Material Name="over"><Property Epsilon="4" Kappa="0.01"/>
         <Primitives><Box Priority="3"><P1 X="10" Y="4" Z="5"/><P2 X="12" Y="6" Z="6"/></Box></Primitives></Material>
+      <LumpedElement Name="rc" Direction="2" R="75" C="2e-13" Caps="1"><Primitives><Box Priority="5"><P1 X="2" Y="9" Z="4"/><P2 X="3" Y="10" Z="7"/></Box></Primitives></LumpedElement>
       <Excitation Name="soft" Type="0" Excite="0.3,0,1"><Primitives><Box Priority="0"><P1 X="4" Y="7" Z="5"/><P2 X="5" Y="7" Z="7"/></Box></Primitives></Excitation>
       <Excitation Name="hard" Type="1" Excite="0,0.5,0"><Primitives><Box Priority="0"><P1 X="15" Y="10" Z="9"/><P2 X="15" Y="11" Z="9"/></Box></Primitives></Excitation>
       <ProbeBox Name="ut" Type="0"><FD_Samples>2e9,4e9,6e9</FD_Samples><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="4"/><P2 X="7" Y="7" Z="8.4"/></Box></Primitives></ProbeBox>

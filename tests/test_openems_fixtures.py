@@ -55,6 +55,7 @@ CASES = [
     ("adv_drude_slab", 3e-6), ("adv_lorentz_slab", 3e-6), ("adv_lorentz2_slab", 3e-6),
     ("adv_lorentz_mag_slab", 3e-6), ("adv_debye_slab", 3e-6), ("adv_debye2_slab", 3e-6),
     ("adv_debye_offgrid", 3e-6), ("adv_lorentz_coarse", 3e-6),
+    ("rs_51_debye", 5e-6), ("lumped_port", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -174,7 +175,7 @@ def test_probe_skip_warnings():
 
 @have
 @pytest.mark.parametrize("case,why", [
-    ("nonuniform_materials", "weighting"), ("lumped_port", "LumpedElement"), ("pml", "PML"),
+    ("nonuniform_materials", "weighting"), ("lumped_rc", "series"), ("pml", "PML"),
     ("sweep_exc_sphere", "Sphere")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
