@@ -31,7 +31,7 @@ LORENTZ, DRUDE, DEBYE = 0, 1, 2
 TRAPEZOIDAL, LEAPFROG = 0, 1
 GAUSSIAN = 0
 
-OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR = 1, 2, 3, 4, 5, 6
+OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR, OP_UPML = 1, 2, 3, 4, 5, 6, 7
 # Mur options (MurBoundary::openems_order / openems_corners / count_energy).
 MUR_OPENEMS_ORDER, MUR_OPENEMS_CORNERS, MUR_COUNT_ENERGY = 1, 2, 4
 
@@ -150,6 +150,12 @@ class RunOutcome(C.Structure):
     ]
 
 
+class UpmlTable(C.Structure):
+    """``ems_upml`` (include/ems_gpu.h)."""
+
+    _fields_ = [("n", C.c_size_t * 2), ("axis", C.c_void_p * 2), ("node", C.c_void_p * 2), ("co", C.c_void_p * 2)]
+
+
 class MurTable(C.Structure):
     """``ems_mur`` (include/ems_gpu.h)."""
 
@@ -198,6 +204,7 @@ def host_lib() -> C.CDLL:
             "ems_model_openems_timestep": (d, [p, i]),
             "ems_model_zero_edges": (i, [p, i, i, p, p]),
             "ems_model_set_edge_circuit": (i, [p, i, p, d, d]),
+            "ems_model_add_openems_pml": (i, [p, p]),
             "ems_model_dt": (d, [p]),
             "ems_model_courant_limit": (d, [p]),
             "ems_model_coeff": (p, [p, i]),
@@ -247,6 +254,7 @@ GPU_SYMBOLS = {
     "ems_gpu_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_set_curl_order": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_gpu_time_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ems_gpu_upml_state": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p, C.c_void_p, C.c_size_t]),
     "ems_gpu_time_dump_count": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p]),
     "ems_gpu_time_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -635,6 +643,35 @@ class Model:
             raise ValueError("edge outside the grid")
         return out[0], out[1]
 
+    def add_openems_pml(self, cells: Sequence[int]) -> int:
+        """openEMS's ``PML_n`` layers of ``cells[f]`` cells on face f
+        (``OpenEmsPml``, src/engine/boundary/upml.rs): rewrites the layer
+        edges' coefficients and adds the layer operator."""
+        k = self._check(self._lib.ems_model_add_openems_pml(self._p, _u64(cells)), "add_openems_pml")
+        self.ops.append((OP_UPML, "upml"))
+        return k
+
+    def upml_table(self, op: int) -> list:
+        """Per side (0 E, 1 H): (axis, node as (i, j, k), co (n, 4)) of the
+        openEMS PML operator ``op`` (copies)."""
+        d = EngineDesc.from_address(self.desc)
+        ops = (OpEntry * d.n_ops).from_address(d.ops) if d.n_ops else []
+        if not 0 <= op < d.n_ops or ops[op].kind != OP_UPML:
+            raise ValueError("not an openEMS PML operator")
+        t = UpmlTable.from_address(ops[op].table)
+        ny, nz = self.nodes[1], self.nodes[2]
+        out = []
+        for sd in range(2):
+            n = int(t.n[sd])
+            if not n:
+                out.append((np.zeros(0, np.int64), np.zeros((0, 3), np.int64), np.zeros((0, 4), np.float32)))
+                continue
+            ax = np.ctypeslib.as_array((C.c_uint8 * n).from_address(t.axis[sd])).astype(np.int64)
+            flat = np.ctypeslib.as_array((C.c_uint64 * n).from_address(t.node[sd])).astype(np.int64)
+            co = np.ctypeslib.as_array((C.c_float * (4 * n)).from_address(t.co[sd])).reshape(n, 4).copy()
+            out.append((ax, np.stack([flat // (ny * nz), (flat // nz) % ny, flat % nz], axis=-1), co))
+        return out
+
     def mur_table(self, op: int) -> dict:
         """The Mur operator ``op``'s entries as handed to the engine (copies):
         axis, node/inner as (i, j, k), k (2 per entry), hold, cap, and the
@@ -748,6 +785,14 @@ class Engine:
         self._dumps = getattr(self, "_dumps", {})
         self._dumps[i.value] = (dims, len(fr))
         return i.value
+
+    def upml_state(self, op: int, side: int, n: int):
+        """(F, v) of the openEMS PML operator ``op``, side 0 E / 1 H."""
+        f = np.empty(n, dtype=np.float32)
+        v = np.empty(n, dtype=np.float32)
+        if n:
+            self._ck(self._lib.ems_gpu_upml_state(self._h, op, side, f.ctypes.data, v.ctypes.data, n))
+        return f, v
 
     def add_time_dump(self, field: int, lo, hi, stride=(1, 1, 1), interval: int = 1) -> int:
         """Time-domain snapshots of E (field 0) or H (field 1) over the node

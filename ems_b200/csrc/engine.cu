@@ -61,6 +61,7 @@ struct ems_gpu {
     uint64_t launches = 0;
     int schedule = 0;
     bool oe_curl = false;  // openEMS's summation order of the curl (ems_gpu_set_curl_order)
+    bool has_upml = false; // openEMS PML layers: per-operator and split schedules only
     std::string err;
     // Autotuning (ems_gpu_autotune): candidate schedules timed over real
     // steps (every schedule gives the same bits), the pick cached by key.
@@ -123,6 +124,7 @@ struct ems_gpu {
         ProbeDev probe;
         MurDevT mur;
         bool mur_energy = false;
+        UpmlSideDev upml[2];  // openEMS PML layers: E, H
     };
     std::vector<Op> ops;
     // Frequency-domain dumps (ems_gpu_freq_dump_add).
@@ -547,13 +549,19 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         if (st) return st;
     }
     // The sweep needs no magnetic sources (their serial hook would sit
-    // between a chunk's H and E updates).
+    // between a chunk's H and E updates) and no openEMS PML layers (their
+    // hooks are not cut into chunks).
     h->sweep_ok = true;
-    for (size_t k = 0; k < d->n_ops; ++k)
+    for (size_t k = 0; k < d->n_ops; ++k) {
         if (d->ops[k].kind == EMS_OP_SOURCE) {
             const auto* sr = (const ems_source*)d->ops[k].table;
             if (sr->kind == EMS_SOFT_H || sr->kind == EMS_HARD_H) h->sweep_ok = false;
         }
+        if (d->ops[k].kind == EMS_OP_UPML) {
+            h->sweep_ok = false;
+            if (h->fused_why.empty()) h->fused_why = "openEMS PML layers";
+        }
+    }
     h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
     h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);
     h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
@@ -921,6 +929,13 @@ ems_status run_step(ems_gpu* h, bool energy) {
                 k_poles_capture<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(f, op.poles.e, true);
                 ++h->launches;
             }
+        } else if (op.kind == EMS_OP_UPML) {
+            // upml.rs:443-454: E start values from u, then the H layer update.
+            if (const uint32_t n = op.upml[0].n + op.upml[1].n) {
+                k_upml_hook<<<blocks_for(n, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], op.upml[0], f.i[0], f.i[1],
+                                                              f.i[2], op.upml[1]);
+                ++h->launches;
+            }
         }
     }
     ems_status st = serial_post_h(h, f);
@@ -962,6 +977,13 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
             if (op.poles.h.n_edges && !(split && h->fold_prev[1])) {
                 k_poles_capture<<<blocks_for(op.poles.h.n_edges, 256), 256, 0, s>>>(f, op.poles.h, false);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_UPML) {
+            // upml.rs:456-464: H start values from i, then the E layer update.
+            if (const uint32_t n = op.upml[0].n + op.upml[1].n) {
+                k_upml_hook<<<blocks_for(n, 256), 256, 0, s>>>(f.i[0], f.i[1], f.i[2], op.upml[1], f.u[0], f.u[1],
+                                                              f.u[2], op.upml[0]);
                 ++h->launches;
             }
         }
@@ -1242,6 +1264,29 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
             P.d.weight = h->upload(pr->weight, pr->n_entries);
             break;
         }
+        case EMS_OP_UPML: {
+            const auto* pm = (const ems_upml*)t;
+            for (int sd = 0; sd < 2; ++sd) {
+                const size_t n = pm->n[sd];
+                UpmlSideDev& D = op.upml[sd];
+                if (n >= (1ull << 31) || (n && (!pm->axis[sd] || !pm->node[sd] || !pm->co[sd]))) return EMS_ERR_INVALID;
+                if (!n) continue;
+                std::vector<uint32_t> node(n);
+                for (size_t e = 0; e < n; ++e) {
+                    if (pm->axis[sd][e] > 2 || pm->node[sd][e] >= g.n) return EMS_ERR_INVALID;
+                    node[e] = dev_index(g, pm->node[sd][e]);
+                }
+                D.n = (uint32_t)n;
+                D.axis = h->upload(pm->axis[sd], n);
+                D.node = h->upload(node.data(), n);
+                D.co = (const float4*)h->upload(pm->co[sd], 4 * n);
+                D.f = h->alloc<float>(n);
+                D.v = h->alloc<float>(n);
+                if (!D.axis || !D.node || !D.co || !D.f || !D.v) return EMS_ERR_NOMEM;
+            }
+            h->has_upml = true;
+            break;
+        }
         case EMS_OP_MUR: {
             const auto* m = (const ems_mur*)t;
             MurDevT& M = op.mur;
@@ -1504,6 +1549,20 @@ ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* 
     return check(h, cudaStreamSynchronize(h->stream), "time dump");
 }
 
+ems_status ems_gpu_upml_state(ems_gpu* h, size_t op, int side, float* f, float* v, size_t cap) {
+    if (!h || op >= h->ops.size() || h->ops[op].kind != EMS_OP_UPML || side < 0 || side > 1 || !f || !v)
+        return EMS_ERR_INVALID;
+    const UpmlSideDev& D = h->ops[op].upml[side];
+    if (cap < D.n) return EMS_ERR_INVALID;
+    if (!D.n) return EMS_OK;
+    cudaSetDevice(h->device);
+    if (check(h, cudaMemcpyAsync(f, D.f, D.n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "PML state") ||
+        check(h, cudaMemcpyAsync(v, D.v, D.n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "PML state") ||
+        check(h, cudaStreamSynchronize(h->stream), "PML state"))
+        return EMS_ERR_CUDA;
+    return EMS_OK;
+}
+
 ems_status ems_gpu_time_dump_count(const ems_gpu* h, size_t id, size_t* n) {
     if (!h || !n || id >= h->tdumps.size()) return EMS_ERR_INVALID;
     *n = h->tdumps[id].states.size();
@@ -1550,14 +1609,15 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     T.cache = cache_path;
     int v = 0;
     if (tune_lookup(T.cache, T.key, &v) &&
-        (v == 1 || ((v == 4 || (v == 3 && !h->oe_curl)) && h->tables_ok) || (v == 5 && h->tables_ok && h->sweep_ok))) {
+        (v == 1 || ((v == 4 || (v == 3 && !h->oe_curl && !h->has_upml)) && h->tables_ok) ||
+         (v == 5 && h->tables_ok && h->sweep_ok))) {
         h->schedule = v;
         return EMS_OK;
     }
     // In-place schedules only (the per-operator, two-kernel and split ones
     // share the CPML state buffers).
     T.cand.clear();
-    if (h->tables_ok) T.cand = h->oe_curl ? std::vector<int>{4} : std::vector<int>{4, 3};
+    if (h->tables_ok) T.cand = (h->oe_curl || h->has_upml) ? std::vector<int>{4} : std::vector<int>{4, 3};
     if (h->tables_ok && h->sweep_ok) T.cand.push_back(5);
     T.cand.push_back(1);
     T.ms.assign(T.cand.size(), 0.0);
@@ -1748,6 +1808,8 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
     if (!h || schedule < 0 || schedule > 5) return EMS_ERR_INVALID;
     if (h->oe_curl && (schedule == 2 || schedule == 3))
         return fail(h, EMS_ERR_INVALID, "the fused and two-kernel schedules sum the curl in the default order only");
+    if (h->has_upml && (schedule == 2 || schedule == 3 || schedule == 5))
+        return fail(h, EMS_ERR_INVALID, "openEMS PML layers run on the per-operator and split schedules only");
     if (schedule == 2 && !h->fused_ok) return fail(h, EMS_ERR_INVALID, "fused schedule unavailable: " + h->fused_why);
     if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
     if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
@@ -1967,6 +2029,7 @@ std::string batch_ineligible(const ems_engine_desc* d) {
             else ph = 1;
         }
         if (kind == EMS_OP_MUR) return "Mur boundaries";
+        if (kind == EMS_OP_UPML) return "openEMS PML layers";
         if (pe >= 0) {
             if (pe < phase_e) return "post_e hooks not in the order lumped, E sources, voltage probes";
             phase_e = pe;

@@ -372,6 +372,8 @@ inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t no
 // one. The side's edges are in (plane, axis, row, z) order, so membership is
 // a binary search.
 inline bool pole_prev_fold(const ems_engine_desc* d, bool electric, bool poles_first) {
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind == EMS_OP_UPML) return false;  // its layer update may write pole edges
     const ems_pole_side* ps = nullptr;
     for (size_t k = 0; k < d->n_ops; ++k)
         if (d->ops[k].kind == EMS_OP_POLES) {

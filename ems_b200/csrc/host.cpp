@@ -124,6 +124,11 @@ struct OpStore {
     std::vector<float> mk;
     std::vector<double> mcap;
     ems_mur mur{};
+    // openEMS PML (side 0 E, 1 H)
+    std::vector<uint8_t> pax[2];
+    std::vector<uint64_t> pnode[2];
+    std::vector<float> pco[2];
+    ems_upml upml{};
 };
 
 }  // namespace
@@ -226,6 +231,7 @@ struct ems_model {
             case EMS_OP_LUMPED: e.table = &o->lumped; break;
             case EMS_OP_SOURCE: e.table = &o->source; break;
             case EMS_OP_MUR: e.table = &o->mur; break;
+            case EMS_OP_UPML: e.table = &o->upml; break;
             default: e.table = &o->probe; break;
             }
             op_list.push_back(e);
@@ -721,6 +727,115 @@ double ems_model_openems_timestep(const ems_model* m, int method) {
     }
     if (method == 1) return (double)(1.0f / std::sqrt((float)w2max));
     return 1.0 / std::sqrt(w2max);
+}
+
+// compiler-rt's __powidf2: a^b by repeated squaring (the f64 powi of the
+// reference's grading).
+static double powi(double a, int b) {
+    const bool recip = b < 0;
+    double r = 1.0;
+    for (;;) {
+        if (b & 1) r *= a;
+        b /= 2;
+        if (b == 0) break;
+        a *= a;
+    }
+    return recip ? 1.0 / r : r;
+}
+
+// openems_pml_sigma (src/engine/boundary/upml.rs:143-150).
+static double oe_pml_sigma(double depth, double width, uint64_t cells) {
+    if (depth <= 0.0 || cells == 0 || width <= 0.0) return 0.0;
+    const double dl = width / (double)cells;
+    const double g = 2.5;
+    return std::log(1e6) * std::log(g) / (2.0 * dl * Z0 * (powi(g, (int)cells) - 1.0)) * std::pow(g, depth / dl);
+}
+
+int ems_model_add_openems_pml(ems_model* m, const uint64_t cells[6]) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    const uint64_t* n = m->n;
+    const double dt = m->dt;
+    // Profile::new (upml.rs:165-196): a = sigma*dt/(2 eps0) at the lines
+    // and the cell midpoints, summed over the faces.
+    std::vector<double> at_node[3], at_mid[3];
+    for (int a = 0; a < 3; ++a) {
+        at_node[a].assign(n[a], 0.0);
+        at_mid[a].assign(n[a], 0.0);
+    }
+    bool any = false;
+    for (int f = 0; f < 6; ++f) {
+        const uint64_t c = cells[f];
+        if (!c) continue;
+        const int ax = f / 2;
+        const bool is_max = f & 1;
+        const uint64_t last = n[ax] - 1;
+        if (c > last) return set_err(m, "PML thicker than the mesh"), -1;
+        const std::vector<double>& l = m->lines[ax];
+        const double inner = is_max ? l[last - c] : l[c], outer = is_max ? l[last] : l[0];
+        const double width = std::fabs(outer - inner);
+        auto a_of = [&](double x) {
+            const double depth = is_max ? x - inner : inner - x;
+            return oe_pml_sigma(depth, width, c) * dt / (2.0 * EPS0);
+        };
+        for (uint64_t k = 0; k <= last; ++k) {
+            at_node[ax][k] += a_of(l[k]);
+            if (k < last) at_mid[ax][k] += a_of(0.5 * (l[k] + l[k + 1]));
+        }
+        any = true;
+    }
+    if (!any) return set_err(m, "no PML face"), -1;
+    const double OE_PML_EPS0 = 8.854187817620389e-12, OE_PML_MU0 = 1.256637062e-6;
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_UPML;
+    // OpenEmsPml::build (upml.rs:660-724): E then H, component, node order.
+    for (int side = 0; side < 2; ++side) {
+        const bool e_side = side == 0;
+        for (int comp = 0; comp < 3; ++comp) {
+            const int p = next_axis(comp), q = prev_axis(comp);
+            std::vector<float>& ca = m->co[(e_side ? 0 : 6) + comp];
+            std::vector<float>& cb = m->co[(e_side ? 3 : 9) + comp];
+            const std::vector<double>* own = e_side ? at_mid : at_node;
+            const std::vector<double>* other = e_side ? at_node : at_mid;
+            for (uint64_t i = 0; i < n[0]; ++i)
+                for (uint64_t j = 0; j < n[1]; ++j)
+                    for (uint64_t k = 0; k < n[2]; ++k) {
+                        const uint64_t node[3] = {i, j, k};
+                        const uint64_t idx = m->index(i, j, k);
+                        if (cb[idx] == 0.0f) continue;  // PEC, padding or no edge
+                        const double aa = own[comp][node[comp]], ap = other[p][node[p]], aq = other[q][node[q]];
+                        if (aa == 0.0 && ap == 0.0 && aq == 0.0) continue;
+                        double geo, mm;
+                        if (e_side) {
+                            geo = m->dual_delta(p, node[p]) * m->dual_delta(q, node[q]) / m->delta(comp, node[comp]);
+                            double eps, kap;
+                            edge_eps(m, comp, node, eps, kap);
+                            mm = OE_PML_EPS0 * eps;
+                        } else {
+                            geo = m->delta(p, node[p]) * m->delta(q, node[q]) / m->dual_delta(comp, node[comp]);
+                            double mu, sig;
+                            edge_mu(m, comp, node, mu, sig);
+                            mm = OE_PML_MU0 * mu;
+                        }
+                        ca[idx] = 0.0f;
+                        cb[idx] = (float)(dt / ((1.0 + ap) * geo));
+                        op->pax[side].push_back((uint8_t)comp);
+                        op->pnode[side].push_back(idx);
+                        op->pco[side].push_back((float)((1.0 - ap) / (1.0 + ap)));
+                        op->pco[side].push_back((float)((1.0 - aq) / (1.0 + aq)));
+                        op->pco[side].push_back((float)((1.0 + aa) / ((1.0 + aq) * mm)));
+                        op->pco[side].push_back((float)((1.0 - aa) / ((1.0 + aq) * mm)));
+                    }
+        }
+    }
+    for (int side = 0; side < 2; ++side) {
+        op->upml.n[side] = op->pnode[side].size();
+        op->upml.axis[side] = op->pax[side].data();
+        op->upml.node[side] = op->pnode[side].data();
+        op->upml.co[side] = op->pco[side].data();
+    }
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
 }
 
 int ems_model_set_edge_circuit(ems_model* m, int axis, const uint64_t node[3], double cap, double cond) {

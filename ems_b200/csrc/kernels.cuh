@@ -411,6 +411,48 @@ __global__ void k_branch_energy(LumpedDevT d, double dt, double* out) {
     out[0] = s;
 }
 
+// One side of openEMS's PML layers on the device (src/engine/boundary/
+// upml.rs:260-420): per edge its axis, node, coefficients (co.x..co.w =
+// (1 − a_p)/(1 + a_p), (1 − a_q)/(1 + a_q), (1 + a_a)/((1 + a_q)·m),
+// (1 − a_a)/((1 + a_q)·m)), flux f and start value v.
+struct UpmlSideDev {
+    uint32_t n = 0;
+    const uint8_t* axis = nullptr;
+    const uint32_t* node = nullptr;
+    const float4* co = nullptr;
+    float* f = nullptr;
+    float* v = nullptr;
+};
+
+// One slab hook of the layers (upml.rs:443-464): threads [0, r.n) take the
+// start values of side r from the fields `src` (Run::refresh), threads
+// [r.n, r.n + a.n) complete the update of side a in the fields `dst` from
+// the flux increment the update kernel left there (Run::apply):
+// F' = flush(flush(co.x·F) + t), x = flush(flush(flush(co.y·v) − flush(co.w·F)) + flush(co.z·F')).
+__global__ void __launch_bounds__(256) k_upml_hook(const float* s0, const float* s1, const float* s2, UpmlSideDev r,
+                                                   float* d0, float* d1, float* d2, UpmlSideDev a) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < r.n) {
+        const uint8_t ax = r.axis[e];
+        const float* F = ax == 0 ? s0 : (ax == 1 ? s1 : s2);
+        r.v[e] = F[r.node[e]];
+        return;
+    }
+    const uint32_t q = e - r.n;
+    if (q >= a.n) return;
+    const uint8_t ax = a.axis[q];
+    float* F = ax == 0 ? d0 : (ax == 1 ? d1 : d2);
+    const uint32_t idx = a.node[q];
+    const float4 c = a.co[q];
+    const float t = F[idx], f0 = a.f[q], v = a.v[q];
+    const float f1 = flush(__fadd_rn(flush(__fmul_rn(c.x, f0)), t));
+    const float x = flush(__fadd_rn(flush(__fsub_rn(flush(__fmul_rn(c.y, v)), flush(__fmul_rn(c.w, f0)))),
+                                    flush(__fmul_rn(c.z, f1))));
+    a.f[q] = f1;
+    a.v[q] = x;
+    F[idx] = x;
+}
+
 // A Mur boundary on the device (src/engine/boundary/mur.rs:103-139):
 // entries [0, n_edges) face edges, [n_edges, n) edges shared by two faces;
 // inner and k 2 per entry, saved 3 per entry (u_b^n, u_1^n of each

@@ -21,9 +21,10 @@ Restated from the reference:
   (period repeated), Dirac, step and custom expressions; openEMS's timing
   (src/sim/map.rs:270-307: the field value at time T gets the sample at
   T − dt − ⌊Delay/dt⌋·dt);
-* PEC, PMC (openEMS's half-cell PMC, src/compile/mod.rs:1556-1626) and
+* PEC, PMC (openEMS's half-cell PMC, src/compile/mod.rs:1556-1626),
   first-order Mur faces (openEMS's options, the hold of faces that carry an
-  E excitation, src/compile/mod.rs:1439-1476);
+  E excitation, src/compile/mod.rs:1439-1476) and PML_n layers (openEMS's
+  uniaxial layer, src/engine/boundary/upml.rs);
 * isotropic or anisotropic materials and metal on box primitives;
   Lorentz, Drude and Debye materials as per-edge leapfrog poles with
   openEMS's edge rule (src/compile/dispersive.rs:1-130);
@@ -38,7 +39,8 @@ Restated from the reference:
   interval and after half a Gaussian's length (src/sim/mod.rs:892-930).
 
 Not restated: csx's general discretisation (primitives other than boxes,
-weighting functions, transformations), PML, openEMS's f32 pole arithmetic,
+weighting functions, transformations, sub-cell sampling of boxes off the
+mesh lines), openEMS's f32 pole arithmetic,
 Mur faces with dispersive media, lumped elements, dumps, cylindrical
 grids.
 """
@@ -57,7 +59,7 @@ from . import probe_files as PF
 C0 = 299792458.0
 TWO_PI = 2.0 * math.pi
 FACE_NAMES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
-PEC_FACE, PMC_FACE, MUR_FACE = 0, 1, 2
+PEC_FACE, PMC_FACE, MUR_FACE, PML_FACE = 0, 1, 2, 3
 MATERIALS = ("Material", "LorentzMaterial", "DebyeMaterial")
 
 
@@ -329,6 +331,8 @@ def parse(text: str) -> OpenEmsFile:
             faces.append((PMC_FACE, None))
         elif u in ("MUR", "2"):
             faces.append((MUR_FACE, None))
+        elif u == "3" or re.fullmatch(r"PML_\d+", u):
+            faces.append((PML_FACE, 8 if u == "3" else int(u[4:])))
         else:
             raise NotImplementedError(f"boundary {v!r} on {name}")
     mur_v = _f(bc.get("MUR_PhaseVelocity")) if bc is not None else None
@@ -516,6 +520,10 @@ class Setup:
         m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
         self.dt = dt
         self._pmc_half_cell(m)
+        self.upml_op = None
+        if any(k == PML_FACE for k, _ in f.faces):
+            self.upml_op = m.add_openems_pml([c if k == PML_FACE else 0 for k, c in f.faces])
+            self.upml_h = m.upml_table(self.upml_op)[1]
         self._lumped(m)
         self._dispersive(m)
         steps = f.max_steps
@@ -619,11 +627,13 @@ class Setup:
                         if self._inside(q, lines[q][i], lo[q], hi[q])
                         and (q != a or self._inside(q, lines[q][i + 1], lo[q], hi[q]))] for q in range(3)]
                 edges += [(i, j, k) for i in rng[0] for j in rng[1] for k in rng[2]]
-            cb = m.coeff(3 + a)
+            ca, cb = m.coeff(a), m.coeff(3 + a)
             kept = []
             for e in edges:
                 if cb[e] == 0.0:
                     self.warnings.append(f"lumped element {p.name!r}: edge {e} is PEC (shorted); ignored")
+                elif ca[e] == 0.0:  # inside a PML layer: the layer replaces the update
+                    self.warnings.append(f"lumped element {p.name!r}: edge {e} inside a PML layer; ignored")
                 else:
                     kept.append(e)
             if not kept or (r is None and c is None):
@@ -1050,7 +1060,38 @@ class Setup:
             shape[a] = n[a]
             wh += float(np.sum((x * wgt.reshape(shape))[valid[a]]))
         from . import eps0, mu0
-        return eps0() * we + mu0() * wh
+        w = eps0() * we + mu0() * wh
+        if self.upml_op is not None and len(self.upml_h[0]):
+            w += mu0() * self._upml_energy_correction(engine, u, co)
+        return w
+
+    def _upml_energy_correction(self, engine, u, co):
+        """What openEMS's measure misses on the PML layers' H edges, whose
+        look-ahead is the flux increment (upml.rs:466-506): Σ x² − inc² with
+        inc = −db·(curl in the default order) and x its layer update."""
+        ax, nodes, c = self.upml_h
+        F, v = engine.upml_state(self.upml_op, 1, len(ax))
+        tiny = np.float32(np.finfo(np.float32).tiny)
+
+        def fl(x):
+            return np.where(np.abs(x) < tiny, np.float32(0.0), x).astype(np.float32)
+
+        i, j, k = nodes[:, 0], nodes[:, 1], nodes[:, 2]
+        t = np.zeros(len(ax), dtype=np.float32)
+        for a in range(3):
+            sel = ax == a
+            ii, jj, kk = i[sel], j[sel], k[sel]
+            if a == 0:
+                t[sel] = (u[2][ii, jj + 1, kk] - u[2][ii, jj, kk]) - (u[1][ii, jj, kk + 1] - u[1][ii, jj, kk])
+            elif a == 1:
+                t[sel] = (u[0][ii, jj, kk + 1] - u[0][ii, jj, kk]) - (u[2][ii + 1, jj, kk] - u[2][ii, jj, kk])
+            else:
+                t[sel] = (u[1][ii + 1, jj, kk] - u[1][ii, jj, kk]) - (u[0][ii, jj + 1, kk] - u[0][ii, jj, kk])
+        db = np.array([co[9 + a][n_] for a, n_ in zip(ax, map(tuple, nodes))], dtype=np.float32)
+        inc = fl(np.float32(0.0) * v - db * t)
+        f1 = fl(fl(c[:, 0] * F) + inc)
+        x = fl(fl(fl(c[:, 1] * v) - fl(c[:, 3] * F)) + fl(c[:, 2] * f1))
+        return float(np.sum(x.astype(np.float64) ** 2 - inc.astype(np.float64) ** 2))
 
     def _drive(self, engine, curl_order) -> int:
         """The reference's run loop for files (src/engine/run.rs:424-540
@@ -1090,6 +1131,7 @@ class Setup:
         does for files (its fields then equal openEMS's where the
         coefficients do), 0 in the engine's default order."""
         engine.set_curl_order(curl_order)
+        self.stopped, self.last_ratio_db = False, None
         if self.criterion is None:
             engine.run(self.steps + 1)
             self.steps_run = self.steps
@@ -1169,7 +1211,7 @@ class Results:
     def write(self, directory: str) -> list:
         os.makedirs(directory, exist_ok=True)
         out = []
-        for name, text in {**self.files(), **self.signal_files()}.items():
+        for name, text in {**self.signal_files(), **self.files()}.items():  # a probe named et or ht wins
             path = os.path.join(directory, name)
             with open(path, "w") as h:
                 h.write(text)

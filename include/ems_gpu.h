@@ -50,7 +50,8 @@ typedef enum {
     EMS_OP_LUMPED = 3, /* serial pre_e / post_e        (src/engine/lumped.rs:1123-1236)      */
     EMS_OP_SOURCE = 4, /* serial post_h or post_e      (src/engine/excite.rs:104-173)        */
     EMS_OP_PROBE = 5,  /* serial post_h or post_e      (src/engine/probe.rs:480-510)         */
-    EMS_OP_MUR = 6     /* serial pre_e / post_e        (src/engine/boundary/mur.rs:781-843)  */
+    EMS_OP_MUR = 6,    /* serial pre_e / post_e        (src/engine/boundary/mur.rs:781-843)  */
+    EMS_OP_UPML = 7    /* slab hooks post_h / post_e   (src/engine/boundary/upml.rs:443-470) */
 } ems_op_kind;
 
 /* One CPML slab: the correction of one field component in one face layer
@@ -200,9 +201,27 @@ typedef struct {
     int32_t count_energy;      /* energy: sum of 1/2 cap u^2 over the last written values */
 } ems_mur;
 
+/* openEMS's uniaxial PML layers (src/engine/boundary/upml.rs:1-140): the
+ * layer edges of side 0 (E edges) and 1 (H dual edges), whose coefficients
+ * the host already rewrote to (0, dt/((A/l)(1 + a_p))) so that the update
+ * kernel leaves the flux increment t in the field. Per edge: axis, node and
+ * the f32 coefficients co[4e..4e+3] = (1 - a_p)/(1 + a_p), (1 - a_q)/(1 + a_q),
+ * (1 + a_a)/((1 + a_q) m), (1 - a_a)/((1 + a_q) m). Each edge keeps its flux
+ * F and start value v (zero at first). After the H update: v of every E
+ * edge = u (refresh), then every H edge: F' = flush(flush(co0*F) + t),
+ * x = flush(flush(flush(co1*v) - flush(co3*F)) + flush(co2*F')), F = F',
+ * v = x, field = x (apply); after the E update the same with the sides
+ * swapped. */
+typedef struct {
+    size_t n[2];
+    const uint8_t* axis[2];
+    const uint64_t* node[2];
+    const float* co[2];
+} ems_upml;
+
 typedef struct {
     int32_t kind; /* ems_op_kind */
-    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe*, ems_mur* */
+    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe*, ems_mur*, ems_upml* */
 } ems_op;
 
 /* Everything an engine is built from: the grid size, the time step, the
@@ -372,6 +391,9 @@ typedef struct {
 } ems_time_dump;
 
 ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* id);
+/* The flux F and start value v of every edge of side `side` (0 E, 1 H) of the
+ * EMS_OP_UPML operator `op`, in table order (cap >= the side's edges). */
+ems_status ems_gpu_upml_state(ems_gpu* h, size_t op, int side, float* f, float* v, size_t cap);
 /* Number of snapshots taken so far. */
 ems_status ems_gpu_time_dump_count(const ems_gpu* h, size_t id, size_t* n);
 /* Snapshot k: 3 values per point (x, y, z components) into out (cap >= 3 *

@@ -83,6 +83,11 @@ int ems_model_build_bound(ems_model* m, double dt, int flags);
  * before any TimeStepFactor (openems_timestep, src/engine/timestep.rs:
  * 213-287). 0 for an unknown method. */
 double ems_model_openems_timestep(const ems_model* m, int method);
+/* openEMS's PML_n layers (OpenEmsPml::with_materials, src/engine/boundary/
+ * upml.rs:560-724) of cells[f] cells on each face f with cells[f] > 0 (the
+ * faces built PEC): rewrites the coefficients of the layer edges and adds
+ * the EMS_OP_UPML operator with their tables. Returns the op index. */
+int ems_model_add_openems_pml(ems_model* m, const uint64_t cells[6]);
 /* Replaces the circuit of the E edge along `axis` at `node` after build: its
  * capacitance `cap` [F] and conductance `cond` [S] (a negative value keeps
  * the medium's), rounded like the model's circuit values, give its ca, cb

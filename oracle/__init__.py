@@ -28,6 +28,7 @@ def lib() -> C.CDLL:
             "oracle_destroy": [p],
             "oracle_threads": [p],
             "oracle_set_curl_order": [p, C.c_int],
+            "oracle_upml_state": [p, C.c_size_t, C.c_int, p, p, C.c_size_t],
             "oracle_run": [p, C.c_uint64],
             "oracle_step_with_energy": [p, p],
             "oracle_download_field": [p, C.c_int, C.c_int, p],
@@ -58,6 +59,14 @@ class OracleEngine:
     @property
     def threads(self) -> int:
         return self._lib.oracle_threads(self._h)
+
+    def upml_state(self, op: int, side: int, n: int):
+        """(F, v) of the openEMS PML operator ``op``, side 0 E / 1 H."""
+        f = np.empty(n, dtype=np.float32)
+        v = np.empty(n, dtype=np.float32)
+        if n and self._lib.oracle_upml_state(self._h, op, side, f.ctypes.data, v.ctypes.data, n) != 0:
+            raise ValueError("not a PML operator")
+        return f, v
 
     def set_curl_order(self, order: int) -> None:
         """0 the reference's default summation order, 1 openEMS's."""

@@ -164,6 +164,17 @@ struct Mur {
     std::vector<float> last;                  // value after the last update
 };
 
+// openEMS's PML layers (src/engine/boundary/upml.rs:260-420 Run): per
+// side (0 E, 1 H) the edges, their coefficients, flux F and start value v,
+// and the edges of each x-plane (by_plane[pstart[i]..pstart[i + 1]]).
+struct Upml {
+    std::vector<uint8_t> axis[2];
+    std::vector<uint64_t> node[2];
+    std::vector<float> co[2];
+    std::vector<float> f[2], v[2];
+    std::vector<uint32_t> by_plane[2], pstart[2];
+};
+
 struct Op {
     int kind = 0;
     std::vector<CpmlSlab> cpml;
@@ -172,6 +183,7 @@ struct Op {
     Source source;
     Probe probe;
     Mur mur;
+    Upml upml;
 };
 
 // src/engine/boundary/mur.rs:252-259 mur_1d: u_b^{n+1} from u_1^n (i),
@@ -468,6 +480,33 @@ struct oracle_engine {
         }
     }
 
+    // Run::refresh (upml.rs:380-392): the start values of side `sd` from
+    // the fields, planes [x0, x1).
+    void upml_refresh(Upml& L, int sd, size_t x0, size_t x1) {
+        const auto& F = sd == 0 ? u : i;
+        for (uint32_t q = L.pstart[sd][x0]; q < L.pstart[sd][x1]; ++q) {
+            const uint32_t e = L.by_plane[sd][q];
+            L.v[sd][e] = F[L.axis[sd][e]][L.node[sd][e]];
+        }
+    }
+
+    // Run::apply (upml.rs:394-418): the layer update of side `sd` from the
+    // flux increment the kernel left in the field, planes [x0, x1).
+    void upml_apply(Upml& L, int sd, size_t x0, size_t x1) {
+        auto& F = sd == 0 ? u : i;
+        for (uint32_t q = L.pstart[sd][x0]; q < L.pstart[sd][x1]; ++q) {
+            const uint32_t e = L.by_plane[sd][q];
+            const float* c = &L.co[sd][4 * (size_t)e];
+            float& t = F[L.axis[sd][e]][L.node[sd][e]];
+            const float f0 = L.f[sd][e];
+            const float f1 = flush(flush(c[0] * f0) + t);
+            const float x = flush(flush(flush(c[1] * L.v[sd][e]) - flush(c[3] * f0)) + flush(c[2] * f1));
+            L.f[sd][e] = f1;
+            L.v[sd][e] = x;
+            t = x;
+        }
+    }
+
     // src/engine/boundary/mur.rs:781-808 pre_e: u_b^n and u_1^n.
     void mur_pre_e(Mur& m) {
         for (size_t e = 0; e < m.node.size(); ++e) {
@@ -587,6 +626,10 @@ struct oracle_engine {
                 } else if (op.kind == EMS_OP_POLES) {
                     poles_correct(op.ph, false, p0, p1);
                     poles_capture(op.pe, true, p0, p1);
+                } else if (op.kind == EMS_OP_UPML) {
+                    // upml.rs:443-454 post_h_slab.
+                    upml_refresh(op.upml, 0, p0, p1);
+                    upml_apply(op.upml, 1, p0, p1);
                 }
             }
         });
@@ -610,6 +653,10 @@ struct oracle_engine {
                 } else if (op.kind == EMS_OP_POLES) {
                     poles_correct(op.pe, true, p0, p1);
                     poles_capture(op.ph, false, p0, p1);
+                } else if (op.kind == EMS_OP_UPML) {
+                    // upml.rs:456-464 post_e_slab.
+                    upml_refresh(op.upml, 1, p0, p1);
+                    upml_apply(op.upml, 0, p0, p1);
                 }
             }
         });
@@ -773,6 +820,30 @@ int oracle_create(const ems_engine_desc* d, int threads, oracle_engine** out) {
             op.probe.f32_sum = p->f32_sum != 0;
             break;
         }
+        case EMS_OP_UPML: {
+            const auto* pm = (const ems_upml*)t;
+            Upml& L = op.upml;
+            for (int sd = 0; sd < 2; ++sd) {
+                const size_t n = pm->n[sd];
+                if (n && (!pm->axis[sd] || !pm->node[sd] || !pm->co[sd])) { delete e; return EMS_ERR_INVALID; }
+                L.axis[sd] = vec(pm->axis[sd], n);
+                L.node[sd] = vec(pm->node[sd], n);
+                L.co[sd] = vec(pm->co[sd], 4 * n);
+                L.f[sd].assign(n, 0.0f);
+                L.v[sd].assign(n, 0.0f);
+                std::vector<uint32_t> cnt(e->nx + 1, 0);
+                for (size_t q = 0; q < n; ++q) {
+                    if (L.axis[sd][q] > 2 || L.node[sd][q] >= e->n) { delete e; return EMS_ERR_INVALID; }
+                    ++cnt[L.node[sd][q] / e->plane + 1];
+                }
+                for (size_t x = 0; x < e->nx; ++x) cnt[x + 1] += cnt[x];
+                L.pstart[sd] = cnt;
+                L.by_plane[sd].assign(n, 0);
+                std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+                for (size_t q = 0; q < n; ++q) L.by_plane[sd][fill[L.node[sd][q] / e->plane]++] = (uint32_t)q;
+            }
+            break;
+        }
         case EMS_OP_MUR: {
             const auto* m = (const ems_mur*)t;
             Mur& M = op.mur;
@@ -829,6 +900,15 @@ int oracle_destroy(oracle_engine* e) {
 }
 
 int oracle_threads(const oracle_engine* e) { return e ? e->pool->size() : 0; }
+
+int oracle_upml_state(oracle_engine* e, size_t op, int side, float* f, float* v, size_t cap) {
+    if (!e || op >= e->ops.size() || e->ops[op].kind != EMS_OP_UPML || side < 0 || side > 1) return EMS_ERR_INVALID;
+    const Upml& L = e->ops[op].upml;
+    if (cap < L.f[side].size()) return EMS_ERR_INVALID;
+    std::memcpy(f, L.f[side].data(), L.f[side].size() * sizeof(float));
+    std::memcpy(v, L.v[side].data(), L.v[side].size() * sizeof(float));
+    return EMS_OK;
+}
 
 int oracle_set_curl_order(oracle_engine* e, int order) {
     if (!e || order < 0 || order > 1) return EMS_ERR_INVALID;

@@ -34,6 +34,9 @@ int oracle_threads(const oracle_engine* e);
 /* 0: the reference's default curl order (a - b) - (c - d); 1: openEMS's
  * order with every operation flushed (CurlOrder, src/engine/kernel.rs:81-108). */
 int oracle_set_curl_order(oracle_engine* e, int order);
+/* The flux F and start value v of every edge of side `side` (0 E, 1 H) of
+ * the EMS_OP_UPML operator `op`, in table order (cap >= the side's edges). */
+int oracle_upml_state(oracle_engine* e, size_t op, int side, float* f, float* v, size_t cap);
 int oracle_run(oracle_engine* e, uint64_t n);
 int oracle_step_with_energy(oracle_engine* e, double* energy);
 int oracle_download_field(oracle_engine* e, int field, int axis, float* host);

@@ -139,6 +139,32 @@ DISP = f"""<?xml version="1.0" encoding="UTF-8"?>
 """
 
 
+PMLM = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="600" endCriteria="0.05">
+    <Excitation Type="0" f0="8e9" fc="6e9"/>
+    <BoundaryCond xmin="PEC" xmax="PML_5" ymin="PML_4" ymax="PMC" zmin="PEC" zmax="PML_3"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <Material Name="block"><Property Epsilon="2.2" Mue="1.3" Kappa="0.02" Sigma="30"/>
+        <Primitives><Box Priority="1"><P1 X="9" Y="0" Z="5"/><P2 X="16" Y="6" Z="12"/></Box></Primitives></Material>
+      <Excitation Name="exc" Type="0" Excite="0.3,0.5,1"><Primitives><Box Priority="0"><P1 X="5" Y="7" Z="4"/><P2 X="6" Y="8" Z="6"/></Box></Primitives></Excitation>
+      <ProbeBox Name="ut" Type="0"><Primitives><Box Priority="0"><P1 X="8" Y="6" Z="0"/><P2 X="8" Y="6" Z="12"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="ein" Type="2"><Primitives><Box Priority="0"><P1 X="14" Y="2" Z="10"/><P2 X="14" Y="2" Z="10"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="hin" Type="3"><Primitives><Box Priority="0"><P1 X="15" Y="1" Z="11"/><P2 X="15" Y="1" Z="11"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="it" Type="1" NormDir="0"><Primitives><Box Priority="0"><P1 X="12" Y="2" Z="2"/><P2 X="12" Y="10" Z="10"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -151,14 +177,17 @@ def _both(text, schedule=0):
 
 
 # Schedules 2 (fused) and 5 (sweep) do not run magnetic sources, 2 not
-# magnetic poles.
+# magnetic poles; openEMS PML layers run on schedules 1 and 4 only.
 @pytest.mark.parametrize("name,text,schedule", [
     ("box", BOX, 0), ("box", BOX, 1), ("box", BOX, 2), ("box", BOX, 3), ("box", BOX, 5),
     ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1),
-    ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5)])
+    ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5),
+    ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes
+    if name == "pml":
+        assert s.stopped  # the end criterion, with the layers' energy correction
     for p in s.probes:
         a, b = rg.series[p.name], ro.series[p.name]
         assert a.shape == b.shape and a.size
