@@ -28,7 +28,9 @@ SOFT_E, HARD_E, SOFT_H, HARD_H = 0, 1, 2, 3
 VOLTAGE, CURRENT = 0, 1
 PEC, PMC = 0, 1
 LORENTZ, DRUDE, DEBYE = 0, 1, 2
-TRAPEZOIDAL, LEAPFROG = 0, 1
+# Pole schemes: trapezoidal, leapfrog, openEMS's f32 arithmetic (Lorentz and
+# Drude poles take the material's own omega_p under it).
+TRAPEZOIDAL, LEAPFROG, OPENEMS_POLES = 0, 1, 2
 GAUSSIAN = 0
 
 OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR, OP_UPML = 1, 2, 3, 4, 5, 6, 7
@@ -205,6 +207,8 @@ def host_lib() -> C.CDLL:
             "ems_model_zero_edges": (i, [p, i, i, p, p]),
             "ems_model_set_edge_circuit": (i, [p, i, p, d, d]),
             "ems_model_add_openems_pml": (i, [p, p]),
+            "ems_model_set_edge_materials": (i, [p, i, i, p, p]),
+            "ems_model_set_mur_media": (i, [p, i, i, p]),
             "ems_model_dt": (d, [p]),
             "ems_model_courant_limit": (d, [p]),
             "ems_model_coeff": (p, [p, i]),
@@ -486,6 +490,24 @@ class Model:
 
     def build(self, courant: float = 0.99, dt: float | None = None) -> "Model":
         self._check(self._lib.ems_model_build(self._p, courant, dt or 0.0), "build!")
+        return self
+
+    def set_edge_materials(self, field: int, axis: int, v0: np.ndarray, v1: np.ndarray) -> "Model":
+        """Per-edge (eps_r, kappa) of the E edges (field 0) or (mu_r,
+        sigma_m) of the H dual edges (field 1) along ``axis``, node arrays,
+        in place of the cell averages (before build)."""
+        a0 = np.ascontiguousarray(v0, dtype=np.float64).ravel()
+        a1 = np.ascontiguousarray(v1, dtype=np.float64).ravel()
+        self._check(self._lib.ems_model_set_edge_materials(self._p, field, axis, a0.ctypes.data, a1.ctypes.data),
+                    "set_edge_materials!")
+        return self
+
+    def set_mur_media(self, face: int, axis: int, v: np.ndarray) -> "Model":
+        """Phase velocities of the edges along ``axis`` on Mur ``face`` (0
+        x_min … 5 z_max), a (n_u, n_w) array over the face plane (u < w the
+        other axes; 0 keeps the local medium); before ``add_mur``."""
+        a = np.ascontiguousarray(v, dtype=np.float64).ravel()
+        self._check(self._lib.ems_model_set_mur_media(self._p, face, axis, a.ctypes.data), "set_mur_media!")
         return self
 
     def build_bound(self, dt: float, openems_rounding: bool = False, openems_sigma_m: bool = False) -> "Model":

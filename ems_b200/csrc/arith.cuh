@@ -13,6 +13,39 @@ namespace emsk {
 // Rounds subnormal results to zero (src/engine/kernel.rs:30-33).
 __device__ __forceinline__ float flush(float x) { return fabsf(x) < FLT_MIN ? 0.0f : x; }
 
+// openEMS's f32 leapfrog of one Lorentz/Drude pole (OpenEmsPole,
+// src/engine/dispersive.rs:846-899, 1414-1425): V <- A·V + B·(u^n − W),
+// W <- W + K·V, returns u − V, every operation flushed. The state (V, W)
+// is held as f64 copies of f32 values.
+__device__ __forceinline__ float oe_pole_step(double A, double K, double B, double& j, double& q, float prev, float u) {
+    const float a = (float)A, k = (float)K, b = (float)B, v0 = (float)j, w0 = (float)q;
+    const float v = flush(__fadd_rn(flush(__fmul_rn(a, v0)), flush(__fmul_rn(b, flush(__fsub_rn(prev, w0))))));
+    j = (double)v;
+    q = (double)flush(__fadd_rn(w0, flush(__fmul_rn(k, v))));
+    return flush(__fsub_rn(u, v));
+}
+
+// openEMS's f32 Debye update of an edge whose np poles are all Debye poles
+// (openems_debye_step, src/engine/dispersive.rs:930-960): constants F, 1 − g,
+// b of pole q at A[q·st], G[q·st], B[q·st]; polarisations Q in j[q].
+__device__ __forceinline__ float oe_debye_edge(const double* A, const double* G, const double* B, uint32_t st,
+                                               double* j, uint32_t np, float prev, float u_star) {
+    const float F = (float)A[0];
+    float sum = 0.0f;
+    for (uint32_t q = 0; q < np; ++q) {
+        const float om = (float)G[q * st], b = (float)B[q * st], Q = (float)j[q];
+        const float P = flush(__fadd_rn(flush(__fmul_rn(om, Q)), flush(__fmul_rn(b, prev))));
+        sum = flush(__fadd_rn(sum, flush(__fsub_rn(P, Q))));
+        j[q] = (double)P;
+    }
+    const float un = flush(__fmul_rn(F, flush(__fsub_rn(u_star, sum))));
+    for (uint32_t q = 0; q < np; ++q) {
+        const float b = (float)B[q * st];
+        j[q] = (double)flush(__fadd_rn((float)j[q], flush(__fmul_rn(b, un))));
+    }
+    return flush(__fsub_rn(u_star, flush(__fsub_rn(u_star, un))));
+}
+
 // flush(ca·u + cb·((a − b) − (c − d))) (src/engine/kernel.rs:252-273).
 __device__ __forceinline__ float e_upd(float ca, float u, float cb, float a, float b, float c, float d) {
     return flush(__fadd_rn(__fmul_rn(ca, u), __fmul_rn(cb, __fsub_rn(__fsub_rn(a, b), __fsub_rn(c, d)))));

@@ -61,11 +61,11 @@ struct PoleRun {
     uint32_t p0;       // state index of the run's first pole
     uint32_t set;      // offset of the run's constants (np poles × {a, inv_c, inv_z})
     uint32_t np;       // poles per edge
-    uint32_t kinds;    // bit q set: pole q is a leapfrog pole
+    uint32_t kinds;    // bit q set: pole q is not trapezoidal (leapfrog or openEMS)
     uint32_t e0;       // edge index of the run's first edge (in the side's table)
     uint32_t axis;     // the edges' axis
     uint32_t node0;    // padded node index of the run's first edge
-    uint32_t pad;
+    uint32_t oe;       // bit q: pole q is openEMS's f32 pole; kOeDebye: an openEMS Debye edge
     double sum_inv_z;
 };
 
@@ -222,13 +222,18 @@ __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets,
         const double cb = (double)cb_f;
         // The field value the update starts from: the one given, or the
         // edge's saved value (magnetic poles, src/engine/dispersive.rs:1173).
-        const double prev = (double)(prev_arr ? prev_arr[R.e0 + (k - R.kb)] : prev_f);
+        const float prev32 = prev_arr ? prev_arr[R.e0 + (k - R.kb)] : prev_f;
+        if (R.oe & kOeDebye) return oe_debye_edge(cs, cs + 1, cs + 2, 3u, pj + p0, R.np, prev32, u_star);
+        const double prev = (double)prev32;
         const double half_prev = __dmul_rn(0.5, prev);
         double s = 0.0;
+        float u32 = u_star;
         for (uint32_t p = 0; p < R.np; ++p) {
             const double a = cs[3 * p], ic = cs[3 * p + 1], iz = cs[3 * p + 2];
             const double jq = pj[p0 + p], qq = pq[p0 + p];
-            if ((R.kinds >> p) & 1u) {
+            if ((R.oe >> p) & 1u) {
+                u32 = oe_pole_step(a, ic, iz, pj[p0 + p], pq[p0 + p], prev32, u32);
+            } else if ((R.kinds >> p) & 1u) {
                 const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
                 pj[p0 + p] = jn;
                 pq[p0 + p] = __dadd_rn(qq, __dmul_rn(dt, jn));
@@ -237,7 +242,7 @@ __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets,
                 s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
             }
         }
-        const float u_new = (float)__ddiv_rn(__dsub_rn((double)u_star, __dmul_rn(cb, s)),
+        const float u_new = (float)__ddiv_rn(__dsub_rn((double)u32, __dmul_rn(cb, s)),
                                              __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
         if (R.kinds != (1u << R.np) - 1u) {
             const double half_new = __dmul_rn(0.5, (double)u_new);

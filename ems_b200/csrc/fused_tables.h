@@ -103,15 +103,19 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
         const uint32_t p0 = e ? pe->pole_end[e - 1] : 0, p1 = pe->pole_end[e];
         const uint32_t np = p1 - p0;
         if (np > kMaxPoles || np == 0) return "more than 16 poles on an edge";
-        std::string key((size_t)np * 24 + 12, '\0');
-        uint32_t kinds = 0;
+        std::string key((size_t)np * 24 + 16, '\0');
+        uint32_t kinds = 0, oe = 0;
         for (uint32_t q = 0; q < np; ++q) {
             const double c3[3] = {pe->a[p0 + q], pe->inv_c[p0 + q], pe->inv_z[p0 + q]};
             std::memcpy(&key[(size_t)q * 24], c3, 24);
-            if (pe->kind[p0 + q] == EMS_POLE_LEAPFROG) kinds |= 1u << q;
+            const uint8_t kd = pe->kind[p0 + q];
+            if (kd != EMS_POLE_TRAPEZOIDAL) kinds |= 1u << q;
+            if (kd == EMS_POLE_OPENEMS) oe |= 1u << q;
+            if (kd == EMS_POLE_OPENEMS_DEBYE) oe |= kOeDebye;
         }
         std::memcpy(&key[(size_t)np * 24], &pe->sum_inv_z[e], 8);
         std::memcpy(&key[(size_t)np * 24 + 8], &kinds, 4);
+        std::memcpy(&key[(size_t)np * 24 + 12], &oe, 4);
         auto it = set_of.find(key);
         uint32_t set;
         if (it == set_of.end()) {
@@ -127,6 +131,7 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
         }
         const bool extend = !R.runs.empty() && row_key == last_row && kk == (uint64_t)last_k + 1 &&
                             R.runs.back().set == set && R.runs.back().np == np && R.runs.back().kinds == kinds &&
+                            R.runs.back().oe == oe &&
                             R.runs.back().p0 + (R.runs.back().ke - R.runs.back().kb) * np == p0 &&
                             R.runs.back().e0 + (R.runs.back().ke - R.runs.back().kb) == e;
         if (extend) {
@@ -134,7 +139,7 @@ inline std::string pole_runs(const ems_pole_side* pe, uint32_t nx, uint32_t ny, 
         } else {
             if (row_key != last_row) R.row_runs[row_key] = uint4{(uint32_t)R.runs.size(), 0, (uint32_t)kk, 0};
             R.runs.push_back(PoleRun{(uint32_t)kk, (uint32_t)kk + 1, p0, set, np, kinds, (uint32_t)e, (uint32_t)pe->axis[e],
-                                     (uint32_t)((ii * ny + jj) * pitch + kk), 0, pe->sum_inv_z[e]});
+                                     (uint32_t)((ii * ny + jj) * pitch + kk), oe, pe->sum_inv_z[e]});
             R.row_runs[row_key].y++;
         }
         R.run_of.push_back((uint32_t)R.runs.size() - 1);

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <tuple>
 #include <string>
@@ -143,6 +144,13 @@ struct ems_model {
     int faces[6] = {0, 0, 0, 0, 0, 0};
     bool built = false;
     bool oe_round = false;  // built with openEMS's coefficient rounding
+    // Per-edge materials given by the caller (ems_model_set_edge_materials)
+    // in place of the averages of the cells: [axis][0 eps_r or mu_r, 1
+    // kappa or sigma_m], reference layout; empty: from the cells.
+    std::vector<double> emat[3][2], hmat[3][2];
+    // Per-edge phase velocities of local-medium Mur faces (MurMedia), keyed
+    // face·3 + axis, one value per node of the face plane (0: none).
+    std::map<int, std::vector<double>> mur_v;
     double dt = 0.0;
     std::vector<float> co[12];
     std::vector<std::unique_ptr<OpStore>> ops;
@@ -459,6 +467,12 @@ static void edge_eps(const ems_model* m, int a, const uint64_t p[3], double& eps
     eps = 1.0;
     kap = 0.0;
     if (p[a] + 1 >= m->n[a]) return;
+    if (!m->emat[a][0].empty()) {
+        const uint64_t idx = m->index(p[0], p[1], p[2]);
+        eps = m->emat[a][0][idx];
+        kap = m->emat[a][1][idx];
+        return;
+    }
     const int b = next_axis(a), c = prev_axis(a);
     double cap_c, g_c;
     m->primary_edge_cg(a, p, cap_c, g_c);
@@ -472,6 +486,12 @@ static void edge_mu(const ems_model* m, int a, const uint64_t p[3], double& mu, 
     sig = 0.0;
     const int b = next_axis(a), c = prev_axis(a);
     if (p[b] + 1 >= m->n[b] || p[c] + 1 >= m->n[c]) return;
+    if (!m->hmat[a][0].empty()) {
+        const uint64_t idx = m->index(p[0], p[1], p[2]);
+        mu = m->hmat[a][0][idx];
+        sig = m->hmat[a][1][idx];
+        return;
+    }
     double l_c, r_c;
     m->dual_edge_lr(a, p, l_c, r_c);
     const double k_ = m->dual_delta(a, p[a]) / (m->delta(b, p[b]) * m->delta(c, p[c]));
@@ -545,7 +565,7 @@ static void compute_coefficients(ems_model* m, double dt, bool openems, bool oe_
                         if (p[b] + 1 < m->n[b] && p[c] + 1 < m->n[c]) {
                             double mu, sig;
                             edge_mu(m, a, p, mu, sig);
-                            if (oe_sigma) sig = oe_sigma_m(m, a, p);
+                            if (oe_sigma && m->hmat[a][1].empty()) sig = oe_sigma_m(m, a, p);
                             double geo = m->delta(b, p[b]) * m->delta(c, p[c]) / m->dual_delta(a, p[a]);
                             double l = store(mu0 * mu * geo);
                             double r = store(sig * geo);
@@ -559,6 +579,31 @@ static void compute_coefficients(ems_model* m, double dt, bool openems, bool oe_
     m->dt = dt;
     m->built = true;
     m->refresh_desc();
+}
+
+int ems_model_set_mur_media(ems_model* m, int face, int axis, const double* v) {
+    if (face < 0 || face > 5 || axis < 0 || axis > 2 || axis == face / 2 || !v)
+        return set_err(m, "invalid Mur media"), EMS_ERR_INVALID;
+    const int a = face / 2, u = a == 0 ? 1 : 0, w = a == 2 ? 1 : 2;
+    const size_t N = (size_t)(m->n[u] * m->n[w]);
+    for (size_t q = 0; q < N; ++q)
+        if (!(std::isfinite(v[q]) && v[q] >= 0.0)) return set_err(m, "Mur media velocities must be finite and >= 0"), EMS_ERR_INVALID;
+    m->mur_v[face * 3 + axis].assign(v, v + N);
+    return EMS_OK;
+}
+
+int ems_model_set_edge_materials(ems_model* m, int field, int axis, const double* v0, const double* v1) {
+    if (m->built) return set_err(m, "set edge materials before build"), EMS_ERR_INVALID;
+    if ((field != 0 && field != 1) || axis < 0 || axis > 2 || !v0 || !v1)
+        return set_err(m, "invalid edge material arrays"), EMS_ERR_INVALID;
+    const size_t N = (size_t)(m->n[0] * m->n[1] * m->n[2]);
+    std::vector<double>* dst = field ? m->hmat[axis] : m->emat[axis];
+    for (size_t q = 0; q < N; ++q)
+        if (!(std::isfinite(v0[q]) && v0[q] > 0.0 && std::isfinite(v1[q]) && v1[q] >= 0.0))
+            return set_err(m, "edge materials must be finite, eps_r/mu_r > 0, kappa/sigma_m >= 0"), EMS_ERR_INVALID;
+    dst[0].assign(v0, v0 + N);
+    dst[1].assign(v1, v1 + N);
+    return EMS_OK;
 }
 
 int ems_model_build(ems_model* m, double courant, double fixed_dt) {
@@ -1143,6 +1188,7 @@ int ems_model_edge_material(const ems_model* m, int field, int axis, const uint6
 
 int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
     if (!m->built) return set_err(m, "build the model first"), -1;
+    if (scheme < 0 || scheme > 2) return set_err(m, "unknown pole scheme"), -1;
     for (const Entry& e : d->entries) {
         bool exists = e.node[0] < m->n[0] && e.node[1] < m->n[1] && e.node[2] < m->n[2];
         int a = e.axis, b = next_axis(a), c = prev_axis(a);
@@ -1159,13 +1205,37 @@ int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
         return std::make_tuple(e.node[0], e.field, e.axis, e.node[1], e.node[2]);
     };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    if (scheme == 2) {
+        // openEMS's poles come first on their edge (src/engine/dispersive.rs:
+        // 2195-2215: the OpenEmsPole list precedes the other entries).
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+            const int ox = d->entries[x].pole.kind == 2, oy = d->entries[y].pole.kind == 2;
+            return std::make_tuple(key(x), ox) < std::make_tuple(key(y), oy);
+        });
+    }
+    // Per edge (scheme 2): whether all of its poles are Debye poles, for
+    // openEMS's Debye update (with_openems_debye, electric edges only).
+    std::vector<char> all_debye(order.size(), 0);
+    if (scheme == 2)
+        for (size_t s0 = 0; s0 < order.size();) {
+            size_t s1 = s0;
+            bool deb = d->entries[order[s0]].field == 0;
+            while (s1 < order.size() && key(order[s1]) == key(order[s0])) {
+                deb = deb && d->entries[order[s1]].pole.kind == 2;
+                ++s1;
+            }
+            for (size_t t = s0; t < s1; ++t) all_debye[t] = deb;
+            s0 = s1;
+        }
     auto op = std::make_unique<OpStore>();
     op->kind = EMS_OP_POLES;
     const double dt = m->dt;
     bool have_last = false;
     std::tuple<uint64_t, int, int, uint64_t, uint64_t> last;
     bool skip_edge = false;
-    for (uint32_t q : order) {
+    double debye_f = 0.0;  // openEMS Debye edge: F of the edge's poles
+    for (size_t oi = 0; oi < order.size(); ++oi) {
+        const uint32_t q = order[oi];
         const Entry& e = d->entries[q];
         auto k = key(q);
         const bool new_edge = !have_last || last != k;
@@ -1195,6 +1265,52 @@ int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
             side.pole_end.push_back(side.pole_end.empty() ? 0 : side.pole_end.back());
         }
         const Pole& p = e.pole;
+        if (scheme == 2 && all_debye[oi]) {
+            // openems_debye_coefficients (src/engine/dispersive.rs:900-928):
+            // beta_p = cb·cp·de_p/(2·tau_p + dt) with cp = eps0·A*/l
+            // (openEMS's eps0), F = f32(1/(1 + sum beta)) over the edge.
+            const double cp = OE_EPS0 * geo;
+            auto beta = [&](const Pole& x) { return (double)coef * cp * x.p1 / (2.0 * x.p2 + dt); };
+            if (new_edge) {
+                double sum = 0.0;
+                for (size_t t = oi; t < order.size() && key(order[t]) == k; ++t) sum += beta(d->entries[order[t]].pole);
+                debye_f = (double)(float)(1.0 / (1.0 + sum));
+            }
+            side.kind.push_back(EMS_POLE_OPENEMS_DEBYE);
+            side.a.push_back(debye_f);
+            side.inv_c.push_back((double)(float)(1.0 - dt / (p.p2 + 0.5 * dt)));
+            side.inv_z.push_back((double)(float)beta(p));
+            side.half_l.push_back(0.0);
+            side.pole_end.back() += 1;
+            continue;
+        }
+        if (scheme == 2 && p.kind != 2) {
+            // OpenEmsPole::coefficients (src/engine/dispersive.rs:888-899):
+            // omega_p as given (the material's 2·pi·f_plasma), the edge's
+            // f32 coefficient vi and its f32 capacitance (inductance) with
+            // openEMS's vacuum constants (e_edge_circuit / h_edge_inductance,
+            // src/engine/coeffs.rs:776-810).
+            double circuit;
+            if (e.field == 0) {
+                double eps, kap;
+                edge_eps(m, a, e.node, eps, kap);
+                circuit = (double)(float)(OE_EPS0 * eps * geo);
+            } else {
+                double mu, sig;
+                edge_mu(m, a, e.node, mu, sig);
+                circuit = (double)(float)(OE_MU0 * mu * geo);
+            }
+            const double vi = (double)coef;
+            const double w0 = p.kind == 0 ? p.p2 : 0.0, gamma = p.kind == 0 ? p.p3 : p.p2;
+            const double half = gamma * dt / 2.0, dd = 1.0 + half, wp2 = p.p1 * p.p1;
+            side.kind.push_back(EMS_POLE_OPENEMS);
+            side.a.push_back((double)(float)((1.0 - half) / dd));
+            side.inv_c.push_back((double)(float)(w0 * w0 * dt / (wp2 * circuit * vi)));
+            side.inv_z.push_back((double)(float)(vi * dt * wp2 * circuit / dd));
+            side.half_l.push_back(0.0);
+            side.pole_end.back() += 1;
+            continue;
+        }
         double l = 0.0, r = 0.0, inv_c = 0.0;
         if (p.kind == 0) {  // Lorentz
             l = 1.0 / (mm * p.p1 * p.p1);
@@ -1426,19 +1542,21 @@ int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6],
     std::string bad;
     auto local = [&](int f, int t, int o, const std::array<uint64_t, 3>& node) -> float {
         const int a = f / 2;
+        const auto given = m->mur_v.find(f * 3 + t);
+        if (given != m->mur_v.end()) {
+            const int u = a == 0 ? 1 : 0, w = a == 2 ? 1 : 2;
+            const double v = given->second[node[u] * n[w] + node[w]];
+            if (v > 0.0) return (float)coefficient(v, dt, face_delta(f));
+        }
         const auto in = inner_of(f, node);
         auto hf = node;
         hf[a] = std::min(node[a], in[a]);
         const uint64_t pi[3] = {in[0], in[1], in[2]};
-        double cap = 0.0, cond = 0.0;
-        m->primary_edge_cg(t, pi, cap, cond);
-        const int tb = next_axis(t), tc = prev_axis(t);
-        const double eps = cap * (m->delta(t, in[t]) / (m->dual_delta(tb, in[tb]) * m->dual_delta(tc, in[tc]))) / EPS0;
+        double eps, kap;
+        edge_eps(m, t, pi, eps, kap);
         const uint64_t ph[3] = {hf[0], hf[1], hf[2]};
-        double l = 0.0, r = 0.0;
-        m->dual_edge_lr(o, ph, l, r);
-        const int ob = next_axis(o), oc = prev_axis(o);
-        const double mu = l * (m->dual_delta(o, hf[o]) / (m->delta(ob, hf[ob]) * m->delta(oc, hf[oc]))) / MU0;
+        double mu, sig;
+        edge_mu(m, o, ph, mu, sig);
         const double v = C0 / std::sqrt(eps * mu);
         if (!(std::isfinite(v) && v > 0.0)) {
             bad = "Mur boundary: local phase velocity must be finite and > 0";

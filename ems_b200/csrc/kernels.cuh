@@ -14,6 +14,7 @@ namespace emsk {
 
 constexpr unsigned kRowThreads = 128;  // threads of a z-row block
 constexpr uint32_t kMaxPoles = 16;     // poles per edge held in registers
+constexpr uint32_t kOeDebye = 1u << 31;  // PoleRun::oe: an edge of openEMS Debye poles
 
 struct Grid {
     uint32_t nx, ny, nz, pitch;  // pitch: padded z-row length (multiple of 32)
@@ -217,14 +218,21 @@ __global__ void k_poles_correct(const __grid_constant__ Grid g, const __grid_con
     float* fld = electric ? f.u[ax] : f.i[ax];
     const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
     const uint32_t p0 = e ? p.pole_end[e - 1] : 0u, p1 = p.pole_end[e];
-    const double prev = (double)p.prev[e];
+    const float prev_f = p.prev[e];
+    if (p.kind[p0] == 3) {  // openEMS Debye edge
+        fld[idx] = oe_debye_edge(p.a + p0, p.inv_c + p0, p.inv_z + p0, 1u, p.j + p0, p1 - p0, prev_f, fld[idx]);
+        return;
+    }
+    const double prev = (double)prev_f;
     const double half_prev = __dmul_rn(0.5, prev);
-    const double u_star = (double)fld[idx];
+    float u32 = fld[idx];
     double s = 0.0;
     bool trap = false;
     for (uint32_t q = p0; q < p1; ++q) {
         const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
-        if (p.kind[q] == 1) {  // leapfrog: j^{n+1/2} from u^n, then q^{n+1}
+        if (p.kind[q] == 2) {  // openEMS's f32 pole, before the others
+            u32 = oe_pole_step(a, ic, iz, p.j[q], p.q[q], prev_f, u32);
+        } else if (p.kind[q] == 1) {  // leapfrog: j^{n+1/2} from u^n, then q^{n+1}
             const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
             p.j[q] = jn;
             p.q[q] = __dadd_rn(qq, __dmul_rn(dt, jn));
@@ -234,12 +242,13 @@ __global__ void k_poles_correct(const __grid_constant__ Grid g, const __grid_con
             s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
         }
     }
+    const double u_star = (double)u32;
     const float u_new = (float)__ddiv_rn(__dsub_rn(u_star, __dmul_rn(cb, s)),
                                          __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), p.sum_inv_z[e])));
     if (trap) {
         const double half_new = __dmul_rn(0.5, (double)u_new);
         for (uint32_t q = p0; q < p1; ++q) {
-            if (p.kind[q] == 1) continue;
+            if (p.kind[q] != 0) continue;
             const double a = p.a[q], ic = p.inv_c[q], iz = p.inv_z[q], jq = p.j[q], qq = p.q[q];
             const double kk = __dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev);
             const double jb = __dmul_rn(__dadd_rn(kk, half_new), iz);
@@ -368,6 +377,7 @@ __device__ __forceinline__ double pole_energy_block(const PoleSideDev& e, const 
     for (int side = 0; side < 2; ++side) {
         const PoleSideDev& p = side == 0 ? e : h;
         for (size_t q = threadIdx.x; q < p.n_poles; q += blockDim.x) {
+            if (p.kind[q] >= 2) continue;  // openEMS's poles hold no energy
             const double a = __dmul_rn(__dmul_rn(p.half_l[q], p.j[q]), p.j[q]);
             const double b = __dmul_rn(__dmul_rn(__dmul_rn(0.5, p.inv_c[q]), p.q[q]), p.q[q]);
             s = __dadd_rn(s, __dadd_rn(a, b));
@@ -381,6 +391,7 @@ __global__ void __launch_bounds__(1024) k_pole_energy(PoleSideDev e, PoleSideDev
     for (int side = 0; side < 2; ++side) {
         const PoleSideDev& p = side == 0 ? e : h;
         for (size_t q = threadIdx.x; q < p.n_poles; q += blockDim.x) {
+            if (p.kind[q] >= 2) continue;  // openEMS's poles hold no energy
             const double a = __dmul_rn(__dmul_rn(p.half_l[q], p.j[q]), p.j[q]);
             const double b = __dmul_rn(__dmul_rn(__dmul_rn(0.5, p.inv_c[q]), p.q[q]), p.q[q]);
             s = __dadd_rn(s, __dadd_rn(a, b));

@@ -336,19 +336,28 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
     const uint32_t idx = __ldg(p.node + e);
     const int ax = (int)__ldg(p.axis + e);
     const uint32_t p0 = e ? __ldg(p.pole_end + e - 1) : 0u;
-    const double prev = (double)p.prev[e];
+    const float prev32 = p.prev[e];
+    const double prev = (double)prev32;
     float* fld = electric ? f.u[ax] : f.i[ax];
-    const double u_star = (double)fld[idx];
+    float u32 = fld[idx];
     const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
     const double j0 = p.j[p0], q0 = p.q[p0];
     const PoleRun R = runs[r];
     const double half_prev = __dmul_rn(0.5, prev);
     const double* cs = sets + R.set;
+    if (R.oe & kOeDebye) {
+        const float u_new = oe_debye_edge(cs, cs + 1, cs + 2, 3u, p.j + p0, R.np, prev32, u32);
+        fld[idx] = u_new;
+        if (save_prev) p.prev[e] = u_new;
+        return;
+    }
     double s = 0.0;
     for (uint32_t q = 0; q < R.np; ++q) {
         const double a = cs[3 * q], ic = cs[3 * q + 1], iz = cs[3 * q + 2];
         const double jq = q ? p.j[p0 + q] : j0, qq = q ? p.q[p0 + q] : q0;
-        if ((R.kinds >> q) & 1u) {
+        if ((R.oe >> q) & 1u) {
+            u32 = oe_pole_step(a, ic, iz, p.j[p0 + q], p.q[p0 + q], prev32, u32);
+        } else if ((R.kinds >> q) & 1u) {
             const double jn = __dadd_rn(__dmul_rn(a, jq), __dmul_rn(iz, __dsub_rn(prev, __dmul_rn(qq, ic))));
             p.j[p0 + q] = jn;
             p.q[p0 + q] = __dadd_rn(qq, __dmul_rn(dt, jn));
@@ -357,7 +366,7 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
             s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
         }
     }
-    const float u_new = (float)__ddiv_rn(__dsub_rn(u_star, __dmul_rn(cb, s)),
+    const float u_new = (float)__ddiv_rn(__dsub_rn((double)u32, __dmul_rn(cb, s)),
                                          __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
     if (R.kinds != (1u << R.np) - 1u) {
         const double half_new = __dmul_rn(0.5, (double)u_new);

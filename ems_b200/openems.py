@@ -283,6 +283,7 @@ class OpenEmsFile:
     mur_velocity: float | None
     props: list
     background: dict | None = None
+    cell_constant: bool = False   # CellConstantMaterial: cell-centre materials
 
 
 def _f(x, default=None):
@@ -375,7 +376,7 @@ def parse(text: str) -> OpenEmsFile:
     # openEMS does).
     os_ = int(float(fd.get("OverSampling", "4")))
     end = float(fd.get("endCriteria", "0"))
-    end = 1e-5 if end == 0.0 else (None if end < 0 else end)
+    end = 1e-6 if end == 0.0 else (None if end < 0 else end)  # openEMS default: -60 dB
     factor = float(fd.get("TimeStepFactor", "1"))
     method = int(float(fd.get("TimeStepMethod", "3")))
     bg = cs.find("BackgroundMaterial")
@@ -386,7 +387,8 @@ def parse(text: str) -> OpenEmsFile:
                        _f(fd.get("MaxTime")), _f(fd.get("TimeStep")),
                        factor if 0.0 < factor <= 1.0 else 1.0, method if method in (1, 3) else 1,
                        os_ if os_ >= 2 else 4, sig, faces, mur_v, props,
-                       dict(bg.attrib) if bg is not None else None)
+                       dict(bg.attrib) if bg is not None else None,
+                       fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"))
 
 
 # ---------------------------------------------------------------------------
@@ -507,7 +509,13 @@ class Setup:
         m = Model(*lines_m)
         self.lines_m = lines_m
         m.faces([PMC if k == PMC_FACE else PEC for k, _ in f.faces])
+        # openEMS's inside tolerance of metal, material and excitation
+        # primitives: 1e-3 of the smallest cell width, drawing units.
+        self.tol = 1e-3 * min(float(np.min(np.diff(v))) for v in f.lines if len(v) > 1)
+        self.lumped_edges = {(a, *e) for a, edges in self._lumped_boxes() for e in edges}
         self._materials(m)
+        if not f.cell_constant:
+            self._sampled_materials(m)
         # Time step: openEMS's criterion, TimeStepFactor, or TimeStep.
         if f.timestep is not None:
             base = f.timestep
@@ -544,6 +552,131 @@ class Setup:
         tol = 1e-9 * max(1.0, abs(hi - lo), abs(self.file.lines[a][-1] - self.file.lines[a][0]))
         return lo - tol <= x <= hi + tol
 
+    def _inside_prim(self, x, lo, hi):
+        """Closed inside test of metal, materials and excitations with the
+        tolerance ``self.tol`` (src/compile/openems.rs:5-30)."""
+        return lo - self.tol <= x <= hi + self.tol
+
+    def _sampled_materials(self, m):
+        """Edge materials from point samples the openEMS way (csx's
+        sub-cell discretisation with openEMS's rules, src/compile/
+        openems.rs:36-60 and 83-98): an E edge along a averages eps_r and
+        kappa over the quarters of its dual face, sampled at the edge's
+        midpoint along a and a quarter of the adjacent cell widths either
+        side in the other axes, area-weighted; an H dual edge along a
+        combines mu_r over the two halves of the dual edge, sampled at the
+        face centre across and at x_n -+ dx/4 along a, length-weighted
+        harmonic, and sigma_m by openEMS's rule (harmonic, a lossless upper
+        half gives 0, a lossless lower half is left out). Each sample takes
+        the highest-priority material containing it (closed, with the
+        inside tolerance; at equal priority the one defined first), metal
+        not counted, else the background. Faces of the domain see their
+        in-domain parts only."""
+        f = self.file
+        n = self.nodes
+        lines = [np.asarray(v, dtype=np.float64) for v in f.lines]
+        d = [np.diff(v) for v in lines]
+        bg = f.background
+        props = []
+        items = []
+        for p in f.props:
+            if p.kind not in MATERIALS:
+                continue
+            iso = p.attrs.get("Isotropy", "1") != "0"
+            props.append([_vec3(p.prop.get(k), dv, iso) for k, dv in
+                          (("Epsilon", 1.0), ("Kappa", 0.0), ("Mue", 1.0), ("Sigma", 0.0))])
+            for b in p.boxes:
+                items.append((b.priority, -p.order, len(props) - 1, b))
+        items.sort(key=lambda t: (t[0], t[1]))
+        base = ([_vec3(bg.get(k), dv, True) for k, dv in
+                 (("Epsilon", 1.0), ("Kappa", 0.0), ("Mue", 1.0), ("Sigma", 0.0))]
+                if bg else [[1.0] * 3, [0.0] * 3, [1.0] * 3, [0.0] * 3])
+        table = np.array([base] + props, dtype=np.float64)  # [prop, quantity, axis]
+
+        def winner(xs):
+            """Property index (0 background) on the grid of coordinates xs."""
+            idx = np.zeros([len(x) for x in xs], dtype=np.int64)
+            for _, _, pi, b in items:
+                ins = []
+                for q in range(3):
+                    lo, hi = min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])
+                    ins.append((xs[q] >= lo - self.tol) & (xs[q] <= hi + self.tol))
+                mask = ins[0][:, None, None] & ins[1][None, :, None] & ins[2][None, None, :]
+                idx[mask] = pi + 1
+            return idx
+
+        def sides(q):
+            """Sample coordinates and weights of the lower and upper halves
+            around each node line of axis q (weight 0 outside)."""
+            x = lines[q]
+            lo_w = np.zeros(n[q])
+            hi_w = np.zeros(n[q])
+            lo_x = x.copy()
+            hi_x = x.copy()
+            if n[q] > 1:
+                lo_w[1:] = 0.5 * d[q]
+                hi_w[:-1] = 0.5 * d[q]
+                lo_x[1:] = x[1:] - 0.25 * d[q]
+                hi_x[:-1] = x[:-1] + 0.25 * d[q]
+            return [(lo_x, lo_w), (hi_x, hi_w)]
+
+        def centres(q):
+            x = lines[q]
+            c = np.ones(n[q]) * x[-1]
+            if n[q] > 1:
+                c[:-1] = 0.5 * (x[:-1] + x[1:])
+            return c
+
+        for a in range(3):
+            b, c = (a + 1) % 3, (a + 2) % 3
+            # E edges along a.
+            num_e = np.zeros(n)
+            num_k = np.zeros(n)
+            den = np.zeros(n)
+            for xb, wb in sides(b):
+                for xc, wc in sides(c):
+                    xs = [None] * 3
+                    xs[a], xs[b], xs[c] = centres(a), xb, xc
+                    w = np.ones(n)
+                    shape = [1, 1, 1]
+                    shape[b] = n[b]
+                    w = w * wb.reshape(shape)
+                    shape = [1, 1, 1]
+                    shape[c] = n[c]
+                    w = w * wc.reshape(shape)
+                    pid = winner(xs)
+                    num_e += w * table[pid, 0, a]
+                    num_k += w * table[pid, 1, a]
+                    den += w
+            ok = den > 0
+            eps = np.where(ok, num_e / np.where(ok, den, 1.0), 1.0)
+            kap = np.where(ok, num_k / np.where(ok, den, 1.0), 0.0)
+            m.set_edge_materials(0, a, eps, kap)
+            # H dual edges along a.
+            length = np.zeros(n)
+            inv_mu = np.zeros(n)
+            inv_sg = np.zeros(n)
+            hi_zero = np.zeros(n, dtype=bool)
+            for side, (xa, wa) in enumerate(sides(a)):
+                xs = [None] * 3
+                xs[a], xs[b], xs[c] = xa, centres(b), centres(c)
+                shape = [1, 1, 1]
+                shape[a] = n[a]
+                w = np.broadcast_to(wa.reshape(shape), n)
+                pid = winner(xs)
+                mu = table[pid, 2, a]
+                sg = table[pid, 3, a]
+                has = w > 0
+                length += w
+                inv_mu += np.where(has, w / mu, 0.0)
+                inv_sg += np.where(has & (sg != 0.0), w / np.where(sg != 0.0, sg, 1.0), 0.0)
+                if side == 1:
+                    hi_zero |= has & (sg == 0.0)
+            ok = length > 0
+            mu_e = np.where(ok, length / np.where(ok, inv_mu, 1.0), 1.0)
+            sg_e = np.where(ok & ~hi_zero & (inv_sg > 0), length / np.where(inv_sg > 0, inv_sg, 1.0), 0.0)
+            m.set_edge_materials(1, a, mu_e, sg_e)
+
     def _materials(self, m):
         f = self.file
         mats = [p for p in f.props if p.kind in ("Metal",) + MATERIALS]
@@ -572,17 +705,17 @@ class Setup:
                     rng = []
                     for q in range(3):
                         pts = cen[q] if q == a else np.array(lines[q])
-                        rng.append([i for i, x in enumerate(pts) if self._inside(q, x, lo[q], hi[q])])
+                        rng.append([i for i, x in enumerate(pts) if self._inside_prim(x, lo[q], hi[q])])
                     if not all(rng):
                         continue
                     for i in rng[0]:
                         for j in rng[1]:
                             run = []
                             for k in rng[2] + [None]:
-                                keep = k is not None
+                                keep = k is not None and (a, i, j, k) not in self.lumped_edges
                                 if keep and over:
                                     mid = [cen[q][x] if q == a else lines[q][x] for q, x in enumerate((i, j, k))]
-                                    keep = not any(all(self._inside(q, mid[q], min(ob.p1[q], ob.p2[q]),
+                                    keep = not any(all(self._inside_prim(mid[q], min(ob.p1[q], ob.p2[q]),
                                                                     max(ob.p1[q], ob.p2[q])) for q in range(3))
                                                    for ob, _ in over)
                                 if keep and run and k == run[-1] + 1:
@@ -599,26 +732,16 @@ class Setup:
             cs = m.cells().box([c[0] for c in cells], [c[-1] + 1 for c in cells])
             m.fill(cs, mat)
 
-    def _lumped(self, m):
-        """Parallel R/C lumped elements the openEMS way (src/sim/map.rs:
-        46-255, 1525-1680): spread like a homogeneous material over their
-        E edges (G_e = g_e·S/R, C_e = g_e·C·S with g_e the edge's dual
-        face over its length, outer lines counting full cells, and
-        S = Σ over positions along the element of 1/Σ g_e), their R and C
-        replacing the medium's conductance and capacitance, and PEC caps
-        on the two end planes (Caps, the default)."""
-        f = self.file
-        n, lines = self.nodes, f.lines
-        for p in f.props:
+    def _lumped_boxes(self):
+        """(axis, edges) of every lumped element: the E edges along its
+        direction whose both nodes lie in one of its boxes (closed, the
+        boxes snap to the mesh)."""
+        out = []
+        n, lines = self.nodes, self.file.lines
+        for p in self.file.props:
             if p.kind != "LumpedElement":
                 continue
             a = int(float(p.attrs.get("Direction", "0")))
-            r = _f(p.attrs.get("R"))
-            c = _f(p.attrs.get("C"))
-            if p.attrs.get("L") is not None or p.attrs.get("LEtype", "0") not in ("0", "-1"):
-                raise NotImplementedError(f"lumped element {p.name!r}: inductors and series elements")
-            r = r if r is not None and r > 0 and math.isfinite(r) else None
-            c = c if c is not None and c > 0 and math.isfinite(c) else None
             edges = []
             for b in p.boxes:
                 lo = [min(b.p1[q], b.p2[q]) for q in range(3)]
@@ -627,16 +750,48 @@ class Setup:
                         if self._inside(q, lines[q][i], lo[q], hi[q])
                         and (q != a or self._inside(q, lines[q][i + 1], lo[q], hi[q]))] for q in range(3)]
                 edges += [(i, j, k) for i in rng[0] for j in rng[1] for k in rng[2]]
+            out.append((a, edges))
+        return out
+
+    def _lumped(self, m):
+        """Parallel R/C lumped elements the openEMS way (src/sim/map.rs:
+        46-255, 540-600, 1525-1680): spread like a homogeneous material
+        over their E edges (G_e = g_e·S/R, C_e = g_e·C·S with g_e the edge's
+        dual face over its length, outer lines counting full cells, and
+        S = Σ over positions along the element of 1/Σ g_e), their R and C
+        replacing the medium's conductance and capacitance, and PEC caps
+        on the two end planes over the element's whole box (Caps, the
+        default). The element's own edges are its own whatever metal lies
+        there (they take the medium under the metal,
+        src/compile/openems.rs:69-81); on edges inside a PML layer the
+        layer replaces the update, so the element's R and C act only
+        outside it, spread over all its edges all the same."""
+        f = self.file
+        n = self.nodes
+        boxes = iter(self._lumped_boxes())
+        for p in f.props:
+            if p.kind != "LumpedElement":
+                continue
+            a, edges = next(boxes)
+            r = _f(p.attrs.get("R"))
+            c = _f(p.attrs.get("C"))
+            if p.attrs.get("L") is not None or p.attrs.get("LEtype", "0") not in ("0", "-1"):
+                raise NotImplementedError(f"lumped element {p.name!r}: inductors and series elements")
+            r = r if r is not None and r > 0 and math.isfinite(r) else None
+            c = c if c is not None and c > 0 and math.isfinite(c) else None
             ca, cb = m.coeff(a), m.coeff(3 + a)
-            kept = []
+            kept, layer = [], []
             for e in edges:
                 if cb[e] == 0.0:
                     self.warnings.append(f"lumped element {p.name!r}: edge {e} is PEC (shorted); ignored")
                 elif ca[e] == 0.0:  # inside a PML layer: the layer replaces the update
-                    self.warnings.append(f"lumped element {p.name!r}: edge {e} inside a PML layer; ignored")
+                    layer.append(e)
                 else:
                     kept.append(e)
-            if not kept or (r is None and c is None):
+            if layer:
+                self.warnings.append(f"lumped element {p.name!r}: {len(layer)} of its {len(kept) + len(layer)} "
+                                     "edge(s) lie inside a PML layer and are ignored there")
+            if not kept + layer or (r is None and c is None):
                 continue
 
             # openems_edge_geometry (src/sim/map.rs:164-218).
@@ -648,17 +803,17 @@ class Setup:
                     area *= self.model_dual(t, e[t]) * (2.0 if e[t] in (0, n[t] - 1) else 1.0)
                 return area / self.model_delta(a, e[a])
 
-            w = {e: geo(e) for e in kept}
+            w = {e: geo(e) for e in kept + layer}
             per = {}
-            for e in kept:
+            for e in kept + layer:
                 per[e[a]] = per.get(e[a], 0.0) + w[e]
             S = sum(1.0 / x for x in per.values())
             for e in kept:
                 m.set_edge_circuit(a, e, cap=c * w[e] * S if c is not None else -1.0,
                                    cond=1.0 / (r / (w[e] * S)) if r is not None else -1.0)
             if p.attrs.get("Caps", "1") != "0":
-                lo = [min(e[q] for e in kept) for q in range(3)]
-                hi = [max(e[q] + (1 if q == a else 0) for e in kept) for q in range(3)]
+                lo = [min(e[q] for e in kept + layer) for q in range(3)]
+                hi = [max(e[q] + (1 if q == a else 0) for e in kept + layer) for q in range(3)]
                 for t in range(3):
                     if t == a or hi[t] == lo[t]:
                         continue
@@ -679,7 +834,7 @@ class Setup:
             if p.kind not in MATERIALS + ("Metal",):
                 continue
             for b in p.boxes:
-                if all(self._inside(q, pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
+                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
                     key = (b.priority, -p.order)
                     if best is None or key > best[0]:
                         best = (key, p)
@@ -687,13 +842,14 @@ class Setup:
 
     def _dispersive(self, m):
         """Lorentz, Drude and Debye poles the openEMS way (src/compile/
-        dispersive.rs:1-130): every E edge (H dual edge) gets the full poles
-        of the dispersive property winning at its midpoint (the centre of
-        the face it pierces), ω_p = 2π·f_plasma·√ε_e with the edge's own
-        averaged static ε_e (μ_e), ω_0 = 2π·f_Lor, γ = 1/τ; Debye Δε, τ as
-        given, dropped below three time steps; integrated with the leapfrog
-        scheme."""
-        from . import LEAPFROG, Dispersive, Pole
+        dispersive.rs:1-130, 480-560): every E edge (H dual edge) gets the
+        full poles of the dispersive property winning at its midpoint (the
+        centre of the face it pierces), ω_p = 2π·f_plasma, ω_0 = 2π·f_Lor,
+        γ = 1/τ, Debye Δε, τ as given, dropped below three time steps; all
+        with openEMS's f32 arithmetic (OpenEmsPole with the edge's own
+        capacitance or inductance, openEMS's Debye update on edges of Debye
+        poles alone)."""
+        from . import OPENEMS_POLES, Dispersive, Pole
         f = self.file
         disp = [p for p in f.props if p.kind in ("LorentzMaterial", "DebyeMaterial")]
         if not disp:
@@ -741,12 +897,11 @@ class Setup:
                             w = self._winner(pt)
                             if w is None or w.kind not in ("LorentzMaterial", "DebyeMaterial"):
                                 continue
-                            inf = m.edge_material(field_, a, node)[0]
-                            for pole in self._poles(w, field_, a, inf):
+                            for pole in self._poles(w, field_, a, 1.0):
                                 d.add_edge(field_, a, node, pole)
                                 count += 1
         if count:
-            m.add_dispersive(d, LEAPFROG)
+            m.add_dispersive(d, OPENEMS_POLES)
 
     def _poles(self, p, field_, a, inf):
         from . import Pole
@@ -808,10 +963,28 @@ class Setup:
                     lo[t] = hi[t] = layer
                     m.zero_edges(field_, a, lo, hi)
 
+    def _excitation_winner(self, pt):
+        """The excitation property that owns point ``pt``: the highest
+        priority containing it, ties to the one defined first, disabled
+        ones included (excitation_priority, src/compile/openems.rs:
+        245-300)."""
+        best = None
+        for p in self.file.props:
+            if p.kind != "Excitation":
+                continue
+            for b in p.boxes:
+                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
+                    key = (b.priority, -p.order)
+                    if best is None or key > best[0]:
+                        best = (key, p)
+        return best[1] if best else None
+
     def _excitation_edges(self):
         """(E?, axis, node, weight per unit amplitude, property) of every
         driven edge: E edges whose both nodes lie in the closed box, H dual
-        edges whose midpoint does; weight = Excite × (dual) edge length."""
+        edges whose midpoint does; weight = Excite × (dual) edge length.
+        openEMS gives each edge to one excitation: the one owning the edge
+        midpoint (E types) or the dual edge's (H types)."""
         out = []
         f = self.file
         n = self.nodes
@@ -834,14 +1007,14 @@ class Setup:
                     for q in range(3):
                         if e_type:
                             pts = [i for i in range(n[q] - (1 if q == a else 0))
-                                   if self._inside(q, lines[q][i], lo[q], hi[q])
-                                   and (q != a or self._inside(q, lines[q][i + 1], lo[q], hi[q]))]
+                                   if self._inside_prim(lines[q][i], lo[q], hi[q])
+                                   and (q != a or self._inside_prim(lines[q][i + 1], lo[q], hi[q]))]
                         else:
                             if q == a:
-                                pts = [i for i in range(n[q]) if self._inside(q, lines[q][i], lo[q], hi[q])]
+                                pts = [i for i in range(n[q]) if self._inside_prim(lines[q][i], lo[q], hi[q])]
                             else:
                                 pts = [i for i in range(n[q] - 1)
-                                       if self._inside(q, 0.5 * (lines[q][i] + lines[q][i + 1]), lo[q], hi[q])]
+                                       if self._inside_prim(0.5 * (lines[q][i] + lines[q][i + 1]), lo[q], hi[q])]
                         rng.append(pts)
                     for i in rng[0]:
                         for j in rng[1]:
@@ -851,6 +1024,11 @@ class Setup:
                                     length = self.model_delta(a, node[a])
                                 else:
                                     length = self.model_dual(a, node[a])
+                                mid = [0.5 * (lines[q][node[q]] + lines[q][node[q] + 1])
+                                       if ((q == a) == e_type) and node[q] + 1 < n[q] else lines[q][node[q]]
+                                       for q in range(3)]
+                                if self._excitation_winner(mid) is not p:
+                                    continue
                                 out.append((e_type, typ, a, node, exc[a] * length, p))
         return out
 
@@ -884,7 +1062,50 @@ class Setup:
             if held:
                 steps = int(math.floor(2.0 * f.signal.delay / self.dt)) + 1
                 hold = {fc: steps + 10 for fc in held}
+        self._mur_media(m, [fc for fc, v in faces.items() if v is None])
         m.add_mur(faces, hold=hold, flags=MUR_COUNT_ENERGY | MUR_OPENEMS_CORNERS | MUR_OPENEMS_ORDER)
+
+    def _mur_media(self, m, faces):
+        """The medium of each edge of a Mur face without a phase velocity
+        the openEMS way (mur_point_media, src/compile/mod.rs:1641-1699): the
+        material at one point, the edge's start node across and the middle
+        of the boundary cell along the normal (closed, metal not counted),
+        ε along the edge and μ along the other tangential axis,
+        v = c0/√(εμ)."""
+        f = self.file
+        n = self.nodes
+        lines = f.lines
+        mats = [p for p in f.props if p.kind in MATERIALS]
+        for fc in faces:
+            a = fc // 2
+            plane, inner = (n[a] - 1, n[a] - 2) if fc % 2 else (0, 1)
+            mid = 0.5 * (lines[a][plane] + lines[a][inner])
+            u, w = [q for q in range(3) if q != a]
+            for t in (u, w):
+                o = w if t == u else u
+                v = np.zeros((n[u], n[w]))
+                for pu in range(n[u]):
+                    for pw in range(n[w]):
+                        node = [0, 0, 0]
+                        node[a], node[u], node[w] = plane, pu, pw
+                        if node[t] + 1 >= n[t]:
+                            continue
+                        pt = [lines[q][node[q]] for q in range(3)]
+                        pt[a] = mid
+                        best = None
+                        for p in mats:
+                            for b in p.boxes:
+                                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q]))
+                                       for q in range(3)):
+                                    key = (b.priority, -p.order)
+                                    if best is None or key > best[0]:
+                                        best = (key, p)
+                        prop = best[1].prop if best else f.background
+                        iso = best[1].attrs.get("Isotropy", "1") != "0" if best else True
+                        eps = _vec3(prop.get("Epsilon"), 1.0, iso)[t] if prop else 1.0
+                        mu = _vec3(prop.get("Mue"), 1.0, iso)[o] if prop else 1.0
+                        v[pu, pw] = C0 / math.sqrt(eps * mu)
+                m.set_mur_media(fc, t, v)
 
     def _excitations(self, m):
         from . import HARD_E, HARD_H, SOFT_E, SOFT_H

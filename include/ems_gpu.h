@@ -82,8 +82,20 @@ typedef struct {
     const ems_cpml_slab* slabs; /* E and H slabs, in layer order */
 } ems_cpml;
 
-/* Pole kinds of one dispersive branch (src/engine/dispersive.rs:961-971). */
-typedef enum { EMS_POLE_TRAPEZOIDAL = 0, EMS_POLE_LEAPFROG = 1 } ems_pole_kind;
+/* Pole kinds of one dispersive branch (src/engine/dispersive.rs:961-971):
+ * trapezoidal, leapfrog, openEMS's f32 leapfrog of a Lorentz/Drude pole
+ * (OpenEmsPole, dispersive.rs:846-899: a = A, inv_c = K, inv_z = B, state
+ * j = V, q = W; applied before the edge's other poles) and openEMS's f32
+ * Debye update of an edge whose poles are all of that kind
+ * (with_openems_debye, dispersive.rs:1824-1857: a = F, inv_c = 1 - g,
+ * inv_z = b, state j = Q). The two openEMS kinds hold f32 values in the f64
+ * arrays, carry no energy (half_l = 0) and add nothing to sum_inv_z. */
+typedef enum {
+    EMS_POLE_TRAPEZOIDAL = 0,
+    EMS_POLE_LEAPFROG = 1,
+    EMS_POLE_OPENEMS = 2,
+    EMS_POLE_OPENEMS_DEBYE = 3
+} ems_pole_kind;
 
 /* The poles of one field type (electric: E edges; magnetic: H dual edges)
  * of a dispersive medium (src/engine/dispersive.rs:973-1041, Side). Edges

@@ -66,6 +66,21 @@ int ems_model_pec_edges(ems_model* m, int axis, const uint64_t lo[3], const uint
  * (0 PEC, 1 PMC); default all PEC (FaceConditions, src/engine/coeffs.rs). */
 int ems_model_faces(ems_model* m, const int faces[6]);
 
+/* Phase velocities [m/s] of the edges along `axis` on Mur `face` (0 x_min,
+ * 1 x_max, ... 5 z_max) for a face in local-medium mode, in place of the
+ * medium of the edges next to it (MurMedia, src/engine/boundary/mur.rs:
+ * 140-180): one value per node of the face plane, index p[u]·n[w] + p[w]
+ * with u < w the two other axes; 0 keeps the local medium. Before
+ * ems_model_add_mur. */
+int ems_model_set_mur_media(ems_model* m, int face, int axis, const double* v);
+
+/* Per-edge materials in place of the averages of the cells (EdgeMaterials,
+ * src/engine/edge_material.rs:19-67, the form a sub-cell rasteriser such as
+ * csx::discretize produces): for the E edges along `axis` (field 0: v0 =
+ * eps_r, v1 = kappa) or the H dual edges (field 1: v0 = mu_r, v1 = sigma_m),
+ * one value per node in reference layout. Before build. */
+int ems_model_set_edge_materials(ems_model* m, int field, int axis, const double* v0, const double* v1);
+
 /* Computes dt = courant * courant_limit (TimeStep::Courant) or, with
  * fixed_dt > 0, takes it (TimeStep::Fixed), then the coefficients
  * (Coefficients::compute). Must precede the operators. */
@@ -132,7 +147,11 @@ int ems_dispersive_add_edge(ems_dispersive* d, int field, int axis, const uint64
  * dual edge (field 1: mu_r, sigma_m) along `axis` at `node`
  * (EdgeMaterials::from_cells, src/engine/edge_material.rs:376-413). */
 int ems_model_edge_material(const ems_model* m, int field, int axis, const uint64_t node[3], double out[2]);
-/* Installs the medium with scheme 0 trapezoidal / 1 leapfrog; op index. */
+/* Installs the medium with scheme 0 trapezoidal / 1 leapfrog / 2 openEMS's
+ * f32 arithmetic (OpenEmsPole for Lorentz and Drude poles, given the
+ * material's own omega_p, applied first on their edge; openEMS's Debye
+ * update on electric edges whose poles are all Debye poles; other Debye
+ * poles trapezoidal; src/engine/dispersive.rs:846-960); op index. */
 int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme);
 
 /* Waveforms: 0 Gaussian (f0, fc; src/waveform.rs Waveform::Gaussian). */

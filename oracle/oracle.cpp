@@ -375,13 +375,41 @@ struct oracle_engine {
             const size_t idx = p.node[e];
             const double cb = (double)(electric ? co[3 + ax][idx] : co[9 + ax][idx]);
             const size_t p0 = e ? p.pole_end[e - 1] : 0, p1 = p.pole_end[e];
-            const double prev = (double)p.prev[e];
+            const float prev32 = p.prev[e];
+            if (p1 > p0 && p.kind[p0] == EMS_POLE_OPENEMS_DEBYE) {
+                // openems_debye_step (src/engine/dispersive.rs:930-960): the
+                // explicit halves P first, their increments summed in pole
+                // order, then u_new = F·(u* − S) and Q = P + b·u_new; every
+                // operation f32, flushed.
+                const float F = (float)p.a[p0], us = f[idx];
+                float sum = 0.0f;
+                for (size_t q = p0; q < p1; ++q) {
+                    const float om = (float)p.inv_c[q], b = (float)p.inv_z[q], Q = (float)p.j[q];
+                    const float P = flush(flush(om * Q) + flush(b * prev32));
+                    sum = flush(sum + flush(P - Q));
+                    p.j[q] = P;
+                }
+                const float un = flush(F * flush(us - sum));
+                for (size_t q = p0; q < p1; ++q) p.j[q] = flush((float)p.j[q] + flush((float)p.inv_z[q] * un));
+                f[idx] = flush(us - flush(us - un));
+                continue;
+            }
+            const double prev = (double)prev32;
             const double half_prev = 0.5 * prev;
-            const double u_star = (double)f[idx];
+            float u32 = f[idx];
             double s = 0.0;
             double nj[64], nq[64];
             for (size_t q = p0; q < p1; ++q) {
-                if (p.kind[q] == EMS_POLE_LEAPFROG) {
+                if (p.kind[q] == EMS_POLE_OPENEMS) {
+                    // OpenEmsPole (src/engine/dispersive.rs:846-899, 1414-1425):
+                    // V <- A·V + B·(u^n − W), W <- W + K·V, u <- u − V (f32).
+                    const float A = (float)p.a[q], K = (float)p.inv_c[q], B = (float)p.inv_z[q];
+                    const float w = (float)p.q[q];
+                    const float v = flush(flush(A * (float)p.j[q]) + flush(B * flush(prev32 - w)));
+                    nj[q - p0] = v;
+                    nq[q - p0] = flush(w + flush(K * v));
+                    u32 = flush(u32 - v);
+                } else if (p.kind[q] == EMS_POLE_LEAPFROG) {
                     double jn = p.a[q] * p.j[q] + p.inv_z[q] * (prev - p.q[q] * p.inv_c[q]);
                     nj[q - p0] = jn;
                     nq[q - p0] = p.q[q] + dt * jn;
@@ -390,10 +418,11 @@ struct oracle_engine {
                     s += (p.a[q] * p.j[q] - p.q[q] * p.inv_c[q] + half_prev) * p.inv_z[q];
                 }
             }
+            const double u_star = (double)u32;
             const float u_new = (float)((u_star - cb * s) / (1.0 + 0.5 * cb * p.sum_inv_z[e]));
             const double half_new = 0.5 * (double)u_new;
             for (size_t q = p0; q < p1; ++q) {
-                if (p.kind[q] == EMS_POLE_LEAPFROG) {
+                if (p.kind[q] == EMS_POLE_LEAPFROG || p.kind[q] == EMS_POLE_OPENEMS) {
                     p.j[q] = nj[q - p0];
                     p.q[q] = nq[q - p0];
                 } else {
@@ -418,7 +447,7 @@ struct oracle_engine {
     // Σ ½·L·j² + ½·q²/C_p in pole order (src/engine/dispersive.rs:1488-1506).
     static void pole_energy(const PoleSide& p, double& w) {
         for (size_t q = 0; q < p.kind.size(); ++q)
-            w += p.half_l[q] * p.j[q] * p.j[q] + 0.5 * p.inv_c[q] * p.q[q] * p.q[q];
+            if (p.kind[q] < EMS_POLE_OPENEMS) w += p.half_l[q] * p.j[q] * p.j[q] + 0.5 * p.inv_c[q] * p.q[q] * p.q[q];
     }
 
     double operator_energy() const {

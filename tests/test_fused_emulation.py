@@ -94,6 +94,8 @@ def run_oracle(m, state, steps):
     ((12, 11, 9), 4, 3, E.LEAPFROG),
     ((17, 14, 40), 6, 2, E.TRAPEZOIDAL),
     ((21, 7, 33), 4, 5, E.LEAPFROG),
+    ((12, 11, 9), 4, 3, E.OPENEMS_POLES),
+    ((17, 14, 40), 6, 2, E.OPENEMS_POLES),
 ])
 def test_fused_kernel_source_equals_oracle(n, tj, grid, scheme):
     m = model(n, scheme, graded=tj == 4)
@@ -113,6 +115,7 @@ def test_fused_kernel_source_equals_oracle(n, tj, grid, scheme):
     ((9, 10, 13), E.TRAPEZOIDAL, True),
     ((12, 11, 35), E.LEAPFROG, True),
     ((10, 9, 8), E.LEAPFROG, False),
+    ((12, 11, 35), E.OPENEMS_POLES, True),
 ])
 def test_two_kernel_source_equals_oracle(n, scheme, magnetic):
     m = model(n, scheme, magnetic=magnetic)

@@ -12,6 +12,7 @@ and the final fields agree bit for bit. The oracle itself is checked
 against openEMS's own output for the same features in
 test_openems_fixtures.py. Also the command-line entry point.
 """
+import math
 import os
 
 import numpy as np
@@ -197,6 +198,42 @@ def test_openems_models_bit_exact(name, text, schedule):
         assert text_g.splitlines()[1:] == ro.files()[k].splitlines()[1:], (name, k)
     assert_fields_equal(g, o, f"openEMS model {name}")
     assert any(np.any(v != 0) for v in rg.series.values())
+
+
+@pytest.mark.parametrize("schedule", [1, 2, 3, 4, 5])
+def test_openems_pole_arithmetic(schedule):
+    """openEMS's f32 pole kinds on every schedule: Lorentz and Drude poles
+    (OpenEmsPole) alone, with a trapezoidal Debye pole on the same edges
+    (applied first), edges of Debye poles alone (openEMS's Debye update),
+    magnetic poles, beside CPML layers: fields bit for bit with the oracle,
+    energies (which leave these poles out) within 1e-12."""
+    rng = np.random.default_rng(5)
+    lines = [np.cumsum(np.concatenate([[0.0], 1e-3 * (1.0 + 0.3 * rng.random(c))])) for c in (16, 13, 21)]
+    m = E.Model(*lines)
+    m.fill(m.cells().box([3, 3, 3], [12, 10, 17]), m.material(eps_r=2.0, mu_r=1.3, kappa=0.01))
+    m.build()
+    m.add_cpml([3, 0, 3, 3, 0, 4], kappa_max=1.5, alpha_max=0.02)
+    d = E.Dispersive()
+    lor = m.cells().box([4, 4, 4], [11, 9, 12])
+    d.fill_cells(m, lor, [E.Pole.lorentz(3e10, 2e10, 1e9), E.Pole.drude(2e10, 4e9)])
+    d.fill_cells(m, m.cells().box([8, 2, 9], [14, 8, 16]), [E.Pole.debye(1.5, 2e-11), E.Pole.debye(0.7, 5e-11)])
+    d.fill_cells(m, m.cells().box([2, 5, 5], [9, 11, 10]), [E.Pole.drude(1e10, 3e9)], field=1)
+    m.add_dispersive(d, E.OPENEMS_POLES)
+    f0, fc = 10e9, 8e9
+    amp = [math.exp(-((k * m.dt - 1.2e-10) * fc) ** 2) * math.sin(2 * math.pi * f0 * k * m.dt) for k in range(200)]
+    m.add_source_table(E.SOFT_E, [(E.Z, (6, 6, 8), 1.0), (E.Y, (10, 5, 12), 0.6)], np.array(amp))
+    g = E.Engine(m)
+    g.set_schedule(schedule)
+    o = OracleEngine(m, threads=2)
+    eg, eo = [], []
+    for s in range(0, 200, 10):
+        eg.append(g.step_with_energy())
+        eo.append(o.step_with_energy())
+        g.run(9)
+        o.run(9)
+    assert g.schedule == schedule
+    np.testing.assert_allclose(eg, eo, rtol=1e-12, atol=0)
+    assert_fields_equal(g, o, f"openEMS pole kinds, schedule {schedule}")
 
 
 @pytest.mark.parametrize("schedule", [1, 4, 5])

@@ -49,17 +49,23 @@ CASES = [
     ("sweep_probe_fd", 1e-12), ("sweep_probe_times", 1e-12), ("end_criteria", 1e-12),
     ("end_criteria_half", 1e-12), ("end_criteria_mur", 1e-12), ("end_criteria_tem", 1e-12),
     ("adv_mur_dielectric", 1e-12),
-    # Dispersive slabs: the engine's own f64 leapfrog poles, where openEMS
-    # runs its f32 pole arithmetic (the reference measured ~1.5e-6 before
-    # restating it; here 5e-7 ... 1.9e-6).
-    ("adv_drude_slab", 3e-6), ("adv_lorentz_slab", 3e-6), ("adv_lorentz2_slab", 3e-6),
-    ("adv_lorentz_mag_slab", 3e-6), ("adv_debye_slab", 3e-6), ("adv_debye2_slab", 3e-6),
-    ("adv_debye_offgrid", 3e-6), ("adv_lorentz_coarse", 3e-6),
-    ("rs_51_debye", 5e-6), ("lumped_port", 1e-12),
+    # Dispersive slabs with openEMS's f32 pole arithmetic (OpenEmsPole,
+    # openEMS's Debye update): exact.
+    ("adv_drude_slab", 1e-12), ("adv_lorentz_slab", 1e-12), ("adv_lorentz2_slab", 1e-12),
+    ("adv_lorentz_mag_slab", 1e-12), ("adv_debye_slab", 1e-12), ("adv_debye2_slab", 1e-12),
+    ("adv_debye_offgrid", 1e-12), ("adv_lorentz_coarse", 1e-12),
+    ("rs_51_debye", 1e-12), ("lumped_port", 1e-12),
     # openEMS's PML_n layers (single faces, overlaps, lossy media in them,
-    # graded and end-criterion runs).
+    # graded and end-criterion runs, lumped elements reaching into them, a
+    # microstrip filter with lossy substrate and strip in the layers).
     ("pml", 1e-12), ("pml_end", 1e-12), ("pml_face", 1e-12), ("pml_medium", 1e-12), ("rs_162", 1e-12),
     ("rs_443", 1e-12), ("sweep_pml_open", 1e-12), ("adv_pml_vacuum", 1e-12), ("adv_pml_grading", 1e-12),
+    ("pml_exact", 1e-12), ("pml_lumped", 1e-12), ("pml_msl_filter", 1e-12),
+    # Sub-cell material samples (metal not counted), thin metal under a
+    # material, a lumped capacitor over metal with a Drude medium, per-edge
+    # Mur media, excitation ownership: exact but rs_316, whose weak H probe
+    # on the x_min layer face differs by 7.9e-5 (the reference: 7.6e-5).
+    ("metal_material_tie", 1e-12), ("rs_3", 1e-12), ("rs_157", 1e-12), ("rs_316", 1e-4),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
