@@ -205,8 +205,9 @@ def test_openems_pole_arithmetic(schedule):
     """openEMS's f32 pole kinds on every schedule: Lorentz and Drude poles
     (OpenEmsPole) alone, with a trapezoidal Debye pole on the same edges
     (applied first), edges of Debye poles alone (openEMS's Debye update),
-    magnetic poles, beside CPML layers: fields bit for bit with the oracle,
-    energies (which leave these poles out) within 1e-12."""
+    magnetic poles (not on the fused schedule, which has none), beside CPML
+    layers: fields bit for bit with the oracle, energies (which leave these
+    poles out) within 1e-12."""
     rng = np.random.default_rng(5)
     lines = [np.cumsum(np.concatenate([[0.0], 1e-3 * (1.0 + 0.3 * rng.random(c))])) for c in (16, 13, 21)]
     m = E.Model(*lines)
@@ -217,7 +218,8 @@ def test_openems_pole_arithmetic(schedule):
     lor = m.cells().box([4, 4, 4], [11, 9, 12])
     d.fill_cells(m, lor, [E.Pole.lorentz(3e10, 2e10, 1e9), E.Pole.drude(2e10, 4e9)])
     d.fill_cells(m, m.cells().box([8, 2, 9], [14, 8, 16]), [E.Pole.debye(1.5, 2e-11), E.Pole.debye(0.7, 5e-11)])
-    d.fill_cells(m, m.cells().box([2, 5, 5], [9, 11, 10]), [E.Pole.drude(1e10, 3e9)], field=1)
+    if schedule != 2:
+        d.fill_cells(m, m.cells().box([2, 5, 5], [9, 11, 10]), [E.Pole.drude(1e10, 3e9)], field=1)
     m.add_dispersive(d, E.OPENEMS_POLES)
     f0, fc = 10e9, 8e9
     amp = [math.exp(-((k * m.dt - 1.2e-10) * fc) ** 2) * math.sin(2 * math.pi * f0 * k * m.dt) for k in range(200)]
