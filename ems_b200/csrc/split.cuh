@@ -316,33 +316,23 @@ __host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
     return (S.total + tb - 1) / tb;
 }
 
-// Dispersive correction of one side, one edge per thread, the constants
-// read from the edge's run (shared by consecutive edges of a row with equal
-// poles) instead of per pole (src/engine/dispersive.rs:1392-1470). A
-// leapfrog pole's new state does not depend on the corrected value and is
-// stored at once; a trapezoidal pole's is formed from its old state after it.
-// save_prev: also store the corrected value as the edge's saved value (the
-// capture it replaces would read the same value; pole_prev_fold).
-__device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, const PoleSideDev& p, const PoleRun* runs,
-                                           const double* sets, const uint32_t* run_of, int electric, double dt,
-                                           int save_prev, uint32_t e) {
-    if (e >= p.n_edges) return;
-    // The edge's own tables first (independent of each other, so their
-    // latencies overlap): its run, node, axis, first pole and saved value;
-    // then the field, its coefficient and the first pole's state, which
-    // need only those. The run (shared by many edges, from L1) gives the
-    // pole count and constants.
-    const uint32_t r = __ldg(run_of + e);
-    const uint32_t idx = __ldg(p.node + e);
-    const int ax = (int)__ldg(p.axis + e);
-    const uint32_t p0 = e ? __ldg(p.pole_end + e - 1) : 0u;
+// Dispersive correction of edge e of run R, one edge per thread, the
+// constants read from the run (shared by consecutive edges of a row with
+// equal poles) instead of per pole (src/engine/dispersive.rs:1392-1470): idx
+// its padded node, ax its axis, p0 its first pole state. A leapfrog pole's
+// new state does not depend on the corrected value and is stored at once; a
+// trapezoidal pole's is formed from its old state after it. save_prev: also
+// store the corrected value as the edge's saved value (the capture it
+// replaces would read the same value; pole_prev_fold).
+__device__ __forceinline__ void poles_edge_core(const Fields& f, const Coeffs& c, const PoleSideDev& p,
+                                                const PoleRun& R, const double* sets, int electric, double dt,
+                                                int save_prev, uint32_t e, uint32_t idx, int ax, uint32_t p0) {
     const float prev32 = p.prev[e];
     const double prev = (double)prev32;
     float* fld = electric ? f.u[ax] : f.i[ax];
     float u32 = fld[idx];
     const double cb = (double)(electric ? c.c[3 + ax][idx] : c.c[9 + ax][idx]);
     const double j0 = p.j[p0], q0 = p.q[p0];
-    const PoleRun R = runs[r];
     const double half_prev = __dmul_rn(0.5, prev);
     const double* cs = sets + R.set;
     if (R.oe & kOeDebye) {
@@ -384,14 +374,54 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
     if (save_prev) p.prev[e] = u_new;
 }
 
-// Edges [e0, e1) of the side.
-__global__ void __launch_bounds__(256) k_poles_runs(const __grid_constant__ Fields f, const __grid_constant__ Coeffs c,
-                                                    const __grid_constant__ PoleSideDev p, const PoleRun* runs,
-                                                    const double* sets, const uint32_t* run_of, int electric,
-                                                    double dt, int save_prev, uint32_t e0, uint32_t e1) {
-    const uint32_t e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= e1) return;
-    poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e);
+// The correction of edge e found through its run index (edge tables first,
+// independent of each other, so their latencies overlap).
+__device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, const PoleSideDev& p, const PoleRun* runs,
+                                           const double* sets, const uint32_t* run_of, int electric, double dt,
+                                           int save_prev, uint32_t e) {
+    if (e >= p.n_edges) return;
+    const uint32_t r = __ldg(run_of + e);
+    const uint32_t idx = __ldg(p.node + e);
+    const int ax = (int)__ldg(p.axis + e);
+    const uint32_t p0 = e ? __ldg(p.pole_end + e - 1) : 0u;
+    poles_edge_core(f, c, p, runs[r], sets, electric, dt, save_prev, e, idx, ax, p0);
+}
+
+constexpr uint32_t kPoleBlock = 256;
+
+// Edges [e0, e1) of the side, kPoleBlock consecutive edges per block. The
+// runs covering a block's edges (a contiguous range: a run holds
+// consecutive edges) are staged in shared memory and each edge's node, axis
+// and first pole state derived from its run, so the only per-edge traffic
+// is the field, the saved value and the pole state.
+__global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_constant__ Fields f,
+                                                             const __grid_constant__ Coeffs c,
+                                                             const __grid_constant__ PoleSideDev p, const PoleRun* runs,
+                                                             const double* sets, const uint32_t* run_of, int electric,
+                                                             double dt, int save_prev, uint32_t e0, uint32_t e1) {
+    EMS_SHARED PoleRun sr[kPoleBlock];
+    const uint32_t eb = e0 + blockIdx.x * kPoleBlock;
+    if (eb >= e1) return;
+    const uint32_t el = min(eb + kPoleBlock, e1) - 1;
+    const uint32_t r0 = __ldg(run_of + eb), r1 = __ldg(run_of + el);
+    const uint32_t e = eb + threadIdx.x;
+    if (r1 < r0 || r1 - r0 >= kPoleBlock) {  // not a contiguous run range: per edge
+        if (e <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e);
+        return;
+    }
+    const uint32_t nr = r1 - r0 + 1;
+    for (uint32_t t = threadIdx.x; t < nr; t += kPoleBlock) sr[t] = runs[r0 + t];
+    __syncthreads();
+    if (e > el) return;
+    uint32_t lo = 0, hi = nr;  // sr[lo].e0 <= e < sr[lo + 1].e0
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sr[mid].e0 <= e) lo = mid;
+        else hi = mid;
+    }
+    const PoleRun& R = sr[lo];
+    const uint32_t off = e - R.e0;
+    poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, e, R.node0 + off, (int)R.axis, R.p0 + off * R.np);
 }
 
 }  // namespace emsk
