@@ -263,6 +263,7 @@ GPU_SYMBOLS = {
     "ems_gpu_time_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]),
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_interior_box": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_energy_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
     "ems_gpu_last_sample": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
@@ -778,15 +779,24 @@ class Engine:
         self._ck(self._lib.ems_gpu_set_curl_order(self._h, order))
 
     def set_schedule(self, s: int) -> None:
-        """0 automatic, 1 per-operator kernels, 2 fused single pass, 3 two kernels."""
+        """0 automatic, 1 per-operator kernels, 2 fused single pass, 3 two
+        kernels, 4 split, 5 sweep, 6 interior (one pass inside the CPML)."""
         self._ck(self._lib.ems_gpu_set_schedule(self._h, s))
 
     @property
     def schedule(self) -> int:
-        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels, 4 split, 5 sweep."""
+        """The schedule steps run with: 1 per-operator kernels, 2 fused, 3 two kernels, 4 split, 5 sweep,
+        6 interior."""
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value
+
+    @property
+    def interior_box(self) -> tuple:
+        """The interior schedule's box: nodes (lo, hi) per axis."""
+        b = (C.c_uint32 * 6)()
+        self._ck(self._lib.ems_gpu_interior_box(self._h, b))
+        return tuple(b[:3]), tuple(b[3:])
 
     def set_sweep_planes(self, planes: int) -> None:
         """Chunk size of the sweep schedule (5), in x-planes."""

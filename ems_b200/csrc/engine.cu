@@ -32,6 +32,7 @@
 #include "fused_tables.h"
 #include "separate.cuh"
 #include "split.cuh"
+#include "interior.cuh"
 #include "batch.cuh"
 
 #include <thread>
@@ -170,6 +171,10 @@ struct ems_gpu {
     // side; entry [chunks] closes the last range.
     uint32_t sweep_planes = 0;
     bool sweep_ok = false;
+    // The interior schedule (6): the box the one-pass kernel updates, and
+    // why the schedule is unavailable ("" if it is not).
+    InteriorBox ibox{};
+    std::string interior_why = "no tables";
     std::vector<uint32_t> chunk_box[2], chunk_node[2], chunk_edge[2];
     std::vector<SlabGeo> slab_geo;       // to re-cut the shell for another chunk size
     // The chunk loop of a sweep step as a CUDA graph ([0] plain, [1] energy
@@ -562,6 +567,7 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
             if (h->fused_why.empty()) h->fused_why = "openEMS PML layers";
         }
     }
+    h->interior_why = interior_box(d, g, h->ibox);
     h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
     h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);
     h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
@@ -615,6 +621,7 @@ int active_schedule(const ems_gpu* h) {
     case 3: return h->tables_ok ? 3 : 1;
     case 4: return h->tables_ok ? 4 : 1;
     case 5: return h->tables_ok ? (h->sweep_ok ? 5 : 4) : 1;
+    case 6: return h->tables_ok ? (h->interior_why.empty() ? 6 : 4) : 1;
     default: return h->tables_ok ? 4 : 1;
     }
 }
@@ -841,18 +848,126 @@ ems_status run_step_sweep(ems_gpu* h, bool energy) {
     return EMS_OK;
 }
 
+// One step through the interior schedule (interior.cuh): the old fields in
+// one buffer, the new ones written into the other, which becomes the
+// current one. The split H update and its CPML correction over the nodes
+// outside the interior box, the one-pass kernel over the box, the split E
+// update and its CPML correction outside it, then the electric poles and the
+// serial hooks on the new fields. Steps that record the energy run the
+// split schedule in place.
+ems_status run_step_interior(ems_gpu* h) {
+    const Grid& g = h->g;
+    cudaStream_t s = h->stream;
+    if (!h->u2[0]) {
+        // The second buffers start as copies: the entries no kernel writes
+        // (edges that do not exist, row padding) then agree in both.
+        for (int a = 0; a < 3; ++a) {
+            h->u2[a] = h->alloc<float>(g.np);
+            h->i2[a] = h->alloc<float>(g.np);
+            if (!h->u2[a] || !h->i2[a]) return fail(h, EMS_ERR_NOMEM, "second field buffers");
+            if (check(h, cudaMemcpyAsync(h->u2[a], h->u[a], g.np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                      "second field buffers") ||
+                check(h, cudaMemcpyAsync(h->i2[a], h->i[a], g.np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                      "second field buffers"))
+                return EMS_ERR_CUDA;
+        }
+    }
+    // A captured sweep step holds the buffers it was captured with.
+    for (auto& gx : h->sweep_graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    const Fields fa{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    const Fields fb{{h->u2[0], h->u2[1], h->u2[2]}, {h->i2[0], h->i2[1], h->i2[2]}};
+    Coeffs c;
+    for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
+    ems_status st = serial_pre_e(h, fa);
+    if (st) return st;
+    FusedParams P = h->fp;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = fa.u[a];
+        P.io[a] = fa.i[a];
+        P.un[a] = fb.u[a];
+        P.in[a] = fb.i[a];
+    }
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        fs.psi_old = fs.psi_new = h->psi_h[q].first;
+    }
+    P.partials = h->qpartials;
+    P.skip = h->ibox;
+    const bool oe = h->oe_curl;
+    const dim3 qgrd(split_blocks_x(g), g.nx, 1);
+    // The electric saved values u^n, unless the pole kernel kept them.
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_POLES && op.poles.e.n_edges && !(h->fold_prev[0] && h->prev_e_valid)) {
+            k_poles_capture<<<blocks_for(op.poles.e.n_edges, 256), 256, 0, s>>>(fa, op.poles.e, true);
+            ++h->launches;
+        }
+    cudaEvent_t ev = h->prof_begin();
+    if (oe) k_split_h<false, true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    else k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    h->prof_end(0, ev);
+    ++h->launches;
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_CPML)
+            if (const uint32_t nb = shell_blocks(h->shell[0])) {
+                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[0]);
+                ++h->launches;
+            }
+    uint32_t ib[3];
+    interior_blocks(h->ibox, ib);
+    const dim3 igrd(ib[0], ib[1], ib[2]);
+    ev = h->prof_begin();
+    if (oe) k_interior<true><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox);
+    else k_interior<false><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox);
+    h->prof_end(2, ev);
+    ++h->launches;
+    ev = h->prof_begin();
+    if (oe) k_split_e<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    else k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    h->prof_end(1, ev);
+    ++h->launches;
+    for (auto& op : h->ops) {
+        if (op.kind == EMS_OP_CPML) {
+            if (const uint32_t nb = shell_blocks(h->shell[1])) {
+                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[1]);
+                ++h->launches;
+            }
+        } else if (op.kind == EMS_OP_POLES && op.poles.e.n_edges) {
+            k_poles_blocks<<<blocks_for(op.poles.e.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
+                fb, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, h->fold_prev[0] ? 1 : 0, 0u,
+                (uint32_t)op.poles.e.n_edges);
+            ++h->launches;
+        }
+    }
+    h->prev_e_valid = h->fold_prev[0];
+    for (int a = 0; a < 3; ++a) {
+        std::swap(h->u[a], h->u2[a]);
+        std::swap(h->i[a], h->i2[a]);
+    }
+    st = serial_post_h(h, fb);
+    if (st) return st;
+    st = serial_post_e(h, fb);
+    if (st) return st;
+    ++h->step;
+    return EMS_OK;
+}
+
 // One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
     // Only the per-operator, split and sweep steps keep the electric saved values.
-    if (sch != 4 && sch != 5) h->prev_e_valid = false;
+    if (sch != 4 && sch != 5 && sch != 6) h->prev_e_valid = false;
+    if (sch == 6 && !energy) return run_step_interior(h);
     if (sch == 2) return run_step_fused(h, energy);
     if (sch == 3) return run_step_two(h, energy);
     if (sch == 5) return run_step_sweep(h, energy);
     // Schedules 1 and 4 share the hook sequence; split (4) runs the table
     // kernels of split.cuh for the updates and one shell kernel per CPML side.
-    const bool split = sch == 4;
+    const bool split = sch == 4 || sch == 6;
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
@@ -1619,6 +1734,7 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     T.cand.clear();
     if (h->tables_ok) T.cand = (h->oe_curl || h->has_upml) ? std::vector<int>{4} : std::vector<int>{4, 3};
     if (h->tables_ok && h->sweep_ok) T.cand.push_back(5);
+    if (h->tables_ok && h->interior_why.empty()) T.cand.push_back(6);
     T.cand.push_back(1);
     T.ms.assign(T.cand.size(), 0.0);
     T.at = 0;
@@ -1805,7 +1921,7 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 5) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 6) return EMS_ERR_INVALID;
     if (h->oe_curl && (schedule == 2 || schedule == 3))
         return fail(h, EMS_ERR_INVALID, "the fused and two-kernel schedules sum the curl in the default order only");
     if (h->has_upml && (schedule == 2 || schedule == 3 || schedule == 5))
@@ -1815,6 +1931,8 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
     if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
     if (schedule == 5 && !(h->tables_ok && h->sweep_ok))
         return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources") : h->tables_why));
+    if (schedule == 6 && !(h->tables_ok && h->interior_why.empty()))
+        return fail(h, EMS_ERR_INVALID, "interior schedule unavailable: " + (h->tables_ok ? h->interior_why : h->tables_why));
     h->schedule = schedule;
     return EMS_OK;
 }
@@ -1845,6 +1963,17 @@ ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes) {
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {
     if (!h || !active) return EMS_ERR_INVALID;
     *active = active_schedule(h);
+    return EMS_OK;
+}
+
+ems_status ems_gpu_interior_box(ems_gpu* h, uint32_t box[6]) {
+    if (!h || !box) return EMS_ERR_INVALID;
+    if (!(h->tables_ok && h->interior_why.empty()))
+        return fail(h, EMS_ERR_INVALID, "interior schedule unavailable: " + (h->tables_ok ? h->interior_why : h->tables_why));
+    for (int a = 0; a < 3; ++a) {
+        box[a] = h->ibox.lo[a];
+        box[3 + a] = h->ibox.hi[a];
+    }
     return EMS_OK;
 }
 

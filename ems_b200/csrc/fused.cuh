@@ -69,6 +69,13 @@ struct PoleRun {
     double sum_inv_z;
 };
 
+// A box of nodes [lo, hi) per axis whose quads the split kernels leave to
+// the one-pass interior kernel (interior.cuh): lo >= 1, hi <= n − 1, lo[2] and
+// hi[2] multiples of 4. Empty (all 0): the split kernels update every quad.
+struct InteriorBox {
+    uint32_t lo[3], hi[3];
+};
+
 struct FusedParams {
     Grid g;
     const float* uo[3];
@@ -102,6 +109,7 @@ struct FusedParams {
     double* partials;      // per CTA energy share
     int energy;
     int* status;           // nonzero: a bounded wait ran out
+    InteriorBox skip;      // quads the split kernels leave to the interior kernel
 };
 
 #ifndef EMS_HOST_EMULATION

@@ -42,6 +42,12 @@ __device__ __forceinline__ void stq(float* p, const Q4& q) {
 }
 __device__ __forceinline__ Q4 zq() { return Q4{{0.0f, 0.0f, 0.0f, 0.0f}}; }
 
+// Whether the quad (i, j, k0..k0+3) lies in box B (the split kernels leave it
+// to the interior kernel).
+__host__ __device__ __forceinline__ bool in_interior(const InteriorBox& B, uint32_t i, uint32_t j, uint32_t k0) {
+    return i >= B.lo[0] && i < B.hi[0] && j >= B.lo[1] && j < B.hi[1] && k0 >= B.lo[2] && k0 + 4u <= B.hi[2];
+}
+
 // The quad a thread owns: plane i = blockIdx.y; quad q of the plane's
 // ny·pitch/4 (rows are padded to a multiple of 32 floats, so a quad never
 // straddles two rows). False for a quad that lies beyond the plane or in
@@ -65,7 +71,7 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
     double w = 0.0;
-    if (quad_of(g, q, j, k0)) {
+    if (quad_of(g, q, j, k0) && !in_interior(P.skip, i, j, k0)) {
         const uint32_t sj = g.pitch, si = g.ny * g.pitch;
         const uint32_t idx = i * si + j * sj + k0;
         const uint32_t row = i * g.ny + j;
@@ -73,11 +79,11 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
         // Neighbour offsets; 0 where the neighbour does not exist (the value
         // read is then unused).
         const uint32_t oj = jn ? sj : 0u, oi = in_ ? si : 0u, o4 = k0 + 4 < g.nz ? 4u : 0u;
-        const Q4 ux = ldq(P.un[0] + idx), uy = ldq(P.un[1] + idx), uz = ldq(P.un[2] + idx);
-        const Q4 uzj = ldq(P.un[2] + idx + oj), uxj = ldq(P.un[0] + idx + oj);
-        const Q4 uzi = ldq(P.un[2] + idx + oi), uyi = ldq(P.un[1] + idx + oi);
-        const float uy4 = __ldg(P.un[1] + idx + o4), ux4 = __ldg(P.un[0] + idx + o4);
-        const Q4 hx = ldq_rw(P.in[0] + idx), hy = ldq_rw(P.in[1] + idx), hz = ldq_rw(P.in[2] + idx);
+        const Q4 ux = ldq(P.uo[0] + idx), uy = ldq(P.uo[1] + idx), uz = ldq(P.uo[2] + idx);
+        const Q4 uzj = ldq(P.uo[2] + idx + oj), uxj = ldq(P.uo[0] + idx + oj);
+        const Q4 uzi = ldq(P.uo[2] + idx + oi), uyi = ldq(P.uo[1] + idx + oi);
+        const float uy4 = __ldg(P.uo[1] + idx + o4), ux4 = __ldg(P.uo[0] + idx + o4);
+        const Q4 hx = ldq_rw(P.io[0] + idx), hy = ldq_rw(P.io[1] + idx), hz = ldq_rw(P.io[2] + idx);
         const Q4 dax = ldq(lane_row(P, 6, row) + k0), dbx = ldq(lane_row(P, 9, row) + k0);
         const Q4 day = ldq(lane_row(P, 7, row) + k0), dby = ldq(lane_row(P, 10, row) + k0);
         const Q4 daz = ldq(lane_row(P, 8, row) + k0), dbz = ldq(lane_row(P, 11, row) + k0);
@@ -136,7 +142,7 @@ template <bool OE>
 __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
-    if (!quad_of(g, q, j, k0)) return;
+    if (!quad_of(g, q, j, k0) || in_interior(P.skip, i, j, k0)) return;
     const uint32_t sj = g.pitch, si = g.ny * g.pitch;
     const uint32_t idx = i * si + j * sj + k0;
     const uint32_t row = i * g.ny + j;
@@ -145,7 +151,7 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
     const Q4 izj = j > 0 ? ldq(P.in[2] + idx - sj) : zq(), ixj = j > 0 ? ldq(P.in[0] + idx - sj) : zq();
     const Q4 izi = i > 0 ? ldq(P.in[2] + idx - si) : zq(), iyi = i > 0 ? ldq(P.in[1] + idx - si) : zq();
     const float iym = k0 > 0 ? __ldg(P.in[1] + idx - 1) : 0.0f, ixm = k0 > 0 ? __ldg(P.in[0] + idx - 1) : 0.0f;
-    const Q4 ex = ldq_rw(P.un[0] + idx), ey = ldq_rw(P.un[1] + idx), ez = ldq_rw(P.un[2] + idx);
+    const Q4 ex = ldq_rw(P.uo[0] + idx), ey = ldq_rw(P.uo[1] + idx), ez = ldq_rw(P.uo[2] + idx);
     const Q4 cax = ldq(lane_row(P, 0, row) + k0), cbx = ldq(lane_row(P, 3, row) + k0);
     const Q4 cay = ldq(lane_row(P, 1, row) + k0), cby = ldq(lane_row(P, 4, row) + k0);
     const Q4 caz = ldq(lane_row(P, 2, row) + k0), cbz = ldq(lane_row(P, 5, row) + k0);
@@ -236,7 +242,7 @@ __device__ __forceinline__ void shell_node(const FusedParams& P, const ShellBox&
     const uint32_t idx = i * si + j * sj + k, row = i * g.ny + j;
     const uint32_t l0 = Bx.list[0], l1 = Bx.list[1], l2 = Bx.list[2];
     if (SIDE == 0) {
-        const float *ux = P.un[0], *uy = P.un[1], *uz = P.un[2];
+        const float *ux = P.uo[0], *uy = P.uo[1], *uz = P.uo[2];
         if (l0 & 15u) {
             const float A = __fsub_rn(uz[idx + sj], uz[idx]), B = __fsub_rn(uy[idx + 1], uy[idx]);
             const float db = lane_row(P, 9, row)[k];

@@ -334,12 +334,21 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
  * slab hooks), 4 = split (streaming H and E updates, one CPML shell kernel
  * per side, the other hooks per operator), 5 = sweep (the split kernels
  * chunk by chunk along x, so each chunk's E update reads what its H update
- * left in L2; not with magnetic sources). Results are identical bit for
- * bit. Asking for a schedule the model cannot run returns EMS_ERR_INVALID. */
+ * left in L2; not with magnetic sources), 6 = interior (one pass of both
+ * updates over the box inside the CPML layers, the split kernels around it,
+ * old and new fields in two buffers; CPML, electric poles, E sources and
+ * probes only; energy steps run the split kernels). Results are identical
+ * bit for bit. Asking for a schedule the model cannot run returns
+ * EMS_ERR_INVALID. */
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 
-/* The schedule steps run with (1 to 5 as above). */
+/* The schedule steps run with (1 to 6 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
+
+/* The interior schedule's box, nodes [box[0..2], box[3..5]) along x, y, z;
+ * EMS_ERR_INVALID (and why, in ems_gpu_last_error) if the model cannot run
+ * that schedule. */
+ems_status ems_gpu_interior_box(ems_gpu* h, uint32_t box[6]);
 
 /* The order in which the H and E updates sum the four terms of an edge's
  * circulation (CurlOrder, src/engine/kernel.rs:81-108): 0 the reference's

@@ -18,6 +18,7 @@ void fail(const char* what) {
 #include "../../ems_b200/csrc/fused_tables.h"
 #include "../../ems_b200/csrc/separate.cuh"
 #include "../../ems_b200/csrc/split.cuh"
+#include "../../ems_b200/csrc/interior.cuh"
 
 using namespace emsk;
 
@@ -455,6 +456,118 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
             energies[s] = 0.25 * d->dt * w;
         }
         if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P, 0u); }) || !shell(1)) return 2;
+    }
+    for (int c = 0; c < 6; ++c)
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
+            std::memcpy(fields[c] + r * g.nz, &buf[c][r * g.pitch], g.nz * 4);
+    return 0;
+}
+
+// Runs `steps` steps of the interior schedule (interior.cuh: the split H
+// update and CPML correction outside the interior box, the one-pass kernel
+// inside it, the split E update and CPML correction outside it, old and new
+// fields in two buffers) from the fields given in reference layout
+// (overwritten with the result); models with CPML layers and probes only.
+extern "C" int emu_interior_run(const ems_engine_desc* d, uint64_t steps, float** fields, uint32_t* box) {
+    g_err[0] = 0;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE) {
+            std::snprintf(g_err, sizeof g_err, "only CPML and probes are emulated");
+            return 1;
+        }
+    Grid g{};
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "not eligible: %s", T.why.c_str());
+        return 1;
+    }
+    auto pad = [&](const float* src, std::vector<float>& dst) {
+        dst.assign(g.np, 0.0f);
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r) std::memcpy(&dst[r * g.pitch], src + r * g.nz, g.nz * 4);
+    };
+    std::vector<float> buf[6], buf2[6];
+    for (int c = 0; c < 6; ++c) pad(fields[c], buf[c]);
+    for (int c = 0; c < 6; ++c) buf2[c] = buf[c];
+    InteriorBox IB{};
+    const std::string why = interior_box(d, g, IB);
+    if (!why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "no interior schedule: %s", why.c_str());
+        return 1;
+    }
+    for (int a = 0; a < 3; ++a) {
+        box[a] = IB.lo[a];
+        box[3 + a] = IB.hi[a];
+    }
+    std::vector<float> dense[12];
+    FusedParams P{};
+    P.g = g;
+    P.dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (T.lane[l].pooled) {
+            P.lane[l].rid = T.lane[l].rid.data();
+            P.lane[l].rows = T.lane[l].rows.data();
+        } else {
+            pad(d->coeff[l], dense[l]);
+            P.lane[l].dense = dense[l].data();
+        }
+    }
+    std::vector<std::vector<float>> psi;
+    psi.reserve(T.slabs.size());
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    for (const FusedSlabSpec& sp : T.slabs) {
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = (uint32_t)sp.src->lo[a];
+            f.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        f.normal = (uint32_t)sp.src->normal;
+        f.b = sp.src->b;
+        f.a = sp.src->a;
+        f.k = sp.src->k;
+        psi.emplace_back(sp.len, 0.0f);
+        f.psi_old = f.psi_new = psi.back().data();
+    }
+    for (int a = 0; a < 3; ++a) P.cmask[a] = T.cmask[a].data();
+    std::vector<ShellBox> st[2];
+    std::vector<uint32_t> win[2];
+    ShellDev sd[2];
+    for (int side = 0; side < 2; ++side) {
+        uint32_t total = 0;
+        st[side] = shell_boxes(T, d->nodes, side, &total);
+        win[side] = shell_windows(st[side], total);
+        sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u, win[side].data()};
+    }
+    const unsigned gx = split_blocks_x(g);
+    std::vector<double> partials((size_t)gx * g.nx, 0.0);
+    P.partials = partials.data();
+    auto shell = [&](int side) -> bool {
+        const uint32_t blocks = shell_blocks(sd[side]);
+        if (!blocks) return true;
+        const ShellDev S = sd[side];
+        return side ? emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<1>(P, S); })
+                    : emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<0>(P, S); });
+    };
+    uint32_t ib[3];
+    interior_blocks(IB, ib);
+    for (uint64_t s = 0; s < steps; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            P.uo[a] = buf[a].data();
+            P.io[a] = buf[3 + a].data();
+            P.un[a] = buf2[a].data();
+            P.in[a] = buf2[3 + a].data();
+        }
+        P.skip = IB;
+        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P, 0u); }) || !shell(0)) return 2;
+        if (!emu_launch(ib[0], ib[1], ib[2], 32 * kInWarps, 1, [&] { k_interior<false>(P, IB); })) return 2;
+        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P, 0u); }) || !shell(1)) return 2;
+        for (int c = 0; c < 6; ++c) std::swap(buf[c], buf2[c]);
     }
     for (int c = 0; c < 6; ++c)
         for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)

@@ -35,6 +35,8 @@ def emu_lib(asan=False):
     lib.emu_two_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_split_run.restype = C.c_int
     lib.emu_split_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_interior_run.restype = C.c_int
+    lib.emu_interior_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_pole_prev_fold.restype = C.c_int
     lib.emu_pole_prev_fold.argtypes = [C.c_void_p, C.c_int]
     lib.emu_error.restype = C.c_char_p
@@ -169,6 +171,32 @@ def test_split_source_equals_oracle(n, graded):
     np.testing.assert_allclose(en, eo, rtol=1e-12, atol=0)
 
 
+def run_interior(lib, m, state, steps):
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    box = (C.c_uint32 * 6)()
+    assert lib.emu_interior_run(m.desc, steps, ptrs, box) == 0, lib.emu_error().decode()
+    return arrs, list(box)
+
+
+@pytest.mark.parametrize("n,graded", [((40, 22, 140), True), ((13, 11, 30), False), ((36, 9, 70), False)])
+def test_interior_source_equals_oracle(n, graded):
+    """The interior schedule: the split kernels outside the interior box and
+    the one-pass kernel inside it (several tiles along every axis, feeder
+    rows and quads inside and outside the box, x chunks starting inside it),
+    old and new fields in two buffers: fields bit-exact with the oracle."""
+    m = model(n, E.TRAPEZOIDAL, poles=False, graded=graded)
+    state = random_state(m, seed=4)
+    steps = 3
+    got, box = run_interior(emu_lib(), m, state, steps)
+    lo, hi = box[:3], box[3:]
+    assert all(h > l for l, h in zip(lo, hi)) and lo[2] % 4 == 0 and hi[2] % 4 == 0
+    want, _, _ = run_oracle(m, state, steps)
+    for name, a, b in zip(["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"], got, want):
+        bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])} (box {box})"
+
+
 def test_pole_capture_fold_decision():
     """The split schedule lets a pole kernel store the saved field values
     itself only when nothing between the correction and the reference's
@@ -225,6 +253,8 @@ def test_fused_kernel_source_under_address_sanitizer():
         "st = [np.ascontiguousarray(x) for x in T.random_state(m3)]\n"
         "p = (C.c_void_p * 6)(*[a.ctypes.data for a in st])\n"
         "assert T.emu_lib(asan=True).emu_split_run(m3.desc, 3, p, None) == 0\n"
+        "m4 = T.model((36, 9, 70), E.TRAPEZOIDAL, poles=False)\n"
+        "T.run_interior(T.emu_lib(asan=True), m4, T.random_state(m4), 2)\n"
         "print('clean')\n"
     ) % (HERE, os.path.dirname(HERE))
     env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")

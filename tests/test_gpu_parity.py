@@ -183,7 +183,7 @@ def test_invalid_tables_rejected():
 
 
 @pytest.mark.parametrize("n", [40, 67])
-@pytest.mark.parametrize("schedule", [2, 3, 4])
+@pytest.mark.parametrize("schedule", [2, 3, 4, 6])
 def test_dispersive_box_chunks_and_tiles(n, schedule):
     """Sizes whose rows, tiles and x chunks leave remainders."""
     w = W.dispersive_box(n=n, radius=n / 6, slab=3, cpml=4, steps=120)
@@ -217,6 +217,44 @@ def test_split_saved_values_across_uploads_and_schedule_switches():
     assert_fields_equal(g, o, "split with uploads and switches")
     for p in w.probes:
         _series_equal(g, o, p)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_interior_schedule_uploads_switches_and_probes(order):
+    """The interior schedule (one-pass kernel over the interior box, split
+    kernels around it, two field buffers): probe series and fields bit for
+    bit through energy steps (split, in place), a field upload, switches to
+    and from other schedules, in both curl orders; refused where a hook sits
+    between the two updates."""
+    w = W.dispersive_box(n=72, radius=10, slab=4, cpml=6, steps=260)
+    m = w.model
+    g = E.Engine(m)
+    g.set_curl_order(order)
+    o = OracleEngine(m, threads=4)
+    o.set_curl_order(order)
+    rng = np.random.default_rng(9)
+    eg, eo = [], []
+    for sch, n in ((6, 40), (4, 7), (6, 33), (1, 5), (6, 60)):
+        g.set_schedule(sch)
+        assert g.schedule == sch
+        eg.append(g.step_with_energy())
+        eo.append(o.step_with_energy())
+        g.run(n)
+        o.run(n)
+        if sch == 6 and n == 33:
+            v = (rng.standard_normal(m.nodes) * 1e-3).astype(np.float32)
+            g.set_field(1, 2, v)
+            o.set_field(1, 2, v)
+    g.set_schedule(6)
+    g.run(31)
+    o.run(31)
+    assert_fields_equal(g, o, f"interior schedule, curl order {order}")
+    for p in w.probes:
+        _series_equal(g, o, p)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+    mm, _ = mixed_model(scheme=E.LEAPFROG, h_source=True, steps=20)
+    with pytest.raises(E.EngineError):
+        E.Engine(mm).set_schedule(6)
 
 
 @pytest.mark.parametrize("h_source", [True, False])
