@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
     ap.add_argument("--schedule", type=int, default=0,
                     help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split, 5 sweep, 6 interior")
+    ap.add_argument("--interior-planes", type=int, default=0, help="planes per block of the interior kernel (0: default)")
     ap.add_argument("--workload", choices=["box", "sweep", "learned"], default="box",
                     help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
                          "sweep; learned: training and held-out evaluation of the learned early stop")
@@ -302,6 +303,8 @@ def run_ours(args):
     w = workload(args.cells, total_steps + 10)
     eng = E.Engine(w.model, device=dev)
     eng.set_schedule(args.schedule)
+    if args.interior_planes:
+        eng.set_interior_planes(args.interior_planes)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.run(args.warmup)
     torch.cuda.synchronize(dev)

@@ -273,6 +273,7 @@ GPU_SYMBOLS = {
     "ems_gpu_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_gpu_freq_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ems_gpu_set_sweep_planes": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "ems_gpu_set_interior_planes": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ems_gpu_freq_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t]),
     "ems_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
@@ -797,6 +798,10 @@ class Engine:
         b = (C.c_uint32 * 6)()
         self._ck(self._lib.ems_gpu_interior_box(self._h, b))
         return tuple(b[:3]), tuple(b[3:])
+
+    def set_interior_planes(self, planes: int) -> None:
+        """Planes a block of the interior schedule's one-pass kernel marches through."""
+        self._ck(self._lib.ems_gpu_set_interior_planes(self._h, planes))
 
     def set_sweep_planes(self, planes: int) -> None:
         """Chunk size of the sweep schedule (5), in x-planes."""

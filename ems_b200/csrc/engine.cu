@@ -175,6 +175,7 @@ struct ems_gpu {
     // why the schedule is unavailable ("" if it is not).
     InteriorBox ibox{};
     std::string interior_why = "no tables";
+    uint32_t interior_planes = kInPlanes;  // planes a block of the interior kernel marches through
     std::vector<uint32_t> chunk_box[2], chunk_node[2], chunk_edge[2];
     std::vector<SlabGeo> slab_geo;       // to re-cut the shell for another chunk size
     // The chunk loop of a sweep step as a CUDA graph ([0] plain, [1] energy
@@ -898,7 +899,25 @@ ems_status run_step_interior(ems_gpu* h) {
     P.partials = h->qpartials;
     P.skip = h->ibox;
     const bool oe = h->oe_curl;
-    const dim3 qgrd(split_blocks_x(g), g.nx, 1);
+    // The split kernels over the nodes outside the box only: the planes
+    // before and after it, then in its planes the rows before and after it
+    // and the quads of its rows before and after it.
+    const InteriorBox& B = h->ibox;
+    const uint32_t qpr = g.pitch >> 2, zl = B.lo[2] / 4u, zr = B.hi[2] / 4u, nzl = zl + (qpr - zr);
+    auto outer = [&](auto launch) {
+        const uint32_t bx = split_blocks_x(g);
+        P.qmap = QuadMap{};
+        if (B.lo[0]) launch(dim3(bx, B.lo[0], 1), 0u);
+        if (g.nx > B.hi[0]) launch(dim3(bx, g.nx - B.hi[0], 1), B.hi[0]);
+        const uint32_t xn = B.hi[0] - B.lo[0];
+        P.qmap = QuadMap{0u, 0u, 0u, 1u, 0u, 0u, B.lo[1] * qpr};
+        if (P.qmap.count) launch(dim3(blocks_for(P.qmap.count, kSplitThreads), xn, 1), B.lo[0]);
+        P.qmap = QuadMap{0u, B.hi[1] * qpr, 0u, 1u, 0u, 0u, (g.ny - B.hi[1]) * qpr};
+        if (P.qmap.count) launch(dim3(blocks_for(P.qmap.count, kSplitThreads), xn, 1), B.lo[0]);
+        P.qmap = QuadMap{1u, 0u, B.lo[1], nzl, zl, zr, (B.hi[1] - B.lo[1]) * nzl};
+        if (P.qmap.count) launch(dim3(blocks_for(P.qmap.count, kSplitThreads), xn, 1), B.lo[0]);
+        P.qmap = QuadMap{};
+    };
     // The electric saved values u^n, unless the pole kernel kept them.
     for (auto& op : h->ops)
         if (op.kind == EMS_OP_POLES && op.poles.e.n_edges && !(h->fold_prev[0] && h->prev_e_valid)) {
@@ -906,10 +925,12 @@ ems_status run_step_interior(ems_gpu* h) {
             ++h->launches;
         }
     cudaEvent_t ev = h->prof_begin();
-    if (oe) k_split_h<false, true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
-    else k_split_h<false><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    outer([&](dim3 grd, uint32_t i0) {
+        if (oe) k_split_h<false, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+        else k_split_h<false><<<grd, kSplitThreads, 0, s>>>(P, i0);
+        ++h->launches;
+    });
     h->prof_end(0, ev);
-    ++h->launches;
     for (auto& op : h->ops)
         if (op.kind == EMS_OP_CPML)
             if (const uint32_t nb = shell_blocks(h->shell[0])) {
@@ -917,18 +938,20 @@ ems_status run_step_interior(ems_gpu* h) {
                 ++h->launches;
             }
     uint32_t ib[3];
-    interior_blocks(h->ibox, ib);
+    interior_blocks(h->ibox, h->interior_planes, ib);
     const dim3 igrd(ib[0], ib[1], ib[2]);
     ev = h->prof_begin();
-    if (oe) k_interior<true><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox);
-    else k_interior<false><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox);
+    if (oe) k_interior<true><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox, h->interior_planes);
+    else k_interior<false><<<igrd, 32 * kInWarps, 0, s>>>(P, h->ibox, h->interior_planes);
     h->prof_end(2, ev);
     ++h->launches;
     ev = h->prof_begin();
-    if (oe) k_split_e<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
-    else k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
+    outer([&](dim3 grd, uint32_t i0) {
+        if (oe) k_split_e<true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+        else k_split_e<<<grd, kSplitThreads, 0, s>>>(P, i0);
+        ++h->launches;
+    });
     h->prof_end(1, ev);
-    ++h->launches;
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML) {
             if (const uint32_t nb = shell_blocks(h->shell[1])) {
@@ -1948,6 +1971,12 @@ ems_status ems_gpu_set_curl_order(ems_gpu* h, int order) {
             cudaGraphExecDestroy(gx);
             gx = nullptr;
         }
+    return EMS_OK;
+}
+
+ems_status ems_gpu_set_interior_planes(ems_gpu* h, uint32_t planes) {
+    if (!h || planes < 1 || planes > 4096) return EMS_ERR_INVALID;
+    h->interior_planes = planes;
     return EMS_OK;
 }
 

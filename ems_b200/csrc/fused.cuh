@@ -76,6 +76,15 @@ struct InteriorBox {
     uint32_t lo[3], hi[3];
 };
 
+// Which quads of a plane a split-kernel thread takes (the interior
+// schedule's launches over the nodes outside its box): mode 0, quad q0 + t
+// for thread t; mode 1, the quads outside z range [zl, zr) of rows row0,
+// row0 + 1, …: thread t takes row row0 + t / nzl and the (t mod nzl)-th of
+// the row's quads below zl or from zr on. t >= count (if count) takes none.
+struct QuadMap {
+    uint32_t mode, q0, row0, nzl, zl, zr, count;
+};
+
 struct FusedParams {
     Grid g;
     const float* uo[3];
@@ -110,6 +119,7 @@ struct FusedParams {
     int energy;
     int* status;           // nonzero: a bounded wait ran out
     InteriorBox skip;      // quads the split kernels leave to the interior kernel
+    QuadMap qmap;          // which quads a split-kernel thread takes
 };
 
 #ifndef EMS_HOST_EMULATION

@@ -27,7 +27,7 @@ namespace emsk {
 constexpr unsigned kInRows = 8;     // rows a block updates (warp 0 computes the row below them)
 constexpr unsigned kInWarps = kInRows + 1;
 constexpr unsigned kInQuads = 31;   // quads of z-nodes a warp updates (lane 0 computes the quad below them)
-constexpr unsigned kInPlanes = 32;  // planes a block marches through
+constexpr unsigned kInPlanes = 32;  // default planes a block marches through
 
 // H of the quad (i, j, k0..k0+3) from the old fields (uo, io) and the old u
 // of the quad, for a quad whose nodes all have their H and E edges (interior
@@ -59,20 +59,21 @@ __device__ __forceinline__ void interior_h(const FusedParams& P, uint32_t i, uin
 }
 
 // Grid: (z tiles of kInQuads quads, y tiles of kInRows rows, x chunks of
-// kInPlanes planes) over the box. Thread (warp w, lane l): row
+// `planes` planes) over the box; a chunk starts by computing the H values of
+// the plane before it again (or reads them outside the box). Thread (warp w, lane l): row
 // lo[1] + tile·kInRows + w − 1, quad lo[2] + 4·(tile·kInQuads + l − 1); warp 0
 // and lane 0 only provide H values to the others.
 template <bool OE>
 __global__ void __launch_bounds__(32 * kInWarps) k_interior(const __grid_constant__ FusedParams P,
-                                                            const InteriorBox B) {
+                                                            const InteriorBox B, uint32_t planes) {
     EMS_SHARED float4 sh[2][3][kInWarps][32];  // H(i) of every thread's quad, by plane parity
     const Grid& g = P.g;
     const uint32_t sj = g.pitch, si = g.ny * g.pitch;
     const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
     const uint32_t j = B.lo[1] + blockIdx.y * kInRows + w - 1u;
     const uint32_t k0 = B.lo[2] + 4u * (blockIdx.x * kInQuads + l) - 4u;
-    const uint32_t xs = B.lo[0] + blockIdx.z * kInPlanes;
-    const uint32_t xe = xs + kInPlanes < B.hi[0] ? xs + kInPlanes : B.hi[0];
+    const uint32_t xs = B.lo[0] + blockIdx.z * planes;
+    const uint32_t xe = xs + planes < B.hi[0] ? xs + planes : B.hi[0];
     const bool in_box = j < B.hi[1] && k0 + 4u <= B.hi[2];
     const bool feeder = w == 0 || l == 0;
     const bool owner = !feeder && in_box;
@@ -186,12 +187,12 @@ inline std::string interior_box(const ems_engine_desc* d, const Grid& g, Interio
     return "";
 }
 
-// Blocks of k_interior over box B along z, y and x.
-inline void interior_blocks(const InteriorBox& B, uint32_t n[3]) {
+// Blocks of k_interior over box B along z, y and x (chunks of `planes`).
+inline void interior_blocks(const InteriorBox& B, uint32_t planes, uint32_t n[3]) {
     const uint32_t quads = (B.hi[2] - B.lo[2]) / 4u;
     n[0] = (quads + kInQuads - 1u) / kInQuads;
     n[1] = (B.hi[1] - B.lo[1] + kInRows - 1u) / kInRows;
-    n[2] = (B.hi[0] - B.lo[0] + kInPlanes - 1u) / kInPlanes;
+    n[2] = (B.hi[0] - B.lo[0] + planes - 1u) / planes;
 }
 
 }  // namespace emsk

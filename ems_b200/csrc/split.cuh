@@ -48,6 +48,16 @@ __host__ __device__ __forceinline__ bool in_interior(const InteriorBox& B, uint3
     return i >= B.lo[0] && i < B.hi[0] && j >= B.lo[1] && j < B.hi[1] && k0 >= B.lo[2] && k0 + 4u <= B.hi[2];
 }
 
+// The quad index (in the plane) of thread t of a split kernel (QuadMap);
+// ~0u: none.
+__device__ __forceinline__ uint32_t mapped_quad(const FusedParams& P, uint32_t t) {
+    const QuadMap& M = P.qmap;
+    if (M.count && t >= M.count) return ~0u;
+    if (M.mode == 0) return M.q0 + t;
+    const uint32_t r = t / M.nzl, c = t - r * M.nzl;
+    return (M.row0 + r) * (P.g.pitch >> 2) + (c < M.zl ? c : M.zr + (c - M.zl));
+}
+
 // The quad a thread owns: plane i = blockIdx.y; quad q of the plane's
 // ny·pitch/4 (rows are padded to a multiple of 32 floats, so a quad never
 // straddles two rows). False for a quad that lies beyond the plane or in
@@ -128,7 +138,7 @@ template <bool ENERGY, bool OE = false>
 __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P,
                                                                          uint32_t i0) {
     const uint32_t i = i0 + blockIdx.y;
-    const double w = split_h_quad<ENERGY, OE>(P, i, blockIdx.x * kSplitThreads + threadIdx.x);
+    const double w = split_h_quad<ENERGY, OE>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
         if (threadIdx.x == 0) P.partials[(size_t)i * gridDim.x + blockIdx.x] = s;
@@ -173,7 +183,7 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
 
 template <bool OE = false>
 __global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
-    split_e_quad<OE>(P, i0 + blockIdx.y, blockIdx.x * kSplitThreads + threadIdx.x);
+    split_e_quad<OE>(P, i0 + blockIdx.y, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
 }
 
 // Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.

@@ -364,6 +364,12 @@ ems_status ems_gpu_set_curl_order(ems_gpu* h, int order);
  * chunk's fields take under half of L2; larger than nx: one chunk). */
 ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes);
 
+/* Planes a block of the interior schedule's one-pass kernel marches through
+ * (1 to 4096; default 32): a block first computes the H values of the plane
+ * before its chunk again, so short chunks add work and long ones fewer,
+ * longer-lived blocks. */
+ems_status ems_gpu_set_interior_planes(ems_gpu* h, uint32_t planes);
+
 /* Picks the fastest in-place schedule (4, 3, 5 or 1) for this model's grid
  * shape and operators: from `cache_path` (a text file of earlier picks,
  * lines "<key> <schedule> <ms>") if it holds the key, else by timing each

@@ -555,7 +555,8 @@ extern "C" int emu_interior_run(const ems_engine_desc* d, uint64_t steps, float*
                     : emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<0>(P, S); });
     };
     uint32_t ib[3];
-    interior_blocks(IB, ib);
+    const uint32_t planes = 5;  // chunks that start inside the box
+    interior_blocks(IB, planes, ib);
     for (uint64_t s = 0; s < steps; ++s) {
         for (int a = 0; a < 3; ++a) {
             P.uo[a] = buf[a].data();
@@ -564,9 +565,33 @@ extern "C" int emu_interior_run(const ems_engine_desc* d, uint64_t steps, float*
             P.in[a] = buf2[3 + a].data();
         }
         P.skip = IB;
-        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P, 0u); }) || !shell(0)) return 2;
-        if (!emu_launch(ib[0], ib[1], ib[2], 32 * kInWarps, 1, [&] { k_interior<false>(P, IB); })) return 2;
-        if (!emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_e(P, 0u); }) || !shell(1)) return 2;
+        // The engine's launches over the nodes outside the box: planes
+        // before and after it, rows before and after it, quads before and
+        // after it in its rows (QuadMap).
+        const uint32_t qpr = g.pitch >> 2, zl = IB.lo[2] / 4u, zr = IB.hi[2] / 4u, nzl = zl + (qpr - zr);
+        const uint32_t xn = IB.hi[0] - IB.lo[0];
+        auto outer = [&](bool h_side) -> bool {
+            auto go = [&](unsigned bx, unsigned by, uint32_t i0) {
+                return h_side ? emu_launch(bx, by, 1, kSplitThreads, 1, [&] { k_split_h<false>(P, i0); })
+                              : emu_launch(bx, by, 1, kSplitThreads, 1, [&] { k_split_e(P, i0); });
+            };
+            auto nb = [](uint32_t n) { return (n + kSplitThreads - 1) / kSplitThreads; };
+            bool ok = true;
+            P.qmap = QuadMap{};
+            ok = ok && go(gx, IB.lo[0], 0u);
+            ok = ok && go(gx, g.nx - IB.hi[0], IB.hi[0]);
+            P.qmap = QuadMap{0u, 0u, 0u, 1u, 0u, 0u, IB.lo[1] * qpr};
+            ok = ok && go(nb(P.qmap.count), xn, IB.lo[0]);
+            P.qmap = QuadMap{0u, IB.hi[1] * qpr, 0u, 1u, 0u, 0u, (g.ny - IB.hi[1]) * qpr};
+            ok = ok && (P.qmap.count == 0 || go(nb(P.qmap.count), xn, IB.lo[0]));
+            P.qmap = QuadMap{1u, 0u, IB.lo[1], nzl, zl, zr, (IB.hi[1] - IB.lo[1]) * nzl};
+            ok = ok && go(nb(P.qmap.count), xn, IB.lo[0]);
+            P.qmap = QuadMap{};
+            return ok;
+        };
+        if (!outer(true) || !shell(0)) return 2;
+        if (!emu_launch(ib[0], ib[1], ib[2], 32 * kInWarps, 1, [&] { k_interior<false>(P, IB, planes); })) return 2;
+        if (!outer(false) || !shell(1)) return 2;
         for (int c = 0; c < 6; ++c) std::swap(buf[c], buf2[c]);
     }
     for (int c = 0; c < 6; ++c)
