@@ -54,9 +54,9 @@ def _run(cmd: list[str]) -> None:
 
 
 def build_gpu(force: bool = False) -> str:
-    srcs = [os.path.join(CSRC, f) for f in ("engine.cu", "noalloc.cu", "arith.cuh", "kernels.cuh", "fused.cuh", "separate.cuh",
-                                             "split.cuh", "fused_tables.h")]
-    srcs = [s for s in srcs if os.path.exists(s)] + [os.path.join(INCLUDE, "ems_gpu.h")]
+    srcs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
+            if f.endswith((".cuh", ".h")) or f in ("engine.cu", "noalloc.cu")]
+    srcs += [os.path.join(INCLUDE, "ems_gpu.h")]
     if force or _stale(GPU_LIB, srcs):
         tmp = GPU_LIB + ".tmp"
         _run([_nvcc(), *NVCC_ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-o", tmp, os.path.join(CSRC, "engine.cu"),

@@ -24,7 +24,7 @@
 
 namespace emsk {
 
-constexpr unsigned kInRows = 8;     // rows a block updates (warp 0 computes the row below them)
+constexpr unsigned kInRows = 7;     // rows a block updates (warp 0 computes the row below them)
 constexpr unsigned kInWarps = kInRows + 1;
 constexpr unsigned kInQuads = 31;   // quads of z-nodes a warp updates (lane 0 computes the quad below them)
 constexpr unsigned kInPlanes = 32;  // default planes a block marches through
@@ -64,7 +64,7 @@ __device__ __forceinline__ void interior_h(const FusedParams& P, uint32_t i, uin
 // lo[1] + tile·kInRows + w − 1, quad lo[2] + 4·(tile·kInQuads + l − 1); warp 0
 // and lane 0 only provide H values to the others.
 template <bool OE>
-__global__ void __launch_bounds__(32 * kInWarps) k_interior(const __grid_constant__ FusedParams P,
+__global__ void __launch_bounds__(32 * kInWarps, 2) k_interior(const __grid_constant__ FusedParams P,
                                                             const InteriorBox B, uint32_t planes) {
     EMS_SHARED float4 sh[2][3][kInWarps][32];  // H(i) of every thread's quad, by plane parity
     const Grid& g = P.g;
