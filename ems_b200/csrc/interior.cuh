@@ -64,7 +64,7 @@ __device__ __forceinline__ void interior_h(const FusedParams& P, uint32_t i, uin
 // lo[1] + tile·kInRows + w − 1, quad lo[2] + 4·(tile·kInQuads + l − 1); warp 0
 // and lane 0 only provide H values to the others.
 template <bool OE>
-__global__ void __launch_bounds__(32 * kInWarps, 2) k_interior(const __grid_constant__ FusedParams P,
+__global__ void __launch_bounds__(32 * kInWarps, 3) k_interior(const __grid_constant__ FusedParams P,
                                                             const InteriorBox B, uint32_t planes) {
     EMS_SHARED float4 sh[2][3][kInWarps][32];  // H(i) of every thread's quad, by plane parity
     const Grid& g = P.g;
@@ -102,18 +102,10 @@ __global__ void __launch_bounds__(32 * kInWarps, 2) k_interior(const __grid_cons
             hy = ldq(P.in[1] + idx);
             hz = ldq(P.in[2] + idx);
         }
-        Q4 cax, cbx, cay, cby, caz, cbz;
         if (owner) {
             stq(P.in[0] + idx, hx);
             stq(P.in[1] + idx, hy);
             stq(P.in[2] + idx, hz);
-            const uint32_t row = i * g.ny + j;
-            cax = ldq(lane_row(P, 0, row) + k0);
-            cbx = ldq(lane_row(P, 3, row) + k0);
-            cay = ldq(lane_row(P, 1, row) + k0);
-            cby = ldq(lane_row(P, 4, row) + k0);
-            caz = ldq(lane_row(P, 2, row) + k0);
-            cbz = ldq(lane_row(P, 5, row) + k0);
         }
         if (owner || provide) {
             sh[par][0][w][l] = make_float4(hx.v[0], hx.v[1], hx.v[2], hx.v[3]);
@@ -127,6 +119,10 @@ __global__ void __launch_bounds__(32 * kInWarps, 2) k_interior(const __grid_cons
             const float4 xj = sh[par][0][w - 1u][l], zj = sh[par][2][w - 1u][l];
             const float iym = sh[par][1][w][l - 1u].w, ixm = sh[par][0][w][l - 1u].w;
             const Q4 ixj{{xj.x, xj.y, xj.z, xj.w}}, izj{{zj.x, zj.y, zj.z, zj.w}};
+            const uint32_t row = i * g.ny + j;
+            const Q4 cax = ldq(lane_row(P, 0, row) + k0), cbx = ldq(lane_row(P, 3, row) + k0);
+            const Q4 cay = ldq(lane_row(P, 1, row) + k0), cby = ldq(lane_row(P, 4, row) + k0);
+            const Q4 caz = ldq(lane_row(P, 2, row) + k0), cbz = ldq(lane_row(P, 5, row) + k0);
             Q4 nx_, ny_, nz_;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
