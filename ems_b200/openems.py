@@ -73,12 +73,14 @@ _TOKEN = re.compile(r"\s*(?:(\d+\.?\d*(?:[eE][-+]?\d+)?|\.\d+(?:[eE][-+]?\d+)?)|
 
 
 class Expression:
-    """A signal ``f(t)`` in openEMS's expression syntax: numbers, ``t``,
-    ``pi``, + − * / ^, parentheses, unary minus and the functions of
-    ``_FUNCS`` (parsed once into a tree; no evaluation of arbitrary code)."""
+    """A signal ``f(t)`` or a weighting function ``w(x, y, z)`` in openEMS's
+    expression syntax: numbers, the variables named, ``pi``, + − * / ^,
+    parentheses, unary minus and the functions of ``_FUNCS`` (parsed once
+    into a tree; no evaluation of arbitrary code)."""
 
-    def __init__(self, text: str):
+    def __init__(self, text: str, variables=("t",)):
         self.text = text
+        self.variables = tuple(variables)
         self._tok = [(m.group(1), m.group(2), m.group(3)) for m in _TOKEN.finditer(text) if any(m.groups())]
         self._i = 0
         self._tree = self._sum()
@@ -141,8 +143,8 @@ class Expression:
                 if not self._take(")"):
                     raise ValueError(f"expression {self.text!r}: missing )")
                 return ("fn", name, arg)
-            if name == "t":
-                return ("t",)
+            if name in self.variables:
+                return ("var", name)
             if name == "pi":
                 return ("num", math.pi)
             raise ValueError(f"expression {self.text!r}: unknown name {name}")
@@ -158,7 +160,7 @@ class Expression:
             k = n[0]
             if k == "num":
                 return n[1]
-            if k == "t":
+            if k == "var":
                 return t
             if k == "neg":
                 return -ev(n[1])
@@ -168,6 +170,35 @@ class Expression:
             return {"+": a + b, "-": a - b, "*": a * b, "/": a / b if b != 0 else math.inf}.get(k) \
                 if k != "^" else a ** b
         return float(ev(self._tree))
+
+    def evaluate(self, **env):
+        """The expression over numpy arrays (or numbers) of its variables."""
+        fn = {"exp": np.exp, "cos": np.cos, "sin": np.sin, "tan": np.tan, "sqrt": np.sqrt, "abs": np.abs,
+              "log": np.log, "log10": np.log10, "atan": np.arctan, "cosh": np.cosh, "sinh": np.sinh,
+              "tanh": np.tanh}
+
+        def ev(n):
+            k = n[0]
+            if k == "num":
+                return n[1]
+            if k == "var":
+                return np.asarray(env[n[1]], dtype=np.float64)
+            if k == "neg":
+                return -ev(n[1])
+            if k == "fn":
+                return fn[n[1]](ev(n[2]))
+            a, b = ev(n[1]), ev(n[2])
+            if k == "+":
+                return a + b
+            if k == "-":
+                return a - b
+            if k == "*":
+                return a * b
+            if k == "/":
+                return np.divide(a, b)
+            return np.power(a, b)
+        with np.errstate(all="ignore"):
+            return np.asarray(ev(self._tree), dtype=np.float64)
 
 
 # ---------------------------------------------------------------------------
@@ -265,6 +296,9 @@ class Prop:
     boxes: list = field(default_factory=list)
     fd: list = field(default_factory=list)
     order: int = 0
+    # Weighting functions of a material's Epsilon, Mue, Kappa, Sigma: per
+    # quantity three expressions in x, y, z (drawing units), None for 1.
+    weight: dict = field(default_factory=dict)
 
 
 @dataclass
@@ -364,12 +398,26 @@ def parse(text: str) -> OpenEmsFile:
             raise NotImplementedError(f"property {el.tag}")
         if el.tag == "ProbeBox" and len(boxes) > 1:
             raise NotImplementedError(f"probe {el.get('Name')!r} with several primitives")
-        if el.find("Weight") is not None:
-            raise NotImplementedError(f"weighting functions ({el.get('Name')!r})")
+        weight = {}
+        wel = el.find("Weight")
+        if wel is not None and el.tag == "Excitation":
+            if set(wel.attrib) - {"X", "Y", "Z"}:
+                raise NotImplementedError(f"weighting functions ({el.get('Name')!r})")
+            weight["Excite"] = [None if wel.get(c, "1").strip() in ("1", "1.0") else
+                                Expression(wel.get(c), ("x", "y", "z")) for c in "XYZ"]
+        elif wel is not None:
+            if el.tag not in MATERIALS or set(wel.attrib) - {"Epsilon", "Mue", "Kappa", "Sigma"}:
+                raise NotImplementedError(f"weighting functions ({el.get('Name')!r})")
+            iso = el.get("Isotropy", "1") != "0"
+            for key, text in wel.attrib.items():
+                parts = [t.strip() for t in text.split(",")]
+                parts = [parts[0]] * 3 if iso else (parts + ["1"] * 3)[:3]
+                weight[key] = [None if t in ("1", "1.0") else Expression(t, ("x", "y", "z")) for t in parts]
         sub = el.find("Property")
         fds = el.find("FD_Samples")
         props.append(Prop(el.tag, el.get("Name", ""), dict(el.attrib), dict(sub.attrib) if sub is not None else {},
-                          boxes, [float(x) for x in fds.text.split(",")] if fds is not None and fds.text else [], q))
+                          boxes, [float(x) for x in fds.text.split(",")] if fds is not None and fds.text else [], q,
+                          weight))
     # src/fdtd/convert.rs:32-47: OverSampling below 2 → 4; endCriteria
     # absent or 0 → openEMS's default, negative → none; TimeStepFactor
     # outside (0, 1] → 1 and TimeStepMethod other than 1 or 3 → 1 (what
@@ -514,6 +562,8 @@ class Setup:
         self.tol = 1e-3 * min(float(np.min(np.diff(v))) for v in f.lines if len(v) > 1)
         self.lumped_edges = {(a, *e) for a, edges in self._lumped_boxes() for e in edges}
         self._materials(m)
+        if f.cell_constant and any(p.weight for p in f.props):
+            raise NotImplementedError("weighting functions with CellConstantMaterial")
         if not f.cell_constant:
             self._sampled_materials(m)
         # Time step: openEMS's criterion, TimeStepFactor, or TimeStep.
@@ -579,12 +629,15 @@ class Setup:
         bg = f.background
         props = []
         items = []
+        weights = {}  # property index in the table -> weighting functions
         for p in f.props:
             if p.kind not in MATERIALS:
                 continue
             iso = p.attrs.get("Isotropy", "1") != "0"
             props.append([_vec3(p.prop.get(k), dv, iso) for k, dv in
                           (("Epsilon", 1.0), ("Kappa", 0.0), ("Mue", 1.0), ("Sigma", 0.0))])
+            if p.weight:
+                weights[len(props)] = p.weight
             for b in p.boxes:
                 items.append((b.priority, -p.order, len(props) - 1, b))
         items.sort(key=lambda t: (t[0], t[1]))
@@ -592,6 +645,21 @@ class Setup:
                  (("Epsilon", 1.0), ("Kappa", 0.0), ("Mue", 1.0), ("Sigma", 0.0))]
                 if bg else [[1.0] * 3, [0.0] * 3, [1.0] * 3, [0.0] * 3])
         table = np.array([base] + props, dtype=np.float64)  # [prop, quantity, axis]
+        qname = ("Epsilon", "Kappa", "Mue", "Sigma")
+
+        def value(pid, q, a, xs):
+            """Quantity q along a of the samples' materials, each weighted
+            at its sample point (the weighting function of the winning
+            material times its value)."""
+            v = table[pid, q, a]
+            for idx, wt in weights.items():
+                w = wt.get(qname[q])
+                if not w or w[a] is None:
+                    continue
+                I = np.nonzero(pid == idx)
+                if I[0].size:  # (v is a copy: pid indexes the table)
+                    v[I] = v[I] * w[a].evaluate(x=xs[0][I[0]], y=xs[1][I[1]], z=xs[2][I[2]])
+            return v
 
         def winner(xs):
             """Property index (0 background) on the grid of coordinates xs."""
@@ -645,8 +713,8 @@ class Setup:
                     shape[c] = n[c]
                     w = w * wc.reshape(shape)
                     pid = winner(xs)
-                    num_e += w * table[pid, 0, a]
-                    num_k += w * table[pid, 1, a]
+                    num_e += w * value(pid, 0, a, xs)
+                    num_k += w * value(pid, 1, a, xs)
                     den += w
             ok = den > 0
             eps = np.where(ok, num_e / np.where(ok, den, 1.0), 1.0)
@@ -664,8 +732,8 @@ class Setup:
                 shape[a] = n[a]
                 w = np.broadcast_to(wa.reshape(shape), n)
                 pid = winner(xs)
-                mu = table[pid, 2, a]
-                sg = table[pid, 3, a]
+                mu = value(pid, 2, a, xs)
+                sg = value(pid, 3, a, xs)
                 has = w > 0
                 length += w
                 inv_mu += np.where(has, w / mu, 0.0)
@@ -1029,7 +1097,9 @@ class Setup:
                                        for q in range(3)]
                                 if self._excitation_winner(mid) is not p:
                                     continue
-                                out.append((e_type, typ, a, node, exc[a] * length, p))
+                                wx = p.weight.get("Excite", [None] * 3)[a]
+                                g = float(wx.evaluate(x=mid[0], y=mid[1], z=mid[2])) if wx is not None else 1.0
+                                out.append((e_type, typ, a, node, exc[a] * g * length, p))
         return out
 
     def model_delta(self, a, i):
@@ -1104,6 +1174,12 @@ class Setup:
                         iso = best[1].attrs.get("Isotropy", "1") != "0" if best else True
                         eps = _vec3(prop.get("Epsilon"), 1.0, iso)[t] if prop else 1.0
                         mu = _vec3(prop.get("Mue"), 1.0, iso)[o] if prop else 1.0
+                        wt = best[1].weight if best else {}
+                        at = dict(zip("xyz", pt))
+                        if wt.get("Epsilon") and wt["Epsilon"][t] is not None:
+                            eps *= float(wt["Epsilon"][t].evaluate(**at))
+                        if wt.get("Mue") and wt["Mue"][o] is not None:
+                            mu *= float(wt["Mue"][o].evaluate(**at))
                         v[pu, pw] = C0 / math.sqrt(eps * mu)
                 m.set_mur_media(fc, t, v)
 

@@ -66,6 +66,12 @@ CASES = [
     # Mur media, excitation ownership: exact but rs_316, whose weak H probe
     # on the x_min layer face differs by 7.9e-5 (the reference: 7.6e-5).
     ("metal_material_tie", 1e-12), ("rs_3", 1e-12), ("rs_157", 1e-12), ("rs_316", 1e-4),
+    # Materials with weighting functions of x, y, z (isotropic, anisotropic,
+    # on σ_m, a graded layer), evaluated at every sub-cell sample.
+    ("nonuniform_materials", 1e-12), ("sweep_mat_sigma_graded", 1e-12), ("sweep_mat_weight_aniso", 1e-12),
+    ("sweep_mat_weight_coords", 1e-12),
+    # Excitations with weighting functions (evaluated at the edge midpoint).
+    ("custom_weighted", 1e-12), ("sweep_exc_weight", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -195,7 +201,7 @@ def test_probe_skip_warnings():
 
 @have
 @pytest.mark.parametrize("case,why", [
-    ("nonuniform_materials", "weighting"), ("lumped_rc", "series"), ("pml_cyl", "cylindrical"),
+    ("sweep_debye_weight", "weighting"), ("lumped_rc", "series"), ("pml_cyl", "cylindrical"),
     ("sweep_exc_sphere", "Sphere")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
