@@ -286,6 +286,55 @@ class Box:
     p2: tuple
     priority: int = 0
 
+    def inside(self, x, y, z, tol):
+        """Closed inside test with tolerance ``tol`` (drawing units) over
+        broadcastable coordinate arrays."""
+        r = True
+        for q, v in enumerate((x, y, z)):
+            lo, hi = min(self.p1[q], self.p2[q]), max(self.p1[q], self.p2[q])
+            r = r & (v >= lo - tol) & (v <= hi + tol)
+        return r
+
+
+@dataclass
+class Shape:
+    """A sphere, spherical shell, cylinder or cylindrical shell primitive
+    (CSXCAD's closed inside tests, grown by openEMS's inside tolerance;
+    src/compile/openems.rs:5-35); ``p1``/``p2`` its bounding box."""
+    kind: str
+    a: tuple             # centre (spheres) or first axis point (cylinders)
+    b: tuple             # second axis point (cylinders)
+    radius: float
+    width: float         # shell width (0: solid)
+    priority: int
+    p1: tuple = ()
+    p2: tuple = ()
+
+    def __post_init__(self):
+        r = self.radius + 0.5 * self.width
+        pts = [self.a] if self.kind in ("Sphere", "SphericalShell") else [self.a, self.b]
+        self.p1 = tuple(min(p[q] for p in pts) - r for q in range(3))
+        self.p2 = tuple(max(p[q] for p in pts) + r for q in range(3))
+
+    def inside(self, x, y, z, tol):
+        d = [np.asarray(v, dtype=np.float64) - self.a[q] for q, v in enumerate((x, y, z))]
+        if self.kind in ("Sphere", "SphericalShell"):
+            rad = np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2)
+            along = None
+        else:
+            ax = np.array(self.b, dtype=np.float64) - np.array(self.a, dtype=np.float64)
+            length = float(np.sqrt(np.sum(ax * ax)))
+            u = ax / length
+            along = d[0] * u[0] + d[1] * u[1] + d[2] * u[2]
+            rad = np.sqrt(np.maximum(d[0] ** 2 + d[1] ** 2 + d[2] ** 2 - along ** 2, 0.0))
+        if self.width > 0.0:
+            r = np.abs(rad - self.radius) <= 0.5 * self.width + tol
+        else:
+            r = rad <= self.radius + tol
+        if along is not None:
+            r = r & (along >= -tol) & (along <= length + tol)
+        return r
+
 
 @dataclass
 class Prop:
@@ -385,14 +434,27 @@ def parse(text: str) -> OpenEmsFile:
     for q, el in enumerate(list(pr) if pr is not None else []):
         boxes = []
         prims = el.find("Primitives")
+        def pt(e):
+            return tuple(float(e.get(c)) for c in "XYZ")
+
         for b in (list(prims) if prims is not None else []):
-            if b.tag != "Box":
-                raise NotImplementedError(f"primitive {b.tag} in {el.get('Name')!r}")
             if b.find("Transformation") is not None:
                 raise NotImplementedError("transformed primitives")
-            p1, p2 = b.find("P1"), b.find("P2")
-            boxes.append(Box(tuple(float(p1.get(c)) for c in "XYZ"), tuple(float(p2.get(c)) for c in "XYZ"),
-                             int(float(b.get("Priority", "0")))))
+            prio = int(float(b.get("Priority", "0")))
+            if b.tag == "Box":
+                boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
+            elif b.tag == "MultiBox":
+                starts, ends = b.findall("StartP"), b.findall("EndP")
+                boxes += [Box(pt(s0), pt(e0), prio) for s0, e0 in zip(starts, ends)]
+            elif b.tag in ("Sphere", "SphericalShell", "Cylinder", "CylindricalShell") and \
+                    el.tag in MATERIALS + ("Metal",):
+                sph = b.tag.startswith("Spher")
+                a0 = pt(b.find("Center")) if sph else pt(b.find("P1"))
+                b0 = a0 if sph else pt(b.find("P2"))
+                boxes.append(Shape(b.tag, a0, b0, float(b.get("Radius")),
+                                   float(b.get("ShellWidth", "0")) if b.tag.endswith("Shell") else 0.0, prio))
+            else:
+                raise NotImplementedError(f"primitive {b.tag} in {el.get('Name')!r}")
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
                           "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
@@ -562,8 +624,8 @@ class Setup:
         self.tol = 1e-3 * min(float(np.min(np.diff(v))) for v in f.lines if len(v) > 1)
         self.lumped_edges = {(a, *e) for a, edges in self._lumped_boxes() for e in edges}
         self._materials(m)
-        if f.cell_constant and any(p.weight for p in f.props):
-            raise NotImplementedError("weighting functions with CellConstantMaterial")
+        if f.cell_constant and any(p.weight or any(isinstance(b, Shape) for b in p.boxes) for p in f.props):
+            raise NotImplementedError("weighting functions or round primitives with CellConstantMaterial")
         if not f.cell_constant:
             self._sampled_materials(m)
         # Time step: openEMS's criterion, TimeStepFactor, or TimeStep.
@@ -665,11 +727,8 @@ class Setup:
             """Property index (0 background) on the grid of coordinates xs."""
             idx = np.zeros([len(x) for x in xs], dtype=np.int64)
             for _, _, pi, b in items:
-                ins = []
-                for q in range(3):
-                    lo, hi = min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])
-                    ins.append((xs[q] >= lo - self.tol) & (xs[q] <= hi + self.tol))
-                mask = ins[0][:, None, None] & ins[1][None, :, None] & ins[2][None, None, :]
+                mask = np.broadcast_to(b.inside(xs[0][:, None, None], xs[1][None, :, None], xs[2][None, None, :],
+                                                self.tol), idx.shape)
                 idx[mask] = pi + 1
             return idx
 
@@ -764,35 +823,37 @@ class Setup:
             lo = [min(b.p1[a], b.p2[a]) for a in range(3)]
             hi = [max(b.p1[a], b.p2[a]) for a in range(3)]
             if p.kind == "Metal":
-                # Edges whose midpoint lies in the closed box, unless a
-                # material of higher priority (or of equal priority defined
-                # earlier) holds the midpoint too.
+                # Edges whose midpoint lies in the closed primitive, unless
+                # a material of higher priority (or of equal priority
+                # defined earlier) holds the midpoint too, or the edge is a
+                # lumped element's.
                 over = [(ob, op) for (_, _, op, ob) in items if op.kind in MATERIALS and
                         (ob.priority > b.priority or (ob.priority == b.priority and op.order < p.order))]
+                n = self.nodes
                 for a in range(3):
-                    rng = []
+                    xs = []
                     for q in range(3):
-                        pts = cen[q] if q == a else np.array(lines[q])
-                        rng.append([i for i, x in enumerate(pts) if self._inside_prim(x, lo[q], hi[q])])
-                    if not all(rng):
-                        continue
-                    for i in rng[0]:
-                        for j in rng[1]:
-                            run = []
-                            for k in rng[2] + [None]:
-                                keep = k is not None and (a, i, j, k) not in self.lumped_edges
-                                if keep and over:
-                                    mid = [cen[q][x] if q == a else lines[q][x] for q, x in enumerate((i, j, k))]
-                                    keep = not any(all(self._inside_prim(mid[q], min(ob.p1[q], ob.p2[q]),
-                                                                    max(ob.p1[q], ob.p2[q])) for q in range(3))
-                                                   for ob, _ in over)
-                                if keep and run and k == run[-1] + 1:
-                                    run.append(k)
-                                    continue
-                                if run:
-                                    m.pec_edges(a, [i, j, run[0]], [i, j, run[-1]])
-                                run = [k] if keep else []
+                        v = np.array(lines[q], dtype=np.float64)
+                        if q == a:
+                            v = np.concatenate([cen[q], [1e30]])  # no edge from the last line
+                        shape = [1, 1, 1]
+                        shape[q] = n[q]
+                        xs.append(v.reshape(shape))
+                    mask = np.broadcast_to(b.inside(xs[0], xs[1], xs[2], self.tol), tuple(n)).copy()
+                    for ob, _ in over:
+                        mask &= ~np.broadcast_to(ob.inside(xs[0], xs[1], xs[2], self.tol), tuple(n))
+                    for (a2, i, j, k) in self.lumped_edges:
+                        if a2 == a:
+                            mask[i, j, k] = False
+                    for i, j in zip(*np.nonzero(mask.any(axis=2))):
+                        row = np.concatenate([[False], mask[i, j], [False]]).astype(np.int8)
+                        st = np.flatnonzero(np.diff(row) == 1)
+                        en = np.flatnonzero(np.diff(row) == -1) - 1
+                        for k0, k1 in zip(st, en):
+                            m.pec_edges(a, [int(i), int(j), int(k0)], [int(i), int(j), int(k1)])
                 continue
+            if isinstance(b, Shape):
+                continue  # round materials: sampled per edge
             cells = [[i for i, x in enumerate(cen[a]) if self._inside(a, x, lo[a], hi[a])] for a in range(3)]
             if not all(cells):
                 continue
@@ -902,7 +963,7 @@ class Setup:
             if p.kind not in MATERIALS + ("Metal",):
                 continue
             for b in p.boxes:
-                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
+                if bool(b.inside(pt[0], pt[1], pt[2], self.tol)):
                     key = (b.priority, -p.order)
                     if best is None or key > best[0]:
                         best = (key, p)
@@ -1165,8 +1226,7 @@ class Setup:
                         best = None
                         for p in mats:
                             for b in p.boxes:
-                                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q]))
-                                       for q in range(3)):
+                                if bool(b.inside(pt[0], pt[1], pt[2], self.tol)):
                                     key = (b.priority, -p.order)
                                     if best is None or key > best[0]:
                                         best = (key, p)

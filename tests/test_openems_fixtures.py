@@ -72,6 +72,11 @@ CASES = [
     ("sweep_mat_weight_coords", 1e-12),
     # Excitations with weighting functions (evaluated at the edge midpoint).
     ("custom_weighted", 1e-12), ("sweep_exc_weight", 1e-12),
+    # Spheres, spherical and cylindrical shells, oblique cylinders and
+    # multi-boxes, as materials (sampled per edge) and as metal.
+    ("sweep_prim_cyl_oblique", 1e-12), ("sweep_prim_multibox", 1e-12), ("sweep_prim_sphshell", 1e-12),
+    ("sweep_prim_sphshell_metal", 1e-12), ("sweep_tie_cyl_metal", 1e-12), ("sweep_tie_cylshell_metal", 1e-12),
+    ("sweep_tie_sphere_metal", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -202,7 +207,7 @@ def test_probe_skip_warnings():
 @have
 @pytest.mark.parametrize("case,why", [
     ("sweep_debye_weight", "weighting"), ("lumped_rc", "series"), ("pml_cyl", "cylindrical"),
-    ("sweep_exc_sphere", "Sphere")])
+    ("sweep_exc_sphere", "Sphere"), ("sweep_prim_polyhedron_cube", "Polyhedron")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
         OE.load(os.path.join(FIXTURES, case, "model.xml"))
