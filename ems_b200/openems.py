@@ -296,6 +296,63 @@ class Box:
         return r
 
 
+def _transform_matrix(el) -> np.ndarray:
+    """The 4×4 matrix of a CSXCAD <Transformation>: its operations applied
+    to the primitive in the order written (Translate, Rotate_X/Y/Z by an
+    angle in radians, Rotate_Origin about an axis through the origin, Scale,
+    Scale3, Matrix given row by row)."""
+    M = np.eye(4)
+    for op in el:
+        a = [float(v) for v in op.get("Argument", "").split(",") if v.strip()]
+        T = np.eye(4)
+        if op.tag == "Translate":
+            T[:3, 3] = a[:3]
+        elif op.tag in ("Rotate_X", "Rotate_Y", "Rotate_Z", "Rotate_Origin"):
+            if op.tag == "Rotate_Origin":
+                ax, ang = np.array(a[:3]), a[3]
+            else:
+                ax, ang = np.eye(3)["XYZ".index(op.tag[-1])], a[0]
+            k = ax / np.linalg.norm(ax)
+            K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+            T[:3, :3] = np.eye(3) + math.sin(ang) * K + (1.0 - math.cos(ang)) * (K @ K)
+        elif op.tag == "Scale":
+            T[:3, :3] *= a[0]
+        elif op.tag == "Scale3":
+            T[:3, :3] = np.diag(a[:3])
+        elif op.tag == "Matrix":
+            T = np.array(a[:16]).reshape(4, 4)
+        else:
+            raise NotImplementedError(f"transformation {op.tag}")
+        M = T @ M
+    return M
+
+
+@dataclass
+class Transformed:
+    """A primitive under a transformation: the inside test of the
+    primitive at the point mapped back, with the tolerance divided by the
+    transformation's smallest singular value (src/compile/openems.rs:
+    12-16); ``p1``/``p2`` the transformed bounding box."""
+    prim: object
+    M: np.ndarray
+    priority: int
+    p1: tuple = ()
+    p2: tuple = ()
+
+    def __post_init__(self):
+        self.Minv = np.linalg.inv(self.M)
+        self.smin = float(np.linalg.svd(self.M[:3, :3], compute_uv=False).min())
+        c = np.array([[x, y, z, 1.0] for x in (self.prim.p1[0], self.prim.p2[0])
+                      for y in (self.prim.p1[1], self.prim.p2[1]) for z in (self.prim.p1[2], self.prim.p2[2])])
+        w = (self.M @ c.T)[:3]
+        self.p1, self.p2 = tuple(w.min(axis=1)), tuple(w.max(axis=1))
+
+    def inside(self, x, y, z, tol):
+        R = self.Minv
+        loc = [R[r, 0] * x + R[r, 1] * y + R[r, 2] * z + R[r, 3] for r in range(3)]
+        return self.prim.inside(loc[0], loc[1], loc[2], tol / self.smin)
+
+
 @dataclass
 class Shape:
     """A sphere, spherical shell, cylinder or cylindrical shell primitive
@@ -438,8 +495,12 @@ def parse(text: str) -> OpenEmsFile:
             return tuple(float(e.get(c)) for c in "XYZ")
 
         for b in (list(prims) if prims is not None else []):
-            if b.find("Transformation") is not None:
+            tr = b.find("Transformation")
+            if tr is not None and (el.tag not in MATERIALS + ("Metal",) or b.tag not in
+                                   ("Box", "Sphere", "SphericalShell", "Cylinder", "CylindricalShell")):
                 raise NotImplementedError("transformed primitives")
+            if b.get("CoordSystem", "0") != "0":
+                raise NotImplementedError(f"primitive {b.tag} in cylindrical coordinates")
             prio = int(float(b.get("Priority", "0")))
             if b.tag == "Box":
                 boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
@@ -455,6 +516,8 @@ def parse(text: str) -> OpenEmsFile:
                                    float(b.get("ShellWidth", "0")) if b.tag.endswith("Shell") else 0.0, prio))
             else:
                 raise NotImplementedError(f"primitive {b.tag} in {el.get('Name')!r}")
+            if tr is not None:
+                boxes[-1] = Transformed(boxes[-1], _transform_matrix(tr), prio)
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
                           "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
@@ -624,7 +687,7 @@ class Setup:
         self.tol = 1e-3 * min(float(np.min(np.diff(v))) for v in f.lines if len(v) > 1)
         self.lumped_edges = {(a, *e) for a, edges in self._lumped_boxes() for e in edges}
         self._materials(m)
-        if f.cell_constant and any(p.weight or any(isinstance(b, Shape) for b in p.boxes) for p in f.props):
+        if f.cell_constant and any(p.weight or any(not isinstance(b, Box) for b in p.boxes) for p in f.props):
             raise NotImplementedError("weighting functions or round primitives with CellConstantMaterial")
         if not f.cell_constant:
             self._sampled_materials(m)
@@ -852,8 +915,8 @@ class Setup:
                         for k0, k1 in zip(st, en):
                             m.pec_edges(a, [int(i), int(j), int(k0)], [int(i), int(j), int(k1)])
                 continue
-            if isinstance(b, Shape):
-                continue  # round materials: sampled per edge
+            if not isinstance(b, Box):
+                continue  # round and transformed materials: sampled per edge
             cells = [[i for i, x in enumerate(cen[a]) if self._inside(a, x, lo[a], hi[a])] for a in range(3)]
             if not all(cells):
                 continue

@@ -77,6 +77,10 @@ CASES = [
     ("sweep_prim_cyl_oblique", 1e-12), ("sweep_prim_multibox", 1e-12), ("sweep_prim_sphshell", 1e-12),
     ("sweep_prim_sphshell_metal", 1e-12), ("sweep_tie_cyl_metal", 1e-12), ("sweep_tie_cylshell_metal", 1e-12),
     ("sweep_tie_sphere_metal", 1e-12),
+    # Transformed primitives (matrix, translate then rotate, rotation about
+    # an axis, a scaled sphere).
+    ("sweep_tr_matrix", 1e-12), ("sweep_tr_order", 1e-12), ("sweep_tr_rotate_origin", 1e-12),
+    ("sweep_tr_sphere", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
