@@ -442,8 +442,64 @@ def _vec3(text, default, isotropic=True):
     return (v + [default] * 3)[:3]
 
 
+def _face(v: str):
+    """openEMS's reading of a boundary name (src/io/openems/model.rs:11-18):
+    PEC, PMC, MUR and PML_<n> case sensitive; a value starting with a digit
+    or sign by its integer prefix (0 PEC, 1 PMC, 2 MUR, 3 PML_8, else PEC);
+    PML_<n> by the integer prefix of <n> (n <= 0: PEC); anything else PEC."""
+    if v and (v[0].isdigit() or v[0] in "+-"):
+        m = re.match(r"[+-]?\d+", v)
+        k = int(m.group(0)) if m else 0
+        return {1: (PMC_FACE, None), 2: (MUR_FACE, None), 3: (PML_FACE, 8)}.get(k, (PEC_FACE, None))
+    if v == "PMC":
+        return (PMC_FACE, None)
+    if v == "MUR":
+        return (MUR_FACE, None)
+    if v.startswith("PML_"):
+        m = re.match(r"[+-]?\d+", v[4:])
+        if m and int(m.group(0)) > 0:
+            return (PML_FACE, int(m.group(0)))
+    return (PEC_FACE, None)
+
+
+def _parameters(root):
+    """The file's <ParameterSet> constants substituted into the numeric
+    attributes of primitives and material properties (openEMS evaluates
+    them there); the document re-parsed if any were given."""
+    ps = root.find("ContinuousStructure/ParameterSet")
+    if ps is None:
+        return root
+    env = {}
+    for p in ps:
+        if p.get("name") is not None and p.get("value") is not None:
+            env[p.get("name")] = float(p.get("value"))
+    if not env:
+        return root
+
+    def number(t):
+        try:
+            float(t)
+            return t
+        except ValueError:
+            return repr(float(Expression(t, tuple(env)).evaluate(**env)))
+
+    pr = root.find("ContinuousStructure/Properties")
+    for el in (pr.iter() if pr is not None else []):
+        if el.tag in ("Weight", "Attributes"):
+            continue
+        for k, v in list(el.attrib.items()):
+            if k in ("Name", "Function"):
+                continue
+            parts = v.split(",")
+            try:
+                el.set(k, ",".join(number(x.strip()) for x in parts))
+            except ValueError:
+                pass
+    return root
+
+
 def parse(text: str) -> OpenEmsFile:
-    root = ET.fromstring(text)
+    root = _parameters(ET.fromstring(text))
     fd = root.find("FDTD")
     if fd is None:
         raise ValueError("no <FDTD> element")
@@ -464,18 +520,7 @@ def parse(text: str) -> OpenEmsFile:
     bc = fd.find("BoundaryCond")
     faces = []
     for name in FACE_NAMES:
-        v = (bc.get(name) if bc is not None else None) or "PEC"
-        u = v.upper()
-        if u in ("PEC", "0"):
-            faces.append((PEC_FACE, None))
-        elif u in ("PMC", "1"):
-            faces.append((PMC_FACE, None))
-        elif u in ("MUR", "2"):
-            faces.append((MUR_FACE, None))
-        elif u == "3" or re.fullmatch(r"PML_\d+", u):
-            faces.append((PML_FACE, 8 if u == "3" else int(u[4:])))
-        else:
-            raise NotImplementedError(f"boundary {v!r} on {name}")
+        faces.append(_face((bc.get(name) if bc is not None else None) or "PEC"))
     mur_v = _f(bc.get("MUR_PhaseVelocity")) if bc is not None else None
     cs = root.find("ContinuousStructure")
     grid = cs.find("RectilinearGrid")
@@ -484,7 +529,7 @@ def parse(text: str) -> OpenEmsFile:
     unit = float(grid.get("DeltaUnit", "1"))
     lines = []
     for tag in ("XLines", "YLines", "ZLines"):
-        v = sorted(float(x) for x in grid.find(tag).text.split(","))
+        v = sorted(set(float(x) for x in grid.find(tag).text.split(",")))  # openEMS sorts, drops repeats
         lines.append(v)
     props = []
     pr = cs.find("Properties")
@@ -531,7 +576,10 @@ def parse(text: str) -> OpenEmsFile:
             weight["Excite"] = [None if wel.get(c, "1").strip() in ("1", "1.0") else
                                 Expression(wel.get(c), ("x", "y", "z")) for c in "XYZ"]
         elif wel is not None:
-            if el.tag not in MATERIALS or set(wel.attrib) - {"Epsilon", "Mue", "Kappa", "Sigma"}:
+            poles = {"EpsilonPlasmaFrequency", "EpsilonLorPoleFrequency", "EpsilonRelaxTime", "EpsilonDelta",
+                     "MuePlasmaFrequency", "MueLorPoleFrequency", "MueRelaxTime", "MueDelta"}
+            allowed = {"Epsilon", "Mue", "Kappa", "Sigma"} | (poles if el.tag != "Material" else set())
+            if el.tag not in MATERIALS or set(wel.attrib) - allowed:
                 raise NotImplementedError(f"weighting functions ({el.get('Name')!r})")
             iso = el.get("Isotropy", "1") != "0"
             for key, text in wel.attrib.items():
@@ -554,7 +602,7 @@ def parse(text: str) -> OpenEmsFile:
     method = int(float(fd.get("TimeStepMethod", "3")))
     bg = cs.find("BackgroundMaterial")
     for el in cs:
-        if el.tag not in ("Properties", "RectilinearGrid", "BackgroundMaterial"):
+        if el.tag not in ("Properties", "RectilinearGrid", "BackgroundMaterial", "ParameterSet"):
             raise NotImplementedError(f"<{el.tag}> in the structure")
     return OpenEmsFile(lines, unit, int(float(fd.get("NumberOfTimesteps", "0"))), end,
                        _f(fd.get("MaxTime")), _f(fd.get("TimeStep")),
@@ -1089,13 +1137,13 @@ class Setup:
                             w = self._winner(pt)
                             if w is None or w.kind not in ("LorentzMaterial", "DebyeMaterial"):
                                 continue
-                            for pole in self._poles(w, field_, a, 1.0):
+                            for pole in self._poles(w, field_, a, 1.0, pt):
                                 d.add_edge(field_, a, node, pole)
                                 count += 1
         if count:
             m.add_dispersive(d, OPENEMS_POLES)
 
-    def _poles(self, p, field_, a, inf):
+    def _poles(self, p, field_, a, inf, pt=None):
         from . import Pole
         iso = p.attrs.get("Isotropy", "1") != "0"
         order = int(float(p.attrs.get("Order", "1")))
@@ -1105,9 +1153,16 @@ class Setup:
             def get(name, q=q):
                 # "<name>_<order>", or for the first order also "<name>".
                 v = p.prop.get(f"{pre}{name}_{q}")
+                key = f"{pre}{name}_{q}"
                 if v is None and q == 1:
                     v = p.prop.get(f"{pre}{name}")
-                return _vec3(v, 0.0, iso)[a]
+                    key = f"{pre}{name}"
+                x = _vec3(v, 0.0, iso)[a]
+                # A weighting function of the parameter, at the edge midpoint.
+                wf = p.weight.get(key) or (p.weight.get(f"{pre}{name}") if q == 1 else None)
+                if wf and wf[a] is not None and pt is not None:
+                    x *= float(wf[a].evaluate(x=pt[0], y=pt[1], z=pt[2]))
+                return x
 
             if p.kind == "DebyeMaterial":
                 if field_ == 1:

@@ -81,6 +81,10 @@ CASES = [
     # an axis, a scaled sphere).
     ("sweep_tr_matrix", 1e-12), ("sweep_tr_order", 1e-12), ("sweep_tr_rotate_origin", 1e-12),
     ("sweep_tr_sphere", 1e-12),
+    # openEMS's reading of boundary names, unsorted and repeated mesh lines,
+    # ParameterSet constants, weighting functions of pole parameters.
+    ("sweep_bc_spellings", 1e-12), ("sweep_grid_unsorted", 1e-12), ("sweep_param_set", 1e-12),
+    ("sweep_debye_weight", 1e-12), ("sweep_lorentz_weight", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -210,7 +214,7 @@ def test_probe_skip_warnings():
 
 @have
 @pytest.mark.parametrize("case,why", [
-    ("sweep_debye_weight", "weighting"), ("lumped_rc", "series"), ("pml_cyl", "cylindrical"),
+    ("lumped_rc", "series"), ("pml_cyl", "cylindrical"),
     ("sweep_exc_sphere", "Sphere"), ("sweep_prim_polyhedron_cube", "Polyhedron")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
