@@ -566,8 +566,8 @@ def parse(text: str) -> OpenEmsFile:
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
                           "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
-        if el.tag == "ProbeBox" and len(boxes) > 1:
-            raise NotImplementedError(f"probe {el.get('Name')!r} with several primitives")
+        if el.tag == "ProbeBox" and any(not isinstance(b, Box) for b in boxes):
+            raise NotImplementedError(f"probe {el.get('Name')!r} on a primitive other than a box")
         weight = {}
         wel = el.find("Weight")
         if wel is not None and el.tag == "Excitation":
@@ -588,9 +588,16 @@ def parse(text: str) -> OpenEmsFile:
                 weight[key] = [None if t in ("1", "1.0") else Expression(t, ("x", "y", "z")) for t in parts]
         sub = el.find("Property")
         fds = el.find("FD_Samples")
+        fd_list = [float(x) for x in fds.text.split(",")] if fds is not None and fds.text else []
+        if el.tag == "ProbeBox" and len(boxes) > 1:
+            # Several primitives: several probes <name>_0, <name>_1, … in
+            # primitive order, one file each (src/io/openems/model.rs:27-29).
+            for t, b in enumerate(boxes):
+                props.append(Prop(el.tag, f"{el.get('Name', '')}_{t}", dict(el.attrib),
+                                  dict(sub.attrib) if sub is not None else {}, [b], fd_list, q, weight))
+            continue
         props.append(Prop(el.tag, el.get("Name", ""), dict(el.attrib), dict(sub.attrib) if sub is not None else {},
-                          boxes, [float(x) for x in fds.text.split(",")] if fds is not None and fds.text else [], q,
-                          weight))
+                          boxes, fd_list, q, weight))
     # src/fdtd/convert.rs:32-47: OverSampling below 2 → 4; endCriteria
     # absent or 0 → openEMS's default, negative → none; TimeStepFactor
     # outside (0, 1] → 1 and TimeStepMethod other than 1 or 3 → 1 (what

@@ -85,6 +85,8 @@ CASES = [
     # ParameterSet constants, weighting functions of pole parameters.
     ("sweep_bc_spellings", 1e-12), ("sweep_grid_unsorted", 1e-12), ("sweep_param_set", 1e-12),
     ("sweep_debye_weight", 1e-12), ("sweep_lorentz_weight", 1e-12),
+    # A probe box of two primitives: two probes, <name>_0 and <name>_1.
+    ("sweep_probe_two_prims", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
