@@ -354,6 +354,71 @@ class Transformed:
 
 
 @dataclass
+class LinPoly:
+    """An extruded polygon (CSXCAD LinPoly): vertices (X1, X2) in the plane
+    normal to ``normal`` (X1 along the next axis, X2 along the one after),
+    from ``elevation`` over ``length``; the inside test closed, the polygon
+    grown by the tolerance along the bisectors of its corners and the
+    extrusion by the tolerance at both ends (src/compile/openems.rs:
+    386-460)."""
+    normal: int
+    elevation: float
+    length: float
+    vertices: list
+    priority: int
+    p1: tuple = ()
+    p2: tuple = ()
+
+    def __post_init__(self):
+        n, u, w = self.normal, (self.normal + 1) % 3, (self.normal + 2) % 3
+        lo, hi = [0.0] * 3, [0.0] * 3
+        lo[n], hi[n] = sorted((self.elevation, self.elevation + self.length))
+        lo[u], hi[u] = min(v[0] for v in self.vertices), max(v[0] for v in self.vertices)
+        lo[w], hi[w] = min(v[1] for v in self.vertices), max(v[1] for v in self.vertices)
+        self.p1, self.p2 = tuple(lo), tuple(hi)
+
+    def _grown(self, t):
+        v = self.vertices
+        k = len(v)
+        area = sum(v[i][0] * v[(i + 1) % k][1] - v[(i + 1) % k][0] * v[i][1] for i in range(k))
+        sign = 1.0 if area >= 0.0 else -1.0
+
+        def normal(i):
+            a, b = v[i], v[(i + 1) % k]
+            dx, dy = b[0] - a[0], b[1] - a[1]
+            ln = math.hypot(dx, dy)
+            return (sign * dy / ln, -sign * dx / ln) if ln > 0 else None
+
+        out = []
+        for i in range(k):
+            prev = next((normal((i - j) % k) for j in range(1, k) if normal((i - j) % k)), None)
+            q = normal(i)
+            if prev and q:
+                d = 1.0 + prev[0] * q[0] + prev[1] * q[1]
+                m = ((prev[0] + q[0]) / d, (prev[1] + q[1]) / d) if d > 1e-6 else q
+            else:
+                m = prev or q or (0.0, 0.0)
+            out.append((v[i][0] + t * m[0], v[i][1] + t * m[1]))
+        return out
+
+    def inside(self, x, y, z, tol):
+        c = [np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64), np.asarray(z, dtype=np.float64)]
+        n, u, w = self.normal, (self.normal + 1) % 3, (self.normal + 2) % 3
+        lo, hi = sorted((self.elevation, self.elevation + self.length))
+        r = (c[n] >= lo - tol) & (c[n] <= hi + tol)
+        P, Q = np.broadcast_arrays(c[u], c[w])
+        g = self._grown(tol)
+        ins = np.zeros(P.shape, dtype=bool)
+        for i in range(len(g)):
+            (x0, y0), (x1, y1) = g[i], g[(i + 1) % len(g)]
+            cross = ((y0 > Q) != (y1 > Q))
+            with np.errstate(all="ignore"):
+                xi = x0 + (Q - y0) * (x1 - x0) / (y1 - y0)
+            ins ^= cross & (P < xi)
+        return r & ins
+
+
+@dataclass
 class Shape:
     """A sphere, spherical shell, cylinder or cylindrical shell primitive
     (CSXCAD's closed inside tests, grown by openEMS's inside tolerance;
@@ -552,6 +617,10 @@ def parse(text: str) -> OpenEmsFile:
             elif b.tag == "MultiBox":
                 starts, ends = b.findall("StartP"), b.findall("EndP")
                 boxes += [Box(pt(s0), pt(e0), prio) for s0, e0 in zip(starts, ends)]
+            elif b.tag == "LinPoly" and el.tag in MATERIALS + ("Metal",) and tr is None:
+                verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
+                boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
+                                     float(b.get("Length", "0")), verts, prio))
             elif b.tag in ("Sphere", "SphericalShell", "Cylinder", "CylindricalShell") and \
                     el.tag in MATERIALS + ("Metal",):
                 sph = b.tag.startswith("Spher")

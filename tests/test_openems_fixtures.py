@@ -87,6 +87,8 @@ CASES = [
     ("sweep_debye_weight", 1e-12), ("sweep_lorentz_weight", 1e-12),
     # A probe box of two primitives: two probes, <name>_0 and <name>_1.
     ("sweep_probe_two_prims", 1e-12),
+    # Extruded polygons as a material and as metal.
+    ("sweep_prim_linpoly_y", 1e-12), ("sweep_tie_linpoly_metal", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
