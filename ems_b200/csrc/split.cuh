@@ -372,8 +372,12 @@ __device__ __forceinline__ void poles_edge_core(const Fields& f, const Coeffs& c
             s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
         }
     }
-    const float u_new = (float)__ddiv_rn(__dsub_rn((double)u32, __dmul_rn(cb, s)),
-                                         __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
+    // Without trapezoidal poles the denominator is exactly 1 (sum_inv_z = 0)
+    // and the quotient is the numerator itself.
+    const double num = __dsub_rn((double)u32, __dmul_rn(cb, s));
+    const float u_new = R.sum_inv_z == 0.0
+                            ? (float)num
+                            : (float)__ddiv_rn(num, __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
     if (R.kinds != (1u << R.np) - 1u) {
         const double half_new = __dmul_rn(0.5, (double)u_new);
         for (uint32_t q = 0; q < R.np; ++q) {
