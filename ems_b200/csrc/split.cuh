@@ -182,7 +182,7 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
 }
 
 template <bool OE = false>
-__global__ void __launch_bounds__(kSplitThreads) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
+__global__ void __launch_bounds__(kSplitThreads, 7) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
     split_e_quad<OE>(P, i0 + blockIdx.y, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
 }
 
