@@ -617,6 +617,10 @@ def parse(text: str) -> OpenEmsFile:
             elif b.tag == "MultiBox":
                 starts, ends = b.findall("StartP"), b.findall("EndP")
                 boxes += [Box(pt(s0), pt(e0), prio) for s0, e0 in zip(starts, ends)]
+            elif b.tag in ("Cylinder", "CylindricalShell") and el.tag == "ProbeBox" and tr is None:
+                # A probe on a cylinder: the box between its axis points
+                # (a zero-length cylinder is a point probe).
+                boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
             elif b.tag == "LinPoly" and el.tag in MATERIALS + ("Metal",) and tr is None:
                 verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
