@@ -597,6 +597,7 @@ def parse(text: str) -> OpenEmsFile:
         v = sorted(set(float(x) for x in grid.find(tag).text.split(",")))  # openEMS sorts, drops repeats
         lines.append(v)
     props = []
+    skipped_probes = []  # probes on primitives openEMS writes nothing for
     pr = cs.find("Properties")
     for q, el in enumerate(list(pr) if pr is not None else []):
         boxes = []
@@ -618,9 +619,12 @@ def parse(text: str) -> OpenEmsFile:
                 starts, ends = b.findall("StartP"), b.findall("EndP")
                 boxes += [Box(pt(s0), pt(e0), prio) for s0, e0 in zip(starts, ends)]
             elif b.tag in ("Cylinder", "CylindricalShell") and el.tag == "ProbeBox" and tr is None:
-                # A probe on a cylinder: the box between its axis points
-                # (a zero-length cylinder is a point probe).
-                boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
+                # A probe on a zero-length cylinder is a point probe; openEMS
+                # writes no file for one on a longer cylinder.
+                if pt(b.find("P1")) == pt(b.find("P2")):
+                    boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
+                else:
+                    skipped_probes.append(el.get("Name", ""))
             elif b.tag == "LinPoly" and el.tag in MATERIALS + ("Metal",) and tr is None:
                 verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
@@ -639,6 +643,8 @@ def parse(text: str) -> OpenEmsFile:
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
                           "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
+        if el.tag == "ProbeBox" and not boxes and skipped_probes and skipped_probes[-1] == el.get("Name", ""):
+            continue
         if el.tag == "ProbeBox" and any(not isinstance(b, Box) for b in boxes):
             raise NotImplementedError(f"probe {el.get('Name')!r} on a primitive other than a box")
         weight = {}

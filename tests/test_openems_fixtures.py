@@ -89,8 +89,8 @@ CASES = [
     ("sweep_probe_two_prims", 1e-12),
     # Extruded polygons as a material and as metal.
     ("sweep_prim_linpoly_y", 1e-12), ("sweep_tie_linpoly_metal", 1e-12),
-    # Probes on cylinders (the box between the axis points; current-probe
-    # corners half-way between lines).
+    # Probes on cylinders (a zero-length one is a point probe; openEMS
+    # writes nothing for one on a longer cylinder).
     ("current_probe_ties", 1e-12), ("sweep_probe_cylinder_prim", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
