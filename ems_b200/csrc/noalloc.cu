@@ -83,12 +83,15 @@ __global__ void __launch_bounds__(1024) k_energy_total(const double* partials, u
 }
 
 // The device address of `scratch` on each device, found once per device
-// (cudaGetSymbolAddress with that device current).
+// (cudaGetSymbolAddress with that device current), for device ordinals
+// 0..kMaxDevices-1. An address stays cached after a cudaDeviceReset of its
+// device, when it no longer holds.
+constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double* g_scratch[64] = {};
+double* g_scratch[kMaxDevices] = {};
 
 ems_status scratch_on(int device, double** out) {
-    if (device < 0 || device >= 64) return EMS_ERR_INVALID;
+    if (device < 0 || device >= kMaxDevices) return EMS_ERR_INVALID;
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch[device]) {
         void* p = nullptr;
@@ -106,9 +109,11 @@ extern "C" ems_status ems_energy_noalloc(const uint64_t nodes[3], double dt, con
                                          void* stream) {
     if (!nodes || !u || !i || !coeff || !energy || !(dt > 0.0)) return EMS_ERR_INVALID;
     if (nodes[0] < 2 || nodes[1] < 2 || nodes[2] < 2) return EMS_ERR_INVALID;
+    // The product is checked factor by factor, so it cannot wrap: beyond
+    // kMaxNodes the kernel's 32-bit node indexing would not hold.
+    if (nodes[0] > kMaxNodes || nodes[1] > kMaxNodes / nodes[0]) return EMS_ERR_INVALID;
+    if (nodes[2] > kMaxNodes / (nodes[0] * nodes[1])) return EMS_ERR_INVALID;
     const uint64_t n = nodes[0] * nodes[1] * nodes[2];
-    if (n > kMaxNodes || nodes[0] > kMaxNodes || nodes[1] > kMaxNodes || nodes[2] > kMaxNodes)
-        return EMS_ERR_INVALID;  // beyond the 32-bit node indexing of the kernel
     Arrays A;
     for (int a = 0; a < 3; ++a) {
         if (!u[a] || !i[a]) return EMS_ERR_INVALID;

@@ -597,10 +597,10 @@ def parse(text: str) -> OpenEmsFile:
         v = sorted(set(float(x) for x in grid.find(tag).text.split(",")))  # openEMS sorts, drops repeats
         lines.append(v)
     props = []
-    skipped_probes = []  # probes on primitives openEMS writes nothing for
     pr = cs.find("Properties")
     for q, el in enumerate(list(pr) if pr is not None else []):
         boxes = []
+        only_long_cylinders = False  # a probe whose primitives openEMS writes nothing for
         prims = el.find("Primitives")
         def pt(e):
             return tuple(float(e.get(c)) for c in "XYZ")
@@ -624,7 +624,7 @@ def parse(text: str) -> OpenEmsFile:
                 if pt(b.find("P1")) == pt(b.find("P2")):
                     boxes.append(Box(pt(b.find("P1")), pt(b.find("P2")), prio))
                 else:
-                    skipped_probes.append(el.get("Name", ""))
+                    only_long_cylinders = True
             elif b.tag == "LinPoly" and el.tag in MATERIALS + ("Metal",) and tr is None:
                 verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
@@ -643,7 +643,7 @@ def parse(text: str) -> OpenEmsFile:
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
                           "LumpedElement"):
             raise NotImplementedError(f"property {el.tag}")
-        if el.tag == "ProbeBox" and not boxes and skipped_probes and skipped_probes[-1] == el.get("Name", ""):
+        if el.tag == "ProbeBox" and not boxes and only_long_cylinders:
             continue
         if el.tag == "ProbeBox" and any(not isinstance(b, Box) for b in boxes):
             raise NotImplementedError(f"probe {el.get('Name')!r} on a primitive other than a box")

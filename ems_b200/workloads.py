@@ -132,7 +132,7 @@ def patch_antenna(scale: float = 1.0, seed: int = 0x5EED, steps: int = 30000, cp
     sub = 60.0 * mm
     patch = 28.0 * mm
     h = 1.6 * mm
-    air = 25.0 * mm * scale
+    air = 30.0 * mm * scale
     lx = sub + 2 * air
     c = lx / 2
     fine, coarse = 0.25 * mm / scale, 1.0 * mm / scale
@@ -141,9 +141,9 @@ def patch_antenna(scale: float = 1.0, seed: int = 0x5EED, steps: int = 30000, cp
              (c + 8 * mm - 0.5 * mm, c + 8 * mm + 0.5 * mm)]
     xl = graded_lines(lx, fine, coarse, edges, 1.08, rng, 0.1)
     yl = graded_lines(lx, fine, coarse, edges[:4] + [(c - 0.5 * mm, c + 0.5 * mm)], 1.08, rng, 0.1)
-    lz = h + 30.0 * mm * scale
+    lz = h + 62.0 * mm * scale
     zl_sub = np.linspace(0.0, h, 8)
-    zl_air = graded_lines(lz - h, fine, coarse * 2.0, [(0.0, 0.5 * mm)], 1.1, rng, 0.1) + h
+    zl_air = graded_lines(lz - h, fine, coarse, [(0.0, 0.5 * mm)], 1.1, rng, 0.1) + h
     zl = np.concatenate([zl_sub, zl_air[1:]])
     m = E.Model(xl, yl, zl)
     near = lambda lines, v: int(np.argmin(np.abs(lines - v)))  # noqa: E731

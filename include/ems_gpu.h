@@ -292,8 +292,7 @@ ems_status ems_gpu_source_amplitude(ems_gpu* h, size_t op, uint64_t first, const
 /* The energy invariant W^n of a field state, for callers that cannot
  * allocate device memory when they need it (a framework that owns all
  * device memory through its own pool, a real-time loop that must not
- * allocate after start-up). It has no counterpart in the reference: there
- * the engine evaluates W^n on its own fields (Engine::energy).
+ * allocate after start-up). It has no counterpart in the reference.
  *
  * u, i: the six field arrays, i holding i^{n-1/2}; coeff: the twelve
  * coefficient arrays; all device arrays in the reference layout
@@ -306,8 +305,11 @@ ems_status ems_gpu_source_amplitude(ems_gpu* h, size_t op, uint64_t first, const
  * GPU which loads the library holds until the process exits. At most
  * 2^31 - 1 nodes (EMS_ERR_INVALID beyond). The first call on a device looks
  * up that array's address (cudaGetSymbolAddress, with the device current)
- * and should come before any stream capture. All calls share the array:
- * calls that overlap on the GPU (other streams, other host threads) race. */
+ * and should come before any stream capture; device ordinals 0..63 only
+ * (EMS_ERR_INVALID beyond), and an address looked up before a
+ * cudaDeviceReset of its device is kept and no longer valid after it. All
+ * calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race. */
 ems_status ems_energy_noalloc(const uint64_t nodes[3], double dt, const float* const u[3], const float* const i[3],
                               const float* const coeff[12], double* energy, void* stream);
 

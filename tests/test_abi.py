@@ -55,6 +55,20 @@ def test_null_arguments_are_rejected_without_a_device():
     assert lib.ems_gpu_last_error(None) == b"null handle"
 
 
+def test_noalloc_size_checks_without_a_device():
+    """ems_energy_noalloc validates its sizes before any CUDA call, so the
+    refusals run here: a node count beyond 2^31 − 1, one whose product wraps
+    in 64 bits to a small number, and a dimension under 2."""
+    lib = E.gpu_lib()
+    dummy = (C.c_float * 4)()
+    p3 = (C.c_void_p * 3)(*[C.addressof(dummy)] * 3)
+    p12 = (C.c_void_p * 12)(*[C.addressof(dummy)] * 12)
+    out = C.c_double()
+    for dims in [(2048, 2048, 1024), (131073, 65537, 2147434497), (2**63, 2**62, 8), (1, 2, 2)]:
+        nodes = (C.c_uint64 * 3)(*dims)
+        assert lib.ems_energy_noalloc(nodes, 1e-12, p3, p3, p12, C.byref(out), None) == 1, dims
+
+
 def test_gpu_library_is_sm100a():
     """The engine is compiled for sm_100a only (no other SASS or PTX)."""
     from ems_b200 import build

@@ -34,7 +34,8 @@ from ems_b200 import openems as OE
 from ems_b200 import probe_files as PF
 from oracle import OracleEngine
 
-FIXTURES = "/root/reference/tests/fixtures/openems"
+# The reference tree's openEMS fixtures; EMS_REFERENCE_FIXTURES overrides the location.
+FIXTURES = os.environ.get("EMS_REFERENCE_FIXTURES", "/root/reference/tests/fixtures/openems")
 have = pytest.mark.skipif(not os.path.isdir(FIXTURES), reason="reference fixtures not present")
 
 # (case, tolerance): the cases whose features the front end restates.

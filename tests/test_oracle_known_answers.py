@@ -12,7 +12,9 @@ sources, probes and thresholds:
 * determinism across thread counts (tests/engine.rs:412-520);
 * CPML reflection at normal incidence (uniform, graded, CFS, dielectric
   background), a 3-D point source, and late-time stability
-  (tests/cpml.rs:1-300);
+  (tests/cpml.rs:1-300), with the reflection levels the reference printed
+  for the uniform layer, the dielectric backgrounds and the point source
+  (src/engine/boundary/cpml.rs:97-99, 254-256) reproduced within 0.3 dB;
 * energy conservation, dissipation, boundedness and thread determinism with
   dispersive poles (tests/validation_dispersive.rs:377-562).
 
@@ -361,9 +363,20 @@ def normal_reflection(pml_cells, eps_r=1.0, **kw):
     return rel_err(test, ref)
 
 
+# The reflection levels the reference measured and printed for these runs
+# (src/engine/boundary/cpml.rs:97-99 and 254-256, tests/cpml.rs:163-166):
+# eight uniform cells, m = 3, the linear convolution (the default) and the
+# constant rule; the oracle must reproduce them, not only stay below the
+# tests' thresholds.
+LEVEL_DB = 0.3
+
+
 def test_cpml_normal_incidence_uniform():
     r = normal_reflection([DZ] * 8)
     assert db(r) < -70.0, f"reflection {db(r):.1f} dB"
+    assert abs(db(r) - (-85.8)) < LEVEL_DB, f"linear rule: {db(r):.2f} dB, reference −85.8"
+    c = normal_reflection([DZ] * 8, linear=False)
+    assert abs(db(c) - (-83.6)) < LEVEL_DB, f"constant rule: {db(c):.2f} dB, reference −83.6"
     r0 = normal_reflection([DZ] * 8, sigma_factor=0.0)
     assert db(r0) > -1.0, f"window misses the echo: {db(r0):.1f} dB"
 
@@ -380,14 +393,22 @@ def test_cpml_normal_incidence_cfs():
     assert db(r) < -60.0, f"reflection {db(r):.1f} dB"
 
 
-@pytest.mark.parametrize("eps", [4.0, 12.0])
-def test_cpml_normal_incidence_dielectric_background(eps):
+@pytest.mark.parametrize("eps, tuned, vacuum", [(4.0, -85.7, -80.5), (12.0, -85.7, -73.4)])
+def test_cpml_normal_incidence_dielectric_background(eps, tuned, vacuum):
     """σ_max is tuned to the layer's index: as good as in vacuum, and better
-    than the vacuum σ_max by more than 3 dB (tests/cpml.rs:159-178)."""
+    than the vacuum σ_max by more than 3 dB (tests/cpml.rs:159-178). The
+    printed levels (−85.7 dB tuned, −80.5 / −73.4 dB with the vacuum σ_max)
+    are the constant rule's, measured before the linear rule became the
+    default (src/engine/boundary/cpml.rs:254-256); the oracle reproduces them
+    with that rule."""
     r = normal_reflection([DZ] * 8, eps_r=eps)
     assert db(r) < -80.0, f"eps_r {eps}: {db(r):.1f} dB"
     v = normal_reflection([DZ] * 8, eps_r=eps, sigma_factor=math.sqrt(eps))
     assert db(v) > db(r) + 3.0, (db(v), db(r))
+    rc = normal_reflection([DZ] * 8, eps_r=eps, linear=False)
+    vc = normal_reflection([DZ] * 8, eps_r=eps, sigma_factor=math.sqrt(eps), linear=False)
+    assert abs(db(rc) - tuned) < LEVEL_DB, (db(rc), tuned)
+    assert abs(db(vc) - vacuum) < LEVEL_DB, (db(vc), vacuum)
 
 
 def box_run(interior, pml, cpml_kw, probes, steps):
@@ -410,14 +431,21 @@ def box_run(interior, pml, cpml_kw, probes, steps):
 def test_cpml_point_source_3d():
     """tests/cpml.rs:220-265: 12³ interior + 8-cell CPML against a box with
     22 cells of padding, 80 steps: every probe below −60 dB; a lossless layer
-    shows in the window (above −25 dB)."""
+    shows in the window (above −25 dB). The levels the reference printed for
+    the three probes (src/engine/boundary/cpml.rs:98-99): −95.4, −85.4,
+    −84.7 dB with the linear rule and −89.6, −75.0, −72.6 dB with the
+    constant rule, reproduced within 0.3 dB."""
     interior, steps, pad = 12, 80, 22
     h = interior // 2
     probes = [(h - 3, 0, 0), (h - 3, h - 3, 0), (h - 3, h - 3, h - 4)]
     ref = box_run(interior, pad, None, probes, steps)
     test = box_run(interior, 8, {}, probes, steps)
-    errs = [rel_err(t, r) for t, r in zip(test, ref)]
-    assert all(db(e) < -60.0 for e in errs), [db(e) for e in errs]
+    errs = [db(rel_err(t, r)) for t, r in zip(test, ref)]
+    assert all(e < -60.0 for e in errs), errs
+    assert np.all(np.abs(np.array(errs) - [-95.4, -85.4, -84.7]) < LEVEL_DB), errs
+    const = box_run(interior, 8, {"linear": False}, probes, steps)
+    errs = [db(rel_err(t, r)) for t, r in zip(const, ref)]
+    assert np.all(np.abs(np.array(errs) - [-89.6, -75.0, -72.6]) < LEVEL_DB), errs
     lossless = box_run(interior, 8, {"sigma_factor": 0.0}, probes, steps)
     errs = [rel_err(t, r) for t, r in zip(lossless, ref)]
     assert all(db(e) > -25.0 for e in errs), [db(e) for e in errs]

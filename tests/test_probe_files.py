@@ -14,7 +14,8 @@ import pytest
 
 from ems_b200 import probe_files as PF
 
-FIXTURES = "/root/reference/tests/fixtures/openems"
+# The reference tree's openEMS fixtures; EMS_REFERENCE_FIXTURES overrides the location.
+FIXTURES = os.environ.get("EMS_REFERENCE_FIXTURES", "/root/reference/tests/fixtures/openems")
 
 
 def _probe_files():

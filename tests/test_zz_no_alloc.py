@@ -68,5 +68,8 @@ def test_energy_noalloc_rejects_sizes_beyond_its_limit():
     out = torch.zeros(1, dtype=torch.float64, device="cuda:0")
     big = (C.c_uint64 * 3)(2048, 2048, 1024)  # 2^32 nodes: beyond 2^31 − 1
     assert lib.ems_energy_noalloc(big, 1e-12, ptrs3, ptrs3, ptrs12, C.c_void_p(out.data_ptr()), None) == 1
+    # A product that wraps in 64 bits to under 2^31 − 1: rejected too.
+    wrap = (C.c_uint64 * 3)(131073, 65537, 2147434497)
+    assert lib.ems_energy_noalloc(wrap, 1e-12, ptrs3, ptrs3, ptrs12, C.c_void_p(out.data_ptr()), None) == 1
     small = (C.c_uint64 * 3)(1, 2, 2)
     assert lib.ems_energy_noalloc(small, 1e-12, ptrs3, ptrs3, ptrs12, C.c_void_p(out.data_ptr()), None) == 1
