@@ -12,6 +12,7 @@ engine needs a CUDA device and raises if the CUDA library is missing.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from dataclasses import dataclass
 from typing import Sequence
@@ -223,6 +224,7 @@ def host_lib() -> C.CDLL:
             "ems_waveform_value": (d, [i, d, d, d, d]),
             "ems_waveform_duration": (d, [i, d, d]),
             "ems_model_add_lumped_port": (i, [p, i, p, p, d, i, d, d, d, u]),
+            "ems_model_add_lumped": (i, [p, i, p, p, d, d, d, i, i, i, p, u]),
             "ems_model_add_source": (i, [p, i, sz, p, p, p, i, d, d, u]),
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
@@ -491,7 +493,7 @@ class Model:
         return self
 
     def build(self, courant: float = 0.99, dt: float | None = None) -> "Model":
-        self._check(self._lib.ems_model_build(self._p, courant, dt or 0.0), "build!")
+        self._check(self._lib.ems_model_build(self._p, courant, 0.0 if dt is None else dt), "build!")
         return self
 
     def set_edge_materials(self, field: int, axis: int, v0: np.ndarray, v1: np.ndarray) -> "Model":
@@ -576,6 +578,26 @@ class Model:
         k = self._check(self._lib.ems_model_add_lumped_port(self._p, axis, _u64(lo), _u64(hi), r, GAUSSIAN, f0, fc,
                                                             amplitude, n_steps), "add_lumped_port")
         self.ops.append((OP_LUMPED, "port"))
+        return k
+
+    def add_lumped_port_table(self, axis: int, lo: Sequence[int], hi: Sequence[int], r: float,
+                              amp: np.ndarray | None) -> int:
+        """``LumpedPort::new(LumpedBox(axis, lo, hi), r).excite(v)`` with ``amp[n]`` = v((n + ½)·dt)
+        (src/engine/port.rs:102-155); ``amp`` None: a passive port."""
+        return self.add_lumped(axis, lo, hi, r=r, amp=amp, port=True)
+
+    def add_lumped(self, axis: int, lo: Sequence[int], hi: Sequence[int], r: float = 0.0, l: float = 0.0,
+                   c: float = 0.0, series: bool = False, record: bool = False, port: bool = False,
+                   amp: np.ndarray | None = None) -> int:
+        """``LumpedElement::new(LumpedBox(axis, lo, hi)).r(r).l(l).c(c)`` (0: absent) with the
+        parallel or series topology, optionally ``record_current()`` and a Thevenin source
+        sampled at (n + ½)·dt (src/engine/lumped.rs:380-1013)."""
+        a = None if amp is None else np.ascontiguousarray(amp, dtype=np.float64)
+        k = self._check(self._lib.ems_model_add_lumped(self._p, axis, _u64(lo), _u64(hi), r, l, c, int(series),
+                                                       int(record), int(port),
+                                                       None if a is None else a.ctypes.data,
+                                                       0 if a is None else len(a)), "add_lumped")
+        self.ops.append((OP_LUMPED, "port" if port else "lumped"))
         return k
 
     def add_source(self, kind: int, edges: Sequence[tuple[int, Sequence[int], float]], f0: float, fc: float,
@@ -1091,6 +1113,50 @@ def dft(t0: float, dt: float, x: np.ndarray, freqs: Sequence[float]) -> np.ndarr
     im = np.empty(len(f))
     host_lib().ems_dft(t0, dt, x.ctypes.data, len(x), f.ctypes.data, len(f), re.ctypes.data, im.ctypes.data)
     return re + 1j * im
+
+
+class PortResult:
+    """``PortResult`` (src/post/port.rs:60-230): a port's V(f), I(f) and its
+    reference impedance, with the power waves, S11, Z_in and powers."""
+
+    def __init__(self, freqs: Sequence[float], v: np.ndarray, i: np.ndarray, z_ref: complex):
+        self.freqs = np.asarray(freqs, dtype=np.float64)
+        self.v = np.asarray(v, dtype=complex)
+        self.i = np.asarray(i, dtype=complex)
+        self.z_ref = complex(z_ref)
+
+    @classmethod
+    def of_port(cls, v: np.ndarray, i: np.ndarray, dt: float, freqs: Sequence[float], z_ref: complex):
+        """``LumpedPort::analyze_with`` (src/engine/port.rs:202-215): DFTs of V
+        sampled at (n+1)·dt and I at (n+½)·dt."""
+        return cls(freqs, dft(dt, dt, v, freqs), dft(0.5 * dt, dt, i, freqs), z_ref)
+
+    def a(self) -> np.ndarray:
+        return (self.v + self.z_ref * self.i) * (0.5 / math.sqrt(self.z_ref.real))
+
+    def b(self) -> np.ndarray:
+        return (self.v - self.z_ref.conjugate() * self.i) * (0.5 / math.sqrt(self.z_ref.real))
+
+    def z_in(self) -> np.ndarray:
+        return self.v / self.i
+
+    def s11(self) -> np.ndarray:
+        return s_param(self, self)
+
+    def incident_power(self) -> np.ndarray:
+        return 0.5 * np.abs(self.a()) ** 2
+
+    def reflected_power(self) -> np.ndarray:
+        return 0.5 * np.abs(self.b()) ** 2
+
+    def accepted_power(self) -> np.ndarray:
+        return 0.5 * (self.v.real * self.i.real + self.v.imag * self.i.imag)
+
+
+def s_param(out: PortResult, inc: PortResult) -> np.ndarray:
+    """``s_param`` (src/post/port.rs:236-242): S_oi = b_o / a_i."""
+    assert np.array_equal(out.freqs, inc.freqs), "port results at different frequencies"
+    return out.b() / inc.a()
 
 
 def port_result(v: np.ndarray, i: np.ndarray, dt: float, freqs: Sequence[float], z_ref: float = 50.0):

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -111,7 +112,7 @@ struct OpStore {
     ems_poles poles{};
     // lumped
     std::vector<uint64_t> lnode;
-    std::vector<double> lcb, lg, lw, lamp, lrg, lrc;
+    std::vector<double> lcb, lg, lw, lamp, lrg, lrc, ltl, linvc, lz;
     ems_lumped lumped{};
     // source / probe
     std::vector<uint8_t> axis;
@@ -611,8 +612,9 @@ int ems_model_build(ems_model* m, double courant, double fixed_dt) {
     // TimeStep::resolve (src/engine/coeffs.rs:220-240).
     double max = ems_model_courant_limit(m);
     double dt;
-    if (fixed_dt > 0.0) {
-        if (!(std::isfinite(fixed_dt) && fixed_dt <= max)) return set_err(m, "time step above the stability limit"), EMS_ERR_INVALID;
+    if (fixed_dt != 0.0) {  // NaN and negative values included: TimeStep::Fixed
+        if (!(std::isfinite(fixed_dt) && fixed_dt > 0.0)) return set_err(m, "time step must be finite and > 0"), EMS_ERR_INVALID;
+        if (!(fixed_dt <= max)) return set_err(m, "time step above the stability limit"), EMS_ERR_INVALID;
         dt = fixed_dt;
     } else {
         if (!(std::isfinite(courant) && courant > 0.0 && courant <= 1.0)) return set_err(m, "Courant factor must be in (0, 1]"), EMS_ERR_INVALID;
@@ -1356,52 +1358,84 @@ int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
     return (int)m->ops.size() - 1;
 }
 
-int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, int wave,
-                              double f0, double fc, double amplitude, uint64_t n_steps) {
+int ems_model_add_lumped(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, double l,
+                         double c, int series_topology, int record, int port, const double* amp, uint64_t n_amp) {
     if (!m->built) return set_err(m, "build the model first"), -1;
-    if (axis < 0 || axis > 2 || !(r > 0.0) || !std::isfinite(r)) return set_err(m, "invalid lumped port"), -1;
+    if (axis < 0 || axis > 2) return set_err(m, "invalid lumped element axis"), -1;
+    // LumpedElement::validate (src/engine/lumped.rs:700-760): values finite
+    // and > 0 where present (<= 0 here means absent), at least one of them,
+    // a source on a parallel element only with a resistor.
+    const bool has_r = r > 0.0, has_l = l > 0.0, has_c = c > 0.0;
+    for (double v : {r, l, c})
+        if (!(v <= 0.0) && !(std::isfinite(v) && v > 0.0)) return set_err(m, "invalid lumped value"), -1;
+    if (!(has_r || has_l || has_c)) return set_err(m, "lumped element needs at least one of R, L, C"), -1;
+    const bool has_src = amp != nullptr && n_amp > 0;
+    if (has_src && !series_topology && !has_r) return set_err(m, "a source on a parallel lumped element needs a resistance"), -1;
+    if (port && !(has_r && !has_l && !has_c && !series_topology)) return set_err(m, "a lumped port is a resistor"), -1;
     // LumpedBox::new / check_fits (src/engine/lumped.rs:145-215).
     for (int t = 0; t < 3; ++t)
         if (lo[t] > hi[t] || hi[t] >= m->n[t]) return set_err(m, "lumped box outside the grid"), -1;
     if (lo[axis] >= hi[axis]) return set_err(m, "lumped box degenerate along its axis"), -1;
-    const int a = axis, b = next_axis(axis), c = prev_axis(axis);
+    const int a = axis, b = next_axis(axis), cc = prev_axis(axis);
     std::vector<uint64_t> edges;
     for (uint64_t pb = lo[b]; pb <= hi[b]; ++pb)
-        for (uint64_t pc = lo[c]; pc <= hi[c]; ++pc)
+        for (uint64_t pc = lo[cc]; pc <= hi[cc]; ++pc)
             for (uint64_t pa = lo[a]; pa < hi[a]; ++pa) {
                 uint64_t p[3];
                 p[a] = pa;
                 p[b] = pb;
-                p[c] = pc;
+                p[cc] = pc;
                 edges.push_back(m->index(p[0], p[1], p[2]));
             }
-    const double series = (double)(hi[a] - lo[a]);
-    const double cols = (double)((hi[b] - lo[b] + 1) * (hi[c] - lo[c] + 1));
     for (uint64_t e : edges)
         if (m->co[3 + a][e] == 0.0f) return set_err(m, "lumped element edge is PEC"), -1;
-    // LumpedElement::resistor edge_parts: g_e = M/(N·R) (src/engine/lumped.rs:846-852),
-    // folded by fold_parallel (src/engine/lumped.rs:275-282).
-    const double g_e = series / (cols * r);
+    // edge_parts for a box (src/engine/lumped.rs:820-860): Z_e = N·Z/M, so
+    // g_e = M/(N·R), C_e = M·C/N, L_e = N·L/M, R_e = N·R/M.
+    const double mm = (double)(hi[a] - lo[a]);
+    const double nn = (double)((hi[b] - lo[b] + 1) * (hi[cc] - lo[cc] + 1));
+    const bool has_branch = series_topology ? (has_l || has_c) : has_l;
+    const double inf = std::numeric_limits<double>::infinity();
+    double g_e = 0.0, c_e = 0.0, br_r = 0.0, br_l = 0.0, br_c = inf;
+    if (!series_topology) {
+        g_e = has_r ? mm / (nn * r) : 0.0;
+        c_e = has_c ? mm * c / nn : 0.0;
+        br_l = has_l ? nn * l / mm : 0.0;
+    } else if (!has_branch) {
+        g_e = has_r ? mm / (nn * r) : 0.0;
+    } else {
+        br_r = has_r ? nn * r / mm : 0.0;
+        br_l = has_l ? nn * l / mm : 0.0;
+        br_c = has_c ? mm * c / nn : inf;
+    }
     const double dt = m->dt;
     auto op = std::make_unique<OpStore>();
     op->kind = EMS_OP_LUMPED;
+    const bool src_in_branch = has_branch && series_topology;
     for (uint64_t e : edges) {
-        double ca = (double)m->co[a][e], cb = (double)m->co[3 + a][e];
-        double cap = dt * (1.0 + ca) / (2.0 * cb) + 0.0;
-        double cond = (1.0 - ca) / cb + g_e;
-        double den = cap + 0.5 * cond * dt;
-        m->co[a][e] = (float)((cap - 0.5 * cond * dt) / den);
-        m->co[3 + a][e] = (float)(dt / den);
+        // fold_parallel (src/engine/lumped.rs:275-282).
+        if (g_e != 0.0 || c_e != 0.0) {
+            double ca = (double)m->co[a][e], cb = (double)m->co[3 + a][e];
+            double cap = dt * (1.0 + ca) / (2.0 * cb) + c_e;
+            double cond = (1.0 - ca) / cb + g_e;
+            double den = cap + 0.5 * cond * dt;
+            m->co[a][e] = (float)((cap - 0.5 * cond * dt) / den);
+            m->co[3 + a][e] = (float)(dt / den);
+        }
         op->lnode.push_back(e);
         op->lcb.push_back((double)m->co[3 + a][e]);
-        op->lg.push_back(g_e);
-        op->lw.push_back(1.0 / series);
+        op->lg.push_back(src_in_branch ? 0.0 : g_e);
+        op->lw.push_back(1.0 / mm);
         op->lrg.push_back(g_e);
-        op->lrc.push_back(0.0);
+        op->lrc.push_back(c_e);
+        if (has_branch) {
+            // The branch constants of install (src/engine/lumped.rs:960-970).
+            const double inv_c = std::isfinite(br_c) ? 1.0 / br_c : 0.0;
+            op->ltl.push_back(2.0 * br_l / dt);
+            op->linvc.push_back(inv_c);
+            op->lz.push_back(2.0 * br_l / dt + br_r + 0.5 * dt * inv_c);
+        }
     }
-    // Source value amplitude·w(t) at (n + 1/2)·dt (src/engine/lumped.rs:1136-1148).
-    for (uint64_t s = 0; s < n_steps; ++s)
-        op->lamp.push_back(amplitude * ems_waveform_value(wave, f0, fc, ((double)s + 0.5) * dt, dt));
+    if (has_src) op->lamp.assign(amp, amp + n_amp);
     ems_lumped& L = op->lumped;
     L.axis = a;
     L.n_edges = edges.size();
@@ -1409,18 +1443,34 @@ int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], cons
     L.cb = op->lcb.data();
     L.g_src = op->lg.data();
     L.series = hi[a] - lo[a];
-    L.src_in_branch = 0;
-    L.src_w = op->lw.data();
+    L.src_in_branch = src_in_branch ? 1 : 0;
+    L.src_w = has_src ? op->lw.data() : nullptr;
     L.n_src_amp = op->lamp.size();
-    L.src_amp = op->lamp.data();
-    L.has_branch = 0;
-    L.record = 1;
+    L.src_amp = op->lamp.empty() ? nullptr : op->lamp.data();
+    L.has_branch = has_branch ? 1 : 0;
+    L.two_l_dt = has_branch ? op->ltl.data() : nullptr;
+    L.inv_c = has_branch ? op->linvc.data() : nullptr;
+    L.z = has_branch ? op->lz.data() : nullptr;
+    L.record = (record || port) ? 1 : 0;
     L.rec_g = op->lrg.data();
     L.rec_c = op->lrc.data();
-    L.port_columns = (uint64_t)cols;
+    L.port_columns = port ? (uint64_t)nn : 0;
     m->ops.push_back(std::move(op));
     m->refresh_desc();
     return (int)m->ops.size() - 1;
+}
+
+int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, int wave,
+                              double f0, double fc, double amplitude, uint64_t n_steps) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    if (axis < 0 || axis > 2 || !(r > 0.0) || !std::isfinite(r)) return set_err(m, "invalid lumped port"), -1;
+    // LumpedPort::new(region, r).excite_waveform(w, amplitude): a recorded
+    // resistor whose Thevenin source is amplitude·w(t) at (n + 1/2)·dt
+    // (src/engine/port.rs:102-155, src/engine/lumped.rs:1136-1148).
+    std::vector<double> amps;
+    for (uint64_t s = 0; s < n_steps; ++s)
+        amps.push_back(amplitude * ems_waveform_value(wave, f0, fc, ((double)s + 0.5) * m->dt, m->dt));
+    return ems_model_add_lumped(m, axis, lo, hi, r, 0.0, 0.0, 0, 1, 1, amps.data(), amps.size());
 }
 
 int ems_model_add_source(ems_model* m, int kind, size_t n, const int* axis, const uint64_t* nodes, const double* weight,

@@ -81,9 +81,10 @@ int ems_model_set_mur_media(ems_model* m, int face, int axis, const double* v);
  * one value per node in reference layout. Before build. */
 int ems_model_set_edge_materials(ems_model* m, int field, int axis, const double* v0, const double* v1);
 
-/* Computes dt = courant * courant_limit (TimeStep::Courant) or, with
- * fixed_dt > 0, takes it (TimeStep::Fixed), then the coefficients
- * (Coefficients::compute). Must precede the operators. */
+/* Computes dt = courant * courant_limit (TimeStep::Courant, courant in
+ * (0, 1]) or, with fixed_dt != 0, takes it (TimeStep::Fixed: finite, > 0
+ * and at most the limit, src/engine/coeffs.rs:195-230), then the
+ * coefficients (Coefficients::compute). Must precede the operators. */
 int ems_model_build(ems_model* m, double courant, double fixed_dt);
 /* Builds with the time step dt taken as given (TimeStep::Bound,
  * src/engine/coeffs.rs:233-236: a step established elsewhere, such as
@@ -163,6 +164,18 @@ double ems_waveform_duration(int kind, double f0, double fc);
  * sampled for n_steps steps. Returns the op index. */
 int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r,
                               int wave, double f0, double fc, double amplitude, uint64_t n_steps);
+
+/* A lumped element over the node box lo..hi along `axis`
+ * (LumpedElement::new(region).r(r).l(l).c(c).topology(t), src/engine/
+ * lumped.rs:380-1013): r [ohm], l [H], c [F], each absent when <= 0;
+ * series_topology 0 parallel (R and C folded into the edges, L as a branch),
+ * 1 series (R + L + C as a branch, a lone R folded). record: record the
+ * terminal current (record_current). port: a LumpedPort (a resistor that
+ * also records V and I, src/engine/port.rs:102-290). amp[n]: the Thevenin
+ * source value at (n + 1/2)*dt for step n < n_amp, 0 beyond (amp NULL: no
+ * source); a source on a parallel element needs r. Returns the op index. */
+int ems_model_add_lumped(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, double l,
+                         double c, int series_topology, int record, int port, const double* amp, uint64_t n_amp);
 
 /* An edge source of `kind` (ems_source_kind) on n edges with the waveform
  * sampled for n_steps steps. nodes: 3*n indices. Returns the op index. */
