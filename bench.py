@@ -57,8 +57,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=512, help="cells per axis (default: the configuration's 512)")
     ap.add_argument("--schedule", type=int, default=0,
-                    help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split, 5 sweep, 6 interior")
+                    help="0 automatic, 1 per-operator, 2 fused, 3 two kernels, 4 split, 5 sweep, 6 interior, 7 marching")
     ap.add_argument("--interior-planes", type=int, default=0, help="planes per block of the interior kernel (0: default)")
+    ap.add_argument("--march-shape", type=int, default=0, help="marching kernel tile shape (0..3)")
+    ap.add_argument("--march-planes", type=int, default=32, help="planes per block of the marching kernel")
     ap.add_argument("--workload", choices=["box", "sweep", "learned"], default="box",
                     help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
                          "sweep; learned: training and held-out evaluation of the learned early stop")
@@ -226,26 +228,64 @@ def profile_traffic(kernel: str) -> float | None:
     return float(v) if v is not None else None
 
 
+def host_cpu() -> dict:
+    """The host CPU model, its physical and logical core counts."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        import psutil
+
+        phys = psutil.cpu_count(logical=False) or os.cpu_count() or 1
+    except ImportError:
+        phys = os.cpu_count() or 1
+    return {"cpu_model": model, "physical_cores": phys, "logical_cpus": os.cpu_count() or 1}
+
+
 def cpu_baseline(w, seconds: float = 15.0) -> dict:
     """The oracle on the same model, timed on this host's cores for about
-    `seconds` (whole steps of the full model)."""
+    `seconds` (whole steps of the full model), with one thread per physical
+    core (the reference's --numThreads at the full core count); the thread
+    count the reference's default rule picks for this model
+    (src/engine/mod.rs:404-428: physical cores, at most one per 4096 cells
+    and one per five x-planes) is reported beside it, and timed too when it
+    differs."""
     from oracle import OracleEngine
 
-    o = OracleEngine(w.model, threads=os.cpu_count() or 1)
-    t0 = time.perf_counter()
-    o.run(1)
-    t1 = time.perf_counter()
-    per = max(t1 - t0, 1e-6)
-    n = max(1, min(200, int(seconds / per)))
-    t0 = time.perf_counter()
-    o.run(n)
-    el = time.perf_counter() - t0
-    v = w.cells * n / el / 1e6
-    th = o.threads
+    cpu = host_cpu()
+
+    def timed(threads):
+        o = OracleEngine(w.model, threads=threads)
+        t0 = time.perf_counter()
+        o.run(1)
+        per = max(time.perf_counter() - t0, 1e-6)
+        n = max(1, min(200, int(seconds / per)))
+        t0 = time.perf_counter()
+        o.run(n)
+        el = time.perf_counter() - t0
+        th = o.threads
+        o.close()
+        return w.cells * n / el / 1e6, th, n
+
+    v, th, n = timed(cpu["physical_cores"])
+    o = OracleEngine(w.model, threads=0)
+    rule = o.threads
     o.close()
-    return {"value": round(v, 3), "unit": METRIC, "cores": th, "kind": "port",
-            "sample": f"{n} whole steps of the same {w.name} model after 1 untimed step "
-                      f"(oracle: C++ restatement of the reference step, {th} threads)"}
+    out = {"value": round(v, 3), "unit": METRIC, "cores": th, "kind": "port",
+           "sample": f"{n} whole steps of the same {w.name} model after 1 untimed step "
+                     f"(oracle: C++ restatement of the reference step, {th} threads)",
+           "cpu_model": cpu["cpu_model"], "physical_cores": cpu["physical_cores"],
+           "logical_cpus": cpu["logical_cpus"], "default_rule_threads": rule}
+    if rule != th:
+        vr, _, nr = timed(0)
+        out["default_rule_value"] = round(vr, 3)
+    return out
 
 
 def run_reference(args):
@@ -255,7 +295,8 @@ def run_reference(args):
     w = workload(args.cells, max(args.steps + args.warmup + 10, 100))
     from oracle import OracleEngine
 
-    o = OracleEngine(w.model, threads=os.cpu_count() or 1)
+    cpu = host_cpu()
+    o = OracleEngine(w.model, threads=cpu["physical_cores"])
     o.run(args.warmup)
     t0 = time.perf_counter()
     o.run(args.steps)
@@ -268,7 +309,8 @@ def run_reference(args):
         "config": config(w, args),
         "cpu_baseline": {"value": round(v, 3), "unit": METRIC, "cores": o.threads, "kind": "port",
                          "sample": f"{args.steps} whole steps after {args.warmup} warm-up steps, "
-                                   f"{o.threads} threads (C++ restatement of the reference step)"},
+                                   f"{o.threads} threads (C++ restatement of the reference step)",
+                         **cpu},
         "e2e": {"value": round(v, 3), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -305,6 +347,7 @@ def run_ours(args):
     eng.set_schedule(args.schedule)
     if args.interior_planes:
         eng.set_interior_planes(args.interior_planes)
+    eng.set_march(args.march_shape, args.march_planes)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.run(args.warmup)
     torch.cuda.synchronize(dev)
@@ -313,8 +356,7 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    # --- timed region
-    eng.profile(True)
+    # --- timed region (no per-kernel events inside it)
     launches0 = eng.launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -328,6 +370,11 @@ def run_ours(args):
         barrier()
     ms = e0.elapsed_time(e1)
     launches = eng.launches - launches0
+    # Per-kernel device times from a separate pass with events around the
+    # field-update kernels.
+    eng.profile(True)
+    eng.run(min(args.steps, 20))
+    torch.cuda.synchronize(dev)
     kern = {k: eng.profile_read(k) for k in (0, 1, 2)}
     eng.profile(False)
     ms = max_over_ranks(ms, world, f"cuda:{dev}")
@@ -367,7 +414,13 @@ def run_ours(args):
     # update of the split and per-operator schedules (reads u, reads and
     # writes i: 36 B per cell).
     schedule = eng.schedule
-    if schedule == 6:
+    nodes = float(np.prod(w.model.nodes))
+    if schedule == 7:
+        # The marching kernel: reads u and i, writes both (48 B per node),
+        # and reads and writes the ψ of every layer node.
+        kname, (kms, kn) = "march", kern[2]
+        per_launch = 48.0 * nodes + ab["psi"]
+    elif schedule == 6:
         # The one-pass kernel over the interior box: reads u and i, writes
         # both (48 B per node).
         (blo, bhi) = eng.interior_box
@@ -400,10 +453,10 @@ def run_ours(args):
                      "mean_launch_ms": round(kms / kn, 4) if kn else None},
         "step_roofline": {"algorithmic_bytes_per_step": ab["total"], "bytes_per_cell": round(ab["total"] / ab["cells"], 2),
                           "achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peaks["hbm_gbs"], 4)},
-        "kernels_ms": {("h_update", "e_update", "interior" if schedule == 6 else "fused_step")[k]:
+        "kernels_ms": {("h_update", "e_update", {6: "interior", 7: "march"}.get(schedule, "fused_step"))[k]:
                        {"ms": round(v[0], 3), "launches": v[1]} for k, v in kern.items() if v[1]},
         "schedule": {1: "per-operator kernels", 2: "fused single pass", 3: "two kernels", 4: "split",
-                     5: "sweep", 6: "interior"}[schedule],
+                     5: "sweep", 6: "interior", 7: "marching"}[schedule],
         "e2e": {"value": round(e2e, 1), "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 8,
                 "steps": k_e2e},
         "gpu_launches": launches,

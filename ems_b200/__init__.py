@@ -39,6 +39,10 @@ OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR, OP_UPML = 1, 2, 3, 4,
 MUR_OPENEMS_ORDER, MUR_OPENEMS_CORNERS, MUR_COUNT_ENERGY = 1, 2, 4
 
 
+# ems_status codes (include/ems_gpu.h).
+ERR_INVALID, ERR_CUDA, ERR_DIVERGED, ERR_TIMEOUT, ERR_NOMEM = 1, 2, 3, 4, 5
+
+
 class EngineError(RuntimeError):
     """An engine call failed; ``status`` is the ems_status code."""
 
@@ -276,6 +280,9 @@ GPU_SYMBOLS = {
     "ems_gpu_freq_dump_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ems_gpu_set_sweep_planes": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ems_gpu_set_interior_planes": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "ems_gpu_set_march": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    "ems_gpu_check": (C.c_int, [C.c_void_p]),
+    "ems_gpu_test_wait_timeout": (C.c_int, [C.c_void_p, C.c_uint64]),
     "ems_gpu_freq_dump_read": (C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t]),
     "ems_batch_autotune": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ems_batch_create": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_uint64, C.c_void_p]),
@@ -825,6 +832,19 @@ class Engine:
         """Planes a block of the interior schedule's one-pass kernel marches through."""
         self._ck(self._lib.ems_gpu_set_interior_planes(self._h, planes))
 
+    def check(self) -> None:
+        """Raises EngineError with EMS_ERR_TIMEOUT or EMS_ERR_DIVERGED if the
+        device flags were set since the last check (``ems_gpu_check``)."""
+        self._ck(self._lib.ems_gpu_check(self._h))
+
+    def test_wait_timeout(self, limit_ns: int) -> None:
+        """Arms the bounded-wait test hook for the next marching step."""
+        self._ck(self._lib.ems_gpu_test_wait_timeout(self._h, limit_ns))
+
+    def set_march(self, shape: int = 0, planes: int = 32) -> None:
+        """The marching schedule's tile shape (0..3) and planes per block."""
+        self._ck(self._lib.ems_gpu_set_march(self._h, shape, planes))
+
     def set_sweep_planes(self, planes: int) -> None:
         """Chunk size of the sweep schedule (5), in x-planes."""
         self._ck(self._lib.ems_gpu_set_sweep_planes(self._h, planes))
@@ -1037,6 +1057,12 @@ def run_until(stepper, limits: RunLimits) -> RunOutcome:
         try:
             w[0] = stepper.step_with_energy()
             return 0
+        except EngineError as e:
+            if e.status == ERR_DIVERGED:  # an outcome of the run (Diverged), not an error
+                w[0] = float("nan")
+                return ERR_DIVERGED
+            err.append(e)
+            return 1
         except BaseException as e:
             err.append(e)
             return 1

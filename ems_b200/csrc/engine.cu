@@ -33,7 +33,10 @@
 #include "separate.cuh"
 #include "split.cuh"
 #include "interior.cuh"
+#include "march.cuh"
 #include "batch.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <thread>
 #include <unordered_map>
@@ -82,6 +85,8 @@ struct ems_gpu {
     double* partials = nullptr;   // energy partial sums per block
     size_t n_partials = 0;
     double* d_energy = nullptr;   // [0] field part, [1] operator part
+    int* diverged = nullptr;      // set on the device where a marching step writes a non-finite value
+    uint64_t test_wait_ns = 0;    // ems_gpu_test_wait_timeout: the next marching step's waits run out
     struct CpmlDev {
         SlabDev s;
     };
@@ -164,6 +169,19 @@ struct ems_gpu {
     FusedParams fp{};               // everything but the field pointers and ψ_H parity
     std::vector<std::pair<float*, float*>> psi_h;  // ψ of each H slab: (current, other)
     std::vector<std::pair<int, int>> psi_h_at;     // its place in fp.slab[0][c][q]
+    std::vector<size_t> psi_h_dev;                 // its slab in the CPML operator's device slabs
+
+    // Swaps the H-side ψ buffers after a step that wrote the other ones,
+    // and points the per-operator kernels' slabs at the current ones.
+    void swap_psi_h() {
+        std::vector<SlabDev>* dev = nullptr;
+        for (auto& op : ops)
+            if (op.kind == EMS_OP_CPML) dev = &op.cpml;
+        for (size_t q = 0; q < psi_h.size(); ++q) {
+            std::swap(psi_h[q].first, psi_h[q].second);
+            if (dev) (*dev)[psi_h_dev[q]].psi = psi_h[q].first;
+        }
+    }
     // The split schedule: CPML layer shell segments per side (0 H, 1 E).
     ShellDev shell[2] = {};
     // The sweep schedule: x chunks of sweep_planes planes, each chunk's
@@ -176,6 +194,17 @@ struct ems_gpu {
     InteriorBox ibox{};
     std::string interior_why = "no tables";
     uint32_t interior_planes = kInPlanes;  // planes a block of the interior kernel marches through
+    // The marching schedule (7): why it is unavailable ("" if it is not),
+    // its tile shape (kMarchShapes), planes per block, and the tensor maps
+    // of the old fields of each buffer (keyed by the buffer's u_x and shape).
+    std::string march_why = "no tables";
+    int march_shape = 0;
+    uint32_t march_planes = kMarchPlanes;
+    struct MarchMapSet {
+        const float* key = nullptr;
+        int shape = -1;
+        MarchMaps m{};
+    } march_maps[2];
     std::vector<uint32_t> chunk_box[2], chunk_node[2], chunk_edge[2];
     std::vector<SlabGeo> slab_geo;       // to re-cut the shell for another chunk size
     // The chunk loop of a sweep step as a CUDA graph ([0] plain, [1] energy
@@ -493,6 +522,7 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         if (!sp.side) {
             h->psi_h.push_back({sd.psi, nullptr});
             h->psi_h_at.push_back({sp.comp, sp.q});
+            h->psi_h_dev.push_back(q_dev - 1);
         }
     }
     for (int a = 0; a < 3; ++a) {
@@ -569,6 +599,7 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         }
     }
     h->interior_why = interior_box(d, g, h->ibox);
+    h->march_why = march_why(d);
     h->fold_prev[0] = T.has_poles && pole_prev_fold(d, true, T.poles_first);
     h->fold_prev[1] = T.has_poles_h && pole_prev_fold(d, false, T.poles_first);
     h->n_qpartials = (size_t)split_blocks_x(g) * g.nx;
@@ -623,6 +654,7 @@ int active_schedule(const ems_gpu* h) {
     case 4: return h->tables_ok ? 4 : 1;
     case 5: return h->tables_ok ? (h->sweep_ok ? 5 : 4) : 1;
     case 6: return h->tables_ok ? (h->interior_why.empty() ? 6 : 4) : 1;
+    case 7: return h->tables_ok ? (h->march_why.empty() ? 7 : 4) : 1;
     default: return h->tables_ok ? 4 : 1;
     }
 }
@@ -673,7 +705,7 @@ ems_status run_step_fused(ems_gpu* h, bool energy) {
         std::swap(h->u[a], h->u2[a]);
         std::swap(h->i[a], h->i2[a]);
     }
-    for (auto& pr : h->psi_h) std::swap(pr.first, pr.second);
+    h->swap_psi_h();
     Fields nf{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
     st = serial_post_h(h, nf);
     if (st) return st;
@@ -978,19 +1010,183 @@ ems_status run_step_interior(ems_gpu* h) {
     return EMS_OK;
 }
 
+// The tile shapes of the marching kernel: rows per block and ring stages.
+struct MarchShape {
+    uint32_t rows, stages;
+};
+constexpr MarchShape kMarchShapes[] = {{8, 3}, {8, 4}, {4, 4}, {16, 3}};
+constexpr int kNumMarchShapes = (int)(sizeof(kMarchShapes) / sizeof(kMarchShapes[0]));
+
+// cuTensorMapEncodeTiled from the driver (through the runtime, so the
+// library needs no link to libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// The six tensor maps of the old fields of buffer (u, i) for tiles of R rows:
+// extents (pitch, ny, nx), boxes (kMuW, R + 2, 1) and (kMiW, R + 1, 1),
+// out-of-grid entries read as zero.
+static ems_status encode_march_maps(ems_gpu* h, float* const u[3], float* const i[3], uint32_t R, MarchMaps& M) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(h, EMS_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const Grid& g = h->g;
+    const cuuint64_t dims[3] = {g.pitch, g.ny, g.nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.ny * g.pitch * 4};
+    const cuuint32_t ubox[3] = {kMuW, R + 2, 1}, ibox[3] = {kMiW, R + 1, 1}, es[3] = {1, 1, 1};
+    for (int c = 0; c < 3; ++c) {
+        for (int side = 0; side < 2; ++side) {
+            CUresult r = enc(side ? &M.i[c] : &M.u[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, side ? (void*)i[c] : (void*)u[c],
+                             dims, strides, side ? ibox : ubox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(h, EMS_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        }
+    }
+    return EMS_OK;
+}
+
+template <uint32_t R, uint32_t S>
+static ems_status launch_march(ems_gpu* h, const FusedParams& P, const MarchMaps& M, bool oe) {
+    const size_t smem = MarchLayout<R>::bytes(S);
+    uint32_t nb[3];
+    march_blocks(h->g, R, h->march_planes, nb);
+    const dim3 grd(nb[0], nb[1], nb[2]);
+    if (oe) {
+        cudaFuncSetAttribute(k_march<R, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_march<R, S, true><<<grd, 32 * (R + 1), smem, h->stream>>>(P, M, h->march_planes);
+    } else {
+        cudaFuncSetAttribute(k_march<R, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_march<R, S, false><<<grd, 32 * (R + 1), smem, h->stream>>>(P, M, h->march_planes);
+    }
+    return check(h, cudaGetLastError(), "marching kernel");
+}
+
+// One step through the marching schedule (march.cuh): the old fields in one
+// buffer, the one-pass kernel (both updates, both CPML corrections and the
+// electric poles over the whole grid) writing the new ones into the other,
+// then the serial hooks on the new fields. Steps that record the energy run
+// the split schedule in place.
+ems_status run_step_march(ems_gpu* h) {
+    const Grid& g = h->g;
+    cudaStream_t s = h->stream;
+    if (!h->u2[0]) {
+        // The second buffers start as copies: entries no kernel writes
+        // (row padding) then agree in both.
+        for (int a = 0; a < 3; ++a) {
+            h->u2[a] = h->alloc<float>(g.np);
+            h->i2[a] = h->alloc<float>(g.np);
+            if (!h->u2[a] || !h->i2[a]) return fail(h, EMS_ERR_NOMEM, "second field buffers");
+            if (check(h, cudaMemcpyAsync(h->u2[a], h->u[a], g.np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                      "second field buffers") ||
+                check(h, cudaMemcpyAsync(h->i2[a], h->i[a], g.np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                      "second field buffers"))
+                return EMS_ERR_CUDA;
+        }
+    }
+    // The H-side ψ in two buffers: a node's H value is computed again by the
+    // blocks next to its own, which must read the old ψ.
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        if (h->psi_h[q].second) continue;
+        const FSlab& fs = h->fp.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        const size_t len = (size_t)(fs.hi[0] - fs.lo[0]) * (fs.hi[1] - fs.lo[1]) * (fs.hi[2] - fs.lo[2]);
+        float* other = h->alloc<float>(len);
+        if (!other) return fail(h, EMS_ERR_NOMEM, "CPML state");
+        if (check(h, cudaMemcpyAsync(other, h->psi_h[q].first, len * sizeof(float), cudaMemcpyDeviceToDevice, s),
+                  "CPML state"))
+            return EMS_ERR_CUDA;
+        h->psi_h[q].second = other;
+    }
+    if (!h->status) {
+        h->status = h->alloc<int>(1);
+        if (!h->status) return fail(h, EMS_ERR_NOMEM, "status flag");
+    }
+    for (auto& gx : h->sweep_graph)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    const Fields fa{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
+    const Fields fb{{h->u2[0], h->u2[1], h->u2[2]}, {h->i2[0], h->i2[1], h->i2[2]}};
+    Coeffs c;
+    for (int l = 0; l < 12; ++l) c.c[l] = h->co[l];
+    ems_status st = serial_pre_e(h, fa);
+    if (st) return st;
+    FusedParams P = h->fp;
+    for (int a = 0; a < 3; ++a) {
+        P.uo[a] = fa.u[a];
+        P.io[a] = fa.i[a];
+        P.un[a] = fb.u[a];
+        P.in[a] = fb.i[a];
+    }
+    for (size_t q = 0; q < h->psi_h.size(); ++q) {
+        FSlab& fs = P.slab[0][h->psi_h_at[q].first][h->psi_h_at[q].second];
+        fs.psi_old = h->psi_h[q].first;
+        fs.psi_new = h->psi_h[q].second;
+    }
+    P.status = h->status;
+    P.diverged = h->diverged;
+    P.wait_ns = h->test_wait_ns;
+    P.test_extra_tx = h->test_wait_ns ? 16u : 0u;
+    h->test_wait_ns = 0;
+    const int shape = h->march_shape;
+    const uint32_t R = kMarchShapes[shape].rows;
+    auto& ms = h->march_maps[h->u[0] == h->march_maps[0].key ? 0 : 1];
+    if (ms.key != h->u[0] || ms.shape != shape) {
+        st = encode_march_maps(h, h->u, h->i, R, ms.m);
+        if (st) return st;
+        ms.key = h->u[0];
+        ms.shape = shape;
+    }
+    cudaEvent_t ev = h->prof_begin();
+    const bool oe = h->oe_curl;
+    switch (shape) {
+    case 0: st = launch_march<8, 3>(h, P, ms.m, oe); break;
+    case 1: st = launch_march<8, 4>(h, P, ms.m, oe); break;
+    case 2: st = launch_march<4, 4>(h, P, ms.m, oe); break;
+    default: st = launch_march<16, 3>(h, P, ms.m, oe); break;
+    }
+    h->prof_end(2, ev);
+    ++h->launches;
+    if (st) return st;
+    // The kernel applied the electric poles from the old values; the saved
+    // values the split schedule keeps are not current after it.
+    h->prev_e_valid = false;
+    for (int a = 0; a < 3; ++a) {
+        std::swap(h->u[a], h->u2[a]);
+        std::swap(h->i[a], h->i2[a]);
+    }
+    h->swap_psi_h();
+    st = serial_post_h(h, fb);
+    if (st) return st;
+    st = serial_post_e(h, fb);
+    if (st) return st;
+    ++h->step;
+    return EMS_OK;
+}
+
 // One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
 ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
     // Only the per-operator, split and sweep steps keep the electric saved values.
-    if (sch != 4 && sch != 5 && sch != 6) h->prev_e_valid = false;
+    if (sch != 4 && sch != 5 && sch != 6 && sch != 7) h->prev_e_valid = false;
     if (sch == 6 && !energy) return run_step_interior(h);
+    if (sch == 7 && !energy) return run_step_march(h);
     if (sch == 2) return run_step_fused(h, energy);
     if (sch == 3) return run_step_two(h, energy);
     if (sch == 5) return run_step_sweep(h, energy);
     // Schedules 1 and 4 share the hook sequence; split (4) runs the table
     // kernels of split.cuh for the updates and one shell kernel per CPML side.
-    const bool split = sch == 4 || sch == 6;
+    const bool split = sch == 4 || sch == 6 || sch == 7;
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
     Fields f{{h->u[0], h->u[1], h->u[2]}, {h->i[0], h->i[1], h->i[2]}};
@@ -1266,7 +1462,9 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
     h->n_partials = (size_t)blocks_for(g.nz, kRowThreads) * g.ny * g.nx;
     h->partials = h->alloc<double>(h->n_partials);
     h->d_energy = h->alloc<double>(2);
-    if (!h->partials || !h->d_energy) return EMS_ERR_NOMEM;
+    h->diverged = h->alloc<int>(1);
+    if (!h->partials || !h->d_energy || !h->diverged) return EMS_ERR_NOMEM;
+    if (check(h.get(), cudaMemsetAsync(h->diverged, 0, sizeof(int), h->stream), "divergence flag")) return EMS_ERR_CUDA;
     for (size_t k = 0; k < d->n_ops; ++k) {
         ems_gpu::Op op;
         op.kind = d->ops[k].kind;
@@ -1758,6 +1956,7 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     if (h->tables_ok) T.cand = (h->oe_curl || h->has_upml) ? std::vector<int>{4} : std::vector<int>{4, 3};
     if (h->tables_ok && h->sweep_ok) T.cand.push_back(5);
     if (h->tables_ok && h->interior_why.empty()) T.cand.push_back(6);
+    if (h->tables_ok && h->march_why.empty()) T.cand.push_back(7);
     T.cand.push_back(1);
     T.ms.assign(T.cand.size(), 0.0);
     T.at = 0;
@@ -1768,14 +1967,26 @@ ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path) {
     return EMS_OK;
 }
 
-// Reads the device status flag of the fused kernel's bounded waits.
+// Reads (and clears) the device flags: a bounded wait of the fused or
+// marching kernel that ran out (EMS_ERR_TIMEOUT), a non-finite field value a
+// marching step wrote (EMS_ERR_DIVERGED). The errors surface here, at the
+// host's next check, as the reference's stepping itself never fails
+// (src/engine/mod.rs:456-458).
 static ems_status device_status(ems_gpu* h) {
-    if (!h->status) return EMS_OK;
-    int st = 0;
-    if (check(h, cudaMemcpyAsync(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status"))
+    int st[2] = {0, 0};
+    if (h->status &&
+        check(h, cudaMemcpyAsync(&st[0], h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status"))
+        return EMS_ERR_CUDA;
+    if (check(h, cudaMemcpyAsync(&st[1], h->diverged, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status"))
         return EMS_ERR_CUDA;
     if (check(h, cudaStreamSynchronize(h->stream), "status")) return EMS_ERR_CUDA;
-    if (st) return fail(h, EMS_ERR_TIMEOUT, "a bounded wait of the fused kernel ran out");
+    if (st[0] || st[1]) {
+        if (h->status) cudaMemsetAsync(h->status, 0, sizeof(int), h->stream);
+        cudaMemsetAsync(h->diverged, 0, sizeof(int), h->stream);
+        if (check(h, cudaStreamSynchronize(h->stream), "status")) return EMS_ERR_CUDA;
+    }
+    if (st[0]) return fail(h, EMS_ERR_TIMEOUT, "a bounded wait of the fused or marching kernel ran out");
+    if (st[1]) return fail(h, EMS_ERR_DIVERGED, "a marching step wrote a non-finite field value");
     return EMS_OK;
 }
 
@@ -1944,7 +2155,7 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
 }
 
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
-    if (!h || schedule < 0 || schedule > 6) return EMS_ERR_INVALID;
+    if (!h || schedule < 0 || schedule > 7) return EMS_ERR_INVALID;
     if (h->oe_curl && (schedule == 2 || schedule == 3))
         return fail(h, EMS_ERR_INVALID, "the fused and two-kernel schedules sum the curl in the default order only");
     if (h->has_upml && (schedule == 2 || schedule == 3 || schedule == 5))
@@ -1956,6 +2167,8 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
         return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources") : h->tables_why));
     if (schedule == 6 && !(h->tables_ok && h->interior_why.empty()))
         return fail(h, EMS_ERR_INVALID, "interior schedule unavailable: " + (h->tables_ok ? h->interior_why : h->tables_why));
+    if (schedule == 7 && !(h->tables_ok && h->march_why.empty()))
+        return fail(h, EMS_ERR_INVALID, "marching schedule unavailable: " + (h->tables_ok ? h->march_why : h->tables_why));
     h->schedule = schedule;
     return EMS_OK;
 }
@@ -1977,6 +2190,26 @@ ems_status ems_gpu_set_curl_order(ems_gpu* h, int order) {
 ems_status ems_gpu_set_interior_planes(ems_gpu* h, uint32_t planes) {
     if (!h || planes < 1 || planes > 4096) return EMS_ERR_INVALID;
     h->interior_planes = planes;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_check(ems_gpu* h) {
+    if (!h) return EMS_ERR_INVALID;
+    cudaSetDevice(h->device);
+    if (check(h, cudaGetLastError(), "check")) return EMS_ERR_CUDA;
+    return device_status(h);
+}
+
+ems_status ems_gpu_test_wait_timeout(ems_gpu* h, uint64_t limit_ns) {
+    if (!h || !limit_ns || limit_ns > 10000000000ull) return EMS_ERR_INVALID;
+    h->test_wait_ns = limit_ns;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_set_march(ems_gpu* h, int shape, uint32_t planes) {
+    if (!h || shape < 0 || shape >= kNumMarchShapes || planes < 1 || planes > 4096) return EMS_ERR_INVALID;
+    h->march_shape = shape;
+    h->march_planes = planes;
     return EMS_OK;
 }
 

@@ -118,6 +118,9 @@ struct FusedParams {
     double* partials;      // per CTA energy share
     int energy;
     int* status;           // nonzero: a bounded wait ran out
+    int* diverged;         // set by the marching kernel where it writes a non-finite E value
+    uint64_t wait_ns;      // limit of the marching kernel's waits (0: kWaitNs)
+    uint32_t test_extra_tx; // test hook: bytes the marching kernel's first block expects in excess
     InteriorBox skip;      // quads the split kernels leave to the interior kernel
     QuadMap qmap;          // which quads a split-kernel thread takes
 };
@@ -140,8 +143,8 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Waits for phase `parity` of the barrier; gives up (returns false) after
-// kWaitNs nanoseconds.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// `limit_ns` nanoseconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
     uint32_t done = 0;
     const uint64_t t0 = global_ns();
     for (uint32_t it = 0;; ++it) {
@@ -153,7 +156,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
-        if ((it & 63u) == 63u && global_ns() - t0 > kWaitNs) return false;
+        if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -175,7 +178,9 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 // phase counter and a wait that would not succeed is reported.
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t) { *bar = 0; }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) { emu::expect_tx(bar, bytes); }
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return emu::wait(bar, parity); }
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
+    return emu::wait(bar, parity, limit_ns);
+}
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     emu::bulk(dst, src, bytes, bar);
 }
@@ -260,8 +265,12 @@ __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets,
                 s = __dadd_rn(s, __dmul_rn(__dadd_rn(__dsub_rn(__dmul_rn(a, jq), __dmul_rn(qq, ic)), half_prev), iz));
             }
         }
-        const float u_new = (float)__ddiv_rn(__dsub_rn((double)u32, __dmul_rn(cb, s)),
-                                             __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
+        // Without trapezoidal poles the denominator is exactly 1 and the
+        // quotient the numerator itself.
+        const double num = __dsub_rn((double)u32, __dmul_rn(cb, s));
+        const float u_new = R.sum_inv_z == 0.0
+                                ? (float)num
+                                : (float)__ddiv_rn(num, __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, cb), R.sum_inv_z)));
         if (R.kinds != (1u << R.np) - 1u) {
             const double half_new = __dmul_rn(0.5, (double)u_new);
             for (uint32_t p = 0; p < R.np; ++p) {

@@ -1769,7 +1769,9 @@ int ems_drive(const ems_stepper* s, const ems_run_limits* lim, ems_run_outcome* 
     for (;;) {
         if (steps >= max) { reason = 1; break; }
         const uint64_t n = steps;  // timestep of a fresh engine
-        if (s->step_with_energy(s->ctx, &w) != 0) { reason = 3; break; }
+        // A stepper that reports divergence (EMS_ERR_DIVERGED) ends the run
+        // as a non-finite energy does (src/engine/run.rs:156-161).
+        if (const int rc = s->step_with_energy(s->ctx, &w)) { reason = rc == EMS_ERR_DIVERGED ? 2 : 3; break; }
         ++steps;
         ++checks;
         w_max = std::max(w_max, w);

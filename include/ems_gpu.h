@@ -339,12 +339,15 @@ ems_status ems_gpu_profile_read(ems_gpu* h, int kernel, double* ms, uint64_t* la
  * left in L2; not with magnetic sources), 6 = interior (one pass of both
  * updates over the box inside the CPML layers, the split kernels around it,
  * old and new fields in two buffers; CPML, electric poles, E sources and
- * probes only; energy steps run the split kernels). Results are identical
- * bit for bit. Asking for a schedule the model cannot run returns
- * EMS_ERR_INVALID. */
+ * probes only; energy steps run the split kernels), 7 = marching (one pass
+ * of both updates and both CPML corrections over the whole grid, plane
+ * windows staged in shared memory by TMA, old and new fields in two
+ * buffers, then the electric poles and the hooks; the same operators as 6;
+ * energy steps run the split kernels). Results are identical bit for bit.
+ * Asking for a schedule the model cannot run returns EMS_ERR_INVALID. */
 ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule);
 
-/* The schedule steps run with (1 to 6 as above). */
+/* The schedule steps run with (1 to 7 as above). */
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
 
 /* The interior schedule's box, nodes [box[0..2], box[3..5]) along x, y, z;
@@ -371,6 +374,29 @@ ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes);
  * before its chunk again, so short chunks add work and long ones fewer,
  * longer-lived blocks. */
 ems_status ems_gpu_set_interior_planes(ems_gpu* h, uint32_t planes);
+
+/* Synchronises the handle's stream and reports what its device flags hold
+ * since the last check (and clears them): EMS_ERR_TIMEOUT if a bounded wait
+ * of the fused or marching kernel ran out, EMS_ERR_DIVERGED if a marching
+ * step wrote a non-finite field value (NaN or Inf). Field downloads, sample
+ * reads and step_with_energy report the same at their end. This is the
+ * check at which device errors surface: stepping itself never fails, as in
+ * the reference (src/engine/mod.rs:456-458; the run loop's Diverged outcome,
+ * src/engine/run.rs:156-161). */
+ems_status ems_gpu_check(ems_gpu* h);
+
+/* Test hook of the bounded waits: the next marching step's first block
+ * expects 16 more bytes on its first ring barrier than its copies deliver
+ * (every copy lands; the phase never completes) and its waits give up after
+ * `limit_ns` nanoseconds (1 .. 10^10). That block then sets the timeout flag
+ * and returns; the step's result is not defined, and the next check returns
+ * EMS_ERR_TIMEOUT. The handle and the device context stay usable. */
+ems_status ems_gpu_test_wait_timeout(ems_gpu* h, uint64_t limit_ns);
+
+/* The marching schedule's tile shape (0: 8 rows, 3 stages; 1: 8 rows, 4
+ * stages; 2: 4 rows, 4 stages; 3: 16 rows, 3 stages) and the planes a block
+ * marches through (1 to 4096; default 32). */
+ems_status ems_gpu_set_march(ems_gpu* h, int shape, uint32_t planes);
 
 /* Picks the fastest in-place schedule (4, 3, 5 or 1) for this model's grid
  * shape and operators: from `cache_path` (a text file of earlier picks,

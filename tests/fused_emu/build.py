@@ -9,7 +9,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 def build(asan: bool = False) -> str:
     out = os.path.join(HERE, "libfused_emu_asan.so" if asan else "libfused_emu.so")
     deps = [os.path.join(HERE, f) for f in ("harness.cpp", "emu_shim.h")] + [
-        os.path.join(ROOT, "ems_b200", "csrc", f) for f in ("fused.cuh", "kernels.cuh", "arith.cuh", "separate.cuh", "split.cuh", "interior.cuh", "fused_tables.h")]
+        os.path.join(ROOT, "ems_b200", "csrc", f) for f in ("fused.cuh", "kernels.cuh", "arith.cuh", "separate.cuh", "split.cuh", "interior.cuh", "march.cuh", "fused_tables.h")]
     if os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
         return out
     cmd = ["g++", "-std=c++20", "-O1", "-g", "-ffp-contract=off", "-fPIC", "-shared", "-DEMS_HOST_EMULATION",

@@ -10,6 +10,7 @@
 
 #include <atomic>
 #include <barrier>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -69,6 +70,16 @@ inline void sincospi(double x, double* s, double* c) {
 inline unsigned atomicAdd(uint32_t* p, uint32_t v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
 inline int atomicExch(int* p, int v) { return __atomic_exchange_n(p, v, __ATOMIC_SEQ_CST); }
 
+// The host stand-in of a TMA tensor map (what cuTensorMapEncodeTiled is
+// given for the engine's f32 field maps): base, extents (innermost first),
+// the strides of dimensions 1 and 2 in elements, the box.
+struct CUtensorMap {
+    const float* base;
+    uint64_t dim[3];
+    uint64_t stride[2];
+    uint32_t box[3];
+};
+
 namespace emu {
 struct Block {
     std::barrier<>* bar = nullptr;
@@ -76,6 +87,7 @@ struct Block {
     size_t smem_bytes = 0;
     std::vector<double> sums;
     std::atomic<int> errors{0};
+    std::atomic<int> orflag{0};
     char msg[256] = {0};
 };
 extern Block* cur;
@@ -105,13 +117,51 @@ inline void bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     __atomic_store_n(bar, phase | (pend << 32), __ATOMIC_SEQ_CST);
 }
 
-inline bool wait(uint64_t* bar, uint32_t parity) {
+// A tiled 3-D tensor copy global → shared: the box at coordinates (x, y, z),
+// entries outside the tensor zero-filled, completing the box's bytes on
+// `bar`. Checks what the hardware requires: a destination inside shared
+// memory on a 128-byte boundary, and x × 4 bytes a multiple of 16.
+inline void tensor3d(void* dst, const CUtensorMap* m, int x, int y, int z, uint64_t* bar) {
+    const size_t n = (size_t)m->box[0] * m->box[1] * m->box[2];
+    unsigned char* d = (unsigned char*)dst;
+    if (d < cur->smem || d + n * 4 > cur->smem + cur->smem_bytes) fail("tensor copy outside shared memory");
+    if ((uintptr_t)(d - cur->smem) & 127) fail("tensor copy destination not 128-byte aligned");
+    if (((long)x * 4) % 16 != 0) fail("tensor copy x coordinate not 16-byte aligned");
+    float* o = (float*)dst;
+    for (uint32_t c = 0; c < m->box[2]; ++c)
+        for (uint32_t b = 0; b < m->box[1]; ++b)
+            for (uint32_t a = 0; a < m->box[0]; ++a) {
+                const long xx = (long)x + a, yy = (long)y + b, zz = (long)z + c;
+                const bool in = xx >= 0 && yy >= 0 && zz >= 0 && (uint64_t)xx < m->dim[0] &&
+                                (uint64_t)yy < m->dim[1] && (uint64_t)zz < m->dim[2];
+                *o++ = in ? m->base[(uint64_t)zz * m->stride[1] + (uint64_t)yy * m->stride[0] + (uint64_t)xx] : 0.0f;
+            }
+    const uint32_t bytes = (uint32_t)(n * 4);
+    uint64_t v = __atomic_load_n(bar, __ATOMIC_SEQ_CST);
+    uint64_t pend = v >> 32;
+    if (pend < bytes) fail("tensor copy beyond the expected bytes");
+    pend -= bytes;
+    uint64_t phase = v & 0xffffffffull;
+    if (pend == 0) phase++;
+    __atomic_store_n(bar, phase | (pend << 32), __ATOMIC_SEQ_CST);
+}
+
+// __syncthreads_or: a barrier that returns whether any thread passed true.
+inline bool sync_or(bool v);
+
+// A bounded wait: false after `limit_ns` of wall time (or 200 M polls)
+// without the phase completing, as the device code's waits give up.
+inline bool wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = 2000000000ull) {
+    const auto t0 = std::chrono::steady_clock::now();
     for (long it = 0; it < 200000000L; ++it) {
         uint64_t v = __atomic_load_n(bar, __ATOMIC_SEQ_CST);
         if (((v & 0xffffffffull) & 1u) != parity) return true;
+        if ((it & 255) == 255 &&
+            (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count() >
+                limit_ns)
+            return false;
         std::this_thread::yield();
     }
-    fail("mbarrier wait never satisfied");
     return false;
 }
 
@@ -128,3 +178,13 @@ inline double block_sum(double v) {
 }  // namespace emu
 
 inline void __syncthreads() { emu::cur->bar->arrive_and_wait(); }
+
+inline bool emu::sync_or(bool v) {
+    cur->bar->arrive_and_wait();
+    if (v) cur->orflag.store(1);
+    cur->bar->arrive_and_wait();
+    const bool r = cur->orflag.load() != 0;
+    cur->bar->arrive_and_wait();
+    if (threadIdx.x == 0 && threadIdx.y == 0) cur->orflag.store(0);
+    return r;
+}

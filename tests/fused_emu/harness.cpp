@@ -19,6 +19,7 @@ void fail(const char* what) {
 #include "../../ems_b200/csrc/separate.cuh"
 #include "../../ems_b200/csrc/split.cuh"
 #include "../../ems_b200/csrc/interior.cuh"
+#include "../../ems_b200/csrc/march.cuh"
 
 using namespace emsk;
 
@@ -610,4 +611,187 @@ extern "C" int emu_pole_prev_fold(const ems_engine_desc* d, int electric) {
     }
     const bool poles_first = pos_poles >= 0 && pos_cpml >= 0 && pos_poles < pos_cpml;
     return pole_prev_fold(d, electric != 0, poles_first) ? 1 : 0;
+}
+
+// Runs `steps` steps of the marching kernel (march.cuh) with R rows per
+// block, an S-stage ring and x chunks of `planes` from the fields given in
+// reference layout (overwritten with the result); models with CPML layers
+// and probes only (the pole and hook kernels are the split schedule's).
+// Old and new fields in two buffers, H ψ in two buffers, E ψ in place; the
+// tensor copies of the ring are bounds- and alignment-checked.
+template <uint32_t R, uint32_t S>
+static int march_run(const ems_engine_desc* d, uint64_t steps, float** fields, uint32_t planes,
+                     uint32_t test_extra_tx = 0, uint64_t wait_ns = 0) {
+    g_err[0] = 0;
+    for (size_t k = 0; k < d->n_ops; ++k)
+        if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE && d->ops[k].kind != EMS_OP_POLES) {
+            std::snprintf(g_err, sizeof g_err, "only CPML, electric poles and probes are emulated");
+            return 1;
+        }
+    const std::string why = march_why(d);
+    if (!why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "no marching step: %s", why.c_str());
+        return 1;
+    }
+    Grid g{};
+    g.nx = (uint32_t)d->nodes[0];
+    g.ny = (uint32_t)d->nodes[1];
+    g.nz = (uint32_t)d->nodes[2];
+    g.pitch = (g.nz + 31u) & ~31u;
+    g.n = (uint64_t)g.nx * g.ny * g.nz;
+    g.np = (uint64_t)g.nx * g.ny * g.pitch;
+    FusedTables T = build_fused_tables(d, g.pitch);
+    if (!T.why.empty()) {
+        std::snprintf(g_err, sizeof g_err, "not eligible: %s", T.why.c_str());
+        return 1;
+    }
+    auto pad = [&](const float* src, std::vector<float>& dst) {
+        dst.assign(g.np, 0.0f);
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r) std::memcpy(&dst[r * g.pitch], src + r * g.nz, g.nz * 4);
+    };
+    std::vector<float> buf[2][6];
+    for (int c = 0; c < 6; ++c) {
+        pad(fields[c], buf[0][c]);
+        buf[1][c] = buf[0][c];
+    }
+    std::vector<float> dense[12];
+    FusedParams P{};
+    P.g = g;
+    P.dt = d->dt;
+    for (int l = 0; l < 12; ++l) {
+        if (T.lane[l].pooled) {
+            P.lane[l].rid = T.lane[l].rid.data();
+            P.lane[l].rows = T.lane[l].rows.data();
+            P.lane[l].bg = T.lane[l].bg;
+        } else {
+            pad(d->coeff[l], dense[l]);
+            P.lane[l].dense = dense[l].data();
+        }
+    }
+    std::vector<std::vector<float>> psi_e, psi_h0, psi_h1;
+    std::vector<std::pair<int, int>> at_h;
+    psi_e.reserve(T.slabs.size());
+    psi_h0.reserve(T.slabs.size());
+    psi_h1.reserve(T.slabs.size());
+    for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < 3; ++c) P.nslab[side][c] = T.nslab[side][c];
+    for (const FusedSlabSpec& sp : T.slabs) {
+        FSlab& f = P.slab[sp.side][sp.comp][sp.q];
+        for (int a = 0; a < 3; ++a) {
+            f.lo[a] = (uint32_t)sp.src->lo[a];
+            f.hi[a] = (uint32_t)sp.src->hi[a];
+        }
+        f.normal = (uint32_t)sp.src->normal;
+        f.b = sp.src->b;
+        f.a = sp.src->a;
+        f.k = sp.src->k;
+        if (sp.side) {
+            psi_e.emplace_back(sp.len, 0.0f);
+            f.psi_old = f.psi_new = psi_e.back().data();
+        } else {
+            psi_h0.emplace_back(sp.len, 0.0f);
+            psi_h1.emplace_back(sp.len, 0.0f);
+            at_h.push_back({sp.comp, sp.q});
+        }
+    }
+    for (int a = 0; a < 3; ++a) P.cmask[a] = T.cmask[a].data();
+    std::vector<double> pj, pq;
+    if (T.has_poles) {
+        size_t np = 0;
+        for (size_t k = 0; k < d->n_ops; ++k)
+            if (d->ops[k].kind == EMS_OP_POLES) np = ((const ems_poles*)d->ops[k].table)->electric.n_poles;
+        pj.assign(np, 0.0);
+        pq.assign(np, 0.0);
+        P.has_poles = 1;
+        P.runs = T.runs.data();
+        P.sets = T.sets.data();
+        P.row_runs = T.row_runs.data();
+        P.pj = pj.data();
+        P.pq = pq.data();
+    }
+    P.poles_first = T.poles_first ? 1 : 0;
+    int status = 0, diverged = 0;
+    P.status = &status;
+    P.diverged = &diverged;
+    P.test_extra_tx = test_extra_tx;
+    P.wait_ns = wait_ns;
+    using LT = MarchLayout<R>;
+    const size_t smem_bytes = LT::bytes(S);
+    std::vector<unsigned char> smem(smem_bytes + 128);
+    unsigned char* sm = smem.data() + (128 - ((uintptr_t)smem.data() & 127)) % 128;
+    uint32_t nb[3];
+    march_blocks(g, R, planes, nb);
+    const unsigned threads = 32 * (R + 1);
+    int cur = 0;
+    for (uint64_t s = 0; s < steps; ++s) {
+        MarchMaps M{};
+        for (int a = 0; a < 3; ++a) {
+            P.uo[a] = buf[cur][a].data();
+            P.io[a] = buf[cur][3 + a].data();
+            P.un[a] = buf[cur ^ 1][a].data();
+            P.in[a] = buf[cur ^ 1][3 + a].data();
+            M.u[a] = CUtensorMap{P.uo[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMuW, R + 2, 1}};
+            M.i[a] = CUtensorMap{P.io[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMiW, R + 1, 1}};
+        }
+        for (size_t q = 0; q < at_h.size(); ++q) {
+            FSlab& f = P.slab[0][at_h[q].first][at_h[q].second];
+            f.psi_old = (s & 1) ? psi_h1[q].data() : psi_h0[q].data();
+            f.psi_new = (s & 1) ? psi_h0[q].data() : psi_h1[q].data();
+        }
+        blockDim = EmuDim{threads, 1, 1};
+        gridDim = EmuDim{nb[0], nb[1], nb[2]};
+        for (unsigned bz = 0; bz < nb[2]; ++bz)
+            for (unsigned by = 0; by < nb[1]; ++by)
+                for (unsigned bx = 0; bx < nb[0]; ++bx) {
+                    blockIdx = EmuDim{bx, by, bz};
+                    emu::Block blk;
+                    std::barrier<> bar((std::ptrdiff_t)threads);
+                    blk.bar = &bar;
+                    blk.smem = sm;
+                    blk.smem_bytes = smem_bytes;
+                    blk.sums.assign(threads, 0.0);
+                    std::memset(sm, 0xA5, smem_bytes);  // stale shared memory must not matter
+                    emu::cur = &blk;
+                    std::vector<std::thread> th;
+                    for (unsigned t = 0; t < threads; ++t)
+                        th.emplace_back([&, t] {
+                            threadIdx.x = t;
+                            k_march<R, S, false>(P, M, planes);
+                        });
+                    for (auto& x : th) x.join();
+                    emu::cur = nullptr;
+                    if (blk.errors.load()) {
+                        std::snprintf(g_err, sizeof g_err, "step %llu block (%u, %u, %u): %s",
+                                      (unsigned long long)s, bx, by, bz, blk.msg);
+                        return 2;
+                    }
+                }
+        if (status) {
+            std::snprintf(g_err, sizeof g_err, "status flag set at step %llu", (unsigned long long)s);
+            return 3;
+        }
+        if (diverged) {
+            std::snprintf(g_err, sizeof g_err, "divergence flag set at step %llu", (unsigned long long)s);
+            return 4;
+        }
+        cur ^= 1;
+    }
+    for (int c = 0; c < 6; ++c)
+        for (size_t r = 0; r < (size_t)g.nx * g.ny; ++r)
+            std::memcpy(fields[c] + r * g.nz, &buf[cur][c][r * g.pitch], g.nz * 4);
+    return 0;
+}
+
+// One marching step with the bounded-wait test hook armed (the first block
+// expects 16 bytes more than its copies deliver; waits give up after
+// `wait_ns`): 3 when the kernel reports the timeout as the engine reads it.
+extern "C" int emu_march_timeout(const ems_engine_desc* d, float** fields, uint64_t wait_ns) {
+    return march_run<8, 3>(d, 1, fields, 4, 16u, wait_ns);
+}
+
+extern "C" int emu_march_run(const ems_engine_desc* d, uint64_t steps, float** fields, uint32_t rows, uint32_t planes) {
+    if (rows == 8) return march_run<8, 3>(d, steps, fields, planes);
+    if (rows == 3) return march_run<3, 4>(d, steps, fields, planes);
+    std::snprintf(g_err, sizeof g_err, "rows must be 3 or 8");
+    return 1;
 }

@@ -37,6 +37,10 @@ def emu_lib(asan=False):
     lib.emu_split_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.emu_interior_run.restype = C.c_int
     lib.emu_interior_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.emu_march_run.restype = C.c_int
+    lib.emu_march_run.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.emu_march_timeout.restype = C.c_int
+    lib.emu_march_timeout.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
     lib.emu_pole_prev_fold.restype = C.c_int
     lib.emu_pole_prev_fold.argtypes = [C.c_void_p, C.c_int]
     lib.emu_error.restype = C.c_char_p
@@ -195,6 +199,47 @@ def test_interior_source_equals_oracle(n, graded):
     for name, a, b in zip(["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"], got, want):
         bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
         assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])} (box {box})"
+
+
+@pytest.mark.parametrize("n,graded,rows,planes,scheme", [
+    ((13, 11, 30), False, 8, 5, None), ((20, 19, 140), True, 8, 32, E.LEAPFROG),
+    ((9, 14, 131), False, 3, 4, E.TRAPEZOIDAL), ((17, 10, 7), True, 3, 3, None),
+    ((14, 12, 36), False, 8, 4, E.OPENEMS_POLES)])
+def test_march_source_equals_oracle(n, graded, rows, planes, scheme):
+    """The marching kernel (march.cuh): one pass of both updates, both CPML
+    corrections and the electric poles over the whole grid, tensor-copied
+    plane windows in a ring, recomputed rows below the tiles and nodes below
+    the z tiles, x chunks, several z tiles (rows of 131 and 141 nodes) and row
+    remainders, leapfrog, trapezoidal and openEMS poles: fields bit-exact
+    with the oracle."""
+    m = model(n, scheme if scheme is not None else E.TRAPEZOIDAL, poles=scheme is not None, graded=graded)
+    state = random_state(m, seed=5)
+    steps = 3
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    lib = emu_lib()
+    assert lib.emu_march_run(m.desc, steps, ptrs, rows, planes) == 0, lib.emu_error().decode()
+    want, _, _ = run_oracle(m, state, steps)
+    for name, a, b in zip(["u_x", "u_y", "u_z", "i_x", "i_y", "i_z"], arrs, want):
+        bad = np.argwhere(a.view(np.uint32) != b.view(np.uint32))
+        assert bad.size == 0, f"{name}: {len(bad)} differ, first {tuple(bad[0])}"
+
+
+def test_march_bounded_wait_runs_out_and_reports():
+    """The marching kernel's first block expects more bytes than its copies
+    deliver: its wait gives up after the limit, the block sets the status
+    flag and returns (every other block completes), so the step reports a
+    timeout instead of hanging. A NaN in a field sets the divergence flag."""
+    m = model((13, 11, 30), E.TRAPEZOIDAL, poles=False)
+    lib = emu_lib()
+    state = random_state(m, seed=6)
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    assert lib.emu_march_timeout(m.desc, ptrs, 5_000_000) == 3, lib.emu_error().decode()
+    arrs = [np.ascontiguousarray(x.copy()) for x in state]
+    arrs[2][6, 5, 14] = np.nan
+    ptrs = (C.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    assert lib.emu_march_run(m.desc, 1, ptrs, 8, 4) == 4, lib.emu_error().decode()
 
 
 def test_pole_capture_fold_decision():

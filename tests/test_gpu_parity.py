@@ -183,7 +183,7 @@ def test_invalid_tables_rejected():
 
 
 @pytest.mark.parametrize("n", [40, 67])
-@pytest.mark.parametrize("schedule", [2, 3, 4, 6])
+@pytest.mark.parametrize("schedule", [2, 3, 4, 6, 7])
 def test_dispersive_box_chunks_and_tiles(n, schedule):
     """Sizes whose rows, tiles and x chunks leave remainders."""
     w = W.dispersive_box(n=n, radius=n / 6, slab=3, cpml=4, steps=120)
@@ -255,6 +255,64 @@ def test_interior_schedule_uploads_switches_and_probes(order):
     mm, _ = mixed_model(scheme=E.LEAPFROG, h_source=True, steps=20)
     with pytest.raises(E.EngineError):
         E.Engine(mm).set_schedule(6)
+
+
+@pytest.mark.parametrize("shape,planes", [(0, 32), (1, 7), (2, 5), (3, 64)])
+@pytest.mark.parametrize("order", [0, 1])
+def test_march_schedule_uploads_switches_and_probes(order, shape, planes):
+    """The marching schedule (one pass of both updates and both CPML
+    corrections over the whole grid, TMA-staged plane windows, two field
+    buffers) in every tile shape: probe series and fields bit for bit through
+    energy steps (split, in place), a field upload, switches to and from
+    other schedules, in both curl orders; refused where a hook sits between
+    the two updates."""
+    w = W.dispersive_box(n=72, radius=10, slab=4, cpml=6, steps=260)
+    m = w.model
+    g = E.Engine(m)
+    g.set_curl_order(order)
+    g.set_march(shape, planes)
+    o = OracleEngine(m, threads=4)
+    o.set_curl_order(order)
+    rng = np.random.default_rng(9)
+    eg, eo = [], []
+    for sch, n in ((7, 40), (4, 7), (7, 33), (6, 5), (7, 60), (1, 4)):
+        g.set_schedule(sch)
+        assert g.schedule == sch
+        eg.append(g.step_with_energy())
+        eo.append(o.step_with_energy())
+        g.run(n)
+        o.run(n)
+        if sch == 7 and n == 33:
+            v = (rng.standard_normal(m.nodes) * 1e-3).astype(np.float32)
+            g.set_field(1, 2, v)
+            o.set_field(1, 2, v)
+    g.set_schedule(7)
+    g.run(31)
+    o.run(31)
+    assert_fields_equal(g, o, f"marching schedule, curl order {order}, shape {shape}")
+    for p in w.probes:
+        _series_equal(g, o, p)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+    mm, _ = mixed_model(scheme=E.LEAPFROG, h_source=True, steps=20)
+    with pytest.raises(E.EngineError):
+        E.Engine(mm).set_schedule(7)
+
+
+def test_march_schedule_odd_grid_without_layers():
+    """No CPML, a z extent of 131 nodes (two z tiles, the second one of
+    three nodes), rows that leave a short last tile, a PMC face and lossy
+    media: the marching schedule equals the oracle bit for bit."""
+    m = E.Model.uniform([23, 13, 130], [1e-3, 1.1e-3, 0.9e-3])
+    m.fill(m.cells().box([3, 2, 10], [15, 9, 100]), m.material(eps_r=3.0, kappa=0.02))
+    m.faces([E.PEC, E.PMC, E.PEC, E.PEC, E.PEC, E.PEC])
+    m.build()
+    m.add_source(E.SOFT_E, [(E.Y, (11, 6, 64), 1.0)], 20e9, 15e9, 300)
+    p = m.add_probe(E.VOLTAGE, [(E.Y, (11, 6, 70), 1.0)])
+    g, o, eg, eo = _lockstep(m, 160, energy_every=16, schedule=7)
+    assert g.schedule == 7
+    assert_fields_equal(g, o, "march, odd grid")
+    _series_equal(g, o, p)
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
 
 
 @pytest.mark.parametrize("h_source", [True, False])
