@@ -65,7 +65,7 @@ def parse():
                     help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
                          "sweep; learned: training and held-out evaluation of the learned early stop")
     ap.add_argument("--models", type=int, default=64, help="sweep: number of patch variants")
-    ap.add_argument("--sweep-cells", type=int, nargs=2, default=[60, 160], help="sweep: N range (N x N x N/2 cells)")
+    ap.add_argument("--sweep-cells", type=int, nargs=2, default=[60, 160], help="sweep: N range (N x N x N cells)")
     ap.add_argument("--max-steps", type=int, default=40000, help="sweep: step limit per model")
     ap.add_argument("--train", type=int, default=2000, help="learned: training variants")
     ap.add_argument("--test", type=int, default=256, help="learned: held-out variants")
@@ -481,15 +481,16 @@ def run_sweep(args):
     import ems_b200 as E
     from ems_b200 import workloads as W
 
-    ws = [W.patch_variant(s, cells=tuple(args.sweep_cells), steps=args.max_steps) for s in range(args.models)]
+    ws = [W.sweep_variant(s, cells=tuple(args.sweep_cells), steps=args.max_steps) for s in range(args.models)]
     t_exc = E.waveform_duration(2e9, 1.5e9)
     lims = [E.energy_decay_limits(args.max_steps, -40.0, w.model.dt, excitation_end=t_exc, interval=50) for w in ws]
     cells = [w.info["cells"] for w in ws]
     t0 = time.perf_counter()
     b = E.Batch([w.model for w in ws], max_steps=args.max_steps)
     t1 = time.perf_counter()
-    outs_b = E.run_until_batch(b, lims)
-    torch.cuda.synchronize(0)
+    with Clocks(0) as clk:
+        outs_b = E.run_until_batch(b, lims)
+        torch.cuda.synchronize(0)
     t2 = time.perf_counter()
     b.close()
     upd_b = sum(c * o.steps for c, o in zip(cells, outs_b))
@@ -501,13 +502,18 @@ def run_sweep(args):
         torch.cuda.synchronize(0)
         t_one += time.perf_counter() - ta
         g.close()
-    same = all((x.reason, x.steps) == (y.reason, y.steps) for x, y in zip(outs_b, outs_1))
+    # The same outcome per model: stop reason, step and number of checks,
+    # and the final energy (a reduction in another order: within 1e-12).
+    same = all((x.reason, x.steps, x.checks) == (y.reason, y.steps, y.checks) and
+               abs(x.energy - y.energy) <= 1e-12 * max(abs(y.energy), 1e-300) for x, y in zip(outs_b, outs_1))
     line = {
         "metric": "sweep wall time", "value": round(t2 - t1, 3), "unit": "s", "higher_is_better": False,
         "n_gpus": 1, "data": "synthetic",
-        "config": {"workload": f"{args.models} seeded patch variants, N x N x N/2 cells, N in {args.sweep_cells}, "
-                               f"-40 dB energy criterion every 50 steps, max {args.max_steps} steps",
-                   "total_cells": sum(cells)},
+        "config": {"workload": f"{args.models} seeded patch variants, each on its own graded N x N x N mesh, "
+                               f"N in {args.sweep_cells}, -40 dB energy criterion every 50 steps, "
+                               f"max {args.max_steps} steps",
+                   "total_cells": sum(cells), "cells_min": min(cells), "cells_max": max(cells)},
+        "clocks": clk.summary(),
         "batched": {"s": round(t2 - t1, 3), "create_s": round(t1 - t0, 3),
                     "mcell_updates_per_s": round(upd_b / (t2 - t1) / 1e6, 1)},
         "one_at_a_time": {"s": round(t_one, 3), "mcell_updates_per_s": round(upd_b / t_one / 1e6, 1)},

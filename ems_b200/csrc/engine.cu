@@ -1014,7 +1014,7 @@ ems_status run_step_interior(ems_gpu* h) {
 struct MarchShape {
     uint32_t rows, stages;
 };
-constexpr MarchShape kMarchShapes[] = {{8, 3}, {8, 4}, {4, 4}, {16, 3}};
+constexpr MarchShape kMarchShapes[] = {{7, 3}, {15, 3}, {8, 4}, {3, 4}};
 constexpr int kNumMarchShapes = (int)(sizeof(kMarchShapes) / sizeof(kMarchShapes[0]));
 
 // cuTensorMapEncodeTiled from the driver (through the runtime, so the
@@ -1033,7 +1033,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // The six tensor maps of the old fields of buffer (u, i) for tiles of R rows:
-// extents (pitch, ny, nx), boxes (kMuW, R + 2, 1) and (kMiW, R + 1, 1),
+// extents (pitch, ny, nx), boxes (kMW, R + 2, 1) and (kMW, R + 1, 1),
 // out-of-grid entries read as zero.
 static ems_status encode_march_maps(ems_gpu* h, float* const u[3], float* const i[3], uint32_t R, MarchMaps& M) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1041,7 +1041,7 @@ static ems_status encode_march_maps(ems_gpu* h, float* const u[3], float* const 
     const Grid& g = h->g;
     const cuuint64_t dims[3] = {g.pitch, g.ny, g.nx};
     const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.ny * g.pitch * 4};
-    const cuuint32_t ubox[3] = {kMuW, R + 2, 1}, ibox[3] = {kMiW, R + 1, 1}, es[3] = {1, 1, 1};
+    const cuuint32_t ubox[3] = {kMW, R + 2, 1}, ibox[3] = {kMW, R + 1, 1}, es[3] = {1, 1, 1};
     for (int c = 0; c < 3; ++c) {
         for (int side = 0; side < 2; ++side) {
             CUresult r = enc(side ? &M.i[c] : &M.u[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, side ? (void*)i[c] : (void*)u[c],
@@ -1071,10 +1071,10 @@ static ems_status launch_march(ems_gpu* h, const FusedParams& P, const MarchMaps
 }
 
 // One step through the marching schedule (march.cuh): the old fields in one
-// buffer, the one-pass kernel (both updates, both CPML corrections and the
-// electric poles over the whole grid) writing the new ones into the other,
-// then the serial hooks on the new fields. Steps that record the energy run
-// the split schedule in place.
+// buffer, the one-pass kernel (both updates and both CPML corrections over
+// the whole grid) writing the new ones into the other, the electric poles on
+// the new fields (u^n from the old buffer), then the serial hooks on the new
+// fields. Steps that record the energy run the split schedule in place.
 ems_status run_step_march(ems_gpu* h) {
     const Grid& g = h->g;
     cudaStream_t s = h->stream;
@@ -1149,16 +1149,22 @@ ems_status run_step_march(ems_gpu* h) {
     cudaEvent_t ev = h->prof_begin();
     const bool oe = h->oe_curl;
     switch (shape) {
-    case 0: st = launch_march<8, 3>(h, P, ms.m, oe); break;
-    case 1: st = launch_march<8, 4>(h, P, ms.m, oe); break;
-    case 2: st = launch_march<4, 4>(h, P, ms.m, oe); break;
-    default: st = launch_march<16, 3>(h, P, ms.m, oe); break;
+    case 0: st = launch_march<7, 3>(h, P, ms.m, oe); break;
+    case 1: st = launch_march<15, 3>(h, P, ms.m, oe); break;
+    case 2: st = launch_march<8, 4>(h, P, ms.m, oe); break;
+    default: st = launch_march<3, 4>(h, P, ms.m, oe); break;
     }
     h->prof_end(2, ev);
     ++h->launches;
     if (st) return st;
-    // The kernel applied the electric poles from the old values; the saved
-    // values the split schedule keeps are not current after it.
+    // The electric poles on the new fields, u^n read from the old buffer.
+    for (auto& op : h->ops)
+        if (op.kind == EMS_OP_POLES && op.poles.e.n_edges) {
+            k_poles_blocks<true><<<blocks_for(op.poles.e.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
+                fb, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, 0, 0u, (uint32_t)op.poles.e.n_edges, fa);
+            ++h->launches;
+        }
+    // The saved values the split schedule keeps are not current after it.
     h->prev_e_valid = false;
     for (int a = 0; a < 3; ++a) {
         std::swap(h->u[a], h->u2[a]);

@@ -194,8 +194,8 @@ __device__ __forceinline__ void fence_mbar_init() {}
 // contains the node, in order: ψ = flush(b·ψ + a·s), t = flush(t + coef·(k·s + ψ)),
 // s the derivative term along the slab's normal (sA along next(c), sB along prev(c)).
 template <bool WRITE>
-__device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c, float t,
-                                        float coef, float sA, float sB) {
+__device__ __forceinline__ float cpml_body_inl(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c,
+                                               float t, float coef, float sA, float sB) {
     const int na = (c + 1) % 3;
     for (int q = 0; q < n; ++q) {
         const FSlab& s = list[q];
@@ -208,6 +208,13 @@ __device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, ui
         t = flush(__fadd_rn(t, __fmul_rn(coef, __fadd_rn(__fmul_rn(s.k[d], sv), psi))));
     }
     return t;
+}
+
+// The same, out of line (most nodes lie in no layer).
+template <bool WRITE>
+__device__ __noinline__ float cpml_body(const FSlab* list, int n, uint32_t i, uint32_t j, uint32_t k, int c, float t,
+                                        float coef, float sA, float sB) {
+    return cpml_body_inl<WRITE>(list, n, i, j, k, c, t, coef, sA, sB);
 }
 
 // The CPML slabs containing node (i, j, k): one bit per slab (cmask).
@@ -234,9 +241,9 @@ __device__ __forceinline__ float cpml_apply(const FusedParams& P, uint32_t bits,
 // (src/engine/dispersive.rs:1392-1470), if the edge has poles. A leapfrog
 // pole's new state does not depend on the corrected voltage and is stored
 // at once; a trapezoidal pole's is formed from its old state after it.
-__device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets, double* pj, double* pq, double dt,
-                                        const uint4 rr, uint32_t k, float u_star, float prev_f, float cb_f,
-                                        const float* prev_arr) {
+__device__ __forceinline__ float poles_run_inl(const PoleRun* runs, const double* sets, double* pj, double* pq,
+                                               double dt, const uint4 rr, uint32_t k, float u_star, float prev_f,
+                                               float cb_f, const float* prev_arr) {
     for (uint32_t q = 0; q < rr.y; ++q) {
         const PoleRun R = runs[rr.x + q];
         if (k < R.kb || k >= R.ke) continue;
@@ -286,6 +293,13 @@ __device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets,
         return u_new;
     }
     return u_star;
+}
+
+// The same, out of line.
+__device__ __noinline__ float poles_run(const PoleRun* runs, const double* sets, double* pj, double* pq, double dt,
+                                        const uint4 rr, uint32_t k, float u_star, float prev_f, float cb_f,
+                                        const float* prev_arr) {
+    return poles_run_inl(runs, sets, pj, pq, dt, rr, k, u_star, prev_f, cb_f, prev_arr);
 }
 
 // The pole correction of one edge, if its row has runs (the common case,

@@ -339,11 +339,14 @@ __host__ __device__ inline uint32_t shell_blocks(const ShellDev& S) {
 // new state does not depend on the corrected value and is stored at once; a
 // trapezoidal pole's is formed from its old state after it. save_prev: also
 // store the corrected value as the edge's saved value (the capture it
-// replaces would read the same value; pole_prev_fold).
+// replaces would read the same value; pole_prev_fold). prev_field: the field
+// array holding u^n (the old buffer of a two-buffer step), read in place of
+// the saved value; null: the saved value.
 __device__ __forceinline__ void poles_edge_core(const Fields& f, const Coeffs& c, const PoleSideDev& p,
                                                 const PoleRun& R, const double* sets, int electric, double dt,
-                                                int save_prev, uint32_t e, uint32_t idx, int ax, uint32_t p0) {
-    const float prev32 = p.prev[e];
+                                                int save_prev, uint32_t e, uint32_t idx, int ax, uint32_t p0,
+                                                const float* prev_field = nullptr) {
+    const float prev32 = prev_field ? prev_field[idx] : p.prev[e];
     const double prev = (double)prev32;
     float* fld = electric ? f.u[ax] : f.i[ax];
     float u32 = fld[idx];
@@ -398,13 +401,14 @@ __device__ __forceinline__ void poles_edge_core(const Fields& f, const Coeffs& c
 // independent of each other, so their latencies overlap).
 __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, const PoleSideDev& p, const PoleRun* runs,
                                            const double* sets, const uint32_t* run_of, int electric, double dt,
-                                           int save_prev, uint32_t e) {
+                                           int save_prev, uint32_t e, const Fields* old = nullptr) {
     if (e >= p.n_edges) return;
     const uint32_t r = __ldg(run_of + e);
     const uint32_t idx = __ldg(p.node + e);
     const int ax = (int)__ldg(p.axis + e);
     const uint32_t p0 = e ? __ldg(p.pole_end + e - 1) : 0u;
-    poles_edge_core(f, c, p, runs[r], sets, electric, dt, save_prev, e, idx, ax, p0);
+    poles_edge_core(f, c, p, runs[r], sets, electric, dt, save_prev, e, idx, ax, p0,
+                    old ? (electric ? old->u[ax] : old->i[ax]) : nullptr);
 }
 
 constexpr uint32_t kPoleBlock = 256;
@@ -413,12 +417,15 @@ constexpr uint32_t kPoleBlock = 256;
 // runs covering a block's edges (a contiguous range: a run holds
 // consecutive edges) are staged in shared memory and each edge's node, axis
 // and first pole state derived from its run, so the only per-edge traffic
-// is the field, the saved value and the pole state.
+// is the field, the saved value and the pole state. OLD: u^n comes from the
+// old buffer `old` of a two-buffer step instead of the saved values.
+template <bool OLD = false>
 __global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_constant__ Fields f,
                                                              const __grid_constant__ Coeffs c,
                                                              const __grid_constant__ PoleSideDev p, const PoleRun* runs,
                                                              const double* sets, const uint32_t* run_of, int electric,
-                                                             double dt, int save_prev, uint32_t e0, uint32_t e1) {
+                                                             double dt, int save_prev, uint32_t e0, uint32_t e1,
+                                                             const __grid_constant__ Fields old = Fields{}) {
     EMS_SHARED PoleRun sr[kPoleBlock];
     const uint32_t eb = e0 + blockIdx.x * kPoleBlock;
     if (eb >= e1) return;
@@ -426,7 +433,7 @@ __global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_consta
     const uint32_t r0 = __ldg(run_of + eb), r1 = __ldg(run_of + el);
     const uint32_t e = eb + threadIdx.x;
     if (r1 < r0 || r1 - r0 >= kPoleBlock) {  // not a contiguous run range: per edge
-        if (e <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e);
+        if (e <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e, OLD ? &old : nullptr);
         return;
     }
     const uint32_t nr = r1 - r0 + 1;
@@ -441,7 +448,8 @@ __global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_consta
     }
     const PoleRun& R = sr[lo];
     const uint32_t off = e - R.e0;
-    poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, e, R.node0 + off, (int)R.axis, R.p0 + off * R.np);
+    poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, e, R.node0 + off, (int)R.axis, R.p0 + off * R.np,
+                    OLD ? (electric ? old.u[R.axis] : old.i[R.axis]) : nullptr);
 }
 
 }  // namespace emsk

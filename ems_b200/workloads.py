@@ -17,6 +17,8 @@ with the shapes, sizes and value ranges of the configuration it stands for.
 * :func:`patch_antenna` — a graded-mesh patch antenna: FR-4 slab on a PEC
   z_min ground, PEC patch, 50 Ω lumped port along z, CPML on the other
   five faces (about 200×200×80 cells for the full configuration).
+* :func:`sweep_variant` — one seeded patch variant of the batched sweep on
+  its own graded N × N × N mesh (N in 60…160).
 """
 from __future__ import annotations
 
@@ -203,5 +205,68 @@ def patch_variant(seed: int, cells: tuple[int, int] = (60, 160), steps: int = 60
     port = m.add_lumped_port(E.Z, [px, py, 0], [px, py, nsub], 50.0, 2e9, 1.5e9, 1.0, steps)
     nn = m.nodes
     return Workload(f"patch_variant_{seed}_{nn[0] - 1}x{nn[1] - 1}x{nn[2] - 1}", m, steps, port=port,
+                    info={"seed": seed, "side_mm": side / mm, "eps_r": eps, "h_mm": h / mm, "offset_mm": off / mm,
+                          "cells": (nn[0] - 1) * (nn[1] - 1) * (nn[2] - 1), "f0": 2e9, "fc": 1.5e9})
+
+
+def density_lines(length: float, n: int, fine_at: list[float], ratio: float, width: float) -> np.ndarray:
+    """Exactly n cells over [0, length], graded: the cell density is `ratio`
+    times higher at the points `fine_at` than far from them (a Gaussian bump
+    of half-width `width` around each), the lines placed at the inverse of
+    the cumulative density."""
+    x = np.linspace(0.0, length, 20001)
+    bump = np.zeros_like(x)
+    for c in fine_at:
+        bump = np.maximum(bump, np.exp(-((x - c) / width) ** 2))
+    dens = 1.0 + (ratio - 1.0) * bump
+    cum = np.concatenate([[0.0], np.cumsum(0.5 * (dens[1:] + dens[:-1]) * np.diff(x))])
+    cum *= n / cum[-1]
+    lines = np.interp(np.arange(n + 1, dtype=float), cum, x)
+    lines[0], lines[-1] = 0.0, length
+    return lines
+
+
+def sweep_variant(seed: int, cells: tuple[int, int] = (60, 160), steps: int = 60000, cpml: int = 8,
+                  courant: float = 0.99) -> Workload:
+    """One seeded patch-antenna variant of the batched sweep: patch side
+    8–30 mm, substrate ε_r 2.2–10.2 and thickness 0.8–3.2 mm, port offset
+    2–10 mm from the patch centre, PEC ground at z_min, CPML on the other
+    five faces, 50 Ω port with a Gaussian f0 = 2 GHz, fc = 1.5 GHz; meshed to
+    its own size, N × N × N cells with N drawn from `cells`: x and y graded
+    three times finer at the patch edges and the port than far from them, z
+    with uniform substrate cells below air cells that grow away from it."""
+    mm = 1e-3
+    rng = np.random.default_rng(seed)
+    side = rng.uniform(8.0, 30.0) * mm
+    eps = rng.uniform(2.2, 10.2)
+    h = rng.uniform(0.8, 3.2) * mm
+    off = rng.uniform(2.0, 10.0) * mm
+    n = int(rng.integers(cells[0], cells[1] + 1))
+    sub = 2.2 * side + 10 * mm
+    lx = sub + 2 * 12.0 * mm
+    c = lx / 2
+    width = max(1.0 * mm, 4.0 * lx / n)
+    xl = density_lines(lx, n, [c - side / 2, c + side / 2, c + off], 3.0, width)
+    yl = density_lines(lx, n, [c - side / 2, c + side / 2, c], 3.0, width)
+    nsub = max(3, min(n // 5, int(round(h / (0.4 * lx / n)))))
+    air = 0.8 * lx
+    za = density_lines(air, n - nsub, [0.0], 3.0, 3.0 * width)
+    zl = np.concatenate([np.linspace(0.0, h, nsub + 1), h + za[1:]])
+    m = E.Model(xl, yl, zl)
+    near = lambda lines, v: int(np.argmin(np.abs(lines - v)))  # noqa: E731
+    i0, i1 = near(xl, c - sub / 2), near(xl, c + sub / 2)
+    j0, j1 = near(yl, c - sub / 2), near(yl, c + sub / 2)
+    m.fill(m.cells().box([i0, j0, 0], [i1, j1, nsub]), m.material(eps_r=eps))
+    p0, p1 = near(xl, c - side / 2), near(xl, c + side / 2)
+    q0, q1 = near(yl, c - side / 2), near(yl, c + side / 2)
+    m.pec_edges(E.X, [p0, q0, nsub], [p1 - 1, q1, nsub])
+    m.pec_edges(E.Y, [p0, q0, nsub], [p1, q1 - 1, nsub])
+    m.faces([E.PEC] * 6)
+    m.build(courant=courant)
+    m.add_cpml([cpml, cpml, cpml, cpml, 0, cpml])
+    px, py = near(xl, c + off), near(yl, c)
+    port = m.add_lumped_port(E.Z, [px, py, 0], [px, py, nsub], 50.0, 2e9, 1.5e9, 1.0, steps)
+    nn = m.nodes
+    return Workload(f"sweep_variant_{seed}_{nn[0] - 1}x{nn[1] - 1}x{nn[2] - 1}", m, steps, port=port,
                     info={"seed": seed, "side_mm": side / mm, "eps_r": eps, "h_mm": h / mm, "offset_mm": off / mm,
                           "cells": (nn[0] - 1) * (nn[1] - 1) * (nn[2] - 1), "f0": 2e9, "fc": 1.5e9})

@@ -393,9 +393,10 @@ ems_status ems_gpu_check(ems_gpu* h);
  * EMS_ERR_TIMEOUT. The handle and the device context stay usable. */
 ems_status ems_gpu_test_wait_timeout(ems_gpu* h, uint64_t limit_ns);
 
-/* The marching schedule's tile shape (0: 8 rows, 3 stages; 1: 8 rows, 4
- * stages; 2: 4 rows, 4 stages; 3: 16 rows, 3 stages) and the planes a block
- * marches through (1 to 4096; default 32). */
+/* The marching schedule's tile shape (0: 7 rows, 3 stages, two blocks per
+ * SM; 1: 15 rows, 3 stages, one block; 2: 8 rows, 4 stages, one block; 3: 3
+ * rows, 4 stages, three blocks) and the planes a block marches through (1
+ * to 4096; default 32). */
 ems_status ems_gpu_set_march(ems_gpu* h, int shape, uint32_t planes);
 
 /* Picks the fastest in-place schedule (4, 3, 5 or 1) for this model's grid

@@ -88,6 +88,7 @@ struct Block {
     std::vector<double> sums;
     std::atomic<int> errors{0};
     std::atomic<int> orflag{0};
+    std::barrier<>* wbar[32] = {};  // per warp of 32 threads (__syncwarp), where a kernel needs it
     char msg[256] = {0};
 };
 extern Block* cur;
@@ -148,6 +149,7 @@ inline void tensor3d(void* dst, const CUtensorMap* m, int x, int y, int z, uint6
 
 // __syncthreads_or: a barrier that returns whether any thread passed true.
 inline bool sync_or(bool v);
+inline void syncwarp();
 
 // A bounded wait: false after `limit_ns` of wall time (or 200 M polls)
 // without the phase completing, as the device code's waits give up.
@@ -178,6 +180,16 @@ inline double block_sum(double v) {
 }  // namespace emu
 
 inline void __syncthreads() { emu::cur->bar->arrive_and_wait(); }
+
+// __syncwarp: the 32 threads of the caller's warp meet.
+inline void emu::syncwarp() {
+    std::barrier<>* b = cur->wbar[threadIdx.x / 32];
+    if (!b) {
+        fail("__syncwarp without warp barriers");
+        return;
+    }
+    b->arrive_and_wait();
+}
 
 inline bool emu::sync_or(bool v) {
     cur->bar->arrive_and_wait();

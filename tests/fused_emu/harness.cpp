@@ -5,6 +5,8 @@
 // the surrounding tables' sizes (the tests run it under the same sizes).
 #include "emu_shim.h"
 
+#include <memory>
+
 thread_local EmuDim threadIdx;
 EmuDim blockIdx, blockDim, gridDim;
 namespace emu {
@@ -624,8 +626,8 @@ static int march_run(const ems_engine_desc* d, uint64_t steps, float** fields, u
                      uint32_t test_extra_tx = 0, uint64_t wait_ns = 0) {
     g_err[0] = 0;
     for (size_t k = 0; k < d->n_ops; ++k)
-        if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE && d->ops[k].kind != EMS_OP_POLES) {
-            std::snprintf(g_err, sizeof g_err, "only CPML, electric poles and probes are emulated");
+        if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE) {
+            std::snprintf(g_err, sizeof g_err, "only CPML and probes are emulated");
             return 1;
         }
     const std::string why = march_why(d);
@@ -730,8 +732,8 @@ static int march_run(const ems_engine_desc* d, uint64_t steps, float** fields, u
             P.io[a] = buf[cur][3 + a].data();
             P.un[a] = buf[cur ^ 1][a].data();
             P.in[a] = buf[cur ^ 1][3 + a].data();
-            M.u[a] = CUtensorMap{P.uo[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMuW, R + 2, 1}};
-            M.i[a] = CUtensorMap{P.io[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMiW, R + 1, 1}};
+            M.u[a] = CUtensorMap{P.uo[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMW, R + 2, 1}};
+            M.i[a] = CUtensorMap{P.io[a], {g.pitch, g.ny, g.nx}, {g.pitch, (uint64_t)g.ny * g.pitch}, {kMW, R + 1, 1}};
         }
         for (size_t q = 0; q < at_h.size(); ++q) {
             FSlab& f = P.slab[0][at_h[q].first][at_h[q].second];
@@ -747,6 +749,9 @@ static int march_run(const ems_engine_desc* d, uint64_t steps, float** fields, u
                     emu::Block blk;
                     std::barrier<> bar((std::ptrdiff_t)threads);
                     blk.bar = &bar;
+                    std::vector<std::unique_ptr<std::barrier<>>> wbars;
+                    for (unsigned q = 0; q < threads / 32; ++q) wbars.emplace_back(new std::barrier<>(32));
+                    for (unsigned q = 0; q < threads / 32; ++q) blk.wbar[q] = wbars[q].get();
                     blk.smem = sm;
                     blk.smem_bytes = smem_bytes;
                     blk.sums.assign(threads, 0.0);
@@ -786,12 +791,13 @@ static int march_run(const ems_engine_desc* d, uint64_t steps, float** fields, u
 // expects 16 bytes more than its copies deliver; waits give up after
 // `wait_ns`): 3 when the kernel reports the timeout as the engine reads it.
 extern "C" int emu_march_timeout(const ems_engine_desc* d, float** fields, uint64_t wait_ns) {
-    return march_run<8, 3>(d, 1, fields, 4, 16u, wait_ns);
+    return march_run<7, 3>(d, 1, fields, 4, 16u, wait_ns);
 }
 
 extern "C" int emu_march_run(const ems_engine_desc* d, uint64_t steps, float** fields, uint32_t rows, uint32_t planes) {
-    if (rows == 8) return march_run<8, 3>(d, steps, fields, planes);
+    if (rows == 7) return march_run<7, 3>(d, steps, fields, planes);
+    if (rows == 8) return march_run<8, 4>(d, steps, fields, planes);
     if (rows == 3) return march_run<3, 4>(d, steps, fields, planes);
-    std::snprintf(g_err, sizeof g_err, "rows must be 3 or 8");
+    std::snprintf(g_err, sizeof g_err, "rows must be 3, 7 or 8");
     return 1;
 }
