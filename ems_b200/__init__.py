@@ -12,6 +12,7 @@ engine needs a CUDA device and raises if the CUDA library is missing.
 from __future__ import annotations
 
 import ctypes as C
+import cmath
 import math
 import os
 from dataclasses import dataclass
@@ -34,7 +35,7 @@ LORENTZ, DRUDE, DEBYE = 0, 1, 2
 TRAPEZOIDAL, LEAPFROG, OPENEMS_POLES = 0, 1, 2
 GAUSSIAN = 0
 
-OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR, OP_UPML = 1, 2, 3, 4, 5, 6, 7
+OP_CPML, OP_POLES, OP_LUMPED, OP_SOURCE, OP_PROBE, OP_MUR, OP_UPML, OP_SHEET = 1, 2, 3, 4, 5, 6, 7, 8
 # Mur options (MurBoundary::openems_order / openems_corners / count_energy).
 MUR_OPENEMS_ORDER, MUR_OPENEMS_CORNERS, MUR_COUNT_ENERGY = 1, 2, 4
 
@@ -67,6 +68,7 @@ class FreqDumpSpec(C.Structure):
         ("n_freqs", C.c_size_t),
         ("freqs", C.c_void_p),
         ("interval", C.c_uint64),
+        ("sampler", C.c_void_p),
     ]
 
 
@@ -74,7 +76,7 @@ class TimeDumpSpec(C.Structure):
     """``ems_time_dump`` (include/ems_gpu.h)."""
 
     _fields_ = [("field", C.c_int32), ("lo", C.c_uint64 * 3), ("hi", C.c_uint64 * 3), ("stride", C.c_uint64 * 3),
-                ("inv_len", C.c_void_p * 3), ("interval", C.c_uint64)]
+                ("inv_len", C.c_void_p * 3), ("interval", C.c_uint64), ("sampler", C.c_void_p)]
 
 
 class EngineDesc(C.Structure):
@@ -233,6 +235,13 @@ def host_lib() -> C.CDLL:
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
             "ems_model_add_mur": (i, [p, p, p, p, i]),
+            "ems_model_add_sheet": (i, [p, sz, p, p, p, p, p, p, p, d, p, p]),
+            "ems_sheet_layer_profile": (sz, [d, d, d, p, sz]),
+            "ems_sampler_new": (p, [p, i, i, p, p, p]),
+            "ems_sampler_new_indices": (p, [p, i, i, p, p]),
+            "ems_sampler_table": (p, [p]),
+            "ems_sampler_coords": (p, [p, i, p]),
+            "ems_sampler_free": (None, [p]),
             "ems_model_probe_f32": (i, [p, i, i]),
             "ems_model_desc": (p, [p]),
             "ems_dft": (None, [d, d, p, sz, p, sz, p, p]),
@@ -607,6 +616,34 @@ class Model:
         self.ops.append((OP_LUMPED, "port" if port else "lumped"))
         return k
 
+    def add_sheet(self, edges: Sequence[tuple], f_max: float | None = None) -> int:
+        """``ConductingSheet::new(f_max)``, ``push(SheetEdge{..})`` per edge, ``add_to``
+        (src/engine/sheet.rs:529-935): each edge is ``(axis, node, normal, sigma, thickness)``
+        or with ``upper_share=(c, g)`` appended. ``f_max`` None: 1/(10·dt). Sets
+        ``sheet_edges`` / ``sheet_skipped`` (PEC edges and duplicates) of the returned op."""
+        n = len(edges)
+        axis = (C.c_int * max(n, 1))(*[e[0] for e in edges])
+        nodes = _u64([c for e in edges for c in e[1]] or [0])
+        normal = (C.c_int * max(n, 1))(*[e[2] for e in edges])
+        sig = _f64([e[3] for e in edges] or [0.0])
+        th = _f64([e[4] for e in edges] or [0.0])
+        sc = _f64([(e[5][0] if len(e) > 5 and e[5] is not None else -1.0) for e in edges] or [0.0])
+        sg = _f64([(e[5][1] if len(e) > 5 and e[5] is not None else -1.0) for e in edges] or [0.0])
+        inst, skip = C.c_uint64(0), C.c_uint64(0)
+        k = self._check(self._lib.ems_model_add_sheet(self._p, n, axis, nodes, normal, sig, th, sc, sg,
+                                                      0.0 if f_max is None else float(f_max),
+                                                      C.byref(inst), C.byref(skip)), "add_sheet")
+        self.ops.append((OP_SHEET, "sheet"))
+        self.sheet_edges = getattr(self, "sheet_edges", {})
+        self.sheet_edges[k] = (int(inst.value), int(skip.value))
+        return k
+
+    def add_sheet_rect(self, normal: int, plane: int, start: Sequence[int], stop: Sequence[int], sigma: float,
+                       t: float, f_max: float | None = None) -> int:
+        """``ConductingSheet::add_rect`` (src/engine/sheet.rs:573-603) then ``add_to``: every
+        tangential edge of the node rectangle start..=stop on node plane ``plane``."""
+        return self.add_sheet(sheet_rect_edges(normal, plane, start, stop, sigma, t), f_max)
+
     def add_source(self, kind: int, edges: Sequence[tuple[int, Sequence[int], float]], f0: float, fc: float,
                    n_steps: int) -> int:
         """``EdgeSource::new(|t| Gaussian{f0, fc}.value(t)).kind(kind).edge(axis, node, w)...``"""
@@ -863,6 +900,30 @@ class Engine:
         dims = [(hi[a] - lo[a]) // stride[a] + 1 for a in range(3)]
         self._dumps = getattr(self, "_dumps", {})
         self._dumps[i.value] = (dims, len(fr))
+        return i.value
+
+    def add_sampled_freq_dump(self, sampler: "Sampler", freqs, interval: int = 1) -> int:
+        """``FreqDump::new(sampler, freqs).interval(interval)`` (src/engine/dump.rs:1420-1700):
+        a running DFT on the device of the sampler's quantity at its points."""
+        fr = np.ascontiguousarray(freqs, dtype=np.float64)
+        z3 = (C.c_uint64 * 3)(0, 0, 0)
+        spec = FreqDumpSpec(0, z3, z3, z3, (C.c_void_p * 3)(None, None, None), len(fr), fr.ctypes.data, interval,
+                            sampler.table)
+        i = C.c_size_t()
+        self._ck(self._lib.ems_gpu_freq_dump_add(self._h, C.byref(spec), C.byref(i)))
+        self._dumps = getattr(self, "_dumps", {})
+        self._dumps[i.value] = (list(sampler.dims), len(fr))
+        return i.value
+
+    def add_sampled_time_dump(self, sampler: "Sampler", interval: int = 1) -> int:
+        """``TimeDump::new(sampler).schedule(Schedule::Every(interval))`` (src/engine/dump.rs:
+        1230-1418): snapshots of the sampler's quantity kept on the device (f64)."""
+        z3 = (C.c_uint64 * 3)(0, 0, 0)
+        spec = TimeDumpSpec(0, z3, z3, z3, (C.c_void_p * 3)(None, None, None), interval, sampler.table)
+        i = C.c_size_t()
+        self._ck(self._lib.ems_gpu_time_dump_add(self._h, C.byref(spec), C.byref(i)))
+        self._tdumps = getattr(self, "_tdumps", {})
+        self._tdumps[i.value] = list(sampler.dims)
         return i.value
 
     def upml_state(self, op: int, side: int, n: int):
@@ -1129,6 +1190,154 @@ def energy_decay_limits(max_steps: int, db: float, dt: float, excitation_end: fl
     """``RunLimits::new(max).end_criteria(EndCriteria::energy_decay_db(db)).excitation_end(end)``."""
     return RunLimits(max_steps, 1, 10.0 ** (db / 10.0), interval, 1 if excitation_end is not None else 0,
                      excitation_end or 0.0, dt)
+
+
+DUMP_E, DUMP_H, DUMP_J, DUMP_ROTH, DUMP_D, DUMP_B = 0, 1, 2, 3, 4, 5
+NODES, CELL_CENTERS, NATIVE = 0, 1, 2
+DUMP_NAMES = ("E", "H", "J", "RotH", "D", "B")
+
+
+class Sampler:
+    """``FieldSampler`` (src/engine/dump.rs:487-940): ``quantity`` (DUMP_E … DUMP_B)
+    converted to field units and interpolated at the sample points of the node box between
+    corners ``a`` and ``b`` (inclusive, any order) with ``stride``, at ``position`` NODES,
+    CELL_CENTERS or NATIVE; with ``indices`` (three increasing lists) the explicit points
+    and openEMS's rules (``FieldSampler::openems``). The table lives as long as this object."""
+
+    def __init__(self, model: "Model", quantity: int, position: int = NODES, a: Sequence[int] | None = None,
+                 b: Sequence[int] | None = None, stride: Sequence[int] = (1, 1, 1),
+                 indices: Sequence[Sequence[int]] | None = None):
+        self._lib = host_lib()
+        self._model = model
+        self.quantity, self.position = quantity, position
+        if indices is not None:
+            arrs = [np.ascontiguousarray(v, dtype=np.uint64) for v in indices]
+            ptrs = (C.c_void_p * 3)(*[x.ctypes.data for x in arrs])
+            ns = (C.c_size_t * 3)(*[len(x) for x in arrs])
+            h = self._lib.ems_sampler_new_indices(model._p, quantity, position, ptrs, ns)
+        else:
+            n = model.nodes
+            a = [0, 0, 0] if a is None else list(a)
+            b = [x - 1 for x in n] if b is None else list(b)
+            h = self._lib.ems_sampler_new(model._p, quantity, position, _u64(a), _u64(b), _u64(stride))
+        if not h:
+            raise ValueError(f"sampler: {self._lib.ems_model_error(model._p).decode()}")
+        self._h = h
+        self.table = self._lib.ems_sampler_table(h)
+        self.coords = []
+        for ax in range(3):
+            cnt = C.c_size_t()
+            ptr = self._lib.ems_sampler_coords(h, ax, C.byref(cnt))
+            self.coords.append(np.ctypeslib.as_array((C.c_double * cnt.value).from_address(ptr)).copy())
+        self.dims = tuple(len(c) for c in self.coords)
+
+    @property
+    def name(self) -> str:
+        return DUMP_NAMES[self.quantity]
+
+    @property
+    def from_currents(self) -> bool:
+        return self.quantity in (DUMP_H, DUMP_B, DUMP_ROTH)
+
+    def __len__(self) -> int:
+        return int(np.prod(self.dims))
+
+    def time(self, state: int, dt: float) -> float:
+        """``FieldSampler::time`` with ``DumpTiming::State`` (dump.rs:786-812)."""
+        return (state - 0.5 if self.from_currents else float(state)) * dt
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.ems_sampler_free(h)
+            self._h = None
+
+
+def sheet_rect_edges(normal: int, plane: int, start: Sequence[int], stop: Sequence[int], sigma: float,
+                     t: float) -> list[tuple]:
+    """The edges ``ConductingSheet::add_rect`` pushes (src/engine/sheet.rs:573-603): for
+    (d, o) in ((next, prev), (prev, next)) of the normal, d from start to stop − 1 and o
+    from start to stop, on node plane ``plane``."""
+    p, q = (normal + 1) % 3, (normal + 2) % 3
+    out = []
+    for d, o in ((p, q), (q, p)):
+        for a in range(start[d], stop[d]):
+            for b in range(start[o], stop[o] + 1):
+                node = [0, 0, 0]
+                node[normal], node[d], node[o] = plane, a, b
+                out.append((d, tuple(node), normal, sigma, t))
+    return out
+
+
+def skin_depth(sigma: float, f: float) -> float:
+    """``skin_depth`` (src/engine/sheet.rs:237-239): √(2/(ω·μ0·σ))."""
+    return math.sqrt(2.0 / (2.0 * math.pi * f * mu0() * sigma))
+
+
+def layer_profile(sigma: float, thickness: float, f_max: float) -> np.ndarray:
+    """``layer_profile`` (src/engine/sheet.rs:244-271), from the host library."""
+    L = host_lib()
+    n = L.ems_sheet_layer_profile(sigma, thickness, f_max, None, 0)
+    out = np.zeros(max(n, 1))
+    L.ems_sheet_layer_profile(sigma, thickness, f_max, out.ctypes.data, len(out))
+    return out[:n]
+
+
+def _coth_csch(x: complex) -> tuple[complex, complex]:
+    e1 = cmath.exp(-x)
+    e2 = e1 * e1
+    den = 1.0 - e2
+    return (1.0 + e2) / den, e1 * 2.0 / den
+
+
+def _csqrt(z: complex) -> complex:
+    r, a = cmath.polar(z)
+    return cmath.rect(math.sqrt(r), 0.5 * a)
+
+
+def slab_impedance(sigma: float, t: float, f: float) -> tuple[complex, complex]:
+    """``slab_impedance`` (src/engine/sheet.rs:288-298): [Z11, Z12] per square of the exact
+    slab, Z_c·coth(γt) and Z_c·csch(γt)."""
+    w = 2.0 * math.pi * f
+    y = complex(sigma, w * eps0())
+    jwm = complex(0.0, w * mu0())
+    gamma = _csqrt(jwm * y)
+    zc = _csqrt(jwm / y)
+    coth, csch = _coth_csch(gamma * t)
+    return zc * coth, zc * csch
+
+
+def _z_to_abcd(z11: complex, z12: complex) -> list[complex]:
+    a = z11 / z12
+    return [a, (z11 * z11 - z12 * z12) / z12, 1.0 / z12, a]
+
+
+def slab_abcd(sigma: float, t: float, f: float) -> list[complex]:
+    """``slab_abcd`` (src/engine/sheet.rs:300-303): the exact slab's chain matrix."""
+    return _z_to_abcd(*slab_impedance(sigma, t, f))
+
+
+def model_abcd(sigma: float, t: float, f_max: float, f: float) -> list[complex]:
+    """``model_abcd`` (src/engine/sheet.rs:313-345): the chain matrix of the ladder the
+    operator integrates (continuous time), shunt half layers at the ends."""
+    w = 2.0 * math.pi * f
+    dz = layer_profile(sigma, t, f_max)
+
+    def mul(m, n):
+        return [m[0] * n[0] + m[1] * n[2], m[0] * n[1] + m[1] * n[3],
+                m[2] * n[0] + m[3] * n[2], m[2] * n[1] + m[3] * n[3]]
+
+    def shunt(v):
+        return [1.0 + 0j, 0j, complex(sigma * v, w * eps0() * v), 1.0 + 0j]
+
+    def series(ln):
+        return [1.0 + 0j, complex(0.0, w * mu0() * ln), 0j, 1.0 + 0j]
+
+    m = shunt(0.5 * dz[0])
+    for k, d in enumerate(dz):
+        m = mul(m, series(d))
+        m = mul(m, shunt(0.5 * (d + (dz[k + 1] if k + 1 < len(dz) else 0.0))))
+    return m
 
 
 def dft(t0: float, dt: float, x: np.ndarray, freqs: Sequence[float]) -> np.ndarray:

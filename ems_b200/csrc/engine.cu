@@ -35,6 +35,7 @@
 #include "interior.cuh"
 #include "march.cuh"
 #include "batch.cuh"
+#include "sheet.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -131,6 +132,8 @@ struct ems_gpu {
         MurDevT mur;
         bool mur_energy = false;
         UpmlSideDev upml[2];  // openEMS PML layers: E, H
+        SheetDevT sheet;
+        size_t sheet_nodes = 0, sheet_layers = 0;
     };
     std::vector<Op> ops;
     // Frequency-domain dumps (ems_gpu_freq_dump_add).
@@ -584,15 +587,16 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         ems_status st = build_chunks(h, S);
         if (st) return st;
     }
-    // The sweep needs no magnetic sources (their serial hook would sit
-    // between a chunk's H and E updates) and no openEMS PML layers (their
-    // hooks are not cut into chunks).
+    // The sweep needs no magnetic sources or conducting sheets (their serial
+    // post_h hooks would sit between a chunk's H and E updates) and no
+    // openEMS PML layers (their hooks are not cut into chunks).
     h->sweep_ok = true;
     for (size_t k = 0; k < d->n_ops; ++k) {
         if (d->ops[k].kind == EMS_OP_SOURCE) {
             const auto* sr = (const ems_source*)d->ops[k].table;
             if (sr->kind == EMS_SOFT_H || sr->kind == EMS_HARD_H) h->sweep_ok = false;
         }
+        if (d->ops[k].kind == EMS_OP_SHEET) h->sweep_ok = false;
         if (d->ops[k].kind == EMS_OP_UPML) {
             h->sweep_ok = false;
             if (h->fused_why.empty()) h->fused_why = "openEMS PML layers";
@@ -1335,7 +1339,115 @@ ems_status run_step(ems_gpu* h, bool energy) {
     return EMS_OK;
 }
 
-// Serial post_h hooks in registration order: magnetic sources, current probes.
+// Uploads a conducting-sheet table (include/ems_gpu.h, ems_sheet) after
+// checking every index it holds, and builds the post_h table: per dual
+// edge with a nonzero correction, the (edge, corr) pairs in edge order.
+ems_status setup_sheet(ems_gpu* h, const ems_sheet* t, ems_gpu::Op& op) {
+    auto fail = [](const char* why) {
+        std::fprintf(stderr, "ems_gpu: conducting sheet: %s\n", why);
+        return EMS_ERR_INVALID;
+    };
+    const Grid& g = h->g;
+    const size_t ne = t->n_edges, nc = t->n_couplings;
+    if (ne >= (1ull << 31) || nc >= (1ull << 31) || t->n_konst >= (1ull << 31) || t->n_a >= (1ull << 31))
+        return fail("table too large");
+    if (ne && (!t->axis || !t->node || !t->nn || !t->konst0 || !t->a0 || !t->coupling_end || !t->c_edge))
+        return fail("missing arrays");
+    if (nc && (!t->c_axis || !t->c_node || !t->w_up || !t->w_dn || !t->corr || !t->ecorr)) return fail("missing arrays");
+    if ((t->n_konst && (!t->two_c || !t->cp || !t->inv_den)) || (t->n_a && !t->a)) return fail("missing arrays");
+    std::vector<uint32_t> node(ne), n0(ne), l0(ne), c0(ne + 1, 0), cnode(nc);
+    std::vector<uint64_t> keys(ne);
+    uint64_t nodes_total = 0, layers_total = 0;
+    uint32_t c = 0;
+    for (size_t e = 0; e < ne; ++e) {
+        const uint32_t nn = t->nn[e], end = t->coupling_end[e];
+        if (t->axis[e] > 2 || t->node[e] >= g.n || nn < 2 || end < c || end > nc ||
+            (uint64_t)t->konst0[e] + nn > t->n_konst || (uint64_t)t->a0[e] + nn - 1 > t->n_a)
+            return fail("edge entry out of range");
+        node[e] = dev_index(g, t->node[e]);
+        keys[e] = t->node[e] * 3 + t->axis[e];
+        n0[e] = (uint32_t)nodes_total;
+        l0[e] = (uint32_t)layers_total;
+        nodes_total += nn;
+        layers_total += nn - 1;
+        if (nodes_total >= (1ull << 31)) return fail("ladders too large");
+        c = end;
+        c0[e + 1] = end;
+    }
+    if (c != nc) return fail("couplings not covered by the edges");
+    // Each sheet edge is written by one thread of post_e: no edge twice.
+    std::sort(keys.begin(), keys.end());
+    if (std::adjacent_find(keys.begin(), keys.end()) != keys.end()) return fail("an edge listed twice");
+    std::unordered_map<uint64_t, uint32_t> tix;
+    std::vector<std::vector<std::pair<uint32_t, double>>> tlist;
+    std::vector<uint8_t> taxis;
+    std::vector<uint32_t> tnode;
+    for (size_t e = 0; e < ne; ++e)
+        for (uint32_t q = c0[e]; q < c0[e + 1]; ++q) {
+            if (t->c_axis[q] > 2 || t->c_node[q] >= g.n) return fail("coupling out of range");
+            cnode[q] = dev_index(g, t->c_node[q]);
+            if (t->corr[q] == 0.0) continue;
+            const uint64_t key = t->c_node[q] * 3 + t->c_axis[q];
+            auto it = tix.find(key);
+            if (it == tix.end()) {
+                it = tix.emplace(key, (uint32_t)tlist.size()).first;
+                tlist.emplace_back();
+                taxis.push_back(t->c_axis[q]);
+                tnode.push_back(cnode[q]);
+            }
+            tlist[it->second].emplace_back((uint32_t)e, t->corr[q]);
+        }
+    std::vector<uint32_t> t0(1, 0), tedge;
+    std::vector<double> tcorr;
+    for (const auto& l : tlist) {
+        for (const auto& [e, k] : l) {
+            tedge.push_back(e);
+            tcorr.push_back(k);
+        }
+        t0.push_back((uint32_t)tedge.size());
+    }
+    SheetDevT& D = op.sheet;
+    D.n_edges = (uint32_t)ne;
+    D.n_targets = (uint32_t)tlist.size();
+    op.sheet_nodes = nodes_total;
+    op.sheet_layers = layers_total;
+    if (!ne) return EMS_OK;
+    D.axis = h->upload(t->axis, ne);
+    D.node = h->upload(node.data(), ne);
+    D.nn = h->upload(t->nn, ne);
+    D.k0 = h->upload(t->konst0, ne);
+    D.a0 = h->upload(t->a0, ne);
+    D.n0 = h->upload(n0.data(), ne);
+    D.l0 = h->upload(l0.data(), ne);
+    D.c0 = h->upload(c0.data(), ne + 1);
+    D.c_edge = h->upload(t->c_edge, ne);
+    D.c_axis = h->upload(t->c_axis, nc);
+    D.c_node = h->upload(cnode.data(), nc);
+    D.w_up = h->upload(t->w_up, nc);
+    D.w_dn = h->upload(t->w_dn, nc);
+    D.ecorr = h->upload(t->ecorr, nc);
+    D.two_c = h->upload(t->two_c, t->n_konst);
+    D.cp = h->upload(t->cp, t->n_konst);
+    D.inv_den = h->upload(t->inv_den, t->n_konst);
+    D.a = h->upload(t->a, t->n_a);
+    D.u = h->alloc<double>(nodes_total);
+    D.h = h->alloc<double>(layers_total);
+    D.x = h->alloc<double>(nodes_total);
+    D.wcorr = h->alloc<double>(ne);
+    D.t_axis = h->upload(taxis.data(), taxis.size());
+    D.t_node = h->upload(tnode.data(), tnode.size());
+    D.t0 = h->upload(t0.data(), t0.size());
+    D.t_edge = h->upload(tedge.data(), tedge.size());
+    D.t_corr = h->upload(tcorr.data(), tcorr.size());
+    if (!D.axis || !D.node || !D.nn || !D.k0 || !D.a0 || !D.n0 || !D.l0 || !D.c0 || !D.c_edge || !D.c_axis ||
+        !D.c_node || !D.w_up || !D.w_dn || !D.ecorr || !D.two_c || !D.cp || !D.inv_den || !D.a || !D.u || !D.h ||
+        !D.x || !D.wcorr || !D.t_axis || !D.t_node || !D.t0 || !D.t_edge || !D.t_corr)
+        return EMS_ERR_NOMEM;
+    return EMS_OK;
+}
+
+// Serial post_h hooks in registration order: magnetic sources, conducting
+// sheets, current probes.
 ems_status serial_post_h(ems_gpu* h, const Fields& f) {
     cudaStream_t s = h->stream;
     for (auto& op : h->ops) {
@@ -1345,6 +1457,11 @@ ems_status serial_post_h(ems_gpu* h, const Fields& f) {
             bool hard = sd.kind == EMS_HARD_H;
             if (!hard && a == 0.0f) continue;
             k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.i[0], f.i[1], f.i[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_SHEET && op.sheet.n_edges) {
+            const SheetDevT& sd = op.sheet;
+            k_sheet_post_h<<<blocks_for(sd.n_targets + sd.n_edges, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], f.i[0],
+                                                                                      f.i[1], f.i[2], sd);
             ++h->launches;
         } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_CURRENT && h->step % op.probe.interval == 0) {
             ems_gpu::ProbeDev& p = op.probe;
@@ -1373,7 +1490,7 @@ ems_status serial_pre_e(ems_gpu* h, const Fields& f) {
 }
 
 // Serial post_e hooks in registration order: lumped elements, Mur
-// boundaries, electric sources, voltage probes.
+// boundaries, electric sources, conducting sheets, voltage probes.
 ems_status serial_post_e(ems_gpu* h, const Fields& f) {
     cudaStream_t s = h->stream;
     for (auto& op : h->ops) {
@@ -1414,6 +1531,10 @@ ems_status serial_post_e(ems_gpu* h, const Fields& f) {
             bool hard = sd.kind == EMS_HARD_E;
             if (!hard && a == 0.0f) continue;
             k_source<<<blocks_for(sd.n, 256), 256, 0, s>>>(f.u[0], f.u[1], f.u[2], sd.axis, sd.node, sd.weight, sd.n, a, hard);
+            ++h->launches;
+        } else if (op.kind == EMS_OP_SHEET && op.sheet.n_edges) {
+            const SheetDevT& sd = op.sheet;
+            k_sheet_post_e<<<blocks_for(sd.n_edges, 128), 128, 0, s>>>(f.u[0], f.u[1], f.u[2], f.i[0], f.i[1], f.i[2], sd);
             ++h->launches;
         } else if (op.kind == EMS_OP_PROBE && op.probe.quantity == EMS_PROBE_VOLTAGE && h->step % op.probe.interval == 0) {
             ems_gpu::ProbeDev& p = op.probe;
@@ -1687,6 +1808,11 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
             }
             break;
         }
+        case EMS_OP_SHEET: {
+            ems_status st = setup_sheet(h.get(), (const ems_sheet*)t, op);
+            if (st) return st;
+            break;
+        }
         default:
             return EMS_ERR_INVALID;
         }
@@ -1825,8 +1951,56 @@ ems_status ems_gpu_run(ems_gpu* h, uint64_t n) {
     return check(h, cudaGetLastError(), "run");
 }
 
+// A sampler's table into a dump (include/ems_gpu.h, ems_sampler): every tap
+// of nonzero weight must lie in the grid and in the factor box, the factor
+// box in the grid. Sets the dump's points and field (1: i, 0: u).
+static ems_status dump_sampler(ems_gpu* h, const ems_sampler* sp, DumpDev& d, int* field, uint64_t* npts) {
+    const Grid& g = h->g;
+    const uint64_t nn[3] = {g.nx, g.ny, g.nz};
+    if (sp->quantity < EMS_DUMP_E || sp->quantity > EMS_DUMP_B || !sp->tap_idx || !sp->tap_w)
+        return fail(h, EMS_ERR_INVALID, "sampler: invalid table");
+    uint64_t n = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (!sp->dims[a] || sp->dims[a] >= (1u << 30)) return fail(h, EMS_ERR_INVALID, "sampler: invalid dims");
+        n *= sp->dims[a];
+        if (n >= (1ull << 31)) return fail(h, EMS_ERR_INVALID, "sampler: too many points");
+        if (sp->factors && (!sp->fac_dims[a] || sp->fac_lo[a] + sp->fac_dims[a] > nn[a]))
+            return fail(h, EMS_ERR_INVALID, "sampler: factor box outside the grid");
+    }
+    const uint64_t off[3] = {0, 3 * sp->dims[0], 3 * (sp->dims[0] + sp->dims[1])};
+    const uint64_t taps = 2 * 3 * (sp->dims[0] + sp->dims[1] + sp->dims[2]);
+    for (int a = 0; a < 3; ++a)
+        for (uint64_t q = 2 * off[a]; q < 2 * (off[a] + 3 * sp->dims[a]); ++q) {
+            if (sp->tap_w[q] == 0.0) continue;
+            const uint64_t x = sp->tap_idx[q];
+            if (x >= nn[a] || (sp->factors && (x < sp->fac_lo[a] || x >= sp->fac_lo[a] + sp->fac_dims[a])))
+                return fail(h, EMS_ERR_INVALID, "sampler: a tap outside the grid or the factor box");
+        }
+    const uint64_t vol = sp->factors ? sp->fac_dims[0] * sp->fac_dims[1] * sp->fac_dims[2] : 0;
+    if (vol >= (1ull << 31)) return fail(h, EMS_ERR_INVALID, "sampler: factor box too large");
+    d.samp = 1;
+    d.roth = sp->quantity == EMS_DUMP_ROTH;
+    for (int a = 0; a < 3; ++a) {
+        d.n[a] = (uint32_t)sp->dims[a];
+        d.off[a] = (uint32_t)off[a];
+        d.flo[a] = (uint32_t)sp->fac_lo[a];
+        d.fdim[a] = (uint32_t)sp->fac_dims[a];
+        d.lo[a] = 0;
+        d.st[a] = 1;
+        d.inv_len[a] = nullptr;
+    }
+    d.tidx = h->upload(sp->tap_idx, taps);
+    d.tw = h->upload(sp->tap_w, taps);
+    d.fac = sp->factors ? h->upload(sp->factors, 3 * vol) : nullptr;
+    if (!d.tidx || !d.tw || (sp->factors && !d.fac)) return fail(h, EMS_ERR_NOMEM, "sampler");
+    *field = (sp->quantity == EMS_DUMP_H || sp->quantity == EMS_DUMP_B || sp->quantity == EMS_DUMP_ROTH) ? 1 : 0;
+    *npts = n;
+    return EMS_OK;
+}
+
 ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* id) {
-    if (!h || !spec || !id || spec->field < 0 || spec->field > 1 || !spec->freqs || !spec->n_freqs) return EMS_ERR_INVALID;
+    if (!h || !spec || !id || !spec->freqs || !spec->n_freqs) return EMS_ERR_INVALID;
+    if (!spec->sampler && (spec->field < 0 || spec->field > 1)) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     const Grid& g = h->g;
     const uint32_t nn[3] = {g.nx, g.ny, g.nz};
@@ -1834,7 +2008,12 @@ ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* 
     DumpDev& d = D.d;
     d = DumpDev{};
     uint64_t npts = 1;
-    for (int a = 0; a < 3; ++a) {
+    int field = spec->field;
+    if (spec->sampler) {
+        ems_status st = dump_sampler(h, spec->sampler, d, &field, &npts);
+        if (st) return st;
+    }
+    for (int a = 0; a < 3 && !spec->sampler; ++a) {
         const uint64_t st = spec->stride[a] ? spec->stride[a] : 1;
         if (spec->lo[a] > spec->hi[a] || spec->hi[a] >= nn[a] || !spec->inv_len[a]) return EMS_ERR_INVALID;
         d.lo[a] = (uint32_t)spec->lo[a];
@@ -1851,10 +2030,10 @@ ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* 
     d.nf = (uint32_t)spec->n_freqs;
     d.freqs = h->upload(spec->freqs, spec->n_freqs);
     d.dt = h->dt;
-    d.t0 = spec->field ? -0.5 * h->dt : 0.0;
+    d.t0 = field ? -0.5 * h->dt : 0.0;
     d.acc = h->alloc<double>(npts * spec->n_freqs * 6);
     if (!d.freqs || !d.acc) return fail(h, EMS_ERR_NOMEM, "dump");
-    D.field = spec->field;
+    D.field = field;
     D.interval = spec->interval ? spec->interval : 1;
     h->dumps.push_back(D);
     *id = h->dumps.size() - 1;
@@ -1862,7 +2041,8 @@ ems_status ems_gpu_freq_dump_add(ems_gpu* h, const ems_freq_dump* spec, size_t* 
 }
 
 ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* id) {
-    if (!h || !spec || !id || spec->field < 0 || spec->field > 1) return EMS_ERR_INVALID;
+    if (!h || !spec || !id) return EMS_ERR_INVALID;
+    if (!spec->sampler && (spec->field < 0 || spec->field > 1)) return EMS_ERR_INVALID;
     cudaSetDevice(h->device);
     const Grid& g = h->g;
     const uint32_t nn[3] = {g.nx, g.ny, g.nz};
@@ -1870,7 +2050,12 @@ ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* 
     DumpDev& d = T.d;
     d = DumpDev{};
     uint64_t npts = 1;
-    for (int a = 0; a < 3; ++a) {
+    int field = spec->field;
+    if (spec->sampler) {
+        ems_status st = dump_sampler(h, spec->sampler, d, &field, &npts);
+        if (st) return st;
+    }
+    for (int a = 0; a < 3 && !spec->sampler; ++a) {
         const uint64_t st = spec->stride[a] ? spec->stride[a] : 1;
         if (spec->lo[a] > spec->hi[a] || spec->hi[a] >= nn[a] || !spec->inv_len[a]) return EMS_ERR_INVALID;
         d.lo[a] = (uint32_t)spec->lo[a];
@@ -1884,7 +2069,7 @@ ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* 
     d.pitch = g.pitch;
     d.ny = g.ny;
     d.npts = (uint32_t)npts;
-    T.field = spec->field;
+    T.field = field;
     T.interval = spec->interval ? spec->interval : 1;
     h->tdumps.push_back(std::move(T));
     *id = h->tdumps.size() - 1;
@@ -2012,6 +2197,9 @@ ems_status ems_gpu_step_with_energy(ems_gpu* h, double* energy) {
         } else if (op.kind == EMS_OP_MUR && op.mur_energy) {
             k_mur_energy<<<1, 1024, 0, h->stream>>>(op.mur, h->d_energy + 1);
             ++h->launches;
+        } else if (op.kind == EMS_OP_SHEET && op.sheet.n_edges) {
+            k_sheet_energy<<<1, 1024, 0, h->stream>>>(op.sheet, h->dt, h->d_energy + 1);
+            ++h->launches;
         } else {
             continue;
         }
@@ -2080,6 +2268,9 @@ ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t
         if (which > 0 && !o.lumped.columns) return EMS_ERR_INVALID;
         src = which == 0 ? o.lumped.rec : (which == 1 ? o.lumped.pv : o.lumped.pi);
         cnt = o.lumped.count;
+    } else if (o.kind == EMS_OP_SHEET && (which == 0 || which == 1)) {
+        src = which == 0 ? o.sheet.u : o.sheet.h;
+        cnt = which == 0 ? o.sheet_nodes : o.sheet_layers;
     } else {
         return fail(h, EMS_ERR_INVALID, "no such series");
     }
@@ -2170,7 +2361,7 @@ ems_status ems_gpu_set_schedule(ems_gpu* h, int schedule) {
     if (schedule == 3 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "two-kernel schedule unavailable: " + h->tables_why);
     if (schedule == 4 && !h->tables_ok) return fail(h, EMS_ERR_INVALID, "split schedule unavailable: " + h->tables_why);
     if (schedule == 5 && !(h->tables_ok && h->sweep_ok))
-        return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources") : h->tables_why));
+        return fail(h, EMS_ERR_INVALID, "sweep schedule unavailable: " + (h->tables_ok ? std::string("magnetic sources, conducting sheets or openEMS PML layers") : h->tables_why));
     if (schedule == 6 && !(h->tables_ok && h->interior_why.empty()))
         return fail(h, EMS_ERR_INVALID, "interior schedule unavailable: " + (h->tables_ok ? h->interior_why : h->tables_why));
     if (schedule == 7 && !(h->tables_ok && h->march_why.empty()))
@@ -2426,6 +2617,7 @@ std::string batch_ineligible(const ems_engine_desc* d) {
             else ph = 1;
         }
         if (kind == EMS_OP_MUR) return "Mur boundaries";
+        if (kind == EMS_OP_SHEET) return "conducting sheets";
         if (kind == EMS_OP_UPML) return "openEMS PML layers";
         if (pe >= 0) {
             if (pe < phase_e) return "post_e hooks not in the order lumped, E sources, voltage probes";

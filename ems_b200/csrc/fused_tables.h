@@ -181,6 +181,7 @@ inline std::string fused_ineligible(const ems_engine_desc* d, uint32_t pitch) {
             const auto* s = (const ems_source*)d->ops[k].table;
             if (s->kind == EMS_SOFT_H || s->kind == EMS_HARD_H) return "magnetic sources";
         }
+        if (kind == EMS_OP_SHEET) return "conducting sheets";
     }
     if (pitch > 1024) return "z rows longer than 1024 nodes";
     return "";

@@ -13,6 +13,7 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <numeric>
 #include <tuple>
 #include <string>
 #include <thread>
@@ -131,6 +132,12 @@ struct OpStore {
     std::vector<uint64_t> pnode[2];
     std::vector<float> pco[2];
     ems_upml upml{};
+    // conducting sheets
+    std::vector<uint8_t> sax, cax;
+    std::vector<uint64_t> snode, cnode;
+    std::vector<uint32_t> snn, sk0, sa0, send;
+    std::vector<double> scedge, cwup, cwdn, ccorr, cecorr, two_c, cp, inv_den, sa;
+    ems_sheet sheet{};
 };
 
 }  // namespace
@@ -241,6 +248,7 @@ struct ems_model {
             case EMS_OP_SOURCE: e.table = &o->source; break;
             case EMS_OP_MUR: e.table = &o->mur; break;
             case EMS_OP_UPML: e.table = &o->upml; break;
+            case EMS_OP_SHEET: e.table = &o->sheet; break;
             default: e.table = &o->probe; break;
             }
             op_list.push_back(e);
@@ -1717,6 +1725,472 @@ int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6],
     M.cap = M.count_energy ? op->mcap.data() : nullptr;
     M.openems_order = (flags & 1) ? 1 : 0;
     M.openems_corners = (flags & 2) ? 1 : 0;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Field samplers (src/engine/dump.rs:281-760).
+
+struct ems_sampler_host {
+    ems_sampler t{};
+    std::vector<uint32_t> idx;
+    std::vector<double> w, fac, coords[3];
+};
+
+namespace {
+
+// A sample position along one axis (dump.rs:291-303): node j, centre of
+// cell j (j = n - 1: the virtual cell beyond the last node), raw node j.
+enum class Pos { Node, Mid, Raw };
+struct PosJ {
+    Pos k;
+    uint64_t j;
+};
+struct Tap2 {
+    uint64_t i[2];
+    double w[2];
+};
+
+// dual_coord (dump.rs:305-317).
+double dual_coord(const ems_model* m, int a, uint64_t j) {
+    const auto& l = m->lines[a];
+    const uint64_t n = l.size();
+    if (j + 1 < n) return 0.5 * (l[j] + l[j + 1]);
+    if (n >= 2) return l[n - 1] + 0.5 * (l[n - 1] - l[n - 2]);
+    return l[n - 1];
+}
+
+// oe_dual (dump.rs:319-329): the dual length with full outer cells.
+double oe_dual(const ems_model* m, int a, uint64_t j) {
+    const uint64_t n = m->n[a];
+    const double d = m->dual_delta(a, j);
+    return (n >= 2 && (j == 0 || j == n - 1)) ? 2.0 * d : d;
+}
+
+// taps (dump.rs:331-433), Cartesian grids.
+Tap2 sampler_taps(const ems_model* m, bool dual, int comp, int a, PosJ pos, bool oe) {
+    const uint64_t n = m->n[a];
+    auto d = [&](uint64_t i) { return m->delta(a, i); };
+    auto one = [](uint64_t i, double w) { return Tap2{{i, i}, {w, 0.0}}; };
+    const Tap2 zero{{0, 0}, {0.0, 0.0}};
+    if (n < 2) return (!dual && comp == a) ? zero : one(0, 1.0);
+    auto lin = [&](uint64_t j) {
+        if (j == 0) return one(0, 1.0);
+        if (j == n - 1) return one(n - 2, 1.0);
+        const double dl = d(j - 1), dh = d(j);
+        return Tap2{{j - 1, j}, {dh / (dl + dh), dl / (dl + dh)}};
+    };
+    const uint64_t j = pos.j;
+    if (pos.k == Pos::Mid && j + 1 >= n) return zero;
+    const bool own = comp == a;
+    if (!dual && own) {
+        if (pos.k == Pos::Node) {
+            Tap2 t = lin(j);
+            t.w[0] = t.w[0] / d(t.i[0]);
+            t.w[1] = t.w[1] / d(t.i[1]);
+            return t;
+        }
+        if (pos.k == Pos::Mid) return one(j, 1.0 / d(j));
+        return j + 1 < n ? one(j, 1.0 / d(j)) : zero;
+    }
+    if (!dual) {
+        if (pos.k == Pos::Mid) return Tap2{{j, j + 1}, {0.5, 0.5}};
+        return one(j, 1.0);
+    }
+    if (own) {
+        if (pos.k != Pos::Mid) return one(j, 1.0 / m->dual_delta(a, j));
+        if (oe) {
+            const double x = oe_dual(m, a, j), y = oe_dual(m, a, j + 1);
+            return Tap2{{j, j + 1}, {y / (x + y) / m->dual_delta(a, j), x / (x + y) / m->dual_delta(a, j + 1)}};
+        }
+        return Tap2{{j, j + 1}, {0.5 / m->dual_delta(a, j), 0.5 / m->dual_delta(a, j + 1)}};
+    }
+    if (pos.k == Pos::Node) {
+        if (oe) return (j == 0 || j == n - 1) ? zero : Tap2{{j - 1, j}, {0.5, 0.5}};
+        return lin(j);
+    }
+    return one(j, 1.0);
+}
+
+ems_sampler_host* sampler_build(ems_model* m, int q, const std::vector<PosJ> pos[3], bool oe) {
+    const bool dual = q == EMS_DUMP_H || q == EMS_DUMP_B;
+    auto s = std::make_unique<ems_sampler_host>();
+    for (int a = 0; a < 3; ++a)
+        for (const PosJ& p : pos[a]) {
+            double c;
+            if (p.k == Pos::Node || (p.k == Pos::Raw && !dual)) c = m->lines[a][p.j];
+            else c = dual_coord(m, a, p.j);
+            s->coords[a].push_back(c);
+        }
+    const uint64_t dims[3] = {pos[0].size(), pos[1].size(), pos[2].size()};
+    const uint64_t off[3] = {0, 3 * dims[0], 3 * (dims[0] + dims[1])};
+    const uint64_t total = 3 * (dims[0] + dims[1] + dims[2]);
+    s->idx.assign(2 * total, 0);
+    s->w.assign(2 * total, 0.0);
+    uint64_t lo[3] = {UINT64_MAX, UINT64_MAX, UINT64_MAX}, hi[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (uint64_t k = 0; k < dims[a]; ++k) {
+                const Tap2 t = sampler_taps(m, dual, c, a, pos[a][k], oe);
+                const uint64_t e = 2 * (off[a] + (uint64_t)c * dims[a] + k);
+                for (int u = 0; u < 2; ++u) {
+                    s->idx[e + u] = (uint32_t)t.i[u];
+                    s->w[e + u] = t.w[u];
+                    if (t.w[u] != 0.0) {
+                        lo[a] = std::min(lo[a], t.i[u]);
+                        hi[a] = std::max(hi[a], t.i[u]);
+                    }
+                }
+            }
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] > hi[a]) lo[a] = hi[a] = 0;
+    ems_sampler& T = s->t;
+    T.quantity = q;
+    for (int a = 0; a < 3; ++a) {
+        T.dims[a] = dims[a];
+        T.fac_lo[a] = lo[a];
+        T.fac_dims[a] = hi[a] - lo[a] + 1;
+    }
+    T.tap_idx = s->idx.data();
+    T.tap_w = s->w.data();
+    T.factors = nullptr;
+    // Factors (dump.rs:626-660 rot H, 700-750 prepare): per component over
+    // the tap box, z fastest.
+    if (q == EMS_DUMP_ROTH || q == EMS_DUMP_J || q == EMS_DUMP_D || q == EMS_DUMP_B) {
+        const uint64_t vol = T.fac_dims[0] * T.fac_dims[1] * T.fac_dims[2];
+        s->fac.assign(3 * vol, 0.0);
+        const double dt = m->dt;
+        for (int c = 0; c < 3; ++c) {
+            const int ob = next_axis(c), oc = prev_axis(c);
+            uint64_t at = (uint64_t)c * vol;
+            for (uint64_t i = lo[0]; i <= hi[0]; ++i)
+                for (uint64_t j = lo[1]; j <= hi[1]; ++j)
+                    for (uint64_t k = lo[2]; k <= hi[2]; ++k, ++at) {
+                        const uint64_t p[3] = {i, j, k};
+                        const uint64_t idx = m->index(i, j, k);
+                        double f = 0.0;
+                        if (q == EMS_DUMP_ROTH) {
+                            if (p[c] + 1 < m->n[c]) {
+                                double area = m->dual_delta(ob, p[ob]) * m->dual_delta(oc, p[oc]);
+                                if (oe)
+                                    for (int t : {ob, oc})
+                                        if (m->n[t] >= 2 && (p[t] == 0 || p[t] == m->n[t] - 1)) area *= 2.0;
+                                f = area > 0.0 ? m->delta(c, p[c]) / area : 0.0;
+                            }
+                        } else if (q == EMS_DUMP_B) {
+                            if (p[ob] + 1 < m->n[ob] && p[oc] + 1 < m->n[oc]) {
+                                const float da = m->co[6 + c][idx], db = m->co[9 + c][idx];
+                                const double area = m->delta(ob, p[ob]) * m->delta(oc, p[oc]);
+                                if (db != 0.0f && area > 0.0) {
+                                    const double l = dt * (1.0 + (double)da) / (2.0 * (double)db);
+                                    f = l * m->dual_delta(c, p[c]) / area;
+                                }
+                            }
+                        } else if (p[c] + 1 < m->n[c]) {
+                            const float ca = m->co[c][idx], cb = m->co[3 + c][idx];
+                            const double area = m->dual_delta(ob, p[ob]) * m->dual_delta(oc, p[oc]);
+                            if (cb != 0.0f && area > 0.0) {
+                                const double a = (double)ca, b = (double)cb;
+                                const double v = q == EMS_DUMP_D ? dt * (1.0 + a) / (2.0 * b) : (1.0 - a) / b;
+                                f = v * m->delta(c, p[c]) / area;
+                            }
+                        }
+                        s->fac[at] = f;
+                    }
+        }
+        T.factors = s->fac.data();
+    }
+    return s.release();
+}
+
+}  // namespace
+
+ems_sampler_host* ems_sampler_new(ems_model* m, int quantity, int position, const uint64_t a[3], const uint64_t b[3],
+                                  const uint64_t stride[3]) {
+    if (quantity < EMS_DUMP_E || quantity > EMS_DUMP_B || position < 0 || position > 2)
+        return set_err(m, "sampler: invalid quantity or position"), nullptr;
+    if ((quantity == EMS_DUMP_J || quantity == EMS_DUMP_D || quantity == EMS_DUMP_B) && !m->built)
+        return set_err(m, "sampler: J, D and B need the built model's coefficients"), nullptr;
+    std::vector<PosJ> pos[3];
+    for (int x = 0; x < 3; ++x) {
+        const uint64_t lo = std::min(a[x], b[x]), hi = std::max(a[x], b[x]);
+        const uint64_t st = (stride && stride[x]) ? stride[x] : 1;
+        // DumpRegion::check_fits (dump.rs:210-225).
+        if (hi >= m->n[x]) return set_err(m, "dump box exceeds the grid"), nullptr;
+        if (position == 1 && hi > lo) {
+            for (uint64_t j = lo; j < hi; j += st) pos[x].push_back({Pos::Mid, j});
+        } else {
+            for (uint64_t j = lo; j <= hi; j += st) pos[x].push_back({position == 2 ? Pos::Raw : Pos::Node, j});
+        }
+    }
+    return sampler_build(m, quantity, pos, false);
+}
+
+ems_sampler_host* ems_sampler_new_indices(ems_model* m, int quantity, int position, const uint64_t* const idx[3],
+                                          const size_t n[3]) {
+    if (quantity < EMS_DUMP_E || quantity > EMS_DUMP_B || position < 0 || position > 2)
+        return set_err(m, "sampler: invalid quantity or position"), nullptr;
+    if ((quantity == EMS_DUMP_J || quantity == EMS_DUMP_D || quantity == EMS_DUMP_B) && !m->built)
+        return set_err(m, "sampler: J, D and B need the built model's coefficients"), nullptr;
+    std::vector<PosJ> pos[3];
+    for (int x = 0; x < 3; ++x) {
+        if (!n[x] || !idx[x]) return set_err(m, "dump sample indices must be increasing and inside the grid"), nullptr;
+        for (size_t q = 0; q < n[x]; ++q) {
+            if (idx[x][q] >= m->n[x] || (q && idx[x][q] <= idx[x][q - 1]))
+                return set_err(m, "dump sample indices must be increasing and inside the grid"), nullptr;
+            pos[x].push_back({position == 1 ? Pos::Mid : (position == 2 ? Pos::Raw : Pos::Node), idx[x][q]});
+        }
+    }
+    return sampler_build(m, quantity, pos, true);
+}
+
+const ems_sampler* ems_sampler_table(const ems_sampler_host* s) { return s ? &s->t : nullptr; }
+
+const double* ems_sampler_coords(const ems_sampler_host* s, int axis, size_t* n) {
+    if (!s || axis < 0 || axis > 2) return nullptr;
+    if (n) *n = s->coords[axis].size();
+    return s->coords[axis].data();
+}
+
+void ems_sampler_free(ems_sampler_host* s) { delete s; }
+
+// ---------------------------------------------------------------------------
+// Conducting sheets (src/engine/sheet.rs).
+
+namespace {
+
+constexpr double kSurfaceLayer = 0.15;  // SURFACE_LAYER, sheet.rs:224
+constexpr double kGrowth = 1.15;        // GROWTH, sheet.rs:233
+
+// skin_depth (sheet.rs:237-239): sqrt(2/(ω μ0 σ)).
+double skin_depth(double sigma, double f) { return std::sqrt(2.0 / (2.0 * PI * f * MU0 * sigma)); }
+
+// layer_profile (sheet.rs:244-271): outer layers 0.15 skin depths at f_max
+// thick, each further one 1.15 times thicker up to the middle, mirrored; a
+// sheet thinner than two outer layers gets uniform layers of at most one
+// outer layer each.
+std::vector<double> layer_profile(double sigma, double t, double f_max) {
+    const double s = kSurfaceLayer * skin_depth(sigma, f_max);
+    const bool ok = std::isfinite(s) && s > 0.0;
+    if (!ok || t <= 2.0 * s) {
+        size_t n = 1;
+        if (ok) {
+            const double q = std::ceil(t / s);
+            n = q >= 1.0 ? (size_t)q : 1;
+        }
+        return std::vector<double>(n, t / (double)n);
+    }
+    const double half_t = 0.5 * t;
+    std::vector<double> half;
+    double acc = 0.0, dz = s;
+    while (acc + dz < half_t) {
+        half.push_back(dz);
+        acc += dz;
+        dz *= kGrowth;
+    }
+    const double rem = half_t - acc;
+    if (!half.empty() && rem < 0.5 * half.back()) half.back() += rem;
+    else half.push_back(rem);
+    std::vector<double> out = half;
+    out.insert(out.end(), half.rbegin(), half.rend());
+    return out;
+}
+
+// sheet_geometry on a Cartesian grid (sheet.rs:352-400): g = w/l (w the
+// dual length across the edge in the sheet, l the edge length) and the
+// share f_up of the crossing dual edges on the + side of the normal.
+void sheet_geometry(const ems_model* m, int d, int nrm, const uint64_t node[3], double& g, double& f_up) {
+    const int t = 3 - nrm - d;
+    const uint64_t k = node[nrm];
+    const double up = k + 1 < m->n[nrm] ? m->delta(nrm, k) : 0.0;
+    const double dn = k > 0 ? m->delta(nrm, k - 1) : 0.0;
+    f_up = up / (up + dn);
+    g = m->dual_delta(t, node[t]) / m->delta(d, node[d]);
+}
+
+}  // namespace
+
+size_t ems_sheet_layer_profile(double sigma, double thickness, double f_max, double* out, size_t cap) {
+    const std::vector<double> v = layer_profile(sigma, thickness, f_max);
+    for (size_t q = 0; q < v.size() && q < cap; ++q) out[q] = v[q];
+    return v.size();
+}
+
+int ems_model_add_sheet(ems_model* m, size_t n, const int* axis, const uint64_t* nodes, const int* normal,
+                        const double* sigma, const double* thickness, const double* share_c, const double* share_g,
+                        double f_max, uint64_t* installed, uint64_t* skipped) {
+    if (!m->built) return set_err(m, "build the model first"), -1;
+    if (n && (!axis || !nodes || !normal || !sigma || !thickness)) return set_err(m, "conducting sheet: missing arrays"), -1;
+    auto has_share = [&](size_t e) { return share_c && share_g && (share_c[e] >= 0.0 || share_g[e] >= 0.0); };
+    // ConductingSheet::validate (sheet.rs:635-656).
+    for (size_t e = 0; e < n; ++e) {
+        const int a = axis[e], nr = normal[e];
+        const uint64_t* p = nodes + 3 * e;
+        if (a < 0 || a > 2 || nr < 0 || nr > 2 || a == nr)
+            return set_err(m, "conducting sheet edge: the edge is not tangential to the sheet"), -1;
+        if (!(std::isfinite(sigma[e]) && sigma[e] > 0.0))
+            return set_err(m, "conducting sheet edge: conductivity must be finite and > 0"), -1;
+        if (!(std::isfinite(thickness[e]) && thickness[e] > 0.0))
+            return set_err(m, "conducting sheet edge: thickness must be finite and > 0"), -1;
+        if (has_share(e) && !(share_c[e] >= 0.0 && share_c[e] <= 1.0 && share_g[e] >= 0.0 && share_g[e] <= 1.0))
+            return set_err(m, "conducting sheet edge: shares must be in [0, 1]"), -1;
+        if (p[0] >= m->n[0] || p[1] >= m->n[1] || p[2] >= m->n[2] || p[a] + 1 >= m->n[a])
+            return set_err(m, "conducting sheet edge: not an edge of the grid"), -1;
+    }
+    if (f_max != 0.0 && !(std::isfinite(f_max) && f_max > 0.0))
+        return set_err(m, "conducting sheet: f_max must be finite and > 0"), -1;
+    const double dt = m->dt;
+    const double fm = f_max > 0.0 ? f_max : 0.1 / dt;
+    // install (sheet.rs:658-933): edges sorted by (node, axis), stable.
+    std::vector<size_t> order(n);
+    std::iota(order.begin(), order.end(), (size_t)0);
+    auto key = [&](size_t e) { return std::make_tuple(nodes[3 * e], nodes[3 * e + 1], nodes[3 * e + 2], axis[e]); };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return key(x) < key(y); });
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_SHEET;
+    std::map<std::vector<uint64_t>, std::pair<uint32_t, uint32_t>> ladders;
+    uint64_t n_skip = 0;
+    bool have_last = false;
+    uint64_t last_idx = 0;
+    int last_axis = -1;
+    auto bits = [](double v) {
+        uint64_t b;
+        std::memcpy(&b, &v, 8);
+        return b;
+    };
+    for (size_t q : order) {
+        const int d = axis[q], nrm = normal[q];
+        const uint64_t* p = nodes + 3 * q;
+        const uint64_t idx = m->index(p[0], p[1], p[2]);
+        if (have_last && last_idx == idx && last_axis == d) {  // a duplicate
+            ++n_skip;
+            continue;
+        }
+        have_last = true;
+        last_idx = idx;
+        last_axis = d;
+        const double ca = (double)m->co[d][idx], cb = (double)m->co[3 + d][idx];
+        if (cb == 0.0) {  // PEC
+            ++n_skip;
+            continue;
+        }
+        const double c_edge = dt * (1.0 + ca) / (2.0 * cb);
+        const double g_edge = (1.0 - ca) / cb;
+        double geo, f_up;
+        sheet_geometry(m, d, nrm, p, geo, f_up);
+        const double sc = has_share(q) ? share_c[q] : f_up;
+        const double sg = has_share(q) ? share_g[q] : f_up;
+        // The ladder: shunt G_k, C_k on the nodes (half layers around
+        // each), series L_j per layer, the split edge C and G on the faces.
+        const std::vector<double> dz = layer_profile(sigma[q], thickness[q], fm);
+        const size_t nn = dz.size() + 1;
+        std::vector<double> a, g_node(nn, 0.0), c_node(nn, 0.0);
+        for (size_t j = 0; j < dz.size(); ++j) {
+            const double z = dz[j];
+            for (size_t kk : {j, j + 1}) {
+                g_node[kk] += 0.5 * sigma[q] * z * geo;
+                c_node[kk] += 0.5 * EPS0 * z * geo;
+            }
+            a.push_back(dt * geo / (2.0 * MU0 * z));
+        }
+        c_node[0] += sc * c_edge;
+        g_node[0] += sg * g_edge;
+        c_node[nn - 1] += (1.0 - sc) * c_edge;
+        g_node[nn - 1] += (1.0 - sg) * g_edge;
+        // Thomas factorisation of the constant tridiagonal matrix.
+        std::vector<double> konst;
+        double prev_cp = 0.0;
+        for (size_t kk = 0; kk < nn; ++kk) {
+            const double a_up = kk + 1 < nn ? a[kk] : 0.0;
+            const double a_dn = kk > 0 ? a[kk - 1] : 0.0;
+            const double tc = 2.0 * c_node[kk] / dt;
+            const double diag = tc + g_node[kk] + a_up + a_dn;
+            const double den = diag + a_dn * prev_cp;
+            const double cpk = -a_up / den;
+            konst.insert(konst.end(), {tc, cpk, 1.0 / den});
+            prev_cp = cpk;
+        }
+        // Edges with bit-identical constants share them.
+        std::vector<uint64_t> kb;
+        for (double v : a) kb.push_back(bits(v));
+        for (double v : konst) kb.push_back(bits(v));
+        auto it = ladders.find(kb);
+        if (it == ladders.end()) {
+            std::pair<uint32_t, uint32_t> at((uint32_t)op->two_c.size(), (uint32_t)op->sa.size());
+            for (size_t kk = 0; kk < nn; ++kk) {
+                op->two_c.push_back(konst[3 * kk]);
+                op->cp.push_back(konst[3 * kk + 1]);
+                op->inv_den.push_back(konst[3 * kk + 2]);
+            }
+            op->sa.insert(op->sa.end(), a.begin(), a.end());
+            it = ladders.emplace(kb, at).first;
+        }
+        // The four dual edges around the dual face, with their sign in the
+        // E update and their shares of the two faces.
+        const int b = next_axis(d), c = prev_axis(d);
+        const std::array<std::tuple<int, int, double>, 4> around = {
+            {{c, -1, 1.0}, {c, b, -1.0}, {b, -1, -1.0}, {b, c, 1.0}}};
+        for (const auto& [ax, off, sgn] : around) {
+            uint64_t mm[3] = {p[0], p[1], p[2]};
+            if (off >= 0) {
+                if (mm[off] == 0) continue;
+                mm[off] -= 1;
+            }
+            const int pp = next_axis(ax), qq = prev_axis(ax);
+            if (mm[pp] + 1 >= m->n[pp] || mm[qq] + 1 >= m->n[qq]) continue;
+            double w_up = 1.0, w_dn = 0.0;
+            if (ax == nrm) {
+                w_up = f_up;
+                w_dn = 1.0 - f_up;
+            } else if (off == nrm) {
+                w_up = 0.0;
+                w_dn = 1.0;
+            }
+            const uint64_t mi = m->index(mm[0], mm[1], mm[2]);
+            const double da = (double)m->co[6 + ax][mi], db = (double)m->co[9 + ax][mi];
+            const double corr = -db * sgn * w_dn;
+            const double ecorr = db == 0.0 ? 0.0 : 0.5 * dt * (1.0 + da) / (2.0 * db) * corr;
+            op->cax.push_back((uint8_t)ax);
+            op->cnode.push_back(mi);
+            op->cwup.push_back(sgn * w_up);
+            op->cwdn.push_back(sgn * w_dn);
+            op->ccorr.push_back(corr);
+            op->cecorr.push_back(ecorr);
+        }
+        op->sax.push_back((uint8_t)d);
+        op->snode.push_back(idx);
+        op->snn.push_back((uint32_t)nn);
+        op->sk0.push_back(it->second.first);
+        op->sa0.push_back(it->second.second);
+        op->send.push_back((uint32_t)op->cax.size());
+        op->scedge.push_back(c_edge);
+    }
+    if (installed) *installed = op->sax.size();
+    if (skipped) *skipped = n_skip;
+    ems_sheet& S = op->sheet;
+    S.n_edges = op->sax.size();
+    S.axis = op->sax.data();
+    S.node = op->snode.data();
+    S.nn = op->snn.data();
+    S.konst0 = op->sk0.data();
+    S.a0 = op->sa0.data();
+    S.coupling_end = op->send.data();
+    S.c_edge = op->scedge.data();
+    S.n_couplings = op->cax.size();
+    S.c_axis = op->cax.data();
+    S.c_node = op->cnode.data();
+    S.w_up = op->cwup.data();
+    S.w_dn = op->cwdn.data();
+    S.corr = op->ccorr.data();
+    S.ecorr = op->cecorr.data();
+    S.n_konst = op->two_c.size();
+    S.two_c = op->two_c.data();
+    S.cp = op->cp.data();
+    S.inv_den = op->inv_den.data();
+    S.n_a = op->sa.size();
+    S.a = op->sa.data();
     m->ops.push_back(std::move(op));
     m->refresh_desc();
     return (int)m->ops.size() - 1;

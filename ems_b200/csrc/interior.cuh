@@ -170,7 +170,7 @@ inline std::string interior_box(const ems_engine_desc* d, const Grid& g, Interio
             const int kind = ((const ems_source*)op.table)->kind;
             if (kind == EMS_SOFT_H || kind == EMS_HARD_H) return "magnetic sources";
         } else if (op.kind != EMS_OP_PROBE) {
-            return "lumped elements, Mur faces or openEMS PML layers";
+            return "lumped elements, Mur faces, openEMS PML layers or conducting sheets";
         }
     }
     lo[2] = (lo[2] + 3u) & ~3u;

@@ -542,20 +542,88 @@ struct DumpDev {
     const double* freqs;
     double dt, t0;
     double* acc;  // [nf][npts][3] complex, re and im interleaved
+    // A sampler's table (samp != 0; n holds its dims): taps, factors.
+    int32_t samp = 0, roth = 0;
+    uint32_t off[3];
+    const uint32_t* tidx = nullptr;
+    const double* tw = nullptr;
+    uint32_t flo[3], fdim[3];
+    const double* fac = nullptr;
 };
 
-// Time-domain snapshot (src/engine/dump.rs TimeDump with native positions):
-// the field values E = u/Δ or H = i/Δ* of every point of the box, in f64,
-// into out[p·3 + component].
+__device__ __forceinline__ double dump_get(const DumpDev& d, int c, uint32_t i, uint32_t j, uint32_t k) {
+    return (double)d.f[c][((size_t)i * d.ny + j) * d.pitch + k];
+}
+
+// The three components of point p: native (E = u/Δ or H = i/Δ* of the
+// edge that starts at the node) or through a sampler (FieldSampler::
+// sample_from, src/engine/dump.rs:846-906: Σ wx·wy·wz·m·x over the taps
+// of nonzero weight, x the unknown or, for rot H, the circulation of i
+// around the primary edge, dump.rs:814-834).
+__device__ __forceinline__ void dump_point(const DumpDev& d, uint32_t p, double x[3]) {
+    const uint32_t iz = p % d.n[2], r = p / d.n[2], iy = r % d.n[1], ix = r / d.n[1];
+    if (!d.samp) {
+        const uint32_t i = d.lo[0] + ix * d.st[0], j = d.lo[1] + iy * d.st[1], k = d.lo[2] + iz * d.st[2];
+        const size_t idx = ((size_t)i * d.ny + j) * d.pitch + k;
+        x[0] = __dmul_rn((double)d.f[0][idx], d.inv_len[0][i]);
+        x[1] = __dmul_rn((double)d.f[1][idx], d.inv_len[1][j]);
+        x[2] = __dmul_rn((double)d.f[2][idx], d.inv_len[2][k]);
+        return;
+    }
+    const size_t vol = (size_t)d.fdim[0] * d.fdim[1] * d.fdim[2];
+    for (int c = 0; c < 3; ++c) {
+        const uint32_t ex = 2 * (d.off[0] + c * d.n[0] + ix), ey = 2 * (d.off[1] + c * d.n[1] + iy),
+                       ez = 2 * (d.off[2] + c * d.n[2] + iz);
+        double v = 0.0;
+        for (int tx = 0; tx < 2; ++tx) {
+            const double wx = d.tw[ex + tx];
+            if (wx == 0.0) continue;
+            for (int ty = 0; ty < 2; ++ty) {
+                const double wy = d.tw[ey + ty];
+                if (wy == 0.0) continue;
+                for (int tz = 0; tz < 2; ++tz) {
+                    const double wz = d.tw[ez + tz];
+                    if (wz == 0.0) continue;
+                    const uint32_t nd[3] = {d.tidx[ex + tx], d.tidx[ey + ty], d.tidx[ez + tz]};
+                    double val;
+                    if (d.roth) {
+                        const int a = (c + 1) % 3, b = (c + 2) % 3;
+                        val = __dsub_rn(dump_get(d, b, nd[0], nd[1], nd[2]), dump_get(d, a, nd[0], nd[1], nd[2]));
+                        if (nd[a] > 0) {
+                            uint32_t q[3] = {nd[0], nd[1], nd[2]};
+                            q[a] -= 1;
+                            val = __dsub_rn(val, dump_get(d, b, q[0], q[1], q[2]));
+                        }
+                        if (nd[b] > 0) {
+                            uint32_t q[3] = {nd[0], nd[1], nd[2]};
+                            q[b] -= 1;
+                            val = __dadd_rn(val, dump_get(d, a, q[0], q[1], q[2]));
+                        }
+                    } else {
+                        val = dump_get(d, c, nd[0], nd[1], nd[2]);
+                    }
+                    double m = 1.0;
+                    if (d.fac)
+                        m = d.fac[c * vol + ((size_t)(nd[0] - d.flo[0]) * d.fdim[1] + (nd[1] - d.flo[1])) * d.fdim[2] +
+                                  (nd[2] - d.flo[2])];
+                    v = __dadd_rn(v, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(wx, wy), wz), m), val));
+                }
+            }
+        }
+        x[c] = v;
+    }
+}
+
+// Time-domain snapshot (src/engine/dump.rs TimeDump): the three components
+// of every point, in f64, into out[p·3 + component].
 __global__ void __launch_bounds__(256) k_snapshot(const __grid_constant__ DumpDev d, double* out) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= d.npts) return;
-    const uint32_t iz = p % d.n[2], r = p / d.n[2], iy = r % d.n[1], ix = r / d.n[1];
-    const uint32_t i = d.lo[0] + ix * d.st[0], j = d.lo[1] + iy * d.st[1], k = d.lo[2] + iz * d.st[2];
-    const size_t idx = ((size_t)i * d.ny + j) * d.pitch + k;
-    out[3 * (size_t)p] = __dmul_rn((double)d.f[0][idx], d.inv_len[0][i]);
-    out[3 * (size_t)p + 1] = __dmul_rn((double)d.f[1][idx], d.inv_len[1][j]);
-    out[3 * (size_t)p + 2] = __dmul_rn((double)d.f[2][idx], d.inv_len[2][k]);
+    double x[3];
+    dump_point(d, p, x);
+    out[3 * (size_t)p] = x[0];
+    out[3 * (size_t)p + 1] = x[1];
+    out[3 * (size_t)p + 2] = x[2];
 }
 
 __device__ __forceinline__ double frac_toward_zero(double x) { return x - trunc(x); }
@@ -563,12 +631,8 @@ __device__ __forceinline__ double frac_toward_zero(double x) { return x - trunc(
 __global__ void __launch_bounds__(256) k_dump(const __grid_constant__ DumpDev d, double m) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= d.npts) return;
-    const uint32_t iz = p % d.n[2], r = p / d.n[2], iy = r % d.n[1], ix = r / d.n[1];
-    const uint32_t i = d.lo[0] + ix * d.st[0], j = d.lo[1] + iy * d.st[1], k = d.lo[2] + iz * d.st[2];
-    const size_t idx = ((size_t)i * d.ny + j) * d.pitch + k;
-    const double x[3] = {__dmul_rn((double)d.f[0][idx], d.inv_len[0][i]),
-                         __dmul_rn((double)d.f[1][idx], d.inv_len[1][j]),
-                         __dmul_rn((double)d.f[2][idx], d.inv_len[2][k])};
+    double x[3];
+    dump_point(d, p, x);
     for (uint32_t q = 0; q < d.nf; ++q) {
         const double fq = d.freqs[q];
         const double a = __dmul_rn(fq, d.dt);

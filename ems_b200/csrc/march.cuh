@@ -652,7 +652,7 @@ inline std::string march_why(const ems_engine_desc* d) {
             const int kind = ((const ems_source*)op.table)->kind;
             if (kind == EMS_SOFT_H || kind == EMS_HARD_H) return "magnetic sources";
         } else if (op.kind != EMS_OP_PROBE) {
-            return "lumped elements, Mur faces or openEMS PML layers";
+            return "lumped elements, Mur faces, openEMS PML layers or conducting sheets";
         }
     }
     if (pos_cpml >= 0 && pos_poles >= 0 && pos_poles < pos_cpml) return "poles registered before the CPML";

@@ -51,7 +51,8 @@ typedef enum {
     EMS_OP_SOURCE = 4, /* serial post_h or post_e      (src/engine/excite.rs:104-173)        */
     EMS_OP_PROBE = 5,  /* serial post_h or post_e      (src/engine/probe.rs:480-510)         */
     EMS_OP_MUR = 6,    /* serial pre_e / post_e        (src/engine/boundary/mur.rs:781-843)  */
-    EMS_OP_UPML = 7    /* slab hooks post_h / post_e   (src/engine/boundary/upml.rs:443-470) */
+    EMS_OP_UPML = 7,   /* slab hooks post_h / post_e   (src/engine/boundary/upml.rs:443-470) */
+    EMS_OP_SHEET = 8   /* serial post_h / post_e       (src/engine/sheet.rs:941-1050)        */
 } ems_op_kind;
 
 /* One CPML slab: the correction of one field component in one face layer
@@ -231,9 +232,54 @@ typedef struct {
     const float* co[2];
 } ems_upml;
 
+/* Conducting sheets (src/engine/sheet.rs:403-1090, ConductingSheet): thin
+ * lossy conductors on mesh planes. Sheet edge e (the E edge along axis[e]
+ * at node[e]) carries a ladder across the sheet's thickness: nn[e] node
+ * voltages u_0..u_{nn-1} (u_0 the face on the + side along the normal,
+ * which the field array holds; u_{nn-1} the - face) and nn[e] - 1 layer
+ * currents h_j, all f64 and zero at first. Its constants: per node
+ * two_c = 2C_k/dt, cp = Thomas c'_k, inv_den = 1/den_k from konst0[e]; per
+ * layer a = dt/(2L_j) from a0[e] (edges with equal ladders share them);
+ * c_edge the edge capacitance dt(1 + ca)/(2cb). Couplings
+ * [coupling_end[e-1], coupling_end[e]) are the dual edges around its dual
+ * face: the H entry (c_axis, c_node), its signed weights w_up, w_dn in
+ * Ampere's law of the two faces, corr and ecorr = L·corr/2 with
+ * L = dt(1 + da)/(2db) the dual edge's inductance.
+ *   post_h, per edge: u_0 = u[edge]; per coupling with corr != 0, in edge
+ *     then coupling order: i = flush(i + f32(corr·(u_{nn-1} - u_0)));
+ *   post_e, per edge: s_up = sum w_up·i, s_dn = sum w_dn·i (from 0, in
+ *     coupling order), one tridiagonal solve for the mean voltages x_k,
+ *     h_j += 2a_j(x_j - x_{j+1}), u_k = 2x_k - u_k, u[edge] = flush(f32(u_0)).
+ * Energy: sum_k two_c·dt·u_k^2/4 - c_edge·u[edge]^2/2 + sum_j L_j·h_j^2/2
+ * (L_j = dt/(2a_j)) plus sum ecorr·i·(u_{nn-1} - u[edge]) taken at the
+ * end of the last post_e. */
+typedef struct {
+    size_t n_edges;
+    const uint8_t* axis;
+    const uint64_t* node;
+    const uint32_t* nn;
+    const uint32_t* konst0;
+    const uint32_t* a0;
+    const uint32_t* coupling_end;
+    const double* c_edge;
+    size_t n_couplings;
+    const uint8_t* c_axis;
+    const uint64_t* c_node;
+    const double* w_up;
+    const double* w_dn;
+    const double* corr;
+    const double* ecorr;
+    size_t n_konst;
+    const double* two_c;
+    const double* cp;
+    const double* inv_den;
+    size_t n_a;
+    const double* a;
+} ems_sheet;
+
 typedef struct {
     int32_t kind; /* ems_op_kind */
-    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe*, ems_mur*, ems_upml* */
+    const void* table; /* ems_cpml*, ems_poles*, ems_lumped*, ems_source*, ems_probe*, ems_mur*, ems_upml*, ems_sheet* */
 } ems_op;
 
 /* Everything an engine is built from: the grid size, the time step, the
@@ -274,7 +320,10 @@ ems_status ems_gpu_upload_field(ems_gpu* h, int field, int axis, const float* ho
 
 /* Samples of operator `op` (index into desc->ops): a probe's values
  * (which = 0), a lumped element's current record (which = 0) or, for a
- * port, its voltage (which = 1) and current (which = 2). Writes up to
+ * port, its voltage (which = 1) and current (which = 2), or a conducting
+ * sheet's ladder state: every edge's node voltages (which = 0) or layer
+ * currents (which = 1), edge after edge (ConductingSheet::lower_voltage,
+ * src/engine/sheet.rs:628-633, is the last node of an edge). Writes up to
  * `cap` values into `out` (may be NULL) and the total count into *n. */
 ems_status ems_gpu_samples(ems_gpu* h, size_t op, int which, double* out, size_t cap, size_t* n);
 
@@ -408,6 +457,37 @@ ems_status ems_gpu_set_march(ems_gpu* h, int shape, uint32_t planes);
  * the reference, whose CPU engine has a single code path. */
 ems_status ems_gpu_autotune(ems_gpu* h, const char* cache_path);
 
+/* ---- Field samplers (FieldSampler, src/engine/dump.rs:487-940): one
+ * quantity converted to field units and interpolated at a set of sample
+ * points, dims[0] x dims[1] x dims[2] points, z fastest. Built on the host
+ * (ems_sampler_new, include/ems_host.h).
+ *
+ * Every value is a tensor product of 1-D rules: component c at sample
+ * (p, q, r) is the sum, in the order x tap, y tap, z tap, skipping taps of
+ * weight 0, of wx*wy*wz*m*x with x the unknown of component c at the tap
+ * node (u for E, J, D; i for H, B; for rot H the circulation of i around
+ * the primary edge c, i_b(p) - i_a(p) - i_b(p - a) + i_a(p - b) with (a, b)
+ * the axes after c) and m the factor of component c at that node (1 when
+ * `factors` is NULL). Along axis a, component c's two taps of sample s are
+ * entries 2*(off[a] + c*dims[a] + s) + t, t = 0, 1, of tap_idx (the node
+ * index along a) and tap_w, with off = {0, 3*dims[0], 3*(dims[0] + dims[1])}.
+ * The factors cover the node box fac_lo + [0, fac_dims) (every node any
+ * tap of weight != 0 reads), z fastest, component c at
+ * c * fac_dims[0]*fac_dims[1]*fac_dims[2]. */
+typedef enum {
+    EMS_DUMP_E = 0, EMS_DUMP_H = 1, EMS_DUMP_J = 2, EMS_DUMP_ROTH = 3, EMS_DUMP_D = 4, EMS_DUMP_B = 5
+} ems_dump_quantity;
+
+typedef struct {
+    int32_t quantity;   /* ems_dump_quantity */
+    uint64_t dims[3];
+    const uint32_t* tap_idx;
+    const double* tap_w;
+    uint64_t fac_lo[3];
+    uint64_t fac_dims[3];
+    const double* factors;
+} ems_sampler;
+
 /* ---- Frequency-domain field dumps (src/engine/dump.rs:1420-1700,
  * FreqDump with DumpPosition::Native and DumpTiming::State): a running DFT
  * on the device of one field over a box of nodes.
@@ -428,6 +508,8 @@ typedef struct {
     size_t n_freqs;
     const double* freqs;
     uint64_t interval;
+    const ems_sampler* sampler; /* not NULL: its points and quantity (field, box and inv_len unused);
+                                   H, B and rot H at (m - 1/2)*dt */
 } ems_freq_dump;
 
 /* Adds a dump (before or between runs); *id is its index. */
@@ -444,6 +526,7 @@ typedef struct {
     uint64_t lo[3], hi[3], stride[3];
     const double* inv_len[3];
     uint64_t interval;
+    const ems_sampler* sampler; /* as in ems_freq_dump */
 } ems_time_dump;
 
 ems_status ems_gpu_time_dump_add(ems_gpu* h, const ems_time_dump* spec, size_t* id);

@@ -204,6 +204,50 @@ int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, c
 int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6], const uint64_t hold_until[6],
                       int flags);
 
+/* Conducting sheets (ConductingSheet::new(f_max), push, add_to;
+ * src/engine/sheet.rs:529-935) on the built model, Cartesian, outlines on
+ * mesh lines: n sheet edges, edge e the E edge along axis[e] at node
+ * nodes[3e..3e+2] on a sheet normal to normal[e], of conductivity sigma[e]
+ * [S/m] and thickness thickness[e] [m]; share_c/share_g (NULL, or < 0 for
+ * an edge: the default) the shares of the edge's capacitance and
+ * conductance on the + side. f_max: the highest frequency the layers
+ * resolve (0: 1/(10 dt)). Edges are installed in node order; PEC edges and
+ * duplicates are skipped. Writes the installed and skipped counts (either
+ * may be NULL) and returns the op index, or -1 for an invalid edge or
+ * f_max (nothing added). */
+int ems_model_add_sheet(ems_model* m, size_t n, const int* axis, const uint64_t* nodes, const int* normal,
+                        const double* sigma, const double* thickness, const double* share_c, const double* share_g,
+                        double f_max, uint64_t* installed, uint64_t* skipped);
+
+/* Layer thicknesses of a sheet (sigma, thickness) resolved up to f_max
+ * (layer_profile, src/engine/sheet.rs:244-271): writes up to `cap` values
+ * and returns their number. */
+size_t ems_sheet_layer_profile(double sigma, double thickness, double f_max, double* out, size_t cap);
+
+/* Field samplers (FieldSampler::new, src/engine/dump.rs:508-528): the
+ * table (include/ems_gpu.h, ems_sampler) of `quantity` (ems_dump_quantity)
+ * over the node box between corners a and b (any order, inclusive) with
+ * `stride` (0 counts as 1; NULL: 1) at `position` 0 nodes, 1 cell centres
+ * (the node along a degenerate axis), 2 native (raw edge values, no
+ * interpolation). J, D and B take their factors from the built model's
+ * coefficients. NULL for a box outside the grid (the model's error says
+ * why). Cartesian grids. */
+typedef struct ems_sampler_host ems_sampler_host;
+ems_sampler_host* ems_sampler_new(ems_model* m, int quantity, int position, const uint64_t a[3], const uint64_t b[3],
+                                  const uint64_t stride[3]);
+/* FieldSampler::openems (src/engine/dump.rs:530-571): explicit increasing
+ * sample indices per axis (node indices; cell indices for cell centres,
+ * n - 1 the virtual cell beyond the last node, value 0) with openEMS's
+ * rules: H at a node is the plain mean of its dual edges (0 on the outer
+ * nodes), H along its axis at a cell centre interpolated between the dual
+ * edges' midpoints, rot H over dual faces with full outer cells. */
+ems_sampler_host* ems_sampler_new_indices(ems_model* m, int quantity, int position, const uint64_t* const idx[3],
+                                          const size_t n[3]);
+const ems_sampler* ems_sampler_table(const ems_sampler_host* s);
+/* Coordinates [m] of the sample points along `axis` (*n of them). */
+const double* ems_sampler_coords(const ems_sampler_host* s, int axis, size_t* n);
+void ems_sampler_free(ems_sampler_host* s);
+
 /* Sums probe `op`'s entries in f32 (openEMS's current probes, the
  * `f32_sum` of Probe, src/engine/probe.rs:381-392) when `on`. */
 int ems_model_probe_f32(ems_model* m, int op, int on);

@@ -34,6 +34,7 @@ def lib() -> C.CDLL:
             "oracle_download_field": [p, C.c_int, C.c_int, p],
             "oracle_upload_field": [p, C.c_int, C.c_int, p],
             "oracle_samples": [p, C.c_size_t, C.c_int, p, C.c_size_t, p],
+            "oracle_sample": [p, p, p],
         }.items():
             f = getattr(L, name)
             f.restype = C.c_int
@@ -93,6 +94,13 @@ class OracleEngine:
         v = np.ascontiguousarray(values, dtype=np.float32)
         if self._lib.oracle_upload_field(self._h, field, axis, v.ctypes.data) != 0:
             raise RuntimeError("oracle_upload_field failed")
+
+    def sample(self, sampler) -> np.ndarray:
+        """The current state through an ``ems_b200.Sampler``: (points, 3) f64."""
+        out = np.zeros((len(sampler), 3), dtype=np.float64)
+        if self._lib.oracle_sample(self._h, sampler.table, out.ctypes.data) != 0:
+            raise RuntimeError("oracle_sample failed")
+        return out
 
     def samples(self, op: int, which: int = 0) -> np.ndarray:
         n = C.c_size_t()

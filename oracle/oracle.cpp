@@ -10,8 +10,12 @@
 // built here, so the oracle is pinned by the reference's own known-answer
 // tests restated on it (tests/test_oracle_known_answers.py: cavity modes,
 // energy invariant and decay, run-loop stop, thread determinism, CPML
-// reflection levels, dispersive energy; tests/test_mur.py: Mur reflection,
-// stability, determinism) and by the reference's golden vectors, the
+// reflection levels as printed, dispersive energy;
+// tests/test_oracle_dispersive_validation.py: poles against the continuum
+// and the discrete susceptibilities; tests/test_oracle_lumped.py: lumped
+// elements and ports; tests/test_oracle_sheet.py: conducting sheets against
+// the exact slab; tests/test_mur.py: Mur reflection, stability,
+// determinism) and by the reference's golden vectors, the
 // openEMS probe files of its XML fixtures, which the oracle reproduces to
 // 1e-4 or better on every fixture whose features the openEMS front end
 // (ems_b200/openems.py) restates (tests/test_openems_fixtures.py).
@@ -175,6 +179,18 @@ struct Upml {
     std::vector<uint32_t> by_plane[2], pstart[2];
 };
 
+// Conducting sheets (src/engine/sheet.rs:403-522): per edge its ladder
+// (nodes n0..n0+nn of u, layers l0..l0+nn-1 of h), its constants from k0
+// (per node) and a0 (per layer), its couplings [c0, c1).
+struct Sheet {
+    std::vector<uint8_t> axis, c_axis;
+    std::vector<uint64_t> node, c_node;
+    std::vector<uint32_t> nn, k0, a0, c0, c1, n0, l0;
+    std::vector<double> c_edge, w_up, w_dn, corr, ecorr, two_c, cp, inv_den, a;
+    std::vector<double> u, h, x;
+    double w_corr = 0.0;
+};
+
 struct Op {
     int kind = 0;
     std::vector<CpmlSlab> cpml;
@@ -184,6 +200,7 @@ struct Op {
     Probe probe;
     Mur mur;
     Upml upml;
+    Sheet sheet;
 };
 
 // src/engine/boundary/mur.rs:252-259 mur_1d: u_b^{n+1} from u_1^n (i),
@@ -464,6 +481,8 @@ struct oracle_engine {
                 const Mur& m = op.mur;
                 for (size_t e = 0; e < m.node.size(); ++e)
                     x += 0.5 * m.cap[e] * (double)m.last[e] * (double)m.last[e];
+            } else if (op.kind == EMS_OP_SHEET) {
+                x = sheet_energy(op.sheet);
             } else if (op.kind == EMS_OP_LUMPED && op.lumped.has_branch) {
                 // src/engine/lumped.rs:1066-1077 branch_energy
                 const Lumped& l = op.lumped;
@@ -475,6 +494,75 @@ struct oracle_engine {
             w += x;
         }
         return w;
+    }
+
+    // ---- conducting sheets
+    // post_h (src/engine/sheet.rs:950-972): the + face voltage from the
+    // array, then the dual edges on the - side see u- - u+.
+    void sheet_post_h(Sheet& s) {
+        for (size_t e = 0; e < s.axis.size(); ++e) {
+            const size_t n0 = s.n0[e], nn = s.nn[e];
+            s.u[n0] = (double)u[s.axis[e]][s.node[e]];
+            const double diff = s.u[n0 + nn - 1] - s.u[n0];
+            for (uint32_t c = s.c0[e]; c < s.c1[e]; ++c)
+                if (s.corr[c] != 0.0) {
+                    float& v = i[s.c_axis[c]][s.c_node[c]];
+                    v = flush(v + (float)(s.corr[c] * diff));
+                }
+        }
+    }
+
+    // post_e (src/engine/sheet.rs:974-1050): the ladder and both faces by
+    // the trapezoidal rule, one tridiagonal solve per edge (Thomas, the
+    // factorisation precomputed), the + face written back.
+    void sheet_post_e(Sheet& s) {
+        double w_corr = 0.0;
+        for (size_t e = 0; e < s.axis.size(); ++e) {
+            double s_up = 0.0, s_dn = 0.0, s_e = 0.0;
+            for (uint32_t c = s.c0[e]; c < s.c1[e]; ++c) {
+                const double iv = (double)i[s.c_axis[c]][s.c_node[c]];
+                s_up += s.w_up[c] * iv;
+                s_dn += s.w_dn[c] * iv;
+                s_e += s.ecorr[c] * iv;
+            }
+            const size_t nn = s.nn[e], k0 = s.k0[e], ka = s.a0[e];
+            double* U = s.u.data() + s.n0[e];
+            double* H = s.h.data() + s.l0[e];
+            double* X = s.x.data();
+            for (size_t k = 0; k < nn; ++k) {
+                double r = s.two_c[k0 + k] * U[k];
+                if (k + 1 < nn) r -= H[k];
+                if (k > 0) r += H[k - 1] + s.a[ka + k - 1] * X[k - 1];
+                if (k == 0) r += s_up;
+                if (k + 1 == nn) r += s_dn;
+                X[k] = r * s.inv_den[k0 + k];
+            }
+            for (size_t k = nn - 1; k-- > 0;) X[k] -= s.cp[k0 + k] * X[k + 1];
+            for (size_t j = 0; j + 1 < nn; ++j) H[j] += 2.0 * s.a[ka + j] * (X[j] - X[j + 1]);
+            for (size_t k = 0; k < nn; ++k) U[k] = 2.0 * X[k] - U[k];
+            const float up = flush((float)U[0]);
+            u[s.axis[e]][s.node[e]] = up;
+            w_corr += s_e * (U[nn - 1] - (double)up);
+        }
+        s.w_corr = w_corr;
+    }
+
+    // energy (src/engine/sheet.rs:1052-1083), edge by edge.
+    double sheet_energy(const Sheet& s) const {
+        double w = 0.0;
+        for (size_t e = 0; e < s.axis.size(); ++e) {
+            const size_t nn = s.nn[e], k0 = s.k0[e], ka = s.a0[e];
+            const double* U = s.u.data() + s.n0[e];
+            const double* H = s.h.data() + s.l0[e];
+            for (size_t k = 0; k < nn; ++k) w += 0.25 * s.two_c[k0 + k] * dt * U[k] * U[k];
+            const double stored = U[0];
+            w -= 0.5 * s.c_edge[e] * stored * stored;
+            for (size_t j = 0; j + 1 < nn; ++j) {
+                const double l = dt / (2.0 * s.a[ka + j]);
+                w += 0.5 * l * H[j] * H[j];
+            }
+        }
+        return w + s.w_corr;
     }
 
     // ---- serial hooks
@@ -666,6 +754,7 @@ struct oracle_engine {
         for (Op& op : ops) {
             if (op.kind == EMS_OP_SOURCE) source_apply(op.source, true);
             else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, true);
+            else if (op.kind == EMS_OP_SHEET) sheet_post_h(op.sheet);
         }
         for (Op& op : ops) {
             if (op.kind == EMS_OP_LUMPED) lumped_pre_e(op.lumped);
@@ -694,6 +783,7 @@ struct oracle_engine {
             else if (op.kind == EMS_OP_MUR) mur_post_e(op.mur);
             else if (op.kind == EMS_OP_SOURCE) source_apply(op.source, false);
             else if (op.kind == EMS_OP_PROBE) probe_sample(op.probe, false);
+            else if (op.kind == EMS_OP_SHEET) sheet_post_e(op.sheet);
         }
         ++step;
     }
@@ -900,6 +990,53 @@ int oracle_create(const ems_engine_desc* d, int threads, oracle_engine** out) {
             M.last.assign(m->n, 0.0f);
             break;
         }
+        case EMS_OP_SHEET: {
+            const auto* st = (const ems_sheet*)t;
+            Sheet& S = op.sheet;
+            const size_t ne = st->n_edges, nc = st->n_couplings;
+            S.axis = vec(st->axis, ne);
+            S.node = vec(st->node, ne);
+            S.nn = vec(st->nn, ne);
+            S.k0 = vec(st->konst0, ne);
+            S.a0 = vec(st->a0, ne);
+            S.c_edge = vec(st->c_edge, ne);
+            S.c_axis = vec(st->c_axis, nc);
+            S.c_node = vec(st->c_node, nc);
+            S.w_up = vec(st->w_up, nc);
+            S.w_dn = vec(st->w_dn, nc);
+            S.corr = vec(st->corr, nc);
+            S.ecorr = vec(st->ecorr, nc);
+            S.two_c = vec(st->two_c, st->n_konst);
+            S.cp = vec(st->cp, st->n_konst);
+            S.inv_den = vec(st->inv_den, st->n_konst);
+            S.a = vec(st->a, st->n_a);
+            uint32_t nodes_total = 0, layers_total = 0, c = 0, max_nn = 0;
+            for (size_t q = 0; q < ne; ++q) {
+                const uint32_t nn = S.nn[q], end = st->coupling_end[q];
+                if (nn < 2 || S.axis[q] > 2 || S.node[q] >= e->n || end < c || end > nc ||
+                    S.k0[q] + (size_t)nn > st->n_konst || S.a0[q] + (size_t)nn - 1 > st->n_a) {
+                    delete e;
+                    return EMS_ERR_INVALID;
+                }
+                S.c0.push_back(c);
+                S.c1.push_back(end);
+                c = end;
+                S.n0.push_back(nodes_total);
+                S.l0.push_back(layers_total);
+                nodes_total += nn;
+                layers_total += nn - 1;
+                max_nn = std::max(max_nn, nn);
+            }
+            for (size_t q = 0; q < nc; ++q)
+                if (S.c_axis[q] > 2 || S.c_node[q] >= e->n) {
+                    delete e;
+                    return EMS_ERR_INVALID;
+                }
+            S.u.assign(nodes_total, 0.0);
+            S.h.assign(layers_total, 0.0);
+            S.x.assign(max_nn, 0.0);
+            break;
+        }
         default:
             delete e;
             return EMS_ERR_INVALID;
@@ -976,6 +1113,68 @@ int oracle_upload_field(oracle_engine* e, int field, int axis, const float* host
     return EMS_OK;
 }
 
+int oracle_sample(oracle_engine* e, const ems_sampler* s, double* out) {
+    if (!e || !s || !out) return EMS_ERR_INVALID;
+    const uint64_t nd[3] = {e->nx, e->ny, e->nz};
+    const bool cur = s->quantity == EMS_DUMP_H || s->quantity == EMS_DUMP_B || s->quantity == EMS_DUMP_ROTH;
+    const bool roth = s->quantity == EMS_DUMP_ROTH;
+    const auto& F = cur ? e->i : e->u;
+    auto get = [&](int c, const uint64_t p[3]) -> double { return (double)F[c][(p[0] * e->ny + p[1]) * e->nz + p[2]]; };
+    // circulation (src/engine/dump.rs:814-834): i around the primary edge c.
+    auto circ = [&](int c, const uint64_t p[3]) {
+        const int a = (c + 1) % 3, b = (c + 2) % 3;
+        double v = get(b, p) - get(a, p);
+        if (p[a] > 0) {
+            uint64_t q[3] = {p[0], p[1], p[2]};
+            q[a] -= 1;
+            v -= get(b, q);
+        }
+        if (p[b] > 0) {
+            uint64_t q[3] = {p[0], p[1], p[2]};
+            q[b] -= 1;
+            v += get(a, q);
+        }
+        return v;
+    };
+    const uint64_t* dims = s->dims;
+    const uint64_t off[3] = {0, 3 * dims[0], 3 * (dims[0] + dims[1])};
+    const uint64_t vol = s->fac_dims[0] * s->fac_dims[1] * s->fac_dims[2];
+    for (int a = 0; a < 3; ++a)
+        for (uint64_t q = 0; q < 6 * dims[a]; ++q)
+            if (s->tap_w[2 * off[a] + q] != 0.0 && s->tap_idx[2 * off[a] + q] >= nd[a]) return EMS_ERR_INVALID;
+    size_t at = 0;
+    for (uint64_t p = 0; p < dims[0]; ++p)
+        for (uint64_t q = 0; q < dims[1]; ++q)
+            for (uint64_t r = 0; r < dims[2]; ++r, ++at)
+                for (int c = 0; c < 3; ++c) {
+                    const uint64_t ex = 2 * (off[0] + c * dims[0] + p), ey = 2 * (off[1] + c * dims[1] + q),
+                                   ez = 2 * (off[2] + c * dims[2] + r);
+                    double v = 0.0;
+                    for (int tx = 0; tx < 2; ++tx) {
+                        const double wx = s->tap_w[ex + tx];
+                        if (wx == 0.0) continue;
+                        for (int ty = 0; ty < 2; ++ty) {
+                            const double wy = s->tap_w[ey + ty];
+                            if (wy == 0.0) continue;
+                            for (int tz = 0; tz < 2; ++tz) {
+                                const double wz = s->tap_w[ez + tz];
+                                if (wz == 0.0) continue;
+                                const uint64_t node[3] = {s->tap_idx[ex + tx], s->tap_idx[ey + ty], s->tap_idx[ez + tz]};
+                                const double x = roth ? circ(c, node) : get(c, node);
+                                double m = 1.0;
+                                if (s->factors)
+                                    m = s->factors[c * vol + ((node[0] - s->fac_lo[0]) * s->fac_dims[1] +
+                                                              (node[1] - s->fac_lo[1])) * s->fac_dims[2] +
+                                                   (node[2] - s->fac_lo[2])];
+                                v += wx * wy * wz * m * x;
+                            }
+                        }
+                    }
+                    out[3 * at + c] = v;
+                }
+    return EMS_OK;
+}
+
 int oracle_samples(oracle_engine* e, size_t op, int which, double* out, size_t cap, size_t* n) {
     if (!e || !n || op >= e->ops.size()) return EMS_ERR_INVALID;
     const Op& o = e->ops[op];
@@ -984,6 +1183,8 @@ int oracle_samples(oracle_engine* e, size_t op, int which, double* out, size_t c
     else if (o.kind == EMS_OP_LUMPED && which == 0) v = &o.lumped.rec;
     else if (o.kind == EMS_OP_LUMPED && which == 1) v = &o.lumped.port_v;
     else if (o.kind == EMS_OP_LUMPED && which == 2) v = &o.lumped.port_i;
+    else if (o.kind == EMS_OP_SHEET && which == 0) v = &o.sheet.u;
+    else if (o.kind == EMS_OP_SHEET && which == 1) v = &o.sheet.h;
     else return EMS_ERR_INVALID;
     *n = v->size();
     if (out) std::memcpy(out, v->data(), std::min(cap, v->size()) * sizeof(double));

@@ -42,6 +42,9 @@ int oracle_step_with_energy(oracle_engine* e, double* energy);
 int oracle_download_field(oracle_engine* e, int field, int axis, float* host);
 int oracle_upload_field(oracle_engine* e, int field, int axis, const float* host);
 int oracle_samples(oracle_engine* e, size_t op, int which, double* out, size_t cap, size_t* n);
+/* The current state sampled by `s` (FieldSampler::sample_with,
+ * src/engine/dump.rs:836-906): 3 values per point, z fastest. */
+int oracle_sample(oracle_engine* e, const ems_sampler* s, double* out);
 
 #ifdef __cplusplus
 }
