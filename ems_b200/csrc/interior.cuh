@@ -28,6 +28,15 @@ constexpr unsigned kInRows = 7;     // rows a block updates (warp 0 computes the
 constexpr unsigned kInWarps = kInRows + 1;
 constexpr unsigned kInQuads = 31;   // quads of z-nodes a warp updates (lane 0 computes the quad below them)
 constexpr unsigned kInPlanes = 32;  // default planes a block marches through
+constexpr unsigned kInPrefetch = 2; // planes ahead whose old fields are prefetched into L2
+
+__device__ __forceinline__ void l2_prefetch(const float* p) {
+#ifndef EMS_HOST_EMULATION
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+#else
+    (void)p;
+#endif
+}
 
 // H of the quad (i, j, k0..k0+3) from the old fields (uo, io) and the old u
 // of the quad, for a quad whose nodes all have their H and E edges (interior
@@ -94,6 +103,18 @@ __global__ void __launch_bounds__(32 * kInWarps, 3) k_interior(const __grid_cons
     for (uint32_t i = xs; i < xe; ++i) {
         const uint32_t par = (i - xs) & 1u;
         const uint32_t idx = i * si + j * sj + k0;
+        // The old fields of the plane kInPrefetch ahead into L2, so that the
+        // loads of the next planes (and this plane's reads of plane i + 1)
+        // wait for L2 rather than for DRAM.
+        if ((owner || provide) && i + kInPrefetch < g.nx) {
+            const uint32_t pf = idx + kInPrefetch * si;
+            l2_prefetch(P.uo[0] + pf);
+            l2_prefetch(P.uo[1] + pf);
+            l2_prefetch(P.uo[2] + pf);
+            l2_prefetch(P.io[0] + pf);
+            l2_prefetch(P.io[1] + pf);
+            l2_prefetch(P.io[2] + pf);
+        }
         Q4 ux, uy, uz, hx, hy, hz;
         if (owner || (provide && !outside)) {
             interior_h<OE>(P, i, j, k0, ux, uy, uz, hx, hy, hz);

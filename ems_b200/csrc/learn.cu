@@ -1,12 +1,12 @@
 // learn.cu — kernels of the learned early stop (include/ems_learn.h), sm_100a.
 //
 // A small 1-D CNN (convolutions as im2col + GEMM, then two dense layers)
-// trained and run on these kernels. The GEMM is a bf16 tensor-core kernel
-// (mma.sync m16n8k16, f32 accumulation): 64×64 output tiles, four warps of
-// 32×32, K in steps of 32 staged in shared memory. The matrices here are
-// small (≤ 10^4 rows, ≤ 2·10^3 columns), so the kernel takes A and B with
-// arbitrary element strides (a transposed operand is just other strides),
-// which keeps the backward pass free of transpose copies.
+// trained and run on these kernels. The GEMM runs on the tcgen05 tensor
+// cores (bf16 operands from shared memory, f32 accumulator in tensor
+// memory). The matrices here are small (≤ 10^5 rows, ≤ 2·10^3 columns), so
+// the kernel takes A and B with arbitrary element strides (a transposed
+// operand is just other strides), which keeps the backward pass free of
+// transpose copies.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -16,86 +16,169 @@
 
 namespace {
 
-constexpr int GM = 64, GN = 64, GK = 32, GPAD = 8;
+// The GEMM C = alpha·A·B + beta·C on the fifth-generation tensor cores:
+// one CTA of four warps per 128×128 tile of C, the f32 accumulator in
+// tensor memory (128 lanes × 128 columns), K in chunks of 64. The four
+// warps stage each chunk of A (128×64) and B (64×128) in shared memory in
+// the no-swizzle K-major core-matrix layout: 8 rows × 8 bf16 (16 bytes per
+// row) per core matrix, [k/8][row][8], so that the core matrices of one row
+// group lie 128 bytes apart (stride offset) and the two K halves of one
+// K=16 step M·16 bytes apart (leading offset). One elected thread issues
+// four tcgen05.mma (M 128, N 128, K 16, bf16 in, f32 out) and commits them
+// to an mbarrier; the CTA waits on it (bounded) before reusing the buffers.
+// Operands are read with arbitrary element strides (a transposed operand
+// is other strides), zero outside the matrix.
+constexpr int TM = 128, TN = 128, TK = 64;
+constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTileBytesA = TM * TK * 2, kTileBytesB = TN * TK * 2;
+// A, B, the barrier, the tensor-memory address; padded so at most three
+// CTAs share an SM (3 × 128 tensor-memory columns of the 512).
+constexpr uint32_t kGemmSmem = 64 * 1024;
+constexpr uint64_t kGemmWaitNs = 1000000000ull;
 
-__device__ __forceinline__ uint16_t bf16_bits(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ int g_learn_fail = 0;
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
-__global__ void __launch_bounds__(128) k_gemm(const uint16_t* __restrict__ A, int64_t sa0, int64_t sa1,
-                                              const uint16_t* __restrict__ B, int64_t sb0, int64_t sb1, float* C,
-                                              int64_t ldc, int M, int N, int K, float alpha, float beta) {
-    // As[m][k] (row-major A tile), Bs[n][k] (B tile stored column by column,
-    // the layout of the MMA's "col" operand); rows padded against bank conflicts.
-    __shared__ __align__(16) uint16_t As[GM][GK + GPAD];
-    __shared__ __align__(16) uint16_t Bs[GN][GK + GPAD];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int e = tid; e < GM * GK; e += 128) {
-            const int r = e / GK, c = e - r * GK;
-            const int i = m0 + r, k = k0 + c;
-            As[r][c] = (i < M && k < K) ? A[i * sa0 + k * sa1] : (uint16_t)0;
-        }
-        for (int e = tid; e < GN * GK; e += 128) {
-            const int r = e / GK, c = e - r * GK;  // r: column n, c: k
-            const int j = n0 + r, k = k0 + c;
-            Bs[r][c] = (j < N && k < K) ? B[k * sb0 + j * sb1] : (uint16_t)0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GK; kk += 16) {
-            uint32_t af[2][4], bf[4][2];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                const int r = wm + mi * 16 + g;
-                af[mi][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + t * 2]);
-                af[mi][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + t * 2]);
-                af[mi][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 8 + t * 2]);
-                af[mi][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 8 + t * 2]);
-            }
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) {
-                const int n = wn + ni * 8 + g;
-                bf[ni][0] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + t * 2]);
-                bf[ni][1] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 8 + t * 2]);
-            }
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], af[mi], bf[ni]);
-        }
-        __syncthreads();
+// Waits for phase `parity`; false after kGemmWaitNs.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    const uint64_t t0 = now_ns();
+    for (uint32_t it = 0;; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 63u) == 63u && now_ns() - t0 > kGemmWaitNs) return false;
     }
+}
+
+// Shared-memory matrix descriptor, no swizzle: start, leading and stride
+// byte offsets in 16-byte units, version 1 (bits 46-47).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: f32 accumulator (bits 4-5 = 1), A
+// and B bf16 (bits 7-9, 10-12 = 1), both K-major, N/8 at bit 17, M/16 at 24.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                            ((uint32_t)(TM >> 4) << 24);
+
+__global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t* __restrict__ A, int64_t sa0, int64_t sa1,
+                                                 const uint16_t* __restrict__ B, int64_t sb0, int64_t sb1, float* C,
+                                                 int64_t ldc, int M, int N, int K, float alpha, float beta) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint16_t* As = reinterpret_cast<uint16_t*>(smem);
+    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + kTileBytesA);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTileBytesA + kTileBytesB);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTileBytesA + kTileBytesB + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    const int chunks = (K + TK - 1) / TK;
+    for (int ch = 0; ch < chunks; ++ch) {
+        const int k0 = ch * TK;
+        // Stage the chunk: element (r, c) of a 128×64 tile at [c/8][r][c%8].
+        for (int e = tid; e < TM * TK; e += 128) {
+            const int r = e / TK, c = e - r * TK;
+            const int i = m0 + r, k = k0 + c;
+            As[((c >> 3) * TM + r) * 8 + (c & 7)] = (i < M && k < K) ? A[i * sa0 + k * sa1] : (uint16_t)0;
+        }
+        for (int e = tid; e < TN * TK; e += 128) {
+            const int r = e / TK, c = e - r * TK;  // r: column n of C, c: k
+            const int j = n0 + r, k = k0 + c;
+            Bs[((c >> 3) * TN + r) * 8 + (c & 7)] = (j < N && k < K) ? B[k * sb0 + j * sb1] : (uint16_t)0;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+            for (int s = 0; s < TK / 16; ++s) {
+                const uint64_t da = smem_desc(a0 + s * 2 * TM * 16, TM * 16, 128);
+                const uint64_t db = smem_desc(b0 + s * 2 * TN * 16, TN * 16, 128);
+                const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(bar))
+                         : "memory");
+        }
+        if (!bar_wait(bar, (uint32_t)(ch & 1))) ok = false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    // The epilogue's tensor-memory loads are warp-collective: every thread
+    // takes the same branch.
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok && tid == 0) atomicExch(&g_learn_fail, 1);
+    if (ok) {
+        // Warp w reads tensor-memory lanes 32w..32w+31: row 32w + lane of the tile.
+        const int i = m0 + warp * 32 + lane;
+        for (int cb = 0; cb < TN; cb += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(taddr)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (i < M) {
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int i = m0 + wm + mi * 16 + g + (c >= 2 ? 8 : 0);
-                const int j = n0 + wn + ni * 8 + t * 2 + (c & 1);
-                if (i < M && j < N) {
-                    float* p = C + i * ldc + j;
-                    *p = beta != 0.0f ? alpha * acc[mi][ni][c] + beta * *p : alpha * acc[mi][ni][c];
+                for (int q = 0; q < 16; ++q) {
+                    const int j = n0 + cb + q;
+                    if (j < N) {
+                        float* p = C + i * ldc + j;
+                        const float x = __uint_as_float(v[q]);
+                        *p = beta != 0.0f ? alpha * x + beta * *p : alpha * x;
+                    }
                 }
             }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
 }
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
 
 __global__ void k_to_bf16(const float* src, uint16_t* dst, size_t n) {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -213,10 +296,27 @@ int ems_learn_gemm_bf16(const uint16_t* A, int64_t sa0, int64_t sa1, const uint1
                         float* C, int64_t ldc, int M, int N, int K, float alpha, float beta, void* stream) {
     if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return 1;
     // Element offsets are formed in 64 bits; one grid dimension per tile axis.
-    if ((M + GM - 1) / GM > 65535) return 1;
-    dim3 grid((N + GN - 1) / GN, (M + GM - 1) / GM);
-    k_gemm<<<grid, 128, 0, (cudaStream_t)stream>>>(A, sa0, sa1, B, sb0, sb1, C, ldc, M, N, K, alpha, beta);
+    if ((M + TM - 1) / TM > 65535) return 1;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem) != cudaSuccess)
+            return 2;
+        attr = true;
+    }
+    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
+    k_gemm_tc<<<grid, 128, kGemmSmem, (cudaStream_t)stream>>>(A, sa0, sa1, B, sb0, sb1, C, ldc, M, N, K, alpha, beta);
     return launched();
+}
+
+int ems_learn_check(void) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_learn_fail, sizeof(int)) != cudaSuccess) return 2;
+    if (v) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_learn_fail, &zero, sizeof(int));
+        return 4;
+    }
+    return 0;
 }
 
 int ems_learn_to_bf16(const float* src, uint16_t* dst, size_t n, void* stream) {

@@ -13,15 +13,15 @@ then taken from the live samples followed by the predicted tail.
 
 Layers (channels-last activations, weights W[out][fan_in]):
 
-    conv 2→32, kernel 8, stride 4, SiLU    (K_IN 1024 → 255)
-    conv 32→64, kernel 8, stride 4, SiLU   (255 → 62)
-    conv 64→128, kernel 8, stride 4, SiLU  (62 → 14)
-    dense 1792→64, SiLU
+    conv 2→32, kernel 8, stride 4, SiLU    (K_IN 2048 → 511)
+    conv 32→64, kernel 8, stride 4, SiLU   (511 → 126)
+    conv 64→128, kernel 8, stride 4, SiLU  (126 → 30)
+    dense 3840→64, SiLU
     dense 64→2·T_OUT                       (V then I)
 
-about 0.25 M parameters. Every layer runs on the kernels of
-libems_learn.so (include/ems_learn.h): im2col, the bf16 tensor-core GEMM
-(f32 accumulation), bias + activation, their adjoints, MSE and Adam; the
+about 0.38 M parameters. Every layer runs on the kernels of
+libems_learn.so (include/ems_learn.h): im2col, the bf16 tcgen05
+tensor-core GEMM (f32 accumulator in tensor memory), bias + activation, their adjoints, MSE and Adam; the
 f32 master weights are copied to bf16 for the GEMMs. torch only holds the
 device buffers and the stream.
 """
@@ -36,7 +36,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-K_IN = 1024      # samples of V and I the network reads
+K_IN = 2048      # samples of V and I the network reads
 T_OUT = 384      # predicted samples per signal
 DT_REF = 6.4e-12  # [s] spacing of the input samples
 STRIDE = 16      # spacing of the predicted samples, in DT_REF
@@ -66,6 +66,7 @@ def learn_lib() -> C.CDLL:
             "ems_learn_bias_grad": [p, p, i, i, p],
             "ems_learn_mse": [p, p, p, p, sz, p],
             "ems_learn_adam": [p, p, p, p, p, sz, f, f, f, f, i, p],
+            "ems_learn_check": [],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

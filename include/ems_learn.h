@@ -25,10 +25,17 @@ extern "C" {
 
 /* C[i][j] = alpha * sum_k A(i,k) B(k,j) + beta * C[i][j] with
  * A(i,k) = A[i*sa0 + k*sa1], B(k,j) = B[k*sb0 + j*sb1] (bf16), C f32 with
- * row stride ldc: bf16 tensor-core MMA (m16n8k16), f32 accumulation.
- * beta = 0 ignores C's old contents. Returns 0, or 1 for invalid sizes. */
+ * row stride ldc: tcgen05 tensor-core MMA (bf16 operands staged in shared
+ * memory, f32 accumulator in tensor memory), 128x128 tiles of C.
+ * beta = 0 ignores C's old contents. Returns 0, 1 for invalid sizes or 2
+ * for a launch error; a bounded wait inside the kernel that ran out is
+ * reported by ems_learn_check. */
 int ems_learn_gemm_bf16(const uint16_t* A, int64_t sa0, int64_t sa1, const uint16_t* B, int64_t sb0, int64_t sb1,
                         float* C, int64_t ldc, int M, int N, int K, float alpha, float beta, void* stream);
+
+/* 0, or 4 (and clears the flag) if a GEMM's bounded wait for its tensor-core
+ * work ran out since the last call; 2 if the flag cannot be read. */
+int ems_learn_check(void);
 
 /* dst[q] = bf16(src[q]) for q < n. */
 int ems_learn_to_bf16(const float* src, uint16_t* dst, size_t n, void* stream);

@@ -1,5 +1,6 @@
 """The learned early stop's CUDA kernels (libems_learn.so) against their CPU
-restatements: the bf16 tensor-core GEMM against numpy on bf16-rounded
+restatements: the bf16 tcgen05 tensor-core GEMM (f32 accumulator in tensor
+memory) against numpy on bf16-rounded
 operands, im2col/col2im as adjoints, Adam against its formula, and the
 network's forward pass and gradients against oracle/cnn.py; then a short
 training run that must learn (the loss falls below 40 % of its start)."""
@@ -26,7 +27,9 @@ def _bf16_bits(x):
 
 @pytest.mark.parametrize("M,N,K,trans_a,trans_b,beta", [
     (64, 64, 32, False, False, 0.0), (100, 37, 70, False, True, 0.0), (5, 300, 513, True, False, 0.5),
-    (129, 65, 17, True, True, 1.0), (1, 1, 1, False, False, 0.0)])
+    (129, 65, 17, True, True, 1.0), (1, 1, 1, False, False, 0.0), (128, 128, 64, False, False, 0.0),
+    (16320, 32, 16, False, True, 0.0), (896, 128, 512, False, True, 0.0), (64, 768, 64, True, False, 0.0),
+    (512, 1792, 64, True, False, 1.0)])
 def test_gemm_matches_numpy(M, N, K, trans_a, trans_b, beta):
     t = _torch()
     from ems_b200.learn import learn_lib
@@ -47,6 +50,7 @@ def test_gemm_matches_numpy(M, N, K, trans_a, trans_b, beta):
                                  1.0, beta, None)
     assert st == 0
     t.cuda.synchronize()
+    assert lib.ems_learn_check() == 0
     want = (af.T if trans_a else af) @ (bf.T if trans_b else bf) + beta * c0
     got = Cd.cpu().numpy()
     err = np.max(np.abs(got - want)) / max(1.0, np.max(np.abs(want)))
