@@ -824,7 +824,7 @@ ems_status run_step_sweep(ems_gpu* h, bool energy) {
         const PoleSideDev& ps = side ? poles->poles.h : poles->poles.e;
         const uint32_t e0 = h->chunk_edge[side][ch], e1 = h->chunk_edge[side][ch + 1];
         if (!ps.n_edges || e1 == e0) return;
-        k_poles_blocks<<<blocks_for(e1 - e0, kPoleEdges), kPoleBlock, 0, s>>>(f, c, ps, side ? P.runs_h : P.runs, side ? P.sets_h : P.sets,
+        k_poles_blocks<<<blocks_for(e1 - e0, kPoleBlock), kPoleBlock, 0, s>>>(f, c, ps, side ? P.runs_h : P.runs, side ? P.sets_h : P.sets,
                                                              h->run_of[side], side ? 0 : 1, h->dt,
                                                              h->fold_prev[side] ? 1 : 0, e0, e1);
         ++h->launches;
@@ -995,7 +995,7 @@ ems_status run_step_interior(ems_gpu* h) {
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_POLES && op.poles.e.n_edges) {
-            k_poles_blocks<<<blocks_for(op.poles.e.n_edges, kPoleEdges), kPoleBlock, 0, s>>>(
+            k_poles_blocks<<<blocks_for(op.poles.e.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
                 fb, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, h->fold_prev[0] ? 1 : 0, 0u,
                 (uint32_t)op.poles.e.n_edges);
             ++h->launches;
@@ -1164,7 +1164,7 @@ ems_status run_step_march(ems_gpu* h) {
     // The electric poles on the new fields, u^n read from the old buffer.
     for (auto& op : h->ops)
         if (op.kind == EMS_OP_POLES && op.poles.e.n_edges) {
-            k_poles_blocks<true><<<blocks_for(op.poles.e.n_edges, kPoleEdges), kPoleBlock, 0, s>>>(
+            k_poles_blocks<true><<<blocks_for(op.poles.e.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
                 fb, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, 0, 0u, (uint32_t)op.poles.e.n_edges, fa);
             ++h->launches;
         }
@@ -1261,7 +1261,7 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.h.n_edges && split) {
-                k_poles_blocks<<<blocks_for(op.poles.h.n_edges, kPoleEdges), kPoleBlock, 0, s>>>(
+                k_poles_blocks<<<blocks_for(op.poles.h.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
                     f, c, op.poles.h, P.runs_h, P.sets_h, h->run_of[1], 0, h->dt, h->fold_prev[1] ? 1 : 0, 0u,
                     (uint32_t)op.poles.h.n_edges);
                 ++h->launches;
@@ -1311,7 +1311,7 @@ ems_status run_step(ems_gpu* h, bool energy) {
             }
         } else if (op.kind == EMS_OP_POLES) {
             if (op.poles.e.n_edges && split) {
-                k_poles_blocks<<<blocks_for(op.poles.e.n_edges, kPoleEdges), kPoleBlock, 0, s>>>(
+                k_poles_blocks<<<blocks_for(op.poles.e.n_edges, kPoleBlock), kPoleBlock, 0, s>>>(
                     f, c, op.poles.e, P.runs, P.sets, h->run_of[0], 1, h->dt, h->fold_prev[0] ? 1 : 0, 0u,
                     (uint32_t)op.poles.e.n_edges);
                 ++h->launches;

@@ -135,7 +135,7 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
 
 // Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
 template <bool ENERGY, bool OE = false>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 8) k_split_h(const __grid_constant__ FusedParams P,
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 7) k_split_h(const __grid_constant__ FusedParams P,
                                                                          uint32_t i0) {
     const uint32_t i = i0 + blockIdx.y;
     const double w = split_h_quad<ENERGY, OE>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
@@ -411,111 +411,14 @@ __device__ __forceinline__ void poles_edge(const Fields& f, const Coeffs& c, con
                     old ? (electric ? old->u[ax] : old->i[ax]) : nullptr);
 }
 
-constexpr uint32_t kPoleBlock = 256;            // threads per block
-constexpr uint32_t kPoleEdges = 2 * kPoleBlock;  // edges per block: two per thread
+constexpr uint32_t kPoleBlock = 256;
 
-// Whether the edges of run R take the leapfrog-only path: every pole
-// leapfrog (ems form), at most two, no openEMS pole, no trapezoidal
-// denominator.
-__device__ __forceinline__ bool pole_run_leapfrog(const PoleRun& R) {
-    return R.oe == 0u && R.np >= 1u && R.np <= 2u && R.kinds == (1u << R.np) - 1u && R.sum_inv_z == 0.0;
-}
-
-// Two leapfrog edges of one thread (ea of run A, ez of run Z): every load
-// of both first, so their latencies overlap, then the arithmetic of
-// poles_edge_core's leapfrog branch for each, then the stores.
-// j ← a·j + k_b·(u^n − q/C), q += dt·j, u = u* − cb·Σj (src/engine/
-// dispersive.rs:1392-1470).
-__device__ __forceinline__ void poles_pair_leapfrog(const Fields& f, const Coeffs& c, const PoleSideDev& p,
-                                                    const PoleRun& A, const PoleRun& Z, const double* sets,
-                                                    int electric, double dt, int save_prev, uint32_t ea, uint32_t ez,
-                                                    const float* old_a, const float* old_z) {
-    const uint32_t oa = ea - A.e0, oz = ez - Z.e0;
-    const uint32_t ia = A.node0 + oa, iz = Z.node0 + oz;
-    const uint32_t pa = A.p0 + oa * A.np, pz = Z.p0 + oz * Z.np;
-    float* fa = electric ? f.u[A.axis] : f.i[A.axis];
-    float* fz = electric ? f.u[Z.axis] : f.i[Z.axis];
-    const float* ka = electric ? c.c[3 + A.axis] : c.c[9 + A.axis];
-    const float* kz = electric ? c.c[3 + Z.axis] : c.c[9 + Z.axis];
-    const float pra = old_a ? old_a[ia] : p.prev[ea];
-    const float prz = old_z ? old_z[iz] : p.prev[ez];
-    const float ua = fa[ia], uz = fz[iz];
-    const float cba = ka[ia], cbz = kz[iz];
-    double ja[2], qa[2], jz[2], qz[2];
-    ja[0] = p.j[pa];
-    qa[0] = p.q[pa];
-    jz[0] = p.j[pz];
-    qz[0] = p.q[pz];
-    if (A.np > 1u) {
-        ja[1] = p.j[pa + 1];
-        qa[1] = p.q[pa + 1];
-    }
-    if (Z.np > 1u) {
-        jz[1] = p.j[pz + 1];
-        qz[1] = p.q[pz + 1];
-    }
-    const double* csa = sets + A.set;
-    const double* csz = sets + Z.set;
-    const double preva = (double)pra, prevz = (double)prz;
-    double sa = 0.0, sz = 0.0;
-#pragma unroll
-    for (uint32_t q = 0; q < 2u; ++q) {
-        if (q < A.np) {
-            const double jn = __dadd_rn(__dmul_rn(csa[3 * q], ja[q]),
-                                        __dmul_rn(csa[3 * q + 2], __dsub_rn(preva, __dmul_rn(qa[q], csa[3 * q + 1]))));
-            qa[q] = __dadd_rn(qa[q], __dmul_rn(dt, jn));
-            ja[q] = jn;
-            sa = __dadd_rn(sa, jn);
-        }
-        if (q < Z.np) {
-            const double jn = __dadd_rn(__dmul_rn(csz[3 * q], jz[q]),
-                                        __dmul_rn(csz[3 * q + 2], __dsub_rn(prevz, __dmul_rn(qz[q], csz[3 * q + 1]))));
-            qz[q] = __dadd_rn(qz[q], __dmul_rn(dt, jn));
-            jz[q] = jn;
-            sz = __dadd_rn(sz, jn);
-        }
-    }
-    const float na = (float)__dsub_rn((double)ua, __dmul_rn((double)cba, sa));
-    const float nz = (float)__dsub_rn((double)uz, __dmul_rn((double)cbz, sz));
-    p.j[pa] = ja[0];
-    p.q[pa] = qa[0];
-    if (A.np > 1u) {
-        p.j[pa + 1] = ja[1];
-        p.q[pa + 1] = qa[1];
-    }
-    p.j[pz] = jz[0];
-    p.q[pz] = qz[0];
-    if (Z.np > 1u) {
-        p.j[pz + 1] = jz[1];
-        p.q[pz + 1] = qz[1];
-    }
-    fa[ia] = na;
-    fz[iz] = nz;
-    if (save_prev) {
-        p.prev[ea] = na;
-        p.prev[ez] = nz;
-    }
-}
-
-// The run of edge e among the block's staged runs: sr[lo].e0 <= e < sr[lo + 1].e0.
-__device__ __forceinline__ uint32_t pole_run_find(const PoleRun* sr, uint32_t nr, uint32_t e) {
-    uint32_t lo = 0, hi = nr;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (sr[mid].e0 <= e) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Edges [e0, e1) of the side, kPoleEdges consecutive edges per block, two
-// per thread (e and e + kPoleBlock). The runs covering a block's edges (a
-// contiguous range: a run holds consecutive edges) are staged in shared
-// memory and each edge's node, axis and first pole state derived from its
-// run, so the only per-edge traffic is the field, the saved value and the
-// pole state; pairs of leapfrog edges load all of it before computing.
-// OLD: u^n comes from the old buffer `old` of a two-buffer step instead of
-// the saved values.
+// Edges [e0, e1) of the side, kPoleBlock consecutive edges per block. The
+// runs covering a block's edges (a contiguous range: a run holds
+// consecutive edges) are staged in shared memory and each edge's node, axis
+// and first pole state derived from its run, so the only per-edge traffic
+// is the field, the saved value and the pole state. OLD: u^n comes from the
+// old buffer `old` of a two-buffer step instead of the saved values.
 template <bool OLD = false>
 __global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_constant__ Fields f,
                                                              const __grid_constant__ Coeffs c,
@@ -523,43 +426,30 @@ __global__ void __launch_bounds__(kPoleBlock) k_poles_blocks(const __grid_consta
                                                              const double* sets, const uint32_t* run_of, int electric,
                                                              double dt, int save_prev, uint32_t e0, uint32_t e1,
                                                              const __grid_constant__ Fields old = Fields{}) {
-    EMS_SHARED PoleRun sr[kPoleEdges];
-    const uint32_t eb = e0 + blockIdx.x * kPoleEdges;
+    EMS_SHARED PoleRun sr[kPoleBlock];
+    const uint32_t eb = e0 + blockIdx.x * kPoleBlock;
     if (eb >= e1) return;
-    const uint32_t el = min(eb + kPoleEdges, e1) - 1;
+    const uint32_t el = min(eb + kPoleBlock, e1) - 1;
     const uint32_t r0 = __ldg(run_of + eb), r1 = __ldg(run_of + el);
-    const uint32_t ea = eb + threadIdx.x, ez = ea + kPoleBlock;
-    if (r1 < r0 || r1 - r0 >= kPoleEdges) {  // not a contiguous run range: per edge
-        if (ea <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, ea, OLD ? &old : nullptr);
-        if (ez <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, ez, OLD ? &old : nullptr);
+    const uint32_t e = eb + threadIdx.x;
+    if (r1 < r0 || r1 - r0 >= kPoleBlock) {  // not a contiguous run range: per edge
+        if (e <= el) poles_edge(f, c, p, runs, sets, run_of, electric, dt, save_prev, e, OLD ? &old : nullptr);
         return;
     }
     const uint32_t nr = r1 - r0 + 1;
     for (uint32_t t = threadIdx.x; t < nr; t += kPoleBlock) sr[t] = runs[r0 + t];
     __syncthreads();
-    const bool va = ea <= el, vz = ez <= el;
-    const uint32_t la = va ? pole_run_find(sr, nr, ea) : 0u;
-    const uint32_t lz = vz ? pole_run_find(sr, nr, ez) : 0u;
-    if (va && vz && pole_run_leapfrog(sr[la]) && pole_run_leapfrog(sr[lz])) {
-        const PoleRun& A = sr[la];
-        const PoleRun& Z = sr[lz];
-        poles_pair_leapfrog(f, c, p, A, Z, sets, electric, dt, save_prev, ea, ez,
-                            OLD ? (electric ? old.u[A.axis] : old.i[A.axis]) : nullptr,
-                            OLD ? (electric ? old.u[Z.axis] : old.i[Z.axis]) : nullptr);
-        return;
+    if (e > el) return;
+    uint32_t lo = 0, hi = nr;  // sr[lo].e0 <= e < sr[lo + 1].e0
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sr[mid].e0 <= e) lo = mid;
+        else hi = mid;
     }
-    if (va) {
-        const PoleRun& R = sr[la];
-        const uint32_t off = ea - R.e0;
-        poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, ea, R.node0 + off, (int)R.axis, R.p0 + off * R.np,
-                        OLD ? (electric ? old.u[R.axis] : old.i[R.axis]) : nullptr);
-    }
-    if (vz) {
-        const PoleRun& R = sr[lz];
-        const uint32_t off = ez - R.e0;
-        poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, ez, R.node0 + off, (int)R.axis, R.p0 + off * R.np,
-                        OLD ? (electric ? old.u[R.axis] : old.i[R.axis]) : nullptr);
-    }
+    const PoleRun& R = sr[lo];
+    const uint32_t off = e - R.e0;
+    poles_edge_core(f, c, p, R, sets, electric, dt, save_prev, e, R.node0 + off, (int)R.axis, R.p0 + off * R.np,
+                    OLD ? (electric ? old.u[R.axis] : old.i[R.axis]) : nullptr);
 }
 
 }  // namespace emsk

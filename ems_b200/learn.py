@@ -38,8 +38,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 K_IN = 2048      # samples of V and I the network reads
 T_OUT = 384      # predicted samples per signal
-DT_REF = 6.4e-12  # [s] spacing of the input samples
-STRIDE = 16      # spacing of the predicted samples, in DT_REF
+DT_REF = 6.4e-12  # [s] spacing of the input samples (K_IN of them: 13.1 ns)
+STRIDE = 16      # spacing of the predicted samples, in DT_REF (102.4 ps; 39 ns of ring-down)
 WINDOW = 4 * STRIDE  # verification window after the input, in DT_REF
 CONVS = [(2, 32, 8, 4), (32, 64, 8, 4), (64, 128, 8, 4)]  # (c_in, c_out, kernel, stride)
 HIDDEN = 64
