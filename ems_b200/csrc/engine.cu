@@ -187,6 +187,11 @@ struct ems_gpu {
     }
     // The split schedule: CPML layer shell segments per side (0 H, 1 E).
     ShellDev shell[2] = {};
+    // The split schedule's row CPML (split.cuh row_cpml): the x/y-normal
+    // slabs inside the update kernels over the rows that hold them, a shell
+    // of the z-normal slabs only; off where the plan does not apply.
+    RowCpml rowc;
+    ShellDev shell_z[2] = {};
     // The sweep schedule: x chunks of sweep_planes planes, each chunk's
     // shell boxes (first box, first node) and pole edges (first edge) per
     // side; entry [chunks] closes the last range.
@@ -586,6 +591,41 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
         const uint32_t S = (uint32_t)std::max(2.0, std::min(64.0, std::floor(0.45 * (l2 > 0 ? l2 : 50 << 20) / plane)));
         ems_status st = build_chunks(h, S);
         if (st) return st;
+    }
+    // Row CPML: with the CPML registered before every other slab operator
+    // (its corrections then come first after each update) and no openEMS
+    // PML layers.
+    {
+        bool cpml_first = true, seen_cpml = false;
+        for (size_t k = 0; k < d->n_ops; ++k) {
+            const int kind = d->ops[k].kind;
+            if (kind == EMS_OP_CPML) seen_cpml = true;
+            if ((kind == EMS_OP_POLES || kind == EMS_OP_UPML) && !seen_cpml) cpml_first = false;
+            if (kind == EMS_OP_UPML) cpml_first = false;
+        }
+        h->rowc = RowCpml{};
+        const uint64_t nodes3[3] = {g.nx, g.ny, g.nz};
+        if (seen_cpml && cpml_first) {
+            const RowCpml R = row_cpml_plan(h->slab_geo, h->nslab, nodes3);
+            if (R.ok) {
+                const std::vector<SlabGeo> zs = z_slabs(h->slab_geo);
+                for (int side = 0; side < 2; ++side) {
+                    uint32_t total = 0;
+                    const std::vector<ShellBox> boxes = shell_boxes(zs, h->nslab[side], nodes3, side, &total);
+                    ShellDev& Sd = h->shell_z[side];
+                    Sd = ShellDev{};
+                    Sd.n_box = (uint32_t)boxes.size();
+                    Sd.total = total;
+                    if (Sd.n_box) {
+                        Sd.box = h->upload(boxes.data(), boxes.size());
+                        const std::vector<uint32_t> win = shell_windows(boxes, total);
+                        Sd.first_box = h->upload(win.data(), win.size());
+                        if (!Sd.box || !Sd.first_box) return fail(h, EMS_ERR_NOMEM, "CPML z shell");
+                    }
+                }
+                h->rowc = R;
+            }
+        }
     }
     // The sweep needs no magnetic sources or conducting sheets (their serial
     // post_h hooks would sit between a chunk's H and E updates) and no
@@ -1185,6 +1225,44 @@ ems_status run_step_march(ems_gpu* h) {
 
 // One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
+// One update of the split schedule with the row CPML (h->rowc): the CPML
+// variant of the update kernel over the planes [0, x_lo) and [x_hi, nx) and,
+// in the planes between, over the rows [0, y_lo) and [y_hi, ny); the plain
+// kernel over the other rows. Quads are numbered row by row within a plane,
+// so each part is a contiguous range of the plane's quads (QuadMap mode 0).
+template <int SIDE>
+void launch_split_rows(ems_gpu* h, const FusedParams& P0, bool oe, cudaStream_t s) {
+    const Grid& g = h->g;
+    const RowCpml& R = h->rowc;
+    const uint32_t qpr = g.pitch >> 2;
+    const uint32_t xl = R.x_lo[SIDE], xh = R.x_hi[SIDE], yl = R.y_lo[SIDE], yh = R.y_hi[SIDE];
+    auto go = [&](bool cpml, uint32_t i0, uint32_t planes, uint32_t q0, uint32_t count) {
+        if (!planes || !count) return;
+        FusedParams P = P0;
+        P.qmap = QuadMap{0u, q0, 0u, 0u, 0u, 0u, count};
+        const dim3 grd(blocks_for(count, kSplitThreads), planes, 1);
+        if (SIDE == 0) {
+            if (cpml && oe) k_split_h<false, true, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else if (cpml) k_split_h<false, false, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else if (oe) k_split_h<false, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else k_split_h<false><<<grd, kSplitThreads, 0, s>>>(P, i0);
+        } else {
+            if (cpml && oe) k_split_e<true, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else if (cpml) k_split_e<false, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else if (oe) k_split_e<true><<<grd, kSplitThreads, 0, s>>>(P, i0);
+            else k_split_e<<<grd, kSplitThreads, 0, s>>>(P, i0);
+        }
+        ++h->launches;
+    };
+    const uint32_t all = g.ny * qpr;
+    go(true, 0u, xl, 0u, all);
+    go(true, xh, g.nx - xh, 0u, all);
+    const uint32_t mid = xh > xl ? xh - xl : 0u;
+    go(true, xl, mid, 0u, yl * qpr);
+    go(true, xl, mid, yh * qpr, (g.ny - yh) * qpr);
+    go(false, xl, mid, yl * qpr, (yh > yl ? yh - yl : 0u) * qpr);
+}
+
 ems_status run_step(ems_gpu* h, bool energy) {
     const int sch = active_schedule(h);
     // Only the per-operator, split and sweep steps keep the electric saved values.
@@ -1220,7 +1298,12 @@ ems_status run_step(ems_gpu* h, bool energy) {
     const dim3 qgrd(split_blocks_x(g), g.nx, 1);
     cudaEvent_t ev = h->prof_begin();
     const bool oe = h->oe_curl;
-    if (split) {
+    // The row CPML: split schedule, steps without energy.
+    const bool rows = sch == 4 && !energy && h->rowc.ok;
+    if (rows) {
+        launch_split_rows<0>(h, P, oe, s);
+        --h->launches;  // counted per launch inside; one is added below
+    } else if (split) {
         if (energy) {
             if (oe) k_split_h<true, true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
             else k_split_h<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
@@ -1248,8 +1331,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
     // Slab hooks after the H update, in registration order.
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML && split) {
-            if (const uint32_t nb = shell_blocks(h->shell[0])) {
-                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[0]);
+            const ShellDev& Sh = rows ? h->shell_z[0] : h->shell[0];
+            if (const uint32_t nb = shell_blocks(Sh)) {
+                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, Sh);
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_CPML) {
@@ -1287,7 +1371,10 @@ ems_status run_step(ems_gpu* h, bool energy) {
     st = serial_pre_e(h, f);
     if (st) return st;
     ev = h->prof_begin();
-    if (split) {
+    if (rows) {
+        launch_split_rows<1>(h, P, oe, s);
+        --h->launches;
+    } else if (split) {
         if (oe) k_split_e<true><<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
         else k_split_e<<<qgrd, kSplitThreads, 0, s>>>(P, 0u);
     } else {
@@ -1298,8 +1385,9 @@ ems_status run_step(ems_gpu* h, bool energy) {
     ++h->launches;
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML && split) {
-            if (const uint32_t nb = shell_blocks(h->shell[1])) {
-                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[1]);
+            const ShellDev& Se = rows ? h->shell_z[1] : h->shell[1];
+            if (const uint32_t nb = shell_blocks(Se)) {
+                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, Se);
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_CPML) {

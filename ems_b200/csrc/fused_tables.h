@@ -284,12 +284,13 @@ inline FusedTables build_fused_tables(const ems_engine_desc* d, uint32_t pitch) 
 struct SlabGeo {
     int side, comp, q;
     uint32_t lo[3], hi[3];
+    int normal;
 };
 
 inline std::vector<SlabGeo> slab_geometry(const FusedTables& T) {
     std::vector<SlabGeo> out;
     for (const FusedSlabSpec& sp : T.slabs) {
-        SlabGeo g{sp.side, sp.comp, sp.q, {}, {}};
+        SlabGeo g{sp.side, sp.comp, sp.q, {}, {}, (int)sp.src->normal};
         for (int a = 0; a < 3; ++a) {
             g.lo[a] = (uint32_t)sp.src->lo[a];
             g.hi[a] = (uint32_t)sp.src->hi[a];
@@ -340,6 +341,7 @@ inline std::vector<ShellBox> shell_boxes(const std::vector<SlabGeo>& slabs, cons
                     uint32_t cnt = 0, list = 0;
                     for (int q = 0; valid && q < (int)by[c].size(); ++q) {
                         const SlabGeo* sl = by[c][q];
+                        if (!sl) continue;  // a slab left out of this shell
                         bool in = true;
                         for (int a = 0; a < 3; ++a) in = in && sl->lo[a] <= lo[a] && hi[a] <= sl->hi[a];
                         if (!in) continue;
@@ -359,6 +361,64 @@ inline std::vector<ShellBox> shell_boxes(const std::vector<SlabGeo>& slabs, cons
                 out.push_back(B);
             }
     *total = (uint32_t)sum;
+    return out;
+}
+
+// The split schedule's row CPML (split.cuh row_cpml): the slabs normal to x
+// or y are applied by the update kernels to the rows they hold, the z-normal
+// ones by a shell over the z-layer nodes. Valid when, for every side and
+// component, no z-normal slab comes before an x- or y-normal one (so the
+// chain keeps its order). Fills, per side, the planes [0, x_lo) ∪ [x_hi, nx)
+// and, of the other planes, the rows [0, y_lo) ∪ [y_hi, ny) that hold an x-
+// or y-normal slab of that side (the update's CPML variant runs over them).
+struct RowCpml {
+    bool ok = false;
+    uint32_t x_lo[2] = {0, 0}, x_hi[2] = {0, 0}, y_lo[2] = {0, 0}, y_hi[2] = {0, 0};
+};
+
+inline RowCpml row_cpml_plan(const std::vector<SlabGeo>& slabs, const int nslab[2][3], const uint64_t nodes[3]) {
+    RowCpml R;
+    for (int side = 0; side < 2; ++side) {
+        for (int c = 0; c < 3; ++c) {
+            std::vector<int> normal(nslab[side][c], -1);
+            for (const SlabGeo& sp : slabs)
+                if (sp.side == side && sp.comp == c) normal[sp.q] = sp.normal;
+            bool seen_z = false;
+            for (int nq : normal) {
+                if (nq < 0) return R;
+                if (nq == 2) seen_z = true;
+                else if (seen_z) return R;
+            }
+        }
+        uint32_t xl = 0, xh = (uint32_t)nodes[0], yl = 0, yh = (uint32_t)nodes[1];
+        for (const SlabGeo& sp : slabs) {
+            if (sp.side != side || sp.normal == 2) continue;
+            const int a = sp.normal;
+            const uint32_t n = (uint32_t)nodes[a];
+            uint32_t& lo = a == 0 ? xl : yl;
+            uint32_t& hi = a == 0 ? xh : yh;
+            // A low-face layer starts at 0, a high-face one ends at the last
+            // node or its padding; one that does neither is not a face layer.
+            if (sp.lo[a] == 0) lo = std::max(lo, sp.hi[a]);
+            else if (sp.hi[a] + 1 >= n) hi = std::min(hi, sp.lo[a]);
+            else return R;
+        }
+        if (xl > xh) xl = xh;
+        if (yl > yh) yl = yh;
+        R.x_lo[side] = xl;
+        R.x_hi[side] = xh;
+        R.y_lo[side] = yl;
+        R.y_hi[side] = yh;
+    }
+    R.ok = true;
+    return R;
+}
+
+// The slabs of `slabs` normal to z.
+inline std::vector<SlabGeo> z_slabs(const std::vector<SlabGeo>& slabs) {
+    std::vector<SlabGeo> out;
+    for (const SlabGeo& sp : slabs)
+        if (sp.normal == 2) out.push_back(sp);
     return out;
 }
 

@@ -70,13 +70,44 @@ __device__ __forceinline__ bool quad_of(const Grid& g, uint32_t q, uint32_t& j, 
     return k0 < g.nz;
 }
 
+// The CPML corrections of component C of the quad (i, j, k0..k0+3) by the
+// slabs normal to x or y that hold the row, in the slabs' order, applied to
+// the updated values t before they are stored (mask bit e: node e has the
+// component): the part of the chain cpml_body applies, on the curl
+// differences the update just formed (s = A or −B by the slab's normal). The
+// z-normal slabs come after them in every list (checked at set-up) and run
+// in the shell kernel over the z-layer nodes only.
+template <int SIDE, int C>
+__device__ __forceinline__ void row_cpml(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k0, uint32_t mask,
+                                         Q4& t, const Q4& coef, const Q4& A, const Q4& B) {
+    constexpr uint32_t na = (C + 1) % 3;
+    const int n = P.nslab[SIDE][C];
+    for (int q = 0; q < n; ++q) {
+        const FSlab& s = P.slab[SIDE][C][q];
+        if (s.normal == 2u || i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1]) continue;
+        const uint32_t d = s.normal == 0u ? i - s.lo[0] : j - s.lo[1];
+        const float b = __ldg(s.b + d), a = __ldg(s.a + d), kk = __ldg(s.k + d);
+        const uint32_t base = ((i - s.lo[0]) * (s.hi[1] - s.lo[1]) + (j - s.lo[1])) * (s.hi[2] - s.lo[2]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t k = k0 + e;
+            if (!((mask >> e) & 1u) || k < s.lo[2] || k >= s.hi[2]) continue;
+            const uint32_t at = base + (k - s.lo[2]);
+            const float sv = s.normal == na ? A.v[e] : __fmul_rn(-1.0f, B.v[e]);
+            const float psi = flush(__fadd_rn(__fmul_rn(b, s.psi_old[at]), __fmul_rn(a, sv)));
+            s.psi_new[at] = psi;
+            t.v[e] = flush(__fadd_rn(t.v[e], __fmul_rn(coef.v[e], __fadd_rn(__fmul_rn(kk, sv), psi))));
+        }
+    }
+}
+
 // H update of every dual edge (src/engine/kernel.rs:447-511, 571-618), four
 // z-nodes per thread; with ENERGY each block writes its share of the energy
 // invariant in units of dt/4 (src/engine/kernel.rs:132-244). Entries the
 // update does not write (edges that do not exist, row padding) are stored
 // back as read. OE: openEMS's summation order. Grid: (quads of a plane /
 // kSplitThreads, nx).
-template <bool ENERGY, bool OE>
+template <bool ENERGY, bool OE, bool ROWCPML = false>
 __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
@@ -126,6 +157,40 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
                 if (in_ && jn) w = __dadd_rn(w, weight(daz.v[e], __dmul_rn((double)hz.v[e], (double)nz_.v[e]), dbz.v[e]));
             }
         }
+        if (ROWCPML) {
+            // The curl differences of the shell kernel's H side (shell_node).
+            Q4 A, B;
+            uint32_t mx = 0, my = 0, mz = 0;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t k = k0 + e;
+                const bool kn = k + 1 < g.nz;
+                mx |= (jn && kn ? 1u : 0u) << e;
+                my |= (in_ && kn ? 1u : 0u) << e;
+                mz |= (in_ && jn && k < g.nz ? 1u : 0u) << e;
+            }
+            const Q4 mdbx{{-dbx.v[0], -dbx.v[1], -dbx.v[2], -dbx.v[3]}};
+            const Q4 mdby{{-dby.v[0], -dby.v[1], -dby.v[2], -dby.v[3]}};
+            const Q4 mdbz{{-dbz.v[0], -dbz.v[1], -dbz.v[2], -dbz.v[3]}};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                A.v[e] = __fsub_rn(uzj.v[e], uz.v[e]);
+                B.v[e] = __fsub_rn(e < 3 ? uy.v[e + 1] : uy4, uy.v[e]);
+            }
+            row_cpml<0, 0>(P, i, j, k0, mx, nx_, mdbx, A, B);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                A.v[e] = __fsub_rn(e < 3 ? ux.v[e + 1] : ux4, ux.v[e]);
+                B.v[e] = __fsub_rn(uzi.v[e], uz.v[e]);
+            }
+            row_cpml<0, 1>(P, i, j, k0, my, ny_, mdby, A, B);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                A.v[e] = __fsub_rn(uyi.v[e], uy.v[e]);
+                B.v[e] = __fsub_rn(uxj.v[e], ux.v[e]);
+            }
+            row_cpml<0, 2>(P, i, j, k0, mz, nz_, mdbz, A, B);
+        }
         if (jn) stq(P.in[0] + idx, nx_);
         if (in_) stq(P.in[1] + idx, ny_);
         if (in_ && jn) stq(P.in[2] + idx, nz_);
@@ -134,11 +199,11 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
 }
 
 // Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
-template <bool ENERGY, bool OE = false>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 7) k_split_h(const __grid_constant__ FusedParams P,
-                                                                         uint32_t i0) {
+template <bool ENERGY, bool OE = false, bool ROWCPML = false>
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : (ROWCPML ? 4 : 7)) k_split_h(
+    const __grid_constant__ FusedParams P, uint32_t i0) {
     const uint32_t i = i0 + blockIdx.y;
-    const double w = split_h_quad<ENERGY, OE>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
+    const double w = split_h_quad<ENERGY, OE, ROWCPML>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
         if (threadIdx.x == 0) P.partials[(size_t)i * gridDim.x + blockIdx.x] = s;
@@ -148,7 +213,7 @@ __global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : 7) k_split_h(const
 // E update of every edge (src/engine/kernel.rs:624-697), four z-nodes per
 // thread; OE: openEMS's summation order. Grid: (quads of a plane /
 // kSplitThreads, nx).
-template <bool OE>
+template <bool OE, bool ROWCPML = false>
 __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, uint32_t q) {
     const Grid& g = P.g;
     uint32_t j = 0, k0 = 0;
@@ -176,14 +241,45 @@ __device__ __forceinline__ void split_e_quad(const FusedParams& P, uint32_t i, u
         if (yj) ny_.v[e] = e_upd_t<OE>(cay.v[e], ey.v[e], cby.v[e], ix.v[e], ix0, iz.v[e], izi.v[e]);
         if (k + 1 < g.nz) nz_.v[e] = e_upd_t<OE>(caz.v[e], ez.v[e], cbz.v[e], iy.v[e], iyi.v[e], ix.v[e], ixj.v[e]);
     }
+    if (ROWCPML) {
+        // The curl differences of the shell kernel's E side (shell_node).
+        Q4 A, B;
+        uint32_t mx = 0, my = 0, mz = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t k = k0 + e;
+            mx |= (xi && k < g.nz ? 1u : 0u) << e;
+            my |= (yj && k < g.nz ? 1u : 0u) << e;
+            mz |= (k + 1 < g.nz ? 1u : 0u) << e;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            A.v[e] = __fsub_rn(iz.v[e], izj.v[e]);
+            B.v[e] = __fsub_rn(iy.v[e], e > 0 ? iy.v[e - 1] : iym);
+        }
+        row_cpml<1, 0>(P, i, j, k0, mx, nx_, cbx, A, B);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            A.v[e] = __fsub_rn(ix.v[e], e > 0 ? ix.v[e - 1] : ixm);
+            B.v[e] = __fsub_rn(iz.v[e], izi.v[e]);
+        }
+        row_cpml<1, 1>(P, i, j, k0, my, ny_, cby, A, B);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            A.v[e] = __fsub_rn(iy.v[e], iyi.v[e]);
+            B.v[e] = __fsub_rn(ix.v[e], ixj.v[e]);
+        }
+        row_cpml<1, 2>(P, i, j, k0, mz, nz_, cbz, A, B);
+    }
     if (xi) stq(P.un[0] + idx, nx_);
     if (yj) stq(P.un[1] + idx, ny_);
     stq(P.un[2] + idx, nz_);
 }
 
-template <bool OE = false>
-__global__ void __launch_bounds__(kSplitThreads, 7) k_split_e(const __grid_constant__ FusedParams P, uint32_t i0) {
-    split_e_quad<OE>(P, i0 + blockIdx.y, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
+template <bool OE = false, bool ROWCPML = false>
+__global__ void __launch_bounds__(kSplitThreads, ROWCPML ? 4 : 7) k_split_e(const __grid_constant__ FusedParams P,
+                                                                         uint32_t i0) {
+    split_e_quad<OE, ROWCPML>(P, i0 + blockIdx.y, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
 }
 
 // Blocks of the split update kernels: (quads of a plane / kSplitThreads) × nx.

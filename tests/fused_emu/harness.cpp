@@ -370,7 +370,21 @@ static bool emu_launch(unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsig
 // updates, one CPML shell kernel per side) from the fields given in reference
 // layout (overwritten with the result); models without dispersive media,
 // lumped elements or sources (those hooks are the per-operator kernels).
+static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, double* energies, bool rows);
+
 extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** fields, double* energies) {
+    return split_run(d, steps, fields, energies, false);
+}
+
+// The same with the row CPML of the engine's split steps (launch_split_rows
+// in engine.cu): the update kernels' CPML variant over the x-layer planes
+// and y-layer rows, the plain one elsewhere, then the z-slab shell. Steps
+// without energy (the engine's energy steps take the full shell).
+extern "C" int emu_split_rows_run(const ems_engine_desc* d, uint64_t steps, float** fields) {
+    return split_run(d, steps, fields, nullptr, true);
+}
+
+static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, double* energies, bool rows) {
     g_err[0] = 0;
     for (size_t k = 0; k < d->n_ops; ++k)
         if (d->ops[k].kind != EMS_OP_CPML && d->ops[k].kind != EMS_OP_PROBE) {
@@ -433,15 +447,47 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
     std::vector<ShellBox> st[2];
     std::vector<uint32_t> win[2];
     ShellDev sd[2];
+    RowCpml R;
+    if (rows) {
+        int ns[2][3];
+        for (int a = 0; a < 2; ++a)
+            for (int c = 0; c < 3; ++c) ns[a][c] = T.nslab[a][c];
+        R = row_cpml_plan(slab_geometry(T), ns, d->nodes);
+        if (!R.ok) {
+            std::snprintf(g_err, sizeof g_err, "row CPML plan does not apply");
+            return 1;
+        }
+    }
     for (int side = 0; side < 2; ++side) {
         uint32_t total = 0;
-        st[side] = shell_boxes(T, d->nodes, side, &total);
+        st[side] = rows ? shell_boxes(z_slabs(slab_geometry(T)), T.nslab[side], d->nodes, side, &total)
+                        : shell_boxes(T, d->nodes, side, &total);
         win[side] = shell_windows(st[side], total);
         sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u, win[side].data()};
     }
     const unsigned gx = split_blocks_x(g);
     std::vector<double> partials((size_t)gx * g.nx, 0.0);
     P.partials = partials.data();
+    // launch_split_rows of engine.cu, emulated.
+    auto rows_update = [&](int side) -> bool {
+        const uint32_t qpr = g.pitch >> 2;
+        const uint32_t xl = R.x_lo[side], xh = R.x_hi[side], yl = R.y_lo[side], yh = R.y_hi[side];
+        auto go = [&](bool cpml, uint32_t i0, uint32_t planes, uint32_t q0, uint32_t count) -> bool {
+            if (!planes || !count) return true;
+            FusedParams Q = P;
+            Q.qmap = QuadMap{0u, q0, 0u, 0u, 0u, 0u, count};
+            const unsigned bx = (count + kSplitThreads - 1) / kSplitThreads;
+            if (side == 0)
+                return cpml ? emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_h<false, false, true>(Q, i0); })
+                            : emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_h<false>(Q, i0); });
+            return cpml ? emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_e<false, true>(Q, i0); })
+                        : emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_e(Q, i0); });
+        };
+        const uint32_t all = g.ny * qpr, mid = xh > xl ? xh - xl : 0u;
+        return go(true, 0u, xl, 0u, all) && go(true, xh, g.nx - xh, 0u, all) && go(true, xl, mid, 0u, yl * qpr) &&
+               go(true, xl, mid, yh * qpr, (g.ny - yh) * qpr) &&
+               go(false, xl, mid, yl * qpr, (yh > yl ? yh - yl : 0u) * qpr);
+    };
     auto shell = [&](int side) -> bool {
         const uint32_t blocks = shell_blocks(sd[side]);
         if (!blocks) return true;
@@ -450,6 +496,10 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
                     : emu_launch(blocks, 1, 1, 32 * kShellWarps, 1, [&] { k_shell<0>(P, S); });
     };
     for (uint64_t s = 0; s < steps; ++s) {
+        if (rows) {
+            if (!rows_update(0) || !shell(0) || !rows_update(1) || !shell(1)) return 2;
+            continue;
+        }
         bool ok = energies ? emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<true>(P, 0u); })
                            : emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<false>(P, 0u); });
         if (!ok || !shell(0)) return 2;
