@@ -187,11 +187,10 @@ struct ems_gpu {
     }
     // The split schedule: CPML layer shell segments per side (0 H, 1 E).
     ShellDev shell[2] = {};
-    // The split schedule's row CPML (split.cuh row_cpml): the x/y-normal
-    // slabs inside the update kernels over the rows that hold them, a shell
-    // of the z-normal slabs only; off where the plan does not apply.
+    // The split schedule's row CPML (split.cuh row_cpml): every slab's
+    // correction inside the update kernels' CPML variant over the quads that
+    // hold layer nodes, no shell kernel; off where the plan does not apply.
     RowCpml rowc;
-    ShellDev shell_z[2] = {};
     // The sweep schedule: x chunks of sweep_planes planes, each chunk's
     // shell boxes (first box, first node) and pole edges (first edge) per
     // side; entry [chunks] closes the last range.
@@ -603,29 +602,8 @@ ems_status setup_fused(ems_gpu* h, const ems_engine_desc* d) {
             if ((kind == EMS_OP_POLES || kind == EMS_OP_UPML) && !seen_cpml) cpml_first = false;
             if (kind == EMS_OP_UPML) cpml_first = false;
         }
-        h->rowc = RowCpml{};
         const uint64_t nodes3[3] = {g.nx, g.ny, g.nz};
-        if (seen_cpml && cpml_first) {
-            const RowCpml R = row_cpml_plan(h->slab_geo, h->nslab, nodes3);
-            if (R.ok) {
-                const std::vector<SlabGeo> zs = z_slabs(h->slab_geo);
-                for (int side = 0; side < 2; ++side) {
-                    uint32_t total = 0;
-                    const std::vector<ShellBox> boxes = shell_boxes(zs, h->nslab[side], nodes3, side, &total);
-                    ShellDev& Sd = h->shell_z[side];
-                    Sd = ShellDev{};
-                    Sd.n_box = (uint32_t)boxes.size();
-                    Sd.total = total;
-                    if (Sd.n_box) {
-                        Sd.box = h->upload(boxes.data(), boxes.size());
-                        const std::vector<uint32_t> win = shell_windows(boxes, total);
-                        Sd.first_box = h->upload(win.data(), win.size());
-                        if (!Sd.box || !Sd.first_box) return fail(h, EMS_ERR_NOMEM, "CPML z shell");
-                    }
-                }
-                h->rowc = R;
-            }
-        }
+        h->rowc = (seen_cpml && cpml_first) ? row_cpml_plan(h->slab_geo, nodes3) : RowCpml{};
     }
     // The sweep needs no magnetic sources or conducting sheets (their serial
     // post_h hooks would sit between a chunk's H and E updates) and no
@@ -1226,21 +1204,25 @@ ems_status run_step_march(ems_gpu* h) {
 // One step through the per-operator kernels; energy: record the
 // invariant's field part into d_energy[0].
 // One update of the split schedule with the row CPML (h->rowc): the CPML
-// variant of the update kernel over the planes [0, x_lo) and [x_hi, nx) and,
-// in the planes between, over the rows [0, y_lo) and [y_hi, ny); the plain
-// kernel over the other rows. Quads are numbered row by row within a plane,
-// so each part is a contiguous range of the plane's quads (QuadMap mode 0).
+// variant of the update kernel over every quad that holds a layer node of
+// the side (the x-layer planes whole; in the other planes the y-layer rows
+// whole and, of the rows between, the quads at both ends that reach into
+// the z layers), the plain kernel over the rest. Quads are numbered row by
+// row within a plane: QuadMap mode 0 takes a range of a plane's quads, mode
+// 1 the quads [0, zl) and [zr, ...) of each of a range of rows (zl = 0: the
+// quads from zr on).
 template <int SIDE>
 void launch_split_rows(ems_gpu* h, const FusedParams& P0, bool oe, cudaStream_t s) {
     const Grid& g = h->g;
     const RowCpml& R = h->rowc;
-    const uint32_t qpr = g.pitch >> 2;
-    const uint32_t xl = R.x_lo[SIDE], xh = R.x_hi[SIDE], yl = R.y_lo[SIDE], yh = R.y_hi[SIDE];
-    auto go = [&](bool cpml, uint32_t i0, uint32_t planes, uint32_t q0, uint32_t count) {
-        if (!planes || !count) return;
+    const uint32_t qpr = g.pitch >> 2, qrow = (g.nz + 3u) / 4u;
+    const uint32_t xl = R.lo[SIDE][0], xh = R.hi[SIDE][0], yl = R.lo[SIDE][1], yh = R.hi[SIDE][1];
+    const uint32_t zl = (R.lo[SIDE][2] + 3u) / 4u, zr = std::max(zl, R.hi[SIDE][2] / 4u);
+    auto go = [&](bool cpml, uint32_t i0, uint32_t planes, const QuadMap& M) {
+        if (!planes || !M.count) return;
         FusedParams P = P0;
-        P.qmap = QuadMap{0u, q0, 0u, 0u, 0u, 0u, count};
-        const dim3 grd(blocks_for(count, kSplitThreads), planes, 1);
+        P.qmap = M;
+        const dim3 grd(blocks_for(M.count, kSplitThreads), planes, 1);
         if (SIDE == 0) {
             if (cpml && oe) k_split_h<false, true, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
             else if (cpml) k_split_h<false, false, true><<<grd, kSplitThreads, 0, s>>>(P, i0);
@@ -1254,13 +1236,14 @@ void launch_split_rows(ems_gpu* h, const FusedParams& P0, bool oe, cudaStream_t 
         }
         ++h->launches;
     };
-    const uint32_t all = g.ny * qpr;
-    go(true, 0u, xl, 0u, all);
-    go(true, xh, g.nx - xh, 0u, all);
-    const uint32_t mid = xh > xl ? xh - xl : 0u;
-    go(true, xl, mid, 0u, yl * qpr);
-    go(true, xl, mid, yh * qpr, (g.ny - yh) * qpr);
-    go(false, xl, mid, yl * qpr, (yh > yl ? yh - yl : 0u) * qpr);
+    const uint32_t mid = xh > xl ? xh - xl : 0u, rows = yh > yl ? yh - yl : 0u;
+    const uint32_t ends = zl + (qrow > zr ? qrow - zr : 0u), inner = zr - zl;
+    go(true, 0u, xl, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, g.ny * qpr});
+    go(true, xh, g.nx - xh, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, g.ny * qpr});
+    go(true, xl, mid, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, yl * qpr});
+    go(true, xl, mid, QuadMap{0u, yh * qpr, 0u, 0u, 0u, 0u, (g.ny - yh) * qpr});
+    go(true, xl, mid, QuadMap{1u, 0u, yl, ends, zl, zr, rows * ends});
+    go(false, xl, mid, QuadMap{1u, 0u, yl, inner, 0u, zl, rows * inner});
 }
 
 ems_status run_step(ems_gpu* h, bool energy) {
@@ -1331,9 +1314,8 @@ ems_status run_step(ems_gpu* h, bool energy) {
     // Slab hooks after the H update, in registration order.
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML && split) {
-            const ShellDev& Sh = rows ? h->shell_z[0] : h->shell[0];
-            if (const uint32_t nb = shell_blocks(Sh)) {
-                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, Sh);
+            if (const uint32_t nb = rows ? 0u : shell_blocks(h->shell[0])) {
+                k_shell<0><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[0]);
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_CPML) {
@@ -1385,9 +1367,8 @@ ems_status run_step(ems_gpu* h, bool energy) {
     ++h->launches;
     for (auto& op : h->ops) {
         if (op.kind == EMS_OP_CPML && split) {
-            const ShellDev& Se = rows ? h->shell_z[1] : h->shell[1];
-            if (const uint32_t nb = shell_blocks(Se)) {
-                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, Se);
+            if (const uint32_t nb = rows ? 0u : shell_blocks(h->shell[1])) {
+                k_shell<1><<<nb, 32 * kShellWarps, 0, s>>>(P, h->shell[1]);
                 ++h->launches;
             }
         } else if (op.kind == EMS_OP_CPML) {

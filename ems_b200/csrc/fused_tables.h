@@ -364,62 +364,37 @@ inline std::vector<ShellBox> shell_boxes(const std::vector<SlabGeo>& slabs, cons
     return out;
 }
 
-// The split schedule's row CPML (split.cuh row_cpml): the slabs normal to x
-// or y are applied by the update kernels to the rows they hold, the z-normal
-// ones by a shell over the z-layer nodes. Valid when, for every side and
-// component, no z-normal slab comes before an x- or y-normal one (so the
-// chain keeps its order). Fills, per side, the planes [0, x_lo) ∪ [x_hi, nx)
-// and, of the other planes, the rows [0, y_lo) ∪ [y_hi, ny) that hold an x-
-// or y-normal slab of that side (the update's CPML variant runs over them).
+// The split schedule's row CPML (split.cuh row_cpml): the update kernels'
+// CPML variant applies every slab's correction itself over the quads that
+// hold layer nodes, so no shell kernel runs. Per side: the planes [0, x_lo)
+// and [x_hi, nx), the rows [0, y_lo) and [y_hi, ny) and the z-nodes [0, z_lo)
+// and [z_hi, nz) hold the slabs normal to x, y and z (every slab lies on a
+// face: it starts at 0 or ends at the last node or its padding).
 struct RowCpml {
     bool ok = false;
-    uint32_t x_lo[2] = {0, 0}, x_hi[2] = {0, 0}, y_lo[2] = {0, 0}, y_hi[2] = {0, 0};
+    uint32_t lo[2][3] = {}, hi[2][3] = {};
 };
 
-inline RowCpml row_cpml_plan(const std::vector<SlabGeo>& slabs, const int nslab[2][3], const uint64_t nodes[3]) {
+inline RowCpml row_cpml_plan(const std::vector<SlabGeo>& slabs, const uint64_t nodes[3]) {
     RowCpml R;
-    for (int side = 0; side < 2; ++side) {
-        for (int c = 0; c < 3; ++c) {
-            std::vector<int> normal(nslab[side][c], -1);
-            for (const SlabGeo& sp : slabs)
-                if (sp.side == side && sp.comp == c) normal[sp.q] = sp.normal;
-            bool seen_z = false;
-            for (int nq : normal) {
-                if (nq < 0) return R;
-                if (nq == 2) seen_z = true;
-                else if (seen_z) return R;
-            }
+    for (int side = 0; side < 2; ++side)
+        for (int a = 0; a < 3; ++a) {
+            R.lo[side][a] = 0;
+            R.hi[side][a] = (uint32_t)nodes[a];
         }
-        uint32_t xl = 0, xh = (uint32_t)nodes[0], yl = 0, yh = (uint32_t)nodes[1];
-        for (const SlabGeo& sp : slabs) {
-            if (sp.side != side || sp.normal == 2) continue;
-            const int a = sp.normal;
-            const uint32_t n = (uint32_t)nodes[a];
-            uint32_t& lo = a == 0 ? xl : yl;
-            uint32_t& hi = a == 0 ? xh : yh;
-            // A low-face layer starts at 0, a high-face one ends at the last
-            // node or its padding; one that does neither is not a face layer.
-            if (sp.lo[a] == 0) lo = std::max(lo, sp.hi[a]);
-            else if (sp.hi[a] + 1 >= n) hi = std::min(hi, sp.lo[a]);
-            else return R;
-        }
-        if (xl > xh) xl = xh;
-        if (yl > yh) yl = yh;
-        R.x_lo[side] = xl;
-        R.x_hi[side] = xh;
-        R.y_lo[side] = yl;
-        R.y_hi[side] = yh;
+    for (const SlabGeo& sp : slabs) {
+        const int a = sp.normal, side = sp.side;
+        if (a < 0 || a > 2 || side < 0 || side > 1) return RowCpml{};
+        const uint32_t n = (uint32_t)nodes[a];
+        if (sp.lo[a] == 0) R.lo[side][a] = std::max(R.lo[side][a], sp.hi[a]);
+        else if (sp.hi[a] + 1 >= n) R.hi[side][a] = std::min(R.hi[side][a], sp.lo[a]);
+        else return RowCpml{};
     }
+    for (int side = 0; side < 2; ++side)
+        for (int a = 0; a < 3; ++a)
+            if (R.lo[side][a] > R.hi[side][a]) R.lo[side][a] = R.hi[side][a];
     R.ok = true;
     return R;
-}
-
-// The slabs of `slabs` normal to z.
-inline std::vector<SlabGeo> z_slabs(const std::vector<SlabGeo>& slabs) {
-    std::vector<SlabGeo> out;
-    for (const SlabGeo& sp : slabs)
-        if (sp.normal == 2) out.push_back(sp);
-    return out;
 }
 
 inline std::vector<ShellBox> shell_boxes(const FusedTables& T, const uint64_t nodes[3], int side, uint32_t* total,

@@ -70,13 +70,13 @@ __device__ __forceinline__ bool quad_of(const Grid& g, uint32_t q, uint32_t& j, 
     return k0 < g.nz;
 }
 
-// The CPML corrections of component C of the quad (i, j, k0..k0+3) by the
-// slabs normal to x or y that hold the row, in the slabs' order, applied to
-// the updated values t before they are stored (mask bit e: node e has the
-// component): the part of the chain cpml_body applies, on the curl
-// differences the update just formed (s = A or −B by the slab's normal). The
-// z-normal slabs come after them in every list (checked at set-up) and run
-// in the shell kernel over the z-layer nodes only.
+// The CPML corrections of component C of the quad (i, j, k0..k0+3), applied
+// to the updated values t before they are stored (mask bit e: node e has the
+// component): for every slab of the side and component that holds the node,
+// in the slabs' order, the chain of cpml_body on the curl differences the
+// update just formed (s = A or −B by the slab's normal). The update kernels'
+// CPML variant runs it over every quad that holds a layer node, so no shell
+// kernel follows them.
 template <int SIDE, int C>
 __device__ __forceinline__ void row_cpml(const FusedParams& P, uint32_t i, uint32_t j, uint32_t k0, uint32_t mask,
                                          Q4& t, const Q4& coef, const Q4& A, const Q4& B) {
@@ -84,19 +84,18 @@ __device__ __forceinline__ void row_cpml(const FusedParams& P, uint32_t i, uint3
     const int n = P.nslab[SIDE][C];
     for (int q = 0; q < n; ++q) {
         const FSlab& s = P.slab[SIDE][C][q];
-        if (s.normal == 2u || i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1]) continue;
-        const uint32_t d = s.normal == 0u ? i - s.lo[0] : j - s.lo[1];
-        const float b = __ldg(s.b + d), a = __ldg(s.a + d), kk = __ldg(s.k + d);
+        if (i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1]) continue;
         const uint32_t base = ((i - s.lo[0]) * (s.hi[1] - s.lo[1]) + (j - s.lo[1])) * (s.hi[2] - s.lo[2]);
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const uint32_t k = k0 + e;
             if (!((mask >> e) & 1u) || k < s.lo[2] || k >= s.hi[2]) continue;
+            const uint32_t d = s.normal == 0u ? i - s.lo[0] : (s.normal == 1u ? j - s.lo[1] : k - s.lo[2]);
             const uint32_t at = base + (k - s.lo[2]);
             const float sv = s.normal == na ? A.v[e] : __fmul_rn(-1.0f, B.v[e]);
-            const float psi = flush(__fadd_rn(__fmul_rn(b, s.psi_old[at]), __fmul_rn(a, sv)));
+            const float psi = flush(__fadd_rn(__fmul_rn(__ldg(s.b + d), s.psi_old[at]), __fmul_rn(__ldg(s.a + d), sv)));
             s.psi_new[at] = psi;
-            t.v[e] = flush(__fadd_rn(t.v[e], __fmul_rn(coef.v[e], __fadd_rn(__fmul_rn(kk, sv), psi))));
+            t.v[e] = flush(__fadd_rn(t.v[e], __fmul_rn(coef.v[e], __fadd_rn(__fmul_rn(__ldg(s.k + d), sv), psi))));
         }
     }
 }

@@ -377,9 +377,9 @@ extern "C" int emu_split_run(const ems_engine_desc* d, uint64_t steps, float** f
 }
 
 // The same with the row CPML of the engine's split steps (launch_split_rows
-// in engine.cu): the update kernels' CPML variant over the x-layer planes
-// and y-layer rows, the plain one elsewhere, then the z-slab shell. Steps
-// without energy (the engine's energy steps take the full shell).
+// in engine.cu): the update kernels' CPML variant over every quad holding a
+// layer node, the plain one elsewhere, no shell. Steps without energy (the
+// engine's energy steps take the shell).
 extern "C" int emu_split_rows_run(const ems_engine_desc* d, uint64_t steps, float** fields) {
     return split_run(d, steps, fields, nullptr, true);
 }
@@ -449,10 +449,7 @@ static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, d
     ShellDev sd[2];
     RowCpml R;
     if (rows) {
-        int ns[2][3];
-        for (int a = 0; a < 2; ++a)
-            for (int c = 0; c < 3; ++c) ns[a][c] = T.nslab[a][c];
-        R = row_cpml_plan(slab_geometry(T), ns, d->nodes);
+        R = row_cpml_plan(slab_geometry(T), d->nodes);
         if (!R.ok) {
             std::snprintf(g_err, sizeof g_err, "row CPML plan does not apply");
             return 1;
@@ -460,8 +457,7 @@ static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, d
     }
     for (int side = 0; side < 2; ++side) {
         uint32_t total = 0;
-        st[side] = rows ? shell_boxes(z_slabs(slab_geometry(T)), T.nslab[side], d->nodes, side, &total)
-                        : shell_boxes(T, d->nodes, side, &total);
+        st[side] = shell_boxes(T, d->nodes, side, &total);
         win[side] = shell_windows(st[side], total);
         sd[side] = ShellDev{st[side].data(), (uint32_t)st[side].size(), total, 0u, win[side].data()};
     }
@@ -470,23 +466,28 @@ static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, d
     P.partials = partials.data();
     // launch_split_rows of engine.cu, emulated.
     auto rows_update = [&](int side) -> bool {
-        const uint32_t qpr = g.pitch >> 2;
-        const uint32_t xl = R.x_lo[side], xh = R.x_hi[side], yl = R.y_lo[side], yh = R.y_hi[side];
-        auto go = [&](bool cpml, uint32_t i0, uint32_t planes, uint32_t q0, uint32_t count) -> bool {
-            if (!planes || !count) return true;
+        const uint32_t qpr = g.pitch >> 2, qrow = (g.nz + 3u) / 4u;
+        const uint32_t xl = R.lo[side][0], xh = R.hi[side][0], yl = R.lo[side][1], yh = R.hi[side][1];
+        const uint32_t zl = (R.lo[side][2] + 3u) / 4u, zr = std::max(zl, R.hi[side][2] / 4u);
+        auto go = [&](bool cpml, uint32_t i0, uint32_t planes, const QuadMap& M) -> bool {
+            if (!planes || !M.count) return true;
             FusedParams Q = P;
-            Q.qmap = QuadMap{0u, q0, 0u, 0u, 0u, 0u, count};
-            const unsigned bx = (count + kSplitThreads - 1) / kSplitThreads;
+            Q.qmap = M;
+            const unsigned bx = (M.count + kSplitThreads - 1) / kSplitThreads;
             if (side == 0)
                 return cpml ? emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_h<false, false, true>(Q, i0); })
                             : emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_h<false>(Q, i0); });
             return cpml ? emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_e<false, true>(Q, i0); })
                         : emu_launch(bx, planes, 1, kSplitThreads, 1, [&] { k_split_e(Q, i0); });
         };
-        const uint32_t all = g.ny * qpr, mid = xh > xl ? xh - xl : 0u;
-        return go(true, 0u, xl, 0u, all) && go(true, xh, g.nx - xh, 0u, all) && go(true, xl, mid, 0u, yl * qpr) &&
-               go(true, xl, mid, yh * qpr, (g.ny - yh) * qpr) &&
-               go(false, xl, mid, yl * qpr, (yh > yl ? yh - yl : 0u) * qpr);
+        const uint32_t mid = xh > xl ? xh - xl : 0u, nrows = yh > yl ? yh - yl : 0u;
+        const uint32_t ends = zl + (qrow > zr ? qrow - zr : 0u), inner = zr - zl;
+        return go(true, 0u, xl, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, g.ny * qpr}) &&
+               go(true, xh, g.nx - xh, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, g.ny * qpr}) &&
+               go(true, xl, mid, QuadMap{0u, 0u, 0u, 0u, 0u, 0u, yl * qpr}) &&
+               go(true, xl, mid, QuadMap{0u, yh * qpr, 0u, 0u, 0u, 0u, (g.ny - yh) * qpr}) &&
+               go(true, xl, mid, QuadMap{1u, 0u, yl, ends, zl, zr, nrows * ends}) &&
+               go(false, xl, mid, QuadMap{1u, 0u, yl, inner, 0u, zl, nrows * inner});
     };
     auto shell = [&](int side) -> bool {
         const uint32_t blocks = shell_blocks(sd[side]);
@@ -497,7 +498,7 @@ static int split_run(const ems_engine_desc* d, uint64_t steps, float** fields, d
     };
     for (uint64_t s = 0; s < steps; ++s) {
         if (rows) {
-            if (!rows_update(0) || !shell(0) || !rows_update(1) || !shell(1)) return 2;
+            if (!rows_update(0) || !rows_update(1)) return 2;
             continue;
         }
         bool ok = energies ? emu_launch(gx, g.nx, 1, kSplitThreads, 1, [&] { k_split_h<true>(P, 0u); })

@@ -178,13 +178,15 @@ def test_split_source_equals_oracle(n, graded):
 
 
 @pytest.mark.parametrize("n,graded,faces", [((10, 9, 12), False, None), ((12, 11, 35), True, None),
-                                             ((14, 13, 18), True, [3, 2, 4, 3, 2, 3]), ((9, 14, 40), False, [0, 3, 2, 0, 3, 3])])
+                                             ((14, 13, 18), True, [3, 2, 4, 3, 2, 3]), ((9, 14, 40), False, [0, 3, 2, 0, 3, 3]),
+                                             ((8, 9, 7), False, [2, 2, 2, 2, 1, 1]), ((11, 8, 6), True, [1, 0, 2, 1, 3, 3])])
 def test_split_rows_source_equals_oracle(n, graded, faces):
-    """The split schedule with the row CPML: the x- and y-normal slabs applied
-    inside the update kernels' CPML variant over the x-layer planes and the
-    y-layer rows, the plain kernel elsewhere, the z-normal slabs in the shell
-    after them (corners of two and three layers, faces without a layer).
-    Fields bit-exact against the oracle."""
+    """The split schedule with the row CPML: every slab's correction applied
+    inside the update kernels' CPML variant over the quads holding layer
+    nodes (x-layer planes, y-layer rows, the z-layer quads at the row ends),
+    the plain kernel elsewhere, no shell (corners of two and three layers,
+    faces without a layer, z layers that overlap inside one quad). Fields
+    bit-exact against the oracle."""
     m = model(n, E.TRAPEZOIDAL, poles=False, graded=graded, cpml=0)
     m.add_cpml(faces or [3, 4, 3, 0, 3, 3], kappa_max=1.5, alpha_max=0.02)
     state = random_state(m, seed=5)
