@@ -435,8 +435,12 @@ def run_ours(args):
         kname, (kms, kn) = "sweep_chunks", kern[0]
         per_launch = ab["total"]
     else:
+        # The H update: 36 B per cell; with the H half of ψ where the CPML
+        # runs inside it (the two-kernel schedule; the split schedule's row
+        # CPML, timed as one span over its launches).
         kname, (kms, kn) = ("step_h" if schedule == 3 else "update_h"), kern[0]
-        per_launch = 36.0 * ab["cells"] + (0.5 * ab["psi"] if schedule == 3 else 0.0)
+        inside = schedule == 3 or (schedule == 4 and eng.row_cpml)
+        per_launch = 36.0 * ab["cells"] + (0.5 * ab["psi"] if inside else 0.0)
     achieved = per_launch / (kms * 1e-3 / kn) / 1e9 if kn else None
     step_gbs = ab["total"] / (ms * 1e-3 / args.steps) / 1e9 / (world)
     traffic = profile_traffic(kname)

@@ -279,6 +279,8 @@ GPU_SYMBOLS = {
     "ems_gpu_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ems_gpu_interior_box": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_row_cpml": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ems_gpu_set_row_cpml": (C.c_int, [C.c_void_p, C.c_int]),
     "ems_energy_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
     "ems_gpu_last_sample": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
@@ -857,6 +859,17 @@ class Engine:
         v = C.c_int()
         self._ck(self._lib.ems_gpu_schedule(self._h, C.byref(v)))
         return v.value
+
+    def set_row_cpml(self, on: bool) -> None:
+        """The split schedule's row CPML on or off (``ems_gpu_set_row_cpml``)."""
+        self._ck(self._lib.ems_gpu_set_row_cpml(self._h, int(on)))
+
+    @property
+    def row_cpml(self) -> bool:
+        """Whether split steps apply the CPML inside the update kernels (no shell kernel)."""
+        v = C.c_int()
+        self._ck(self._lib.ems_gpu_row_cpml(self._h, C.byref(v)))
+        return bool(v.value)
 
     @property
     def interior_box(self) -> tuple:

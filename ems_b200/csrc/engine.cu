@@ -189,8 +189,10 @@ struct ems_gpu {
     ShellDev shell[2] = {};
     // The split schedule's row CPML (split.cuh row_cpml): every slab's
     // correction inside the update kernels' CPML variant over the quads that
-    // hold layer nodes, no shell kernel; off where the plan does not apply.
+    // hold layer nodes, no shell kernel; used when switched on
+    // (ems_gpu_set_row_cpml) and the plan applies.
     RowCpml rowc;
+    bool row_cpml_on = false;
     // The sweep schedule: x chunks of sweep_planes planes, each chunk's
     // shell boxes (first box, first node) and pole edges (first edge) per
     // side; entry [chunks] closes the last range.
@@ -1282,7 +1284,7 @@ ems_status run_step(ems_gpu* h, bool energy) {
     cudaEvent_t ev = h->prof_begin();
     const bool oe = h->oe_curl;
     // The row CPML: split schedule, steps without energy.
-    const bool rows = sch == 4 && !energy && h->rowc.ok;
+    const bool rows = sch == 4 && !energy && h->rowc.ok && h->row_cpml_on;
     if (rows) {
         launch_split_rows<0>(h, P, oe, s);
         --h->launches;  // counted per launch inside; one is added below
@@ -2491,6 +2493,21 @@ ems_status ems_gpu_set_sweep_planes(ems_gpu* h, uint32_t planes) {
 ems_status ems_gpu_schedule(const ems_gpu* h, int* active) {
     if (!h || !active) return EMS_ERR_INVALID;
     *active = active_schedule(h);
+    return EMS_OK;
+}
+
+ems_status ems_gpu_row_cpml(const ems_gpu* h, int* on) {
+    if (!h || !on) return EMS_ERR_INVALID;
+    *on = h->tables_ok && h->rowc.ok && h->row_cpml_on ? 1 : 0;
+    return EMS_OK;
+}
+
+ems_status ems_gpu_set_row_cpml(ems_gpu* h, int on) {
+    if (!h) return EMS_ERR_INVALID;
+    if (on && !(h->tables_ok && h->rowc.ok))
+        return fail(h, EMS_ERR_INVALID, "row CPML unavailable (no CPML, a slab operator registered before it, "
+                                        "openEMS PML layers, or a slab off the faces)");
+    h->row_cpml_on = on != 0;
     return EMS_OK;
 }
 

@@ -199,7 +199,7 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
 
 // Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
 template <bool ENERGY, bool OE = false, bool ROWCPML = false>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : (ROWCPML ? 4 : 7)) k_split_h(
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : (ROWCPML ? 4 : 8)) k_split_h(
     const __grid_constant__ FusedParams P, uint32_t i0) {
     const uint32_t i = i0 + blockIdx.y;
     const double w = split_h_quad<ENERGY, OE, ROWCPML>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));

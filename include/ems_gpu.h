@@ -404,6 +404,17 @@ ems_status ems_gpu_schedule(const ems_gpu* h, int* active);
  * that schedule. */
 ems_status ems_gpu_interior_box(ems_gpu* h, uint32_t box[6]);
 
+/* The row CPML of the split schedule: steps without energy apply the CPML
+ * corrections inside the update kernels (a CPML variant of each update over
+ * the quads that hold layer nodes, no shell kernel) instead of the shell
+ * kernels; identical results. Off by default (on B200 it measures slower
+ * than the shells on the 512^3 dispersive box). ems_gpu_set_row_cpml
+ * returns EMS_ERR_INVALID for on = 1 where it does not apply (no CPML, a
+ * slab operator registered before the CPML, openEMS PML layers, a slab off
+ * the faces); ems_gpu_row_cpml reports whether steps use it. */
+ems_status ems_gpu_set_row_cpml(ems_gpu* h, int on);
+ems_status ems_gpu_row_cpml(const ems_gpu* h, int* on);
+
 /* The order in which the H and E updates sum the four terms of an edge's
  * circulation (CurlOrder, src/engine/kernel.rs:81-108): 0 the reference's
  * default (a - b) - (c - d); 1 openEMS's, ((a - b) + d) - c for H and

@@ -193,6 +193,57 @@ def test_dispersive_box_chunks_and_tiles(n, schedule):
     np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
 
 
+def _row_cpml_model(n, faces):
+    m = E.Model.uniform([n, n + 3, n + 7], [0.5e-3] * 3)
+    sph = m.cells().sphere([n / 2, n / 2, n / 2], n / 6)
+    m.fill(sph, m.material(eps_r=2.0))
+    m.build()
+    m.add_cpml(faces)
+    d = E.Dispersive()
+    d.fill_cells(m, sph, W.lorentz_poles(3))
+    m.add_dispersive(d, E.LEAPFROG)
+    amp = np.array([np.exp(-(((s + 0.5) * m.dt - 30e-12) / 10e-12) ** 2) for s in range(200)])
+    m.add_source_table(E.SOFT_E, [(E.X, (n // 3, n // 2, n // 2), 1.0), (E.Z, (n // 2, 2, n // 2), 0.5)], amp)
+    return m
+
+
+@pytest.mark.parametrize("n,faces", [(40, [4] * 6), (33, [4, 3, 0, 4, 5, 2]), (29, [1, 2, 3, 0, 1, 6])])
+def test_split_row_cpml(n, faces):
+    """The split schedule's row CPML (every slab's correction inside the
+    updates' CPML variant, no shell kernel), with every face or some faces
+    in a layer: fields bit for bit against the oracle, energy steps (which
+    take the shells) within 1e-12."""
+    m = _row_cpml_model(n, faces)
+    g = E.Engine(m)
+    g.set_row_cpml(True)
+    assert g.row_cpml and g.schedule == 4
+    o = OracleEngine(m, threads=4)
+    eg, eo = [], []
+    for s in range(150):
+        if s % 25 == 0:
+            eg.append(g.step_with_energy())
+            eo.append(o.step_with_energy())
+        else:
+            g.run(1)
+            o.run(1)
+    assert_fields_equal(g, o, f"row CPML {n} {faces}")
+    np.testing.assert_allclose(eg, eo, rtol=ENERGY_RTOL, atol=0)
+    g.set_row_cpml(False)
+    assert not g.row_cpml
+
+
+def test_row_cpml_refused_without_cpml_first():
+    m = E.Model.uniform([20, 20, 20], [0.5e-3] * 3)
+    m.build()
+    d = E.Dispersive()
+    d.fill_cells(m, m.cells().sphere([10, 10, 10], 4), W.lorentz_poles(3))
+    m.add_dispersive(d, E.LEAPFROG)
+    m.add_cpml([3] * 6)
+    g = E.Engine(m)
+    with pytest.raises(E.EngineError):
+        g.set_row_cpml(True)
+
+
 def test_split_saved_values_across_uploads_and_schedule_switches():
     """The split schedule's pole kernels store the saved field values
     themselves where that is exact; a field upload or a step on another
