@@ -86,17 +86,39 @@ __device__ __forceinline__ void row_cpml(const FusedParams& P, uint32_t i, uint3
         const FSlab& s = P.slab[SIDE][C][q];
         if (i < s.lo[0] || i >= s.hi[0] || j < s.lo[1] || j >= s.hi[1]) continue;
         const uint32_t base = ((i - s.lo[0]) * (s.hi[1] - s.lo[1]) + (j - s.lo[1])) * (s.hi[2] - s.lo[2]);
+        // The slab's nodes of the quad; every load of them first (the four
+        // ψ entries are distinct, so their loads need not wait for the
+        // stores), then the four chains, then the stores.
+        uint32_t in = 0;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const uint32_t k = k0 + e;
-            if (!((mask >> e) & 1u) || k < s.lo[2] || k >= s.hi[2]) continue;
-            const uint32_t d = s.normal == 0u ? i - s.lo[0] : (s.normal == 1u ? j - s.lo[1] : k - s.lo[2]);
-            const uint32_t at = base + (k - s.lo[2]);
-            const float sv = s.normal == na ? A.v[e] : __fmul_rn(-1.0f, B.v[e]);
-            const float psi = flush(__fadd_rn(__fmul_rn(__ldg(s.b + d), s.psi_old[at]), __fmul_rn(__ldg(s.a + d), sv)));
-            s.psi_new[at] = psi;
-            t.v[e] = flush(__fadd_rn(t.v[e], __fmul_rn(coef.v[e], __fadd_rn(__fmul_rn(__ldg(s.k + d), sv), psi))));
+            in |= (((mask >> e) & 1u) && k >= s.lo[2] && k < s.hi[2] ? 1u : 0u) << e;
         }
+        if (!in) continue;
+        float psi[4], cb_[4], ca_[4], ck_[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            psi[e] = 0.0f;
+            cb_[e] = ca_[e] = ck_[e] = 0.0f;
+            if (!((in >> e) & 1u)) continue;
+            const uint32_t k = k0 + e;
+            const uint32_t d = s.normal == 0u ? i - s.lo[0] : (s.normal == 1u ? j - s.lo[1] : k - s.lo[2]);
+            psi[e] = s.psi_old[base + (k - s.lo[2])];
+            cb_[e] = __ldg(s.b + d);
+            ca_[e] = __ldg(s.a + d);
+            ck_[e] = __ldg(s.k + d);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (!((in >> e) & 1u)) continue;
+            const float sv = s.normal == na ? A.v[e] : __fmul_rn(-1.0f, B.v[e]);
+            psi[e] = flush(__fadd_rn(__fmul_rn(cb_[e], psi[e]), __fmul_rn(ca_[e], sv)));
+            t.v[e] = flush(__fadd_rn(t.v[e], __fmul_rn(coef.v[e], __fadd_rn(__fmul_rn(ck_[e], sv), psi[e]))));
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if ((in >> e) & 1u) s.psi_new[base + (k0 + e - s.lo[2])] = psi[e];
     }
 }
 
