@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--interior-planes", type=int, default=0, help="planes per block of the interior kernel (0: default)")
     ap.add_argument("--march-shape", type=int, default=0, help="marching kernel tile shape (0..3)")
     ap.add_argument("--march-planes", type=int, default=32, help="planes per block of the marching kernel")
+    ap.add_argument("--row-cpml", action="store_true", help="split schedule: the CPML inside the updates (opt-in)")
     ap.add_argument("--workload", choices=["box", "sweep", "learned"], default="box",
                     help="box: the 512^3 dispersive box (the headline line); sweep: the batched patch-variant "
                          "sweep; learned: training and held-out evaluation of the learned early stop")
@@ -348,6 +349,8 @@ def run_ours(args):
     if args.interior_planes:
         eng.set_interior_planes(args.interior_planes)
     eng.set_march(args.march_shape, args.march_planes)
+    if args.row_cpml:
+        eng.set_row_cpml(True)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.run(args.warmup)
     torch.cuda.synchronize(dev)
