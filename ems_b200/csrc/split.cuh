@@ -219,11 +219,16 @@ __device__ __forceinline__ double split_h_quad(const FusedParams& P, uint32_t i,
     return w;
 }
 
-// Grid: (quads of a plane / kSplitThreads, planes); plane i0 + blockIdx.y.
+// Grid: (quads of a plane / kSplitThreads, planes): planes i0 .. i0 +
+// gridDim.y − 1 from the last to the first. An H update reads the u of the
+// plane above its own; in descending order a plane's blocks find it in L2,
+// loaded by the blocks just before them (as the E update, ascending, finds
+// the i of the plane below), and the update ends on the planes the E update
+// starts with. Seven blocks of 72 registers per SM.
 template <bool ENERGY, bool OE = false, bool ROWCPML = false>
-__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : (ROWCPML ? 4 : 8)) k_split_h(
+__global__ void __launch_bounds__(kSplitThreads, ENERGY ? 1 : (ROWCPML ? 4 : 7)) k_split_h(
     const __grid_constant__ FusedParams P, uint32_t i0) {
-    const uint32_t i = i0 + blockIdx.y;
+    const uint32_t i = i0 + (gridDim.y - 1u - blockIdx.y);
     const double w = split_h_quad<ENERGY, OE, ROWCPML>(P, i, mapped_quad(P, blockIdx.x * kSplitThreads + threadIdx.x));
     if (ENERGY) {
         const double s = block_sum<kSplitThreads>(w);
