@@ -217,16 +217,17 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profile_traffic(kernel: str) -> float | None:
+def profile_traffic(kernel: str, workload: str) -> float | None:
     """DRAM bytes per launch of `kernel` scaled to the full configuration,
-    from the committed ncu summary (profiles/traffic.json), if present."""
+    from the committed ncu summary (profiles/traffic.json), if present and
+    recorded for this workload (None for other sizes)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    v = d.get(kernel, {}).get("bytes_per_launch_full_config")
-    return float(v) if v is not None else None
+        d = json.load(f).get(kernel, {})
+    v = d.get("bytes_per_launch_full_config")
+    return float(v) if v is not None and d.get("workload") == workload else None
 
 
 def host_cpu() -> dict:
@@ -446,7 +447,7 @@ def run_ours(args):
         per_launch = 36.0 * ab["cells"] + (0.5 * ab["psi"] if inside else 0.0)
     achieved = per_launch / (kms * 1e-3 / kn) / 1e9 if kn else None
     step_gbs = ab["total"] / (ms * 1e-3 / args.steps) / 1e9 / (world)
-    traffic = profile_traffic(kname)
+    traffic = profile_traffic(kname, w.name)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
