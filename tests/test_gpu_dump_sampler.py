@@ -78,3 +78,33 @@ def test_sampled_freq_dumps():
             w = want[q][k]
             assert np.abs(w).max() > 0, (q, sp.name)
             assert np.abs(got - w).max() <= 1e-9 * np.abs(w).max(), (q, sp.name, k)
+
+
+def test_dump_files_from_the_device(tmp_path):
+    """The device dumps written as the reference's HDF5 dump files
+    (ems_b200/h5.py) and read back: the snapshots as f32 of the device's
+    values with their steps and times, the transform's complex values and
+    the number of accumulated states."""
+    from ems_b200 import h5
+
+    m, _ = small_cavity(kappa=0.02)
+    s_e = E.Sampler(m, E.DUMP_E, E.NODES)
+    s_h = E.Sampler(m, E.DUMP_H, E.CELL_CENTERS)
+    freqs = [2e9, 3e9]
+    g = E.Engine(m)
+    td = g.add_sampled_time_dump(s_h, interval=10)
+    fd = g.add_sampled_freq_dump(s_e, freqs, interval=3)
+    steps = 60
+    g.run(steps)
+    st, v = g.time_dump(td)
+    h5.write_time_dump(str(tmp_path / "ht.h5"), "ht", 4, s_h, st, [s_h.time(int(k), m.dt) for k in st], v)
+    d = h5.read(str(tmp_path / "ht.h5"))
+    assert d["attrs"]["quantity"] == "H" and d["attrs"]["position"] == "cell_centers"
+    np.testing.assert_array_equal(d["step"]["data"], st)
+    np.testing.assert_array_equal(d["time"]["data"], [(k - 0.5) * m.dt for k in st])
+    assert np.array_equal(d["H"]["data"], v.astype(np.float32)) and np.abs(v).max() > 0
+    vals = np.stack([g.freq_dump(fd, k) for k in range(len(freqs))])
+    h5.write_freq_dump(str(tmp_path / "ef.h5"), "ef", 5, s_e, freqs, vals, samples=steps // 3 + 1)
+    d = h5.read(str(tmp_path / "ef.h5"))
+    assert d["attrs"]["samples"] == steps // 3 + 1
+    assert np.array_equal(d["E"]["data"], vals) and np.abs(vals).max() > 0
