@@ -29,7 +29,7 @@ X, Y, Z = 0, 1, 2
 SOFT_E, HARD_E, SOFT_H, HARD_H = 0, 1, 2, 3
 VOLTAGE, CURRENT = 0, 1
 PEC, PMC = 0, 1
-LORENTZ, DRUDE, DEBYE = 0, 1, 2
+LORENTZ, DRUDE, DEBYE, SHEET_BRANCH = 0, 1, 2, 3
 # Pole schemes: trapezoidal, leapfrog, openEMS's f32 arithmetic (Lorentz and
 # Drude poles take the material's own omega_p under it).
 TRAPEZOIDAL, LEAPFROG, OPENEMS_POLES = 0, 1, 2
@@ -397,6 +397,13 @@ class Pole:
     @staticmethod
     def debye(delta_eps: float, tau: float) -> "Pole":
         return Pole(DEBYE, delta_eps, tau)
+
+    @staticmethod
+    def sheet_branch(inductance: float, resistance: float) -> "Pole":
+        """A series R-L branch of openEMS's conducting-sheet model on one E
+        edge (src/engine/openems_sheet.rs), for ``Dispersive.add_edge``
+        with the openEMS pole scheme."""
+        return Pole(SHEET_BRANCH, inductance, resistance)
 
 
 class Dispersive:

@@ -14,6 +14,7 @@
 #include <map>
 #include <memory>
 #include <numeric>
+#include <unordered_map>
 #include <tuple>
 #include <string>
 #include <thread>
@@ -159,6 +160,10 @@ struct ems_model {
     // Per-edge phase velocities of local-medium Mur faces (MurMedia), keyed
     // face·3 + axis, one value per node of the face plane (0: none).
     std::map<int, std::vector<double>> mur_v;
+    // Capacitances that replaced an E edge's medium (ems_model_set_edge_circuit),
+    // keyed axis·N + node index: the circuit openEMS's poles of that edge
+    // are formed with (src/sim/map.rs:1583-1588).
+    std::unordered_map<uint64_t, double> edge_cap;
     double dt = 0.0;
     std::vector<float> co[12];
     std::vector<std::unique_ptr<OpStore>> ops;
@@ -542,6 +547,7 @@ static double oe_sigma_m(const ems_model* m, int a, const uint64_t p[3]) {
 static void compute_coefficients(ems_model* m, double dt, bool openems, bool oe_sigma = false) {
     const uint64_t N = m->n[0] * m->n[1] * m->n[2];
     for (int l = 0; l < 12; ++l) m->co[l].assign(N, 0.0f);
+    m->edge_cap.clear();
     bool pec_face[3][2];
     for (int t = 0; t < 3; ++t)
         for (int s = 0; s < 2; ++s) pec_face[t][s] = m->faces[2 * t + s] == 0;
@@ -916,6 +922,7 @@ int ems_model_set_edge_circuit(ems_model* m, int axis, const uint64_t node[3], d
     const uint64_t idx = m->index(node[0], node[1], node[2]);
     m->co[axis][idx] = (float)((C - 0.5 * G * dt) / den);
     m->co[3 + axis][idx] = (float)(dt / den);
+    m->edge_cap[(uint64_t)axis * m->co[0].size() + idx] = C;
     return EMS_OK;
 }
 
@@ -1178,10 +1185,11 @@ int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset
 
 int ems_dispersive_add_edge(ems_dispersive* d, int field, int axis, const uint64_t node[3], int kind, double p1,
                             double p2, double p3) {
-    if ((field != 0 && field != 1) || axis < 0 || axis > 2 || kind < 0 || kind > 2) return EMS_ERR_INVALID;
+    if ((field != 0 && field != 1) || axis < 0 || axis > 2 || kind < 0 || kind > 3) return EMS_ERR_INVALID;
     const double v[3] = {p1, p2, kind == 0 ? p3 : 0.0};
     for (double x : v)
         if (!(std::isfinite(x) && x >= 0.0)) return EMS_ERR_INVALID;
+    if (kind == 3 && (field != 0 || !(p1 > 0.0))) return EMS_ERR_INVALID;  // a branch: L > 0, R >= 0, E edges
     if (p1 == 0.0) return EMS_OK;  // Pole::is_null
     d->entries.push_back(Entry{field, axis, {node[0], node[1], node[2]}, Pole{kind, p1, p2, p3}});
     return EMS_OK;
@@ -1294,6 +1302,23 @@ int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
             side.pole_end.back() += 1;
             continue;
         }
+        if (p.kind == 3) {
+            // An openEMS conducting-sheet branch of inductance L = p1 and
+            // resistance R = p2 (src/engine/openems_sheet.rs:56-80): the
+            // f32 state x = cb·j with x <- ka·x + kb·u^n before the E update
+            // and u <- u − x after it, ka = f32((L/dt − R/2)/(L/dt + R/2)),
+            // kb = f32(cb/(L/dt + R/2)) with the edge's f32 coefficient cb:
+            // an openEMS pole step with K = 0. It adds no energy.
+            if (scheme != 2) return set_err(m, "conducting-sheet branches need the openEMS pole scheme"), -1;
+            const double den = p.p1 / dt + 0.5 * p.p2;
+            side.kind.push_back(EMS_POLE_OPENEMS);
+            side.a.push_back((double)(float)((p.p1 / dt - 0.5 * p.p2) / den));
+            side.inv_c.push_back(0.0);
+            side.inv_z.push_back((double)(float)((double)coef / den));
+            side.half_l.push_back(0.0);
+            side.pole_end.back() += 1;
+            continue;
+        }
         if (scheme == 2 && p.kind != 2) {
             // OpenEmsPole::coefficients (src/engine/dispersive.rs:888-899):
             // omega_p as given (the material's 2·pi·f_plasma), the edge's
@@ -1302,9 +1327,13 @@ int ems_model_add_dispersive(ems_model* m, ems_dispersive* d, int scheme) {
             // src/engine/coeffs.rs:776-810).
             double circuit;
             if (e.field == 0) {
+                // The edge's capacitance: a parallel R/C lumped element folded
+                // into it replaced the medium's (openEMS forms the poles from
+                // the edge with the element folded in).
+                const auto it = m->edge_cap.find((uint64_t)a * m->co[0].size() + idx);
                 double eps, kap;
                 edge_eps(m, a, e.node, eps, kap);
-                circuit = (double)(float)(OE_EPS0 * eps * geo);
+                circuit = it != m->edge_cap.end() ? it->second : (double)(float)(OE_EPS0 * eps * geo);
             } else {
                 double mu, sig;
                 edge_mu(m, a, e.node, mu, sig);

@@ -489,6 +489,7 @@ class OpenEmsFile:
     props: list
     background: dict | None = None
     cell_constant: bool = False   # CellConstantMaterial: cell-centre materials
+    f_max: float | None = None    # <FDTD f_max>: the explicit highest frequency
 
 
 def _f(x, default=None):
@@ -641,7 +642,7 @@ def parse(text: str) -> OpenEmsFile:
             if tr is not None:
                 boxes[-1] = Transformed(boxes[-1], _transform_matrix(tr), prio)
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
-                          "LumpedElement"):
+                          "LumpedElement", "ConductingSheet"):
             raise NotImplementedError(f"property {el.tag}")
         if el.tag == "ProbeBox" and not boxes and only_long_cylinders:
             continue
@@ -695,11 +696,17 @@ def parse(text: str) -> OpenEmsFile:
                        factor if 0.0 < factor <= 1.0 else 1.0, method if method in (1, 3) else 1,
                        os_ if os_ >= 2 else 4, sig, faces, mur_v, props,
                        dict(bg.attrib) if bg is not None else None,
-                       fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"))
+                       fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"), _f(fd.get("f_max")))
 
 
 # ---------------------------------------------------------------------------
 # Snapping (src/sim/map.rs:1816-1870).
+
+def _box_nodes(lo, hi):
+    """The nodes of the inclusive box lo..hi."""
+    return [(i, j, k) for i in range(lo[0], hi[0] + 1) for j in range(lo[1], hi[1] + 1)
+            for k in range(lo[2], hi[2] + 1)]
+
 
 def snap_lower(lines, x):
     best = 0
@@ -820,6 +827,8 @@ class Setup:
         # primitives: 1e-3 of the smallest cell width, drawing units.
         self.tol = 1e-3 * min(float(np.min(np.diff(v))) for v in f.lines if len(v) > 1)
         self.lumped_edges = {(a, *e) for a, edges in self._lumped_boxes() for e in edges}
+        self.sheet_edges: set = set()     # (axis, i, j, k) of the conducting-sheet edges with a circuit
+        self.sheet_branches: list = []    # (axis, node, [(L, R), (L, R)])
         self._materials(m)
         if f.cell_constant and any(p.weight or any(not isinstance(b, Box) for b in p.boxes) for p in f.props):
             raise NotImplementedError("weighting functions or round primitives with CellConstantMaterial")
@@ -836,6 +845,7 @@ class Setup:
             dt = period / (math.floor(period / dt) + 1.0)
         m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
         self.dt = dt
+        self._sheets(m)
         self._pmc_half_cell(m)
         self.upml_op = None
         if any(k == PML_FACE for k, _ in f.faces):
@@ -1026,6 +1036,10 @@ class Setup:
                 # lumped element's.
                 over = [(ob, op) for (_, _, op, ob) in items if op.kind in MATERIALS and
                         (ob.priority > b.priority or (ob.priority == b.priority and op.order < p.order))]
+                # A conducting sheet that wins over the metal there makes the
+                # edge a sheet edge, not PEC (sheet_over_metal).
+                over += [(ob, op) for op in f.props if op.kind == "ConductingSheet" for ob in op.boxes
+                         if ob.priority > b.priority or (ob.priority == b.priority and op.order < p.order)]
                 n = self.nodes
                 for a in range(3):
                     xs = []
@@ -1134,7 +1148,14 @@ class Setup:
             for e in kept + layer:
                 per[e[a]] = per.get(e[a], 0.0) + w[e]
             S = sum(1.0 / x for x in per.values())
+            on_sheet = [e for e in kept if (a, *e) in self.sheet_edges]
+            if on_sheet:
+                self.warnings.append(f"lumped element {p.name!r}: {len(on_sheet)} of its {len(kept) + len(layer)} "
+                                     "edge(s) lie on conducting-sheet edges and are ignored there (openEMS's sheet "
+                                     "keeps them)")
             for e in kept:
+                if (a, *e) in self.sheet_edges:
+                    continue
                 m.set_edge_circuit(a, e, cap=c * w[e] * S if c is not None else -1.0,
                                    cond=1.0 / (r / (w[e] * S)) if r is not None else -1.0)
             if p.attrs.get("Caps", "1") != "0":
@@ -1149,15 +1170,121 @@ class Setup:
                         blo[a] = bhi[a] = plane
                         blo[t], bhi[t] = lo[t], hi[t] - 1
                         blo[o], bhi[o] = lo[o], hi[o]
-                        m.zero_edges(0, t, blo, bhi)
+                        if not any((t, *e) in self.sheet_edges for e in _box_nodes(blo, bhi)):
+                            m.zero_edges(0, t, blo, bhi)
+                            continue
+                        for e in _box_nodes(blo, bhi):  # the cap leaves sheet edges alone
+                            if (t, *e) not in self.sheet_edges:
+                                m.zero_edges(0, t, e, e)
 
-    def _winner(self, pt):
+    def _sheets(self, m):
+        """openEMS's conducting sheets (emulate, src/compile/openems_sheet.rs:
+        300-500): every in-plane E edge of a flat Box primitive on a mesh
+        plane whose midpoint the sheet holds and wins (priority among
+        materials, metal and sheets; lumped elements do not count) becomes a
+        sheet edge, unless it lies on an outer mesh plane (left to the
+        boundary). An edge in the first cell of its own axis, or with a node
+        coordinate on a line that an absorbing boundary claims (Mur: the
+        first and last two lines, PML_n: n + 1), is PEC. Its width is the
+        dual edge across it at its start node, half of it on a border edge
+        (one of the two neighbouring cells across it, at the start node,
+        not held by a sheet, or the first cell of that axis, or in the
+        boundary's lines); its circuit (openems_sheet.edge_circuit at the
+        bin of the sheet's σ, t at the excitation's frequency) replaces the
+        edge's medium, its two branches become sheet-branch poles. The time
+        step was fixed before (openEMS's ignores the sheets)."""
+        from . import openems_sheet as OS
+        f = self.file
+        sheets = [p for p in f.props if p.kind == "ConductingSheet"]
+        if not sheets:
+            return
+        n, lines, dt = self.nodes, f.lines, self.dt
+        freq = OS.sheet_frequency(f.signal, f.f_max)
+
+        def reach(face):
+            k, c = f.faces[face]
+            return 1 if k == MUR_FACE else (int(c) if k == PML_FACE else 0)
+
+        region = [(reach(2 * a), n[a] - 1 - reach(2 * a + 1)) for a in range(3)]
+
+        def in_region(a, i):
+            return i > 0 and (i <= region[a][0] or i >= region[a][1])
+
+        def sheet_at(name, pt):
+            w = self._winner(pt)
+            return w is not None and w.kind == "ConductingSheet" and (not name or w.name == name)
+
+        done = set()
+        for p in sheets:
+            sigma, th = _f(p.attrs.get("Conductivity")), _f(p.attrs.get("Thickness"))
+            if not (sigma is not None and th is not None and math.isfinite(sigma) and sigma > 0
+                    and math.isfinite(th) and th > 0):
+                self.warnings.append(f"conducting sheet {p.name!r}: needs Conductivity > 0 and Thickness > 0; "
+                                     "ignored")
+                continue
+            row = OS.TABLE[OS.bin_index(sigma, th, freq)]
+            for b in p.boxes:
+                if not isinstance(b, Box):
+                    raise NotImplementedError(f"conducting sheet {p.name!r}: primitives other than boxes")
+                lo = [min(b.p1[q], b.p2[q]) for q in range(3)]
+                hi = [max(b.p1[q], b.p2[q]) for q in range(3)]
+                flat = [q for q in range(3) if hi[q] == lo[q]]
+                if len(flat) != 1:
+                    raise NotImplementedError(f"conducting sheet {p.name!r}: a box that is not flat along one "
+                                              "axis")
+                nrm = flat[0]
+                plane = [i for i, x in enumerate(lines[nrm]) if x == lo[nrm]]
+                if not plane:
+                    raise NotImplementedError(f"conducting sheet {p.name!r}: off the mesh planes")
+                for d in range(3):
+                    if d == nrm:
+                        continue
+                    t = 3 - d - nrm
+                    along = [i for i in range(n[d] - 1)
+                             if self._inside_prim(0.5 * (lines[d][i] + lines[d][i + 1]), lo[d], hi[d])]
+                    across = [i for i in range(n[t]) if self._inside_prim(lines[t][i], lo[t], hi[t])]
+                    for i_d in along:
+                        for i_t in across:
+                            node = [0, 0, 0]
+                            node[d], node[t], node[nrm] = i_d, i_t, plane[0]
+                            node = tuple(node)
+                            if (d, node) in done:
+                                continue
+                            done.add((d, node))
+                            if any(a != d and (node[a] == 0 or node[a] + 1 == n[a]) for a in range(3)):
+                                continue
+                            mid = [lines[q][node[q]] for q in range(3)]
+                            mid[d] = 0.5 * (lines[d][node[d]] + lines[d][node[d] + 1])
+                            if not sheet_at(p.name, mid):
+                                continue
+
+                            def holds(c):
+                                pt = list(mid)
+                                pt[d] = lines[d][node[d]]
+                                pt[t] = 0.5 * (lines[t][c] + lines[t][c + 1])
+                                return c != 0 and not in_region(t, c) and sheet_at("", pt)
+
+                            interior = holds(node[t] - 1) and holds(node[t])
+                            if node[d] == 0 or any(in_region(q, node[q]) for q in (d, t, nrm)):
+                                m.zero_edges(0, d, node, node)
+                                continue
+                            dual = self.model_dual(t, node[t])
+                            width = dual if interior else 0.5 * dual
+                            branches, c_dt2, g_e = OS.edge_circuit(sigma, th, self.model_delta(d, node[d]) / width,
+                                                                   row)
+                            m.set_edge_circuit(d, node, cap=c_dt2 * dt * dt, cond=g_e)
+                            self.sheet_edges.add((d, *node))
+                            self.sheet_branches.append((d, node, branches))
+
+    def _winner(self, pt, sheets: bool = True):
         """The property holding point ``pt`` (drawing units) by openEMS's
         priority (closed bounds; at equal priority the one defined first),
-        among materials and metal; None for the background."""
+        among materials, metal and (``sheets``) conducting sheets; None for
+        the background."""
         best = None
+        kinds = MATERIALS + ("Metal",) + (("ConductingSheet",) if sheets else ())
         for p in self.file.props:
-            if p.kind not in MATERIALS + ("Metal",):
+            if p.kind not in kinds:
                 continue
             for b in p.boxes:
                 if bool(b.inside(pt[0], pt[1], pt[2], self.tol)):
@@ -1179,6 +1306,10 @@ class Setup:
         f = self.file
         disp = [p for p in f.props if p.kind in ("LorentzMaterial", "DebyeMaterial")]
         if not disp:
+            if self.sheet_branches:
+                d = Dispersive()
+                self._sheet_poles(d)
+                m.add_dispersive(d, OPENEMS_POLES)
             return
         if any(k == MUR_FACE for k, _ in f.faces):
             raise NotImplementedError("Mur faces with dispersive materials (openEMS's Mur reads before the poles)")
@@ -1226,8 +1357,18 @@ class Setup:
                             for pole in self._poles(w, field_, a, 1.0, pt):
                                 d.add_edge(field_, a, node, pole)
                                 count += 1
+        count += self._sheet_poles(d)
         if count:
             m.add_dispersive(d, OPENEMS_POLES)
+
+    def _sheet_poles(self, d) -> int:
+        """The conducting-sheet branches as sheet-branch poles of their
+        edges (the reference's OpenEmsSheetBranches: the same f32 update)."""
+        from . import Pole
+        for a, node, branches in self.sheet_branches:
+            for ind, res in branches:
+                d.add_edge(0, a, node, Pole.sheet_branch(ind, res))
+        return 2 * len(self.sheet_branches)
 
     def _poles(self, p, field_, a, inf, pt=None):
         from . import Pole
@@ -1282,8 +1423,11 @@ class Setup:
     def _pmc_half_cell(self, m):
         """openEMS's PMC (src/compile/mod.rs:1556-1626): the tangential H of
         the dual layer next to the face, the tangential E and the normal H
-        on the face are never updated."""
+        on the face are never updated, except the H dual edge of the same
+        direction and node as a conducting-sheet edge (src/compile/mod.rs:
+        1180-1184)."""
         n = self.nodes
+        keep = {(a, tuple(e)) for a, *e in self.sheet_edges}
         for face, (k, _) in enumerate(self.file.faces):
             if k != PMC_FACE:
                 continue
@@ -1294,7 +1438,22 @@ class Setup:
                 for field_, layer in todo:
                     lo, hi = [0, 0, 0], [n[0] - 1, n[1] - 1, n[2] - 1]
                     lo[t] = hi[t] = layer
-                    m.zero_edges(field_, a, lo, hi)
+                    kept = [e for (ka, e) in keep if ka == a and e[t] == layer] if field_ == 1 else []
+                    if not kept:
+                        m.zero_edges(field_, a, lo, hi)
+                        continue
+                    # Row by row along the last in-plane axis, around the kept edges.
+                    u, w = [q for q in range(3) if q != t]
+                    for iu in range(n[u]):
+                        skip = sorted(e[w] for e in kept if e[u] == iu)
+                        start = 0
+                        for stop in skip + [n[w]]:
+                            if stop > start:
+                                blo, bhi = list(lo), list(hi)
+                                blo[u] = bhi[u] = iu
+                                blo[w], bhi[w] = start, stop - 1
+                                m.zero_edges(field_, a, blo, bhi)
+                            start = stop + 1
 
     def _excitation_winner(self, pt):
         """The excitation property that owns point ``pt``: the highest
@@ -1455,22 +1614,34 @@ class Setup:
         for e_type, typ, a, node, w, p in self.excited:
             by_prop.setdefault(p.order, (typ, p, []))[2].append((a, node, w))
         for order in sorted(by_prop):
-            typ, p, edges = by_prop[order]
-            kind = kinds[typ]
-            hard = typ in (1, 3)
-            lag = dt if hard else 0.5 * dt
-            delay = _f(p.attrs.get("Delay"), 0.0)
-            shift = lag + (math.floor(delay / dt) if delay > 0 else 0) * dt
-            # The kind's sample time of step n (SourceKind).
-            t_of = {SOFT_E: lambda s: (s + 0.5) * dt, HARD_E: lambda s: (s + 1.0) * dt,
-                    SOFT_H: lambda s: s * dt, HARD_H: lambda s: (s + 0.5) * dt}[kind]
-            amp = np.zeros(steps)
-            for s in range(steps):
-                tau = t_of(s) - shift
-                amp[s] = 0.0 if tau < -0.25 * dt else f.signal.value(tau, dt)
-            m.add_source_table(kind, edges, amp)
-            if typ in (2, 3):
-                self.h_sources.append((typ == 3, edges, amp.astype(np.float32)))
+            typ0, p, all_edges = by_prop[order]
+            groups = [(typ0, all_edges)]
+            on = [e for e in all_edges if (e[0], *e[1]) in self.sheet_edges] if typ0 == 1 else []
+            if on:
+                # openEMS's sheet edges keep their update under a hard E
+                # source: it adds to them as a soft one (src/sim/map.rs:
+                # 688-700, 773-792).
+                self.warnings.append(f"excitation {p.name!r}: hard E source on {len(on)} conducting-sheet edge(s); "
+                                     "excited as a soft source there (openEMS's sheet keeps its update)")
+                groups = [(0, on), (1, [e for e in all_edges if (e[0], *e[1]) not in self.sheet_edges])]
+            for typ, edges in groups:
+                if not edges:
+                    continue
+                kind = kinds[typ]
+                hard = typ in (1, 3)
+                lag = dt if hard else 0.5 * dt
+                delay = _f(p.attrs.get("Delay"), 0.0)
+                shift = lag + (math.floor(delay / dt) if delay > 0 else 0) * dt
+                # The kind's sample time of step n (SourceKind).
+                t_of = {SOFT_E: lambda s: (s + 0.5) * dt, HARD_E: lambda s: (s + 1.0) * dt,
+                        SOFT_H: lambda s: s * dt, HARD_H: lambda s: (s + 0.5) * dt}[kind]
+                amp = np.zeros(steps)
+                for s in range(steps):
+                    tau = t_of(s) - shift
+                    amp[s] = 0.0 if tau < -0.25 * dt else f.signal.value(tau, dt)
+                m.add_source_table(kind, edges, amp)
+                if typ in (2, 3):
+                    self.h_sources.append((typ == 3, edges, amp.astype(np.float32)))
 
     def _probes(self, m):
         from . import CURRENT, VOLTAGE

@@ -141,7 +141,11 @@ int ems_dispersive_fill(ems_dispersive* d, const ems_model* m, const ems_cellset
 /* Adds one pole of `kind` (parameters as for ems_dispersive_fill), unscaled,
  * to the E edge (field 0) or H dual edge (field 1) along `axis` at `node`
  * (Dispersive::push of an EdgePole, src/engine/dispersive.rs:474-507): the
- * openEMS files' rule of full poles per edge. */
+ * openEMS files' rule of full poles per edge. Kind 3, E edges and the
+ * openEMS pole scheme only: a branch of openEMS's conducting-sheet model,
+ * p1 = L [H], p2 = R [Ohm] (OpenEmsSheetBranches::push,
+ * src/engine/openems_sheet.rs:56-80), installed with the edge's coefficient
+ * as it is when ems_model_add_dispersive runs. */
 int ems_dispersive_add_edge(ems_dispersive* d, int field, int axis, const uint64_t node[3], int kind, double p1,
                             double p2, double p3);
 /* The averaged static material of the E edge (field 0: eps_r, kappa) or H

@@ -166,6 +166,42 @@ PMLM = f"""<?xml version="1.0" encoding="UTF-8"?>
 """
 
 
+# openEMS's conducting-sheet model: a copper sheet on the plane x = 8 (a
+# lumped resistor partly on it, a hard E source across it), a resistive
+# sheet on z = 5 under a Lorentz block and a metal strip of lower priority,
+# PMC faces (the H edges next to sheet edges kept).
+SHEET = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="400" endCriteria="1e-30">
+    <Excitation Type="0" f0="5e9" fc="4e9"/>
+    <BoundaryCond xmin="PEC" xmax="PEC" ymin="PMC" ymax="PMC" zmin="PEC" zmax="PEC"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <LorentzMaterial Name="lor"><Property Epsilon="2.0" EpsilonPlasmaFrequency="5e9" EpsilonLorPoleFrequency="8e9" EpsilonRelaxTime="1e-9"/>
+        <Primitives><Box Priority="2"><P1 X="10" Y="2" Z="5"/><P2 X="14" Y="9" Z="8"/></Box></Primitives></LorentzMaterial>
+      <Metal Name="strip"><Primitives><Box Priority="1"><P1 X="11" Y="3" Z="5"/><P2 X="13" Y="5" Z="5"/></Box></Primitives></Metal>
+      <ConductingSheet Name="cu" Conductivity="5.8e7" Thickness="3.5e-5">
+        <Primitives><Box Priority="3"><P1 X="8" Y="2" Z="2"/><P2 X="8" Y="10" Z="10"/></Box></Primitives></ConductingSheet>
+      <ConductingSheet Name="res" Conductivity="1e4" Thickness="1e-5">
+        <Primitives><Box Priority="3"><P1 X="9" Y="1" Z="5"/><P2 X="15" Y="11" Z="5"/></Box></Primitives></ConductingSheet>
+      <LumpedElement Name="r1" Direction="2" Caps="1" R="75"><Primitives><Box Priority="0"><P1 X="8" Y="4.6" Z="4"/><P2 X="9" Y="4.6" Z="7"/></Box></Primitives></LumpedElement>
+      <Excitation Name="exc" Type="1" Excite="0,1,0"><Primitives><Box Priority="0"><P1 X="7" Y="6" Z="6"/><P2 X="9" Y="7" Z="6"/></Box></Primitives></Excitation>
+      <Excitation Name="soft" Type="0" Excite="0,0,1"><Primitives><Box Priority="0"><P1 X="4" Y="5.2" Z="3"/><P2 X="4" Y="5.2" Z="6"/></Box></Primitives></Excitation>
+      <ProbeBox Name="ut" Type="0"><Primitives><Box Priority="0"><P1 X="12" Y="6" Z="0"/><P2 X="12" Y="6" Z="12"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="e8" Type="2"><Primitives><Box Priority="0"><P1 X="8" Y="7" Z="6"/><P2 X="8" Y="7" Z="6"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="h" Type="3"><Primitives><Box Priority="0"><P1 X="13" Y="4" Z="9"/><P2 X="13" Y="4" Z="9"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -183,7 +219,8 @@ def _both(text, schedule=0):
     ("box", BOX, 0), ("box", BOX, 1), ("box", BOX, 2), ("box", BOX, 3), ("box", BOX, 5),
     ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1),
     ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5),
-    ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4)])
+    ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4),
+    ("sheet", SHEET, 0), ("sheet", SHEET, 1), ("sheet", SHEET, 3)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes

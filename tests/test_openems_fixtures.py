@@ -93,6 +93,15 @@ CASES = [
     # Probes on cylinders (a zero-length one is a point probe; openEMS
     # writes nothing for one on a longer cylinder).
     ("current_probe_ties", 1e-12), ("sweep_probe_cylinder_prim", 1e-12),
+    # openEMS's conducting-sheet model (ems_b200/openems_sheet.py): copper
+    # and resistive sheets, graded meshes, a sheet across a TEM line with
+    # PMC walls (the H edges next to sheet edges kept), sheets beside Mur
+    # and PML faces (PEC rows), under metal and Lorentz media, a hard
+    # source across a sheet (soft there), lumped resistors on sheet edges
+    # (ignored there) and in Lorentz media (poles from the folded edge).
+    ("sweep_sheet_copper", 1e-12), ("sweep_sheet_full", 1e-12), ("sweep_sheet_graded", 1e-12),
+    ("sweep_sheet_resistive", 1e-12), ("adv_sheet_copper", 1e-12), ("rs_316_sheet", 1e-12), ("rs_77", 1e-12),
+    ("rs_99", 1e-12), ("rs_287", 1e-12), ("rs_51", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
