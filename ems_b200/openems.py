@@ -419,6 +419,36 @@ class LinPoly:
 
 
 @dataclass
+class Wire:
+    """A wire (CSXCAD Wire): the points within ``radius`` of its polyline
+    (segments with round ends), closed; grown by the inside tolerance
+    (src/compile/openems.rs:509-512); ``p1``/``p2`` its bounding box."""
+    points: list
+    radius: float
+    priority: int
+    p1: tuple = ()
+    p2: tuple = ()
+
+    def __post_init__(self):
+        self.p1 = tuple(min(p[a] for p in self.points) - self.radius for a in range(3))
+        self.p2 = tuple(max(p[a] for p in self.points) + self.radius for a in range(3))
+
+    def inside(self, x, y, z, tol):
+        c = np.broadcast_arrays(np.asarray(x, np.float64), np.asarray(y, np.float64), np.asarray(z, np.float64))
+        r2 = (self.radius + tol) ** 2
+        out = np.zeros(c[0].shape, dtype=bool)
+        pts = self.points if len(self.points) > 1 else self.points * 2
+        for a, b in zip(pts[:-1], pts[1:]):
+            d = [b[q] - a[q] for q in range(3)]
+            dd = sum(v * v for v in d)
+            t = sum((c[q] - a[q]) * d[q] for q in range(3)) / dd if dd > 0 else np.zeros(c[0].shape)
+            t = np.clip(t, 0.0, 1.0)
+            dist2 = sum((c[q] - (a[q] + t * d[q])) ** 2 for q in range(3))
+            out |= dist2 <= r2
+        return out
+
+
+@dataclass
 class Shape:
     """A sphere, spherical shell, cylinder or cylindrical shell primitive
     (CSXCAD's closed inside tests, grown by openEMS's inside tolerance;
@@ -630,6 +660,18 @@ def parse(text: str) -> OpenEmsFile:
                 verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
                                      float(b.get("Length", "0")), verts, prio))
+            elif b.tag == "Wire" and el.tag == "Metal" and tr is None:
+                radius = float(b.get("WireRadius", "0"))
+                if radius < 0.5 * min(float(np.min(np.diff(v))) for v in lines if len(v) > 1):
+                    # Thinner wires get an in-cell correction (the reference's
+                    # compile::wire), not restated.
+                    raise NotImplementedError(f"wire {el.get('Name')!r} thinner than half the smallest cell")
+                boxes.append(Wire([pt(v) for v in b.findall("Vertex")], radius, prio))
+            elif b.tag == "Polygon" and el.tag in ("Metal", "ConductingSheet") and tr is None:
+                # A flat polygon: an extruded one of length 0.
+                verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
+                boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")), 0.0,
+                                     verts, prio))
             elif b.tag in ("Sphere", "SphericalShell", "Cylinder", "CylindricalShell") and \
                     el.tag in MATERIALS + ("Metal",):
                 sph = b.tag.startswith("Spher")
@@ -1224,11 +1266,12 @@ class Setup:
                 continue
             row = OS.TABLE[OS.bin_index(sigma, th, freq)]
             for b in p.boxes:
-                if not isinstance(b, Box):
-                    raise NotImplementedError(f"conducting sheet {p.name!r}: primitives other than boxes")
+                if not (isinstance(b, Box) or (isinstance(b, LinPoly) and b.length == 0.0)):
+                    raise NotImplementedError(f"conducting sheet {p.name!r}: primitives other than boxes and "
+                                              "polygons")
                 lo = [min(b.p1[q], b.p2[q]) for q in range(3)]
                 hi = [max(b.p1[q], b.p2[q]) for q in range(3)]
-                flat = [q for q in range(3) if hi[q] == lo[q]]
+                flat = [b.normal] if isinstance(b, LinPoly) else [q for q in range(3) if hi[q] == lo[q]]
                 if len(flat) != 1:
                     raise NotImplementedError(f"conducting sheet {p.name!r}: a box that is not flat along one "
                                               "axis")

@@ -102,6 +102,10 @@ CASES = [
     ("sweep_sheet_copper", 1e-12), ("sweep_sheet_full", 1e-12), ("sweep_sheet_graded", 1e-12),
     ("sweep_sheet_resistive", 1e-12), ("adv_sheet_copper", 1e-12), ("rs_316_sheet", 1e-12), ("rs_77", 1e-12),
     ("rs_99", 1e-12), ("rs_287", 1e-12), ("rs_51", 1e-12),
+    # Flat polygons as metal and as conducting sheets; metal wires (at least
+    # half a cell thick).
+    ("sweep_prim_polygon_x", 1e-12), ("sweep_sheet_triangle", 1e-12), ("sweep_sheet_triangle_r", 1e-12),
+    ("sweep_prim_wire", 1e-12), ("sweep_prim_wire_thick", 1e-12), ("sweep_tie_wire_z", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
