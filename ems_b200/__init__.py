@@ -231,6 +231,7 @@ def host_lib() -> C.CDLL:
             "ems_waveform_duration": (d, [i, d, d]),
             "ems_model_add_lumped_port": (i, [p, i, p, p, d, i, d, d, d, u]),
             "ems_model_add_lumped": (i, [p, i, p, p, d, d, d, i, i, i, p, u]),
+            "ems_model_add_lumped_openems": (i, [p, i, p, p, d, d, d, i, d, i, p, p, u]),
             "ems_model_add_source": (i, [p, i, sz, p, p, p, i, d, d, u]),
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
@@ -623,6 +624,24 @@ class Model:
                                                        None if a is None else a.ctypes.data,
                                                        0 if a is None else len(a)), "add_lumped")
         self.ops.append((OP_LUMPED, "port" if port else "lumped"))
+        return k
+
+    def add_lumped_openems(self, axis: int, lo: Sequence[int], hi: Sequence[int], r: float = 0.0, l: float = 0.0,
+                           c: float = 0.0, series: bool = False, omega: float = 0.0, explicit: bool = True,
+                           src_w: np.ndarray | None = None, amp: np.ndarray | None = None) -> int:
+        """A lumped element with an inductor or in series as an openEMS file has it
+        (``ems_model_add_lumped_openems``; src/sim/map.rs:820-1000, 1525-1632): the
+        element replaces the medium of its edges, the edge capacitance is limited at
+        ``omega``, openEMS's order and (parallel inductor, ``explicit``) its explicit
+        f32 update; ``src_w`` (per edge) and ``amp`` (at (n + ½)·dt) its Thevenin
+        source (a parallel element with a resistor)."""
+        w = None if src_w is None else np.ascontiguousarray(src_w, dtype=np.float64)
+        a = None if amp is None else np.ascontiguousarray(amp, dtype=np.float64)
+        k = self._check(self._lib.ems_model_add_lumped_openems(
+            self._p, axis, _u64(lo), _u64(hi), r, l, c, int(series), omega, int(explicit),
+            None if w is None else w.ctypes.data, None if a is None else a.ctypes.data,
+            0 if a is None else len(a)), "add_lumped_openems")
+        self.ops.append((OP_LUMPED, "lumped"))
         return k
 
     def add_sheet(self, edges: Sequence[tuple], f_max: float | None = None) -> int:

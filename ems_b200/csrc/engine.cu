@@ -1747,6 +1747,14 @@ ems_status ems_gpu_create(const ems_engine_desc* d, int device, ems_gpu** out) {
                 D.rec_g = h->upload(l->rec_g, ne);
                 D.rec_c = h->upload(l->rec_c, ne);
             }
+            D.openems_order = l->openems_order;
+            if (l->oe_k) {
+                if (!L.has_branch || !l->oe_vi || !l->openems_order) return EMS_ERR_INVALID;
+                D.oe_k = h->upload(l->oe_k, ne);
+                D.oe_vi = h->upload(l->oe_vi, ne);
+                D.oe_s = h->alloc<float>(ne);
+                if (!D.oe_k || !D.oe_vi || !D.oe_s) return EMS_ERR_NOMEM;
+            }
             D.v = h->alloc<double>(ne);
             D.bj = h->alloc<double>(ne);
             D.bq = h->alloc<double>(ne);

@@ -114,7 +114,8 @@ struct OpStore {
     ems_poles poles{};
     // lumped
     std::vector<uint64_t> lnode;
-    std::vector<double> lcb, lg, lw, lamp, lrg, lrc, ltl, linvc, lz;
+    std::vector<double> lcb, lg, lw, lamp, lrg, lrc, ltl, linvc, lz, loevi;
+    std::vector<float> loek;
     ems_lumped lumped{};
     // source / probe
     std::vector<uint8_t> axis;
@@ -1492,6 +1493,148 @@ int ems_model_add_lumped(ems_model* m, int axis, const uint64_t lo[3], const uin
     L.rec_g = op->lrg.data();
     L.rec_c = op->lrc.data();
     L.port_columns = port ? (uint64_t)nn : 0;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
+int ems_model_add_lumped_openems(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r,
+                                 double l, double c, int series_topology, double omega, int explicit_inductor,
+                                 const double* src_w, const double* amp, uint64_t n_amp) {
+    if (!m->built || !m->oe_round) return set_err(m, "build the model with openEMS's rounding first"), -1;
+    if (axis < 0 || axis > 2) return set_err(m, "invalid lumped element axis"), -1;
+    const bool has_r = r > 0.0, has_l = l > 0.0, has_c = c > 0.0;
+    for (double v : {r, l, c})
+        if (!(v <= 0.0) && !(std::isfinite(v) && v > 0.0)) return set_err(m, "invalid lumped value"), -1;
+    if (!(has_l || series_topology)) return set_err(m, "an element with an inductor or in series"), -1;
+    const bool has_src = src_w != nullptr && amp != nullptr && n_amp > 0;
+    if (has_src && (series_topology || !has_r)) return set_err(m, "the element's source needs a parallel resistor"), -1;
+    for (int t = 0; t < 3; ++t)
+        if (lo[t] > hi[t] || hi[t] >= m->n[t]) return set_err(m, "lumped box outside the grid"), -1;
+    if (lo[axis] >= hi[axis]) return set_err(m, "lumped box degenerate along its axis"), -1;
+    const int a = axis, b = next_axis(axis), cc = prev_axis(axis);
+    std::vector<uint64_t> edges;
+    std::vector<std::array<uint64_t, 3>> pos;
+    for (uint64_t pb = lo[b]; pb <= hi[b]; ++pb)
+        for (uint64_t pc = lo[cc]; pc <= hi[cc]; ++pc)
+            for (uint64_t pa = lo[a]; pa < hi[a]; ++pa) {
+                std::array<uint64_t, 3> p{};
+                p[a] = pa;
+                p[b] = pb;
+                p[cc] = pc;
+                edges.push_back(m->index(p[0], p[1], p[2]));
+                pos.push_back(p);
+            }
+    for (uint64_t e : edges)
+        if (m->co[3 + a][e] == 0.0f) return set_err(m, "lumped element edge is PEC"), -1;
+    // csx's equal parts per edge (src/sim/map.rs:198-205): R·p/s, L·p/s,
+    // C·s/p with p edges in parallel and s in series.
+    const double s_n = (double)(hi[a] - lo[a]);
+    const double p_n = (double)((hi[b] - lo[b] + 1) * (hi[cc] - lo[cc] + 1));
+    const double r_e = has_r ? r * p_n / s_n : 0.0, l_e = has_l ? l * p_n / s_n : 0.0;
+    const double c_e = has_c ? c * s_n / p_n : 0.0;
+    const bool series = series_topology != 0;
+    const double dt = m->dt, inf = std::numeric_limits<double>::infinity();
+    auto store = [](double x) { return (double)(float)x; };
+    // capacitance_limit (src/sim/map.rs:1608-1632).
+    double limit = inf;
+    if (omega > 0.0 && std::isfinite(omega)) {
+        if (!series) {
+            if (has_r) limit = std::min(limit, 1.0 / (20.0 * omega * r_e));
+            if (has_l) limit = std::min(limit, 1.0 / (20.0 * omega * omega * l_e));
+        } else {
+            const double x = (has_l ? omega * l_e : 0.0) - (has_c ? 1.0 / (omega * c_e) : 0.0);
+            const double z = std::hypot(has_r ? r_e : 0.0, x);
+            if (z > 0.0) limit = 1.0 / (20.0 * omega * z);
+        }
+    }
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_LUMPED;
+    std::vector<double> den(edges.size());
+    for (size_t q = 0; q < edges.size(); ++q) {
+        // replace_medium (src/sim/map.rs:1525-1606): the element's C and 1/R
+        // replace the medium's, the capacitance limited at omega.
+        const uint64_t i = edges[q];
+        const float fa = m->co[a][i], fb = m->co[3 + a][i];
+        const double ca = fa, cb = fb;
+        if ((!series && !has_c && !has_r && !(omega > 0.0)) || !std::isfinite(cb)) {
+            den[q] = dt * (1.0 + ca) / (2.0 * cb);
+            continue;
+        }
+        double eps, kap;
+        edge_eps(m, a, pos[q].data(), eps, kap);
+        const double geo = m->dual_delta(b, pos[q][b]) * m->dual_delta(cc, pos[q][cc]) / m->delta(a, pos[q][a]);
+        double cap = store(OE_EPS0 * eps * geo), cond = store(kap * geo);
+        const double dd = cap + 0.5 * cond * dt;
+        if (!((float)((cap - 0.5 * cond * dt) / dd) == fa && (float)(dt / dd) == fb)) {
+            cap = dt * (1.0 + ca) / (2.0 * cb);
+            cond = (1.0 - ca) / cb;
+        }
+        if (!series && has_c) cap = store(c_e);
+        if (series) cond = 0.0;
+        if (!series && has_r) cond = store(1.0 / r_e);
+        double c_own = (!series && has_c) ? c_e : cap;
+        if (cap > limit) {
+            cap = store(limit);
+            c_own = limit;
+        }
+        const double d2 = cap + 0.5 * cond * dt;
+        m->co[a][i] = (float)((cap - 0.5 * cond * dt) / d2);
+        m->co[3 + a][i] = (float)(dt / d2);
+        den[q] = c_own + ((!series && has_r) ? 0.5 * (dt / r_e) : 0.0);
+    }
+    // install (src/engine/lumped.rs:880-1000) with the medium folded: the
+    // branch (r, l, c) of a series element, (0, l, inf) of a parallel one;
+    // openEMS's order; its explicit inductor for a parallel one.
+    const double br_r = series && has_r ? r_e : 0.0, br_l = has_l ? l_e : 0.0;
+    const double br_c = series && has_c ? c_e : inf;
+    const double g_e = (!series && has_r) ? 1.0 / r_e : 0.0;
+    // openEMS's explicit inductor is stable while dt²/(L_e·C_e) = dt·cb/L_e
+    // stays at most 1 on every edge; beyond, the trapezoidal branch
+    // (src/sim/map.rs:928-958).
+    double worst = 0.0;
+    for (uint64_t e : edges) worst = std::max(worst, dt * (double)m->co[3 + a][e] / l_e);
+    const bool oe = explicit_inductor && !series && has_l && worst <= 1.0;
+    for (size_t q = 0; q < edges.size(); ++q) {
+        const uint64_t e = edges[q];
+        op->lnode.push_back(e);
+        op->lcb.push_back((double)m->co[3 + a][e]);
+        op->lg.push_back(series ? 0.0 : g_e);
+        op->lw.push_back(has_src ? src_w[q] : 0.0);
+        op->lrg.push_back(g_e);
+        op->lrc.push_back(!series ? c_e : 0.0);
+        const double inv_c = std::isfinite(br_c) ? 1.0 / br_c : 0.0;
+        op->ltl.push_back(2.0 * br_l / dt);
+        op->linvc.push_back(inv_c);
+        op->lz.push_back(2.0 * br_l / dt + br_r + 0.5 * dt * inv_c);
+        if (oe) {
+            op->loek.push_back((float)(dt / br_l) * (float)(dt / den[q]));
+            op->loevi.push_back(dt / den[q]);
+        }
+    }
+    if (has_src) op->lamp.assign(amp, amp + n_amp);
+    ems_lumped& L = op->lumped;
+    L.axis = a;
+    L.n_edges = edges.size();
+    L.node = op->lnode.data();
+    L.cb = op->lcb.data();
+    L.g_src = op->lg.data();
+    L.series = hi[a] - lo[a];
+    L.src_in_branch = series ? 1 : 0;
+    L.src_w = has_src ? op->lw.data() : nullptr;
+    L.n_src_amp = op->lamp.size();
+    L.src_amp = op->lamp.empty() ? nullptr : op->lamp.data();
+    L.has_branch = 1;
+    L.two_l_dt = op->ltl.data();
+    L.inv_c = op->linvc.data();
+    L.z = op->lz.data();
+    L.record = 0;
+    L.rec_g = op->lrg.data();
+    L.rec_c = op->lrc.data();
+    L.port_columns = 0;
+    L.openems_order = 1;
+    L.oe_k = oe ? op->loek.data() : nullptr;
+    L.oe_vi = oe ? op->loevi.data() : nullptr;
     m->ops.push_back(std::move(op));
     m->refresh_desc();
     return (int)m->ops.size() - 1;

@@ -75,6 +75,10 @@ struct LumpedDevT {
     double* bu_prev = nullptr;
     double* j_avg = nullptr;
     double* ru_prev = nullptr;
+    int openems_order = 0;
+    const float* oe_k = nullptr;   // openEMS's explicit inductor (f32 state oe_s)
+    const double* oe_vi = nullptr;
+    float* oe_s = nullptr;
 };
 
 struct ProbeDevT {
@@ -304,7 +308,7 @@ __global__ void k_probe(const float* f0, const float* f1, const float* f2, Probe
 // Lumped element pre_e: saves u^n (src/engine/lumped.rs:1106-1121).
 __device__ __forceinline__ void lumped_pre_e_edge(const float* u, const LumpedDevT& d, uint32_t e) {
     const double x = (double)u[d.node[e]];
-    if (d.has_branch) d.bu_prev[e] = x;
+    if (d.has_branch && !d.openems_order) d.bu_prev[e] = x;  // openEMS's order keeps the post_e value
     if (d.record) d.ru_prev[e] = x;
 }
 
@@ -322,11 +326,22 @@ __device__ __forceinline__ void lumped_post_e_block(float* u, const LumpedDevT& 
     for (uint32_t e = threadIdx.x; e < d.n; e += blockDim.x) {
         const uint32_t idx = d.node[e];
         if (d.src_w) d.v[e] = active ? __dadd_rn(0.0, __dmul_rn(d.src_w[e], val)) : 0.0;
-        if (active && !d.src_in_branch) {
+        // In openEMS's order a resistor's source acts like a soft one, after
+        // the branch.
+        if (active && !d.src_in_branch && !d.openems_order) {
             const double add = __dmul_rn(__dmul_rn(d.cb[e], d.g_src[e]), d.v[e]);
             if (add != 0.0) u[idx] = (float)__dadd_rn((double)u[idx], add);
         }
-        if (d.has_branch) {
+        if (d.has_branch && d.oe_k) {
+            // openEMS's explicit inductor in f32 (src/engine/lumped.rs:1168-1177).
+            const float u_l = (float)d.bu_prev[e];
+            d.oe_s[e] = flush(__fadd_rn(d.oe_s[e], flush(__fmul_rn(d.oe_k[e], u_l))));
+            const float u_new = flush(__fsub_rn(u[idx], d.oe_s[e]));
+            d.bj[e] = __ddiv_rn((double)d.oe_s[e], d.oe_vi[e]);
+            d.j_avg[e] = d.bj[e];
+            u[idx] = u_new;
+            d.bu_prev[e] = (double)u_new;
+        } else if (d.has_branch) {
             const double v_br = (active && d.src_in_branch) ? d.v[e] : 0.0;
             const double u_star = (double)u[idx];
             const double kk = __dadd_rn(__dsub_rn(__dsub_rn(__dmul_rn(d.two_l_dt[e], d.bj[e]), __dmul_rn(d.bq[e], d.inv_c[e])), v_br),
@@ -338,6 +353,11 @@ __device__ __forceinline__ void lumped_post_e_block(float* u, const LumpedDevT& 
             d.bq[e] = __dadd_rn(d.bq[e], __dmul_rn(dt, jb));
             d.j_avg[e] = jb;
             u[idx] = (float)u_new;
+            if (d.openems_order) d.bu_prev[e] = (double)(float)u_new;
+        }
+        if (active && !d.src_in_branch && d.openems_order) {
+            const double add = __dmul_rn(__dmul_rn(d.cb[e], d.g_src[e]), d.v[e]);
+            if (add != 0.0) u[idx] = (float)__dadd_rn((double)u[idx], add);
         }
     }
     __syncthreads();

@@ -888,6 +888,12 @@ class Setup:
         m.build_bound(dt, openems_rounding=True, openems_sigma_m=True)
         self.dt = dt
         self._sheets(m)
+        # Lumped elements with an inductor or in series (openEMS keeps the H
+        # edge of their direction and node at a PMC wall, and their E edges).
+        self.branch_edges = set()
+        for (a, edges), p in zip(self._lumped_boxes(), [q for q in f.props if q.kind == "LumpedElement"]):
+            if p.attrs.get("L") is not None or p.attrs.get("LEtype", "0") not in ("0", "-1"):
+                self.branch_edges |= {(a, *e) for e in edges}
         self._pmc_half_cell(m)
         self.upml_op = None
         if any(k == PML_FACE for k, _ in f.faces):
@@ -1157,10 +1163,14 @@ class Setup:
             a, edges = next(boxes)
             r = _f(p.attrs.get("R"))
             c = _f(p.attrs.get("C"))
-            if p.attrs.get("L") is not None or p.attrs.get("LEtype", "0") not in ("0", "-1"):
-                raise NotImplementedError(f"lumped element {p.name!r}: inductors and series elements")
             r = r if r is not None and r > 0 and math.isfinite(r) else None
             c = c if c is not None and c > 0 and math.isfinite(c) else None
+            ind = _f(p.attrs.get("L"))
+            ind = ind if ind is not None and ind > 0 and math.isfinite(ind) else None
+            series = p.attrs.get("LEtype", "0") not in ("0", "-1")
+            if ind is not None or series:
+                self._branch_element(m, p, a, edges, r, ind, c, series)
+                continue
             ca, cb = m.coeff(a), m.coeff(3 + a)
             kept, layer = [], []
             for e in edges:
@@ -1218,6 +1228,60 @@ class Setup:
                         for e in _box_nodes(blo, bhi):  # the cap leaves sheet edges alone
                             if (t, *e) not in self.sheet_edges:
                                 m.zero_edges(0, t, e, e)
+
+    def _branch_element(self, m, p, a, edges, r, ind, c, series):
+        """A lumped element with an inductor or in series the openEMS way
+        (src/sim/map.rs:820-1000, 1525-1632; ``Model.add_lumped_openems``):
+        caps first, the element's values in csx's equal parts replacing the
+        medium of its edges, the edge capacitance limited by the branch
+        impedance at the excitation's frequency (series elements; parallel
+        ones with an inductor and no capacitor), openEMS's order and, for a
+        parallel inductor, its explicit f32 update (the trapezoidal branch
+        where that is unstable). An excitation on its edges stays a plain
+        soft source, added after the element. Not restated: elements with
+        edges in PML layers or on conducting-sheet edges (openEMS installs
+        them over the sheet), poles on their edges (openEMS corrects those
+        after the element), edge sets that are not one box."""
+        n = self.nodes
+        if not edges:
+            return
+        if any((a, *e) in self.sheet_edges for e in edges):
+            raise NotImplementedError(f"lumped element {p.name!r}: an inductor or series element on a "
+                                      "conducting sheet")
+        lo = [min(e[q] for e in edges) for q in range(3)]
+        hi = [max(e[q] for e in edges) for q in range(3)]
+        box = {(i, j, k) for i in range(lo[0], hi[0] + 1) for j in range(lo[1], hi[1] + 1)
+               for k in range(lo[2], hi[2] + 1)}
+        box = {e for e in box if e[a] <= hi[a]}
+        if set(edges) != box:
+            raise NotImplementedError(f"lumped element {p.name!r}: edges that are not one box")
+        ca = m.coeff(a)
+        if any(ca[e] == 0.0 for e in edges):
+            raise NotImplementedError(f"lumped element {p.name!r}: an inductor or series element in a PML layer "
+                                      "or on PEC")
+        if p.attrs.get("Caps", "1") != "0":
+            for t in range(3):
+                if t == a or hi[t] == lo[t]:
+                    continue
+                o = 3 - a - t
+                for plane in (lo[a], hi[a] + 1):
+                    blo, bhi = [0, 0, 0], [0, 0, 0]
+                    blo[a] = bhi[a] = plane
+                    blo[t], bhi[t] = lo[t], hi[t] - 1
+                    blo[o], bhi[o] = lo[o], hi[o]
+                    for e in _box_nodes(blo, bhi):
+                        if (t, *e) not in self.sheet_edges:
+                            m.zero_edges(0, t, e, e)
+        f = self.file.signal
+        nyq = f.nyquist_frequency()
+        parallel = not series
+        use = (not parallel) or (c is None and ind is not None)
+        omega = 2.0 * math.pi * nyq if (use and nyq) else 0.0
+        hi_node = list(hi)
+        hi_node[a] += 1
+        m.add_lumped_openems(a, lo, hi_node, r=r or 0.0, l=ind or 0.0, c=c or 0.0, series=series, omega=omega,
+                             explicit=parallel)
+        self.inductor_edges = getattr(self, "inductor_edges", set()) | {(a, *e) for e in edges}
 
     def _sheets(self, m):
         """openEMS's conducting sheets (emulate, src/compile/openems_sheet.rs:
@@ -1397,6 +1461,10 @@ class Setup:
                             w = self._winner(pt)
                             if w is None or w.kind not in ("LorentzMaterial", "DebyeMaterial"):
                                 continue
+                            if field_ == 0 and (a, *node) in getattr(self, "inductor_edges", ()):
+                                raise NotImplementedError("poles on the edges of a lumped element with an "
+                                                          "inductor or in series (openEMS corrects them after "
+                                                          "the element)")
                             for pole in self._poles(w, field_, a, 1.0, pt):
                                 d.add_edge(field_, a, node, pole)
                                 count += 1
@@ -1466,11 +1534,13 @@ class Setup:
     def _pmc_half_cell(self, m):
         """openEMS's PMC (src/compile/mod.rs:1556-1626): the tangential H of
         the dual layer next to the face, the tangential E and the normal H
-        on the face are never updated, except the H dual edge of the same
-        direction and node as a conducting-sheet edge (src/compile/mod.rs:
-        1180-1184)."""
+        on the face are never updated, except a lumped element's E edges
+        and the H dual edge of the same direction and node as a
+        conducting-sheet edge or an edge of a lumped element with an
+        inductor or in series (src/compile/mod.rs:1180-1197)."""
         n = self.nodes
-        keep = {(a, tuple(e)) for a, *e in self.sheet_edges}
+        keep = {(a, tuple(e)) for a, *e in self.sheet_edges | self.branch_edges}
+        keep_e = {(a, tuple(e)) for a, *e in self.lumped_edges}
         for face, (k, _) in enumerate(self.file.faces):
             if k != PMC_FACE:
                 continue
@@ -1481,7 +1551,7 @@ class Setup:
                 for field_, layer in todo:
                     lo, hi = [0, 0, 0], [n[0] - 1, n[1] - 1, n[2] - 1]
                     lo[t] = hi[t] = layer
-                    kept = [e for (ka, e) in keep if ka == a and e[t] == layer] if field_ == 1 else []
+                    kept = [e for (ka, e) in (keep if field_ == 1 else keep_e) if ka == a and e[t] == layer]
                     if not kept:
                         m.zero_edges(field_, a, lo, hi)
                         continue

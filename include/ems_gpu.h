@@ -131,7 +131,13 @@ typedef struct {
  * (source weight, V_s share), and with a branch 2L/dt, 1/C, z; with a
  * current record g and c. src_amp[n] is the source value at (n+1/2)*dt
  * for step n (n < n_src_amp; 0 beyond). A port (port_columns > 0) also
- * records V = sum(u)/columns after each step and I = -record. */
+ * records V = sum(u)/columns after each step and I = -record.
+ * openems_order (openEMS files, LumpedElement::openems_order): the branch
+ * is driven by the voltage its own update left the step before (not u^n
+ * saved in pre_e) and the source is added after the branch; with oe_k
+ * (parallel inductor, openEMS's explicit update in f32): per edge the f32
+ * state s <- f32(s + f32(oe_k*f32(u_prev))), u <- f32(u - s), the branch
+ * current s/oe_vi. NULL oe_k: the trapezoidal branch. */
 typedef struct {
     int32_t axis;
     size_t n_edges;
@@ -151,6 +157,9 @@ typedef struct {
     const double* rec_g;
     const double* rec_c;
     uint64_t port_columns;      /* > 0: a lumped port (src/engine/port.rs:262-290) */
+    int32_t openems_order;      /* openEMS's operation order around the branch */
+    const float* oe_k;          /* NULL, or per edge f32(dt/L)*f32(dt/(C + G dt/2)) */
+    const double* oe_vi;        /* with oe_k: per edge dt/(C + G dt/2) */
 } ems_lumped;
 
 /* Edge source kinds (src/engine/excite.rs:13-40). */

@@ -180,6 +180,19 @@ int ems_model_add_lumped_port(ems_model* m, int axis, const uint64_t lo[3], cons
  * source); a source on a parallel element needs r. Returns the op index. */
 int ems_model_add_lumped(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r, double l,
                          double c, int series_topology, int record, int port, const double* amp, uint64_t n_amp);
+/* A lumped element with an inductor or in series the way an openEMS file
+ * has it (src/sim/map.rs:820-1000, 1525-1632; model built with openEMS's
+ * rounding): R, L, C spread in csx's equal parts (R·p/s, L·p/s, C·s/p), the
+ * element's C and 1/R replacing the medium's on its edges, the edge
+ * capacitance limited at omega (> 0: 1/(20·omega·R_e), 1/(20·omega²·L_e)
+ * of a parallel element, 1/(20·omega·|Z_e|) of a series branch), openEMS's
+ * order around the branch, and for a parallel inductor with
+ * explicit_inductor openEMS's explicit f32 update. src_w (per edge) and
+ * amp[n] (the source at (n + 1/2)·dt): the element's Thevenin source of a
+ * parallel element with a resistor, or NULL. Returns the op index. */
+int ems_model_add_lumped_openems(ems_model* m, int axis, const uint64_t lo[3], const uint64_t hi[3], double r,
+                                 double l, double c, int series_topology, double omega, int explicit_inductor,
+                                 const double* src_w, const double* amp, uint64_t n_amp);
 
 /* An edge source of `kind` (ems_source_kind) on n edges with the waveform
  * sampled for n_steps steps. nodes: 3*n indices. Returns the op index. */

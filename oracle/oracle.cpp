@@ -134,6 +134,9 @@ struct Lumped {
     uint64_t series = 1;
     bool src_in_branch = false, has_src = false, has_branch = false, record = false;
     uint64_t port_columns = 0;
+    bool openems_order = false;
+    std::vector<float> oe_k, oe_s;  // openEMS's explicit inductor: f32 constant and state
+    std::vector<double> oe_vi;
     std::vector<double> v, bj, bq, bu_prev, j_avg, ru_prev;
     std::vector<double> rec, port_v, port_i;
 };
@@ -661,14 +664,16 @@ struct oracle_engine {
         // src/engine/lumped.rs:1106-1121 pre_e_impl.
         for (size_t e = 0; e < l.node.size(); ++e) {
             double x = (double)u[l.axis][l.node[e]];
-            if (l.has_branch) l.bu_prev[e] = x;
+            if (l.has_branch && !l.openems_order) l.bu_prev[e] = x;
             if (l.record) l.ru_prev[e] = x;
         }
     }
 
     void lumped_post_e(Lumped& l) {
-        // src/engine/lumped.rs:1123-1236 post_e_impl (non-openEMS order),
-        // src/engine/port.rs:276-290 LumpedPort::post_e.
+        // src/engine/lumped.rs:1123-1236 post_e_impl (openEMS's order: the
+        // branch driven by its own previous result, the source after it;
+        // its explicit f32 inductor), src/engine/port.rs:276-290
+        // LumpedPort::post_e.
         float* U = u[l.axis].data();
         const size_t ne = l.node.size();
         bool active = false;
@@ -680,14 +685,25 @@ struct oracle_engine {
                 for (size_t e = 0; e < ne; ++e) l.v[e] += l.src_w[e] * val;
             }
         }
-        if (active && !l.src_in_branch) {
+        auto add_sources = [&]() {
             for (size_t e = 0; e < ne; ++e) {
                 double add = l.cb[e] * l.g_src[e] * l.v[e];
                 if (add != 0.0) U[l.node[e]] = (float)((double)U[l.node[e]] + add);
             }
-        }
+        };
+        if (active && !l.src_in_branch && !l.openems_order) add_sources();
         if (l.has_branch) {
             for (size_t e = 0; e < ne; ++e) {
+                if (!l.oe_k.empty()) {
+                    const float u_l = (float)l.bu_prev[e];
+                    l.oe_s[e] = flush(l.oe_s[e] + flush(l.oe_k[e] * u_l));
+                    const float u_new = flush(U[l.node[e]] - l.oe_s[e]);
+                    l.bj[e] = (double)l.oe_s[e] / l.oe_vi[e];
+                    l.j_avg[e] = l.bj[e];
+                    U[l.node[e]] = u_new;
+                    l.bu_prev[e] = (double)u_new;
+                    continue;
+                }
                 double v_br = (active && l.src_in_branch) ? l.v[e] : 0.0;
                 double u_star = (double)U[l.node[e]];
                 double k = l.two_l_dt[e] * l.bj[e] - l.bq[e] * l.inv_c[e] - v_br + 0.5 * l.bu_prev[e];
@@ -699,8 +715,10 @@ struct oracle_engine {
                 l.bq[e] += dt * jb;
                 l.j_avg[e] = jb;
                 U[l.node[e]] = (float)u_new;
+                if (l.openems_order) l.bu_prev[e] = (double)(float)u_new;
             }
         }
+        if (active && !l.src_in_branch && l.openems_order) add_sources();
         if (l.record) {
             double sum = 0.0;
             for (size_t e = 0; e < ne; ++e) {
@@ -912,6 +930,13 @@ int oracle_create(const ems_engine_desc* d, int threads, oracle_engine** out) {
                 L.rec_c = vec(l->rec_c, ne);
             }
             L.port_columns = l->port_columns;
+            L.openems_order = l->openems_order != 0;
+            if (l->oe_k) {
+                if (!L.has_branch || !l->oe_vi || !L.openems_order) { delete e; return EMS_ERR_INVALID; }
+                L.oe_k.assign(l->oe_k, l->oe_k + ne);
+                L.oe_vi = vec(l->oe_vi, ne);
+                L.oe_s.assign(ne, 0.0f);
+            }
             L.v.assign(ne, 0.0);
             L.bj.assign(ne, 0.0);
             L.bq.assign(ne, 0.0);

@@ -202,6 +202,41 @@ SHEET = f"""<?xml version="1.0" encoding="UTF-8"?>
 """
 
 
+# Lumped elements with an inductor or in series (openEMS's order; the
+# explicit f32 inductor of a parallel L and of a parallel R||L whose edge
+# capacitance openEMS limits; series RLC and series R branches), soft
+# sources on two of them, PMC walls across one.
+LUMPED = f"""<?xml version="1.0" encoding="UTF-8"?>
+<openEMS>
+  <FDTD NumberOfTimesteps="400" endCriteria="1e-30">
+    <Excitation Type="0" f0="3e9" fc="2e9"/>
+    <BoundaryCond xmin="PEC" xmax="PEC" ymin="PEC" ymax="PEC" zmin="PMC" zmax="PMC"/>
+  </FDTD>
+  <ContinuousStructure CoordSystem="0">
+    <Properties>
+      <Material Name="sub"><Property Epsilon="3.0" Kappa="0.01"/>
+        <Primitives><Box Priority="1"><P1 X="0" Y="0" Z="0"/><P2 X="16" Y="13" Z="3"/></Box></Primitives></Material>
+      <LumpedElement Name="pl" Direction="2" Caps="1" L="3e-9"><Primitives><Box Priority="0"><P1 X="4" Y="4" Z="3"/><P2 X="5" Y="4" Z="6"/></Box></Primitives></LumpedElement>
+      <LumpedElement Name="prl" Direction="2" Caps="1" R="60" L="2e-9"><Primitives><Box Priority="0"><P1 X="10" Y="4" Z="4"/><P2 X="10" Y="4" Z="7"/></Box></Primitives></LumpedElement>
+      <LumpedElement Name="srlc" Direction="1" Caps="0" LEtype="1" R="25" L="2e-9" C="1e-12"><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="5"/><P2 X="7" Y="9" Z="5"/></Box></Primitives></LumpedElement>
+      <LumpedElement Name="sr" Direction="2" Caps="1" LEtype="1" R="80"><Primitives><Box Priority="0"><P1 X="13" Y="9" Z="0"/><P2 X="13" Y="9" Z="2"/></Box></Primitives></LumpedElement>
+      <Excitation Name="e1" Type="0" Excite="0,0,1"><Primitives><Box Priority="0"><P1 X="10" Y="4" Z="4"/><P2 X="10" Y="4" Z="7"/></Box></Primitives></Excitation>
+      <Excitation Name="e2" Type="0" Excite="0,1,0"><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="5"/><P2 X="7" Y="9" Z="5"/></Box></Primitives></Excitation>
+      <ProbeBox Name="u_pl" Type="0"><Primitives><Box Priority="0"><P1 X="4" Y="4" Z="3"/><P2 X="4" Y="4" Z="6"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="u_s" Type="0"><Primitives><Box Priority="0"><P1 X="7" Y="7" Z="5"/><P2 X="7" Y="9" Z="5"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="u_sr" Type="0"><Primitives><Box Priority="0"><P1 X="13" Y="9" Z="0"/><P2 X="13" Y="9" Z="2"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="h" Type="3"><Primitives><Box Priority="0"><P1 X="8" Y="6" Z="8"/><P2 X="8" Y="6" Z="8"/></Box></Primitives></ProbeBox>
+    </Properties>
+    <RectilinearGrid DeltaUnit="0.001" CoordSystem="0">
+      <XLines>{_lines(X)}</XLines>
+      <YLines>{_lines(Y)}</YLines>
+      <ZLines>{_lines(Z)}</ZLines>
+    </RectilinearGrid>
+  </ContinuousStructure>
+</openEMS>
+"""
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -220,7 +255,8 @@ def _both(text, schedule=0):
     ("sine", SINE, 0), ("sine", SINE, 1), ("sine", SINE, 3), ("pulses", PULSES, 0), ("pulses", PULSES, 1),
     ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5),
     ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4),
-    ("sheet", SHEET, 0), ("sheet", SHEET, 1), ("sheet", SHEET, 3)])
+    ("sheet", SHEET, 0), ("sheet", SHEET, 1), ("sheet", SHEET, 3),
+    ("lumped", LUMPED, 0), ("lumped", LUMPED, 1), ("lumped", LUMPED, 3)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes
