@@ -232,6 +232,7 @@ def host_lib() -> C.CDLL:
             "ems_model_add_lumped_port": (i, [p, i, p, p, d, i, d, d, d, u]),
             "ems_model_add_lumped": (i, [p, i, p, p, d, d, d, i, i, i, p, u]),
             "ems_model_add_lumped_openems": (i, [p, i, p, p, d, d, d, i, d, i, p, p, u]),
+            "ems_model_add_absorbing_sheet": (i, [p, i, u, i, p, p, d, i]),
             "ems_model_add_source": (i, [p, i, sz, p, p, p, i, d, d, u]),
             "ems_model_add_source_table": (i, [p, i, sz, p, p, p, p, u]),
             "ems_model_add_probe": (i, [p, i, sz, p, p, p, u]),
@@ -642,6 +643,18 @@ class Model:
             None if w is None else w.ctypes.data, None if a is None else a.ctypes.data,
             0 if a is None else len(a)), "add_lumped_openems")
         self.ops.append((OP_LUMPED, "lumped"))
+        return k
+
+    def add_absorbing_sheet(self, normal: int, plane: int, positive: bool, start: Sequence[int],
+                            stop: Sequence[int], velocity: float = 0.0, openems_order: bool = False) -> int:
+        """``AbsorbingSheet::new(engine, AbcSheet{..}, velocity)`` (src/engine/boundary/abc.rs):
+        first-order Mur on the tangential E edges of the rectangle start..stop on mesh
+        plane ``plane`` normal to ``normal``, absorbing waves along +normal (``positive``)
+        or -normal; ``velocity`` <= 0: the local medium velocity per edge."""
+        k = self._check(self._lib.ems_model_add_absorbing_sheet(self._p, normal, plane, int(positive), _u64(start),
+                                                                _u64(stop), velocity, int(openems_order)),
+                        "add_absorbing_sheet")
+        self.ops.append((OP_MUR, "abc"))
         return k
 
     def add_sheet(self, edges: Sequence[tuple], f_max: float | None = None) -> int:

@@ -1902,6 +1902,85 @@ int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6],
     return (int)m->ops.size() - 1;
 }
 
+// An absorbing sheet inside the domain (AbsorbingSheet::new,
+// src/engine/boundary/abc.rs:131-240): the tangential E edges of the
+// rectangle start..stop on mesh plane `plane` normal to `normal`, each with
+// its neighbour one node against the outward normal (positive: +normal) and
+// the first-order Mur coefficient (v·dt − Δ)/(v·dt + Δ) with v·dt rounded to
+// f32 in openEMS's order; v the given velocity or, for velocity <= 0, the
+// local c0/sqrt(eps_r·mu_r) of the neighbour edge and the H face spanning
+// both. Edges kept at zero (metal) are left out unless the plane is outer.
+// The update is a Mur face's (pre_e saves u_b^n and u_1^n, post_e writes
+// u_b), so the sheet is an EMS_OP_MUR table of face edges.
+int ems_model_add_absorbing_sheet(ems_model* m, int normal, uint64_t plane, int positive, const uint64_t start[3],
+                                  const uint64_t stop[3], double velocity, int openems_order) {
+    if (!m->built) return set_err(m, "build the model before adding operators"), -1;
+    if (normal < 0 || normal > 2) return set_err(m, "absorbing sheet: invalid normal"), -1;
+    const uint64_t* n = m->n;
+    const int a = normal;
+    if (plane >= n[a]) return set_err(m, "absorbing sheet: plane outside the mesh"), -1;
+    if (positive ? plane == 0 : plane + 1 >= n[a])
+        return set_err(m, "absorbing sheet: no mesh plane on its absorbing side"), -1;
+    const uint64_t inner_plane = positive ? plane - 1 : plane + 1;
+    for (int d = 0; d < 3; ++d)
+        if (d != a && (start[d] > stop[d] || stop[d] >= n[d])) return set_err(m, "absorbing sheet: invalid range"), -1;
+    const uint64_t lo = std::min(plane, inner_plane);
+    const double delta = m->delta(a, lo), dt = m->dt;
+    const bool outer = plane == 0 || plane == n[a] - 1;
+    auto op = std::make_unique<OpStore>();
+    op->kind = EMS_OP_MUR;
+    for (int t = 0; t < 3; ++t) {
+        if (t == a) continue;
+        const int o = 3 - a - t;
+        for (uint64_t p = start[t]; p < stop[t]; ++p)
+            for (uint64_t q = start[o]; q <= stop[o]; ++q) {
+                uint64_t node[3], inner[3];
+                node[a] = plane;
+                node[t] = p;
+                node[o] = q;
+                const uint64_t idx = m->index(node[0], node[1], node[2]);
+                if (!outer && m->co[t][idx] == 0.0f && m->co[3 + t][idx] == 0.0f) continue;
+                for (int d = 0; d < 3; ++d) inner[d] = node[d];
+                inner[a] = inner_plane;
+                double v = velocity;
+                if (!(velocity > 0.0)) {
+                    double eps, kap, mu, sig;
+                    edge_eps(m, t, inner, eps, kap);
+                    uint64_t face[3] = {node[0], node[1], node[2]};
+                    face[a] = lo;
+                    edge_mu(m, o, face, mu, sig);
+                    v = C0 / std::sqrt(eps * mu);
+                }
+                if (!(std::isfinite(v) && v > 0.0)) return set_err(m, "absorbing sheet: invalid phase velocity"), -1;
+                const double vdt = openems_order ? (double)(float)(v * dt) : v * dt;
+                const float k = (float)((vdt - delta) / (vdt + delta));
+                const uint64_t in_idx = m->index(inner[0], inner[1], inner[2]);
+                op->axis.push_back((uint8_t)t);
+                op->node.push_back(idx);
+                op->inner.push_back(in_idx);
+                op->inner.push_back(in_idx);
+                op->mk.push_back(k);
+                op->mk.push_back(k);
+                op->mcap.push_back(0.0);
+            }
+    }
+    ems_mur& M = op->mur;
+    M.n = op->node.size();
+    M.n_edges = M.n;
+    M.axis = op->axis.data();
+    M.node = op->node.data();
+    M.inner = op->inner.data();
+    M.k = op->mk.data();
+    M.hold = nullptr;
+    M.count_energy = 0;
+    M.cap = nullptr;
+    M.openems_order = openems_order ? 1 : 0;
+    M.openems_corners = 0;
+    m->ops.push_back(std::move(op));
+    m->refresh_desc();
+    return (int)m->ops.size() - 1;
+}
+
 // ---------------------------------------------------------------------------
 // Field samplers (src/engine/dump.rs:281-760).
 

@@ -684,7 +684,7 @@ def parse(text: str) -> OpenEmsFile:
             if tr is not None:
                 boxes[-1] = Transformed(boxes[-1], _transform_matrix(tr), prio)
         if el.tag not in ("Material", "Metal", "Excitation", "ProbeBox", "LorentzMaterial", "DebyeMaterial",
-                          "LumpedElement", "ConductingSheet"):
+                          "LumpedElement", "ConductingSheet", "AbsorbingBC"):
             raise NotImplementedError(f"property {el.tag}")
         if el.tag == "ProbeBox" and not boxes and only_long_cylinders:
             continue
@@ -910,6 +910,7 @@ class Setup:
         self.h_sources = []
         self.excited = self._excitation_edges()
         self._mur(m)
+        self._absorbing_sheets(m)
         self._excitations(m)
         self.probes: list[ProbeSpec] = []
         self._probes(m)
@@ -1671,6 +1672,55 @@ class Setup:
                 hold = {fc: steps + 10 for fc in held}
         self._mur_media(m, [fc for fc, v in faces.items() if v is None])
         m.add_mur(faces, hold=hold, flags=MUR_COUNT_ENERGY | MUR_OPENEMS_CORNERS | MUR_OPENEMS_ORDER)
+
+    def _absorbing_sheets(self, m):
+        """csx ``AbsorbingBC`` properties (src/compile/mod.rs:106-125,
+        1999-2080, 1424-1432): every box, snapped to the nearest mesh lines,
+        must be flat along exactly one axis (the sheet normal; volumes,
+        lines and points are ignored with a warning); NormalSignPositive
+        is the sign of the normal into the region the sheet terminates, so
+        the sheet absorbs waves along the opposite sign; PhaseVelocity > 0
+        as given, 0 the local medium velocity (negative or not finite: the
+        local one, with a warning); AbsorbingBoundaryType other than 0
+        (MUR_1ST) runs as first-order Mur with a warning. Installed with
+        openEMS's order (``Model.add_absorbing_sheet``)."""
+        f = self.file
+        lines = f.lines
+        for p in f.props:
+            if p.kind != "AbsorbingBC":
+                continue
+            if not p.boxes:
+                self.warnings.append(f"AbsorbingBC {p.name!r}: no primitive; ignored")
+                continue
+            typ = int(float(p.attrs.get("AbsorbingBoundaryType", "0")))
+            if typ != 0:
+                self.warnings.append(f"AbsorbingBC {p.name!r}: AbsorbingBoundaryType {typ} not implemented; "
+                                     "first-order Mur (MUR_1ST) used")
+            v = _f(p.attrs.get("PhaseVelocity"), 0.0)
+            if not (math.isfinite(v) and v > 0.0):
+                if v != 0.0:
+                    self.warnings.append(f"AbsorbingBC {p.name!r}: PhaseVelocity {v} invalid; local medium "
+                                         "velocity used")
+                v = 0.0
+            positive = p.attrs.get("NormalSignPositive", "0") in ("0", "false", "False")
+            for b in p.boxes:
+                if not isinstance(b, Box):
+                    raise NotImplementedError(f"AbsorbingBC {p.name!r}: primitives other than boxes")
+                snap = [(int(np.argmin(np.abs(np.asarray(lines[q]) - b.p1[q]))),
+                         int(np.argmin(np.abs(np.asarray(lines[q]) - b.p2[q])))) for q in range(3)]
+                start = [min(x) for x in snap]
+                stop = [max(x) for x in snap]
+                flat = [q for q in range(3) if start[q] == stop[q]]
+                if len(flat) != 1:
+                    what = "a volume" if not flat else "a line or point"
+                    self.warnings.append(f"AbsorbingBC {p.name!r}: primitive is {what} on the mesh, not a sheet; "
+                                         "ignored")
+                    continue
+                d = flat[0]
+                if b.p1[d] != b.p2[d]:
+                    self.warnings.append(f"AbsorbingBC {p.name!r}: primitive has a thickness along "
+                                         f"{'xyz'[d]}; flattened onto mesh plane {start[d]}")
+                m.add_absorbing_sheet(d, start[d], positive, start, stop, velocity=v, openems_order=True)
 
     def _mur_media(self, m, faces):
         """The medium of each edge of a Mur face without a phase velocity

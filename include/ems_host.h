@@ -221,6 +221,17 @@ int ems_model_add_probe(ems_model* m, int quantity, size_t n, const int* axis, c
 int ems_model_add_mur(ems_model* m, const int mode[6], const double velocity[6], const uint64_t hold_until[6],
                       int flags);
 
+/* An absorbing sheet inside the domain (csx AbsorbingBC, AbsorbingSheet::new,
+ * src/engine/boundary/abc.rs:131-240): first-order Mur on the tangential E
+ * edges of the rectangle start..stop (inclusive nodes; the normal entry
+ * ignored) on mesh plane `plane` normal to `normal`, absorbing waves that
+ * travel along +normal (positive) or -normal, at phase velocity `velocity`
+ * [m/s] or, for velocity <= 0, the local c0/sqrt(eps_r mu_r) per edge;
+ * openems_order: openEMS's order of the update and its f32 v·dt. Installed
+ * as an EMS_OP_MUR table of face edges. Returns the op index or -1. */
+int ems_model_add_absorbing_sheet(ems_model* m, int normal, uint64_t plane, int positive, const uint64_t start[3],
+                                  const uint64_t stop[3], double velocity, int openems_order);
+
 /* Conducting sheets (ConductingSheet::new(f_max), push, add_to;
  * src/engine/sheet.rs:529-935) on the built model, Cartesian, outlines on
  * mesh lines: n sheet edges, edge e the E edge along axis[e] at node

@@ -237,6 +237,13 @@ LUMPED = f"""<?xml version="1.0" encoding="UTF-8"?>
 """
 
 
+# An absorbing sheet (AbsorbingBC) across the lumped model, absorbing
+# waves along -x at the local medium velocity.
+ABC = LUMPED.replace("</Properties>", """  <AbsorbingBC Name="abc" NormalSignPositive="1" PhaseVelocity="0">
+        <Primitives><Box Priority="0"><P1 X="12" Y="0" Z="0"/><P2 X="12" Y="13" Z="12"/></Box></Primitives></AbsorbingBC>
+    </Properties>""")
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -256,7 +263,7 @@ def _both(text, schedule=0):
     ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5),
     ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4),
     ("sheet", SHEET, 0), ("sheet", SHEET, 1), ("sheet", SHEET, 3),
-    ("lumped", LUMPED, 0), ("lumped", LUMPED, 1), ("lumped", LUMPED, 3)])
+    ("lumped", LUMPED, 0), ("lumped", LUMPED, 1), ("lumped", LUMPED, 3), ("abc", ABC, 0), ("abc", ABC, 1)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes

@@ -113,6 +113,8 @@ CASES = [
     # the low-impedance series branch; tests/openems_rsweep.rs rs_109 1e-3).
     ("lumped_l", 1e-12), ("lumped_graded_rl", 1e-12), ("lumped_exc", 1e-4), ("lumped_graded", 1e-4),
     ("lumped_rc", 2e-3), ("rs_109", 1e-3),
+    # Absorbing sheets (AbsorbingBC) inside the domain, both normal signs.
+    ("sweep_abc_line_s0_t0", 1e-12), ("sweep_abc_line_s1_t1", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
