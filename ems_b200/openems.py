@@ -49,6 +49,7 @@ from __future__ import annotations
 import math
 import os
 import re
+import struct
 import xml.etree.ElementTree as ET
 from dataclasses import dataclass, field
 
@@ -419,6 +420,42 @@ class LinPoly:
 
 
 @dataclass
+class Polyhedron:
+    """A closed triangle mesh (CSXCAD Polyhedron): vertices and faces
+    (vertex index triples); inside where the solid angle its faces subtend
+    sums to 4π, or 2π on a face (the generalised winding number, van
+    Oosterom and Strackee's triangle solid angle; closed), not grown by the
+    inside tolerance (the
+    reference grows only the primitives it lists, src/compile/openems.rs:
+    459-525); ``p1``/``p2`` its bounding box."""
+    vertices: list
+    faces: list
+    priority: int
+    p1: tuple = ()
+    p2: tuple = ()
+
+    def __post_init__(self):
+        self.p1 = tuple(min(v[a] for v in self.vertices) for a in range(3))
+        self.p2 = tuple(max(v[a] for v in self.vertices) for a in range(3))
+
+    def inside(self, x, y, z, tol):
+        c = np.broadcast_arrays(np.asarray(x, np.float64), np.asarray(y, np.float64), np.asarray(z, np.float64))
+        total = np.zeros(c[0].shape)
+        for f in self.faces:
+            r = [[self.vertices[i][q] - c[q] for q in range(3)] for i in f]
+            (ax, ay, az), (bx, by, bz), (cx, cy, cz) = r
+            det = ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx)
+            la = np.sqrt(ax * ax + ay * ay + az * az)
+            lb = np.sqrt(bx * bx + by * by + bz * bz)
+            lc = np.sqrt(cx * cx + cy * cy + cz * cz)
+            den = (la * lb * lc + (ax * bx + ay * by + az * bz) * lc + (ax * cx + ay * cy + az * cz) * lb
+                   + (bx * cx + by * cy + bz * cz) * la)
+            total += 2.0 * np.arctan2(det, den)
+        # 4π inside, 0 outside, 2π on a face: closed, as CSXCAD's inside tests.
+        return np.abs(total) > math.pi
+
+
+@dataclass
 class Wire:
     """A wire (CSXCAD Wire): the points within ``radius`` of its polyline
     (segments with round ends), closed; grown by the inside tolerance
@@ -520,6 +557,7 @@ class OpenEmsFile:
     background: dict | None = None
     cell_constant: bool = False   # CellConstantMaterial: cell-centre materials
     f_max: float | None = None    # <FDTD f_max>: the explicit highest frequency
+    notes: list = field(default_factory=list)  # warnings of the reading
 
 
 def _f(x, default=None):
@@ -594,7 +632,29 @@ def _parameters(root):
     return root
 
 
-def parse(text: str) -> OpenEmsFile:
+def read_stl(path: str) -> list:
+    """The triangles of an STL file, ASCII or binary: [(v0, v1, v2)]."""
+    with open(path, "rb") as h:
+        data = h.read()
+    if data[:5].lower() == b"solid" and b"facet" in data[:1024]:
+        verts = [tuple(float(x) for x in ln.split()[1:4]) for ln in data.decode("ascii", "replace").splitlines()
+                 if ln.strip().startswith("vertex")]
+        if len(verts) % 3:
+            raise ValueError(f"{path}: vertices not in threes")
+        return [tuple(verts[3 * i:3 * i + 3]) for i in range(len(verts) // 3)]
+    n = struct.unpack_from("<I", data, 80)[0]
+    if len(data) < 84 + 50 * n:
+        raise ValueError(f"{path}: truncated binary STL")
+    tris = []
+    for i in range(n):
+        v = struct.unpack_from("<12f", data, 84 + 50 * i)
+        tris.append(((v[3], v[4], v[5]), (v[6], v[7], v[8]), (v[9], v[10], v[11])))
+    return tris
+
+
+def parse(text: str, base_dir: str | None = None) -> OpenEmsFile:
+    """An openEMS model file; ``base_dir``: where files it names (STL
+    meshes) are read from (the current directory without one)."""
     root = _parameters(ET.fromstring(text))
     fd = root.find("FDTD")
     if fd is None:
@@ -628,6 +688,7 @@ def parse(text: str) -> OpenEmsFile:
         v = sorted(set(float(x) for x in grid.find(tag).text.split(",")))  # openEMS sorts, drops repeats
         lines.append(v)
     props = []
+    notes: list[str] = []
     pr = cs.find("Properties")
     for q, el in enumerate(list(pr) if pr is not None else []):
         boxes = []
@@ -637,6 +698,12 @@ def parse(text: str) -> OpenEmsFile:
             return tuple(float(e.get(c)) for c in "XYZ")
 
         for b in (list(prims) if prims is not None else []):
+            if el.tag == "LumpedElement" and b.tag != "Box":
+                # src/io/openems/model.rs:396-411: openEMS places lumped
+                # elements on boxes only and skips other primitives.
+                notes.append(f"lumped element {el.get('Name', '')!r}: a {b.tag} primitive is not supported by "
+                             "openEMS (boxes only); skipped, as openEMS does")
+                continue
             tr = b.find("Transformation")
             if tr is not None and (el.tag not in MATERIALS + ("Metal",) or b.tag not in
                                    ("Box", "Sphere", "SphericalShell", "Cylinder", "CylindricalShell")):
@@ -660,6 +727,19 @@ def parse(text: str) -> OpenEmsFile:
                 verts = [(float(q.get("X1")), float(q.get("X2"))) for q in b.findall("Vertex")]
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")),
                                      float(b.get("Length", "0")), verts, prio))
+            elif b.tag == "Polyhedron" and el.tag in MATERIALS + ("Metal",) and tr is None:
+                verts = [tuple(float(x) for x in v.text.split(",")) for v in b.findall("Vertex")]
+                tri = [tuple(int(x) for x in f_.text.split(",")) for f_ in b.findall("Face")]
+                if not verts or not tri or any(len(f_) != 3 or max(f_) >= len(verts) for f_ in tri):
+                    raise NotImplementedError(f"polyhedron in {el.get('Name')!r}: faces other than triangles")
+                boxes.append(Polyhedron(verts, tri, prio))
+            elif b.tag == "PolyhedronReader" and el.tag in MATERIALS + ("Metal",) and tr is None:
+                if b.get("FileType", "STL").upper() != "STL":
+                    raise NotImplementedError(f"PolyhedronReader in {el.get('Name')!r}: file type "
+                                              f"{b.get('FileType')!r}")
+                tris = read_stl(os.path.join(base_dir or ".", b.get("FileName", "")))
+                verts = [v for t in tris for v in t]
+                boxes.append(Polyhedron(verts, [(3 * i, 3 * i + 1, 3 * i + 2) for i in range(len(tris))], prio))
             elif b.tag == "Wire" and el.tag == "Metal" and tr is None:
                 radius = float(b.get("WireRadius", "0"))
                 if radius < 0.5 * min(float(np.min(np.diff(v))) for v in lines if len(v) > 1):
@@ -673,7 +753,7 @@ def parse(text: str) -> OpenEmsFile:
                 boxes.append(LinPoly(int(float(b.get("NormDir", "2"))), float(b.get("Elevation", "0")), 0.0,
                                      verts, prio))
             elif b.tag in ("Sphere", "SphericalShell", "Cylinder", "CylindricalShell") and \
-                    el.tag in MATERIALS + ("Metal",):
+                    el.tag in MATERIALS + ("Metal", "Excitation"):
                 sph = b.tag.startswith("Spher")
                 a0 = pt(b.find("Center")) if sph else pt(b.find("P1"))
                 b0 = a0 if sph else pt(b.find("P2"))
@@ -738,7 +818,8 @@ def parse(text: str) -> OpenEmsFile:
                        factor if 0.0 < factor <= 1.0 else 1.0, method if method in (1, 3) else 1,
                        os_ if os_ >= 2 else 4, sig, faces, mur_v, props,
                        dict(bg.attrib) if bg is not None else None,
-                       fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"), _f(fd.get("f_max")))
+                       fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"), _f(fd.get("f_max")),
+                       notes)
 
 
 # ---------------------------------------------------------------------------
@@ -857,7 +938,7 @@ class Setup:
     def __init__(self, f: OpenEmsFile):
         from . import PEC, PMC, Model
         self.file = f
-        self.warnings: list[str] = []
+        self.warnings: list[str] = list(f.notes)
         u = f.unit
         lines_m = [np.array(v) * u for v in f.lines]
         n = [len(v) for v in f.lines]
@@ -1579,7 +1660,9 @@ class Setup:
             if p.kind != "Excitation":
                 continue
             for b in p.boxes:
-                if all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3)):
+                inside = (all(self._inside_prim(pt[q], min(b.p1[q], b.p2[q]), max(b.p1[q], b.p2[q])) for q in range(3))
+                          if isinstance(b, Box) else bool(b.inside(pt[0], pt[1], pt[2], self.tol)))
+                if inside:
                     key = (b.priority, -p.order)
                     if best is None or key > best[0]:
                         best = (key, p)
@@ -1587,8 +1670,9 @@ class Setup:
 
     def _excitation_edges(self):
         """(E?, axis, node, weight per unit amplitude, property) of every
-        driven edge: E edges whose both nodes lie in the closed box, H dual
-        edges whose midpoint does; weight = Excite × (dual) edge length.
+        driven edge: E edges whose both nodes lie in the closed box (whose
+        midpoint lies in a sphere, cylinder or shell), H dual edges whose
+        midpoint does; weight = Excite × (dual) edge length.
         openEMS gives each edge to one excitation: the one owning the edge
         midpoint (E types) or the dual edge's (H types)."""
         out = []
@@ -1610,8 +1694,15 @@ class Setup:
                     if exc[a] == 0.0:
                         continue
                     rng = []
+                    box = isinstance(b, Box)
                     for q in range(3):
-                        if e_type:
+                        if e_type and not box:
+                            # A round primitive: the candidates of its
+                            # bounding box, then both nodes inside it.
+                            pts = [i for i in range(n[q] - (1 if q == a else 0))
+                                   if lines[q][i + (1 if q == a else 0)] >= lo[q] - self.tol
+                                   and lines[q][i] <= hi[q] + self.tol]
+                        elif e_type:
                             pts = [i for i in range(n[q] - (1 if q == a else 0))
                                    if self._inside_prim(lines[q][i], lo[q], hi[q])
                                    and (q != a or self._inside_prim(lines[q][i + 1], lo[q], hi[q]))]
@@ -1626,6 +1717,11 @@ class Setup:
                         for j in rng[1]:
                             for k in rng[2]:
                                 node = (i, j, k)
+                                if e_type and not box:
+                                    pm = [lines[q][node[q]] for q in range(3)]
+                                    pm[a] = 0.5 * (lines[a][node[a]] + lines[a][node[a] + 1])
+                                    if not b.inside(*pm, self.tol):
+                                        continue
                                 if e_type:
                                     length = self.model_delta(a, node[a])
                                 else:
@@ -2116,7 +2212,7 @@ class Results:
 
 def load(path: str) -> Setup:
     with open(path) as h:
-        return Setup(parse(h.read()))
+        return Setup(parse(h.read(), os.path.dirname(os.path.abspath(path))))
 
 
 def loads(text: str) -> Setup:

@@ -115,6 +115,13 @@ CASES = [
     ("lumped_rc", 2e-3), ("rs_109", 1e-3),
     # Absorbing sheets (AbsorbingBC) inside the domain, both normal signs.
     ("sweep_abc_line_s0_t0", 1e-12), ("sweep_abc_line_s1_t1", 1e-12),
+    # An excitation on a sphere (E edges by their midpoint); a lumped element
+    # on a cylinder (skipped, as openEMS does); a polyhedron material (a
+    # cube) exact, one read from an STL file (a tetrahedron) to 2.4e-4 (a
+    # known gap: the reference reaches 1e-6 with csx's polyhedron test, a
+    # third-party crate not in its tree).
+    ("sweep_exc_sphere", 1e-12), ("sweep_lumped_on_cyl", 1e-12), ("sweep_prim_polyhedron_cube", 1e-12),
+    ("sweep_prim_stl", 5e-4),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
@@ -245,7 +252,7 @@ def test_probe_skip_warnings():
 @have
 @pytest.mark.parametrize("case,why", [
     ("rs_l_order", "on a conducting sheet"), ("pml_cyl", "cylindrical"),
-    ("sweep_exc_sphere", "Sphere"), ("sweep_prim_polyhedron_cube", "Polyhedron")])
+    ("sweep_prim_curve_diag", "Curve"), ("sweep_prim_cs_cyl_box", "cylindrical")])
 def test_unsupported_features_refused(case, why):
     with pytest.raises(NotImplementedError, match=why):
         OE.load(os.path.join(FIXTURES, case, "model.xml"))
