@@ -70,7 +70,11 @@ MATERIALS = ("Material", "LorentzMaterial", "DebyeMaterial")
 _FUNCS = {"exp": math.exp, "cos": math.cos, "sin": math.sin, "tan": math.tan, "sqrt": math.sqrt,
           "abs": abs, "log": math.log, "log10": math.log10, "atan": math.atan, "cosh": math.cosh,
           "sinh": math.sinh, "tanh": math.tanh}
-_TOKEN = re.compile(r"\s*(?:(\d+\.?\d*(?:[eE][-+]?\d+)?|\.\d+(?:[eE][-+]?\d+)?)|([A-Za-z_]\w*)|(.))")
+_TOKEN = re.compile(r"\s*(?:(\d+\.?\d*(?:[eE][-+]?\d+)?|\.\d+(?:[eE][-+]?\d+)?)|([A-Za-z_]\w*)|(<=|>=|!=|.))")
+
+
+_COMPARE = {"<": lambda a, b: a < b, ">": lambda a, b: a > b, "<=": lambda a, b: a <= b,
+            ">=": lambda a, b: a >= b, "=": lambda a, b: a == b, "!=": lambda a, b: a != b}
 
 
 class Expression:
@@ -84,7 +88,7 @@ class Expression:
         self.variables = tuple(variables)
         self._tok = [(m.group(1), m.group(2), m.group(3)) for m in _TOKEN.finditer(text) if any(m.groups())]
         self._i = 0
-        self._tree = self._sum()
+        self._tree = self._compare()
         if self._i != len(self._tok):
             raise ValueError(f"expression {text!r}: unexpected {self._tok[self._i]}")
 
@@ -96,6 +100,17 @@ class Expression:
             self._i += 1
             return True
         return False
+
+    def _compare(self):
+        """fparser's comparisons (lowest precedence): 1 where true, else 0."""
+        node = self._sum()
+        while True:
+            for op in ("<=", ">=", "!=", "<", ">", "="):
+                if self._take(op):
+                    node = (op, node, self._sum())
+                    break
+            else:
+                return node
 
     def _sum(self):
         node = self._product()
@@ -140,7 +155,7 @@ class Expression:
             if name in _FUNCS:
                 if not self._take("("):
                     raise ValueError(f"expression {self.text!r}: {name} needs (")
-                arg = self._sum()
+                arg = self._compare()
                 if not self._take(")"):
                     raise ValueError(f"expression {self.text!r}: missing )")
                 return ("fn", name, arg)
@@ -150,7 +165,7 @@ class Expression:
                 return ("num", math.pi)
             raise ValueError(f"expression {self.text!r}: unknown name {name}")
         if self._take("("):
-            node = self._sum()
+            node = self._compare()
             if not self._take(")"):
                 raise ValueError(f"expression {self.text!r}: missing )")
             return node
@@ -168,6 +183,8 @@ class Expression:
             if k == "fn":
                 return _FUNCS[n[1]](ev(n[2]))
             a, b = ev(n[1]), ev(n[2])
+            if k in _COMPARE:
+                return 1.0 if _COMPARE[k](a, b) else 0.0
             return {"+": a + b, "-": a - b, "*": a * b, "/": a / b if b != 0 else math.inf}.get(k) \
                 if k != "^" else a ** b
         return float(ev(self._tree))
@@ -197,6 +214,8 @@ class Expression:
                 return a * b
             if k == "/":
                 return np.divide(a, b)
+            if k in _COMPARE:
+                return np.where(_COMPARE[k](a, b), 1.0, 0.0)
             return np.power(a, b)
         with np.errstate(all="ignore"):
             return np.asarray(ev(self._tree), dtype=np.float64)
@@ -537,6 +556,9 @@ class Prop:
     # Weighting functions of a material's Epsilon, Mue, Kappa, Sigma: per
     # quantity three expressions in x, y, z (drawing units), None for 1.
     weight: dict = field(default_factory=dict)
+    # The property's user attributes (its <Attributes> child: a waveguide
+    # probe's ModeFunctionX/Y/Z).
+    user: dict = field(default_factory=dict)
 
 
 @dataclass
@@ -798,8 +820,9 @@ def parse(text: str, base_dir: str | None = None) -> OpenEmsFile:
                 props.append(Prop(el.tag, f"{el.get('Name', '')}_{t}", dict(el.attrib),
                                   dict(sub.attrib) if sub is not None else {}, [b], fd_list, q, weight))
             continue
+        user_el = el.find("Attributes")
         props.append(Prop(el.tag, el.get("Name", ""), dict(el.attrib), dict(sub.attrib) if sub is not None else {},
-                          boxes, fd_list, q, weight))
+                          boxes, fd_list, q, weight, dict(user_el.attrib) if user_el is not None else {}))
     # src/fdtd/convert.rs:32-47: OverSampling below 2 → 4; endCriteria
     # absent or 0 → openEMS's default, negative → none; TimeStepFactor
     # outside (0, 1] → 1 and TimeStepMethod other than 1 or 3 → 1 (what
@@ -929,6 +952,9 @@ class ProbeSpec:
     oversampling: int | None = None
     start_time: float = 0.0
     stop_time: float = 0.0
+    # Waveguide probes: (weight, [(area, mode (2,), (op x, op y))]) for the
+    # mode purity column.
+    purity: tuple | None = None
 
 
 class Setup:
@@ -1902,6 +1928,113 @@ class Setup:
                 if typ in (2, 3):
                     self.h_sources.append((typ == 3, edges, amp.astype(np.float32)))
 
+    def _mode_probe(self, m, p, typ, weight, os_, window):
+        """A waveguide (mode-matching) probe with openEMS's sampling
+        (src/compile/mode.rs:1-60, 147-258, 386-540): the box snapped to
+        the nearest lines, its normal NormDir or its flat axis; samples at
+        the box's nodes (voltage, type 10) or at the centres of its cells
+        (current, type 11), never on the outermost mesh lines; the mode
+        function ModeFunctionX/Y/Z (drawing units) at each sample,
+        normalised by the probe itself, V = w·Σ E_t·f·A/√(Σ|f_t|²·A) with
+        E_t at a node the linear interpolation of the two edges along t
+        through it, I = w·Σ H_t·f·A/√(Σ|f_t|²·A) with H_t at the cell's
+        lower corner (the mean of the two dual edges beside it, each the
+        mean of the H planes k ± ½). The value is one probe; each sample's
+        two field components are probes too, for the mode purity
+        w·(Σ A·F·f)²/(Σ A·|F|²·Σ A·|f|²)."""
+        from . import CURRENT, VOLTAGE
+        f, n = self.file, self.nodes
+        lines, lm, unit = f.lines, self.lines_m, f.unit
+        funcs = []
+        for c in "XYZ":
+            src = p.user.get(f"ModeFunction{c}", "0")
+            funcs.append(Expression(src, ("x", "y", "z")))
+        b0 = p.boxes[0]
+        near = lambda q, v: int(np.argmin(np.abs(np.asarray(lines[q]) - v)))  # noqa: E731
+        start = [near(q, b0.p1[q]) for q in range(3)]
+        stop = [near(q, b0.p2[q]) for q in range(3)]
+        norm = p.attrs.get("NormDir")
+        if norm is not None:
+            nn = int(float(norm))
+        else:
+            flat = [q for q in range(3) if start[q] == stop[q]]
+            if len(flat) != 1:
+                self.warnings.append(f"waveguide probe {p.name!r}: no normal direction; ignored")
+                return
+            nn = flat[0]
+        k = start[nn]
+        lo = [min(start[q], stop[q]) for q in range(3)]
+        hi = [max(start[q], stop[q]) for q in range(3)]
+        current = typ == 11
+        ta, tb = [q for q in range(3) if q != nn]
+        delta = lambda q, i: float(lm[q][i + 1] - lm[q][i])  # noqa: E731
+
+        def rng(d):
+            top = hi[d] - 1 if current else hi[d]
+            return range(max(lo[d], 1), min(top, n[d] - 2) + 1)
+
+        samples = []
+        for i in rng(ta):
+            for j in rng(tb):
+                pt = [0.0] * 3
+                pt[nn] = float(lm[nn][k])
+                if current:
+                    pt[ta] = 0.5 * float(lm[ta][i] + lm[ta][i + 1])
+                    pt[tb] = 0.5 * float(lm[tb][j] + lm[tb][j + 1])
+                    area = delta(ta, i) * delta(tb, j)
+                else:
+                    pt[ta], pt[tb] = float(lm[ta][i]), float(lm[tb][j])
+                    area = self.model_dual(ta, i) * self.model_dual(tb, j)
+                env = dict(x=pt[0] / unit, y=pt[1] / unit, z=pt[2] / unit)
+                samples.append(((i, j), (float(funcs[ta].evaluate(**env)), float(funcs[tb].evaluate(**env))), area))
+        ra, rb = rng(ta), rng(tb)
+        llo, lhi = [k] * 3, [k] * 3
+        if len(ra) and len(rb):
+            llo[ta], lhi[ta], llo[tb], lhi[tb] = ra[0], ra[-1], rb[0], rb[-1]
+        at = lambda idx: tuple(float(lm[q][idx[q]]) for q in range(3))  # noqa: E731
+        location = ((at(llo), llo), (at(lhi), lhi))
+        q_kind = CURRENT if current else VOLTAGE
+        norm2 = sum((fv[0] ** 2 + fv[1] ** 2) * area for _, fv, area in samples)
+        kind = "current_mode" if current else "voltage_mode"
+        if not (norm2 > 0.0 and math.isfinite(norm2)):
+            self.warnings.append(f"waveguide probe {p.name!r}: the mode function is zero on the probe plane; "
+                                 "it reads 0")
+            kk = m.add_probe(q_kind, [(0, (0, 0, 0), 0.0)])
+            self.probes.append(ProbeSpec(p.name, kind, [kk], location, p.fd, os_, *window, (weight, [])))
+            return
+        scale = 1.0 / math.sqrt(norm2)
+        planes = ([(k - 1, 0.5), (k, 0.5)] if (k > 0 and k + 1 < n[nn]) else
+                  [(k - 1, 1.0)] if k > 0 else [(k, 1.0)] if k + 1 < n[nn] else [])
+        entries, purity = [], []
+        for (i, j), fv, area in samples:
+            w = area * scale
+            fields = [[], []]
+            for c, (t, o) in enumerate(((ta, tb), (tb, ta))):
+                it, io = (i, j) if c == 0 else (j, i)
+                fc = fv[c] * w
+                node = [0, 0, 0]
+                node[nn], node[o] = k, io
+                if current:
+                    for oc in (io - 1, io):
+                        for kp, wp in planes:
+                            node[t], node[o], node[nn] = it, oc, kp
+                            coef = 0.5 * wp / self.model_dual(t, it)
+                            fields[c].append((t, tuple(node), coef))
+                            if fc != 0.0 and math.isfinite(fc * coef):
+                                entries.append((t, tuple(node), fc * 0.5 * wp / self.model_dual(t, it)))
+                else:
+                    dl, dh = delta(t, it - 1), delta(t, it)
+                    wl, wh = dh / (dl + dh), dl / (dl + dh)
+                    for idx, cw in ((it - 1, wl / dl), (it, wh / dh)):
+                        node[t] = idx
+                        fields[c].append((t, tuple(node), cw))
+                        if fc != 0.0 and math.isfinite(fc * cw):
+                            entries.append((t, tuple(node), fc * cw))
+            ops = tuple(m.add_probe(q_kind, fl) for fl in fields)
+            purity.append((area, fv, ops))
+        kk = m.add_probe(q_kind, [(a, nd, v * weight) for a, nd, v in entries] or [(0, (0, 0, 0), 0.0)])
+        self.probes.append(ProbeSpec(p.name, kind, [kk], location, p.fd, os_, *window, (weight, purity)))
+
     def _probes(self, m):
         from . import CURRENT, VOLTAGE
         f = self.file
@@ -1917,6 +2050,9 @@ class Setup:
             window = (_f(p.attrs.get("StartTime"), 0.0), _f(p.attrs.get("StopTime"), 0.0))
             os_attr = p.attrs.get("OverSampling")
             os_ = int(float(os_attr)) if os_attr is not None else None
+            if typ in (10, 11):
+                self._mode_probe(m, p, typ, weight, os_, window)
+                continue
             if typ not in (0, 1, 2, 3):
                 self.warnings.append(f"probe {p.name!r}: type {typ} not supported; ignored")
                 continue
@@ -2114,6 +2250,27 @@ class Setup:
                 break
         return steps
 
+    @staticmethod
+    def _purity(engine, p) -> np.ndarray:
+        """The mode purity series of a waveguide probe (Probe::mode_purity,
+        src/engine/probe.rs:314-330): w·(Σ A·F·f)²/(Σ A·|F|²·Σ A·|f|²) per
+        sample, 0 where the field is 0."""
+        weight, samples = p.purity
+        n = len(engine.samples(p.ops[0]))
+        if not samples:
+            return np.zeros(n)
+        dot = np.zeros(n)
+        ff = np.zeros(n)
+        mm = 0.0
+        for area, fv, (ox, oy) in samples:
+            fx, fy = np.asarray(engine.samples(ox)), np.asarray(engine.samples(oy))
+            dot += area * (fx * fv[0] + fy * fv[1])
+            ff += area * (fx * fx + fy * fy)
+            mm += area * (fv[0] ** 2 + fv[1] ** 2)
+        den = ff * mm
+        with np.errstate(all="ignore"):
+            return np.where(den > 0.0, weight * dot * dot / np.where(den > 0.0, den, 1.0), 0.0)
+
     def run(self, engine, curl_order: int = 1) -> "Results":
         """Runs ``engine`` (built on ``self.model``) to the end criterion or
         the run length, then one step more, whose H update gives the H-type
@@ -2133,6 +2290,8 @@ class Setup:
         series = {}
         for p in self.probes:
             cols = [np.asarray(engine.samples(k)) for k in p.ops]
+            if p.purity is not None:
+                cols.append(self._purity(engine, p))
             v = np.stack(cols, axis=1)
             magnetic = p.kind in PF.MAGNETIC
             series[p.name] = v[: n + 1] if magnetic else v[:n]

@@ -33,14 +33,18 @@ TITLES = {
     "current": "current integration",
     "efield": "electric field probe",
     "hfield": "magnetic field probe",
+    "voltage_mode": "voltage mode matching",
+    "current_mode": "current mode matching",
 }
 COLUMNS = {
     "voltage": ["voltage"],
     "current": ["current"],
     "efield": ["Ex/(V/m)", "Ey/(V/m)", "Ez/(V/m)"],
     "hfield": ["Hx/(A/m)", "Hy/(A/m)", "Hz/(A/m)"],
+    "voltage_mode": ["voltage", "mode_purity"],
+    "current_mode": ["current", "mode_purity"],
 }
-MAGNETIC = {"current", "hfield"}
+MAGNETIC = {"current", "hfield", "current_mode"}
 
 
 def fmt_g(v: float, prec: int) -> str:

@@ -122,6 +122,11 @@ CASES = [
     # third-party crate not in its tree).
     ("sweep_exc_sphere", 1e-12), ("sweep_lumped_on_cyl", 1e-12), ("sweep_prim_polyhedron_cube", 1e-12),
     ("sweep_prim_stl", 5e-4),
+    # Waveguide (mode-matching) probes with openEMS's sampling and mode
+    # purity: a TE10 guide (sin, 1 and x mode functions, partial boxes,
+    # weights), a graded one (a mode function with comparisons), an iris
+    # between two ports with and without PML.
+    ("adv_wg_te10", 1e-12), ("adv_wg_graded", 1e-12), ("pml_wg_iris", 1e-12), ("e2e_waveguide_iris", 1e-12),
 ]
 NOT_PROBES = {"model.xml", "meta.txt", "console.txt", "et", "ht"}
 
