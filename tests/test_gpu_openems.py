@@ -244,6 +244,15 @@ ABC = LUMPED.replace("</Properties>", """  <AbsorbingBC Name="abc" NormalSignPos
     </Properties>""")
 
 
+# Waveguide mode probes (voltage and current, a sine and a step mode
+# function) on the lumped model's grid.
+WG = LUMPED.replace("</Properties>", """  <ProbeBox Name="wv" Type="10" Weight="2" NormDir="2"><Attributes ModeFunctionX="0" ModeFunctionY="sin(3.14159265*x/16)" ModeFunctionZ="0"/>
+        <Primitives><Box Priority="0"><P1 X="0" Y="0" Z="7"/><P2 X="16" Y="13" Z="7"/></Box></Primitives></ProbeBox>
+      <ProbeBox Name="wi" Type="11" Weight="-1" NormDir="2"><Attributes ModeFunctionX="(y&gt;4)*(y&lt;9)" ModeFunctionY="0" ModeFunctionZ="0"/>
+        <Primitives><Box Priority="0"><P1 X="2" Y="1" Z="8"/><P2 X="14" Y="12" Z="8"/></Box></Primitives></ProbeBox>
+    </Properties>""")
+
+
 def _both(text, schedule=0):
     """Both engines on the model, in openEMS's curl order except on the
     fused and two-kernel schedules, which have only the default one."""
@@ -263,7 +272,8 @@ def _both(text, schedule=0):
     ("disp", DISP, 0), ("disp", DISP, 1), ("disp", DISP, 3), ("disp", DISP, 5),
     ("pml", PMLM, 0), ("pml", PMLM, 1), ("pml", PMLM, 4),
     ("sheet", SHEET, 0), ("sheet", SHEET, 1), ("sheet", SHEET, 3),
-    ("lumped", LUMPED, 0), ("lumped", LUMPED, 1), ("lumped", LUMPED, 3), ("abc", ABC, 0), ("abc", ABC, 1)])
+    ("lumped", LUMPED, 0), ("lumped", LUMPED, 1), ("lumped", LUMPED, 3), ("abc", ABC, 0), ("abc", ABC, 1),
+    ("wg", WG, 0), ("wg", WG, 4)])
 def test_openems_models_bit_exact(name, text, schedule):
     s, g, rg, o, ro = _both(text, schedule)
     assert s.steps > 0 and s.probes
