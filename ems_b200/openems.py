@@ -38,14 +38,16 @@ Restated from the reference:
 * the end criterion: openEMS's energy measure checked every Nyquist
   interval and after half a Gaussian's length (src/sim/mod.rs:892-930).
 
-Not restated: csx's general discretisation (primitives other than boxes,
-weighting functions, transformations, sub-cell sampling of boxes off the
-mesh lines), openEMS's f32 pole arithmetic,
-Mur faces with dispersive media, lumped elements, dumps, cylindrical
-grids.
+A ``DumpBox`` is read and named in the warnings; openEMS's dump files
+(its HDF5/VTK layout) are not written. Refused with ``NotImplementedError``:
+cylindrical grids and primitives, plane-wave excitations, curves,
+transformations of sources and probes, dispersive media on or beside a Mur
+face, lumped elements with inductors or in series on sheets, in PML layers
+or under poles, and the other cases named where they are raised.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import os
 import re
@@ -580,6 +582,7 @@ class OpenEmsFile:
     cell_constant: bool = False   # CellConstantMaterial: cell-centre materials
     f_max: float | None = None    # <FDTD f_max>: the explicit highest frequency
     notes: list = field(default_factory=list)  # warnings of the reading
+    dumps: list = field(default_factory=list)  # (name, DumpType) of the file's DumpBoxes
 
 
 def _f(x, default=None):
@@ -712,7 +715,16 @@ def parse(text: str, base_dir: str | None = None) -> OpenEmsFile:
     props = []
     notes: list[str] = []
     pr = cs.find("Properties")
+    dumps: list[tuple[str, int]] = []
     for q, el in enumerate(list(pr) if pr is not None else []):
+        if el.tag == "DumpBox":
+            # A field dump only writes files: the fields, the steps and
+            # every probe are the same with or without it. Its files are in
+            # openEMS's HDF5/VTK layout (src/io/openems/dump.rs), which this
+            # reader does not write; the run's probe files are.
+            dumps.append((el.get("Name", ""), int(float(el.get("DumpType", "0")))))
+            notes.append(f"dump {el.get('Name', '')!r}: openEMS's dump files are not written")
+            continue
         boxes = []
         only_long_cylinders = False  # a probe whose primitives openEMS writes nothing for
         prims = el.find("Primitives")
@@ -842,7 +854,7 @@ def parse(text: str, base_dir: str | None = None) -> OpenEmsFile:
                        os_ if os_ >= 2 else 4, sig, faces, mur_v, props,
                        dict(bg.attrib) if bg is not None else None,
                        fd.get("CellConstantMaterial", "0") not in ("0", "false", "False"), _f(fd.get("f_max")),
-                       notes)
+                       notes, dumps)
 
 
 # ---------------------------------------------------------------------------
@@ -1007,7 +1019,13 @@ class Setup:
             self.upml_op = m.add_openems_pml([c if k == PML_FACE else 0 for k, c in f.faces])
             self.upml_h = m.upml_table(self.upml_op)[1]
         self._lumped(m)
+        # openEMS's Mur faces take the interior neighbours before the
+        # dispersive correction of their update: the Mur operator is
+        # registered before the poles (src/compile/mod.rs:1258-1263).
+        self.excited = self._excitation_edges()
+        self._mur(m)
         self._dispersive(m)
+        self._refuse_poles_beside_mur(m)
         steps = f.max_steps
         if f.max_time is not None and f.max_time > 0:
             steps = min(steps, int(math.floor(f.max_time / dt)))
@@ -1015,8 +1033,6 @@ class Setup:
         self.criterion = f.end_criteria
         self.model = m
         self.h_sources = []
-        self.excited = self._excitation_edges()
-        self._mur(m)
         self._absorbing_sheets(m)
         self._excitations(m)
         self.probes: list[ProbeSpec] = []
@@ -1526,8 +1542,6 @@ class Setup:
                 self._sheet_poles(d)
                 m.add_dispersive(d, OPENEMS_POLES)
             return
-        if any(k == MUR_FACE for k, _ in f.faces):
-            raise NotImplementedError("Mur faces with dispersive materials (openEMS's Mur reads before the poles)")
         lines, n = f.lines, self.nodes
         co = [m.coeff(lane) for lane in (3, 4, 5, 9, 10, 11)]
         d = Dispersive()
@@ -1795,6 +1809,34 @@ class Setup:
         self._mur_media(m, [fc for fc, v in faces.items() if v is None])
         m.add_mur(faces, hold=hold, flags=MUR_COUNT_ENERGY | MUR_OPENEMS_CORNERS | MUR_OPENEMS_ORDER)
 
+    def _refuse_poles_beside_mur(self, m):
+        """openEMS's Mur faces take the interior neighbours before the
+        poles' correction of their update (src/compile/mod.rs:1258-1263),
+        an interplay not restated here: E pole edges on a Mur face plane or
+        on the plane inside it (tangential to the face) are refused."""
+        from . import OP_POLES, EngineDesc, OpEntry, PolesTable
+        mur = [fc for fc, (k, _) in enumerate(self.file.faces) if k == MUR_FACE]
+        d = EngineDesc.from_address(m.desc)
+        if not mur or not d.n_ops:
+            return
+        n = self.nodes
+        for o in (OpEntry * d.n_ops).from_address(d.ops):
+            if o.kind != OP_POLES:
+                continue
+            pe = PolesTable.from_address(o.table).electric
+            ne = int(pe.n_edges)
+            if not ne:
+                continue
+            flat = np.ctypeslib.as_array((ctypes.c_uint64 * ne).from_address(pe.node)).astype(np.int64)
+            axis = np.ctypeslib.as_array((ctypes.c_uint8 * ne).from_address(pe.axis))
+            ijk = (flat // (n[1] * n[2]), (flat // n[2]) % n[1], flat % n[2])
+            for fc in mur:
+                fa = fc // 2
+                plane = n[fa] - 1 if fc % 2 else 0
+                if np.any((np.abs(ijk[fa] - plane) <= 1) & (axis != fa)):
+                    raise NotImplementedError("dispersive media on or beside a Mur face (openEMS's Mur reads the "
+                                              "interior neighbours before the poles' correction)")
+
     def _absorbing_sheets(self, m):
         """csx ``AbsorbingBC`` properties (src/compile/mod.rs:106-125,
         1999-2080, 1424-1432): every box, snapped to the nearest mesh lines,
@@ -1925,6 +1967,19 @@ class Setup:
                     tau = t_of(s) - shift
                     amp[s] = 0.0 if tau < -0.25 * dt else f.signal.value(tau, dt)
                 m.add_source_table(kind, edges, amp)
+                if kind == HARD_E:
+                    # openEMS's hard E source edges have no update of their
+                    # own: the operators acting after the update (its Mur
+                    # faces) read them as 0 before the source writes
+                    # (src/sim/map.rs:1007-1027). Not in its PML layers,
+                    # whose update is completed there.
+                    in_pml = set()
+                    if self.upml_op is not None:
+                        ax, nodes, _ = m.upml_table(self.upml_op)[0]
+                        in_pml = {(int(a), *map(int, nd)) for a, nd in zip(ax, nodes)}
+                    for a, node, _ in edges:
+                        if (a, *node) not in in_pml:
+                            m.zero_edges(0, a, node, node)
                 if typ in (2, 3):
                     self.h_sources.append((typ == 3, edges, amp.astype(np.float32)))
 
@@ -2332,7 +2387,9 @@ class Results:
         nyq = s.file.signal.nyquist_interval(dt)
         out = {}
         for p in s.probes:
-            os_ = p.oversampling if (p.oversampling or 0) >= 2 else s.file.oversampling
+            # The probe's own OverSampling, when set, replaces the <FDTD> one
+            # (src/sim/results.rs:616-625).
+            os_ = max(1, p.oversampling) if p.oversampling is not None else s.file.oversampling
             kt = max(1, nyq // os_)
             rows = self.rows(p)
             out[p.name] = PF.ProbeFile("time", p.kind, [[t] + list(x) for st, t, x in rows if st % kt == 0],
